@@ -1,0 +1,1299 @@
+// hfg_kernels.cu -- sm_100a kernels of the grid half of the hybrid fluid step.
+//
+// Every kernel restates one stage of the reference engine's CUDA code
+// (junwei-jiang/Hybrid-Fluid-Simulation, MPhysics/) in a B200-first shape:
+// grid-stride launches sized to the SM count, fused stages, uint8 cell
+// markers, FP64 deterministic reductions and device-resident solver scalars.
+// The reference line each kernel follows is cited beside it.
+#include <cstdio>
+
+#include "hfg_kernels.h"
+
+namespace hfg {
+
+namespace {
+int g_numSMs = 0;
+constexpr int kThreads = 256;
+constexpr int kCgBlocksPerSM = 4;
+
+inline int gridFor(long long n, int threads = kThreads, int perSM = 16) {
+  long long b = (n + threads - 1) / threads;
+  long long cap = (long long)numSMs() * perSM;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+// Grid-stride loop over [0, n).
+#define HFG_FOR(i, n) \
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += (long long)gridDim.x * blockDim.x)
+
+__device__ inline void cellCoord(long long c, const Dim3i& r, int& x, int& y, int& z) {
+  x = (int)(c % r.x);
+  long long t = c / r.x;
+  y = (int)(t % r.y);
+  z = (int)(t / r.y);
+}
+
+// Sum two doubles over the block (fixed tree => deterministic).  Result valid
+// in thread 0.
+__device__ inline void blockSum2(double& a, double& b) {
+  __shared__ double sa[32], sb[32];
+  a = warpSumD(a);
+  b = warpSumD(b);
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) { sa[w] = a; sb[w] = b; }
+  __syncthreads();
+  int nw = blockDim.x >> 5;
+  if (w == 0) {
+    a = lane < nw ? sa[lane] : 0.0;
+    b = lane < nw ? sb[lane] : 0.0;
+    a = warpSumD(a);
+    b = warpSumD(b);
+  }
+  __syncthreads();
+}
+
+// Publish this block's two partial sums; returns true in the one block that
+// finishes last, after which `a`, `b` (thread 0) hold the grid totals summed
+// in a fixed order.
+__device__ inline bool gridSum2(double& a, double& b, double* partials, unsigned int* ticket) {
+  __shared__ bool isLast;
+  blockSum2(a, b);
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = a;
+    partials[2 * blockIdx.x + 1] = b;
+    __threadfence();
+    unsigned int t = atomicAdd(ticket, 1u);
+    isLast = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!isLast) return false;
+  __threadfence();
+  double sa = 0.0, sb = 0.0;
+  for (unsigned int i = threadIdx.x; i < gridDim.x; i += blockDim.x) {
+    sa += __ldcg(partials + 2 * i);
+    sb += __ldcg(partials + 2 * i + 1);
+  }
+  blockSum2(sa, sb);
+  a = sa;
+  b = sb;
+  return true;
+}
+}  // namespace
+
+int numSMs() {
+  if (g_numSMs == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&g_numSMs, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || g_numSMs <= 0)
+      g_numSMs = 148;
+  }
+  return g_numSMs;
+}
+
+int cgPartialsNeeded() { return 2 * numSMs() * kCgBlocksPerSM; }
+
+// ===========================================================================
+// Boundaries and classification
+// ===========================================================================
+
+// Boundary.cpp:129-146 + BoundaryTool.cu:3-26,85-113: re-sample every solid
+// SDF at (cell centre + translation) and keep the first solid that contains
+// the cell.  solidIdx = 0 outside every solid, i+1 inside solid i.
+__global__ void kSolidClassify(Geom g, BoundarySet b, uint8_t* __restrict__ solidIdx, float* const* curSDF) {
+  long long n = g.r.size();
+  HFG_FOR(c, n) {
+    int x, y, z;
+    cellCoord(c, g.r, x, y, z);
+    float cx = __fadd_rn(__fadd_rn(g.ox, 0.5f * g.hx), __fmul_rn(g.hx, (float)x));
+    float cy = __fadd_rn(__fadd_rn(g.oy, 0.5f * g.hy), __fmul_rn(g.hy, (float)y));
+    float cz = __fadd_rn(__fadd_rn(g.oz, 0.5f * g.hz), __fmul_rn(g.hz, (float)z));
+    uint8_t idx = 0;
+    for (int i = 0; i < b.n; ++i) {
+      float v = trilerp(b.sdf[i], g, __fadd_rn(cx, b.tx[i]), __fadd_rn(cy, b.ty[i]), __fadd_rn(cz, b.tz[i]));
+      if (curSDF && curSDF[i]) curSDF[i][c] = v;
+      if (idx == 0 && v < 0.f) idx = (uint8_t)(i + 1);
+    }
+    solidIdx[c] = idx;
+  }
+}
+
+cudaError_t launchSolidClassify(const Geom& g, const BoundarySet& b, uint8_t* solidIdx, float* const* curSDF,
+                                cudaStream_t s) {
+  kSolidClassify<<<gridFor(g.r.size()), kThreads, 0, s>>>(g, b, solidIdx, curSDF);
+  return cudaGetLastError();
+}
+
+__global__ void kSolidFromSDF(long long n, const float* __restrict__ sdf, uint8_t* __restrict__ idx) {
+  HFG_FOR(c, n) idx[c] = sdf[c] < 0.f ? 1 : 0;
+}
+cudaError_t launchSolidFromSDF(long long n, const float* solidSDF, uint8_t* solidIdx, cudaStream_t s) {
+  kSolidFromSDF<<<gridFor(n), kThreads, 0, s>>>(n, solidSDF, solidIdx);
+  return cudaGetLastError();
+}
+
+// The reference's "total boundary SDF" (BoundaryTool.cu:3-26): 0 everywhere
+// with no solid, else -(first solid index) inside and UNKNOWN outside.
+__global__ void kTotalSolidSDF(long long n, int nb, const uint8_t* __restrict__ idx, float* __restrict__ out) {
+  HFG_FOR(c, n) {
+    uint8_t i = idx[c];
+    out[c] = nb == 0 ? 0.f : (i ? -(float)i : kUnknown);
+  }
+}
+cudaError_t launchTotalSolidSDF(long long n, int nb, const uint8_t* solidIdx, float* out, cudaStream_t s) {
+  kTotalSolidSDF<<<gridFor(n), kThreads, 0, s>>>(n, nb, solidIdx, out);
+  return cudaGetLastError();
+}
+
+// Solid face velocity of a face between cells lo (index i-1) and hi (index i)
+// on `axis`: the six faces of a solid cell carry its solid's velocity
+// (BoundaryTool.cu:28-83).  Where two different solids meet the reference
+// races; the higher cell wins here.
+__device__ inline float solidFaceVel(const SolidVelTable& t, uint8_t lo, uint8_t hi, int axis) {
+  uint8_t s = hi ? hi : lo;
+  if (!s) return 0.f;
+  return axis == 0 ? t.vx[s - 1] : (axis == 1 ? t.vy[s - 1] : t.vz[s - 1]);
+}
+
+__global__ void kSolidVelField(Geom g, SolidVelTable t, FaceField out) {
+  for (int a = 0; a < 3; ++a) {
+    Dim3i fr = g.r;
+    if (a == 0) fr.x += 1;
+    if (a == 1) fr.y += 1;
+    if (a == 2) fr.z += 1;
+    long long n = fr.size();
+    HFG_FOR(f, n) {
+      int x, y, z;
+      cellCoord(f, fr, x, y, z);
+      int hx = x, hy = y, hz = z, lx = x, ly = y, lz = z;
+      if (a == 0) lx = x - 1;
+      if (a == 1) ly = y - 1;
+      if (a == 2) lz = z - 1;
+      bool hiIn = (a == 0 ? hx < g.r.x : (a == 1 ? hy < g.r.y : hz < g.r.z));
+      bool loIn = (a == 0 ? lx >= 0 : (a == 1 ? ly >= 0 : lz >= 0));
+      uint8_t hi = hiIn ? t.solidIdx[((long long)hz * g.r.y + hy) * g.r.x + hx] : 0;
+      uint8_t lo = loIn ? t.solidIdx[((long long)lz * g.r.y + ly) * g.r.x + lx] : 0;
+      out.c[a][f] = solidFaceVel(t, lo, hi, a);
+    }
+  }
+}
+cudaError_t launchSolidVelField(const Geom& g, const SolidVelTable& t, FaceField out, cudaStream_t s) {
+  kSolidVelField<<<gridFor(g.r.size()), kThreads, 0, s>>>(g, t, out);
+  return cudaGetLastError();
+}
+
+__global__ void kMarkersInit(long long n, const uint8_t* __restrict__ idx, uint8_t* __restrict__ mk) {
+  HFG_FOR(c, n) mk[c] = idx[c] ? kSolid : kAir;
+}
+cudaError_t launchMarkersInit(long long n, const uint8_t* solidIdx, uint8_t* markers, cudaStream_t s) {
+  kMarkersInit<<<gridFor(n), kThreads, 0, s>>>(n, solidIdx, markers);
+  return cudaGetLastError();
+}
+
+// EulerParticlesTool.cu:27-77: a non-solid cell holding at least one particle
+// (truncating binning) is fluid.  Only "count > 0" matters, so the count is
+// replaced by an idempotent store; cells stay bit-exact.
+__global__ void kMarkersFromParticles(Geom g, const float* __restrict__ pos, long long P, uint8_t* __restrict__ mk) {
+  HFG_FOR(p, P) {
+    long long c = binCell(g, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]);
+    if (mk[c] == kAir) mk[c] = kFluid;
+  }
+}
+cudaError_t launchMarkersFromParticles(const Geom& g, const float* pos, long long P, uint8_t* markers, cudaStream_t s) {
+  if (P <= 0) return cudaSuccess;
+  kMarkersFromParticles<<<gridFor(P), kThreads, 0, s>>>(g, pos, P, markers);
+  return cudaGetLastError();
+}
+
+// statisticalFluidDensity (EulerParticlesTool.cu:27-46) with warp-aggregated
+// integer atomics: lanes that hit the same cell add once.
+__global__ void kBinCounts(Geom g, const float* __restrict__ pos, long long P, unsigned int* __restrict__ counts) {
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < P; base += (long long)gridDim.x * blockDim.x) {
+    long long p = base + threadIdx.x;
+    bool valid = p < P;
+    unsigned int active = __ballot_sync(0xffffffffu, valid);
+    if (!valid) continue;
+    long long c = binCell(g, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]);
+    unsigned int peers = __match_any_sync(active, c);
+    int leader = __ffs(peers) - 1;
+    if ((int)(threadIdx.x & 31) == leader) atomicAdd(counts + c, (unsigned int)__popc(peers));
+  }
+}
+cudaError_t launchBinCounts(const Geom& g, const float* pos, long long P, unsigned int* counts, cudaStream_t s) {
+  if (P <= 0) return cudaSuccess;
+  kBinCounts<<<gridFor(P), kThreads, 0, s>>>(g, pos, P, counts);
+  return cudaGetLastError();
+}
+
+// EulerSolverTool.cu:30-56 buildFluidMarkers (SDF form)
+__global__ void kMarkersFromSDF(long long n, const uint8_t* __restrict__ idx, const float* __restrict__ fsdf,
+                                uint8_t* __restrict__ mk) {
+  HFG_FOR(c, n) mk[c] = idx[c] ? kSolid : (fsdf[c] < 0.f ? kFluid : kAir);
+}
+cudaError_t launchMarkersFromSDF(long long n, const uint8_t* solidIdx, const float* fluidSDF, uint8_t* markers,
+                                 cudaStream_t s) {
+  kMarkersFromSDF<<<gridFor(n), kThreads, 0, s>>>(n, solidIdx, fluidSDF, markers);
+  return cudaGetLastError();
+}
+
+// EulerSolverTool.cu:581-608 generateFluidDomainFromBBox (strict inequalities,
+// every cell rewritten).
+__global__ void kFluidDomainFromBBox(Geom g, float mnx, float mny, float mnz, float mxx, float mxy, float mxz,
+                                     float* __restrict__ out) {
+  HFG_FOR(c, g.r.size()) {
+    int x, y, z;
+    cellCoord(c, g.r, x, y, z);
+    float cx = __fadd_rn(__fadd_rn(g.ox, 0.5f * g.hx), __fmul_rn(g.hx, (float)x));
+    float cy = __fadd_rn(__fadd_rn(g.oy, 0.5f * g.hy), __fmul_rn(g.hy, (float)y));
+    float cz = __fadd_rn(__fadd_rn(g.oz, 0.5f * g.hz), __fmul_rn(g.hz, (float)z));
+    bool in = cx > mnx && cy > mny && cz > mnz && cx < mxx && cy < mxy && cz < mxz;
+    out[c] = in ? -500.f : 500.f;  // FluidDomainValue (Common.h:245)
+  }
+}
+cudaError_t launchFluidDomainFromBBox(const Geom& g, const float mn[3], const float mx[3], float* out, cudaStream_t s) {
+  kFluidDomainFromBBox<<<gridFor(g.r.size()), kThreads, 0, s>>>(g, mn[0], mn[1], mn[2], mx[0], mx[1], mx[2], out);
+  return cudaGetLastError();
+}
+
+// ===========================================================================
+// Pressure projection: matrix-free 7-point Poisson from a one-byte stencil code
+// ===========================================================================
+//
+// code bit 0: the cell is fluid; bits 1..6: the left, right, down, up, back,
+// front neighbour lies inside the grid and is not solid.  This is everything
+// buildPressureMatrixA (EulerSolverTool.cu:58-126) derives from the markers,
+// so A is never stored (the reference keeps 4 floats per cell).
+
+__global__ void kStencilCode(Dim3i r, const uint8_t* __restrict__ mk, uint8_t* __restrict__ code) {
+  HFG_FOR(c, r.size()) {
+    int x, y, z;
+    cellCoord(c, r, x, y, z);
+    uint8_t m = mk[c];
+    uint8_t k = 0;
+    if (m == kFluid) {
+      k = 1;
+      long long sy = r.x, sz = (long long)r.x * r.y;
+      if (x > 0 && mk[c - 1] != kSolid) k |= 2;
+      if (x + 1 < r.x && mk[c + 1] != kSolid) k |= 4;
+      if (y > 0 && mk[c - sy] != kSolid) k |= 8;
+      if (y + 1 < r.y && mk[c + sy] != kSolid) k |= 16;
+      if (z > 0 && mk[c - sz] != kSolid) k |= 32;
+      if (z + 1 < r.z && mk[c + sz] != kSolid) k |= 64;
+    }
+    code[c] = k;
+  }
+}
+cudaError_t launchStencilCode(const Dim3i& r, const uint8_t* markers, uint8_t* code, cudaStream_t s) {
+  kStencilCode<<<gridFor(r.size()), kThreads, 0, s>>>(r, markers, code);
+  return cudaGetLastError();
+}
+
+// Diagonal in the reference's accumulation order (EulerSolverTool.cu:85-120).
+__device__ inline float diagOf(uint8_t k, float sx, float sy, float sz) {
+  if (!(k & 1)) return 1.f;
+  float d = 0.f;
+  if (k & 2) d += sx;
+  if (k & 4) d += sx;
+  if (k & 8) d += sy;
+  if (k & 16) d += sy;
+  if (k & 32) d += sz;
+  if (k & 64) d += sz;
+  return d;
+}
+
+__global__ void kMatrixA(Dim3i r, float sx, float sy, float sz, const uint8_t* __restrict__ code, float* __restrict__ A) {
+  HFG_FOR(c, r.size()) {
+    int x, y, z;
+    cellCoord(c, r, x, y, z);
+    uint8_t k = code[c];
+    float a0 = diagOf(k, sx, sy, sz), a1 = 0.f, a2 = 0.f, a3 = 0.f;
+    if (k & 1) {
+      long long sy_ = r.x, sz_ = (long long)r.x * r.y;
+      if ((k & 4) && (code[c + 1] & 1)) a1 = -sx;
+      if ((k & 16) && (code[c + sy_] & 1)) a2 = -sy;
+      if ((k & 64) && (code[c + sz_] & 1)) a3 = -sz;
+    }
+    A[4 * c] = a0; A[4 * c + 1] = a1; A[4 * c + 2] = a2; A[4 * c + 3] = a3;
+  }
+}
+cudaError_t launchMatrixA(const Dim3i& r, float sx, float sy, float sz, const uint8_t* code, float* A, cudaStream_t s) {
+  kMatrixA<<<gridFor(r.size()), kThreads, 0, s>>>(r, sx, sy, sz, code, A);
+  return cudaGetLastError();
+}
+
+// Neighbour offsets of one cell; a neighbour counts when it is inside the grid
+// and fluid (off-diagonal -s of fdmMatrixVectorMul, EulerSolverTool.cu:219-226;
+// products in float, sum in double as the reference's ternaries do).
+struct Nbr {
+  long long o[6];
+  bool in[6];
+};
+__device__ inline void neighbours(long long c, int x, int y, int z, const Dim3i& r, Nbr& n) {
+  long long sy = r.x, sz = (long long)r.x * r.y;
+  n.in[0] = x > 0; n.o[0] = c - 1;
+  n.in[1] = x + 1 < r.x; n.o[1] = c + 1;
+  n.in[2] = y > 0; n.o[2] = c - sy;
+  n.in[3] = y + 1 < r.y; n.o[3] = c + sy;
+  n.in[4] = z > 0; n.o[4] = c - sz;
+  n.in[5] = z + 1 < r.z; n.o[5] = c + sz;
+}
+
+template <class PF>
+__device__ inline float applyAAt(long long c, uint8_t k, const Nbr& n, const uint8_t* __restrict__ code, float sx,
+                                 float sy, float sz, PF pval) {
+  float pc = pval(c);
+  if (!(k & 1)) return pc;
+  double acc = (double)__fmul_rn(diagOf(k, sx, sy, sz), pc);
+  const float s[6] = {-sx, -sx, -sy, -sy, -sz, -sz};
+#pragma unroll
+  for (int d = 0; d < 6; ++d)
+    if (n.in[d] && (__ldg(code + n.o[d]) & 1)) acc += (double)__fmul_rn(s[d], pval(n.o[d]));
+  return (float)acc;
+}
+
+__global__ void kApplyA(Dim3i r, float sx, float sy, float sz, const uint8_t* __restrict__ code,
+                        const float* __restrict__ xin, float* __restrict__ y) {
+  HFG_FOR(c, r.size()) {
+    int x, yy, z;
+    cellCoord(c, r, x, yy, z);
+    Nbr n;
+    neighbours(c, x, yy, z, r, n);
+    y[c] = applyAAt(c, code[c], n, code, sx, sy, sz, [&](long long i) { return __ldg(xin + i); });
+  }
+}
+cudaError_t launchApplyA(const Dim3i& r, float sx, float sy, float sz, const uint8_t* code, const float* x, float* y,
+                         cudaStream_t s) {
+  kApplyA<<<gridFor(r.size()), kThreads, 0, s>>>(r, sx, sy, sz, code, x, y);
+  return cudaGetLastError();
+}
+
+__device__ inline bool cgStop(const CgState* st, double rr) {
+  double rn = sqrt(rr);
+  if (st->tolMode == 0) return sqrt(rn) < st->tol;  // CuMatrixFreePCG.cpp:28,51
+  double bn = sqrt(st->bb);
+  return bn == 0.0 || rn / bn < st->tol;
+}
+
+__device__ inline float precondZ(int precond, uint8_t k, float rv, float sx, float sy, float sz) {
+  if (precond == 1) return __fdiv_rn(rv, diagOf(k, sx, sy, sz));
+  return rv;
+}
+
+// Divergence + solid terms (FieldMathTool.cu:370-395, EulerSolverTool.cu:128-197)
+// fused with the CG set-up of CuMatrixFreePCG.cpp:22-37 (x0 = 0 so r = b).
+__global__ void kRhsInit(Geom g, ConstFaceField v, ConstFaceField svArr, SolidVelTable svTab,
+                         const uint8_t* __restrict__ mk, const uint8_t* __restrict__ code, float sAx, float sAy,
+                         float sAz, float* __restrict__ bOut, float* __restrict__ r, float* __restrict__ x,
+                         float* __restrict__ p, double* partials, CgState* st) {
+  const Dim3i R = g.r;
+  const Dim3i rx{R.x + 1, R.y, R.z}, ry{R.x, R.y + 1, R.z}, rz{R.x, R.y, R.z + 1};
+  const float ix = 1.0f / g.hx, iy = 1.0f / g.hy, iz = 1.0f / g.hz;
+  const int pcd = st->precond;
+  double bb = 0.0, rzs = 0.0;
+  HFG_FOR(c, R.size()) {
+    int x0, y0, z0;
+    cellCoord(c, R, x0, y0, z0);
+    float b = 0.f;
+    if (mk[c] == kFluid) {
+      long long uL = ((long long)z0 * rx.y + y0) * rx.x + x0, uR = uL + 1;
+      long long vD = ((long long)z0 * ry.y + y0) * ry.x + x0, vU = vD + ry.x;
+      long long wB = ((long long)z0 * rz.y + y0) * rz.x + x0, wF = wB + (long long)rz.x * rz.y;
+      float L = v.c[0][uL], Rr = v.c[0][uR], D = v.c[1][vD], U = v.c[1][vU], B = v.c[2][wB], F = v.c[2][wF];
+      float div = __fadd_rn(__fadd_rn(__fdiv_rn(__fsub_rn(Rr, L), g.hx), __fdiv_rn(__fsub_rn(U, D), g.hy)),
+                            __fdiv_rn(__fsub_rn(F, B), g.hz));
+      b = -div;
+      long long sy = R.x, sz = (long long)R.x * R.y;
+      uint8_t me = svTab.solidIdx ? svTab.solidIdx[c] : 0;
+      auto sv = [&](int axis, long long f, long long nb, bool nbIsHi) -> float {
+        if (svArr.c[0]) return svArr.c[axis][f];
+        uint8_t o = svTab.solidIdx[nb];
+        return nbIsHi ? solidFaceVel(svTab, me, o, axis) : solidFaceVel(svTab, o, me, axis);
+      };
+      long long cl = x0 > 0 ? c - 1 : c, cr = x0 + 1 < R.x ? c + 1 : c;
+      long long cd = y0 > 0 ? c - sy : c, cu = y0 + 1 < R.y ? c + sy : c;
+      long long cb = z0 > 0 ? c - sz : c, cf = z0 + 1 < R.z ? c + sz : c;
+      if (mk[cl] == kSolid) b = __fsub_rn(b, __fmul_rn(ix, __fsub_rn(L, sv(0, uL, cl, false))));
+      if (mk[cr] == kSolid) b = __fadd_rn(b, __fmul_rn(ix, __fsub_rn(Rr, sv(0, uR, cr, true))));
+      if (mk[cd] == kSolid) b = __fsub_rn(b, __fmul_rn(iy, __fsub_rn(D, sv(1, vD, cd, false))));
+      if (mk[cu] == kSolid) b = __fadd_rn(b, __fmul_rn(iy, __fsub_rn(U, sv(1, vU, cu, true))));
+      if (mk[cb] == kSolid) b = __fsub_rn(b, __fmul_rn(iz, __fsub_rn(B, sv(2, wB, cb, false))));
+      if (mk[cf] == kSolid) b = __fadd_rn(b, __fmul_rn(iz, __fsub_rn(F, sv(2, wF, cf, true))));
+    }
+    if (bOut) bOut[c] = b;
+    r[c] = b;
+    x[c] = 0.f;
+    p[c] = 0.f;
+    float zz = precondZ(pcd, code[c], b, sAx, sAy, sAz);
+    bb += (double)b * (double)b;
+    rzs += (double)b * (double)zz;
+  }
+  if (gridSum2(bb, rzs, partials, &st->ticket) && threadIdx.x == 0) {
+    st->bb = bb;
+    st->rr = bb;
+    st->rz = rzs;
+    st->iter = 0;
+    st->beta = 0.f;
+    st->alpha = 0.f;
+    st->done = cgStop(st, bb) || st->maxIter <= 0;  // CuMatrixFreePCG.cpp:28-32
+    st->ticket = 0;
+  }
+}
+cudaError_t launchRhsInit(const Geom& g, ConstFaceField v, ConstFaceField svArr, const SolidVelTable& svTab,
+                          const uint8_t* markers, const uint8_t* code, float ax, float ay, float az, float* b,
+                          float* r, float* x, float* p, double* partials, CgState* st, cudaStream_t s) {
+  kRhsInit<<<numSMs() * kCgBlocksPerSM, kThreads, 0, s>>>(g, v, svArr, svTab, markers, code, ax, ay, az, b, r, x, p,
+                                                          partials, st);
+  return cudaGetLastError();
+}
+
+// One CG direction update p = z + beta*p (scal, then axpy with 1) fused with
+// q = A p and the reduction p.q; the last block forms alpha = r.z / p.Ap
+// (CuMatrixFreePCG.cpp:40-47).  z and p at the six neighbours are recomputed
+// from r and the previous p, so q is never written to memory.
+__global__ void __launch_bounds__(kThreads) kCgDirection(Dim3i R, float sx, float sy, float sz,
+                                                         const uint8_t* __restrict__ code, const float* __restrict__ r,
+                                                         const float* __restrict__ pOld, float* __restrict__ pNew,
+                                                         double* partials, CgState* st) {
+  if (st->done) return;
+  const float beta = st->beta;
+  const int pcd = st->precond;
+  double pq = 0.0, dummy = 0.0;
+  auto pn = [&](long long i) -> float {
+    float z = precondZ(pcd, __ldg(code + i), __ldg(r + i), sx, sy, sz);
+    return __fadd_rn(__fmul_rn(beta, __ldg(pOld + i)), z);
+  };
+  HFG_FOR(c, R.size()) {
+    int x, y, z;
+    cellCoord(c, R, x, y, z);
+    Nbr n;
+    neighbours(c, x, y, z, R, n);
+    uint8_t k = __ldg(code + c);
+    float pc = pn(c);
+    float q = applyAAt(c, k, n, code, sx, sy, sz, pn);
+    pNew[c] = pc;
+    pq += (double)pc * (double)q;
+  }
+  if (gridSum2(pq, dummy, partials, &st->ticket) && threadIdx.x == 0) {
+    st->pAp = pq;
+    st->alpha = (float)(st->rz / pq);
+    st->ticket = 0;
+  }
+}
+cudaError_t launchCgDirection(const Dim3i& r, float sx, float sy, float sz, const uint8_t* code, const float* rr,
+                              const float* pOld, float* pNew, double* partials, CgState* st, cudaStream_t s) {
+  kCgDirection<<<numSMs() * kCgBlocksPerSM, kThreads, 0, s>>>(r, sx, sy, sz, code, rr, pOld, pNew, partials, st);
+  return cudaGetLastError();
+}
+
+// x += alpha p, r -= alpha A p (A p recomputed), then z = M^-1 r and the
+// reductions r.r and r.z; the last block checks convergence and forms beta
+// (CuMatrixFreePCG.cpp:49-63).  The |alpha| < FLT_EPSILON skip of
+// CCuDenseVector::plusAlphaX (CuDenseVector.cpp:178) is kept.
+__global__ void __launch_bounds__(kThreads) kCgUpdate(Dim3i R, float sx, float sy, float sz,
+                                                      const uint8_t* __restrict__ code, const float* __restrict__ p,
+                                                      float* __restrict__ x, float* __restrict__ r, double* partials,
+                                                      CgState* st) {
+  if (st->done) return;
+  const float alpha = st->alpha;
+  const int pcd = st->precond;
+  const bool skip = fabsf(alpha) < FLT_EPSILON;
+  double rr = 0.0, rz = 0.0;
+  HFG_FOR(c, R.size()) {
+    int xx, y, z;
+    cellCoord(c, R, xx, y, z);
+    uint8_t k = __ldg(code + c);
+    float rv = r[c];
+    if (!skip) {
+      Nbr n;
+      neighbours(c, xx, y, z, R, n);
+      float q = applyAAt(c, k, n, code, sx, sy, sz, [&](long long i) { return __ldg(p + i); });
+      x[c] = fmaf(alpha, __ldg(p + c), x[c]);
+      rv = fmaf(-alpha, q, rv);
+      r[c] = rv;
+    }
+    float zz = precondZ(pcd, k, rv, sx, sy, sz);
+    rr += (double)rv * (double)rv;
+    rz += (double)rv * (double)zz;
+  }
+  if (gridSum2(rr, rz, partials, &st->ticket) && threadIdx.x == 0) {
+    st->rr = rr;
+    st->iter += 1;
+    bool stop = cgStop(st, rr);
+    st->beta = (float)(rz / st->rz);
+    st->rz = rz;
+    st->done = stop || st->iter >= st->maxIter;
+    st->ticket = 0;
+  }
+}
+cudaError_t launchCgUpdate(const Dim3i& r, float sx, float sy, float sz, const uint8_t* code, const float* p,
+                           float* x, float* rr, double* partials, CgState* st, cudaStream_t s) {
+  kCgUpdate<<<numSMs() * kCgBlocksPerSM, kThreads, 0, s>>>(r, sx, sy, sz, code, p, x, rr, partials, st);
+  return cudaGetLastError();
+}
+
+// EulerSolverTool.cu:229-322 applyPressureGradient: faces with a fluid side
+// and a solid side take the solid velocity, fluid-fluid/fluid-air faces get
+// -dt/(rho h) * dp, all others and the far boundary faces become UNKNOWN.
+__global__ void kGradient(Geom g, float gx, float gy, float gz, const uint8_t* __restrict__ mk,
+                          const float* __restrict__ p, FaceField v, ConstFaceField svArr, SolidVelTable svTab) {
+  const Dim3i R = g.r;
+  const Dim3i rx{R.x + 1, R.y, R.z}, ry{R.x, R.y + 1, R.z}, rz{R.x, R.y, R.z + 1};
+  HFG_FOR(c, R.size()) {
+    int x, y, z;
+    cellCoord(c, R, x, y, z);
+    long long sy = R.x, sz = (long long)R.x * R.y;
+    long long cl = x > 0 ? c - 1 : c, cd = y > 0 ? c - sy : c, cb = z > 0 ? c - sz : c;
+    uint8_t mc = mk[c];
+    long long fx = ((long long)z * rx.y + y) * rx.x + x;
+    long long fy = ((long long)z * ry.y + y) * ry.x + x;
+    long long fz = ((long long)z * rz.y + y) * rz.x + x;
+    const long long fo[3] = {fx, fy, fz};
+    const long long co[3] = {cl, cd, cb};
+    const float gs[3] = {gx, gy, gz};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      uint8_t ml = mk[co[a]];
+      float* vv = v.c[a];
+      if (ml == kFluid || mc == kFluid) {
+        if (ml == kSolid || mc == kSolid) {
+          float s;
+          if (svArr.c[0]) s = svArr.c[a][fo[a]];
+          else s = solidFaceVel(svTab, co[a] == c ? 0 : svTab.solidIdx[co[a]], svTab.solidIdx[c], a);
+          vv[fo[a]] = s;
+        } else {
+          vv[fo[a]] = __fsub_rn(vv[fo[a]], __fmul_rn(gs[a], __fsub_rn(p[c], p[co[a]])));
+        }
+      } else {
+        vv[fo[a]] = kUnknown;
+      }
+    }
+    if (x == R.x - 1) v.c[0][fx + 1] = kUnknown;
+    if (y == R.y - 1) v.c[1][fy + ry.x] = kUnknown;
+    if (z == R.z - 1) v.c[2][fz + (long long)rz.x * rz.y] = kUnknown;
+  }
+}
+cudaError_t launchGradient(const Geom& g, float gx, float gy, float gz, const uint8_t* markers, const float* p,
+                           FaceField v, ConstFaceField svArr, const SolidVelTable& svTab, cudaStream_t s) {
+  kGradient<<<gridFor(g.r.size()), kThreads, 0, s>>>(g, gx, gy, gz, markers, p, v, svArr, svTab);
+  return cudaGetLastError();
+}
+
+// ===========================================================================
+// Extrapolation (EulerSolverTool.cu:450-557, :904-969)
+// ===========================================================================
+//
+// The reference grows UNKNOWN entries layer by layer from the known ones with
+// 6-neighbour clamp-to-edge steps, 999 layers at most, then sets every layer-d
+// entry to the mean of its neighbours of smaller layer.  Without obstacles the
+// layer of an entry equals its L1 distance to the nearest known entry, so the
+// layers come from a separable exact L1 distance transform (three 1-D min-plus
+// passes); entries are then bucketed by layer and each layer is one launch.
+
+constexpr uint16_t kFar = 0xFFFF;
+
+__global__ void kDistInit(long long n, const float* __restrict__ v, uint16_t* __restrict__ d) {
+  HFG_FOR(i, n) d[i] = (v[i] == kUnknown) ? kFar : 0;
+}
+
+__device__ inline uint16_t satInc(uint16_t a) { return a >= kFar - 1 ? kFar : (uint16_t)(a + 1); }
+
+// 1-D pass along x: one thread per row, forward then backward sweep.
+__global__ void kDistRows(Dim3i r, uint16_t* __restrict__ d) {
+  long long rows = (long long)r.y * r.z;
+  HFG_FOR(row, rows) {
+    uint16_t* q = d + row * r.x;
+    uint16_t prev = kFar;
+    for (int i = 0; i < r.x; ++i) {
+      uint16_t v = q[i];
+      uint16_t cand = satInc(prev);
+      if (cand < v) { v = cand; q[i] = v; }
+      prev = v;
+    }
+    prev = kFar;
+    for (int i = r.x - 1; i >= 0; --i) {
+      uint16_t v = q[i];
+      uint16_t cand = satInc(prev);
+      if (cand < v) { v = cand; q[i] = v; }
+      prev = v;
+    }
+  }
+}
+
+// 1-D pass along y or z: threads walk columns, coalesced across x.
+__global__ void kDistCols(Dim3i r, int axis, uint16_t* __restrict__ d) {
+  long long stride = axis == 1 ? r.x : (long long)r.x * r.y;
+  int len = axis == 1 ? r.y : r.z;
+  long long lines = axis == 1 ? (long long)r.x * r.z : (long long)r.x * r.y;
+  HFG_FOR(l, lines) {
+    long long base;
+    if (axis == 1) {
+      long long x = l % r.x, z = l / r.x;
+      base = z * r.x * (long long)r.y + x;
+    } else {
+      base = l;
+    }
+    uint16_t prev = kFar;
+    for (int i = 0; i < len; ++i) {
+      uint16_t v = d[base + i * stride];
+      uint16_t cand = satInc(prev);
+      if (cand < v) { v = cand; d[base + i * stride] = v; }
+      prev = v;
+    }
+    prev = kFar;
+    for (int i = len - 1; i >= 0; --i) {
+      uint16_t v = d[base + i * stride];
+      uint16_t cand = satInc(prev);
+      if (cand < v) { v = cand; d[base + i * stride] = v; }
+      prev = v;
+    }
+  }
+}
+
+// Histogram of layers 1..nums-1 (layers >= nums stay UNKNOWN).
+__global__ void kDistHist(long long n, const uint16_t* __restrict__ d, int nums, unsigned int* __restrict__ hist) {
+  __shared__ unsigned int sh[kMaxLayers + 1];
+  for (int i = threadIdx.x; i <= kMaxLayers; i += blockDim.x) sh[i] = 0;
+  __syncthreads();
+  HFG_FOR(i, n) {
+    uint16_t v = d[i];
+    if (v >= 1 && v < nums) atomicAdd(&sh[v], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i <= kMaxLayers; i += blockDim.x)
+    if (sh[i]) atomicAdd(hist + i, sh[i]);
+}
+
+__global__ void kExclusiveScanSmall(const unsigned int* __restrict__ hist, unsigned int* __restrict__ off,
+                                    unsigned int* __restrict__ cursor, int n) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    unsigned int s = 0;
+    for (int i = 0; i < n; ++i) { off[i] = s; cursor[i] = s; s += hist[i]; }
+    off[n] = s;
+  }
+}
+
+__global__ void kDistScatter(long long n, long long base, const uint16_t* __restrict__ d, int nums,
+                             unsigned int* __restrict__ cursor, unsigned int* __restrict__ list) {
+  HFG_FOR(i, n) {
+    uint16_t v = d[i];
+    if (v >= 1 && v < nums) {
+      unsigned int slot = atomicAdd(cursor + v, 1u);
+      list[slot] = (unsigned int)(base + i);
+    }
+  }
+}
+
+cudaError_t launchExtrapDistance(const Dim3i rc[3], float* const vals[3], long long off[3], int nums,
+                                 ExtrapScratch sc, cudaStream_t s) {
+  if (nums > kMaxLayers) nums = kMaxLayers;
+  for (int a = 0; a < 3; ++a) {
+    long long n = rc[a].size();
+    uint16_t* d = sc.dist + off[a];
+    kDistInit<<<gridFor(n), kThreads, 0, s>>>(n, vals[a], d);
+    kDistRows<<<gridFor((long long)rc[a].y * rc[a].z), kThreads, 0, s>>>(rc[a], d);
+    kDistCols<<<gridFor((long long)rc[a].x * rc[a].z), kThreads, 0, s>>>(rc[a], 1, d);
+    kDistCols<<<gridFor((long long)rc[a].x * rc[a].y), kThreads, 0, s>>>(rc[a], 2, d);
+  }
+  cudaError_t e = cudaMemsetAsync(sc.hist, 0, sizeof(unsigned int) * (kMaxLayers + 2), s);
+  if (e != cudaSuccess) return e;
+  for (int a = 0; a < 3; ++a) {
+    long long n = rc[a].size();
+    kDistHist<<<gridFor(n, kThreads, 4), kThreads, 0, s>>>(n, sc.dist + off[a], nums, sc.hist);
+  }
+  kExclusiveScanSmall<<<1, 1, 0, s>>>(sc.hist, sc.offsets, sc.cursor, kMaxLayers + 1);
+  for (int a = 0; a < 3; ++a) {
+    long long n = rc[a].size();
+    kDistScatter<<<gridFor(n), kThreads, 0, s>>>(n, off[a], sc.dist + off[a], nums, sc.cursor, sc.list);
+  }
+  return cudaGetLastError();
+}
+
+// One layer: mean of the neighbours with a smaller layer, summed in the fixed
+// order left, right, down, up, back, front (extrapolatingData).
+__global__ void kExtrapLayer(Dim3i r0, Dim3i r1, Dim3i r2, float* v0, float* v1, float* v2, long long off1,
+                             long long off2, const uint16_t* __restrict__ dist, const unsigned int* __restrict__ list,
+                             unsigned int begin, unsigned int count, int d) {
+  HFG_FOR(k, (long long)count) {
+    long long id = list[begin + k];
+    int a = id >= off2 ? 2 : (id >= off1 ? 1 : 0);
+    long long base = a == 2 ? off2 : (a == 1 ? off1 : 0);
+    long long i = id - base;
+    Dim3i r = a == 2 ? r2 : (a == 1 ? r1 : r0);
+    float* v = a == 2 ? v2 : (a == 1 ? v1 : v0);
+    const uint16_t* dd = dist + base;
+    int x, y, z;
+    cellCoord(i, r, x, y, z);
+    long long nb[6] = {linc(x - 1, y, z, r), linc(x + 1, y, z, r), linc(x, y - 1, z, r),
+                       linc(x, y + 1, z, r), linc(x, y, z - 1, r), linc(x, y, z + 1, r)};
+    float acc = 0.f, cnt = 0.f;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      if ((int)dd[nb[q]] < d) {
+        acc = __fadd_rn(acc, v[nb[q]]);
+        cnt = __fadd_rn(cnt, 1.f);
+      }
+    }
+    if (cnt != 0.f) acc = __fdiv_rn(acc, cnt);
+    v[i] = acc;
+  }
+}
+
+cudaError_t launchExtrapLayer(const Dim3i rc[3], float* const vals[3], const long long off[3], ExtrapScratch sc,
+                              unsigned int begin, unsigned int count, int d, cudaStream_t s) {
+  if (count == 0) return cudaSuccess;
+  kExtrapLayer<<<gridFor(count), kThreads, 0, s>>>(rc[0], rc[1], rc[2], vals[0], vals[1], vals[2], off[1], off[2],
+                                                    sc.dist, sc.list, begin, count, d);
+  return cudaGetLastError();
+}
+
+// ===========================================================================
+// Particles
+// ===========================================================================
+
+// Philox4x32-10 (Salmon et al., SC'11): counter-based stream shared with the
+// host so the seeding is reproducible anywhere.
+__host__ __device__ inline void philox10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+  for (int r = 0; r < 10; ++r) {
+    uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
+    uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
+    uint32_t n0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k0, n2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k1;
+    c[1] = (uint32_t)p1;
+    c[3] = (uint32_t)p0;
+    c[0] = n0;
+    c[2] = n2;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+}
+__device__ inline float unit24(uint32_t v) { return (float)(v >> 8) * (1.0f / 16777216.0f); }
+
+// EulerParticlesTool.cu:5-25 findFluidGrid: fluid SDF < 0 and not solid.
+__device__ inline bool seedCell(const float* fsdf, const uint8_t* sidx, long long c) {
+  return fsdf[c] < 0.f && !(sidx && sidx[c]);
+}
+
+__global__ void kSeedCount(long long n, const float* __restrict__ fsdf, const uint8_t* __restrict__ sidx,
+                           unsigned int* __restrict__ blockCounts, int cellsPerBlock) {
+  long long b0 = (long long)blockIdx.x * cellsPerBlock;
+  unsigned int cnt = 0;
+  for (long long c = b0 + threadIdx.x; c < b0 + cellsPerBlock && c < n; c += blockDim.x) cnt += seedCell(fsdf, sidx, c);
+  cnt = __reduce_add_sync(0xffffffffu, cnt);
+  __shared__ unsigned int s[32];
+  if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = cnt;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned int t = 0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += s[i];
+    blockCounts[blockIdx.x] = t;
+  }
+}
+cudaError_t launchSeedCount(const Dim3i& r, const float* fluidSDF, const uint8_t* solidIdx, unsigned int* blockCounts,
+                            int cellsPerBlock, cudaStream_t s) {
+  long long n = r.size();
+  int nb = (int)((n + cellsPerBlock - 1) / cellsPerBlock);
+  kSeedCount<<<nb, kThreads, 0, s>>>(n, fluidSDF, solidIdx, blockCounts, cellsPerBlock);
+  return cudaGetLastError();
+}
+
+__global__ void kSeedScan(unsigned int* counts, int n, unsigned long long* total) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    unsigned long long s = 0;
+    for (int i = 0; i < n; ++i) { unsigned int c = counts[i]; counts[i] = (unsigned int)s; s += c; }
+    *total = s;
+  }
+}
+cudaError_t launchSeedScan(unsigned int* blockCounts, int nBlocks, unsigned long long* total, cudaStream_t s) {
+  kSeedScan<<<1, 1, 0, s>>>(blockCounts, nBlocks, total);
+  return cudaGetLastError();
+}
+
+// EulerParticles.cpp:156-176: particle k of the f-th fluid cell (cells in
+// linear order) at ((x + u) h + o) with u from Philox(cell, k; seed).
+__global__ void kSeedWrite(Geom g, const float* __restrict__ fsdf, const uint8_t* __restrict__ sidx,
+                           const unsigned int* __restrict__ blockOff, int cellsPerBlock, int ppc,
+                           unsigned long long seed, float* __restrict__ pos) {
+  long long n = g.r.size();
+  long long b0 = (long long)blockIdx.x * cellsPerBlock;
+  __shared__ unsigned int warpBase[32];
+  __shared__ unsigned int runBase;
+  if (threadIdx.x == 0) runBase = blockOff[blockIdx.x];
+  __syncthreads();
+  for (long long c0 = b0; c0 < b0 + cellsPerBlock && c0 < n; c0 += blockDim.x) {
+    long long c = c0 + threadIdx.x;
+    bool f = c < b0 + cellsPerBlock && c < n && seedCell(fsdf, sidx, c);
+    unsigned int ball = __ballot_sync(0xffffffffu, f);
+    unsigned int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) warpBase[w] = __popc(ball);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned int s = runBase;
+      for (int i = 0; i < (int)(blockDim.x >> 5); ++i) { unsigned int t = warpBase[i]; warpBase[i] = s; s += t; }
+      runBase = s;
+    }
+    __syncthreads();
+    if (f) {
+      unsigned long long rank = warpBase[w] + __popc(ball & ((1u << lane) - 1u));
+      int x, y, z;
+      cellCoord(c, g.r, x, y, z);
+      for (int k = 0; k < ppc; ++k) {
+        uint32_t ctr[4] = {(uint32_t)c, (uint32_t)((unsigned long long)c >> 32), (uint32_t)k, 0u};
+        philox10(ctr, (uint32_t)seed, (uint32_t)(seed >> 32));
+        float* q = pos + 3 * (rank * ppc + k);
+        q[0] = __fadd_rn(__fmul_rn(__fadd_rn((float)x, unit24(ctr[0])), g.hx), g.ox);
+        q[1] = __fadd_rn(__fmul_rn(__fadd_rn((float)y, unit24(ctr[1])), g.hy), g.oy);
+        q[2] = __fadd_rn(__fmul_rn(__fadd_rn((float)z, unit24(ctr[2])), g.hz), g.oz);
+      }
+    }
+    __syncthreads();
+  }
+}
+cudaError_t launchSeedWrite(const Geom& g, const float* fluidSDF, const uint8_t* solidIdx,
+                            const unsigned int* blockOffsets, int cellsPerBlock, int ppc, unsigned long long seed,
+                            float* pos, cudaStream_t s) {
+  long long n = g.r.size();
+  int nb = (int)((n + cellsPerBlock - 1) / cellsPerBlock);
+  kSeedWrite<<<nb, kThreads, 0, s>>>(g, fluidSDF, solidIdx, blockOffsets, cellsPerBlock, ppc, seed, pos);
+  return cudaGetLastError();
+}
+
+// Particle velocity update before advection:
+//   PIC  (ParticleInCell.cpp:102-104):       v = G2P(vin)
+//   FLIP (FluidImplicitParticle.cpp:107-119): v += G2P(vin - prev)
+//   MIX  (MixPICAndFLIP.cpp:112-129):        v = (1-m)(v + G2P(vin - prev)) + m G2P(vin)
+// with prev = the previous step's P2G output, or prev = 0 on the first FLIP step.
+template <int ALG>
+__global__ void kParticleVelUpdate(Geom g, int mode, ConstFaceField vin, ConstFaceField prev, int first, float mixing,
+                                   const float* __restrict__ pos, float* __restrict__ vel, long long P) {
+  const float keep = (float)(1.0 - (double)mixing);
+  HFG_FOR(p, P) {
+    float px = pos[3 * p], py = pos[3 * p + 1], pz = pos[3 * p + 2];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      Geom fg = faceGeom(g, a);
+      float v = vel[3 * p + a];
+      if (mode == MODE_PIC) {
+        v = g2p<ALG>(vin.c[a], fg, px, py, pz);
+      } else {
+        float pic = (mode == MODE_MIX) ? g2p<ALG>(vin.c[a], fg, px, py, pz) : 0.f;
+        float dv;
+        if (first) {
+          dv = g2p<ALG>(vin.c[a], fg, px, py, pz);
+        } else {
+          // G2P of the face-wise difference vin - prev
+          Taps t;
+          taps<ALG == G2PNEAREST ? LINEAR : ALG>(fg, px, py, pz, t);
+          constexpr int n = TapsN<ALG>::n, sft = TapsN<ALG>::shift;
+          dv = 0.f;
+          if (ALG == G2PNEAREST) {
+            long long i = binCell(fg, px, py, pz);
+            dv = __fsub_rn(__ldg(vin.c[a] + i), __ldg(prev.c[a] + i));
+          } else {
+#pragma unroll
+            for (int z = 0; z < n; ++z)
+#pragma unroll
+              for (int y = 0; y < n; ++y)
+#pragma unroll
+                for (int x = 0; x < n; ++x) {
+                  float w = t.w[0][x] * t.w[1][y] * t.w[2][z];
+                  long long i = linc(t.base[0] + x + sft, t.base[1] + y + sft, t.base[2] + z + sft, fg.r);
+                  dv += w * __fsub_rn(__ldg(vin.c[a] + i), __ldg(prev.c[a] + i));
+                }
+          }
+        }
+        v = __fadd_rn(dv, v);
+        if (mode == MODE_MIX) {
+          v = __fmul_rn(v, keep);
+          v = fmaf(mixing, pic, v);
+        }
+      }
+      vel[3 * p + a] = v;
+    }
+  }
+}
+
+cudaError_t launchParticleVelUpdate(const Geom& g, int mode, int alg, ConstFaceField vin, ConstFaceField prev,
+                                    int firstFlip, float mixing, const float* pos, float* vel, long long P,
+                                    cudaStream_t s) {
+  if (P <= 0) return cudaSuccess;
+  int gr = gridFor(P);
+  switch (alg) {
+    case LINEAR: kParticleVelUpdate<LINEAR><<<gr, kThreads, 0, s>>>(g, mode, vin, prev, firstFlip, mixing, pos, vel, P); break;
+    case QUADRATIC: kParticleVelUpdate<QUADRATIC><<<gr, kThreads, 0, s>>>(g, mode, vin, prev, firstFlip, mixing, pos, vel, P); break;
+    case CUBIC: kParticleVelUpdate<CUBIC><<<gr, kThreads, 0, s>>>(g, mode, vin, prev, firstFlip, mixing, pos, vel, P); break;
+    case G2PNEAREST: kParticleVelUpdate<G2PNEAREST><<<gr, kThreads, 0, s>>>(g, mode, vin, prev, firstFlip, mixing, pos, vel, P); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+__device__ inline void blockMaxToGlobal(float m, unsigned int* dst) {
+  __shared__ float s[32];
+  m = warpMaxF(m);
+  if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    int nw = blockDim.x >> 5;
+    float v = (int)threadIdx.x < nw ? s[threadIdx.x] : 0.f;
+    v = warpMaxF(v);
+    if (threadIdx.x == 0) atomicMax(dst, __float_as_uint(v));
+  }
+}
+
+// First velocity sample of the substep loop (EulerParticles.cpp:249-251):
+// v0 = trilinear(vel, pos) and max |v0| over every component.
+__global__ void kSubstepBegin(Geom g, ConstFaceField vel, const float* __restrict__ pos, float* __restrict__ v0,
+                              long long P, SubstepState* st) {
+  float m = 0.f;
+  HFG_FOR(p, P) {
+    float v[3];
+    sampleFace(vel, g, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2], v);
+    v0[3 * p] = v[0]; v0[3 * p + 1] = v[1]; v0[3 * p + 2] = v[2];
+    m = fmaxf(m, fmaxf(fabsf(v[0]), fmaxf(fabsf(v[1]), fabsf(v[2]))));
+  }
+  blockMaxToGlobal(m, &st[0].maxAbsBits);
+}
+cudaError_t launchSubstepBegin(const Geom& g, ConstFaceField vel, const float* pos, float* v0, long long P,
+                               SubstepState* st, cudaStream_t s) {
+  kSubstepBegin<<<gridFor(P > 0 ? P : 1), kThreads, 0, s>>>(g, vel, pos, v0, P, st);
+  return cudaGetLastError();
+}
+
+// Substep size rule of EulerParticles.cpp:253-275, evaluated identically by
+// every thread from the slot's state.
+__device__ inline float substepSize(const SubstepState& s, float dt, float cfl, float minH, bool& last) {
+  float amax = __uint_as_float(s.maxAbsBits);
+  float d = (amax != 0.f) ? __fdiv_rn(__fmul_rn(cfl, minH), amax) : dt;
+  last = false;
+  if (__fadd_rn(s.subTime, d) >= dt) {
+    d = __fsub_rn(dt, s.subTime);
+    last = true;
+  } else if (__fadd_rn(s.subTime, __fmul_rn(2.f, d)) >= dt) {
+    d = (float)(0.5 * (double)__fsub_rn(dt, s.subTime));
+  }
+  return d;
+}
+
+// One RK1/2/3 substep (EulerParticles.cpp:277-318).  After the last substep the
+// box clamp of fixParticlesPosWithBoundarys (EulerParticlesTool.cu:310-333) is
+// applied to the first `nclamp` particles; otherwise the next v0 and its max
+// are produced for slot+1.
+__global__ void kSubstep(Geom g, ConstFaceField vel, float* __restrict__ pos, float* __restrict__ v0, long long P,
+                         int acc, float dt, float cfl, long long nclamp, SubstepState* st, int slot) {
+  const SubstepState cur = st[slot];
+  if (cur.finished) {
+    // carry the finished state forward so later speculative launches no-op
+    if (blockIdx.x == 0 && threadIdx.x == 0) st[slot + 1] = cur;
+    return;
+  }
+  float minH = fminf(fminf(g.hx, g.hy), g.hz);
+  bool last;
+  float ds = substepSize(cur, dt, cfl, minH, last);
+  float half = (float)(0.5 * (double)ds), tq = (float)(0.75 * (double)ds);
+  float a29 = (float)(2.0 / 9.0 * (double)ds), a39 = (float)(3.0 / 9.0 * (double)ds), a49 = (float)(4.0 / 9.0 * (double)ds);
+  float bmin[3] = {g.ox, g.oy, g.oz};
+  float bmax[3] = {g.ox + (float)g.r.x * g.hx, g.oy + (float)g.r.y * g.hy, g.oz + (float)g.r.z * g.hz};
+  float m = 0.f;
+  HFG_FOR(p, P) {
+    float q[3] = {pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]};
+    float w0[3] = {v0[3 * p], v0[3 * p + 1], v0[3 * p + 2]};
+    if (acc == 0) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) q[a] = fmaf(ds, w0[a], q[a]);
+    } else if (acc == 1) {
+      float mid[3], w1[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) mid[a] = fmaf(half, w0[a], q[a]);
+      sampleFace(vel, g, mid[0], mid[1], mid[2], w1);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) q[a] = fmaf(ds, w1[a], q[a]);
+    } else {
+      float mid[3], tf[3], w1[3], w2[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) mid[a] = fmaf(half, w0[a], q[a]);
+      sampleFace(vel, g, mid[0], mid[1], mid[2], w1);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) tf[a] = fmaf(tq, w1[a], q[a]);
+      sampleFace(vel, g, tf[0], tf[1], tf[2], w2);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        q[a] = fmaf(a29, w0[a], q[a]);
+        q[a] = fmaf(a39, w1[a], q[a]);
+        q[a] = fmaf(a49, w2[a], q[a]);
+      }
+    }
+    if (last) {
+      if (p < nclamp) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) q[a] = fmaxf(bmin[a], fminf(q[a], bmax[a]));
+      }
+    } else {
+      float v[3];
+      sampleFace(vel, g, q[0], q[1], q[2], v);
+      v0[3 * p] = v[0]; v0[3 * p + 1] = v[1]; v0[3 * p + 2] = v[2];
+      m = fmaxf(m, fmaxf(fabsf(v[0]), fmaxf(fabsf(v[1]), fabsf(v[2]))));
+    }
+    pos[3 * p] = q[0]; pos[3 * p + 1] = q[1]; pos[3 * p + 2] = q[2];
+  }
+  if (!last) blockMaxToGlobal(m, &st[slot + 1].maxAbsBits);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st[slot + 1].subTime = __fadd_rn(cur.subTime, ds);
+    st[slot + 1].finished = last ? 1 : 0;
+    st[slot + 1].count = cur.count + 1;
+  }
+}
+cudaError_t launchSubstep(const Geom& g, ConstFaceField vel, float* pos, float* v0, long long P, int acc, float dt,
+                          float cfl, long long nclamp, SubstepState* st, int slot, cudaStream_t s) {
+  kSubstep<<<gridFor(P > 0 ? P : 1), kThreads, 0, s>>>(g, vel, pos, v0, P, acc, dt, cfl, nclamp, st, slot);
+  return cudaGetLastError();
+}
+
+// P2G of particle velocities to the three face grids, value and weight packed
+// as float2 so every corner is one vector atomic
+// (accumulateParticles2CCSField, EulerParticlesTool.cu:79-196).
+template <int ALG>
+__device__ inline void p2gScatter(const Geom& fg, float px, float py, float pz, float val, float2* acc) {
+  if (ALG == P2GSUM) {
+    atomicAdd(&acc[binCell(fg, px, py, pz)].x, val);
+    return;
+  }
+  Taps t;
+  taps<ALG>(fg, px, py, pz, t);
+  constexpr int n = TapsN<ALG>::n, s = TapsN<ALG>::shift;
+#pragma unroll
+  for (int z = 0; z < n; ++z)
+#pragma unroll
+    for (int y = 0; y < n; ++y)
+#pragma unroll
+      for (int x = 0; x < n; ++x) {
+        float w = t.w[0][x] * t.w[1][y] * t.w[2][z];
+        long long i = linc(t.base[0] + x + s, t.base[1] + y + s, t.base[2] + z + s, fg.r);
+        atomicAdd(acc + i, make_float2(w * val, w));
+      }
+}
+
+template <int ALG>
+__global__ void kP2GFace(Geom g, const float* __restrict__ pos, const float* __restrict__ vel, long long P,
+                         float2* a0, float2* a1, float2* a2) {
+  HFG_FOR(p, P) {
+    float px = pos[3 * p], py = pos[3 * p + 1], pz = pos[3 * p + 2];
+    p2gScatter<ALG>(faceGeom(g, 0), px, py, pz, vel[3 * p], a0);
+    p2gScatter<ALG>(faceGeom(g, 1), px, py, pz, vel[3 * p + 1], a1);
+    p2gScatter<ALG>(faceGeom(g, 2), px, py, pz, vel[3 * p + 2], a2);
+  }
+}
+cudaError_t launchP2GFace(const Geom& g, int alg, const float* pos, const float* vel, long long P, float2* acc[3],
+                          cudaStream_t s) {
+  if (P <= 0) return cudaSuccess;
+  int gr = gridFor(P);
+  switch (alg) {
+    case LINEAR: kP2GFace<LINEAR><<<gr, kThreads, 0, s>>>(g, pos, vel, P, acc[0], acc[1], acc[2]); break;
+    case QUADRATIC: kP2GFace<QUADRATIC><<<gr, kThreads, 0, s>>>(g, pos, vel, P, acc[0], acc[1], acc[2]); break;
+    case CUBIC: kP2GFace<CUBIC><<<gr, kThreads, 0, s>>>(g, pos, vel, P, acc[0], acc[1], acc[2]); break;
+    case P2GSUM: kP2GFace<P2GSUM><<<gr, kThreads, 0, s>>>(g, pos, vel, P, acc[0], acc[1], acc[2]); break;
+    default: break;  // G2PNEAREST has no P2G branch in the reference: nothing is accumulated
+  }
+  return cudaGetLastError();
+}
+
+template <int ALG>
+__global__ void kP2GCell(Geom g, const float* __restrict__ pos, const float* __restrict__ val, int span, int comp,
+                         long long P, float2* acc) {
+  HFG_FOR(p, P) p2gScatter<ALG>(g, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2], val[span * p + comp], acc);
+}
+cudaError_t launchP2GCell(const Geom& g, int alg, const float* pos, const float* val, int span, int comp, long long P,
+                          float2* acc, cudaStream_t s) {
+  if (P <= 0) return cudaSuccess;
+  int gr = gridFor(P);
+  switch (alg) {
+    case LINEAR: kP2GCell<LINEAR><<<gr, kThreads, 0, s>>>(g, pos, val, span, comp, P, acc); break;
+    case QUADRATIC: kP2GCell<QUADRATIC><<<gr, kThreads, 0, s>>>(g, pos, val, span, comp, P, acc); break;
+    case CUBIC: kP2GCell<CUBIC><<<gr, kThreads, 0, s>>>(g, pos, val, span, comp, P, acc); break;
+    case P2GSUM: kP2GCell<P2GSUM><<<gr, kThreads, 0, s>>>(g, pos, val, span, comp, P, acc); break;
+    default: break;
+  }
+  return cudaGetLastError();
+}
+
+// normalizeCCSField (EulerParticlesTool.cu:290-308) fused with the copy kept
+// as the next FLIP "previous grid velocity" (MixPICAndFLIP.cpp:135) and the
+// unit-field external-force axpys (ExternalForcesSolver.cpp:57-58).
+__global__ void kNormalize(long long n, const float2* __restrict__ acc, float* __restrict__ out, float* __restrict__ copy,
+                           float add, int doAdd, float add2, int doAdd2) {
+  HFG_FOR(i, n) {
+    float2 a = acc[i];
+    float v = a.y > 0.f ? __fdiv_rn(a.x, a.y) : a.x;
+    if (copy) copy[i] = v;
+    if (doAdd) v = __fadd_rn(add, v);
+    if (doAdd2) v = __fadd_rn(add2, v);
+    out[i] = v;
+  }
+}
+cudaError_t launchNormalize(long long n, const float2* acc, float* out, float* copy, float add, int doAdd, float add2,
+                            int doAdd2, cudaStream_t s) {
+  kNormalize<<<gridFor(n), kThreads, 0, s>>>(n, acc, out, copy, add, doAdd, add2, doAdd2);
+  return cudaGetLastError();
+}
+
+template <int ALG>
+__global__ void kG2PFace(Geom g, ConstFaceField f, const float* __restrict__ pos, long long P, float* __restrict__ out) {
+  HFG_FOR(p, P) {
+    float px = pos[3 * p], py = pos[3 * p + 1], pz = pos[3 * p + 2];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) out[3 * p + a] = g2p<ALG>(f.c[a], faceGeom(g, a), px, py, pz);
+  }
+}
+cudaError_t launchG2PFace(const Geom& g, int alg, ConstFaceField f, const float* pos, long long P, float* out,
+                          cudaStream_t s) {
+  if (P <= 0) return cudaSuccess;
+  int gr = gridFor(P);
+  switch (alg) {
+    case LINEAR: kG2PFace<LINEAR><<<gr, kThreads, 0, s>>>(g, f, pos, P, out); break;
+    case QUADRATIC: kG2PFace<QUADRATIC><<<gr, kThreads, 0, s>>>(g, f, pos, P, out); break;
+    case CUBIC: kG2PFace<CUBIC><<<gr, kThreads, 0, s>>>(g, f, pos, P, out); break;
+    case G2PNEAREST: kG2PFace<G2PNEAREST><<<gr, kThreads, 0, s>>>(g, f, pos, P, out); break;
+    default: return cudaMemsetAsync(out, 0, sizeof(float) * 3 * P, s);  // P2GSUM: G2P writes 0 (:223)
+  }
+  return cudaGetLastError();
+}
+
+template <int ALG>
+__global__ void kG2PCell(Geom g, const float* __restrict__ f, const float* __restrict__ pos, long long P,
+                         float* __restrict__ out, int span, int comp) {
+  HFG_FOR(p, P) out[span * p + comp] = g2p<ALG>(f, g, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]);
+}
+cudaError_t launchG2PCell(const Geom& g, int alg, const float* f, const float* pos, long long P, float* out, int span,
+                          int comp, cudaStream_t s) {
+  if (P <= 0) return cudaSuccess;
+  int gr = gridFor(P);
+  switch (alg) {
+    case LINEAR: kG2PCell<LINEAR><<<gr, kThreads, 0, s>>>(g, f, pos, P, out, span, comp); break;
+    case QUADRATIC: kG2PCell<QUADRATIC><<<gr, kThreads, 0, s>>>(g, f, pos, P, out, span, comp); break;
+    case CUBIC: kG2PCell<CUBIC><<<gr, kThreads, 0, s>>>(g, f, pos, P, out, span, comp); break;
+    case G2PNEAREST: kG2PCell<G2PNEAREST><<<gr, kThreads, 0, s>>>(g, f, pos, P, out, span, comp); break;
+    default: break;
+  }
+  return cudaGetLastError();
+}
+
+__global__ void kSampleFace(Geom g, ConstFaceField f, const float* __restrict__ pos, long long M, float* __restrict__ out) {
+  HFG_FOR(i, M) {
+    float v[3];
+    sampleFace(f, g, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], v);
+    out[3 * i] = v[0]; out[3 * i + 1] = v[1]; out[3 * i + 2] = v[2];
+  }
+}
+cudaError_t launchSampleFace(const Geom& g, ConstFaceField f, const float* pos, long long M, float* out, cudaStream_t s) {
+  if (M <= 0) return cudaSuccess;
+  kSampleFace<<<gridFor(M), kThreads, 0, s>>>(g, f, pos, M, out);
+  return cudaGetLastError();
+}
+__global__ void kSampleCell(Geom g, const float* __restrict__ f, const float* __restrict__ pos, long long M,
+                            float* __restrict__ out) {
+  HFG_FOR(i, M) out[i] = trilerp(f, g, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+}
+cudaError_t launchSampleCell(const Geom& g, const float* f, const float* pos, long long M, float* out, cudaStream_t s) {
+  if (M <= 0) return cudaSuccess;
+  kSampleCell<<<gridFor(M), kThreads, 0, s>>>(g, f, pos, M, out);
+  return cudaGetLastError();
+}
+
+// ===========================================================================
+// Semi-Lagrangian advection (SemiLagrangian.cpp:135-347): back-trace each
+// face / cell centre through `vel` with RK1/2/3, then sample the source field
+// there.  The position fields and the nine axpys of the reference are fused
+// into one pass per output grid.
+// ===========================================================================
+__device__ inline void axpyPt(float a, const float v[3], float p[3]) {
+  if (fabsf(a) < FLT_EPSILON) return;  // plusAlphaX skip
+#pragma unroll
+  for (int k = 0; k < 3; ++k) p[k] = fmaf(a, v[k], p[k]);
+}
+
+__device__ inline void backTrace(ConstFaceField vel, const Geom& g, float dt, int acc, const float in[3], float out[3]) {
+  float v0[3], v1[3], v2[3], mid[3], tf[3];
+  out[0] = in[0]; out[1] = in[1]; out[2] = in[2];
+  sampleFace(vel, g, in[0], in[1], in[2], v0);
+  if (acc == 0) {
+    axpyPt(-dt, v0, out);
+    return;
+  }
+  mid[0] = in[0]; mid[1] = in[1]; mid[2] = in[2];
+  axpyPt(-0.5f * dt, v0, mid);
+  sampleFace(vel, g, mid[0], mid[1], mid[2], v1);
+  if (acc == 1) {
+    axpyPt(-dt, v1, out);
+    return;
+  }
+  tf[0] = in[0]; tf[1] = in[1]; tf[2] = in[2];
+  axpyPt(-0.75f * dt, v1, tf);
+  sampleFace(vel, g, tf[0], tf[1], tf[2], v2);
+  axpyPt(-(float)(2.0 / 9.0) * dt, v0, out);
+  axpyPt(-(float)(3.0 / 9.0) * dt, v1, out);
+  axpyPt(-(float)(4.0 / 9.0) * dt, v2, out);
+}
+
+__global__ void kSLFace(Geom g, int acc, float dt, ConstFaceField vel, ConstFaceField in, FaceField out, float ax,
+                        float ay, float az, int doAdd, float bx, float by, float bz, int doAdd2) {
+  const float add[3] = {ax, ay, az}, add2[3] = {bx, by, bz};
+  for (int a = 0; a < 3; ++a) {
+    Geom fg = faceGeom(g, a);
+    HFG_FOR(f, fg.r.size()) {
+      int x, y, z;
+      cellCoord(f, fg.r, x, y, z);
+      // SemiLagrangian.cpp:60-97 sample points
+      float p[3] = {__fadd_rn(__fmul_rn(__fadd_rn((float)x, 0.5f), g.hx), g.ox),
+                    __fadd_rn(__fmul_rn(__fadd_rn((float)y, 0.5f), g.hy), g.oy),
+                    __fadd_rn(__fmul_rn(__fadd_rn((float)z, 0.5f), g.hz), g.oz)};
+      if (a == 0) p[0] = __fadd_rn(__fmul_rn((float)x, g.hx), g.ox);
+      if (a == 1) p[1] = __fadd_rn(__fmul_rn((float)y, g.hy), g.oy);
+      if (a == 2) p[2] = __fadd_rn(__fmul_rn((float)z, g.hz), g.oz);
+      float q[3];
+      backTrace(vel, g, dt, acc, p, q);
+      float v = trilerp(in.c[a], fg, q[0], q[1], q[2]);
+      if (doAdd) v = __fadd_rn(add[a], v);
+      if (doAdd2) v = __fadd_rn(add2[a], v);
+      out.c[a][f] = v;
+    }
+  }
+}
+cudaError_t launchSLFace(const Geom& g, int acc, float dt, ConstFaceField vel, ConstFaceField in, FaceField out,
+                         const float add[3], int doAdd, const float add2[3], int doAdd2, cudaStream_t s) {
+  kSLFace<<<gridFor(g.r.size()), kThreads, 0, s>>>(g, acc, dt, vel, in, out, add[0], add[1], add[2], doAdd, add2[0],
+                                                   add2[1], add2[2], doAdd2);
+  return cudaGetLastError();
+}
+
+struct CellFields {
+  const float* in[4];
+  float* out[4];
+};
+__global__ void kSLCell(Geom g, int acc, float dt, ConstFaceField vel, CellFields cf, int nf) {
+  HFG_FOR(c, g.r.size()) {
+    int x, y, z;
+    cellCoord(c, g.r, x, y, z);
+    float p[3] = {__fadd_rn(__fmul_rn(__fadd_rn((float)x, 0.5f), g.hx), g.ox),
+                  __fadd_rn(__fmul_rn(__fadd_rn((float)y, 0.5f), g.hy), g.oy),
+                  __fadd_rn(__fmul_rn(__fadd_rn((float)z, 0.5f), g.hz), g.oz)};
+    float q[3];
+    backTrace(vel, g, dt, acc, p, q);
+    for (int k = 0; k < nf; ++k) cf.out[k][c] = trilerp(cf.in[k], g, q[0], q[1], q[2]);
+  }
+}
+cudaError_t launchSLCell(const Geom& g, int acc, float dt, ConstFaceField vel, const float* const* in, float* const* out,
+                         int nfields, cudaStream_t s) {
+  CellFields cf{};
+  for (int k = 0; k < nfields && k < 4; ++k) { cf.in[k] = in[k]; cf.out[k] = out[k]; }
+  kSLCell<<<gridFor(g.r.size()), kThreads, 0, s>>>(g, acc, dt, vel, cf, nfields < 4 ? nfields : 4);
+  return cudaGetLastError();
+}
+
+__global__ void kAddConst(long long n, float* __restrict__ v, float a) {
+  HFG_FOR(i, n) v[i] = __fadd_rn(a, v[i]);
+}
+cudaError_t launchAddConst(long long n, float* v, float a, cudaStream_t s) {
+  kAddConst<<<gridFor(n), kThreads, 0, s>>>(n, v, a);
+  return cudaGetLastError();
+}
+
+}  // namespace hfg

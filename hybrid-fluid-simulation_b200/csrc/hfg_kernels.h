@@ -1,0 +1,141 @@
+// hfg_kernels.h -- host-side launchers for the sm_100a kernels of the grid
+// step.  Every launcher is asynchronous on the given stream and returns
+// cudaGetLastError() of its launch.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "hfg_device.cuh"
+
+namespace hfg {
+
+constexpr int kMaxBoundaries = 32;
+
+// Solid boundaries as the kernels see them: one cell-centred SDF per solid
+// plus its current translation (MPhysics/Boundary.cpp:124-136).
+struct BoundarySet {
+  int n;
+  const float* sdf[kMaxBoundaries];
+  float tx[kMaxBoundaries], ty[kMaxBoundaries], tz[kMaxBoundaries];
+  float vx[kMaxBoundaries], vy[kMaxBoundaries], vz[kMaxBoundaries];
+};
+
+// Device-resident scalars of one CG solve.  The last block of every reduction
+// kernel updates them, so no host round trip is needed per iteration.
+struct CgState {
+  double rz;        // r.z of the current iteration
+  double rr;        // ||r||^2 after the last update
+  double bb;        // ||b||^2
+  double pAp;
+  float alpha, beta;
+  int iter;         // iterations completed
+  int done;         // 1 once converged or out of iterations
+  int maxIter;
+  int precond;      // 0 identity, 1 Jacobi
+  int tolMode;      // 0 reference rule sqrt(||r||) < tol, 1 ||r||/||b|| < tol
+  double tol;
+  unsigned int ticket;  // last-block-done counter
+};
+
+// State of the CFL substep loop of one particle advection
+// (MPhysics/EulerParticles.cpp:241-319).  Slot s is read by substep s and
+// slot s+1 written by it.
+struct SubstepState {
+  unsigned int maxAbsBits;  // max |v| over all sampled components (float bits)
+  float subTime;            // time advanced so far
+  int finished;
+  int count;
+};
+
+struct SolidVelTable {
+  const uint8_t* solidIdx;  // 0 = not solid, i+1 = solid of boundary i
+  float vx[kMaxBoundaries], vy[kMaxBoundaries], vz[kMaxBoundaries];
+};
+
+int numSMs();
+
+// ---- boundaries / classification -------------------------------------------
+cudaError_t launchSolidClassify(const Geom& g, const BoundarySet& b, uint8_t* solidIdx, float* const* curSDF,
+                                cudaStream_t s);
+cudaError_t launchSolidFromSDF(long long n, const float* solidSDF, uint8_t* solidIdx, cudaStream_t s);
+cudaError_t launchTotalSolidSDF(long long n, int nb, const uint8_t* solidIdx, float* out, cudaStream_t s);
+cudaError_t launchSolidVelField(const Geom& g, const SolidVelTable& t, FaceField out, cudaStream_t s);
+cudaError_t launchMarkersInit(long long n, const uint8_t* solidIdx, uint8_t* markers, cudaStream_t s);
+cudaError_t launchMarkersFromParticles(const Geom& g, const float* pos, long long P, uint8_t* markers, cudaStream_t s);
+cudaError_t launchBinCounts(const Geom& g, const float* pos, long long P, unsigned int* counts, cudaStream_t s);
+cudaError_t launchMarkersFromSDF(long long n, const uint8_t* solidIdx, const float* fluidSDF, uint8_t* markers,
+                                 cudaStream_t s);
+cudaError_t launchFluidDomainFromBBox(const Geom& g, const float mn[3], const float mx[3], float* out, cudaStream_t s);
+
+// ---- pressure projection ---------------------------------------------------
+cudaError_t launchStencilCode(const Dim3i& r, const uint8_t* markers, uint8_t* code, cudaStream_t s);
+cudaError_t launchMatrixA(const Dim3i& r, float sx, float sy, float sz, const uint8_t* code, float* A, cudaStream_t s);
+cudaError_t launchApplyA(const Dim3i& r, float sx, float sy, float sz, const uint8_t* code, const float* x, float* y,
+                         cudaStream_t s);
+// RHS (divergence + solid terms) fused with CG set-up: r = b, x = 0, p = 0,
+// ||b||^2 and r.z into the state.  Solid face velocities come from `svArr`
+// when non-null, else from the per-solid table.
+cudaError_t launchRhsInit(const Geom& g, ConstFaceField v, ConstFaceField svArr, const SolidVelTable& svTab,
+                          const uint8_t* markers, const uint8_t* code, float ax, float ay, float az, float* b,
+                          float* r, float* x, float* p, double* partials, CgState* st, cudaStream_t s);
+cudaError_t launchCgDirection(const Dim3i& r, float sx, float sy, float sz, const uint8_t* code, const float* rr,
+                              const float* pOld, float* pNew, double* partials, CgState* st, cudaStream_t s);
+cudaError_t launchCgUpdate(const Dim3i& r, float sx, float sy, float sz, const uint8_t* code, const float* p,
+                           float* x, float* rr, double* partials, CgState* st, cudaStream_t s);
+cudaError_t launchGradient(const Geom& g, float gx, float gy, float gz, const uint8_t* markers, const float* p,
+                           FaceField v, ConstFaceField svArr, const SolidVelTable& svTab, cudaStream_t s);
+int cgPartialsNeeded();
+
+// ---- extrapolation ---------------------------------------------------------
+struct ExtrapScratch {
+  uint16_t* dist;          // total faces
+  unsigned int* list;      // total faces
+  unsigned int* hist;      // kMaxLayers + 2
+  unsigned int* offsets;   // kMaxLayers + 2
+  unsigned int* cursor;    // kMaxLayers + 2
+};
+constexpr int kMaxLayers = 1000;
+cudaError_t launchExtrapDistance(const Dim3i rc[3], float* const vals[3], long long off[3], int nums,
+                                 ExtrapScratch sc, cudaStream_t s);
+cudaError_t launchExtrapLayer(const Dim3i rc[3], float* const vals[3], const long long off[3], ExtrapScratch sc,
+                              unsigned int begin, unsigned int count, int d, cudaStream_t s);
+
+// ---- particles -------------------------------------------------------------
+enum ParticleMode : int { MODE_PIC = 0, MODE_FLIP = 1, MODE_MIX = 2 };
+cudaError_t launchSeedCount(const Dim3i& r, const float* fluidSDF, const uint8_t* solidIdx, unsigned int* blockCounts,
+                            int cellsPerBlock, cudaStream_t s);
+cudaError_t launchSeedScan(unsigned int* blockCounts, int nBlocks, unsigned long long* total, cudaStream_t s);
+cudaError_t launchSeedWrite(const Geom& g, const float* fluidSDF, const uint8_t* solidIdx,
+                            const unsigned int* blockOffsets, int cellsPerBlock, int ppc, unsigned long long seed,
+                            float* pos, cudaStream_t s);
+cudaError_t launchParticleVelUpdate(const Geom& g, int mode, int alg, ConstFaceField vin, ConstFaceField prev,
+                                    int firstFlip, float mixing, const float* pos, float* vel, long long P,
+                                    cudaStream_t s);
+cudaError_t launchSubstepBegin(const Geom& g, ConstFaceField vel, const float* pos, float* v0, long long P,
+                               SubstepState* st, cudaStream_t s);
+cudaError_t launchSubstep(const Geom& g, ConstFaceField vel, float* pos, float* v0, long long P, int acc, float dt,
+                          float cfl, long long nclamp, SubstepState* st, int slot, cudaStream_t s);
+cudaError_t launchP2GFace(const Geom& g, int alg, const float* pos, const float* vel, long long P, float2* acc[3],
+                          cudaStream_t s);
+cudaError_t launchP2GCell(const Geom& g, int alg, const float* pos, const float* val, int span, int comp, long long P,
+                          float2* acc, cudaStream_t s);
+cudaError_t launchNormalize(long long n, const float2* acc, float* out, float* copy, float add, int doAdd,
+                            float add2, int doAdd2, cudaStream_t s);
+cudaError_t launchG2PFace(const Geom& g, int alg, ConstFaceField f, const float* pos, long long P, float* out,
+                          cudaStream_t s);
+cudaError_t launchG2PCell(const Geom& g, int alg, const float* f, const float* pos, long long P, float* out, int span,
+                          int comp, cudaStream_t s);
+cudaError_t launchSampleFace(const Geom& g, ConstFaceField f, const float* pos, long long M, float* out,
+                             cudaStream_t s);
+cudaError_t launchSampleCell(const Geom& g, const float* f, const float* pos, long long M, float* out, cudaStream_t s);
+
+// ---- semi-Lagrangian -------------------------------------------------------
+cudaError_t launchSLFace(const Geom& g, int acc, float dt, ConstFaceField vel, ConstFaceField in, FaceField out,
+                         const float add[3], int doAdd, const float add2[3], int doAdd2, cudaStream_t s);
+cudaError_t launchSLCell(const Geom& g, int acc, float dt, ConstFaceField vel, const float* const* in, float* const* out,
+                         int nfields, cudaStream_t s);
+
+// ---- external forces (unit-field axpy on every face) ------------------------
+cudaError_t launchAddConst(long long n, float* v, float a, cudaStream_t s);
+
+}  // namespace hfg

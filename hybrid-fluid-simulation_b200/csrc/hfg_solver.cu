@@ -1,0 +1,543 @@
+// hfg_solver.cu -- GridSolver: the reference grid step
+// (MPhysics/GridFluidSolver.cpp:336-537) orchestrated as device-resident
+// kernels on one stream.  Host round trips per step: one 4-byte read per
+// chunk of CFL substeps, one per chunk of CG iterations, and one 4 KB read of
+// the extrapolation layer offsets.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "hfg_solver.h"
+
+namespace hfg {
+
+void check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e), HFG_ERR_CUDA);
+}
+
+namespace {
+constexpr int kCgChunk = 16;       // CG iterations launched between convergence reads
+constexpr int kSubstepChunk = 4;   // CFL substeps launched between completion reads
+}  // namespace
+
+// Multigrid preconditioner hooks (hfg_mg.cu).
+Multigrid* mgCreate(const Dim3i& r, int levels, int smooth, bool half);
+void mgDestroy(Multigrid* m);
+void mgSetup(Multigrid* m, const uint8_t* code, float sx, float sy, float sz, cudaStream_t s, long long& launches);
+void mgRunCg(Multigrid* m, const Dim3i& r, float sx, float sy, float sz, const uint8_t* code, float* x, float* rvec,
+             double* partials, CgState* st, CgState* stHost, cudaStream_t s, long long& launches);
+
+GridSolver::GridSolver(float dt, Dim3i res, const float origin[3], const float spacing[3]) {
+  if (res.x <= 0 || res.y <= 0 || res.z <= 0) throw CudaError("resolution must be positive", HFG_ERR_INVALID);
+  if (res.size() >= (1LL << 31)) throw CudaError("grid too large", HFG_ERR_INVALID);
+  g_.r = res;
+  g_.ox = origin[0]; g_.oy = origin[1]; g_.oz = origin[2];
+  g_.hx = spacing[0]; g_.hy = spacing[1]; g_.hz = spacing[2];
+  dt_ = dt;
+  N_ = res.size();
+  fr_[0] = Dim3i{res.x + 1, res.y, res.z};
+  fr_[1] = Dim3i{res.x, res.y + 1, res.z};
+  fr_[2] = Dim3i{res.x, res.y, res.z + 1};
+  Ftot_ = 0;
+  for (int a = 0; a < 3; ++a) { F_[a] = fr_[a].size(); Ftot_ += F_[a]; }
+  hfg_default_options(&opt_);
+  check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  for (int b = 0; b < 2; ++b)
+    for (int a = 0; a < 3; ++a) {
+      vel_[b][a].alloc(F_[a]);
+      color_[b][a].alloc(N_);
+    }
+  for (int b = 0; b < 2; ++b) dom_[b].alloc(N_);
+  for (int a = 0; a < 3; ++a) prev_[a].alloc(F_[a]);
+  solidIdx_.alloc(N_); markers_.alloc(N_); code_.alloc(N_);
+  cgx_.alloc(N_); cgr_.alloc(N_); cgp_[0].alloc(N_); cgp_[1].alloc(N_);
+  partials_.alloc(cgPartialsNeeded());
+  cgState_.alloc(1);
+  subState_.alloc(subSlots_ + 1);
+  dist_.alloc(Ftot_); list_.alloc(Ftot_);
+  hist_.alloc(kMaxLayers + 2); offsets_.alloc(kMaxLayers + 2); cursor_.alloc(kMaxLayers + 2);
+  check(cudaMallocHost((void**)&cgHost_, sizeof(CgState)), "cudaMallocHost");
+  check(cudaMallocHost((void**)&subHost_, sizeof(SubstepState)), "cudaMallocHost");
+  check(cudaMallocHost((void**)&offHost_, sizeof(unsigned int) * (kMaxLayers + 2)), "cudaMallocHost");
+  // GridFluidSolver.cpp:179-195: every field starts at zero
+  for (int b = 0; b < 2; ++b) {
+    for (int a = 0; a < 3; ++a) {
+      check(cudaMemsetAsync(vel_[b][a].p, 0, vel_[b][a].bytes(), stream_), "memset");
+      check(cudaMemsetAsync(color_[b][a].p, 0, color_[b][a].bytes(), stream_), "memset");
+    }
+    check(cudaMemsetAsync(dom_[b].p, 0, dom_[b].bytes(), stream_), "memset");
+  }
+  for (int a = 0; a < 3; ++a) check(cudaMemsetAsync(prev_[a].p, 0, prev_[a].bytes(), stream_), "memset");
+  check(cudaMemsetAsync(solidIdx_.p, 0, N_, stream_), "memset");
+  check(cudaMemsetAsync(markers_.p, 0, N_, stream_), "memset");
+  check(cudaMemsetAsync(cgx_.p, 0, cgx_.bytes(), stream_), "memset");
+  check(cudaMemsetAsync(cgState_.p, 0, sizeof(CgState), stream_), "memset");
+  for (int i = 0; i < 16; ++i) check(cudaEventCreate(&ev_[i]), "cudaEventCreate");
+  check(cudaStreamSynchronize(stream_), "sync");
+}
+
+GridSolver::~GridSolver() {
+  if (stream_) cudaStreamSynchronize(stream_);
+  for (auto* b : bsdf_) delete b;
+  if (mg_) mgDestroy(mg_);
+  if (cgHost_) cudaFreeHost(cgHost_);
+  if (subHost_) cudaFreeHost(subHost_);
+  if (offHost_) cudaFreeHost(offHost_);
+  for (int i = 0; i < 16; ++i)
+    if (ev_[i]) cudaEventDestroy(ev_[i]);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+void GridSolver::launched(cudaError_t e, const char* what, int count) {
+  check(e, what);
+  launches_ += count;
+}
+
+void GridSolver::stageBegin(int i) {
+  if (timing_) check(cudaEventRecord(ev_[2 * i], stream_), "cudaEventRecord");
+}
+void GridSolver::stageEnd(int i) {
+  if (timing_) check(cudaEventRecord(ev_[2 * i + 1], stream_), "cudaEventRecord");
+}
+
+void GridSolver::enableTiming(bool on) { timing_ = on; }
+
+void GridSolver::addBoundary(const float* sdfHost, const float vel[3]) {
+  if ((int)bsdf_.size() >= kMaxBoundaries) throw CudaError("too many solid boundaries", HFG_ERR_INVALID);
+  auto* b = new DArray<float>();
+  b->alloc(N_);
+  check(cudaMemcpyAsync(b->p, sdfHost, N_ * sizeof(float), cudaMemcpyHostToDevice, stream_), "upload sdf");
+  bsdf_.push_back(b);
+  for (int a = 0; a < 3; ++a) { bvel_.push_back(vel ? vel[a] : 0.f); btrans_.push_back(0.f); }
+  check(cudaStreamSynchronize(stream_), "sync");
+}
+
+void GridSolver::addExternalForce(const float f[3]) {
+  for (int a = 0; a < 3; ++a) ext_[a] += f[a];  // ExternalForcesSolver.cpp:45-48
+}
+
+void GridSolver::setVelocity(const float* x, const float* y, const float* z) {
+  const float* s[3] = {x, y, z};
+  for (int b = 0; b < 2; ++b)
+    for (int a = 0; a < 3; ++a)
+      check(cudaMemcpyAsync(vel_[b][a].p, s[a], F_[a] * 4, cudaMemcpyHostToDevice, stream_), "upload velocity");
+  check(cudaStreamSynchronize(stream_), "sync");
+}
+
+void GridSolver::setFluidDomain(const float* d) {
+  for (int b = 0; b < 2; ++b) check(cudaMemcpyAsync(dom_[b].p, d, N_ * 4, cudaMemcpyHostToDevice, stream_), "upload");
+  check(cudaStreamSynchronize(stream_), "sync");
+}
+
+void GridSolver::setColor(const float* x, const float* y, const float* z) {
+  const float* s[3] = {x, y, z};
+  for (int b = 0; b < 2; ++b)
+    for (int a = 0; a < 3; ++a)
+      check(cudaMemcpyAsync(color_[b][a].p, s[a], N_ * 4, cudaMemcpyHostToDevice, stream_), "upload colour");
+  check(cudaStreamSynchronize(stream_), "sync");
+}
+
+// GridFluidSolver.cpp:551-555: bbox written into field 1, copied to field 2.
+void GridSolver::fluidDomainFromBBox(const float mn[3], const float mx[3]) {
+  launched(launchFluidDomainFromBBox(g_, mn, mx, dom_[0].p, stream_), "fluid domain");
+  check(cudaMemcpyAsync(dom_[1].p, dom_[0].p, N_ * 4, cudaMemcpyDeviceToDevice, stream_), "copy");
+  check(cudaStreamSynchronize(stream_), "sync");
+}
+
+void GridSolver::setAdvection(int kind, int acc, int alg, float cfl, float mixing) {
+  if (kind < 0 || kind > 3 || acc < 0 || acc > 2 || alg < 0 || alg > 4)
+    throw CudaError("invalid advection settings", HFG_ERR_INVALID);
+  adv_ = kind; acc_rk_ = acc; alg_ = alg; cfl_ = cfl; mixing_ = mixing;
+  sFlag_ = vFlag_ = velFlag_ = false;
+}
+
+void GridSolver::setParticles(const float* pos, const float* vel, long long n) {
+  if (n < 0) throw CudaError("negative particle count", HFG_ERR_INVALID);
+  P_ = n;
+  ppos_.alloc(3 * n); pvel_.alloc(3 * n); pv0_.alloc(3 * n); pscalar_.alloc(n); pvector_.alloc(3 * n);
+  if (n > 0) {
+    check(cudaMemcpyAsync(ppos_.p, pos, 12 * n, cudaMemcpyHostToDevice, stream_), "upload particles");
+    if (vel) check(cudaMemcpyAsync(pvel_.p, vel, 12 * n, cudaMemcpyHostToDevice, stream_), "upload particles");
+    else check(cudaMemsetAsync(pvel_.p, 0, 12 * n, stream_), "memset");
+    check(cudaMemsetAsync(pscalar_.p, 0, 4 * n, stream_), "memset");
+    check(cudaMemsetAsync(pvector_.p, 0, 12 * n, stream_), "memset");
+  }
+  sFlag_ = vFlag_ = velFlag_ = false;
+  check(cudaStreamSynchronize(stream_), "sync");
+}
+
+// EulerParticles.cpp:140-179 on the device: the fluid cells of the current
+// fluid-domain field that are not inside a solid get `ppc` particles each.
+void GridSolver::seedParticles(int ppc, unsigned long long seed) {
+  if (ppc <= 0) throw CudaError("particles per cell must be positive", HFG_ERR_INVALID);
+  // Cells inside a solid get no particles (findFluidGrid,
+  // EulerParticlesTool.cu:20).  The solids are classified at their current
+  // placement, so a scene seeded before its first step already excludes them.
+  BoundarySet bs{};
+  bs.n = (int)bsdf_.size();
+  for (int i = 0; i < bs.n; ++i) {
+    bs.sdf[i] = bsdf_[i]->p;
+    bs.tx[i] = btrans_[3 * i]; bs.ty[i] = btrans_[3 * i + 1]; bs.tz[i] = btrans_[3 * i + 2];
+  }
+  if (bs.n > 0) launched(launchSolidClassify(g_, bs, solidIdx_.p, nullptr, stream_), "solid classify");
+  else check(cudaMemsetAsync(solidIdx_.p, 0, N_, stream_), "memset");
+  const int cellsPerBlock = 4096;
+  int nb = (int)((N_ + cellsPerBlock - 1) / cellsPerBlock);
+  DArray<unsigned int> counts;
+  counts.alloc(nb);
+  DArray<unsigned long long> total;
+  total.alloc(1);
+  const float* fsdf = dom_[cur()].p;
+  launched(launchSeedCount(g_.r, fsdf, solidIdx_.p, counts.p, cellsPerBlock, stream_), "seed count");
+  launched(launchSeedScan(counts.p, nb, total.p, stream_), "seed scan");
+  unsigned long long nf = 0;
+  check(cudaMemcpyAsync(&nf, total.p, 8, cudaMemcpyDeviceToHost, stream_), "read count");
+  check(cudaStreamSynchronize(stream_), "sync");
+  long long n = (long long)nf * ppc;
+  P_ = n;
+  ppos_.alloc(3 * n); pvel_.alloc(3 * n); pv0_.alloc(3 * n); pscalar_.alloc(n); pvector_.alloc(3 * n);
+  if (n > 0) {
+    launched(launchSeedWrite(g_, fsdf, solidIdx_.p, counts.p, cellsPerBlock, ppc, seed, ppos_.p, stream_), "seed write");
+    check(cudaMemsetAsync(pvel_.p, 0, 12 * n, stream_), "memset");
+    check(cudaMemsetAsync(pscalar_.p, 0, 4 * n, stream_), "memset");
+    check(cudaMemsetAsync(pvector_.p, 0, 12 * n, stream_), "memset");
+  }
+  sFlag_ = vFlag_ = velFlag_ = false;
+  check(cudaStreamSynchronize(stream_), "sync");
+}
+
+void GridSolver::setOptions(const hfg_options_t& o) {
+  if (o.precond < 0 || o.precond > 2 || o.tol_mode < 0 || o.tol_mode > 1 || !(o.tol > 0))
+    throw CudaError("invalid solver options", HFG_ERR_INVALID);
+  if (o.extrapolation_layers < 0 || o.extrapolation_layers > kMaxLayers)
+    throw CudaError("extrapolation layers must be in [0, 1000]", HFG_ERR_INVALID);
+  bool mgChanged = o.precond == HFG_PRECOND_MG &&
+                   (!mg_ || o.mg_levels != opt_.mg_levels || o.mg_smooth != opt_.mg_smooth || o.mg_half != opt_.mg_half);
+  opt_ = o;
+  if (mgChanged) {
+    if (mg_) mgDestroy(mg_);
+    mg_ = mgCreate(g_.r, o.mg_levels, o.mg_smooth, o.mg_half != 0);
+  }
+}
+
+SolidVelTable GridSolver::solidTable() const {
+  SolidVelTable t{};
+  t.solidIdx = solidIdx_.p;
+  for (size_t i = 0; i < bsdf_.size(); ++i) {
+    t.vx[i] = bvel_[3 * i]; t.vy[i] = bvel_[3 * i + 1]; t.vz[i] = bvel_[3 * i + 2];
+  }
+  return t;
+}
+
+// Boundary.cpp:115-122: move (translation += -dt * velocity), re-sample,
+// classify.  Solid face velocities are formed on demand from the per-solid
+// table, never stored.
+void GridSolver::updateBoundarys() {
+  BoundarySet b{};
+  b.n = (int)bsdf_.size();
+  for (int i = 0; i < b.n; ++i) {
+    for (int a = 0; a < 3; ++a) btrans_[3 * i + a] = std::fma(-dt_, bvel_[3 * i + a], btrans_[3 * i + a]);
+    b.sdf[i] = bsdf_[i]->p;
+    b.tx[i] = btrans_[3 * i]; b.ty[i] = btrans_[3 * i + 1]; b.tz[i] = btrans_[3 * i + 2];
+    b.vx[i] = bvel_[3 * i]; b.vy[i] = bvel_[3 * i + 1]; b.vz[i] = bvel_[3 * i + 2];
+  }
+  if (b.n == 0) {
+    check(cudaMemsetAsync(solidIdx_.p, 0, N_, stream_), "memset");
+    return;
+  }
+  launched(launchSolidClassify(g_, b, solidIdx_.p, nullptr, stream_), "solid classify");
+}
+
+// ExternalForcesSolver.cpp:50-58: two unit-field axpys, each skipped when all
+// three of its coefficients are below FLT_EPSILON.
+void GridSolver::forcesTerms(float gv[3], bool& doG, float ev[3], bool& doE) const {
+  for (int a = 0; a < 3; ++a) { gv[a] = gravity_[a] * dt_; ev[a] = ext_[a] * dt_; }
+  auto tiny = [](const float v[3]) {
+    return std::fabs(v[0]) < 1.1920929e-07f && std::fabs(v[1]) < 1.1920929e-07f && std::fabs(v[2]) < 1.1920929e-07f;
+  };
+  doG = !tiny(gv);
+  doE = !tiny(ev);
+}
+
+void GridSolver::p2gFace(const float* vel, float* const out[3], float* const copy[3], const float add[3], bool doAdd,
+                         const float add2[3], bool doAdd2) {
+  for (int a = 0; a < 3; ++a) {
+    acc_[a].alloc(F_[a]);
+    check(cudaMemsetAsync(acc_[a].p, 0, acc_[a].bytes(), stream_), "memset");
+  }
+  float2* acc[3] = {acc_[0].p, acc_[1].p, acc_[2].p};
+  launched(launchP2GFace(g_, alg_, ppos_.p, vel, P_, acc, stream_), "p2g");
+  for (int a = 0; a < 3; ++a)
+    launched(launchNormalize(F_[a], acc_[a].p, out[a], copy ? copy[a] : nullptr, add ? add[a] : 0.f, doAdd,
+                             add2 ? add2[a] : 0.f, doAdd2, stream_),
+             "normalize");
+}
+
+void GridSolver::p2gCell(const float* vals, int span, int comp, float* out) {
+  cacc_.alloc(N_);
+  check(cudaMemsetAsync(cacc_.p, 0, cacc_.bytes(), stream_), "memset");
+  launched(launchP2GCell(g_, alg_, ppos_.p, vals, span, comp, P_, cacc_.p, stream_), "p2g cell");
+  launched(launchNormalize(N_, cacc_.p, out, nullptr, 0.f, 0, 0.f, 0, stream_), "normalize cell");
+}
+
+// EulerParticles.cpp:231-325.  Substeps are launched speculatively in chunks;
+// a launch whose slot is already finished does nothing.
+void GridSolver::advectParticles(const float* const vin[3]) {
+  ConstFaceField v{{vin[0], vin[1], vin[2]}};
+  check(cudaMemsetAsync(subState_.p, 0, sizeof(SubstepState) * (subSlots_ + 1), stream_), "memset");
+  launched(launchSubstepBegin(g_, v, ppos_.p, pv0_.p, P_, subState_.p, stream_), "substep begin");
+  long long nclamp = opt_.clamp_mode == 1 ? std::min<long long>(P_, N_) : P_;
+  int slot = 0;
+  for (;;) {
+    for (int k = 0; k < kSubstepChunk && slot < subSlots_; ++k, ++slot)
+      launched(launchSubstep(g_, v, ppos_.p, pv0_.p, P_, acc_rk_, dt_, cfl_, nclamp, subState_.p, slot, stream_),
+               "substep");
+    check(cudaMemcpyAsync(subHost_, subState_.p + slot, sizeof(SubstepState), cudaMemcpyDeviceToHost, stream_),
+          "read substep state");
+    check(cudaStreamSynchronize(stream_), "substep sync");
+    if (subHost_->finished) { substeps_ = subHost_->count; break; }
+    if (slot >= subSlots_) throw CudaError("CFL substep limit reached", HFG_ERR_STATE);
+  }
+}
+
+// GridFluidSolver.cpp:399-416 with the advection solvers' bodies
+// (SemiLagrangian.cpp:135-186, ParticleInCell.cpp:93-108,
+// FluidImplicitParticle.cpp:98-127, MixPICAndFLIP.cpp:64-136); the external
+// forces of ExternalForcesSolver.cpp:50-58 are folded into the pass that
+// writes the advected velocity.
+void GridSolver::computeAdvection() {
+  int ci = cur(), ni = nxt();
+  float gv[3], ev[3];
+  bool doG, doE;
+  forcesTerms(gv, doG, ev, doE);
+  const float* vin[3] = {vel_[ci][0].p, vel_[ci][1].p, vel_[ci][2].p};
+  float* vout[3] = {vel_[ni][0].p, vel_[ni][1].p, vel_[ni][2].p};
+  if (adv_ == HFG_ADV_SEMI_LAGRANGIAN) {
+    stageBegin(1);
+    launched(launchSLFace(g_, acc_rk_, dt_, cvel(ci), cvel(ci), mvel(ni), gv, doG, ev, doE, stream_), "sl face");
+    if (opt_.advect_scalars) {
+      const float* in[4] = {color_[ci][0].p, color_[ci][1].p, color_[ci][2].p, dom_[ci].p};
+      float* out[4] = {color_[ni][0].p, color_[ni][1].p, color_[ni][2].p, dom_[ni].p};
+      launched(launchSLCell(g_, acc_rk_, dt_, cvel(ci), in, out, 4, stream_), "sl cell");
+    }
+    stageEnd(1);
+    return;
+  }
+  if (P_ <= 0) throw CudaError("particle advection needs particles", HFG_ERR_STATE);
+  stageBegin(1);
+  ConstFaceField prev{{prev_[0].p, prev_[1].p, prev_[2].p}};
+  int mode = adv_ == HFG_ADV_PIC ? MODE_PIC : (adv_ == HFG_ADV_FLIP ? MODE_FLIP : MODE_MIX);
+  int first = (mode != MODE_PIC && !velFlag_) ? 1 : 0;
+  launched(launchParticleVelUpdate(g_, mode, alg_, cvel(ci), prev, first, mixing_, ppos_.p, pvel_.p, P_, stream_),
+           "particle velocity");
+  if (mode != MODE_PIC) velFlag_ = true;
+  advectParticles(vin);
+  float* copy[3] = {prev_[0].p, prev_[1].p, prev_[2].p};
+  p2gFace(pvel_.p, vout, mode == MODE_PIC ? nullptr : copy, gv, doG, ev, doE);
+  if (opt_.advect_scalars) {
+    // colour (CC vector) then fluid domain (CC scalar): G2P once, P2G every step
+    if (!vFlag_) {
+      for (int a = 0; a < 3; ++a)
+        launched(launchG2PCell(g_, alg_, color_[ci][a].p, ppos_.p, P_, pvector_.p, 3, a, stream_), "g2p colour");
+      vFlag_ = true;
+    }
+    for (int a = 0; a < 3; ++a) p2gCell(pvector_.p, 3, a, color_[ni][a].p);
+    if (!sFlag_) {
+      launched(launchG2PCell(g_, alg_, dom_[ci].p, ppos_.p, P_, pscalar_.p, 1, 0, stream_), "g2p domain");
+      sFlag_ = true;
+    }
+    p2gCell(pscalar_.p, 1, 0, dom_[ni].p);
+  }
+  stageEnd(1);
+}
+
+void GridSolver::runCg() {
+  const float sx = dt_ / (1.0f * g_.hx * g_.hx), sy = dt_ / (1.0f * g_.hy * g_.hy), sz = dt_ / (1.0f * g_.hz * g_.hz);
+  if (opt_.precond == HFG_PRECOND_MG) {
+    mgRunCg(mg_, g_.r, sx, sy, sz, code_.p, cgx_.p, cgr_.p, partials_.p, cgState_.p, cgHost_, stream_, launches_);
+    return;
+  }
+  int it = 0;
+  for (;;) {
+    for (int k = 0; k < kCgChunk; ++k, ++it) {
+      float* pOld = cgp_[it & 1].p;
+      float* pNew = cgp_[(it + 1) & 1].p;
+      launched(launchCgDirection(g_.r, sx, sy, sz, code_.p, cgr_.p, pOld, pNew, partials_.p, cgState_.p, stream_),
+               "cg direction");
+      launched(launchCgUpdate(g_.r, sx, sy, sz, code_.p, pNew, cgx_.p, cgr_.p, partials_.p, cgState_.p, stream_),
+               "cg update");
+    }
+    check(cudaMemcpyAsync(cgHost_, cgState_.p, sizeof(CgState), cudaMemcpyDeviceToHost, stream_), "read cg state");
+    check(cudaStreamSynchronize(stream_), "cg sync");
+    if (cgHost_->done) break;
+  }
+}
+
+// PressureSolver.cpp:194-197 + GridFluidSolver.cpp:435-525
+void GridSolver::computePressure() {
+  int ni = nxt();
+  stageBegin(3);
+  if (adv_ == HFG_ADV_SEMI_LAGRANGIAN) {
+    launched(launchMarkersFromSDF(N_, solidIdx_.p, dom_[ni].p, markers_.p, stream_), "markers");
+  } else {
+    launched(launchMarkersInit(N_, solidIdx_.p, markers_.p, stream_), "markers");
+    launched(launchMarkersFromParticles(g_, ppos_.p, P_, markers_.p, stream_), "markers");
+  }
+  launched(launchStencilCode(g_.r, markers_.p, code_.p, stream_), "stencil code");
+  stageEnd(3);
+  stageBegin(4);
+  CgState init{};
+  init.maxIter = (int)std::min<long long>(opt_.max_iter < 0 ? N_ : opt_.max_iter, 0x7fffffff);
+  init.precond = opt_.precond == HFG_PRECOND_JACOBI ? 1 : 0;
+  init.tolMode = opt_.tol_mode;
+  init.tol = opt_.tol;
+  *cgHost_ = init;
+  check(cudaMemcpyAsync(cgState_.p, cgHost_, sizeof(CgState), cudaMemcpyHostToDevice, stream_), "cg state");
+  const float sx = dt_ / (1.0f * g_.hx * g_.hx), sy = dt_ / (1.0f * g_.hy * g_.hy), sz = dt_ / (1.0f * g_.hz * g_.hz);
+  ConstFaceField none{{nullptr, nullptr, nullptr}};
+  launched(launchRhsInit(g_, cvel(ni), none, solidTable(), markers_.p, code_.p, sx, sy, sz, nullptr, cgr_.p, cgx_.p,
+                         cgp_[0].p, partials_.p, cgState_.p, stream_),
+           "rhs");
+  if (opt_.precond == HFG_PRECOND_MG) mgSetup(mg_, code_.p, sx, sy, sz, stream_, launches_);
+  stageEnd(4);
+  stageBegin(5);
+  runCg();
+  cgIters_ = cgHost_->iter;
+  cgResid_ = std::sqrt(cgHost_->rr);
+  cgBnorm_ = std::sqrt(cgHost_->bb);
+  cgConverged_ = cgHost_->iter < cgHost_->maxIter || cgHost_->maxIter == 0 ? 1 : 0;
+  stageEnd(5);
+  stageBegin(6);
+  ConstFaceField noneSv{{nullptr, nullptr, nullptr}};
+  launched(launchGradient(g_, dt_ / (1.0f * g_.hx), dt_ / (1.0f * g_.hy), dt_ / (1.0f * g_.hz), markers_.p, cgx_.p,
+                          mvel(ni), noneSv, solidTable(), stream_),
+           "gradient");
+  stageEnd(6);
+}
+
+// GridFluidSolver.cpp:527-537 -> EulerSolverTool.cu:904-969
+void GridSolver::extrapolate() {
+  stageBegin(7);
+  int ni = nxt();
+  int nums = opt_.extrapolation_layers;
+  extrapDepth_ = 0;
+  if (nums > 1) {
+    float* vals[3] = {vel_[ni][0].p, vel_[ni][1].p, vel_[ni][2].p};
+    long long off[3] = {0, F_[0], F_[0] + F_[1]};
+    ExtrapScratch sc{dist_.p, list_.p, hist_.p, offsets_.p, cursor_.p};
+    launched(launchExtrapDistance(fr_, vals, off, nums, sc, stream_), "extrapolation distance", 17);
+    check(cudaMemcpyAsync(offHost_, offsets_.p, sizeof(unsigned int) * (kMaxLayers + 2), cudaMemcpyDeviceToHost,
+                          stream_),
+          "read layer offsets");
+    check(cudaStreamSynchronize(stream_), "extrapolation sync");
+    for (int d = 1; d < nums && d <= kMaxLayers; ++d) {
+      unsigned int b = offHost_[d], e = offHost_[d + 1];
+      if (e <= b) break;
+      launched(launchExtrapLayer(fr_, vals, off, sc, b, e - b, d, stream_), "extrapolation layer");
+      extrapDepth_ = d;
+    }
+  }
+  stageEnd(7);
+}
+
+void GridSolver::updateWithoutPressure() {
+  stageBegin(0);
+  updateBoundarys();
+  stageEnd(0);
+  computeAdvection();
+}
+
+void GridSolver::solvePressure() {
+  computePressure();
+  extrapolate();
+  bufferFlag_ = !bufferFlag_;  // GridFluidSolver.cpp:393-397
+  time_ += dt_;
+}
+
+void GridSolver::update() {
+  updateWithoutPressure();
+  solvePressure();
+  if (timing_) {
+    check(cudaStreamSynchronize(stream_), "sync");
+    for (int i = 0; i < 8; ++i) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, ev_[2 * i], ev_[2 * i + 1]) == cudaSuccess) stageMs_[i] = ms;
+      else stageMs_[i] = 0.f;
+    }
+    cudaGetLastError();
+  }
+}
+
+void GridSolver::synchronize() { check(cudaStreamSynchronize(stream_), "sync"); }
+
+void GridSolver::getVelocity(int which, float* x, float* y, float* z) {
+  int b = which == 0 ? cur() : nxt();
+  float* d[3] = {x, y, z};
+  for (int a = 0; a < 3; ++a)
+    if (d[a]) check(cudaMemcpyAsync(d[a], vel_[b][a].p, F_[a] * 4, cudaMemcpyDeviceToHost, stream_), "download");
+  synchronize();
+}
+
+void GridSolver::getFluidDomain(float* d) {
+  check(cudaMemcpyAsync(d, dom_[cur()].p, N_ * 4, cudaMemcpyDeviceToHost, stream_), "download");
+  synchronize();
+}
+
+void GridSolver::getColor(float* x, float* y, float* z) {
+  float* d[3] = {x, y, z};
+  for (int a = 0; a < 3; ++a)
+    if (d[a]) check(cudaMemcpyAsync(d[a], color_[cur()][a].p, N_ * 4, cudaMemcpyDeviceToHost, stream_), "download");
+  synchronize();
+}
+
+void GridSolver::getMarkers(uint8_t* m) {
+  check(cudaMemcpyAsync(m, markers_.p, N_, cudaMemcpyDeviceToHost, stream_), "download");
+  synchronize();
+}
+
+void GridSolver::getPressure(float* p) {
+  check(cudaMemcpyAsync(p, cgx_.p, N_ * 4, cudaMemcpyDeviceToHost, stream_), "download");
+  synchronize();
+}
+
+void GridSolver::getSolidSDF(float* s) {
+  DArray<float> tmp;
+  tmp.alloc(N_);
+  launched(launchTotalSolidSDF(N_, (int)bsdf_.size(), solidIdx_.p, tmp.p, stream_), "total sdf");
+  check(cudaMemcpyAsync(s, tmp.p, N_ * 4, cudaMemcpyDeviceToHost, stream_), "download");
+  synchronize();
+}
+
+void GridSolver::getSolidVel(float* x, float* y, float* z) {
+  DArray<float> t[3];
+  for (int a = 0; a < 3; ++a) t[a].alloc(F_[a]);
+  FaceField f{{t[0].p, t[1].p, t[2].p}};
+  launched(launchSolidVelField(g_, solidTable(), f, stream_), "solid vel");
+  float* d[3] = {x, y, z};
+  for (int a = 0; a < 3; ++a) check(cudaMemcpyAsync(d[a], t[a].p, F_[a] * 4, cudaMemcpyDeviceToHost, stream_), "download");
+  synchronize();
+}
+
+void GridSolver::getParticles(float* pos, float* vel) {
+  if (P_ > 0) {
+    if (pos) check(cudaMemcpyAsync(pos, ppos_.p, 12 * P_, cudaMemcpyDeviceToHost, stream_), "download");
+    if (vel) check(cudaMemcpyAsync(vel, pvel_.p, 12 * P_, cudaMemcpyDeviceToHost, stream_), "download");
+  }
+  synchronize();
+}
+
+void GridSolver::getStats(hfg_stats_t* st) {
+  std::memset(st, 0, sizeof(*st));
+  st->cg_iterations = cgIters_;
+  st->cg_residual = cgResid_;
+  st->cg_rhs_norm = cgBnorm_;
+  st->cg_converged = cgConverged_;
+  st->substeps = substeps_;
+  st->extrapolation_layers = extrapDepth_;
+  st->sim_time = time_;
+  st->num_particles = P_;
+  st->fluid_cells = fluidCells_;
+  for (int i = 0; i < 8; ++i) st->stage_ms[i] = stageMs_[i];
+}
+
+}  // namespace hfg

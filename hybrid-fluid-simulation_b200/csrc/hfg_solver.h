@@ -1,0 +1,167 @@
+// hfg_solver.h -- host orchestration of one grid fluid scene on one GPU.
+//
+// GridSolver mirrors CGridFluidSolver (MPhysics/GridFluidSolver.h:17-137):
+// double-buffered face velocities, colour / fluid-domain fields, solid
+// boundaries, the advection solver (semi-Lagrangian, PIC, FLIP or the PIC/FLIP
+// mix with its particles), external forces, the pressure projection and the
+// velocity extrapolation.  All state is device resident; every stage is a
+// kernel on the solver's own stream.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/hfgrid.h"
+#include "hfg_kernels.h"
+
+namespace hfg {
+
+struct CudaError : std::runtime_error {
+  int code;
+  CudaError(const std::string& m, int c) : std::runtime_error(m), code(c) {}
+};
+
+void check(cudaError_t e, const char* what);
+
+// Owning device array.
+template <class T> struct DArray {
+  T* p = nullptr;
+  size_t n = 0;
+  DArray() = default;
+  DArray(const DArray&) = delete;
+  DArray& operator=(const DArray&) = delete;
+  ~DArray() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    if (count == n && p) return;
+    release();
+    if (count == 0) return;
+    cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      throw CudaError(std::string("cudaMalloc failed: ") + cudaGetErrorString(e), HFG_ERR_NOMEM);
+    }
+    n = count;
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+struct Multigrid;  // hfg_mg.cu
+
+class GridSolver {
+ public:
+  GridSolver(float dt, Dim3i res, const float origin[3], const float spacing[3]);
+  ~GridSolver();
+
+  // ---- setters (GridFluidSolver.cpp:198-244) ----
+  void addBoundary(const float* sdfHost, const float vel[3]);
+  void addExternalForce(const float f[3]);
+  void setVelocity(const float* x, const float* y, const float* z);
+  void setFluidDomain(const float* d);
+  void setColor(const float* x, const float* y, const float* z);
+  void fluidDomainFromBBox(const float mn[3], const float mx[3]);
+  void setAdvection(int kind, int acc, int alg, float cfl, float mixing);
+  void seedParticles(int ppc, unsigned long long seed);
+  void setParticles(const float* pos, const float* vel, long long n);
+  void setOptions(const hfg_options_t& o);
+  void enableTiming(bool on);
+
+  // ---- the step (GridFluidSolver.cpp:336-370) ----
+  void update();
+  void updateWithoutPressure();
+  void solvePressure();
+
+  // ---- getters ----
+  void getVelocity(int which, float* x, float* y, float* z);
+  void getFluidDomain(float* d);
+  void getColor(float* x, float* y, float* z);
+  void getMarkers(uint8_t* m);
+  void getPressure(float* p);
+  void getSolidSDF(float* s);
+  void getSolidVel(float* x, float* y, float* z);
+  void getParticles(float* pos, float* vel);
+  void getStats(hfg_stats_t* st);
+  void synchronize();
+
+  const Geom& geom() const { return g_; }
+  cudaStream_t stream() const { return stream_; }
+  long long numParticles() const { return P_; }
+  long long launches() const { return launches_; }
+  const hfg_options_t& options() const { return opt_; }
+
+ private:
+  void updateBoundarys();
+  void computeAdvection();
+  void advectParticles(const float* const vin[3]);
+  void p2gFace(const float* vel, float* const out[3], float* const copy[3], const float add[3], bool doAdd,
+               const float add2[3], bool doAdd2);
+  void p2gCell(const float* vals, int span, int comp, float* out);
+  void computePressure();
+  void runCg();
+  void extrapolate();
+  void forcesTerms(float gv[3], bool& doG, float ev[3], bool& doE) const;
+  int cur() const { return bufferFlag_ ? 1 : 0; }  // velocity/colour/domain "current" buffer
+  int nxt() const { return bufferFlag_ ? 0 : 1; }
+  ConstFaceField cvel(int b) const { return ConstFaceField{{vel_[b][0].p, vel_[b][1].p, vel_[b][2].p}}; }
+  FaceField mvel(int b) { return FaceField{{vel_[b][0].p, vel_[b][1].p, vel_[b][2].p}}; }
+  SolidVelTable solidTable() const;
+  void launched(cudaError_t e, const char* what, int count = 1);
+  void stageBegin(int i);
+  void stageEnd(int i);
+
+  Geom g_;
+  Dim3i fr_[3];
+  long long N_, F_[3], Ftot_;
+  float dt_;
+  double time_ = 0.0;
+  bool bufferFlag_ = true;
+  hfg_options_t opt_;
+  cudaStream_t stream_ = nullptr;
+  long long launches_ = 0;
+
+  DArray<float> vel_[2][3], prev_[3], color_[2][3], dom_[2], solidVel_[3];
+  DArray<uint8_t> solidIdx_, markers_, code_;
+  DArray<float> cgx_, cgr_, cgp_[2];
+  DArray<double> partials_;
+  DArray<CgState> cgState_;
+  CgState* cgHost_ = nullptr;  // pinned
+  DArray<SubstepState> subState_;
+  SubstepState* subHost_ = nullptr;  // pinned
+  int subSlots_ = 4096;
+  DArray<float2> acc_[3], cacc_;
+  DArray<uint16_t> dist_;
+  DArray<unsigned int> list_, hist_, offsets_, cursor_;
+  unsigned int* offHost_ = nullptr;  // pinned
+
+  long long P_ = 0;
+  DArray<float> ppos_, pvel_, pv0_, pscalar_, pvector_;
+
+  std::vector<DArray<float>*> bsdf_;
+  std::vector<float> bvel_, btrans_;
+  float ext_[3] = {0, 0, 0};
+  float gravity_[3] = {0.f, -9.8f, 0.f};  // ExternalForcesSolver.h:25
+
+  int adv_ = HFG_ADV_SEMI_LAGRANGIAN, acc_rk_ = HFG_RK3, alg_ = HFG_LINEAR;
+  float cfl_ = 1.f, mixing_ = 0.1f;
+  bool sFlag_ = false, vFlag_ = false, velFlag_ = false;
+
+  // last-step statistics
+  long long cgIters_ = 0;
+  double cgResid_ = 0, cgBnorm_ = 0;
+  int cgConverged_ = 0, substeps_ = 0, extrapDepth_ = 0;
+  long long fluidCells_ = -1;
+
+  Multigrid* mg_ = nullptr;
+
+  bool timing_ = false;
+  cudaEvent_t ev_[16] = {};
+  float stageMs_[8] = {};
+};
+
+}  // namespace hfg

@@ -1,0 +1,455 @@
+"""ctypes binding of libhfgrid.so (include/hfgrid.h) for Python callers.
+
+The library is the product: C++ host code and sm_100a CUDA kernels behind a
+C ABI.  This module only marshals arguments.  `Solver` mirrors the reference's
+CGridFluidSolver (MPhysics/GridFluidSolver.h:17-137) with numpy arrays in and
+out; the `op_*` functions mirror the reference's per-stage Invoker functions
+and take CUDA device pointers (torch tensors are accepted) plus a stream.
+
+There is no fallback: if libhfgrid.so cannot be loaded or a call fails, an
+exception is raised.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhfgrid.so")
+
+# enums (include/hfgrid.h)
+ADV_SEMI_LAGRANGIAN, ADV_PIC, ADV_FLIP, ADV_MIX_PIC_FLIP = 0, 1, 2, 3
+RK1, RK2, RK3 = 0, 1, 2
+P2GSUM, G2PNEAREST, LINEAR, QUADRATIC, CUBIC = 0, 1, 2, 3, 4
+PRECOND_IDENTITY, PRECOND_JACOBI, PRECOND_MG = 0, 1, 2
+TOL_REFERENCE, TOL_RELATIVE = 0, 1
+HFG_OK, HFG_ERR_NOT_CONVERGED = 0, -5
+
+
+class HfgError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"hfgrid error {code}: {msg}")
+        self.code = code
+
+
+class Options(C.Structure):
+    _fields_ = [
+        ("precond", C.c_int), ("tol_mode", C.c_int), ("tol", C.c_double), ("max_iter", C.c_longlong),
+        ("clamp_mode", C.c_int), ("advect_scalars", C.c_int), ("extrapolation_layers", C.c_int),
+        ("mg_levels", C.c_int), ("mg_smooth", C.c_int), ("mg_half", C.c_int),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("cg_iterations", C.c_longlong), ("cg_residual", C.c_double), ("cg_rhs_norm", C.c_double),
+        ("cg_converged", C.c_int), ("substeps", C.c_int), ("extrapolation_layers", C.c_int),
+        ("sim_time", C.c_double), ("num_particles", C.c_longlong), ("fluid_cells", C.c_longlong),
+        ("stage_ms", C.c_float * 8),
+    ]
+
+    def as_dict(self) -> dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "stage_ms"}
+        d["stage_ms"] = list(self.stage_ms)
+        return d
+
+
+_lib = None
+
+I3 = C.c_int * 3
+F3 = C.c_float * 3
+PF = C.POINTER(C.c_float)
+PU8 = C.POINTER(C.c_uint8)
+VP = C.c_void_p
+
+
+def _signatures(lib):
+    S = C.c_void_p  # hfg_solver_t
+    sig = {
+        "hfg_init": (C.c_int, [C.c_int]),
+        "hfg_last_error": (C.c_char_p, []),
+        "hfg_version": (C.c_char_p, []),
+        "hfg_default_options": (None, [C.POINTER(Options)]),
+        "hfg_solver_create": (C.c_int, [C.c_float, I3, F3, F3, C.POINTER(S)]),
+        "hfg_solver_destroy": (C.c_int, [S]),
+        "hfg_solver_add_solid_boundary": (C.c_int, [S, PF, F3]),
+        "hfg_solver_add_external_force": (C.c_int, [S, F3]),
+        "hfg_solver_set_velocity_field": (C.c_int, [S, PF, PF, PF]),
+        "hfg_solver_set_fluid_domain_field": (C.c_int, [S, PF]),
+        "hfg_solver_set_color_field": (C.c_int, [S, PF, PF, PF]),
+        "hfg_solver_generate_fluid_domain_from_bbox": (C.c_int, [S, F3, F3]),
+        "hfg_solver_set_advection": (C.c_int, [S, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float]),
+        "hfg_solver_seed_particles": (C.c_int, [S, C.c_int, C.c_ulonglong]),
+        "hfg_solver_set_particles": (C.c_int, [S, PF, PF, C.c_longlong]),
+        "hfg_solver_set_options": (C.c_int, [S, C.POINTER(Options)]),
+        "hfg_solver_enable_timing": (C.c_int, [S, C.c_int]),
+        "hfg_solver_update": (C.c_int, [S]),
+        "hfg_solver_update_steps": (C.c_int, [S, C.c_int]),
+        "hfg_solver_update_without_pressure": (C.c_int, [S]),
+        "hfg_solver_solve_pressure": (C.c_int, [S]),
+        "hfg_solver_get_velocity_field": (C.c_int, [S, C.c_int, PF, PF, PF]),
+        "hfg_solver_get_fluid_domain_field": (C.c_int, [S, PF]),
+        "hfg_solver_get_color_field": (C.c_int, [S, PF, PF, PF]),
+        "hfg_solver_get_markers": (C.c_int, [S, PU8]),
+        "hfg_solver_get_pressure": (C.c_int, [S, PF]),
+        "hfg_solver_get_solid_sdf": (C.c_int, [S, PF]),
+        "hfg_solver_get_solid_vel_field": (C.c_int, [S, PF, PF, PF]),
+        "hfg_solver_num_particles": (C.c_longlong, [S]),
+        "hfg_solver_get_particles": (C.c_int, [S, PF, PF]),
+        "hfg_solver_get_stats": (C.c_int, [S, C.POINTER(Stats)]),
+        "hfg_solver_get_grid": (C.c_int, [S, I3, F3, F3]),
+        "hfg_solver_stream": (C.c_void_p, [S]),
+        "hfg_solver_launch_count": (C.c_longlong, [S]),
+        "hfg_solver_synchronize": (C.c_int, [S]),
+        "hfg_op_markers_from_particles": (C.c_int, [I3, F3, F3, VP, VP, C.c_longlong, VP, VP]),
+        "hfg_op_bin_counts": (C.c_int, [I3, F3, F3, VP, C.c_longlong, VP, VP]),
+        "hfg_op_markers_from_sdf": (C.c_int, [I3, VP, VP, VP, VP]),
+        "hfg_op_build_matrix_a": (C.c_int, [I3, F3, C.c_float, VP, VP, VP]),
+        "hfg_op_apply_a": (C.c_int, [I3, F3, C.c_float, VP, VP, VP, VP]),
+        "hfg_op_build_rhs": (C.c_int, [I3, F3, VP, VP, VP, VP, VP, VP, VP, VP, VP]),
+        "hfg_op_project": (C.c_int, [I3, F3, C.c_float, VP, VP, VP, VP, VP, VP, VP, C.c_int, C.c_int, C.c_double,
+                                     C.c_longlong, VP, C.POINTER(C.c_double), VP]),
+        "hfg_op_extrapolate_fc": (C.c_int, [I3, VP, VP, VP, C.c_int, VP]),
+        "hfg_op_extrapolate_cc": (C.c_int, [I3, VP, C.c_int, VP]),
+        "hfg_op_sample_fc": (C.c_int, [I3, F3, F3, VP, VP, VP, VP, C.c_longlong, VP, VP]),
+        "hfg_op_sample_cc": (C.c_int, [I3, F3, F3, VP, VP, C.c_longlong, VP, VP]),
+        "hfg_op_g2p_fc": (C.c_int, [I3, F3, F3, VP, VP, VP, VP, C.c_longlong, C.c_int, VP, VP]),
+        "hfg_op_g2p_cc": (C.c_int, [I3, F3, F3, VP, VP, C.c_longlong, C.c_int, VP, VP]),
+        "hfg_op_p2g_fc": (C.c_int, [I3, F3, F3, VP, VP, C.c_longlong, C.c_int, VP, VP, VP, VP, VP, VP, VP]),
+        "hfg_op_p2g_cc": (C.c_int, [I3, F3, F3, VP, VP, C.c_longlong, C.c_int, C.c_int, VP, VP, VP]),
+        "hfg_op_advect_particles": (C.c_int, [I3, F3, F3, VP, VP, VP, VP, C.c_longlong, C.c_float, C.c_float,
+                                              C.c_int, C.c_int, C.POINTER(C.c_int), VP]),
+        "hfg_op_sl_advect_fc": (C.c_int, [I3, F3, F3, VP, VP, VP, VP, VP, VP, C.c_float, C.c_int, VP, VP, VP, VP]),
+        "hfg_op_sl_advect_cc": (C.c_int, [I3, F3, F3, VP, VP, VP, VP, C.c_float, C.c_int, VP, VP]),
+        "hfg_op_fluid_domain_from_bbox": (C.c_int, [I3, F3, F3, F3, F3, VP, VP]),
+        "hfg_op_seed_particles": (C.c_int, [I3, F3, F3, VP, VP, C.c_int, C.c_ulonglong, VP, C.c_longlong,
+                                            C.POINTER(C.c_longlong), VP]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+def lib():
+    """Load libhfgrid.so (raises if it is missing: there is no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} not built; run `python {os.path.join(HERE, 'build.py')}`")
+        _lib = _signatures(C.CDLL(LIB_PATH))
+    return _lib
+
+
+def _check(code: int):
+    if code != HFG_OK:
+        raise HfgError(code, lib().hfg_last_error().decode())
+
+
+def init(device: int = 0):
+    _check(lib().hfg_init(device))
+
+
+def default_options() -> Options:
+    o = Options()
+    lib().hfg_default_options(C.byref(o))
+    return o
+
+
+def _f3(v) -> F3:
+    return F3(*[float(x) for x in v])
+
+
+def _i3(v) -> I3:
+    return I3(*[int(x) for x in v])
+
+
+def _fptr(a: np.ndarray):
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(PF)
+
+
+def face_shapes(res):
+    nx, ny, nz = res
+    return ((nz, ny, nx + 1), (nz, ny + 1, nx), (nz + 1, ny, nx))
+
+
+class Solver:
+    """CGridFluidSolver on the GPU (GridFluidSolver.cpp:32-41)."""
+
+    def __init__(self, dt: float, res, origin=(0.0, 0.0, 0.0), spacing=(1.0, 1.0, 1.0)):
+        self.res = tuple(int(r) for r in res)
+        self.origin = tuple(float(o) for o in origin)
+        self.spacing = tuple(float(h) for h in spacing)
+        self.dt = float(dt)
+        h = C.c_void_p()
+        _check(lib().hfg_solver_create(C.c_float(dt), _i3(self.res), _f3(origin), _f3(spacing), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().hfg_solver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def n_cells(self) -> int:
+        return self.res[0] * self.res[1] * self.res[2]
+
+    # ---- setters ----
+    def add_solid_boundary(self, sdf: np.ndarray, vel=(0.0, 0.0, 0.0)):
+        a = np.ascontiguousarray(sdf, dtype=np.float32).reshape(-1)
+        assert a.size == self.n_cells
+        _check(lib().hfg_solver_add_solid_boundary(self._h, _fptr(a), _f3(vel)))
+
+    def add_external_force(self, f):
+        _check(lib().hfg_solver_add_external_force(self._h, _f3(f)))
+
+    def set_velocity_field(self, x, y, z):
+        xs = [np.ascontiguousarray(v, dtype=np.float32).reshape(-1) for v in (x, y, z)]
+        _check(lib().hfg_solver_set_velocity_field(self._h, *[_fptr(v) for v in xs]))
+
+    def set_fluid_domain_field(self, d):
+        a = np.ascontiguousarray(d, dtype=np.float32).reshape(-1)
+        _check(lib().hfg_solver_set_fluid_domain_field(self._h, _fptr(a)))
+
+    def set_color_field(self, x, y, z):
+        xs = [np.ascontiguousarray(v, dtype=np.float32).reshape(-1) for v in (x, y, z)]
+        _check(lib().hfg_solver_set_color_field(self._h, *[_fptr(v) for v in xs]))
+
+    def generate_fluid_domain_from_bbox(self, mn, mx):
+        _check(lib().hfg_solver_generate_fluid_domain_from_bbox(self._h, _f3(mn), _f3(mx)))
+
+    def set_advection(self, kind: int, accuracy: int = RK3, alg: int = LINEAR, cfl: float = 1.0, mixing: float = 0.1):
+        _check(lib().hfg_solver_set_advection(self._h, kind, accuracy, alg, C.c_float(cfl), C.c_float(mixing)))
+
+    def seed_particles(self, per_cell: int, seed: int):
+        _check(lib().hfg_solver_seed_particles(self._h, per_cell, seed))
+
+    def set_particles(self, pos: np.ndarray, vel: Optional[np.ndarray] = None):
+        p = np.ascontiguousarray(pos, dtype=np.float32).reshape(-1)
+        v = None if vel is None else np.ascontiguousarray(vel, dtype=np.float32).reshape(-1)
+        _check(lib().hfg_solver_set_particles(self._h, _fptr(p), None if v is None else _fptr(v), p.size // 3))
+
+    def set_options(self, **kw):
+        o = default_options()
+        for k, v in kw.items():
+            setattr(o, k, v)
+        _check(lib().hfg_solver_set_options(self._h, C.byref(o)))
+
+    def enable_timing(self, on=True):
+        _check(lib().hfg_solver_enable_timing(self._h, int(on)))
+
+    # ---- step ----
+    def update(self, steps: int = 1):
+        if steps == 1:
+            _check(lib().hfg_solver_update(self._h))
+        else:
+            _check(lib().hfg_solver_update_steps(self._h, steps))
+
+    def update_without_pressure(self):
+        _check(lib().hfg_solver_update_without_pressure(self._h))
+
+    def solve_pressure(self):
+        _check(lib().hfg_solver_solve_pressure(self._h))
+
+    def synchronize(self):
+        _check(lib().hfg_solver_synchronize(self._h))
+
+    # ---- getters ----
+    def velocity_field(self, which: int = 0):
+        out = [np.empty(s, np.float32) for s in face_shapes(self.res)]
+        _check(lib().hfg_solver_get_velocity_field(self._h, which, *[_fptr(o) for o in out]))
+        return out
+
+    def fluid_domain_field(self):
+        out = np.empty(self.res[::-1], np.float32)
+        _check(lib().hfg_solver_get_fluid_domain_field(self._h, _fptr(out)))
+        return out
+
+    def color_field(self):
+        out = [np.empty(self.res[::-1], np.float32) for _ in range(3)]
+        _check(lib().hfg_solver_get_color_field(self._h, *[_fptr(o) for o in out]))
+        return out
+
+    def markers(self):
+        out = np.empty(self.res[::-1], np.uint8)
+        _check(lib().hfg_solver_get_markers(self._h, out.ctypes.data_as(PU8)))
+        return out
+
+    def pressure(self):
+        out = np.empty(self.res[::-1], np.float32)
+        _check(lib().hfg_solver_get_pressure(self._h, _fptr(out)))
+        return out
+
+    def solid_sdf(self):
+        out = np.empty(self.res[::-1], np.float32)
+        _check(lib().hfg_solver_get_solid_sdf(self._h, _fptr(out)))
+        return out
+
+    def solid_vel_field(self):
+        out = [np.empty(s, np.float32) for s in face_shapes(self.res)]
+        _check(lib().hfg_solver_get_solid_vel_field(self._h, *[_fptr(o) for o in out]))
+        return out
+
+    @property
+    def num_particles(self) -> int:
+        return int(lib().hfg_solver_num_particles(self._h))
+
+    def particles(self):
+        n = self.num_particles
+        pos = np.empty((n, 3), np.float32)
+        vel = np.empty((n, 3), np.float32)
+        _check(lib().hfg_solver_get_particles(self._h, _fptr(pos), _fptr(vel)))
+        return pos, vel
+
+    def copy_particles_into(self, pos: np.ndarray, vel: Optional[np.ndarray] = None):
+        _check(lib().hfg_solver_get_particles(self._h, _fptr(pos), None if vel is None else _fptr(vel)))
+
+    def stats(self) -> dict:
+        s = Stats()
+        _check(lib().hfg_solver_get_stats(self._h, C.byref(s)))
+        return s.as_dict()
+
+    @property
+    def stream(self) -> int:
+        return int(lib().hfg_solver_stream(self._h) or 0)
+
+    @property
+    def launch_count(self) -> int:
+        return int(lib().hfg_solver_launch_count(self._h))
+
+
+# ---------------------------------------------------------------- operators --
+def _ptr(t) -> Optional[int]:
+    """Device pointer of a torch tensor (or an int address / None)."""
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return t
+    return int(t.data_ptr())
+
+
+def _stream(stream) -> Optional[int]:
+    if stream is None:
+        import torch
+        return int(torch.cuda.current_stream().cuda_stream)
+    return int(stream)
+
+
+def op_markers_from_particles(res, origin, spacing, solid_sdf, pos, markers, stream=None):
+    n = pos.numel() // 3
+    _check(lib().hfg_op_markers_from_particles(_i3(res), _f3(origin), _f3(spacing), _ptr(solid_sdf), _ptr(pos), n,
+                                               _ptr(markers), _stream(stream)))
+
+
+def op_bin_counts(res, origin, spacing, pos, counts, stream=None):
+    _check(lib().hfg_op_bin_counts(_i3(res), _f3(origin), _f3(spacing), _ptr(pos), pos.numel() // 3, _ptr(counts),
+                                   _stream(stream)))
+
+
+def op_markers_from_sdf(res, solid_sdf, fluid_sdf, markers, stream=None):
+    _check(lib().hfg_op_markers_from_sdf(_i3(res), _ptr(solid_sdf), _ptr(fluid_sdf), _ptr(markers), _stream(stream)))
+
+
+def op_build_matrix_a(res, spacing, dt, markers, A, stream=None):
+    _check(lib().hfg_op_build_matrix_a(_i3(res), _f3(spacing), C.c_float(dt), _ptr(markers), _ptr(A), _stream(stream)))
+
+
+def op_apply_a(res, spacing, dt, markers, x, y, stream=None):
+    _check(lib().hfg_op_apply_a(_i3(res), _f3(spacing), C.c_float(dt), _ptr(markers), _ptr(x), _ptr(y),
+                                _stream(stream)))
+
+
+def op_build_rhs(res, spacing, vel, solid_vel, markers, b, stream=None):
+    _check(lib().hfg_op_build_rhs(_i3(res), _f3(spacing), *[_ptr(v) for v in vel], *[_ptr(v) for v in solid_vel],
+                                  _ptr(markers), _ptr(b), _stream(stream)))
+
+
+def op_project(res, spacing, dt, markers, vel, solid_vel, precond=PRECOND_IDENTITY, tol_mode=TOL_REFERENCE,
+               tol=1e-3, max_iter=-1, p_out=None, stream=None):
+    stats = (C.c_double * 3)()
+    code = lib().hfg_op_project(_i3(res), _f3(spacing), C.c_float(dt), _ptr(markers), *[_ptr(v) for v in vel],
+                                *[_ptr(v) for v in solid_vel], precond, tol_mode, C.c_double(tol), max_iter,
+                                _ptr(p_out), stats, _stream(stream))
+    if code not in (HFG_OK, HFG_ERR_NOT_CONVERGED):
+        _check(code)
+    return {"iterations": int(stats[0]), "residual": stats[1], "rhs_norm": stats[2], "converged": code == HFG_OK}
+
+
+def op_extrapolate_fc(res, vel, layers=1000, stream=None):
+    _check(lib().hfg_op_extrapolate_fc(_i3(res), *[_ptr(v) for v in vel], layers, _stream(stream)))
+
+
+def op_extrapolate_cc(res, f, layers=1000, stream=None):
+    _check(lib().hfg_op_extrapolate_cc(_i3(res), _ptr(f), layers, _stream(stream)))
+
+
+def op_sample_fc(res, origin, spacing, vel, pos, out, stream=None):
+    _check(lib().hfg_op_sample_fc(_i3(res), _f3(origin), _f3(spacing), *[_ptr(v) for v in vel], _ptr(pos),
+                                  pos.numel() // 3, _ptr(out), _stream(stream)))
+
+
+def op_sample_cc(res, origin, spacing, f, pos, out, stream=None):
+    _check(lib().hfg_op_sample_cc(_i3(res), _f3(origin), _f3(spacing), _ptr(f), _ptr(pos), pos.numel() // 3,
+                                  _ptr(out), _stream(stream)))
+
+
+def op_g2p_fc(res, origin, spacing, vel, pos, alg, out, stream=None):
+    _check(lib().hfg_op_g2p_fc(_i3(res), _f3(origin), _f3(spacing), *[_ptr(v) for v in vel], _ptr(pos),
+                               pos.numel() // 3, alg, _ptr(out), _stream(stream)))
+
+
+def op_g2p_cc(res, origin, spacing, f, pos, alg, out, stream=None):
+    _check(lib().hfg_op_g2p_cc(_i3(res), _f3(origin), _f3(spacing), _ptr(f), _ptr(pos), pos.numel() // 3, alg,
+                               _ptr(out), _stream(stream)))
+
+
+def op_p2g_fc(res, origin, spacing, pos, vel, alg, out, weights=(None, None, None), stream=None):
+    _check(lib().hfg_op_p2g_fc(_i3(res), _f3(origin), _f3(spacing), _ptr(pos), _ptr(vel), pos.numel() // 3, alg,
+                               *[_ptr(v) for v in out], *[_ptr(w) for w in weights], _stream(stream)))
+
+
+def op_p2g_cc(res, origin, spacing, pos, val, alg, out, weights=None, normalize=True, stream=None):
+    _check(lib().hfg_op_p2g_cc(_i3(res), _f3(origin), _f3(spacing), _ptr(pos), _ptr(val), pos.numel() // 3, alg,
+                               int(normalize), _ptr(out), _ptr(weights), _stream(stream)))
+
+
+def op_advect_particles(res, origin, spacing, vel, pos, dt, cfl=1.0, accuracy=RK3, clamp_mode=1, stream=None):
+    n = C.c_int(0)
+    _check(lib().hfg_op_advect_particles(_i3(res), _f3(origin), _f3(spacing), *[_ptr(v) for v in vel], _ptr(pos),
+                                         pos.numel() // 3, C.c_float(dt), C.c_float(cfl), accuracy, clamp_mode,
+                                         C.byref(n), _stream(stream)))
+    return n.value
+
+
+def op_sl_advect_fc(res, origin, spacing, field, vel, dt, accuracy, out, stream=None):
+    _check(lib().hfg_op_sl_advect_fc(_i3(res), _f3(origin), _f3(spacing), *[_ptr(v) for v in field],
+                                     *[_ptr(v) for v in vel], C.c_float(dt), accuracy, *[_ptr(v) for v in out],
+                                     _stream(stream)))
+
+
+def op_sl_advect_cc(res, origin, spacing, field, vel, dt, accuracy, out, stream=None):
+    _check(lib().hfg_op_sl_advect_cc(_i3(res), _f3(origin), _f3(spacing), _ptr(field), *[_ptr(v) for v in vel],
+                                     C.c_float(dt), accuracy, _ptr(out), _stream(stream)))
+
+
+def op_fluid_domain_from_bbox(res, origin, spacing, mn, mx, out, stream=None):
+    _check(lib().hfg_op_fluid_domain_from_bbox(_i3(res), _f3(origin), _f3(spacing), _f3(mn), _f3(mx), _ptr(out),
+                                               _stream(stream)))
+
+
+def op_seed_particles(res, origin, spacing, fluid_sdf, solid_sdf, per_cell, seed, pos=None, capacity=0, stream=None):
+    n = C.c_longlong(0)
+    _check(lib().hfg_op_seed_particles(_i3(res), _f3(origin), _f3(spacing), _ptr(fluid_sdf), _ptr(solid_sdf),
+                                       per_cell, seed, _ptr(pos), capacity, C.byref(n), _stream(stream)))
+    return n.value

@@ -1,0 +1,220 @@
+/* hfgrid.h -- C ABI of the B200-native grid half of the hybrid fluid step.
+ *
+ * libhfgrid.so replaces, for one GPU, the grid solver of the reference engine
+ * junwei-jiang/Hybrid-Fluid-Simulation (MPhysics/).  Two layers are exported:
+ *
+ *   hfg_solver_*  a handle-based mirror of CGridFluidSolver
+ *                 (MPhysics/GridFluidSolver.h:17-137): same construction,
+ *                 setters, update()/updateWithoutPressure()/solvePressure()
+ *                 split and getters, with host buffers in and out;
+ *   hfg_op_*      one entry point per reference "Invoker" stage of the step
+ *                 (device pointers + a CUDA stream), the operator API the
+ *                 parity tests drive.
+ *
+ * The reference-compatible MPhysicsAPI exports live in mphysics.h.
+ *
+ * Every function returns HFG_OK (0) or a negative status; hfg_last_error()
+ * gives the message of the last failure on the calling thread.  No C++
+ * exception crosses this boundary.  Arrays follow the reference layout:
+ * cell-centred (nx*ny*nz, x fastest), face-centred X (nx+1)*ny*nz,
+ * Y nx*(ny+1)*nz, Z nx*ny*(nz+1); particles as xyz triples; FP32 values,
+ * uint8 cell markers (0 air, 1 fluid, 2 solid).
+ */
+#ifndef HFGRID_H
+#define HFGRID_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HFG_API __attribute__((visibility("default")))
+
+enum {
+  HFG_OK = 0,
+  HFG_ERR_INVALID = -1,      /* bad argument */
+  HFG_ERR_CUDA = -2,         /* CUDA runtime error */
+  HFG_ERR_NOMEM = -3,        /* device allocation failed */
+  HFG_ERR_STATE = -4,        /* call not valid in the solver's state */
+  HFG_ERR_NOT_CONVERGED = -5,/* CG hit its iteration cap (stats still valid) */
+  HFG_ERR_UNSUPPORTED = -6,
+  HFG_ERR_TIMEOUT = -7
+};
+
+/* Advection solvers (GridFluidSolver.cpp:90-158). */
+enum { HFG_ADV_SEMI_LAGRANGIAN = 0, HFG_ADV_PIC = 1, HFG_ADV_FLIP = 2, HFG_ADV_MIX_PIC_FLIP = 3 };
+/* EAdvectionAccuracy (MPhysics/EnumType.h:12-17). */
+enum { HFG_RK1 = 0, HFG_RK2 = 1, HFG_RK3 = 2 };
+/* EPGTransferAlgorithm (MPhysics/EnumType.h:19-26). */
+enum { HFG_P2GSUM = 0, HFG_G2PNEAREST = 1, HFG_LINEAR = 2, HFG_QUADRATIC = 3, HFG_CUBIC = 4 };
+/* CG preconditioners: identity is the reference's "InvDia" (PressureSolver.cpp:12-15). */
+enum { HFG_PRECOND_IDENTITY = 0, HFG_PRECOND_JACOBI = 1, HFG_PRECOND_MG = 2 };
+/* CG stopping rules: the reference's sqrt(||r||_2) < tol (CuMatrixFreePCG.cpp:28,51),
+ * or the relative ||r||_2 / ||b||_2 < tol. */
+enum { HFG_TOL_REFERENCE = 0, HFG_TOL_RELATIVE = 1 };
+
+typedef struct hfg_solver_s* hfg_solver_t;
+
+typedef struct {
+  int precond;            /* HFG_PRECOND_* (default identity) */
+  int tol_mode;           /* HFG_TOL_* (default reference) */
+  double tol;             /* default 1e-3 (CuMatrixFreePCG.h:28) */
+  long long max_iter;     /* <0: N cells (PressureSolver.cpp:150-151) */
+  int clamp_mode;         /* 1: clamp the first min(N,P) particles like the
+                             reference launch (EulerParticlesTool.cu:880);
+                             0: clamp every particle */
+  int advect_scalars;     /* 1: also carry the colour / fluid-domain fields */
+  int extrapolation_layers; /* default 1000 (GridFluidSolver.cpp:176) */
+  int mg_levels;          /* multigrid levels for HFG_PRECOND_MG (0 = auto) */
+  int mg_smooth;          /* smoothing sweeps per level (0 = default) */
+  int mg_half;            /* 1: multigrid smoothing stores in half precision */
+} hfg_options_t;
+
+typedef struct {
+  long long cg_iterations;
+  double cg_residual;       /* final ||r||_2 (FP64 reduction on the GPU) */
+  double cg_rhs_norm;       /* ||b||_2 */
+  int cg_converged;
+  int substeps;             /* CFL substeps of the last particle advection */
+  int extrapolation_layers; /* deepest layer filled by the last extrapolation */
+  double sim_time;
+  long long num_particles;
+  long long fluid_cells;
+  float stage_ms[8];        /* boundaries, advection, forces, markers, rhs,
+                               cg, gradient, extrapolation (when timing on) */
+} hfg_stats_t;
+
+/* ---- library ---------------------------------------------------------- */
+HFG_API int hfg_init(int device);
+HFG_API const char* hfg_last_error(void);
+HFG_API const char* hfg_version(void);
+HFG_API void hfg_default_options(hfg_options_t* o);
+
+/* ---- CGridFluidSolver mirror ----------------------------------------- */
+/* CGridFluidSolver(dt, res, origin, spacing)  GridFluidSolver.cpp:32-41,161-196 */
+HFG_API int hfg_solver_create(float dt, const int res[3], const float origin[3], const float spacing[3],
+                              hfg_solver_t* out);
+HFG_API int hfg_solver_destroy(hfg_solver_t s);
+/* addSolidBoundary / generateSolidSDFFromCLDGrid(.., vel)  GridFluidSolver.cpp:203-206,557-562 */
+HFG_API int hfg_solver_add_solid_boundary(hfg_solver_t s, const float* sdf, const float vel[3]);
+/* addExternalForce  GridFluidSolver.cpp:198-201 */
+HFG_API int hfg_solver_add_external_force(hfg_solver_t s, const float force[3]);
+/* setVelocityField / setFluidDomainField / setColorField  GridFluidSolver.cpp:208-229 */
+HFG_API int hfg_solver_set_velocity_field(hfg_solver_t s, const float* x, const float* y, const float* z);
+HFG_API int hfg_solver_set_fluid_domain_field(hfg_solver_t s, const float* d);
+HFG_API int hfg_solver_set_color_field(hfg_solver_t s, const float* x, const float* y, const float* z);
+/* generateFluidDomainFromBBox  GridFluidSolver.cpp:551-555 */
+HFG_API int hfg_solver_generate_fluid_domain_from_bbox(hfg_solver_t s, const float mn[3], const float mx[3]);
+/* setAdvectionSolver (SemiLagrangian / PIC / FLIP / MixPICAndFLIP)  GridFluidSolver.cpp:90-158 */
+HFG_API int hfg_solver_set_advection(hfg_solver_t s, int kind, int accuracy, int transfer_alg, float cfl,
+                                     float mixing);
+/* CEulerParticles::generateParticlesInFluid with a seeded counter-based stream
+ * in place of rand()  EulerParticles.cpp:140-179 */
+HFG_API int hfg_solver_seed_particles(hfg_solver_t s, int per_cell, unsigned long long seed);
+/* CEulerParticles::setParticlesPos / setParticlesVel (host arrays of 3n)  EulerParticles.cpp:125-133 */
+HFG_API int hfg_solver_set_particles(hfg_solver_t s, const float* pos, const float* vel, long long n);
+HFG_API int hfg_solver_set_options(hfg_solver_t s, const hfg_options_t* o);
+HFG_API int hfg_solver_enable_timing(hfg_solver_t s, int on);
+/* update / updateWithoutPressure / solvePressure  GridFluidSolver.cpp:336-357 */
+HFG_API int hfg_solver_update(hfg_solver_t s);
+HFG_API int hfg_solver_update_steps(hfg_solver_t s, int steps);
+HFG_API int hfg_solver_update_without_pressure(hfg_solver_t s);
+HFG_API int hfg_solver_solve_pressure(hfg_solver_t s);
+/* getVelocityField (which=0) / getVelocityFieldBeforePressure (which=1)  GridFluidSolver.cpp:302-324 */
+HFG_API int hfg_solver_get_velocity_field(hfg_solver_t s, int which, float* x, float* y, float* z);
+HFG_API int hfg_solver_get_fluid_domain_field(hfg_solver_t s, float* d);
+HFG_API int hfg_solver_get_color_field(hfg_solver_t s, float* x, float* y, float* z);
+/* getPressureSolver()->getMarkers() / getConstVectorx()  PressureSolver.h:25-31 */
+HFG_API int hfg_solver_get_markers(hfg_solver_t s, uint8_t* markers);
+HFG_API int hfg_solver_get_pressure(hfg_solver_t s, float* p);
+/* getSolidSDFField (the total solid marker field)  GridFluidSolver.cpp:292-295 */
+HFG_API int hfg_solver_get_solid_sdf(hfg_solver_t s, float* sdf);
+HFG_API int hfg_solver_get_solid_vel_field(hfg_solver_t s, float* x, float* y, float* z);
+HFG_API long long hfg_solver_num_particles(hfg_solver_t s);
+HFG_API int hfg_solver_get_particles(hfg_solver_t s, float* pos, float* vel);
+HFG_API int hfg_solver_get_stats(hfg_solver_t s, hfg_stats_t* st);
+HFG_API int hfg_solver_get_grid(hfg_solver_t s, int res[3], float origin[3], float spacing[3]);
+/* The CUDA stream every kernel of this solver runs on (cudaStream_t). */
+HFG_API void* hfg_solver_stream(hfg_solver_t s);
+/* Launches of this library's kernels since creation (counted on the host). */
+HFG_API long long hfg_solver_launch_count(hfg_solver_t s);
+HFG_API int hfg_solver_synchronize(hfg_solver_t s);
+
+/* ---- operators (device pointers, asynchronous on `stream` unless noted) -- */
+/* buildFluidMarkersInvoker(solidSDF, particles)  EulerParticlesTool.cu:366-411 */
+HFG_API int hfg_op_markers_from_particles(const int res[3], const float origin[3], const float spacing[3],
+                                          const float* solid_sdf, const float* pos, long long n, uint8_t* markers,
+                                          void* stream);
+/* statisticalFluidDensity counts  EulerParticlesTool.cu:27-46,413-441 */
+HFG_API int hfg_op_bin_counts(const int res[3], const float origin[3], const float spacing[3], const float* pos,
+                              long long n, unsigned int* counts, void* stream);
+/* buildFluidMarkersInvoker(solidSDF, fluidSDF)  EulerSolverTool.cu:629-648 */
+HFG_API int hfg_op_markers_from_sdf(const int res[3], const float* solid_sdf, const float* fluid_sdf,
+                                    uint8_t* markers, void* stream);
+/* buildPressureFdmMatrixAInvoker  EulerSolverTool.cu:650-664 ([diag,+x,+y,+z] per cell) */
+HFG_API int hfg_op_build_matrix_a(const int res[3], const float spacing[3], float dt, const uint8_t* markers,
+                                  float* A, void* stream);
+/* fdmMatrixVectorMulInvoker  EulerSolverTool.cu:706-720 */
+HFG_API int hfg_op_apply_a(const int res[3], const float spacing[3], float dt, const uint8_t* markers,
+                           const float* x, float* y, void* stream);
+/* divergence + buildPressureVectorbInvoker  PressureSolver.cpp:223-227 */
+HFG_API int hfg_op_build_rhs(const int res[3], const float spacing[3], const float* vx, const float* vy,
+                             const float* vz, const float* svx, const float* svy, const float* svz,
+                             const uint8_t* markers, float* b, void* stream);
+/* the projection of CPressureSolver::solvePressure after the markers
+ * (PressureSolver.cpp:210-233): RHS, CG, pressure gradient in place on v.
+ * Blocks until the solve finishes; stats (3 doubles: iterations, ||r||, ||b||) optional. */
+HFG_API int hfg_op_project(const int res[3], const float spacing[3], float dt, const uint8_t* markers, float* vx,
+                           float* vy, float* vz, const float* svx, const float* svy, const float* svz, int precond,
+                           int tol_mode, double tol, long long max_iter, float* p, double* stats, void* stream);
+/* extrapolatingDataInvoker on a face-centred field  EulerSolverTool.cu:904-969 (blocks) */
+HFG_API int hfg_op_extrapolate_fc(const int res[3], float* vx, float* vy, float* vz, int layers, void* stream);
+/* extrapolatingDataInvoker on one cell-centred scalar field  EulerSolverTool.cu:812-842 (blocks) */
+HFG_API int hfg_op_extrapolate_cc(const int res[3], float* f, int layers, void* stream);
+/* sampleFaceCenteredVectorFieldInvoker at n points (trilinear)  FieldMathTool.cu:894-1002 */
+HFG_API int hfg_op_sample_fc(const int res[3], const float origin[3], const float spacing[3], const float* vx,
+                             const float* vy, const float* vz, const float* pos, long long n, float* out,
+                             void* stream);
+/* sampleCellCenteredScalarFieldInvoker at n points (trilinear)  FieldMathTool.cu:526-573 */
+HFG_API int hfg_op_sample_cc(const int res[3], const float origin[3], const float spacing[3], const float* f,
+                             const float* pos, long long n, float* out, void* stream);
+/* tranferFCVField2ParticlesInvoker  EulerParticlesTool.cu:805-868 */
+HFG_API int hfg_op_g2p_fc(const int res[3], const float origin[3], const float spacing[3], const float* vx,
+                          const float* vy, const float* vz, const float* pos, long long n, int alg, float* out,
+                          void* stream);
+/* tranferCCSField2ParticlesInvoker  EulerParticlesTool.cu:713-741 */
+HFG_API int hfg_op_g2p_cc(const int res[3], const float origin[3], const float spacing[3], const float* f,
+                          const float* pos, long long n, int alg, float* out, void* stream);
+/* tranferParticles2FCVFieldInvoker (normalised)  EulerParticlesTool.cu:601-711; weights optional */
+HFG_API int hfg_op_p2g_fc(const int res[3], const float origin[3], const float spacing[3], const float* pos,
+                          const float* vel, long long n, int alg, float* vx, float* vy, float* vz, float* wx,
+                          float* wy, float* wz, void* stream);
+/* tranferParticles2CCSFieldInvoker  EulerParticlesTool.cu:443-496 */
+HFG_API int hfg_op_p2g_cc(const int res[3], const float origin[3], const float spacing[3], const float* pos,
+                          const float* val, long long n, int alg, int normalize, float* f, float* w, void* stream);
+/* CEulerParticles::advectParticlesInVelField  EulerParticles.cpp:231-325 (blocks; returns substeps) */
+HFG_API int hfg_op_advect_particles(const int res[3], const float origin[3], const float spacing[3],
+                                    const float* vx, const float* vy, const float* vz, float* pos, long long n,
+                                    float dt, float cfl, int accuracy, int clamp_mode, int* substeps, void* stream);
+/* CSemiLagrangian::advect (face-centred)  SemiLagrangian.cpp:169-186 */
+HFG_API int hfg_op_sl_advect_fc(const int res[3], const float origin[3], const float spacing[3], const float* ix,
+                                const float* iy, const float* iz, const float* vx, const float* vy, const float* vz,
+                                float dt, int accuracy, float* ox, float* oy, float* oz, void* stream);
+/* CSemiLagrangian::advect (cell-centred scalar)  SemiLagrangian.cpp:135-150 */
+HFG_API int hfg_op_sl_advect_cc(const int res[3], const float origin[3], const float spacing[3], const float* in,
+                                const float* vx, const float* vy, const float* vz, float dt, int accuracy, float* out,
+                                void* stream);
+/* generateFluidDomainFromBBoxInvoker  EulerSolverTool.cu:989-1013 */
+HFG_API int hfg_op_fluid_domain_from_bbox(const int res[3], const float origin[3], const float spacing[3],
+                                          const float mn[3], const float mx[3], float* out, void* stream);
+/* particle seeding (see hfg_solver_seed_particles); pos may be NULL to count only (blocks) */
+HFG_API int hfg_op_seed_particles(const int res[3], const float origin[3], const float spacing[3],
+                                  const float* fluid_sdf, const float* solid_sdf, int per_cell,
+                                  unsigned long long seed, float* pos, long long capacity, long long* count,
+                                  void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HFGRID_H */

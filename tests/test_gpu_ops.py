@@ -1,0 +1,282 @@
+"""Parity of each CUDA stage of the grid step against the CPU oracle.
+
+Every test drives libhfgrid.so through its C ABI (hfg_op_*) on seeded inputs
+and compares with the oracle restatement of the same reference stage.
+Integer and index work (markers, bin counts, layers, seeding) must be
+bit-exact; floating-point results are held to the tolerances written in each
+test (FP32 kernels vs the FP32 operation-by-operation oracle, or vs FP64).
+"""
+import numpy as np
+import pytest
+import torch
+
+import hfgrid
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+RES = (13, 11, 9)           # ragged on purpose
+ORIGIN = (0.25, -0.5, 1.0)
+SPACING = (0.1, 0.12, 0.09)
+
+
+def dev(a, dtype=None):
+    t = torch.from_numpy(np.ascontiguousarray(a))
+    if dtype is not None:
+        t = t.to(dtype)
+    return t.cuda()
+
+
+def host(t):
+    torch.cuda.synchronize()
+    return t.cpu().numpy()
+
+
+def face_arrays(res, rng, scale=1.0):
+    return [(rng.standard_normal(s) * scale).astype(np.float32) for s in oracle.face_shapes(res)]
+
+
+def random_particles(rng, n, res=RES, origin=ORIGIN, spacing=SPACING, margin=0.5):
+    lo = np.array(origin) - margin * np.array(spacing)
+    hi = np.array(origin) + (np.array(res) + margin) * np.array(spacing)
+    return (lo + rng.random((n, 3)) * (hi - lo)).astype(np.float32)
+
+
+def rel_err(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+
+
+def test_markers_and_bins_bit_exact(cuda):
+    rng = np.random.default_rng(1)
+    solid = rng.standard_normal(RES[::-1]).astype(np.float32)
+    pos = random_particles(rng, 5000)
+    # particles exactly on cell faces and outside the grid exercise truncation/clamping
+    pos[:50, 0] = (ORIGIN[0] + SPACING[0] * rng.integers(-2, RES[0] + 2, 50)).astype(np.float32)
+    mk_ref, cnt_ref = oracle.markers_from_particles(RES, ORIGIN, SPACING, solid, pos)
+    mk = torch.empty(RES[::-1], dtype=torch.uint8, device=cuda)
+    cnt = torch.empty(RES[::-1], dtype=torch.int32, device=cuda)
+    hfgrid.op_markers_from_particles(RES, ORIGIN, SPACING, dev(solid), dev(pos), mk)
+    hfgrid.op_bin_counts(RES, ORIGIN, SPACING, dev(pos), cnt)
+    assert np.array_equal(host(mk), mk_ref)
+    assert np.array_equal(host(cnt).astype(np.uint32), cnt_ref)
+    # empty particle set: solid cells only
+    hfgrid.op_markers_from_particles(RES, ORIGIN, SPACING, dev(solid), dev(pos[:0]), mk)
+    assert np.array_equal(host(mk), np.where(solid < 0, 2, 0).astype(np.uint8))
+
+
+def test_markers_from_sdf(cuda):
+    rng = np.random.default_rng(2)
+    solid = rng.standard_normal(RES[::-1]).astype(np.float32)
+    fluid = rng.standard_normal(RES[::-1]).astype(np.float32)
+    mk = torch.empty(RES[::-1], dtype=torch.uint8, device=cuda)
+    hfgrid.op_markers_from_sdf(RES, dev(solid), dev(fluid), mk)
+    assert np.array_equal(host(mk), oracle.markers_from_sdf(RES, solid, fluid))
+
+
+def random_markers(rng, res=RES, p=(0.3, 0.5, 0.2)):
+    return rng.choice(np.array([0, 1, 2], np.uint8), size=res[::-1], p=p)
+
+
+def test_matrix_a_exact(cuda):
+    rng = np.random.default_rng(3)
+    mk = random_markers(rng)
+    A = torch.empty(4 * np.prod(RES), dtype=torch.float32, device=cuda)
+    hfgrid.op_build_matrix_a(RES, SPACING, 0.05, dev(mk), A)
+    assert np.array_equal(host(A), oracle.build_matrix_a(RES, SPACING, 0.05, mk))
+
+
+def test_apply_a(cuda):
+    rng = np.random.default_rng(4)
+    mk = random_markers(rng)
+    x = rng.standard_normal(RES[::-1]).astype(np.float32)
+    y = torch.empty(RES[::-1], dtype=torch.float32, device=cuda)
+    hfgrid.op_apply_a(RES, SPACING, 0.05, dev(mk), dev(x), y)
+    ref = oracle.apply_a(RES, SPACING, 0.05, mk, x)
+    # products in FP32, sum in FP64 on both sides: identical up to the last bit
+    np.testing.assert_allclose(host(y), ref, rtol=1e-6, atol=1e-6 * np.abs(ref).max())
+
+
+def test_rhs(cuda):
+    rng = np.random.default_rng(5)
+    mk = random_markers(rng)
+    v = face_arrays(RES, rng)
+    sv = face_arrays(RES, rng, 0.3)
+    b = torch.empty(RES[::-1], dtype=torch.float32, device=cuda)
+    hfgrid.op_build_rhs(RES, SPACING, [dev(a) for a in v], [dev(a) for a in sv], dev(mk), b)
+    ref = oracle.build_rhs(RES, SPACING, v, sv, mk)
+    np.testing.assert_allclose(host(b), ref, rtol=1e-5, atol=1e-5 * np.abs(ref).max())
+
+
+def blob_markers(res, rng):
+    """Fluid blob with solid walls and some air, like a dam break."""
+    nz, ny, nx = res[::-1]
+    mk = np.zeros((nz, ny, nx), np.uint8)
+    mk[:, : ny // 2 + 1, : nx // 2 + 2] = 1
+    mk[0, :, :] = mk[-1, :, :] = 2
+    mk[:, 0, :] = mk[:, -1, :] = 2
+    mk[:, :, 0] = mk[:, :, -1] = 2
+    mk[rng.random(mk.shape) < 0.03] = 2
+    return mk
+
+
+@pytest.mark.parametrize("precond,tol_mode,tol", [(0, 0, 1e-3), (1, 1, 1e-7)])
+def test_project(cuda, precond, tol_mode, tol):
+    rng = np.random.default_rng(6)
+    res = (20, 18, 16)
+    h = (1 / 20, 1 / 18, 1 / 16)
+    dt = 1 / 60
+    mk = blob_markers(res, rng)
+    v = face_arrays(res, rng, 0.5)
+    sv = face_arrays(res, rng, 0.1)
+    vd = [dev(a) for a in v]
+    p = torch.empty(res[::-1], dtype=torch.float32, device=cuda)
+    st = hfgrid.op_project(res, h, dt, dev(mk), vd, [dev(a) for a in sv], precond=precond, tol_mode=tol_mode,
+                           tol=tol, max_iter=-1, p_out=p)
+    v64, p64, st64 = oracle.project(res, h, dt, mk, v, sv, precond=precond, tol_mode=tol_mode, tol=1e-10 if
+                                    tol_mode == 1 else tol, max_iter=-1, dbl=1)
+    assert st["converged"]
+    # the CG stops on its own residual rule: pressure within 1e-4 relative of
+    # the FP64 solve, velocities (known faces) likewise
+    assert rel_err(host(p), p64) < 1e-4
+    for a in range(3):
+        g, r = host(vd[a]), v64[a]
+        known = r != np.finfo(np.float32).max
+        assert np.array_equal(g == np.finfo(np.float32).max, ~known)
+        assert rel_err(g[known], r[known]) < 1e-4
+
+
+def test_extrapolation_bit_exact(cuda):
+    rng = np.random.default_rng(7)
+    res = (17, 12, 10)
+    U = np.finfo(np.float32).max
+    v = face_arrays(res, rng)
+    for a in range(3):
+        unknown = rng.random(v[a].shape) < 0.9
+        unknown[..., :3] = True
+        v[a][unknown] = U
+    # one fully unknown component: nothing to extrapolate from
+    v[2][:] = U
+    ref = oracle.extrapolate_fc(res, v, 1000)
+    vd = [dev(a) for a in v]
+    hfgrid.op_extrapolate_fc(res, vd, 1000)
+    for a in range(3):
+        assert np.array_equal(host(vd[a]), ref[a])
+    # a depth cap: only the first few layers are filled
+    vd = [dev(a) for a in v]
+    hfgrid.op_extrapolate_fc(res, vd, 3)
+    ref3 = oracle.extrapolate_fc(res, v, 3)
+    for a in range(3):
+        assert np.array_equal(host(vd[a]), ref3[a])
+
+
+def test_extrapolation_cc_layers(cuda):
+    rng = np.random.default_rng(8)
+    res = (31, 7, 5)
+    U = np.finfo(np.float32).max
+    f = rng.standard_normal(res[::-1]).astype(np.float32)
+    f[rng.random(f.shape) < 0.97] = U
+    f.flat[0] = 1.0
+    ref = oracle.extrapolate(res, f, 1000)
+    fd = dev(f)
+    hfgrid.op_extrapolate_cc(res, fd, 1000)
+    assert np.array_equal(host(fd), ref)
+
+
+def test_sampling(cuda):
+    rng = np.random.default_rng(9)
+    v = face_arrays(RES, rng)
+    pos = random_particles(rng, 3000, margin=2.0)
+    out = torch.empty((3000, 3), dtype=torch.float32, device=cuda)
+    hfgrid.op_sample_fc(RES, ORIGIN, SPACING, [dev(a) for a in v], dev(pos), out)
+    ref = oracle.sample_fc(RES, ORIGIN, SPACING, v, pos)
+    np.testing.assert_allclose(host(out), ref, rtol=2e-5, atol=2e-5)
+    f = rng.standard_normal(RES[::-1]).astype(np.float32)
+    o1 = torch.empty(3000, dtype=torch.float32, device=cuda)
+    hfgrid.op_sample_cc(RES, ORIGIN, SPACING, dev(f), dev(pos), o1)
+    np.testing.assert_allclose(host(o1), oracle.sample_cc(RES, ORIGIN, SPACING, f, pos), rtol=2e-5, atol=2e-5)
+
+
+@pytest.mark.parametrize("alg", [hfgrid.LINEAR, hfgrid.QUADRATIC, hfgrid.CUBIC, hfgrid.G2PNEAREST])
+def test_g2p(cuda, alg):
+    rng = np.random.default_rng(10 + alg)
+    v = face_arrays(RES, rng)
+    pos = random_particles(rng, 2000)
+    out = torch.empty((2000, 3), dtype=torch.float32, device=cuda)
+    hfgrid.op_g2p_fc(RES, ORIGIN, SPACING, [dev(a) for a in v], dev(pos), alg, out)
+    np.testing.assert_allclose(host(out), oracle.g2p_fc(RES, ORIGIN, SPACING, v, pos, alg), rtol=1e-5, atol=1e-5)
+    f = rng.standard_normal(RES[::-1]).astype(np.float32)
+    o1 = torch.empty(2000, dtype=torch.float32, device=cuda)
+    hfgrid.op_g2p_cc(RES, ORIGIN, SPACING, dev(f), dev(pos), alg, o1)
+    np.testing.assert_allclose(host(o1), oracle.g2p_cc(RES, ORIGIN, SPACING, f, pos, alg), rtol=1e-5, atol=1e-5)
+
+
+@pytest.mark.parametrize("alg", [hfgrid.LINEAR, hfgrid.QUADRATIC, hfgrid.CUBIC, hfgrid.P2GSUM])
+def test_p2g(cuda, alg):
+    rng = np.random.default_rng(20 + alg)
+    pos = random_particles(rng, 4000)
+    vel = rng.standard_normal((4000, 3)).astype(np.float32)
+    outs = [torch.empty(s, dtype=torch.float32, device=cuda) for s in oracle.face_shapes(RES)]
+    ws = [torch.empty(s, dtype=torch.float32, device=cuda) for s in oracle.face_shapes(RES)]
+    hfgrid.op_p2g_fc(RES, ORIGIN, SPACING, dev(pos), dev(vel), alg, outs, ws)
+    ref, wref = oracle.p2g_fc(RES, ORIGIN, SPACING, pos, vel, alg, dbl=1)
+    for a in range(3):
+        # unordered FP32 atomics vs an ordered FP64 sum
+        np.testing.assert_allclose(host(outs[a]), ref[a], rtol=1e-4, atol=1e-4)
+        np.testing.assert_allclose(host(ws[a]), wref[a], rtol=1e-5, atol=1e-4)
+    val = rng.standard_normal(4000).astype(np.float32)
+    f = torch.empty(RES[::-1], dtype=torch.float32, device=cuda)
+    w = torch.empty(RES[::-1], dtype=torch.float32, device=cuda)
+    hfgrid.op_p2g_cc(RES, ORIGIN, SPACING, dev(pos), dev(val), alg, f, w)
+    fr, wr = oracle.p2g_cc(RES, ORIGIN, SPACING, pos, val, alg)
+    np.testing.assert_allclose(host(f), fr, rtol=1e-4, atol=1e-4)
+    np.testing.assert_allclose(host(w), wr, rtol=1e-4, atol=1e-4)
+
+
+@pytest.mark.parametrize("acc", [0, 1, 2])
+def test_advect_particles(cuda, acc):
+    rng = np.random.default_rng(30 + acc)
+    v = face_arrays(RES, rng, 0.3)
+    pos = random_particles(rng, 3000, margin=0.0)
+    pd = dev(pos)
+    n = hfgrid.op_advect_particles(RES, ORIGIN, SPACING, [dev(a) for a in v], pd, 0.05, 1.0, acc, 1)
+    ref, nref = oracle.advect_particles(RES, ORIGIN, SPACING, v, pos, 0.05, 1.0, acc, 1, dbl=1)
+    assert n == nref
+    np.testing.assert_allclose(host(pd), ref, rtol=1e-5, atol=2e-5)
+
+
+@pytest.mark.parametrize("acc", [0, 1, 2])
+def test_semi_lagrangian(cuda, acc):
+    rng = np.random.default_rng(40 + acc)
+    v = face_arrays(RES, rng, 0.2)
+    f = face_arrays(RES, rng)
+    out = [torch.empty(s, dtype=torch.float32, device=cuda) for s in oracle.face_shapes(RES)]
+    hfgrid.op_sl_advect_fc(RES, ORIGIN, SPACING, [dev(a) for a in f], [dev(a) for a in v], 0.05, acc, out)
+    ref = oracle.sl_advect_fc(RES, ORIGIN, SPACING, f, v, 0.05, acc, dbl=1)
+    for a in range(3):
+        np.testing.assert_allclose(host(out[a]), ref[a], rtol=1e-4, atol=1e-4)
+    c = rng.standard_normal(RES[::-1]).astype(np.float32)
+    o1 = torch.empty(RES[::-1], dtype=torch.float32, device=cuda)
+    hfgrid.op_sl_advect_cc(RES, ORIGIN, SPACING, dev(c), [dev(a) for a in v], 0.05, acc, o1)
+    np.testing.assert_allclose(host(o1), oracle.sl_advect_cc(RES, ORIGIN, SPACING, c, v, 0.05, acc), rtol=1e-4,
+                               atol=1e-4)
+
+
+def test_fluid_domain_and_seeding_bit_exact(cuda):
+    res = (24, 20, 16)
+    h = tuple(1.0 / r for r in res)
+    o = (0.0, 0.0, 0.0)
+    out = torch.empty(res[::-1], dtype=torch.float32, device=cuda)
+    hfgrid.op_fluid_domain_from_bbox(res, o, h, (0, 0, 0), (0.4, 0.6, 1.0), out)
+    ref = oracle.fluid_domain_from_bbox(res, o, h, (0, 0, 0), (0.4, 0.6, 1.0))
+    dom = host(out)
+    assert np.array_equal(dom, ref)
+    rng = np.random.default_rng(50)
+    solid = np.where(rng.random(res[::-1]) < 0.1, -1.0, 1.0).astype(np.float32)
+    n = hfgrid.op_seed_particles(res, o, h, out, dev(solid), 8, 1234)
+    pos = torch.empty((n, 3), dtype=torch.float32, device=cuda)
+    hfgrid.op_seed_particles(res, o, h, out, dev(solid), 8, 1234, pos, n)
+    pref = oracle.seed_particles(res, o, h, dom, solid, 8, 1234)
+    assert pref.shape[0] == n
+    assert np.array_equal(host(pos), pref)

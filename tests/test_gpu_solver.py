@@ -1,0 +1,162 @@
+"""Multi-step parity of the GPU grid solver (libhfgrid.so) with the oracle.
+
+Identical seeded inputs go to both: boundary SDFs, the bbox fluid domain and
+bit-identical seeded particles.  After a few full steps (boundaries ->
+advection -> forces -> markers -> CG -> gradient -> extrapolation) the GPU
+state must match the FP64 oracle within the tolerances below.  Particle
+positions carry the CFL-substepped RK3 of every step, so they are the most
+sensitive output.
+"""
+import numpy as np
+import pytest
+
+import hfgrid
+import oracle
+import scenes
+
+pytestmark = pytest.mark.gpu
+
+U = np.finfo(np.float32).max
+
+
+def rel_l2(a, b, mask=None):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    if mask is not None:
+        a, b = a[mask], b[mask]
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+
+
+def oracle_twin(scene, gpu, dbl, precond, tol_mode, tol, max_iter, kind=hfgrid.ADV_MIX_PIC_FLIP, scalars=True):
+    o = oracle.Solver(scene.dt, scene.res, scene.origin, scene.spacing, dbl=dbl)
+    for sdf, vel in scenes.boundaries(scene):
+        o.add_solid_boundary(sdf, vel)
+    mn, mx = scenes.fluid_bbox(scene)
+    o.set_fluid_domain_field(oracle.fluid_domain_from_bbox(scene.res, scene.origin, scene.spacing, mn, mx))
+    o.set_advection(kind, 2, 2, scene.cfl, scene.mixing, 1, int(scalars))
+    if kind != hfgrid.ADV_SEMI_LAGRANGIAN:
+        pos, vel = gpu.particles()
+        o.set_particles(pos, vel)
+    o.set_pcg(precond, tol_mode, tol, max_iter)
+    return o
+
+
+def small_scene(n=(20, 18, 16)):
+    sc = scenes.Scene(res=n, solids=[scenes.Solid("sphere", (0.55, 0.2, 0.5), (0.15, 0, 0))], seed=7)
+    return sc
+
+
+def test_seeding_matches_oracle(cuda):
+    sc = small_scene()
+    g = scenes.gpu_solver(sc)
+    pos, vel = g.particles()
+    dom = oracle.fluid_domain_from_bbox(sc.res, sc.origin, sc.spacing, *scenes.fluid_bbox(sc))
+    ref = oracle.seed_particles(sc.res, sc.origin, sc.spacing, dom, scenes.total_solid(sc), sc.per_cell, sc.seed)
+    assert np.array_equal(pos, ref)
+    assert not vel.any()
+
+
+@pytest.mark.parametrize("steps", [1, 4])
+def test_mix_pic_flip_steps(cuda, steps):
+    sc = small_scene()
+    g = scenes.gpu_solver(sc, precond=1, tol_mode=1, tol=1e-6, max_iter=400, advect_scalars=True)
+    o = oracle_twin(sc, g, 1, 1, 1, 1e-6, 400)
+    for _ in range(steps):
+        g.update()
+        o.update()
+    gs, os_ = g.stats(), o.stats()
+    assert gs["substeps"] == os_["substeps"]
+    gp, gv = g.particles()
+    op, ov = o.particles()
+    assert np.abs(gp - op).max() < 1e-4 * steps
+    assert rel_l2(gv, ov) < 1e-3
+    mk_g, mk_o = g.markers(), o.markers()
+    assert (mk_g != mk_o).mean() < 2e-3
+    vg, vo = g.velocity_field(), o.velocity_field()
+    for a in range(3):
+        known = (vg[a] != U) & (vo[a] != U)
+        assert np.array_equal(vg[a] == U, vo[a] == U) or steps > 1
+        assert rel_l2(vg[a], vo[a], known) < 2e-3
+    dg, do = g.fluid_domain_field(), o.fluid_domain_field()
+    assert rel_l2(dg, do) < 1e-3
+
+
+def test_reference_parity_mode_one_step(cuda):
+    """The reference's own pressure settings: identity preconditioner and the
+    sqrt(||r||) < 1e-3 rule, N-iteration cap (PressureSolver.cpp:150-151)."""
+    sc = small_scene((16, 16, 12))
+    g = scenes.gpu_solver(sc, precond=0, tol_mode=0, tol=1e-3, max_iter=-1, advect_scalars=True)
+    o = oracle_twin(sc, g, 1, 0, 0, 1e-3, -1)
+    g.update()
+    o.update()
+    assert np.array_equal(g.markers(), o.markers())
+    assert np.array_equal(g.solid_sdf(), o.solid_sdf())
+    vg, vo = g.velocity_field(), o.velocity_field()
+    for a in range(3):
+        assert np.array_equal(vg[a] == U, vo[a] == U)
+        known = vo[a] != U
+        assert rel_l2(vg[a], vo[a], known) < 1e-3
+    assert rel_l2(g.pressure(), o.pressure()) < 1e-3
+
+
+def test_semi_lagrangian_solver(cuda):
+    sc = small_scene((16, 14, 12))
+    g = scenes.gpu_solver(sc, precond=1, tol_mode=1, tol=1e-7, max_iter=500, advect_scalars=True,
+                          kind=hfgrid.ADV_SEMI_LAGRANGIAN)
+    o = oracle_twin(sc, g, 1, 1, 1, 1e-9, 2000, kind=hfgrid.ADV_SEMI_LAGRANGIAN)
+    for _ in range(3):
+        g.update()
+        o.update()
+    assert (g.markers() != o.markers()).mean() < 2e-3
+    vg, vo = g.velocity_field(), o.velocity_field()
+    for a in range(3):
+        known = (vg[a] != U) & (vo[a] != U)
+        assert rel_l2(vg[a], vo[a], known) < 1e-3
+
+
+def _integration_case(kind):
+    """IntegrationTest-GridFluidSolver.cpp:228-402 inputs: a 4^3 grid, unit
+    spacing, solid (-0.5) everywhere except listed cells (+0.5), fluid where
+    j - 2.5 < 0 except listed cells."""
+    res = (4, 4, 4)
+    fluid = np.zeros(res[::-1], np.float32)
+    for j in range(4):
+        fluid[:, j, :] = j - 2.5
+    solid = np.full(res[::-1], -0.5, np.float32)
+    if kind == 1:
+        open_cells = [21, 22, 25, 26, 29, 30, 37, 38, 41, 42, 45, 46]      # :251-262
+        dry = []
+    else:
+        open_cells = [17, 18, 21, 22, 25, 26, 29, 30, 33, 34, 37, 38, 41, 42, 45, 46]  # :341-356
+        dry = [17, 18, 33, 34]                                              # :337-340
+    solid.reshape(-1)[open_cells] = 0.5
+    fluid.reshape(-1)[dry] = 0.5
+    return res, solid, fluid
+
+
+def test_integration_rest(cuda):
+    """IntegrationTest-GridFluidSolver.cpp:228-311: a closed column of water
+    stays at rest (every face |u| < 1e-4 for 3 steps, dt = 1)."""
+    res, solid, fluid = _integration_case(1)
+    s = hfgrid.Solver(1.0, res)
+    s.set_fluid_domain_field(fluid)
+    s.add_solid_boundary(solid)
+    for _ in range(3):
+        s.update()
+        for comp in s.velocity_field():
+            assert np.abs(comp).max() < 1e-4
+
+
+def test_integration_free_fall(cuda):
+    """IntegrationTest-GridFluidSolver.cpp:313-402: water above an air gap
+    falls freely, u_y = -9.8 dt (k+1) on the listed faces for 10 steps."""
+    res, solid, fluid = _integration_case(2)
+    dt = 0.01
+    s = hfgrid.Solver(dt, res)
+    s.set_fluid_domain_field(fluid)
+    s.add_solid_boundary(solid)
+    for k in range(10):
+        s.update()
+        vy = s.velocity_field()[1].reshape(-1)
+        for f in (25, 26, 29, 30, 33, 34, 45, 46, 49, 50, 53, 54):
+            assert abs(vy[f] + 9.8 * dt * (k + 1)) < 1e-4
