@@ -1,0 +1,314 @@
+"""Benchmark: Mcell-steps/s of the full grid step on the 256^3 dam break.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--res 256]
+
+Workload (one step = one full CGridFluidSolver::update): the 256^3 dam break
+on the unit cube -- fluid in x < 0.4, y < 0.6, walls plus two static boxes of
+side 0.2 on the floor, 8 particles per fluid cell (seeded), PIC/FLIP mix with
+FLIP weight 0.95, CFL 1, linear transfers, RK3, gravity -9.8, dt = 1/60,
+Jacobi-preconditioned CG to a relative residual of 1e-6 with at most 200
+iterations, full velocity extrapolation.  The scene state (~3.5 GB) is far
+larger than the 126 MB L2, so no L2 flush is needed between steps.
+
+One process per GPU (torchrun for N > 1); every rank steps its own replica of
+the scene (weak scaling, no data-path collective); the time is the maximum
+over ranks of the CUDA-event time on each solver's stream.
+
+--impl reference times the reference path on the host CPU (the reference has
+no CPU implementation of the grid step, so its CPU restatement in oracle/ is
+timed, FP64 with all host threads) on a bounded sample: one step of the same
+dam-break layout at 128^3 per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "hybrid-fluid-simulation_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "Mcell-steps/s at 256^3 (dam break, plain FP32 path)"
+UNIT = "Mcell-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--res", type=int, default=256)
+    ap.add_argument("--precond", default="jacobi", choices=["jacobi", "identity", "mg"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-sample-res", type=int, default=128)
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        cmd = ["nvidia-smi", f"--id={self.index}",
+               "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+               "clocks_event_reasons.sw_power_cap",
+               "--format=csv,noheader,nounits", "-lms", "200"]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.rows.append(parts)
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args):
+    """CPU arm: the oracle's FP64 restatement of the same step, rank 0 only."""
+    world, rank, _ = dist_setup(args)
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle
+    import scenes
+
+    n = args.cpu_sample_res
+    threads = os.cpu_count() or 1
+    oracle.lib().orc_set_num_threads(threads)
+    sc = scenes.dam_break_256(n=n)
+    o = oracle.Solver(sc.dt, sc.res, sc.origin, sc.spacing, dbl=1)
+    for sdf, v in scenes.boundaries(sc):
+        o.add_solid_boundary(sdf, v)
+    dom = oracle.fluid_domain_from_bbox(sc.res, sc.origin, sc.spacing, *scenes.fluid_bbox(sc))
+    o.set_fluid_domain_field(dom)
+    o.set_advection(3, 2, 2, sc.cfl, sc.mixing, 1, 0)
+    o.set_particles(oracle.seed_particles(sc.res, sc.origin, sc.spacing, dom, scenes.total_solid(sc), sc.per_cell,
+                                          sc.seed))
+    o.set_pcg(1, 1, 1e-6, 200)
+    for _ in range(args.warmup):
+        o.update()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.update()
+    dt = time.perf_counter() - t0
+    value = sc.n_cells * args.steps / dt / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"dam break, bounded CPU sample at {n}^3 (one step per timed step)",
+                   "res": [n, n, n], "particles": o.num_particles, "pcg": "jacobi rel 1e-6 max 200"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} steps of the dam-break layout at {n}^3 (FP64 oracle)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_sample(n=64, steps=2):
+    """Oracle FP64 on the host cores, bounded sample (same layout at n^3)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    import scenes
+    threads = os.cpu_count() or 1
+    oracle.lib().orc_set_num_threads(threads)
+    sc = scenes.dam_break_256(n=n)
+    o = oracle.Solver(sc.dt, sc.res, sc.origin, sc.spacing, dbl=1)
+    for sdf, v in scenes.boundaries(sc):
+        o.add_solid_boundary(sdf, v)
+    dom = oracle.fluid_domain_from_bbox(sc.res, sc.origin, sc.spacing, *scenes.fluid_bbox(sc))
+    o.set_fluid_domain_field(dom)
+    o.set_advection(3, 2, 2, sc.cfl, sc.mixing, 1, 0)
+    o.set_particles(oracle.seed_particles(sc.res, sc.origin, sc.spacing, dom, scenes.total_solid(sc), sc.per_cell,
+                                          sc.seed))
+    o.set_pcg(1, 1, 1e-6, 200)
+    o.update()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.update()
+    dt = time.perf_counter() - t0
+    return {"value": sc.n_cells * steps / dt / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{steps} steps (after 1 warm-up) of the dam-break layout at {n}^3, FP64 oracle, {threads} threads"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import numpy as np
+    import torch
+    import hfgrid
+    import scenes
+
+    world, rank, local = dist_setup(args)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    hfgrid.init(local)
+    torch.cuda.set_device(local)
+    precond = {"jacobi": hfgrid.PRECOND_JACOBI, "identity": hfgrid.PRECOND_IDENTITY, "mg": hfgrid.PRECOND_MG}[args.precond]
+    sc = scenes.dam_break_256(seed=rank, n=args.res)
+    s = scenes.gpu_solver(sc, precond=precond, tol_mode=hfgrid.TOL_RELATIVE, tol=1e-6, max_iter=200,
+                          advect_scalars=False)
+    stream = torch.cuda.ExternalStream(s.stream)
+
+    for _ in range(args.warmup):
+        s.update()
+    s.synchronize()
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    barrier()
+    clocks.start()
+    launches0 = s.launch_count
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        s.update()
+    ev1.record(stream)
+    ev1.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    launches = s.launch_count - launches0
+    clk = clocks.stop()
+    st = s.stats()
+
+    # e2e: the viewer loop of the reference (Application/main.cpp:74-93): the
+    # frame's rigid-boundary motion in (3 floats per solid, from host values),
+    # update(dt), then copyEulerParticlesPos/VelToCPU into pinned host buffers.
+    e2e = None
+    if not args.no_e2e:
+        n = s.num_particles
+        hpos = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
+        hvel = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
+        pos_np, vel_np = hpos.numpy(), hvel.numpy()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        nb = 1 + len(sc.solids)
+        for _ in range(args.steps):
+            for i, sol in enumerate(sc.solids):
+                s.set_boundary_velocity(i + 1, sol.velocity)
+            s.update()
+            s.copy_particles_into(pos_np, vel_np)
+        e1.record(stream)
+        e1.synchronize()
+        barrier()
+        ems = e0.elapsed_time(e1)
+        e2e = {"ms": ems, "d2h": 24 * n, "h2d": 12 * (nb - 1)}
+
+    # dominant kernel: one CG iteration (direction + update kernels) timed
+    # back-to-back on the last system
+    cg_ms = s.time_cg(40)
+
+    def max_over_ranks(v):
+        if pg is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    ms = max_over_ranks(ms)
+    if e2e:
+        e2e["ms"] = max_over_ranks(e2e["ms"])
+    cg_ms = max_over_ranks(cg_ms)
+
+    if rank == 0:
+        import json as _json
+        peaks = {}
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+                peaks = _json.load(f)
+        except OSError:
+            pass
+        hbm = float(peaks.get("hbm_gbs", 6650.0))
+        N = sc.n_cells
+        value = N * args.steps * world / (ms / 1e3) / 1e6
+        algo_bytes = 25.0 * N  # compulsory bytes per CG iteration (d, x, r read + markers + x, r, d written)
+        achieved = algo_bytes / (cg_ms / 1e3) / 1e9
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded dam break)",
+            "config": {"workload": f"dam break {args.res}^3, walls + two static boxes, 8 ppc, PIC/FLIP 0.95, "
+                                   f"{args.precond}-PCG rel 1e-6 max 200", "res": [args.res] * 3,
+                       "cells": N, "particles": s.num_particles, "l2": "state > L2 (no flush needed)",
+                       "parallelism": f"replicas x{world}", "cg_iterations_last": st["cg_iterations"],
+                       "substeps_last": st["substeps"], "extrapolation_layers_last": st["extrapolation_layers"]},
+            "roofline": {"bound": "hbm", "kernel": "CG iteration (kCgDirection + kCgUpdate)",
+                         "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": None, "algorithmic_bytes_per_iter": algo_bytes, "ms_per_iter": cg_ms,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback"},
+            "clocks": clk,
+            "gpu_launches": launches,
+        }
+        if e2e:
+            line["e2e"] = {"value": N * args.steps * world / (e2e["ms"] / 1e3) / 1e6, "unit": UNIT,
+                           "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"],
+                           "what": "per step: solid velocities in, update(), particle pos+vel out to pinned host"}
+        if world == 1 and args.cpu_sample_res > 0:
+            try:
+                line["cpu_baseline"] = cpu_baseline_sample(args.cpu_sample_res)
+            except Exception as ex:  # the product number stands without it
+                line["cpu_baseline"] = {"value": None, "error": str(ex)}
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

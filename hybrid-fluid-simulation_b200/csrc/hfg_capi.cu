@@ -140,6 +140,14 @@ HFG_API int hfg_solver_add_solid_boundary(hfg_solver_t s, const float* sdf, cons
     return HFG_OK;
   });
 }
+HFG_API int hfg_solver_set_boundary_velocity(hfg_solver_t s, int index, const float vel[3]) {
+  return guarded([&]() -> int {
+    SOLVER(s);
+    NEED(vel, "null velocity");
+    S.setBoundaryVelocity(index, vel);
+    return HFG_OK;
+  });
+}
 HFG_API int hfg_solver_add_external_force(hfg_solver_t s, const float force[3]) {
   return guarded([&]() -> int {
     SOLVER(s);
@@ -332,6 +340,15 @@ HFG_API int hfg_solver_synchronize(hfg_solver_t s) {
   return guarded([&]() -> int {
     SOLVER(s);
     S.synchronize();
+    return HFG_OK;
+  });
+}
+
+HFG_API int hfg_solver_time_cg(hfg_solver_t s, int iters, float* ms) {
+  return guarded([&]() -> int {
+    SOLVER(s);
+    NEED(ms && iters > 0, "invalid arguments");
+    *ms = S.timeCg(iters);
     return HFG_OK;
   });
 }

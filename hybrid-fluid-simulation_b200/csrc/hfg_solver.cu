@@ -112,6 +112,11 @@ void GridSolver::addBoundary(const float* sdfHost, const float vel[3]) {
   check(cudaStreamSynchronize(stream_), "sync");
 }
 
+void GridSolver::setBoundaryVelocity(int index, const float vel[3]) {
+  if (index < 0 || index >= (int)bsdf_.size()) throw CudaError("boundary index out of range", HFG_ERR_INVALID);
+  for (int a = 0; a < 3; ++a) bvel_[3 * index + a] = vel[a];
+}
+
 void GridSolver::addExternalForce(const float f[3]) {
   for (int a = 0; a < 3; ++a) ext_[a] += f[a];  // ExternalForcesSolver.cpp:45-48
 }
@@ -469,6 +474,34 @@ void GridSolver::update() {
 }
 
 void GridSolver::synchronize() { check(cudaStreamSynchronize(stream_), "sync"); }
+
+float GridSolver::timeCg(int iters) {
+  if (iters <= 0) throw CudaError("iterations must be positive", HFG_ERR_INVALID);
+  const float sx = dt_ / (1.0f * g_.hx * g_.hx), sy = dt_ / (1.0f * g_.hy * g_.hy), sz = dt_ / (1.0f * g_.hz * g_.hz);
+  CgState st{};
+  st.maxIter = 0x7fffffff;
+  st.precond = opt_.precond == HFG_PRECOND_JACOBI ? 1 : 0;
+  st.tolMode = HFG_TOL_RELATIVE;
+  st.tol = 0.0;  // never converges: every launch does its work
+  st.rz = 1.0;
+  st.bb = 1.0;
+  *cgHost_ = st;
+  check(cudaMemcpyAsync(cgState_.p, cgHost_, sizeof(CgState), cudaMemcpyHostToDevice, stream_), "cg state");
+  check(cudaEventRecord(ev_[14], stream_), "event");
+  for (int it = 0; it < iters; ++it) {
+    launched(launchCgDirection(g_.r, sx, sy, sz, code_.p, cgr_.p, cgp_[it & 1].p, cgp_[(it + 1) & 1].p, partials_.p,
+                               cgState_.p, stream_),
+             "cg direction");
+    launched(launchCgUpdate(g_.r, sx, sy, sz, code_.p, cgp_[(it + 1) & 1].p, cgx_.p, cgr_.p, partials_.p,
+                            cgState_.p, stream_),
+             "cg update");
+  }
+  check(cudaEventRecord(ev_[15], stream_), "event");
+  check(cudaEventSynchronize(ev_[15]), "event sync");
+  float ms = 0.f;
+  check(cudaEventElapsedTime(&ms, ev_[14], ev_[15]), "elapsed");
+  return ms / iters;
+}
 
 void GridSolver::getVelocity(int which, float* x, float* y, float* z) {
   int b = which == 0 ? cur() : nxt();

@@ -62,6 +62,7 @@ class GridSolver {
   // ---- setters (GridFluidSolver.cpp:198-244) ----
   void addBoundary(const float* sdfHost, const float vel[3]);
   void addExternalForce(const float f[3]);
+  void setBoundaryVelocity(int index, const float vel[3]);
   void setVelocity(const float* x, const float* y, const float* z);
   void setFluidDomain(const float* d);
   void setColor(const float* x, const float* y, const float* z);
@@ -88,6 +89,7 @@ class GridSolver {
   void getParticles(float* pos, float* vel);
   void getStats(hfg_stats_t* st);
   void synchronize();
+  float timeCg(int iters);
 
   const Geom& geom() const { return g_; }
   cudaStream_t stream() const { return stream_; }

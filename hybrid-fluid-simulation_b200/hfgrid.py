@@ -77,6 +77,7 @@ def _signatures(lib):
         "hfg_solver_destroy": (C.c_int, [S]),
         "hfg_solver_add_solid_boundary": (C.c_int, [S, PF, F3]),
         "hfg_solver_add_external_force": (C.c_int, [S, F3]),
+        "hfg_solver_set_boundary_velocity": (C.c_int, [S, C.c_int, F3]),
         "hfg_solver_set_velocity_field": (C.c_int, [S, PF, PF, PF]),
         "hfg_solver_set_fluid_domain_field": (C.c_int, [S, PF]),
         "hfg_solver_set_color_field": (C.c_int, [S, PF, PF, PF]),
@@ -104,6 +105,7 @@ def _signatures(lib):
         "hfg_solver_stream": (C.c_void_p, [S]),
         "hfg_solver_launch_count": (C.c_longlong, [S]),
         "hfg_solver_synchronize": (C.c_int, [S]),
+        "hfg_solver_time_cg": (C.c_int, [S, C.c_int, C.POINTER(C.c_float)]),
         "hfg_op_markers_from_particles": (C.c_int, [I3, F3, F3, VP, VP, C.c_longlong, VP, VP]),
         "hfg_op_bin_counts": (C.c_int, [I3, F3, F3, VP, C.c_longlong, VP, VP]),
         "hfg_op_markers_from_sdf": (C.c_int, [I3, VP, VP, VP, VP]),
@@ -211,6 +213,9 @@ class Solver:
         assert a.size == self.n_cells
         _check(lib().hfg_solver_add_solid_boundary(self._h, _fptr(a), _f3(vel)))
 
+    def set_boundary_velocity(self, index: int, vel):
+        _check(lib().hfg_solver_set_boundary_velocity(self._h, index, _f3(vel)))
+
     def add_external_force(self, f):
         _check(lib().hfg_solver_add_external_force(self._h, _f3(f)))
 
@@ -264,6 +269,12 @@ class Solver:
 
     def synchronize(self):
         _check(lib().hfg_solver_synchronize(self._h))
+
+    def time_cg(self, iters: int = 50) -> float:
+        """Mean ms per CG iteration (both kernels) on the last system."""
+        ms = C.c_float(0)
+        _check(lib().hfg_solver_time_cg(self._h, iters, C.byref(ms)))
+        return ms.value
 
     # ---- getters ----
     def velocity_field(self, which: int = 0):

@@ -98,6 +98,10 @@ HFG_API int hfg_solver_create(float dt, const int res[3], const float origin[3],
 HFG_API int hfg_solver_destroy(hfg_solver_t s);
 /* addSolidBoundary / generateSolidSDFFromCLDGrid(.., vel)  GridFluidSolver.cpp:203-206,557-562 */
 HFG_API int hfg_solver_add_solid_boundary(hfg_solver_t s, const float* sdf, const float vel[3]);
+/* Velocity of boundary `index` from the next step on (translation += -dt*vel
+ * per step, Boundary.cpp:124-127); the per-frame rigid-boundary update of the
+ * reference viewer loop (MPhysics.cpp:52-65 transformRigidBoundary). */
+HFG_API int hfg_solver_set_boundary_velocity(hfg_solver_t s, int index, const float vel[3]);
 /* addExternalForce  GridFluidSolver.cpp:198-201 */
 HFG_API int hfg_solver_add_external_force(hfg_solver_t s, const float force[3]);
 /* setVelocityField / setFluidDomainField / setColorField  GridFluidSolver.cpp:208-229 */
@@ -140,6 +144,11 @@ HFG_API void* hfg_solver_stream(hfg_solver_t s);
 /* Launches of this library's kernels since creation (counted on the host). */
 HFG_API long long hfg_solver_launch_count(hfg_solver_t s);
 HFG_API int hfg_solver_synchronize(hfg_solver_t s);
+/* Times `iters` back-to-back CG iterations (both kernels, no host round trip)
+ * on the system of the last pressure solve with CUDA events on the solver's
+ * stream; writes the mean milliseconds per iteration.  Overwrites the pressure
+ * of the last step (the next update recomputes it). */
+HFG_API int hfg_solver_time_cg(hfg_solver_t s, int iters, float* ms_per_iter);
 
 /* ---- operators (device pointers, asynchronous on `stream` unless noted) -- */
 /* buildFluidMarkersInvoker(solidSDF, particles)  EulerParticlesTool.cu:366-411 */

@@ -19,6 +19,19 @@ pytestmark = pytest.mark.gpu
 U = np.finfo(np.float32).max
 
 
+def vel_rel_l2(vg, vo):
+    """Relative L2 error of the whole face velocity field over the faces both
+    sides know (a single component can be ~0 everywhere, e.g. u_z of a
+    z-symmetric scene, so the norm is taken over all three together)."""
+    num = den = 0.0
+    for a in range(3):
+        k = (vg[a] != U) & (vo[a] != U)
+        d = vg[a][k].astype(np.float64) - vo[a][k].astype(np.float64)
+        num += float(d @ d)
+        den += float(vo[a][k].astype(np.float64) @ vo[a][k].astype(np.float64))
+    return (num / max(den, 1e-300)) ** 0.5
+
+
 def rel_l2(a, b, mask=None):
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
@@ -74,9 +87,8 @@ def test_mix_pic_flip_steps(cuda, steps):
     assert (mk_g != mk_o).mean() < 2e-3
     vg, vo = g.velocity_field(), o.velocity_field()
     for a in range(3):
-        known = (vg[a] != U) & (vo[a] != U)
         assert np.array_equal(vg[a] == U, vo[a] == U) or steps > 1
-        assert rel_l2(vg[a], vo[a], known) < 2e-3
+    assert vel_rel_l2(vg, vo) < 2e-3
     dg, do = g.fluid_domain_field(), o.fluid_domain_field()
     assert rel_l2(dg, do) < 1e-3
 
@@ -94,9 +106,8 @@ def test_reference_parity_mode_one_step(cuda):
     vg, vo = g.velocity_field(), o.velocity_field()
     for a in range(3):
         assert np.array_equal(vg[a] == U, vo[a] == U)
-        known = vo[a] != U
-        assert rel_l2(vg[a], vo[a], known) < 1e-3
-    assert rel_l2(g.pressure(), o.pressure()) < 1e-3
+    assert vel_rel_l2(vg, vo) < 1e-4
+    assert rel_l2(g.pressure(), o.pressure()) < 1e-4
 
 
 def test_semi_lagrangian_solver(cuda):
@@ -108,10 +119,7 @@ def test_semi_lagrangian_solver(cuda):
         g.update()
         o.update()
     assert (g.markers() != o.markers()).mean() < 2e-3
-    vg, vo = g.velocity_field(), o.velocity_field()
-    for a in range(3):
-        known = (vg[a] != U) & (vo[a] != U)
-        assert rel_l2(vg[a], vo[a], known) < 1e-3
+    assert vel_rel_l2(g.velocity_field(), o.velocity_field()) < 1e-3
 
 
 def _integration_case(kind):
