@@ -401,7 +401,7 @@ HFG_API int hfg_op_build_matrix_a(const int res[3], const float spacing[3], floa
   return guarded([&]() -> int {
     NEED(validRes(res) && spacing && markers && A, "invalid arguments");
     Dim3i r = toRes(res);
-    Scratch<uint8_t> code(r.size(), st(stream));
+    Scratch<Code> code(r.size(), st(stream));
     float sx, sy, sz;
     scalesA(spacing, dt, sx, sy, sz);
     check(launchStencilCode(r, markers, code.p, st(stream)), "code");
@@ -414,7 +414,7 @@ HFG_API int hfg_op_apply_a(const int res[3], const float spacing[3], float dt, c
   return guarded([&]() -> int {
     NEED(validRes(res) && spacing && markers && x && y, "invalid arguments");
     Dim3i r = toRes(res);
-    Scratch<uint8_t> code(r.size(), st(stream));
+    Scratch<Code> code(r.size(), st(stream));
     float sx, sy, sz;
     scalesA(spacing, dt, sx, sy, sz);
     check(launchStencilCode(r, markers, code.p, st(stream)), "code");
@@ -429,9 +429,9 @@ HFG_API int hfg_op_build_rhs(const int res[3], const float spacing[3], const flo
     NEED(validRes(res) && spacing && vx && vy && vz && svx && svy && svz && markers && b, "invalid arguments");
     Geom g = toGeom(res, nullptr, spacing);
     long long N = g.r.size();
-    Scratch<uint8_t> code(N, st(stream));
+    Scratch<Code> code(N, st(stream));
     Scratch<float> r(N, st(stream)), x(N, st(stream)), p(N, st(stream));
-    Scratch<double> part(cgPartialsNeeded(), st(stream));
+    Scratch<double> part(cgPartialsNeeded(g.r), st(stream));
     Scratch<CgState> cs(1, st(stream));
     CgState init{};
     init.maxIter = 1;
@@ -440,7 +440,7 @@ HFG_API int hfg_op_build_rhs(const int res[3], const float spacing[3], const flo
     check(launchStencilCode(g.r, markers, code.p, st(stream)), "code");
     ConstFaceField v{{vx, vy, vz}}, sv{{svx, svy, svz}};
     SolidVelTable none{};
-    check(launchRhsInit(g, v, sv, none, markers, code.p, 1.f, 1.f, 1.f, b, r.p, x.p, p.p, part.p, cs.p, st(stream)),
+    check(launchRhsInit(g, v, sv, none, markers, code.p, 1.f, 1.f, 1.f, b, r.p, x.p, p.p, part.p, cs.p, 0, st(stream)),
           "rhs");
     check(cudaStreamSynchronize(st(stream)), "sync");
     return HFG_OK;
@@ -457,9 +457,9 @@ HFG_API int hfg_op_project(const int res[3], const float spacing[3], float dt, c
     Geom g = toGeom(res, nullptr, spacing);
     long long N = g.r.size();
     cudaStream_t s = st(stream);
-    Scratch<uint8_t> code(N, s);
+    Scratch<Code> code(N, s);
     Scratch<float> r(N, s), x(N, s), p0(N, s), p1(N, s);
-    Scratch<double> part(cgPartialsNeeded(), s);
+    Scratch<double> part(cgPartialsNeeded(g.r), s);
     Scratch<CgState> cs(1, s);
     CgState init{};
     init.maxIter = (int)std::min<long long>(max_iter < 0 ? N : max_iter, 0x7fffffff);
@@ -472,14 +472,19 @@ HFG_API int hfg_op_project(const int res[3], const float spacing[3], float dt, c
     check(launchStencilCode(g.r, markers, code.p, s), "code");
     ConstFaceField v{{vx, vy, vz}}, sv{{svx, svy, svz}};
     SolidVelTable none{};
-    check(launchRhsInit(g, v, sv, none, markers, code.p, sx, sy, sz, nullptr, r.p, x.p, p0.p, part.p, cs.p, s), "rhs");
+    check(launchRhsInit(g, v, sv, none, markers, code.p, sx, sy, sz, nullptr, r.p, x.p, p0.p, part.p, cs.p,
+                        init.precond, s),
+          "rhs");
     CgState host{};
     float* pb[2] = {p0.p, p1.p};
     int it = 0;
     for (;;) {
       for (int k = 0; k < 16; ++k, ++it) {
-        check(launchCgDirection(g.r, sx, sy, sz, code.p, r.p, pb[it & 1], pb[(it + 1) & 1], part.p, cs.p, s), "cg");
-        check(launchCgUpdate(g.r, sx, sy, sz, code.p, pb[(it + 1) & 1], x.p, r.p, part.p, cs.p, s), "cg");
+        check(launchCgDirection(g.r, sx, sy, sz, code.p, r.p, pb[it & 1], pb[(it + 1) & 1], part.p, cs.p,
+                                init.precond, s),
+              "cg");
+        check(launchCgUpdate(g.r, sx, sy, sz, code.p, pb[(it + 1) & 1], x.p, r.p, part.p, cs.p, init.precond, s),
+              "cg");
       }
       check(cudaMemcpyAsync(&host, cs.p, sizeof(host), cudaMemcpyDeviceToHost, s), "read state");
       check(cudaStreamSynchronize(s), "sync");

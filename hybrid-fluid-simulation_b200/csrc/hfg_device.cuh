@@ -108,6 +108,80 @@ __device__ inline void sampleFace(const ConstFaceField& v, const Geom& cc, float
   for (int a = 0; a < 3; ++a) out[a] = trilerp(v.c[a], faceGeom(cc, a), px, py, pz);
 }
 
+// Trilinear sampling of a face-centred field, restated for speed: the cell
+// coordinate u = (p - o) / h of each axis is formed once (with a reciprocal),
+// and the per-axis base index and weight serve all three components (the
+// component's own axis uses the face grid, shifted by h/2; the other two the
+// cell-centred one).  Mathematically the reference's trilinear formula
+// (FieldMathTool.cu:52-104) and its LINEAR transfer weights
+// (EulerParticlesTool.cu:113-115); rounding differs in the last bits.
+struct AxisW {
+  int i0, i1;
+  float w1;
+};
+
+__device__ __forceinline__ void axisWeights(float t, int n, AxisW& a) {
+  float f = floorf(t);
+  a.w1 = t - f;
+  int i = (int)f;
+  a.i0 = clampi(i, n);
+  a.i1 = clampi(i + 1, n);
+}
+
+struct FaceSampler {
+  AxisW cc[3], fc[3];
+  __device__ __forceinline__ FaceSampler(const Geom& g, float px, float py, float pz) {
+    float ux = (px - g.ox) * (1.0f / g.hx), uy = (py - g.oy) * (1.0f / g.hy), uz = (pz - g.oz) * (1.0f / g.hz);
+    axisWeights(ux - 0.5f, g.r.x, cc[0]);
+    axisWeights(uy - 0.5f, g.r.y, cc[1]);
+    axisWeights(uz - 0.5f, g.r.z, cc[2]);
+    axisWeights(ux, g.r.x + 1, fc[0]);
+    axisWeights(uy, g.r.y + 1, fc[1]);
+    axisWeights(uz, g.r.z + 1, fc[2]);
+  }
+  // weights and 8 linear indices of component `a` (corner order z, y, x)
+  __device__ __forceinline__ void corners(const Geom& g, int a, long long idx[8], float w[8]) const {
+    const AxisW& X = a == 0 ? fc[0] : cc[0];
+    const AxisW& Y = a == 1 ? fc[1] : cc[1];
+    const AxisW& Z = a == 2 ? fc[2] : cc[2];
+    long long nx = g.r.x + (a == 0), ny = g.r.y + (a == 1);
+    long long r0 = (long long)Z.i0 * ny, r1 = (long long)Z.i1 * ny;
+    long long b00 = (r0 + Y.i0) * nx, b01 = (r0 + Y.i1) * nx, b10 = (r1 + Y.i0) * nx, b11 = (r1 + Y.i1) * nx;
+    idx[0] = b00 + X.i0; idx[1] = b00 + X.i1; idx[2] = b01 + X.i0; idx[3] = b01 + X.i1;
+    idx[4] = b10 + X.i0; idx[5] = b10 + X.i1; idx[6] = b11 + X.i0; idx[7] = b11 + X.i1;
+    float x0 = 1.f - X.w1, x1 = X.w1, y0 = 1.f - Y.w1, y1 = Y.w1, z0 = 1.f - Z.w1, z1 = Z.w1;
+    w[0] = x0 * y0 * z0; w[1] = x1 * y0 * z0; w[2] = x0 * y1 * z0; w[3] = x1 * y1 * z0;
+    w[4] = x0 * y0 * z1; w[5] = x1 * y0 * z1; w[6] = x0 * y1 * z1; w[7] = x1 * y1 * z1;
+  }
+  __device__ __forceinline__ float sample(const Geom& g, int a, const float* __restrict__ f) const {
+    long long idx[8];
+    float w[8];
+    corners(g, a, idx, w);
+    float v = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v = fmaf(w[k], __ldg(f + idx[k]), v);
+    return v;
+  }
+  // sample of the difference field f - h at the same point
+  __device__ __forceinline__ float sampleDiff(const Geom& g, int a, const float* __restrict__ f,
+                                              const float* __restrict__ h) const {
+    long long idx[8];
+    float w[8];
+    corners(g, a, idx, w);
+    float v = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v = fmaf(w[k], __fsub_rn(__ldg(f + idx[k]), __ldg(h + idx[k])), v);
+    return v;
+  }
+};
+
+__device__ __forceinline__ void sampleFaceFast(const ConstFaceField& v, const Geom& g, float px, float py, float pz,
+                                               float out[3]) {
+  FaceSampler s(g, px, py, pz);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) out[a] = s.sample(g, a, v.c[a]);
+}
+
 // Transfer-kernel weights (MPhysics/EulerMathTool.cu:268-294).
 __device__ inline float kLinear(float o) {
   float a = fabsf(o);
@@ -187,6 +261,59 @@ __device__ inline float warpMaxF(float v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
   return v;
+}
+
+__device__ inline unsigned int flatTid() { return threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z); }
+__device__ inline unsigned int flatBlock() { return blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z); }
+__device__ inline unsigned int numBlocks() { return gridDim.x * gridDim.y * gridDim.z; }
+__device__ inline unsigned int blockThreads() { return blockDim.x * blockDim.y * blockDim.z; }
+
+// Sum two doubles over the block (fixed tree => deterministic).  Result valid
+// in thread 0.  Works for 1-D, 2-D and 3-D blocks of a multiple of 32 threads.
+__device__ inline void blockSum2(double& a, double& b) {
+  __shared__ double sa[32], sb[32];
+  unsigned int t = flatTid();
+  a = warpSumD(a);
+  b = warpSumD(b);
+  unsigned int lane = t & 31, w = t >> 5;
+  if (lane == 0) { sa[w] = a; sb[w] = b; }
+  __syncthreads();
+  unsigned int nw = blockThreads() >> 5;
+  if (w == 0) {
+    a = lane < nw ? sa[lane] : 0.0;
+    b = lane < nw ? sb[lane] : 0.0;
+    a = warpSumD(a);
+    b = warpSumD(b);
+  }
+  __syncthreads();
+}
+
+// Publish this block's two partial sums; returns true in the one block that
+// finishes last, after which `a`, `b` (thread 0) hold the grid totals summed
+// in a fixed order (independent of block scheduling).
+__device__ inline bool gridSum2(double& a, double& b, double* partials, unsigned int* ticket) {
+  __shared__ bool isLast;
+  blockSum2(a, b);
+  unsigned int t = flatTid(), blk = flatBlock(), nb = numBlocks();
+  if (t == 0) {
+    partials[2 * blk] = a;
+    partials[2 * blk + 1] = b;
+    __threadfence();
+    unsigned int k = atomicAdd(ticket, 1u);
+    isLast = (k == nb - 1);
+  }
+  __syncthreads();
+  if (!isLast) return false;
+  __threadfence();
+  double sa = 0.0, sb = 0.0;
+  for (unsigned int i = t; i < nb; i += blockThreads()) {
+    sa += __ldcg(partials + 2 * i);
+    sb += __ldcg(partials + 2 * i + 1);
+  }
+  blockSum2(sa, sb);
+  a = sa;
+  b = sb;
+  return true;
 }
 
 }  // namespace hfg

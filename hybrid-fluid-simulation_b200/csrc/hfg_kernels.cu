@@ -14,7 +14,6 @@ namespace hfg {
 namespace {
 int g_numSMs = 0;
 constexpr int kThreads = 256;
-constexpr int kCgBlocksPerSM = 4;
 
 inline int gridFor(long long n, int threads = kThreads, int perSM = 16) {
   long long b = (n + threads - 1) / threads;
@@ -35,51 +34,6 @@ __device__ inline void cellCoord(long long c, const Dim3i& r, int& x, int& y, in
   z = (int)(t / r.y);
 }
 
-// Sum two doubles over the block (fixed tree => deterministic).  Result valid
-// in thread 0.
-__device__ inline void blockSum2(double& a, double& b) {
-  __shared__ double sa[32], sb[32];
-  a = warpSumD(a);
-  b = warpSumD(b);
-  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  if (lane == 0) { sa[w] = a; sb[w] = b; }
-  __syncthreads();
-  int nw = blockDim.x >> 5;
-  if (w == 0) {
-    a = lane < nw ? sa[lane] : 0.0;
-    b = lane < nw ? sb[lane] : 0.0;
-    a = warpSumD(a);
-    b = warpSumD(b);
-  }
-  __syncthreads();
-}
-
-// Publish this block's two partial sums; returns true in the one block that
-// finishes last, after which `a`, `b` (thread 0) hold the grid totals summed
-// in a fixed order.
-__device__ inline bool gridSum2(double& a, double& b, double* partials, unsigned int* ticket) {
-  __shared__ bool isLast;
-  blockSum2(a, b);
-  if (threadIdx.x == 0) {
-    partials[2 * blockIdx.x] = a;
-    partials[2 * blockIdx.x + 1] = b;
-    __threadfence();
-    unsigned int t = atomicAdd(ticket, 1u);
-    isLast = (t == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (!isLast) return false;
-  __threadfence();
-  double sa = 0.0, sb = 0.0;
-  for (unsigned int i = threadIdx.x; i < gridDim.x; i += blockDim.x) {
-    sa += __ldcg(partials + 2 * i);
-    sb += __ldcg(partials + 2 * i + 1);
-  }
-  blockSum2(sa, sb);
-  a = sa;
-  b = sb;
-  return true;
-}
 }  // namespace
 
 int numSMs() {
@@ -92,7 +46,6 @@ int numSMs() {
   return g_numSMs;
 }
 
-int cgPartialsNeeded() { return 2 * numSMs() * kCgBlocksPerSM; }
 
 // ===========================================================================
 // Boundaries and classification
@@ -144,16 +97,6 @@ __global__ void kTotalSolidSDF(long long n, int nb, const uint8_t* __restrict__ 
 cudaError_t launchTotalSolidSDF(long long n, int nb, const uint8_t* solidIdx, float* out, cudaStream_t s) {
   kTotalSolidSDF<<<gridFor(n), kThreads, 0, s>>>(n, nb, solidIdx, out);
   return cudaGetLastError();
-}
-
-// Solid face velocity of a face between cells lo (index i-1) and hi (index i)
-// on `axis`: the six faces of a solid cell carry its solid's velocity
-// (BoundaryTool.cu:28-83).  Where two different solids meet the reference
-// races; the higher cell wins here.
-__device__ inline float solidFaceVel(const SolidVelTable& t, uint8_t lo, uint8_t hi, int axis) {
-  uint8_t s = hi ? hi : lo;
-  if (!s) return 0.f;
-  return axis == 0 ? t.vx[s - 1] : (axis == 1 ? t.vy[s - 1] : t.vz[s - 1]);
 }
 
 __global__ void kSolidVelField(Geom g, SolidVelTable t, FaceField out) {
@@ -253,282 +196,6 @@ __global__ void kFluidDomainFromBBox(Geom g, float mnx, float mny, float mnz, fl
 }
 cudaError_t launchFluidDomainFromBBox(const Geom& g, const float mn[3], const float mx[3], float* out, cudaStream_t s) {
   kFluidDomainFromBBox<<<gridFor(g.r.size()), kThreads, 0, s>>>(g, mn[0], mn[1], mn[2], mx[0], mx[1], mx[2], out);
-  return cudaGetLastError();
-}
-
-// ===========================================================================
-// Pressure projection: matrix-free 7-point Poisson from a one-byte stencil code
-// ===========================================================================
-//
-// code bit 0: the cell is fluid; bits 1..6: the left, right, down, up, back,
-// front neighbour lies inside the grid and is not solid.  This is everything
-// buildPressureMatrixA (EulerSolverTool.cu:58-126) derives from the markers,
-// so A is never stored (the reference keeps 4 floats per cell).
-
-__global__ void kStencilCode(Dim3i r, const uint8_t* __restrict__ mk, uint8_t* __restrict__ code) {
-  HFG_FOR(c, r.size()) {
-    int x, y, z;
-    cellCoord(c, r, x, y, z);
-    uint8_t m = mk[c];
-    uint8_t k = 0;
-    if (m == kFluid) {
-      k = 1;
-      long long sy = r.x, sz = (long long)r.x * r.y;
-      if (x > 0 && mk[c - 1] != kSolid) k |= 2;
-      if (x + 1 < r.x && mk[c + 1] != kSolid) k |= 4;
-      if (y > 0 && mk[c - sy] != kSolid) k |= 8;
-      if (y + 1 < r.y && mk[c + sy] != kSolid) k |= 16;
-      if (z > 0 && mk[c - sz] != kSolid) k |= 32;
-      if (z + 1 < r.z && mk[c + sz] != kSolid) k |= 64;
-    }
-    code[c] = k;
-  }
-}
-cudaError_t launchStencilCode(const Dim3i& r, const uint8_t* markers, uint8_t* code, cudaStream_t s) {
-  kStencilCode<<<gridFor(r.size()), kThreads, 0, s>>>(r, markers, code);
-  return cudaGetLastError();
-}
-
-// Diagonal in the reference's accumulation order (EulerSolverTool.cu:85-120).
-__device__ inline float diagOf(uint8_t k, float sx, float sy, float sz) {
-  if (!(k & 1)) return 1.f;
-  float d = 0.f;
-  if (k & 2) d += sx;
-  if (k & 4) d += sx;
-  if (k & 8) d += sy;
-  if (k & 16) d += sy;
-  if (k & 32) d += sz;
-  if (k & 64) d += sz;
-  return d;
-}
-
-__global__ void kMatrixA(Dim3i r, float sx, float sy, float sz, const uint8_t* __restrict__ code, float* __restrict__ A) {
-  HFG_FOR(c, r.size()) {
-    int x, y, z;
-    cellCoord(c, r, x, y, z);
-    uint8_t k = code[c];
-    float a0 = diagOf(k, sx, sy, sz), a1 = 0.f, a2 = 0.f, a3 = 0.f;
-    if (k & 1) {
-      long long sy_ = r.x, sz_ = (long long)r.x * r.y;
-      if ((k & 4) && (code[c + 1] & 1)) a1 = -sx;
-      if ((k & 16) && (code[c + sy_] & 1)) a2 = -sy;
-      if ((k & 64) && (code[c + sz_] & 1)) a3 = -sz;
-    }
-    A[4 * c] = a0; A[4 * c + 1] = a1; A[4 * c + 2] = a2; A[4 * c + 3] = a3;
-  }
-}
-cudaError_t launchMatrixA(const Dim3i& r, float sx, float sy, float sz, const uint8_t* code, float* A, cudaStream_t s) {
-  kMatrixA<<<gridFor(r.size()), kThreads, 0, s>>>(r, sx, sy, sz, code, A);
-  return cudaGetLastError();
-}
-
-// Neighbour offsets of one cell; a neighbour counts when it is inside the grid
-// and fluid (off-diagonal -s of fdmMatrixVectorMul, EulerSolverTool.cu:219-226;
-// products in float, sum in double as the reference's ternaries do).
-struct Nbr {
-  long long o[6];
-  bool in[6];
-};
-__device__ inline void neighbours(long long c, int x, int y, int z, const Dim3i& r, Nbr& n) {
-  long long sy = r.x, sz = (long long)r.x * r.y;
-  n.in[0] = x > 0; n.o[0] = c - 1;
-  n.in[1] = x + 1 < r.x; n.o[1] = c + 1;
-  n.in[2] = y > 0; n.o[2] = c - sy;
-  n.in[3] = y + 1 < r.y; n.o[3] = c + sy;
-  n.in[4] = z > 0; n.o[4] = c - sz;
-  n.in[5] = z + 1 < r.z; n.o[5] = c + sz;
-}
-
-template <class PF>
-__device__ inline float applyAAt(long long c, uint8_t k, const Nbr& n, const uint8_t* __restrict__ code, float sx,
-                                 float sy, float sz, PF pval) {
-  float pc = pval(c);
-  if (!(k & 1)) return pc;
-  double acc = (double)__fmul_rn(diagOf(k, sx, sy, sz), pc);
-  const float s[6] = {-sx, -sx, -sy, -sy, -sz, -sz};
-#pragma unroll
-  for (int d = 0; d < 6; ++d)
-    if (n.in[d] && (__ldg(code + n.o[d]) & 1)) acc += (double)__fmul_rn(s[d], pval(n.o[d]));
-  return (float)acc;
-}
-
-__global__ void kApplyA(Dim3i r, float sx, float sy, float sz, const uint8_t* __restrict__ code,
-                        const float* __restrict__ xin, float* __restrict__ y) {
-  HFG_FOR(c, r.size()) {
-    int x, yy, z;
-    cellCoord(c, r, x, yy, z);
-    Nbr n;
-    neighbours(c, x, yy, z, r, n);
-    y[c] = applyAAt(c, code[c], n, code, sx, sy, sz, [&](long long i) { return __ldg(xin + i); });
-  }
-}
-cudaError_t launchApplyA(const Dim3i& r, float sx, float sy, float sz, const uint8_t* code, const float* x, float* y,
-                         cudaStream_t s) {
-  kApplyA<<<gridFor(r.size()), kThreads, 0, s>>>(r, sx, sy, sz, code, x, y);
-  return cudaGetLastError();
-}
-
-__device__ inline bool cgStop(const CgState* st, double rr) {
-  double rn = sqrt(rr);
-  if (st->tolMode == 0) return sqrt(rn) < st->tol;  // CuMatrixFreePCG.cpp:28,51
-  double bn = sqrt(st->bb);
-  return bn == 0.0 || rn / bn < st->tol;
-}
-
-__device__ inline float precondZ(int precond, uint8_t k, float rv, float sx, float sy, float sz) {
-  if (precond == 1) return __fdiv_rn(rv, diagOf(k, sx, sy, sz));
-  return rv;
-}
-
-// Divergence + solid terms (FieldMathTool.cu:370-395, EulerSolverTool.cu:128-197)
-// fused with the CG set-up of CuMatrixFreePCG.cpp:22-37 (x0 = 0 so r = b).
-__global__ void kRhsInit(Geom g, ConstFaceField v, ConstFaceField svArr, SolidVelTable svTab,
-                         const uint8_t* __restrict__ mk, const uint8_t* __restrict__ code, float sAx, float sAy,
-                         float sAz, float* __restrict__ bOut, float* __restrict__ r, float* __restrict__ x,
-                         float* __restrict__ p, double* partials, CgState* st) {
-  const Dim3i R = g.r;
-  const Dim3i rx{R.x + 1, R.y, R.z}, ry{R.x, R.y + 1, R.z}, rz{R.x, R.y, R.z + 1};
-  const float ix = 1.0f / g.hx, iy = 1.0f / g.hy, iz = 1.0f / g.hz;
-  const int pcd = st->precond;
-  double bb = 0.0, rzs = 0.0;
-  HFG_FOR(c, R.size()) {
-    int x0, y0, z0;
-    cellCoord(c, R, x0, y0, z0);
-    float b = 0.f;
-    if (mk[c] == kFluid) {
-      long long uL = ((long long)z0 * rx.y + y0) * rx.x + x0, uR = uL + 1;
-      long long vD = ((long long)z0 * ry.y + y0) * ry.x + x0, vU = vD + ry.x;
-      long long wB = ((long long)z0 * rz.y + y0) * rz.x + x0, wF = wB + (long long)rz.x * rz.y;
-      float L = v.c[0][uL], Rr = v.c[0][uR], D = v.c[1][vD], U = v.c[1][vU], B = v.c[2][wB], F = v.c[2][wF];
-      float div = __fadd_rn(__fadd_rn(__fdiv_rn(__fsub_rn(Rr, L), g.hx), __fdiv_rn(__fsub_rn(U, D), g.hy)),
-                            __fdiv_rn(__fsub_rn(F, B), g.hz));
-      b = -div;
-      long long sy = R.x, sz = (long long)R.x * R.y;
-      uint8_t me = svTab.solidIdx ? svTab.solidIdx[c] : 0;
-      auto sv = [&](int axis, long long f, long long nb, bool nbIsHi) -> float {
-        if (svArr.c[0]) return svArr.c[axis][f];
-        uint8_t o = svTab.solidIdx[nb];
-        return nbIsHi ? solidFaceVel(svTab, me, o, axis) : solidFaceVel(svTab, o, me, axis);
-      };
-      long long cl = x0 > 0 ? c - 1 : c, cr = x0 + 1 < R.x ? c + 1 : c;
-      long long cd = y0 > 0 ? c - sy : c, cu = y0 + 1 < R.y ? c + sy : c;
-      long long cb = z0 > 0 ? c - sz : c, cf = z0 + 1 < R.z ? c + sz : c;
-      if (mk[cl] == kSolid) b = __fsub_rn(b, __fmul_rn(ix, __fsub_rn(L, sv(0, uL, cl, false))));
-      if (mk[cr] == kSolid) b = __fadd_rn(b, __fmul_rn(ix, __fsub_rn(Rr, sv(0, uR, cr, true))));
-      if (mk[cd] == kSolid) b = __fsub_rn(b, __fmul_rn(iy, __fsub_rn(D, sv(1, vD, cd, false))));
-      if (mk[cu] == kSolid) b = __fadd_rn(b, __fmul_rn(iy, __fsub_rn(U, sv(1, vU, cu, true))));
-      if (mk[cb] == kSolid) b = __fsub_rn(b, __fmul_rn(iz, __fsub_rn(B, sv(2, wB, cb, false))));
-      if (mk[cf] == kSolid) b = __fadd_rn(b, __fmul_rn(iz, __fsub_rn(F, sv(2, wF, cf, true))));
-    }
-    if (bOut) bOut[c] = b;
-    r[c] = b;
-    x[c] = 0.f;
-    p[c] = 0.f;
-    float zz = precondZ(pcd, code[c], b, sAx, sAy, sAz);
-    bb += (double)b * (double)b;
-    rzs += (double)b * (double)zz;
-  }
-  if (gridSum2(bb, rzs, partials, &st->ticket) && threadIdx.x == 0) {
-    st->bb = bb;
-    st->rr = bb;
-    st->rz = rzs;
-    st->iter = 0;
-    st->beta = 0.f;
-    st->alpha = 0.f;
-    st->done = cgStop(st, bb) || st->maxIter <= 0;  // CuMatrixFreePCG.cpp:28-32
-    st->ticket = 0;
-  }
-}
-cudaError_t launchRhsInit(const Geom& g, ConstFaceField v, ConstFaceField svArr, const SolidVelTable& svTab,
-                          const uint8_t* markers, const uint8_t* code, float ax, float ay, float az, float* b,
-                          float* r, float* x, float* p, double* partials, CgState* st, cudaStream_t s) {
-  kRhsInit<<<numSMs() * kCgBlocksPerSM, kThreads, 0, s>>>(g, v, svArr, svTab, markers, code, ax, ay, az, b, r, x, p,
-                                                          partials, st);
-  return cudaGetLastError();
-}
-
-// One CG direction update p = z + beta*p (scal, then axpy with 1) fused with
-// q = A p and the reduction p.q; the last block forms alpha = r.z / p.Ap
-// (CuMatrixFreePCG.cpp:40-47).  z and p at the six neighbours are recomputed
-// from r and the previous p, so q is never written to memory.
-__global__ void __launch_bounds__(kThreads) kCgDirection(Dim3i R, float sx, float sy, float sz,
-                                                         const uint8_t* __restrict__ code, const float* __restrict__ r,
-                                                         const float* __restrict__ pOld, float* __restrict__ pNew,
-                                                         double* partials, CgState* st) {
-  if (st->done) return;
-  const float beta = st->beta;
-  const int pcd = st->precond;
-  double pq = 0.0, dummy = 0.0;
-  auto pn = [&](long long i) -> float {
-    float z = precondZ(pcd, __ldg(code + i), __ldg(r + i), sx, sy, sz);
-    return __fadd_rn(__fmul_rn(beta, __ldg(pOld + i)), z);
-  };
-  HFG_FOR(c, R.size()) {
-    int x, y, z;
-    cellCoord(c, R, x, y, z);
-    Nbr n;
-    neighbours(c, x, y, z, R, n);
-    uint8_t k = __ldg(code + c);
-    float pc = pn(c);
-    float q = applyAAt(c, k, n, code, sx, sy, sz, pn);
-    pNew[c] = pc;
-    pq += (double)pc * (double)q;
-  }
-  if (gridSum2(pq, dummy, partials, &st->ticket) && threadIdx.x == 0) {
-    st->pAp = pq;
-    st->alpha = (float)(st->rz / pq);
-    st->ticket = 0;
-  }
-}
-cudaError_t launchCgDirection(const Dim3i& r, float sx, float sy, float sz, const uint8_t* code, const float* rr,
-                              const float* pOld, float* pNew, double* partials, CgState* st, cudaStream_t s) {
-  kCgDirection<<<numSMs() * kCgBlocksPerSM, kThreads, 0, s>>>(r, sx, sy, sz, code, rr, pOld, pNew, partials, st);
-  return cudaGetLastError();
-}
-
-// x += alpha p, r -= alpha A p (A p recomputed), then z = M^-1 r and the
-// reductions r.r and r.z; the last block checks convergence and forms beta
-// (CuMatrixFreePCG.cpp:49-63).  The |alpha| < FLT_EPSILON skip of
-// CCuDenseVector::plusAlphaX (CuDenseVector.cpp:178) is kept.
-__global__ void __launch_bounds__(kThreads) kCgUpdate(Dim3i R, float sx, float sy, float sz,
-                                                      const uint8_t* __restrict__ code, const float* __restrict__ p,
-                                                      float* __restrict__ x, float* __restrict__ r, double* partials,
-                                                      CgState* st) {
-  if (st->done) return;
-  const float alpha = st->alpha;
-  const int pcd = st->precond;
-  const bool skip = fabsf(alpha) < FLT_EPSILON;
-  double rr = 0.0, rz = 0.0;
-  HFG_FOR(c, R.size()) {
-    int xx, y, z;
-    cellCoord(c, R, xx, y, z);
-    uint8_t k = __ldg(code + c);
-    float rv = r[c];
-    if (!skip) {
-      Nbr n;
-      neighbours(c, xx, y, z, R, n);
-      float q = applyAAt(c, k, n, code, sx, sy, sz, [&](long long i) { return __ldg(p + i); });
-      x[c] = fmaf(alpha, __ldg(p + c), x[c]);
-      rv = fmaf(-alpha, q, rv);
-      r[c] = rv;
-    }
-    float zz = precondZ(pcd, k, rv, sx, sy, sz);
-    rr += (double)rv * (double)rv;
-    rz += (double)rv * (double)zz;
-  }
-  if (gridSum2(rr, rz, partials, &st->ticket) && threadIdx.x == 0) {
-    st->rr = rr;
-    st->iter += 1;
-    bool stop = cgStop(st, rr);
-    st->beta = (float)(rz / st->rz);
-    st->rz = rz;
-    st->done = stop || st->iter >= st->maxIter;
-    st->ticket = 0;
-  }
-}
-cudaError_t launchCgUpdate(const Dim3i& r, float sx, float sy, float sz, const uint8_t* code, const float* p,
-                           float* x, float* rr, double* partials, CgState* st, cudaStream_t s) {
-  kCgUpdate<<<numSMs() * kCgBlocksPerSM, kThreads, 0, s>>>(r, sx, sy, sz, code, p, x, rr, partials, st);
   return cudaGetLastError();
 }
 
@@ -673,13 +340,24 @@ __global__ void kExclusiveScanSmall(const unsigned int* __restrict__ hist, unsig
   }
 }
 
+// Bucket the entries by layer.  Lanes of a warp that share a layer claim
+// their slots with one atomic (neighbouring entries mostly share a layer).
 __global__ void kDistScatter(long long n, long long base, const uint16_t* __restrict__ d, int nums,
                              unsigned int* __restrict__ cursor, unsigned int* __restrict__ list) {
-  HFG_FOR(i, n) {
-    uint16_t v = d[i];
-    if (v >= 1 && v < nums) {
-      unsigned int slot = atomicAdd(cursor + v, 1u);
-      list[slot] = (unsigned int)(base + i);
+  const unsigned int lane = threadIdx.x & 31;
+  for (long long b0 = (long long)blockIdx.x * blockDim.x; b0 < n; b0 += (long long)gridDim.x * blockDim.x) {
+    long long i = b0 + threadIdx.x;
+    unsigned int v = i < n ? d[i] : 0u;
+    bool want = i < n && v >= 1 && (int)v < nums;
+    unsigned int act = __ballot_sync(0xffffffffu, want);
+    if (want) {
+      unsigned int peers = __match_any_sync(act, v);
+      int leader = __ffs(peers) - 1;
+      unsigned int rank = __popc(peers & ((1u << lane) - 1u));
+      unsigned int slot = 0;
+      if ((int)lane == leader) slot = atomicAdd(cursor + v, (unsigned int)__popc(peers));
+      slot = __shfl_sync(peers, slot, leader);
+      list[slot + rank] = (unsigned int)(base + i);
     }
   }
 }
@@ -862,6 +540,34 @@ cudaError_t launchSeedWrite(const Geom& g, const float* fluidSDF, const uint8_t*
 //   FLIP (FluidImplicitParticle.cpp:107-119): v += G2P(vin - prev)
 //   MIX  (MixPICAndFLIP.cpp:112-129):        v = (1-m)(v + G2P(vin - prev)) + m G2P(vin)
 // with prev = the previous step's P2G output, or prev = 0 on the first FLIP step.
+// LINEAR transfers through the shared per-axis weights (the configuration of
+// every benchmark scene): one sampler per particle serves PIC, the FLIP
+// difference and all three components.
+__global__ void kParticleVelUpdateLinear(Geom g, int mode, ConstFaceField vin, ConstFaceField prev, int first,
+                                         float mixing, const float* __restrict__ pos, float* __restrict__ vel,
+                                         long long P) {
+  const float keep = (float)(1.0 - (double)mixing);
+  HFG_FOR(p, P) {
+    FaceSampler fs(g, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      float v = vel[3 * p + a];
+      if (mode == MODE_PIC) {
+        v = fs.sample(g, a, vin.c[a]);
+      } else {
+        float pic = (mode == MODE_MIX || first) ? fs.sample(g, a, vin.c[a]) : 0.f;
+        float dv = first ? pic : fs.sampleDiff(g, a, vin.c[a], prev.c[a]);
+        v = __fadd_rn(dv, v);
+        if (mode == MODE_MIX) {
+          v = __fmul_rn(v, keep);
+          v = fmaf(mixing, pic, v);
+        }
+      }
+      vel[3 * p + a] = v;
+    }
+  }
+}
+
 template <int ALG>
 __global__ void kParticleVelUpdate(Geom g, int mode, ConstFaceField vin, ConstFaceField prev, int first, float mixing,
                                    const float* __restrict__ pos, float* __restrict__ vel, long long P) {
@@ -918,7 +624,7 @@ cudaError_t launchParticleVelUpdate(const Geom& g, int mode, int alg, ConstFaceF
   if (P <= 0) return cudaSuccess;
   int gr = gridFor(P);
   switch (alg) {
-    case LINEAR: kParticleVelUpdate<LINEAR><<<gr, kThreads, 0, s>>>(g, mode, vin, prev, firstFlip, mixing, pos, vel, P); break;
+    case LINEAR: kParticleVelUpdateLinear<<<gr, kThreads, 0, s>>>(g, mode, vin, prev, firstFlip, mixing, pos, vel, P); break;
     case QUADRATIC: kParticleVelUpdate<QUADRATIC><<<gr, kThreads, 0, s>>>(g, mode, vin, prev, firstFlip, mixing, pos, vel, P); break;
     case CUBIC: kParticleVelUpdate<CUBIC><<<gr, kThreads, 0, s>>>(g, mode, vin, prev, firstFlip, mixing, pos, vel, P); break;
     case G2PNEAREST: kParticleVelUpdate<G2PNEAREST><<<gr, kThreads, 0, s>>>(g, mode, vin, prev, firstFlip, mixing, pos, vel, P); break;
@@ -947,7 +653,7 @@ __global__ void kSubstepBegin(Geom g, ConstFaceField vel, const float* __restric
   float m = 0.f;
   HFG_FOR(p, P) {
     float v[3];
-    sampleFace(vel, g, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2], v);
+    sampleFaceFast(vel, g, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2], v);
     v0[3 * p] = v[0]; v0[3 * p + 1] = v[1]; v0[3 * p + 2] = v[2];
     m = fmaxf(m, fmaxf(fabsf(v[0]), fmaxf(fabsf(v[1]), fabsf(v[2]))));
   }
@@ -1004,17 +710,17 @@ __global__ void kSubstep(Geom g, ConstFaceField vel, float* __restrict__ pos, fl
       float mid[3], w1[3];
 #pragma unroll
       for (int a = 0; a < 3; ++a) mid[a] = fmaf(half, w0[a], q[a]);
-      sampleFace(vel, g, mid[0], mid[1], mid[2], w1);
+      sampleFaceFast(vel, g, mid[0], mid[1], mid[2], w1);
 #pragma unroll
       for (int a = 0; a < 3; ++a) q[a] = fmaf(ds, w1[a], q[a]);
     } else {
       float mid[3], tf[3], w1[3], w2[3];
 #pragma unroll
       for (int a = 0; a < 3; ++a) mid[a] = fmaf(half, w0[a], q[a]);
-      sampleFace(vel, g, mid[0], mid[1], mid[2], w1);
+      sampleFaceFast(vel, g, mid[0], mid[1], mid[2], w1);
 #pragma unroll
       for (int a = 0; a < 3; ++a) tf[a] = fmaf(tq, w1[a], q[a]);
-      sampleFace(vel, g, tf[0], tf[1], tf[2], w2);
+      sampleFaceFast(vel, g, tf[0], tf[1], tf[2], w2);
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         q[a] = fmaf(a29, w0[a], q[a]);
@@ -1029,7 +735,7 @@ __global__ void kSubstep(Geom g, ConstFaceField vel, float* __restrict__ pos, fl
       }
     } else {
       float v[3];
-      sampleFace(vel, g, q[0], q[1], q[2], v);
+      sampleFaceFast(vel, g, q[0], q[1], q[2], v);
       v0[3 * p] = v[0]; v0[3 * p + 1] = v[1]; v0[3 * p + 2] = v[2];
       m = fmaxf(m, fmaxf(fabsf(v[0]), fmaxf(fabsf(v[1]), fabsf(v[2]))));
     }
@@ -1072,6 +778,23 @@ __device__ inline void p2gScatter(const Geom& fg, float px, float py, float pz, 
       }
 }
 
+__global__ void kP2GFaceLinear(Geom g, const float* __restrict__ pos, const float* __restrict__ vel, long long P,
+                               float2* a0, float2* a1, float2* a2) {
+  HFG_FOR(p, P) {
+    FaceSampler fs(g, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]);
+    float2* acc[3] = {a0, a1, a2};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      long long idx[8];
+      float w[8];
+      fs.corners(g, a, idx, w);
+      float val = vel[3 * p + a];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) atomicAdd(acc[a] + idx[k], make_float2(w[k] * val, w[k]));
+    }
+  }
+}
+
 template <int ALG>
 __global__ void kP2GFace(Geom g, const float* __restrict__ pos, const float* __restrict__ vel, long long P,
                          float2* a0, float2* a1, float2* a2) {
@@ -1087,7 +810,7 @@ cudaError_t launchP2GFace(const Geom& g, int alg, const float* pos, const float*
   if (P <= 0) return cudaSuccess;
   int gr = gridFor(P);
   switch (alg) {
-    case LINEAR: kP2GFace<LINEAR><<<gr, kThreads, 0, s>>>(g, pos, vel, P, acc[0], acc[1], acc[2]); break;
+    case LINEAR: kP2GFaceLinear<<<gr, kThreads, 0, s>>>(g, pos, vel, P, acc[0], acc[1], acc[2]); break;
     case QUADRATIC: kP2GFace<QUADRATIC><<<gr, kThreads, 0, s>>>(g, pos, vel, P, acc[0], acc[1], acc[2]); break;
     case CUBIC: kP2GFace<CUBIC><<<gr, kThreads, 0, s>>>(g, pos, vel, P, acc[0], acc[1], acc[2]); break;
     case P2GSUM: kP2GFace<P2GSUM><<<gr, kThreads, 0, s>>>(g, pos, vel, P, acc[0], acc[1], acc[2]); break;
@@ -1213,21 +936,21 @@ __device__ inline void axpyPt(float a, const float v[3], float p[3]) {
 __device__ inline void backTrace(ConstFaceField vel, const Geom& g, float dt, int acc, const float in[3], float out[3]) {
   float v0[3], v1[3], v2[3], mid[3], tf[3];
   out[0] = in[0]; out[1] = in[1]; out[2] = in[2];
-  sampleFace(vel, g, in[0], in[1], in[2], v0);
+  sampleFaceFast(vel, g, in[0], in[1], in[2], v0);
   if (acc == 0) {
     axpyPt(-dt, v0, out);
     return;
   }
   mid[0] = in[0]; mid[1] = in[1]; mid[2] = in[2];
   axpyPt(-0.5f * dt, v0, mid);
-  sampleFace(vel, g, mid[0], mid[1], mid[2], v1);
+  sampleFaceFast(vel, g, mid[0], mid[1], mid[2], v1);
   if (acc == 1) {
     axpyPt(-dt, v1, out);
     return;
   }
   tf[0] = in[0]; tf[1] = in[1]; tf[2] = in[2];
   axpyPt(-0.75f * dt, v1, tf);
-  sampleFace(vel, g, tf[0], tf[1], tf[2], v2);
+  sampleFaceFast(vel, g, tf[0], tf[1], tf[2], v2);
   axpyPt(-(float)(2.0 / 9.0) * dt, v0, out);
   axpyPt(-(float)(3.0 / 9.0) * dt, v1, out);
   axpyPt(-(float)(4.0 / 9.0) * dt, v2, out);

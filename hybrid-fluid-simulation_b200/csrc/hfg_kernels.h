@@ -54,6 +54,17 @@ struct SolidVelTable {
 
 int numSMs();
 
+// Solid face velocity of a face between cells lo (index i-1) and hi (index i)
+// on `axis`: the six faces of a solid cell carry its solid's velocity
+// (BoundaryTool.cu:28-83).  Where two different solids meet the reference
+// races; the higher cell wins here.
+__device__ inline float solidFaceVel(const SolidVelTable& t, uint8_t lo, uint8_t hi, int axis) {
+  uint8_t s = hi ? hi : lo;
+  if (!s) return 0.f;
+  return axis == 0 ? t.vx[s - 1] : (axis == 1 ? t.vy[s - 1] : t.vz[s - 1]);
+}
+
+
 // ---- boundaries / classification -------------------------------------------
 cudaError_t launchSolidClassify(const Geom& g, const BoundarySet& b, uint8_t* solidIdx, float* const* curSDF,
                                 cudaStream_t s);
@@ -68,23 +79,31 @@ cudaError_t launchMarkersFromSDF(long long n, const uint8_t* solidIdx, const flo
 cudaError_t launchFluidDomainFromBBox(const Geom& g, const float mn[3], const float mx[3], float* out, cudaStream_t s);
 
 // ---- pressure projection ---------------------------------------------------
-cudaError_t launchStencilCode(const Dim3i& r, const uint8_t* markers, uint8_t* code, cudaStream_t s);
-cudaError_t launchMatrixA(const Dim3i& r, float sx, float sy, float sz, const uint8_t* code, float* A, cudaStream_t s);
-cudaError_t launchApplyA(const Dim3i& r, float sx, float sy, float sz, const uint8_t* code, const float* x, float* y,
+// Per-cell stencil code: bit 0 the cell is fluid; bits 1..6 its left, right,
+// down, up, back, front neighbour is inside the grid and not solid (the
+// diagonal of buildPressureMatrixA, EulerSolverTool.cu:85-120); bits 7..12
+// that neighbour is inside the grid and fluid (the off-diagonals).
+typedef uint16_t Code;
+cudaError_t launchStencilCode(const Dim3i& r, const uint8_t* markers, Code* code, cudaStream_t s);
+cudaError_t launchMatrixA(const Dim3i& r, float sx, float sy, float sz, const Code* code, float* A, cudaStream_t s);
+cudaError_t launchApplyA(const Dim3i& r, float sx, float sy, float sz, const Code* code, const float* x, float* y,
                          cudaStream_t s);
 // RHS (divergence + solid terms) fused with CG set-up: r = b, x = 0, p = 0,
 // ||b||^2 and r.z into the state.  Solid face velocities come from `svArr`
 // when non-null, else from the per-solid table.
 cudaError_t launchRhsInit(const Geom& g, ConstFaceField v, ConstFaceField svArr, const SolidVelTable& svTab,
-                          const uint8_t* markers, const uint8_t* code, float ax, float ay, float az, float* b,
-                          float* r, float* x, float* p, double* partials, CgState* st, cudaStream_t s);
-cudaError_t launchCgDirection(const Dim3i& r, float sx, float sy, float sz, const uint8_t* code, const float* rr,
-                              const float* pOld, float* pNew, double* partials, CgState* st, cudaStream_t s);
-cudaError_t launchCgUpdate(const Dim3i& r, float sx, float sy, float sz, const uint8_t* code, const float* p,
-                           float* x, float* rr, double* partials, CgState* st, cudaStream_t s);
+                          const uint8_t* markers, const Code* code, float ax, float ay, float az, float* b,
+                          float* r, float* x, float* p, double* partials, CgState* st, int precond, cudaStream_t s);
+// precond: 0 identity, 1 Jacobi (must match CgState::precond)
+cudaError_t launchCgDirection(const Dim3i& r, float sx, float sy, float sz, const Code* code, const float* rr,
+                              const float* pOld, float* pNew, double* partials, CgState* st, int precond,
+                              cudaStream_t s);
+cudaError_t launchCgUpdate(const Dim3i& r, float sx, float sy, float sz, const Code* code, const float* p,
+                           float* x, float* rr, double* partials, CgState* st, int precond, cudaStream_t s);
 cudaError_t launchGradient(const Geom& g, float gx, float gy, float gz, const uint8_t* markers, const float* p,
                            FaceField v, ConstFaceField svArr, const SolidVelTable& svTab, cudaStream_t s);
-int cgPartialsNeeded();
+// doubles of reduction scratch the CG kernels need on grid `r`
+int cgPartialsNeeded(const Dim3i& r);
 
 // ---- extrapolation ---------------------------------------------------------
 struct ExtrapScratch {

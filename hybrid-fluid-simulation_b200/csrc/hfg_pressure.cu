@@ -1,0 +1,365 @@
+// hfg_pressure.cu -- the matrix-free pressure Poisson system and its CG on
+// sm_100a.
+//
+// The reference stores A as 4 floats per cell (buildPressureMatrixA,
+// EulerSolverTool.cu:58-126) and runs CG with cuBLAS calls and three blocking
+// host reads per iteration (CuMatrixFreePCG.cpp:22-65).  Here A is rebuilt in
+// registers from a 16-bit stencil code per cell, every CG iteration is two
+// kernels with FP64 block reductions finished by the last block (no host
+// round trip), and the stencil kernels are 2.5-D: a 32x8 thread tile marches
+// along z keeping the below / current / above planes in registers, so the z
+// neighbours cost no extra loads and no division is needed for indexing.
+#include <algorithm>
+
+#include "hfg_kernels.h"
+
+namespace hfg {
+
+namespace {
+constexpr int TX = 32, TY = 8;
+
+struct CgGrid {
+  dim3 grid, block;
+  int zPer;
+};
+
+// Enough blocks to fill every SM several times over, each marching >= 4 planes.
+CgGrid cgGrid(const Dim3i& r) {
+  CgGrid g;
+  g.block = dim3(TX, TY, 1);
+  int bx = (r.x + TX - 1) / TX, by = (r.y + TY - 1) / TY;
+  long long tiles = (long long)bx * by;
+  long long want = (long long)numSMs() * 8;
+  int zc = (int)std::max<long long>(1, (want + tiles - 1) / tiles);
+  zc = std::min(zc, std::max(1, r.z / 4));
+  g.zPer = (r.z + zc - 1) / zc;
+  zc = (r.z + g.zPer - 1) / g.zPer;
+  g.grid = dim3(bx, by, zc);
+  return g;
+}
+
+__device__ __forceinline__ bool nbFluid(Code k, int d) { return (k >> (7 + d)) & 1; }
+
+// Diagonal in the reference's accumulation order (EulerSolverTool.cu:85-120).
+__device__ __forceinline__ float diagOf(Code k, float sx, float sy, float sz) {
+  if (!(k & 1)) return 1.f;
+  float d = 0.f;
+  if (k & 2) d += sx;
+  if (k & 4) d += sx;
+  if (k & 8) d += sy;
+  if (k & 16) d += sy;
+  if (k & 32) d += sz;
+  if (k & 64) d += sz;
+  return d;
+}
+
+template <int PC>
+__device__ __forceinline__ float precondZ(Code k, float rv, float sx, float sy, float sz) {
+  return PC ? __fdiv_rn(rv, diagOf(k, sx, sy, sz)) : rv;
+}
+
+__device__ inline bool cgStop(const CgState* st, double rr) {
+  double rn = sqrt(rr);
+  if (st->tolMode == 0) return sqrt(rn) < st->tol;  // CuMatrixFreePCG.cpp:28,51
+  double bn = sqrt(st->bb);
+  return bn == 0.0 || rn / bn < st->tol;
+}
+
+// (A v)_c for a fluid cell given v at the centre and at its six neighbours
+// (fdmMatrixVectorMul, EulerSolverTool.cu:219-226: products in float, sum in
+// double as the reference's `: 0.0` ternaries make it).
+__device__ __forceinline__ float applyRow(Code k, float sx, float sy, float sz, float vc, float vl, float vr, float vd,
+                                          float vu, float vb, float vf) {
+  if (!(k & 1)) return vc;
+  double acc = (double)__fmul_rn(diagOf(k, sx, sy, sz), vc);
+  if (nbFluid(k, 0)) acc += (double)__fmul_rn(-sx, vl);
+  if (nbFluid(k, 1)) acc += (double)__fmul_rn(-sx, vr);
+  if (nbFluid(k, 2)) acc += (double)__fmul_rn(-sy, vd);
+  if (nbFluid(k, 3)) acc += (double)__fmul_rn(-sy, vu);
+  if (nbFluid(k, 4)) acc += (double)__fmul_rn(-sz, vb);
+  if (nbFluid(k, 5)) acc += (double)__fmul_rn(-sz, vf);
+  return (float)acc;
+}
+}  // namespace
+
+int cgPartialsNeeded(const Dim3i& r) {
+  CgGrid g = cgGrid(r);
+  return 2 * (int)(g.grid.x * g.grid.y * g.grid.z);
+}
+
+// ---------------------------------------------------------------------------
+__global__ void kStencilCode(Dim3i r, const uint8_t* __restrict__ mk, Code* __restrict__ code, int zPer) {
+  int x = blockIdx.x * TX + threadIdx.x, y = blockIdx.y * TY + threadIdx.y;
+  if (x >= r.x || y >= r.y) return;
+  int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, r.z);
+  long long plane = (long long)r.x * r.y;
+  for (int z = z0; z < z1; ++z) {
+    long long c = (long long)z * plane + (long long)y * r.x + x;
+    Code k = 0;
+    if (mk[c] == kFluid) {
+      k = 1;
+      const bool in[6] = {x > 0, x + 1 < r.x, y > 0, y + 1 < r.y, z > 0, z + 1 < r.z};
+      const long long o[6] = {-1, 1, -(long long)r.x, (long long)r.x, -plane, plane};
+#pragma unroll
+      for (int d = 0; d < 6; ++d) {
+        if (!in[d]) continue;
+        uint8_t m = mk[c + o[d]];
+        if (m != kSolid) k |= (Code)(1u << (1 + d));
+        if (m == kFluid) k |= (Code)(1u << (7 + d));
+      }
+    }
+    code[c] = k;
+  }
+}
+cudaError_t launchStencilCode(const Dim3i& r, const uint8_t* markers, Code* code, cudaStream_t s) {
+  CgGrid g = cgGrid(r);
+  kStencilCode<<<g.grid, g.block, 0, s>>>(r, markers, code, g.zPer);
+  return cudaGetLastError();
+}
+
+// The reference's stored matrix [diag, +x, +y, +z] (EulerSolverTool.cu:58-126),
+// bit-exact: used by the operator API and its tests only.
+__global__ void kMatrixA(Dim3i r, float sx, float sy, float sz, const Code* __restrict__ code, float* __restrict__ A) {
+  long long n = r.size();
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    Code k = code[c];
+    float a0 = diagOf(k, sx, sy, sz), a1 = 0.f, a2 = 0.f, a3 = 0.f;
+    if (k & 1) {
+      if (nbFluid(k, 1)) a1 = -sx;
+      if (nbFluid(k, 3)) a2 = -sy;
+      if (nbFluid(k, 5)) a3 = -sz;
+    }
+    A[4 * c] = a0; A[4 * c + 1] = a1; A[4 * c + 2] = a2; A[4 * c + 3] = a3;
+  }
+}
+cudaError_t launchMatrixA(const Dim3i& r, float sx, float sy, float sz, const Code* code, float* A, cudaStream_t s) {
+  int blocks = (int)std::min<long long>((r.size() + 255) / 256, (long long)numSMs() * 16);
+  kMatrixA<<<blocks, 256, 0, s>>>(r, sx, sy, sz, code, A);
+  return cudaGetLastError();
+}
+
+// y = A x (fdmMatrixVectorMulInvoker, EulerSolverTool.cu:706-720)
+__global__ void kApplyA(Dim3i r, float sx, float sy, float sz, const Code* __restrict__ code,
+                        const float* __restrict__ xin, float* __restrict__ y, int zPer) {
+  int x = blockIdx.x * TX + threadIdx.x, yy = blockIdx.y * TY + threadIdx.y;
+  if (x >= r.x || yy >= r.y) return;
+  int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, r.z);
+  long long plane = (long long)r.x * r.y;
+  long long c = (long long)z0 * plane + (long long)yy * r.x + x;
+  float below = z0 > 0 ? xin[c - plane] : 0.f, cur = xin[c];
+  for (int z = z0; z < z1; ++z, c += plane) {
+    float above = z + 1 < r.z ? xin[c + plane] : 0.f;
+    Code k = code[c];
+    float vl = x > 0 ? xin[c - 1] : 0.f, vr = x + 1 < r.x ? xin[c + 1] : 0.f;
+    float vd = yy > 0 ? xin[c - r.x] : 0.f, vu = yy + 1 < r.y ? xin[c + r.x] : 0.f;
+    y[c] = applyRow(k, sx, sy, sz, cur, vl, vr, vd, vu, below, above);
+    below = cur;
+    cur = above;
+  }
+}
+cudaError_t launchApplyA(const Dim3i& r, float sx, float sy, float sz, const Code* code, const float* x, float* y,
+                         cudaStream_t s) {
+  CgGrid g = cgGrid(r);
+  kApplyA<<<g.grid, g.block, 0, s>>>(r, sx, sy, sz, code, x, y, g.zPer);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// RHS: divergence (FieldMathTool.cu:370-395) + solid terms
+// (EulerSolverTool.cu:128-197), fused with the CG set-up of
+// CuMatrixFreePCG.cpp:22-37 (x0 = 0 so r = b).
+template <int PC>
+__global__ void __launch_bounds__(TX* TY) kRhsInit(Geom g, ConstFaceField v, ConstFaceField svArr, SolidVelTable svTab,
+                                                   const uint8_t* __restrict__ mk, const Code* __restrict__ code,
+                                                   float sAx, float sAy, float sAz, float* __restrict__ bOut,
+                                                   float* __restrict__ r, float* __restrict__ xv, float* __restrict__ p,
+                                                   double* partials, CgState* st, int zPer) {
+  const Dim3i R = g.r;
+  const float ix = 1.0f / g.hx, iy = 1.0f / g.hy, iz = 1.0f / g.hz;
+  int x = blockIdx.x * TX + threadIdx.x, y = blockIdx.y * TY + threadIdx.y;
+  double bb = 0.0, rzs = 0.0;
+  if (x < R.x && y < R.y) {
+    int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, R.z);
+    const long long plane = (long long)R.x * R.y;
+    const long long fxRow = R.x + 1, fxPlane = (long long)(R.x + 1) * R.y;
+    const long long fyPlane = (long long)R.x * (R.y + 1);
+    for (int z = z0; z < z1; ++z) {
+      long long c = (long long)z * plane + (long long)y * R.x + x;
+      float b = 0.f;
+      if (mk[c] == kFluid) {
+        long long uL = (long long)z * fxPlane + (long long)y * fxRow + x, uR = uL + 1;
+        long long vD = (long long)z * fyPlane + (long long)y * R.x + x, vU = vD + R.x;
+        long long wB = c, wF = c + plane;
+        float L = v.c[0][uL], Rr = v.c[0][uR], D = v.c[1][vD], U = v.c[1][vU], B = v.c[2][wB], F = v.c[2][wF];
+        float div = __fadd_rn(__fadd_rn(__fdiv_rn(__fsub_rn(Rr, L), g.hx), __fdiv_rn(__fsub_rn(U, D), g.hy)),
+                              __fdiv_rn(__fsub_rn(F, B), g.hz));
+        b = -div;
+        uint8_t me = svTab.solidIdx ? svTab.solidIdx[c] : 0;
+        auto sv = [&](int axis, long long f, long long nb, bool nbIsHi) -> float {
+          if (svArr.c[0]) return svArr.c[axis][f];
+          uint8_t o = svTab.solidIdx[nb];
+          return nbIsHi ? solidFaceVel(svTab, me, o, axis) : solidFaceVel(svTab, o, me, axis);
+        };
+        long long cl = x > 0 ? c - 1 : c, cr = x + 1 < R.x ? c + 1 : c;
+        long long cd = y > 0 ? c - R.x : c, cu = y + 1 < R.y ? c + R.x : c;
+        long long cb = z > 0 ? c - plane : c, cf = z + 1 < R.z ? c + plane : c;
+        if (mk[cl] == kSolid) b = __fsub_rn(b, __fmul_rn(ix, __fsub_rn(L, sv(0, uL, cl, false))));
+        if (mk[cr] == kSolid) b = __fadd_rn(b, __fmul_rn(ix, __fsub_rn(Rr, sv(0, uR, cr, true))));
+        if (mk[cd] == kSolid) b = __fsub_rn(b, __fmul_rn(iy, __fsub_rn(D, sv(1, vD, cd, false))));
+        if (mk[cu] == kSolid) b = __fadd_rn(b, __fmul_rn(iy, __fsub_rn(U, sv(1, vU, cu, true))));
+        if (mk[cb] == kSolid) b = __fsub_rn(b, __fmul_rn(iz, __fsub_rn(B, sv(2, wB, cb, false))));
+        if (mk[cf] == kSolid) b = __fadd_rn(b, __fmul_rn(iz, __fsub_rn(F, sv(2, wF, cf, true))));
+      }
+      if (bOut) bOut[c] = b;
+      r[c] = b;
+      xv[c] = 0.f;
+      p[c] = 0.f;
+      float zz = precondZ<PC>(code[c], b, sAx, sAy, sAz);
+      bb += (double)b * (double)b;
+      rzs += (double)b * (double)zz;
+    }
+  }
+  if (gridSum2(bb, rzs, partials, &st->ticket) && flatTid() == 0) {
+    st->bb = bb;
+    st->rr = bb;
+    st->rz = rzs;
+    st->iter = 0;
+    st->beta = 0.f;
+    st->alpha = 0.f;
+    st->done = cgStop(st, bb) || st->maxIter <= 0;  // CuMatrixFreePCG.cpp:28-32
+    st->ticket = 0;
+  }
+}
+cudaError_t launchRhsInit(const Geom& gm, ConstFaceField v, ConstFaceField svArr, const SolidVelTable& svTab,
+                          const uint8_t* markers, const Code* code, float ax, float ay, float az, float* b, float* r,
+                          float* x, float* p, double* partials, CgState* st, int precond, cudaStream_t s) {
+  CgGrid g = cgGrid(gm.r);
+  if (precond == 1)
+    kRhsInit<1><<<g.grid, g.block, 0, s>>>(gm, v, svArr, svTab, markers, code, ax, ay, az, b, r, x, p, partials, st,
+                                           g.zPer);
+  else
+    kRhsInit<0><<<g.grid, g.block, 0, s>>>(gm, v, svArr, svTab, markers, code, ax, ay, az, b, r, x, p, partials, st,
+                                           g.zPer);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// CG direction: p = z + beta p_old (scal then axpy with 1), q = A p and the
+// reduction p.q; the last block forms alpha = r.z / p.Ap
+// (CuMatrixFreePCG.cpp:40-47, :56-60).  p at the lateral neighbours is
+// recomputed from r and p_old (L1 hits), along z it is carried in registers.
+template <int PC>
+__global__ void __launch_bounds__(TX* TY) kCgDirection(Dim3i R, float sx, float sy, float sz,
+                                                       const Code* __restrict__ code, const float* __restrict__ r,
+                                                       const float* __restrict__ pOld, float* __restrict__ pNew,
+                                                       double* partials, CgState* st, int zPer) {
+  if (st->done) return;
+  const float beta = st->beta;
+  double pq = 0.0, dummy = 0.0;
+  int x = blockIdx.x * TX + threadIdx.x, y = blockIdx.y * TY + threadIdx.y;
+  if (x < R.x && y < R.y) {
+    int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, R.z);
+    const long long plane = (long long)R.x * R.y;
+    auto pn = [&](long long i) -> float {
+      float zz = precondZ<PC>(__ldg(code + i), __ldg(r + i), sx, sy, sz);
+      return __fadd_rn(__fmul_rn(beta, __ldg(pOld + i)), zz);
+    };
+    long long c = (long long)z0 * plane + (long long)y * R.x + x;
+    float below = z0 > 0 ? pn(c - plane) : 0.f;
+    float cur = pn(c);
+    for (int z = z0; z < z1; ++z, c += plane) {
+      float above = z + 1 < R.z ? pn(c + plane) : 0.f;
+      Code k = __ldg(code + c);
+      float q = cur;
+      if (k & 1) {
+        float vl = nbFluid(k, 0) ? pn(c - 1) : 0.f, vr = nbFluid(k, 1) ? pn(c + 1) : 0.f;
+        float vd = nbFluid(k, 2) ? pn(c - R.x) : 0.f, vu = nbFluid(k, 3) ? pn(c + R.x) : 0.f;
+        q = applyRow(k, sx, sy, sz, cur, vl, vr, vd, vu, below, above);
+      }
+      pNew[c] = cur;
+      pq += (double)cur * (double)q;
+      below = cur;
+      cur = above;
+    }
+  }
+  if (gridSum2(pq, dummy, partials, &st->ticket) && flatTid() == 0) {
+    st->pAp = pq;
+    st->alpha = (float)(st->rz / pq);
+    st->ticket = 0;
+  }
+}
+
+// CG update: x += alpha p, r -= alpha A p (A p recomputed), z = M^-1 r, the
+// reductions r.r and r.z; the last block checks convergence and forms beta
+// (CuMatrixFreePCG.cpp:49-63).  The |alpha| < FLT_EPSILON skip of
+// CCuDenseVector::plusAlphaX (CuDenseVector.cpp:178) is kept.
+template <int PC>
+__global__ void __launch_bounds__(TX* TY) kCgUpdate(Dim3i R, float sx, float sy, float sz,
+                                                    const Code* __restrict__ code, const float* __restrict__ p,
+                                                    float* __restrict__ xv, float* __restrict__ r, double* partials,
+                                                    CgState* st, int zPer) {
+  if (st->done) return;
+  const float alpha = st->alpha;
+  const bool skip = fabsf(alpha) < FLT_EPSILON;
+  double rr = 0.0, rz = 0.0;
+  int x = blockIdx.x * TX + threadIdx.x, y = blockIdx.y * TY + threadIdx.y;
+  if (x < R.x && y < R.y) {
+    int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, R.z);
+    const long long plane = (long long)R.x * R.y;
+    long long c = (long long)z0 * plane + (long long)y * R.x + x;
+    float below = z0 > 0 ? __ldg(p + c - plane) : 0.f;
+    float cur = __ldg(p + c);
+    for (int z = z0; z < z1; ++z, c += plane) {
+      float above = z + 1 < R.z ? __ldg(p + c + plane) : 0.f;
+      Code k = __ldg(code + c);
+      float rv = r[c];
+      if (!skip) {
+        float q = cur;
+        if (k & 1) {
+          float vl = nbFluid(k, 0) ? __ldg(p + c - 1) : 0.f, vr = nbFluid(k, 1) ? __ldg(p + c + 1) : 0.f;
+          float vd = nbFluid(k, 2) ? __ldg(p + c - R.x) : 0.f, vu = nbFluid(k, 3) ? __ldg(p + c + R.x) : 0.f;
+          q = applyRow(k, sx, sy, sz, cur, vl, vr, vd, vu, below, above);
+        }
+        xv[c] = fmaf(alpha, cur, xv[c]);
+        rv = fmaf(-alpha, q, rv);
+        r[c] = rv;
+      }
+      float zz = precondZ<PC>(k, rv, sx, sy, sz);
+      rr += (double)rv * (double)rv;
+      rz += (double)rv * (double)zz;
+      below = cur;
+      cur = above;
+    }
+  }
+  if (gridSum2(rr, rz, partials, &st->ticket) && flatTid() == 0) {
+    st->rr = rr;
+    st->iter += 1;
+    bool stop = cgStop(st, rr);
+    st->beta = (float)(rz / st->rz);
+    st->rz = rz;
+    st->done = stop || st->iter >= st->maxIter;
+    st->ticket = 0;
+  }
+}
+
+cudaError_t launchCgDirection(const Dim3i& r, float sx, float sy, float sz, const Code* code, const float* rr,
+                              const float* pOld, float* pNew, double* partials, CgState* st, int precond,
+                              cudaStream_t s) {
+  CgGrid g = cgGrid(r);
+  if (precond == 1)
+    kCgDirection<1><<<g.grid, g.block, 0, s>>>(r, sx, sy, sz, code, rr, pOld, pNew, partials, st, g.zPer);
+  else
+    kCgDirection<0><<<g.grid, g.block, 0, s>>>(r, sx, sy, sz, code, rr, pOld, pNew, partials, st, g.zPer);
+  return cudaGetLastError();
+}
+cudaError_t launchCgUpdate(const Dim3i& r, float sx, float sy, float sz, const Code* code, const float* p, float* x,
+                           float* rr, double* partials, CgState* st, int precond, cudaStream_t s) {
+  CgGrid g = cgGrid(r);
+  if (precond == 1)
+    kCgUpdate<1><<<g.grid, g.block, 0, s>>>(r, sx, sy, sz, code, p, x, rr, partials, st, g.zPer);
+  else
+    kCgUpdate<0><<<g.grid, g.block, 0, s>>>(r, sx, sy, sz, code, p, x, rr, partials, st, g.zPer);
+  return cudaGetLastError();
+}
+
+}  // namespace hfg

@@ -23,8 +23,8 @@ constexpr int kSubstepChunk = 4;   // CFL substeps launched between completion r
 // Multigrid preconditioner hooks (hfg_mg.cu).
 Multigrid* mgCreate(const Dim3i& r, int levels, int smooth, bool half);
 void mgDestroy(Multigrid* m);
-void mgSetup(Multigrid* m, const uint8_t* code, float sx, float sy, float sz, cudaStream_t s, long long& launches);
-void mgRunCg(Multigrid* m, const Dim3i& r, float sx, float sy, float sz, const uint8_t* code, float* x, float* rvec,
+void mgSetup(Multigrid* m, const Code* code, float sx, float sy, float sz, cudaStream_t s, long long& launches);
+void mgRunCg(Multigrid* m, const Dim3i& r, float sx, float sy, float sz, const Code* code, float* x, float* rvec,
              double* partials, CgState* st, CgState* stHost, cudaStream_t s, long long& launches);
 
 GridSolver::GridSolver(float dt, Dim3i res, const float origin[3], const float spacing[3]) {
@@ -51,7 +51,7 @@ GridSolver::GridSolver(float dt, Dim3i res, const float origin[3], const float s
   for (int a = 0; a < 3; ++a) prev_[a].alloc(F_[a]);
   solidIdx_.alloc(N_); markers_.alloc(N_); code_.alloc(N_);
   cgx_.alloc(N_); cgr_.alloc(N_); cgp_[0].alloc(N_); cgp_[1].alloc(N_);
-  partials_.alloc(cgPartialsNeeded());
+  partials_.alloc(cgPartialsNeeded(res));
   cgState_.alloc(1);
   subState_.alloc(subSlots_ + 1);
   dist_.alloc(Ftot_); list_.alloc(Ftot_);
@@ -363,13 +363,14 @@ void GridSolver::runCg() {
     return;
   }
   int it = 0;
+  const int pc = opt_.precond == HFG_PRECOND_JACOBI ? 1 : 0;
   for (;;) {
     for (int k = 0; k < kCgChunk; ++k, ++it) {
       float* pOld = cgp_[it & 1].p;
       float* pNew = cgp_[(it + 1) & 1].p;
-      launched(launchCgDirection(g_.r, sx, sy, sz, code_.p, cgr_.p, pOld, pNew, partials_.p, cgState_.p, stream_),
+      launched(launchCgDirection(g_.r, sx, sy, sz, code_.p, cgr_.p, pOld, pNew, partials_.p, cgState_.p, pc, stream_),
                "cg direction");
-      launched(launchCgUpdate(g_.r, sx, sy, sz, code_.p, pNew, cgx_.p, cgr_.p, partials_.p, cgState_.p, stream_),
+      launched(launchCgUpdate(g_.r, sx, sy, sz, code_.p, pNew, cgx_.p, cgr_.p, partials_.p, cgState_.p, pc, stream_),
                "cg update");
     }
     check(cudaMemcpyAsync(cgHost_, cgState_.p, sizeof(CgState), cudaMemcpyDeviceToHost, stream_), "read cg state");
@@ -401,7 +402,7 @@ void GridSolver::computePressure() {
   const float sx = dt_ / (1.0f * g_.hx * g_.hx), sy = dt_ / (1.0f * g_.hy * g_.hy), sz = dt_ / (1.0f * g_.hz * g_.hz);
   ConstFaceField none{{nullptr, nullptr, nullptr}};
   launched(launchRhsInit(g_, cvel(ni), none, solidTable(), markers_.p, code_.p, sx, sy, sz, nullptr, cgr_.p, cgx_.p,
-                         cgp_[0].p, partials_.p, cgState_.p, stream_),
+                         cgp_[0].p, partials_.p, cgState_.p, init.precond, stream_),
            "rhs");
   if (opt_.precond == HFG_PRECOND_MG) mgSetup(mg_, code_.p, sx, sy, sz, stream_, launches_);
   stageEnd(4);
@@ -490,10 +491,10 @@ float GridSolver::timeCg(int iters) {
   check(cudaEventRecord(ev_[14], stream_), "event");
   for (int it = 0; it < iters; ++it) {
     launched(launchCgDirection(g_.r, sx, sy, sz, code_.p, cgr_.p, cgp_[it & 1].p, cgp_[(it + 1) & 1].p, partials_.p,
-                               cgState_.p, stream_),
+                               cgState_.p, st.precond, stream_),
              "cg direction");
     launched(launchCgUpdate(g_.r, sx, sy, sz, code_.p, cgp_[(it + 1) & 1].p, cgx_.p, cgr_.p, partials_.p,
-                            cgState_.p, stream_),
+                            cgState_.p, st.precond, stream_),
              "cg update");
   }
   check(cudaEventRecord(ev_[15], stream_), "event");

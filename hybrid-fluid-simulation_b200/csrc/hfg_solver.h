@@ -128,7 +128,8 @@ class GridSolver {
   long long launches_ = 0;
 
   DArray<float> vel_[2][3], prev_[3], color_[2][3], dom_[2], solidVel_[3];
-  DArray<uint8_t> solidIdx_, markers_, code_;
+  DArray<uint8_t> solidIdx_, markers_;
+  DArray<Code> code_;
   DArray<float> cgx_, cgr_, cgp_[2];
   DArray<double> partials_;
   DArray<CgState> cgState_;
