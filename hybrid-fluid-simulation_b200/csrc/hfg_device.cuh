@@ -139,14 +139,15 @@ struct FaceSampler {
     axisWeights(uy, g.r.y + 1, fc[1]);
     axisWeights(uz, g.r.z + 1, fc[2]);
   }
-  // weights and 8 linear indices of component `a` (corner order z, y, x)
-  __device__ __forceinline__ void corners(const Geom& g, int a, long long idx[8], float w[8]) const {
+  // weights and 8 linear indices of component `a` (corner order z, y, x);
+  // 32-bit index arithmetic (every grid holds fewer than 2^31 entries)
+  __device__ __forceinline__ void corners(const Geom& g, int a, unsigned idx[8], float w[8]) const {
     const AxisW& X = a == 0 ? fc[0] : cc[0];
     const AxisW& Y = a == 1 ? fc[1] : cc[1];
     const AxisW& Z = a == 2 ? fc[2] : cc[2];
-    long long nx = g.r.x + (a == 0), ny = g.r.y + (a == 1);
-    long long r0 = (long long)Z.i0 * ny, r1 = (long long)Z.i1 * ny;
-    long long b00 = (r0 + Y.i0) * nx, b01 = (r0 + Y.i1) * nx, b10 = (r1 + Y.i0) * nx, b11 = (r1 + Y.i1) * nx;
+    unsigned nx = (unsigned)(g.r.x + (a == 0)), ny = (unsigned)(g.r.y + (a == 1));
+    unsigned r0 = (unsigned)Z.i0 * ny, r1 = (unsigned)Z.i1 * ny;
+    unsigned b00 = (r0 + Y.i0) * nx, b01 = (r0 + Y.i1) * nx, b10 = (r1 + Y.i0) * nx, b11 = (r1 + Y.i1) * nx;
     idx[0] = b00 + X.i0; idx[1] = b00 + X.i1; idx[2] = b01 + X.i0; idx[3] = b01 + X.i1;
     idx[4] = b10 + X.i0; idx[5] = b10 + X.i1; idx[6] = b11 + X.i0; idx[7] = b11 + X.i1;
     float x0 = 1.f - X.w1, x1 = X.w1, y0 = 1.f - Y.w1, y1 = Y.w1, z0 = 1.f - Z.w1, z1 = Z.w1;
@@ -154,7 +155,7 @@ struct FaceSampler {
     w[4] = x0 * y0 * z1; w[5] = x1 * y0 * z1; w[6] = x0 * y1 * z1; w[7] = x1 * y1 * z1;
   }
   __device__ __forceinline__ float sample(const Geom& g, int a, const float* __restrict__ f) const {
-    long long idx[8];
+    unsigned idx[8];
     float w[8];
     corners(g, a, idx, w);
     float v = 0.f;
@@ -165,7 +166,7 @@ struct FaceSampler {
   // sample of the difference field f - h at the same point
   __device__ __forceinline__ float sampleDiff(const Geom& g, int a, const float* __restrict__ f,
                                               const float* __restrict__ h) const {
-    long long idx[8];
+    unsigned idx[8];
     float w[8];
     corners(g, a, idx, w);
     float v = 0.f;

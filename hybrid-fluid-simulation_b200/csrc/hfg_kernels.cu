@@ -5,6 +5,7 @@
 // grid-stride launches sized to the SM count, fused stages, uint8 cell
 // markers, FP64 deterministic reductions and device-resident solver scalars.
 // The reference line each kernel follows is cited beside it.
+#include <algorithm>
 #include <cstdio>
 
 #include "hfg_kernels.h"
@@ -265,24 +266,45 @@ __global__ void kDistInit(long long n, const float* __restrict__ v, uint16_t* __
 
 __device__ inline uint16_t satInc(uint16_t a) { return a >= kFar - 1 ? kFar : (uint16_t)(a + 1); }
 
-// 1-D pass along x: one thread per row, forward then backward sweep.
+// 1-D pass along x: one warp per row, 32 entries at a time.  The forward
+// sweep f[i] = min(d[i], f[i-1] + 1) is a warp prefix-min of d[j] - j plus the
+// carry from the previous chunk; the backward sweep mirrors it.
 __global__ void kDistRows(Dim3i r, uint16_t* __restrict__ d) {
+  constexpr int BIG = 1 << 20;
+  const int lane = threadIdx.x & 31;
+  long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
   long long rows = (long long)r.y * r.z;
-  HFG_FOR(row, rows) {
+  for (long long row = wid; row < rows; row += nw) {
     uint16_t* q = d + row * r.x;
-    uint16_t prev = kFar;
-    for (int i = 0; i < r.x; ++i) {
-      uint16_t v = q[i];
-      uint16_t cand = satInc(prev);
-      if (cand < v) { v = cand; q[i] = v; }
-      prev = v;
+    int carry = BIG;
+    for (int s0 = 0; s0 < r.x; s0 += 32) {
+      int i = s0 + lane;
+      int v = i < r.x ? (q[i] == kFar ? BIG : (int)q[i]) : BIG;
+      int a = v - lane;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, a, o);
+        if (lane >= o) a = min(a, t);
+      }
+      int f = min(a + lane, carry + lane + 1);
+      if (i < r.x) q[i] = (uint16_t)min(f, (int)kFar);
+      carry = __shfl_sync(0xffffffffu, f, 31);
     }
-    prev = kFar;
-    for (int i = r.x - 1; i >= 0; --i) {
-      uint16_t v = q[i];
-      uint16_t cand = satInc(prev);
-      if (cand < v) { v = cand; q[i] = v; }
-      prev = v;
+    carry = BIG;
+    int last = ((r.x - 1) / 32) * 32;
+    for (int s0 = last; s0 >= 0; s0 -= 32) {
+      int i = s0 + lane;
+      int v = i < r.x ? (q[i] == kFar ? BIG : (int)q[i]) : BIG;
+      int b = v + lane;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_down_sync(0xffffffffu, b, o);
+        if (lane + o < 32) b = min(b, t);
+      }
+      int g = min(b - lane, carry + (32 - lane));
+      if (i < r.x) q[i] = (uint16_t)min(g, (int)kFar);
+      carry = __shfl_sync(0xffffffffu, g, 0);
     }
   }
 }
@@ -340,25 +362,33 @@ __global__ void kExclusiveScanSmall(const unsigned int* __restrict__ hist, unsig
   }
 }
 
-// Bucket the entries by layer.  Lanes of a warp that share a layer claim
-// their slots with one atomic (neighbouring entries mostly share a layer).
+// Bucket the entries by layer: a block counts its chunk per layer in shared
+// memory, reserves one global range per (block, layer) and hands out slots
+// with shared-memory atomics.
+constexpr int kScatterChunk = 4096;
 __global__ void kDistScatter(long long n, long long base, const uint16_t* __restrict__ d, int nums,
                              unsigned int* __restrict__ cursor, unsigned int* __restrict__ list) {
-  const unsigned int lane = threadIdx.x & 31;
-  for (long long b0 = (long long)blockIdx.x * blockDim.x; b0 < n; b0 += (long long)gridDim.x * blockDim.x) {
-    long long i = b0 + threadIdx.x;
-    unsigned int v = i < n ? d[i] : 0u;
-    bool want = i < n && v >= 1 && (int)v < nums;
-    unsigned int act = __ballot_sync(0xffffffffu, want);
-    if (want) {
-      unsigned int peers = __match_any_sync(act, v);
-      int leader = __ffs(peers) - 1;
-      unsigned int rank = __popc(peers & ((1u << lane) - 1u));
-      unsigned int slot = 0;
-      if ((int)lane == leader) slot = atomicAdd(cursor + v, (unsigned int)__popc(peers));
-      slot = __shfl_sync(peers, slot, leader);
-      list[slot + rank] = (unsigned int)(base + i);
+  __shared__ unsigned int cnt[kMaxLayers + 1], start[kMaxLayers + 1];
+  for (long long c0 = (long long)blockIdx.x * kScatterChunk; c0 < n; c0 += (long long)gridDim.x * kScatterChunk) {
+    long long c1 = c0 + kScatterChunk < n ? c0 + kScatterChunk : n;
+    for (int i = threadIdx.x; i <= kMaxLayers; i += blockDim.x) cnt[i] = 0;
+    __syncthreads();
+    for (long long i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
+      unsigned int v = d[i];
+      if (v >= 1 && (int)v < nums) atomicAdd(&cnt[v], 1u);
     }
+    __syncthreads();
+    for (int i = threadIdx.x; i <= kMaxLayers; i += blockDim.x) {
+      unsigned int k = cnt[i];
+      start[i] = k ? atomicAdd(cursor + i, k) : 0u;
+      cnt[i] = 0;
+    }
+    __syncthreads();
+    for (long long i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
+      unsigned int v = d[i];
+      if (v >= 1 && (int)v < nums) list[start[v] + atomicAdd(&cnt[v], 1u)] = (unsigned int)(base + i);
+    }
+    __syncthreads();
   }
 }
 
@@ -369,7 +399,7 @@ cudaError_t launchExtrapDistance(const Dim3i rc[3], float* const vals[3], long l
     long long n = rc[a].size();
     uint16_t* d = sc.dist + off[a];
     kDistInit<<<gridFor(n), kThreads, 0, s>>>(n, vals[a], d);
-    kDistRows<<<gridFor((long long)rc[a].y * rc[a].z), kThreads, 0, s>>>(rc[a], d);
+    kDistRows<<<gridFor((long long)rc[a].y * rc[a].z * 32), kThreads, 0, s>>>(rc[a], d);
     kDistCols<<<gridFor((long long)rc[a].x * rc[a].z), kThreads, 0, s>>>(rc[a], 1, d);
     kDistCols<<<gridFor((long long)rc[a].x * rc[a].y), kThreads, 0, s>>>(rc[a], 2, d);
   }
@@ -382,7 +412,9 @@ cudaError_t launchExtrapDistance(const Dim3i rc[3], float* const vals[3], long l
   kExclusiveScanSmall<<<1, 1, 0, s>>>(sc.hist, sc.offsets, sc.cursor, kMaxLayers + 1);
   for (int a = 0; a < 3; ++a) {
     long long n = rc[a].size();
-    kDistScatter<<<gridFor(n), kThreads, 0, s>>>(n, off[a], sc.dist + off[a], nums, sc.cursor, sc.list);
+    int blocks = (int)std::min<long long>((n + kScatterChunk - 1) / kScatterChunk, (long long)numSMs() * 8);
+    if (blocks < 1) blocks = 1;
+    kDistScatter<<<blocks, kThreads, 0, s>>>(n, off[a], sc.dist + off[a], nums, sc.cursor, sc.list);
   }
   return cudaGetLastError();
 }
@@ -785,7 +817,7 @@ __global__ void kP2GFaceLinear(Geom g, const float* __restrict__ pos, const floa
     float2* acc[3] = {a0, a1, a2};
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      long long idx[8];
+      unsigned idx[8];
       float w[8];
       fs.corners(g, a, idx, w);
       float val = vel[3 * p + a];

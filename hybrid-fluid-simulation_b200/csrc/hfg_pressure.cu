@@ -29,7 +29,7 @@ CgGrid cgGrid(const Dim3i& r) {
   g.block = dim3(TX, TY, 1);
   int bx = (r.x + TX - 1) / TX, by = (r.y + TY - 1) / TY;
   long long tiles = (long long)bx * by;
-  long long want = (long long)numSMs() * 8;
+  long long want = (long long)numSMs() * 16;
   int zc = (int)std::max<long long>(1, (want + tiles - 1) / tiles);
   zc = std::min(zc, std::max(1, r.z / 4));
   g.zPer = (r.z + zc - 1) / zc;
@@ -246,41 +246,51 @@ cudaError_t launchRhsInit(const Geom& gm, ConstFaceField v, ConstFaceField svArr
 // ---------------------------------------------------------------------------
 // CG direction: p = z + beta p_old (scal then axpy with 1), q = A p and the
 // reduction p.q; the last block forms alpha = r.z / p.Ap
-// (CuMatrixFreePCG.cpp:40-47, :56-60).  p at the lateral neighbours is
-// recomputed from r and p_old (L1 hits), along z it is carried in registers.
+// (CuMatrixFreePCG.cpp:40-47, :56-60).  p of the current plane (with a one-
+// cell halo) sits in a double-buffered shared tile, p below / above in
+// registers; every p value is formed once per cell plus the halo ring.
 template <int PC>
-__global__ void __launch_bounds__(TX* TY) kCgDirection(Dim3i R, float sx, float sy, float sz,
-                                                       const Code* __restrict__ code, const float* __restrict__ r,
-                                                       const float* __restrict__ pOld, float* __restrict__ pNew,
-                                                       double* partials, CgState* st, int zPer) {
+__global__ void __launch_bounds__(TX* TY, 4) kCgDirection(Dim3i R, float sx, float sy, float sz,
+                                                          const Code* __restrict__ code, const float* __restrict__ r,
+                                                          const float* __restrict__ pOld, float* __restrict__ pNew,
+                                                          double* partials, CgState* st, int zPer) {
   if (st->done) return;
+  __shared__ float tile[2][TY + 2][TX + 2];
   const float beta = st->beta;
   double pq = 0.0, dummy = 0.0;
-  int x = blockIdx.x * TX + threadIdx.x, y = blockIdx.y * TY + threadIdx.y;
-  if (x < R.x && y < R.y) {
-    int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, R.z);
-    const long long plane = (long long)R.x * R.y;
-    auto pn = [&](long long i) -> float {
-      float zz = precondZ<PC>(__ldg(code + i), __ldg(r + i), sx, sy, sz);
-      return __fadd_rn(__fmul_rn(beta, __ldg(pOld + i)), zz);
-    };
-    long long c = (long long)z0 * plane + (long long)y * R.x + x;
-    float below = z0 > 0 ? pn(c - plane) : 0.f;
-    float cur = pn(c);
-    for (int z = z0; z < z1; ++z, c += plane) {
-      float above = z + 1 < R.z ? pn(c + plane) : 0.f;
-      Code k = __ldg(code + c);
-      float q = cur;
-      if (k & 1) {
-        float vl = nbFluid(k, 0) ? pn(c - 1) : 0.f, vr = nbFluid(k, 1) ? pn(c + 1) : 0.f;
-        float vd = nbFluid(k, 2) ? pn(c - R.x) : 0.f, vu = nbFluid(k, 3) ? pn(c + R.x) : 0.f;
-        q = applyRow(k, sx, sy, sz, cur, vl, vr, vd, vu, below, above);
-      }
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int x = blockIdx.x * TX + tx, y = blockIdx.y * TY + ty;
+  const bool in = x < R.x && y < R.y;
+  const int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, R.z);
+  const unsigned plane = (unsigned)R.x * (unsigned)R.y;
+  auto pn = [&](unsigned i) -> float {
+    float zz = precondZ<PC>(__ldg(code + i), __ldg(r + i), sx, sy, sz);
+    return __fadd_rn(__fmul_rn(beta, __ldg(pOld + i)), zz);
+  };
+  unsigned c = (unsigned)z0 * plane + (unsigned)y * (unsigned)R.x + (unsigned)x;
+  float below = (in && z0 > 0) ? pn(c - plane) : 0.f;
+  float cur = in ? pn(c) : 0.f;
+  int buf = 0;
+  for (int z = z0; z < z1; ++z, c += plane, buf ^= 1) {
+    float above = (in && z + 1 < R.z) ? pn(c + plane) : 0.f;
+    Code k = in ? __ldg(code + c) : (Code)0;
+    // halo ring of this plane (zero outside the grid; only read for fluid
+    // neighbours, which are inside by construction)
+    float (*t)[TX + 2] = tile[buf];
+    t[ty + 1][tx + 1] = cur;
+    if (tx == 0) t[ty + 1][0] = (in && x > 0) ? pn(c - 1) : 0.f;
+    if (tx == TX - 1 || x == R.x - 1) t[ty + 1][tx + 2] = (in && x + 1 < R.x) ? pn(c + 1) : 0.f;
+    if (ty == 0) t[0][tx + 1] = (x < R.x && y < R.y && y > 0) ? pn(c - R.x) : 0.f;
+    if (ty == TY - 1 || y == R.y - 1) t[ty + 2][tx + 1] = (in && y + 1 < R.y) ? pn(c + R.x) : 0.f;
+    __syncthreads();
+    if (in) {
+      float q = applyRow(k, sx, sy, sz, cur, t[ty + 1][tx], t[ty + 1][tx + 2], t[ty][tx + 1], t[ty + 2][tx + 1],
+                         below, above);
       pNew[c] = cur;
       pq += (double)cur * (double)q;
-      below = cur;
-      cur = above;
     }
+    below = cur;
+    cur = above;
   }
   if (gridSum2(pq, dummy, partials, &st->ticket) && flatTid() == 0) {
     st->pAp = pq;
@@ -289,47 +299,56 @@ __global__ void __launch_bounds__(TX* TY) kCgDirection(Dim3i R, float sx, float 
   }
 }
 
-// CG update: x += alpha p, r -= alpha A p (A p recomputed), z = M^-1 r, the
-// reductions r.r and r.z; the last block checks convergence and forms beta
-// (CuMatrixFreePCG.cpp:49-63).  The |alpha| < FLT_EPSILON skip of
-// CCuDenseVector::plusAlphaX (CuDenseVector.cpp:178) is kept.
+// CG update: x += alpha p, r -= alpha A p (A p recomputed from the stored p
+// through the same shared tile), z = M^-1 r, the reductions r.r and r.z; the
+// last block checks convergence and forms beta (CuMatrixFreePCG.cpp:49-63).
+// The |alpha| < FLT_EPSILON skip of CCuDenseVector::plusAlphaX
+// (CuDenseVector.cpp:178) is kept.
 template <int PC>
-__global__ void __launch_bounds__(TX* TY) kCgUpdate(Dim3i R, float sx, float sy, float sz,
-                                                    const Code* __restrict__ code, const float* __restrict__ p,
-                                                    float* __restrict__ xv, float* __restrict__ r, double* partials,
-                                                    CgState* st, int zPer) {
+__global__ void __launch_bounds__(TX* TY, 4) kCgUpdate(Dim3i R, float sx, float sy, float sz,
+                                                       const Code* __restrict__ code, const float* __restrict__ p,
+                                                       float* __restrict__ xv, float* __restrict__ r,
+                                                       double* partials, CgState* st, int zPer) {
   if (st->done) return;
+  __shared__ float tile[2][TY + 2][TX + 2];
   const float alpha = st->alpha;
   const bool skip = fabsf(alpha) < FLT_EPSILON;
   double rr = 0.0, rz = 0.0;
-  int x = blockIdx.x * TX + threadIdx.x, y = blockIdx.y * TY + threadIdx.y;
-  if (x < R.x && y < R.y) {
-    int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, R.z);
-    const long long plane = (long long)R.x * R.y;
-    long long c = (long long)z0 * plane + (long long)y * R.x + x;
-    float below = z0 > 0 ? __ldg(p + c - plane) : 0.f;
-    float cur = __ldg(p + c);
-    for (int z = z0; z < z1; ++z, c += plane) {
-      float above = z + 1 < R.z ? __ldg(p + c + plane) : 0.f;
-      Code k = __ldg(code + c);
-      float rv = r[c];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int x = blockIdx.x * TX + tx, y = blockIdx.y * TY + ty;
+  const bool in = x < R.x && y < R.y;
+  const int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, R.z);
+  const unsigned plane = (unsigned)R.x * (unsigned)R.y;
+  unsigned c = (unsigned)z0 * plane + (unsigned)y * (unsigned)R.x + (unsigned)x;
+  float below = (in && z0 > 0) ? __ldg(p + c - plane) : 0.f;
+  float cur = in ? __ldg(p + c) : 0.f;
+  int buf = 0;
+  for (int z = z0; z < z1; ++z, c += plane, buf ^= 1) {
+    float above = (in && z + 1 < R.z) ? __ldg(p + c + plane) : 0.f;
+    Code k = in ? __ldg(code + c) : (Code)0;
+    float rv = in ? r[c] : 0.f;
+    float xo = (in && !skip) ? xv[c] : 0.f;
+    float (*t)[TX + 2] = tile[buf];
+    t[ty + 1][tx + 1] = cur;
+    if (tx == 0) t[ty + 1][0] = (in && x > 0) ? __ldg(p + c - 1) : 0.f;
+    if (tx == TX - 1 || x == R.x - 1) t[ty + 1][tx + 2] = (in && x + 1 < R.x) ? __ldg(p + c + 1) : 0.f;
+    if (ty == 0) t[0][tx + 1] = (x < R.x && y < R.y && y > 0) ? __ldg(p + c - R.x) : 0.f;
+    if (ty == TY - 1 || y == R.y - 1) t[ty + 2][tx + 1] = (in && y + 1 < R.y) ? __ldg(p + c + R.x) : 0.f;
+    __syncthreads();
+    if (in) {
       if (!skip) {
-        float q = cur;
-        if (k & 1) {
-          float vl = nbFluid(k, 0) ? __ldg(p + c - 1) : 0.f, vr = nbFluid(k, 1) ? __ldg(p + c + 1) : 0.f;
-          float vd = nbFluid(k, 2) ? __ldg(p + c - R.x) : 0.f, vu = nbFluid(k, 3) ? __ldg(p + c + R.x) : 0.f;
-          q = applyRow(k, sx, sy, sz, cur, vl, vr, vd, vu, below, above);
-        }
-        xv[c] = fmaf(alpha, cur, xv[c]);
+        float q = applyRow(k, sx, sy, sz, cur, t[ty + 1][tx], t[ty + 1][tx + 2], t[ty][tx + 1], t[ty + 2][tx + 1],
+                           below, above);
+        xv[c] = fmaf(alpha, cur, xo);
         rv = fmaf(-alpha, q, rv);
         r[c] = rv;
       }
       float zz = precondZ<PC>(k, rv, sx, sy, sz);
       rr += (double)rv * (double)rv;
       rz += (double)rv * (double)zz;
-      below = cur;
-      cur = above;
     }
+    below = cur;
+    cur = above;
   }
   if (gridSum2(rr, rz, partials, &st->ticket) && flatTid() == 0) {
     st->rr = rr;
