@@ -716,7 +716,8 @@ __device__ inline float substepSize(const SubstepState& s, float dt, float cfl, 
 // box clamp of fixParticlesPosWithBoundarys (EulerParticlesTool.cu:310-333) is
 // applied to the first `nclamp` particles; otherwise the next v0 and its max
 // are produced for slot+1.
-__global__ void kSubstep(Geom g, ConstFaceField vel, float* __restrict__ pos, float* __restrict__ v0, long long P,
+__global__ void __launch_bounds__(256, 4) kSubstep(Geom g, ConstFaceField vel, float* __restrict__ pos,
+                                                  float* __restrict__ v0, long long P,
                          int acc, float dt, float cfl, long long nclamp, SubstepState* st, int slot) {
   const SubstepState cur = st[slot];
   if (cur.finished) {

@@ -1,20 +1,488 @@
-// hfg_mg.cu -- geometric multigrid preconditioner for the pressure CG.
+// hfg_mg.cu -- mixed-precision geometric multigrid preconditioner for the
+// pressure CG.
+//
+// The reference solves the pressure system with an unpreconditioned CG
+// (PressureSolver.cpp:12-15 copies r into z).  This preconditioner is new: a
+// cell-centred V-cycle on the level hierarchy of the fluid/air/solid markers,
+// used inside an FP32 CG whose dot products and convergence test stay FP64.
+//
+//  * coarsening: a coarse cell is air (Dirichlet, p = 0) if any of its <= 8
+//    children is air, else fluid if any child is fluid, else solid;
+//  * level operators: the same matrix-free 7-point stencil rebuilt from each
+//    level's markers with the scales dt / (rho h^2) of that level (h doubles);
+//  * smoothing: damped Jacobi (omega = 2/3), nu sweeps before and after;
+//  * transfers: restriction = mean of the children's residuals, prolongation =
+//    piecewise-constant injection (the scaled transpose), so the V-cycle is a
+//    symmetric operator and plain CG applies;
+//  * coarsest level (<= 512 cells): many Jacobi sweeps in one block's shared
+//    memory;
+//  * precision: level-0 vectors FP32; every coarser level stores its
+//    right-hand side and iterate in BF16 (or FP16) and computes in FP32.
+//
+// Every kernel returns at once when the CG has converged (CgState::done), so
+// chunks of iterations can be launched without host round trips.
+#include <algorithm>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <vector>
+
 #include "hfg_solver.h"
 
 namespace hfg {
 
-struct Multigrid {
-  int dummy;
+namespace {
+constexpr int BX = 32, BY = 4, BZ = 2;
+constexpr float kOmega = 2.0f / 3.0f;
+constexpr int kCoarseMax = 512;
+constexpr int kCoarseSweeps = 48;
+
+template <class T> __device__ __forceinline__ float ld(const T* p, unsigned i);
+template <> __device__ __forceinline__ float ld<float>(const float* p, unsigned i) { return __ldg(p + i); }
+template <> __device__ __forceinline__ float ld<__nv_bfloat16>(const __nv_bfloat16* p, unsigned i) {
+  return __bfloat162float(p[i]);
+}
+template <class T> __device__ __forceinline__ T cvt(float v);
+template <> __device__ __forceinline__ float cvt<float>(float v) { return v; }
+template <> __device__ __forceinline__ __nv_bfloat16 cvt<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
+
+__device__ __forceinline__ bool nbF(Code k, int d) { return (k >> (7 + d)) & 1; }
+__device__ __forceinline__ float diagOfC(Code k, float sx, float sy, float sz) {
+  if (!(k & 1)) return 1.f;
+  float d = 0.f;
+  if (k & 2) d += sx;
+  if (k & 4) d += sx;
+  if (k & 8) d += sy;
+  if (k & 16) d += sy;
+  if (k & 32) d += sz;
+  if (k & 64) d += sz;
+  return d;
+}
+
+struct Lvl {
+  Dim3i r;
+  float sx, sy, sz;
 };
 
-Multigrid* mgCreate(const Dim3i&, int, int, bool) {
-  throw CudaError("multigrid preconditioner not available in this build", HFG_ERR_UNSUPPORTED);
+dim3 gridOf(const Dim3i& r) { return dim3((r.x + BX - 1) / BX, (r.y + BY - 1) / BY, (r.z + BZ - 1) / BZ); }
+
+__device__ __forceinline__ bool cellOf(const Dim3i& r, int& x, int& y, int& z, unsigned& c) {
+  x = blockIdx.x * BX + threadIdx.x;
+  y = blockIdx.y * BY + threadIdx.y;
+  z = blockIdx.z * BZ + threadIdx.z;
+  if (x >= r.x || y >= r.y || z >= r.z) return false;
+  c = ((unsigned)z * r.y + y) * r.x + x;
+  return true;
 }
+
+// (A v)_c with the value of neighbour d (left, right, down, up, back, front)
+// fetched by get(d); only fluid neighbours are asked for.
+template <class G>
+__device__ __forceinline__ float applyA(const Lvl& L, Code k, float vc, G get) {
+  if (!(k & 1)) return vc;
+  float acc = diagOfC(k, L.sx, L.sy, L.sz) * vc;
+  if (nbF(k, 0)) acc -= L.sx * get(0);
+  if (nbF(k, 1)) acc -= L.sx * get(1);
+  if (nbF(k, 2)) acc -= L.sy * get(2);
+  if (nbF(k, 3)) acc -= L.sy * get(3);
+  if (nbF(k, 4)) acc -= L.sz * get(4);
+  if (nbF(k, 5)) acc -= L.sz * get(5);
+  return acc;
+}
+
+__device__ __forceinline__ void nbrOf(int d, int& dx, int& dy, int& dz) {
+  dx = d == 0 ? -1 : (d == 1 ? 1 : 0);
+  dy = d == 2 ? -1 : (d == 3 ? 1 : 0);
+  dz = d == 4 ? -1 : (d == 5 ? 1 : 0);
+}
+
+// Coarse markers: air if any child is air, else fluid if any child is fluid,
+// else solid.
+__global__ void kCoarsenMarkers(Dim3i rf, Dim3i rc, const uint8_t* __restrict__ mf, uint8_t* __restrict__ mc) {
+  int X, Y, Z;
+  unsigned C;
+  if (!cellOf(rc, X, Y, Z, C)) return;
+  bool anyAir = false, anyFluid = false;
+  for (int k = 0; k < 2; ++k)
+    for (int j = 0; j < 2; ++j)
+      for (int i = 0; i < 2; ++i) {
+        int x = 2 * X + i, y = 2 * Y + j, z = 2 * Z + k;
+        if (x >= rf.x || y >= rf.y || z >= rf.z) continue;
+        uint8_t m = mf[((unsigned)z * rf.y + y) * rf.x + x];
+        anyAir |= m == kAir;
+        anyFluid |= m == kFluid;
+      }
+  mc[C] = anyAir ? kAir : (anyFluid ? kFluid : kSolid);
+}
+
+// First pre-smoothing sweep from z = 0: z = omega b / diag.
+template <class TB, class TZ>
+__global__ void kJacobiFirst(Lvl L, const TB* __restrict__ b, TZ* __restrict__ z, const Code* __restrict__ code,
+                             const CgState* st) {
+  if (st->done) return;
+  int x, y, zz;
+  unsigned c;
+  if (!cellOf(L.r, x, y, zz, c)) return;
+  Code k = code[c];
+  float v = (k & 1) ? kOmega * ld(b, c) / diagOfC(k, L.sx, L.sy, L.sz) : 0.f;
+  z[c] = cvt<TZ>(v);
+}
+
+// One damped-Jacobi sweep zo = zi + omega (b - A zi) / diag.  With a coarse
+// correction `zc` the sweep acts on zi + P zc (prolongation fused in).  With
+// `dot` the sweep also reduces r.z and finishes the CG's beta (level 0, last
+// post-smoothing sweep).
+template <class TB, class TZ, class TC, bool CORR, bool DOT>
+__global__ void kJacobi(Lvl L, Dim3i rc, const TB* __restrict__ b, const TZ* __restrict__ zi, TZ* __restrict__ zo,
+                        const TC* __restrict__ zc, const Code* __restrict__ code, double* partials, CgState* st) {
+  if (st->done) return;
+  int x, y, z;
+  unsigned c;
+  double rz = 0.0, dummy = 0.0;
+  bool in = cellOf(L.r, x, y, z, c);
+  if (in) {
+    const unsigned pl = (unsigned)L.r.x * L.r.y;
+    auto zAt = [&](int d) -> float {
+      int dx, dy, dz;
+      nbrOf(d, dx, dy, dz);
+      unsigned i = c + dx + dy * L.r.x + dz * pl;
+      float v = ld(zi, i);
+      if (CORR) v += ld(zc, ((unsigned)((z + dz) >> 1) * rc.y + ((y + dy) >> 1)) * rc.x + ((x + dx) >> 1));
+      return v;
+    };
+    Code k = code[c];
+    float v = 0.f;
+    float bv = ld(b, c);
+    if (k & 1) {
+      float vc = ld(zi, c);
+      if (CORR) vc += ld(zc, ((unsigned)(z >> 1) * rc.y + (y >> 1)) * rc.x + (x >> 1));
+      float az = applyA(L, k, vc, zAt);
+      v = vc + kOmega * (bv - az) / diagOfC(k, L.sx, L.sy, L.sz);
+    }
+    zo[c] = cvt<TZ>(v);
+    if (DOT) rz = (double)bv * (double)v;
+  }
+  if (DOT) {
+    if (gridSum2(rz, dummy, partials, &st->ticket) && flatTid() == 0) {
+      // first V-cycle after the RHS: beta stays 0, rz initialised
+      if (st->iter == 0) {
+        st->rz = rz;
+        st->beta = 0.f;
+      } else {
+        st->beta = (float)(rz / st->rz);
+        st->rz = rz;
+      }
+      st->ticket = 0;
+    }
+  }
+}
+
+// Residual of level f restricted to level c: bc = mean over the children of
+// (b - A z).
+template <class TB, class TZ, class TBC>
+__global__ void kResidualRestrict(Lvl Lf, Dim3i rc, const TB* __restrict__ b, const TZ* __restrict__ zf,
+                                  const Code* __restrict__ code, TBC* __restrict__ bc, const CgState* st) {
+  if (st->done) return;
+  int X, Y, Z;
+  unsigned C;
+  if (!cellOf(rc, X, Y, Z, C)) return;
+  float s = 0.f;
+  for (int kk = 0; kk < 2; ++kk)
+    for (int j = 0; j < 2; ++j)
+      for (int i = 0; i < 2; ++i) {
+        int x = 2 * X + i, y = 2 * Y + j, z = 2 * Z + kk;
+        if (x >= Lf.r.x || y >= Lf.r.y || z >= Lf.r.z) continue;
+        unsigned c = ((unsigned)z * Lf.r.y + y) * Lf.r.x + x;
+        Code k = code[c];
+        if (!(k & 1)) continue;
+        const unsigned pl = (unsigned)Lf.r.x * Lf.r.y;
+        float az = applyA(Lf, k, ld(zf, c), [&](int d) {
+          int dx, dy, dz;
+          nbrOf(d, dx, dy, dz);
+          return ld(zf, c + dx + dy * Lf.r.x + dz * pl);
+        });
+        s += ld(b, c) - az;
+      }
+  bc[C] = cvt<TBC>(0.125f * s);
+}
+
+// Coarsest level: Jacobi sweeps in one block's shared memory.
+template <class TB, class TZ>
+__global__ void kCoarseSolve(Lvl L, const TB* __restrict__ b, TZ* __restrict__ z, const Code* __restrict__ code,
+                             const CgState* st) {
+  if (st->done) return;
+  __shared__ float za[kCoarseMax], zb[kCoarseMax];
+  unsigned n = (unsigned)L.r.size();
+  for (unsigned c = threadIdx.x; c < n; c += blockDim.x) za[c] = 0.f;
+  __syncthreads();
+  float* cur = za;
+  float* nxt = zb;
+  for (int it = 0; it < kCoarseSweeps; ++it) {
+    for (unsigned c = threadIdx.x; c < n; c += blockDim.x) {
+      Code k = code[c];
+      float v = 0.f;
+      if (k & 1) {
+        const unsigned pl = (unsigned)L.r.x * L.r.y;
+        float az = applyA(L, k, cur[c], [&](int d) {
+          int dx, dy, dz;
+          nbrOf(d, dx, dy, dz);
+          return cur[c + dx + dy * L.r.x + dz * pl];
+        });
+        v = cur[c] + kOmega * (ld(b, c) - az) / diagOfC(k, L.sx, L.sy, L.sz);
+      }
+      nxt[c] = v;
+    }
+    __syncthreads();
+    float* t = cur;
+    cur = nxt;
+    nxt = t;
+  }
+  for (unsigned c = threadIdx.x; c < n; c += blockDim.x) z[c] = cvt<TZ>(cur[c]);
+}
+}  // namespace
+
+// Declared in the CG kernels file: the MG flavour of the two CG kernels.
+cudaError_t launchCgDirectionZ(const Dim3i& r, float sx, float sy, float sz, const Code* code, const float* z,
+                               const float* pOld, float* pNew, double* partials, CgState* st, cudaStream_t s);
+cudaError_t launchCgUpdateNoZ(const Dim3i& r, float sx, float sy, float sz, const Code* code, const float* p,
+                              float* x, float* rr, double* partials, CgState* st, cudaStream_t s);
+
+struct Multigrid {
+  Dim3i r0;
+  int smooth = 2;
+  bool half = true;
+  std::vector<Dim3i> res;            // level resolutions, [0] = fine
+  std::vector<DArray<uint8_t>*> mk;  // levels >= 1
+  std::vector<DArray<Code>*> code;   // levels >= 1
+  std::vector<DArray<uint16_t>*> b16, z16a, z16b;  // levels >= 1 (BF16 / FP16 storage)
+  std::vector<DArray<float>*> b32, z32a, z32b;     // levels >= 1 when !half
+  DArray<float> z0a, z0b;            // level 0 iterate (FP32)
+  DArray<float> p[2];
+  DArray<double> partials;
+  const Code* code0 = nullptr;
+  float s0[3] = {0, 0, 0};
+  ~Multigrid() {
+    for (auto* v : mk) delete v;
+    for (auto* v : code) delete v;
+    for (auto* v : b16) delete v;
+    for (auto* v : z16a) delete v;
+    for (auto* v : z16b) delete v;
+    for (auto* v : b32) delete v;
+    for (auto* v : z32a) delete v;
+    for (auto* v : z32b) delete v;
+  }
+  int levels() const { return (int)res.size(); }
+};
+
+Multigrid* mgCreate(const Dim3i& r, int levels, int smooth, bool half) {
+  auto* m = new Multigrid();
+  m->r0 = r;
+  m->smooth = smooth > 0 ? smooth : 2;
+  m->half = half;
+  m->res.push_back(r);
+  Dim3i cur = r;
+  while ((levels <= 0 || (int)m->res.size() < levels) && cur.size() > kCoarseMax) {
+    Dim3i nx{(cur.x + 1) / 2, (cur.y + 1) / 2, (cur.z + 1) / 2};
+    if (nx.x == cur.x && nx.y == cur.y && nx.z == cur.z) break;
+    m->res.push_back(nx);
+    cur = nx;
+  }
+  if (m->res.back().size() > kCoarseMax) {
+    delete m;
+    throw CudaError("multigrid: coarsest level too large; allow more levels", HFG_ERR_INVALID);
+  }
+  long long N = r.size();
+  m->z0a.alloc(N);
+  m->z0b.alloc(N);
+  m->p[0].alloc(N);
+  m->p[1].alloc(N);
+  m->partials.alloc(std::max(cgPartialsNeeded(r), 2 * (int)(gridOf(r).x * gridOf(r).y * gridOf(r).z)));
+  for (int l = 1; l < m->levels(); ++l) {
+    long long n = m->res[l].size();
+    auto* a = new DArray<uint8_t>();
+    a->alloc(n);
+    m->mk.push_back(a);
+    auto* c = new DArray<Code>();
+    c->alloc(n);
+    m->code.push_back(c);
+    if (half) {
+      auto* b = new DArray<uint16_t>(); b->alloc(n); m->b16.push_back(b);
+      auto* za = new DArray<uint16_t>(); za->alloc(n); m->z16a.push_back(za);
+      auto* zb = new DArray<uint16_t>(); zb->alloc(n); m->z16b.push_back(zb);
+    } else {
+      auto* b = new DArray<float>(); b->alloc(n); m->b32.push_back(b);
+      auto* za = new DArray<float>(); za->alloc(n); m->z32a.push_back(za);
+      auto* zb = new DArray<float>(); zb->alloc(n); m->z32b.push_back(zb);
+    }
+  }
+  return m;
+}
+
 void mgDestroy(Multigrid* m) { delete m; }
-void mgSetup(Multigrid*, const Code*, float, float, float, cudaStream_t, long long&) {}
-void mgRunCg(Multigrid*, const Dim3i&, float, float, float, const Code*, float*, float*, double*, CgState*,
-             CgState*, cudaStream_t, long long&) {
-  throw CudaError("multigrid preconditioner not available in this build", HFG_ERR_UNSUPPORTED);
+
+// Level markers and stencil codes for the current step's fine markers.
+void mgSetupLevels(Multigrid* m, const uint8_t* mk0, const Code* code0, float sx, float sy, float sz, cudaStream_t s,
+                   long long& launches) {
+  m->code0 = code0;
+  m->s0[0] = sx; m->s0[1] = sy; m->s0[2] = sz;
+  const uint8_t* fine = mk0;
+  for (int l = 1; l < m->levels(); ++l) {
+    Dim3i rf = m->res[l - 1], rc = m->res[l];
+    kCoarsenMarkers<<<gridOf(rc), dim3(BX, BY, BZ), 0, s>>>(rf, rc, fine, m->mk[l - 1]->p);
+    check(cudaGetLastError(), "coarsen markers");
+    check(launchStencilCode(rc, m->mk[l - 1]->p, m->code[l - 1]->p, s), "level stencil code");
+    launches += 2;
+    fine = m->mk[l - 1]->p;
+  }
+}
+
+namespace {
+template <class TS>
+const float* vcycleT(Multigrid* m, const float* r0, CgState* st, cudaStream_t s, long long& launches, TS* const* bL,
+                     TS* const* zaL, TS* const* zbL) {
+  const int L = m->levels();
+  std::vector<Lvl> lv(L);
+  for (int l = 0; l < L; ++l) {
+    float f = 1.f;
+    for (int i = 0; i < l; ++i) f *= 0.25f;
+    lv[l] = Lvl{m->res[l], m->s0[0] * f, m->s0[1] * f, m->s0[2] * f};
+  }
+  auto codeOf = [&](int l) -> const Code* { return l == 0 ? m->code0 : m->code[l - 1]->p; };
+  dim3 blk(BX, BY, BZ);
+  const int nu = m->smooth;
+  // which ping-pong buffer holds the current iterate of each level
+  std::vector<int> curBuf(L, 0);
+  float* z0[2] = {m->z0a.p, m->z0b.p};
+  // downward sweep
+  for (int l = 0; l < L - 1; ++l) {
+    if (l == 0) {
+      kJacobiFirst<float, float><<<gridOf(lv[0].r), blk, 0, s>>>(lv[0], r0, z0[0], codeOf(0), st);
+      int cb = 0;
+      for (int k = 1; k < nu; ++k, cb ^= 1)
+        kJacobi<float, float, float, false, false><<<gridOf(lv[0].r), blk, 0, s>>>(
+            lv[0], lv[0].r, r0, z0[cb], z0[cb ^ 1], nullptr, codeOf(0), nullptr, st);
+      curBuf[0] = cb;
+      kResidualRestrict<float, float, TS><<<gridOf(lv[1].r), blk, 0, s>>>(lv[0], lv[1].r, r0, z0[cb], codeOf(0), bL[1],
+                                                                           st);
+      launches += nu + 1;
+    } else {
+      TS* zl[2] = {zaL[l], zbL[l]};
+      kJacobiFirst<TS, TS><<<gridOf(lv[l].r), blk, 0, s>>>(lv[l], bL[l], zl[0], codeOf(l), st);
+      int cb = 0;
+      for (int k = 1; k < nu; ++k, cb ^= 1)
+        kJacobi<TS, TS, TS, false, false><<<gridOf(lv[l].r), blk, 0, s>>>(lv[l], lv[l].r, bL[l], zl[cb],
+                                                                           zl[cb ^ 1], nullptr, codeOf(l), nullptr, st);
+      curBuf[l] = cb;
+      kResidualRestrict<TS, TS, TS><<<gridOf(lv[l + 1].r), blk, 0, s>>>(lv[l], lv[l + 1].r, bL[l], zl[cb], codeOf(l),
+                                                                         bL[l + 1], st);
+      launches += nu + 1;
+    }
+  }
+  // coarsest
+  {
+    int l = L - 1;
+    if (l == 0) {
+      kCoarseSolve<float, float><<<1, 1024, 0, s>>>(lv[0], r0, z0[0], codeOf(0), st);
+      curBuf[0] = 0;
+    } else {
+      kCoarseSolve<TS, TS><<<1, 1024, 0, s>>>(lv[l], bL[l], zaL[l], codeOf(l), st);
+      curBuf[l] = 0;
+    }
+    launches += 1;
+  }
+  // upward sweep: prolongation fused into the first post-smoothing sweep
+  for (int l = L - 2; l >= 0; --l) {
+    const TS* zc = (curBuf[l + 1] == 0) ? zaL[l + 1] : zbL[l + 1];
+    if (l == 0) {
+      int cb = curBuf[0];
+      for (int k = 0; k < nu; ++k, cb ^= 1) {
+        bool last = k == nu - 1;
+        if (k == 0 && last)
+          kJacobi<float, float, TS, true, true><<<gridOf(lv[0].r), blk, 0, s>>>(
+              lv[0], lv[1].r, r0, z0[cb], z0[cb ^ 1], zc, codeOf(0), m->partials.p, st);
+        else if (k == 0)
+          kJacobi<float, float, TS, true, false><<<gridOf(lv[0].r), blk, 0, s>>>(
+              lv[0], lv[1].r, r0, z0[cb], z0[cb ^ 1], zc, codeOf(0), nullptr, st);
+        else if (last)
+          kJacobi<float, float, float, false, true><<<gridOf(lv[0].r), blk, 0, s>>>(
+              lv[0], lv[0].r, r0, z0[cb], z0[cb ^ 1], nullptr, codeOf(0), m->partials.p, st);
+        else
+          kJacobi<float, float, float, false, false><<<gridOf(lv[0].r), blk, 0, s>>>(
+              lv[0], lv[0].r, r0, z0[cb], z0[cb ^ 1], nullptr, codeOf(0), nullptr, st);
+      }
+      curBuf[0] = cb;
+      launches += nu;
+    } else {
+      TS* zl[2] = {zaL[l], zbL[l]};
+      int cb = curBuf[l];
+      for (int k = 0; k < nu; ++k, cb ^= 1) {
+        if (k == 0)
+          kJacobi<TS, TS, TS, true, false><<<gridOf(lv[l].r), blk, 0, s>>>(lv[l], lv[l + 1].r, bL[l], zl[cb],
+                                                                            zl[cb ^ 1], zc, codeOf(l), nullptr, st);
+        else
+          kJacobi<TS, TS, TS, false, false><<<gridOf(lv[l].r), blk, 0, s>>>(lv[l], lv[l].r, bL[l], zl[cb],
+                                                                             zl[cb ^ 1], nullptr, codeOf(l), nullptr,
+                                                                             st);
+      }
+      curBuf[l] = cb;
+      launches += nu;
+    }
+  }
+  check(cudaGetLastError(), "v-cycle");
+  return z0[curBuf[0]];
+}
+}  // namespace
+
+// z = V(r0) (returned: one of the two level-0 buffers), and st->rz /
+// st->beta updated by the last sweep.
+const float* mgVcycle(Multigrid* m, const float* r0, CgState* st, cudaStream_t s, long long& launches) {
+  const int L = m->levels();
+  if (m->half) {
+    std::vector<__nv_bfloat16*> b(L, nullptr), za(L, nullptr), zb(L, nullptr);
+    for (int l = 1; l < L; ++l) {
+      b[l] = (__nv_bfloat16*)m->b16[l - 1]->p;
+      za[l] = (__nv_bfloat16*)m->z16a[l - 1]->p;
+      zb[l] = (__nv_bfloat16*)m->z16b[l - 1]->p;
+    }
+    return vcycleT<__nv_bfloat16>(m, r0, st, s, launches, b.data(), za.data(), zb.data());
+  } else {
+    std::vector<float*> b(L, nullptr), za(L, nullptr), zb(L, nullptr);
+    for (int l = 1; l < L; ++l) {
+      b[l] = m->b32[l - 1]->p;
+      za[l] = m->z32a[l - 1]->p;
+      zb[l] = m->z32b[l - 1]->p;
+    }
+    return vcycleT<float>(m, r0, st, s, launches, b.data(), za.data(), zb.data());
+  }
+}
+
+void mgSetup(Multigrid* m, const uint8_t* mk0, const Code* code, float sx, float sy, float sz, cudaStream_t s,
+             long long& launches) {
+  mgSetupLevels(m, mk0, code, sx, sy, sz, s, launches);
+}
+
+// Preconditioned CG with the V-cycle: the RHS kernel already set r = b,
+// x = 0 and ||b||^2.  Iterations are launched in chunks; every kernel returns
+// immediately once the state says done.
+void mgRunCg(Multigrid* m, const Dim3i& r, float sx, float sy, float sz, const Code* code, float* x, float* rvec,
+             double* partials, CgState* st, CgState* stHost, cudaStream_t s, long long& launches) {
+  (void)partials;
+  check(cudaMemsetAsync(m->p[0].p, 0, m->p[0].bytes(), s), "memset");
+  const float* z = mgVcycle(m, rvec, st, s, launches);  // z0 = V(b), rz = b.z0
+  int it = 0;
+  const int chunk = 4;
+  for (;;) {
+    for (int k = 0; k < chunk; ++k, ++it) {
+      float* pOld = m->p[it & 1].p;
+      float* pNew = m->p[(it + 1) & 1].p;
+      check(launchCgDirectionZ(r, sx, sy, sz, code, z, pOld, pNew, m->partials.p, st, s), "cg direction");
+      check(launchCgUpdateNoZ(r, sx, sy, sz, code, pNew, x, rvec, m->partials.p, st, s), "cg update");
+      launches += 2;
+      z = mgVcycle(m, rvec, st, s, launches);
+    }
+    check(cudaMemcpyAsync(stHost, st, sizeof(CgState), cudaMemcpyDeviceToHost, s), "read cg state");
+    check(cudaStreamSynchronize(s), "cg sync");
+    if (stHost->done) break;
+  }
 }
 
 }  // namespace hfg

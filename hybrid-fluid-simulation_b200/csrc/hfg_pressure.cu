@@ -53,9 +53,10 @@ __device__ __forceinline__ float diagOf(Code k, float sx, float sy, float sz) {
   return d;
 }
 
+// PC: 0 identity, 1 Jacobi, 2 z supplied by the caller (multigrid)
 template <int PC>
 __device__ __forceinline__ float precondZ(Code k, float rv, float sx, float sy, float sz) {
-  return PC ? __fdiv_rn(rv, diagOf(k, sx, sy, sz)) : rv;
+  return PC == 1 ? __fdiv_rn(rv, diagOf(k, sx, sy, sz)) : rv;
 }
 
 __device__ inline bool cgStop(const CgState* st, double rr) {
@@ -244,6 +245,43 @@ cudaError_t launchRhsInit(const Geom& gm, ConstFaceField v, ConstFaceField svArr
 }
 
 // ---------------------------------------------------------------------------
+// Fast row of A for the CG: the diagonal and its reciprocal come from a
+// 64-entry table per launch (indexed by the six "not solid" bits; the entries
+// are summed in the reference's order), the six off-diagonal terms are FP32
+// FMAs on masked neighbour values.
+struct DiagTab {
+  float d[64], inv[64];
+};
+
+__device__ __forceinline__ void buildDiagTab(DiagTab& t, float sx, float sy, float sz) {
+  const int tid = flatTid();
+  if (tid < 64) {
+    Code k = (Code)(1 | (tid << 1));
+    float d = diagOf(k, sx, sy, sz);
+    t.d[tid] = d;
+    t.inv[tid] = d != 0.f ? 1.0f / d : 0.f;
+  }
+}
+
+__device__ __forceinline__ float fastRow(const DiagTab& t, Code k, float sx, float sy, float sz, float vc, float vl,
+                                         float vr, float vd, float vu, float vb, float vf) {
+  if (!(k & 1)) return vc;
+  float nx = ((k >> 7) & 1 ? vl : 0.f) + ((k >> 8) & 1 ? vr : 0.f);
+  float ny = ((k >> 9) & 1 ? vd : 0.f) + ((k >> 10) & 1 ? vu : 0.f);
+  float nz = ((k >> 11) & 1 ? vb : 0.f) + ((k >> 12) & 1 ? vf : 0.f);
+  float q = t.d[(k >> 1) & 63] * vc;
+  q = fmaf(-sx, nx, q);
+  q = fmaf(-sy, ny, q);
+  q = fmaf(-sz, nz, q);
+  return q;
+}
+
+template <int PC>
+__device__ __forceinline__ float fastZ(const DiagTab& t, Code k, float rv) {
+  if (PC != 1) return rv;
+  return (k & 1) ? rv * t.inv[(k >> 1) & 63] : rv;
+}
+
 // CG direction: p = z + beta p_old (scal then axpy with 1), q = A p and the
 // reduction p.q; the last block forms alpha = r.z / p.Ap
 // (CuMatrixFreePCG.cpp:40-47, :56-60).  p of the current plane (with a one-
@@ -256,6 +294,9 @@ __global__ void __launch_bounds__(TX* TY, 4) kCgDirection(Dim3i R, float sx, flo
                                                           double* partials, CgState* st, int zPer) {
   if (st->done) return;
   __shared__ float tile[2][TY + 2][TX + 2];
+  __shared__ DiagTab tab;
+  buildDiagTab(tab, sx, sy, sz);
+  __syncthreads();
   const float beta = st->beta;
   double pq = 0.0, dummy = 0.0;
   const int tx = threadIdx.x, ty = threadIdx.y;
@@ -264,34 +305,34 @@ __global__ void __launch_bounds__(TX* TY, 4) kCgDirection(Dim3i R, float sx, flo
   const int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, R.z);
   const unsigned plane = (unsigned)R.x * (unsigned)R.y;
   auto pn = [&](unsigned i) -> float {
-    float zz = precondZ<PC>(__ldg(code + i), __ldg(r + i), sx, sy, sz);
-    return __fadd_rn(__fmul_rn(beta, __ldg(pOld + i)), zz);
+    float zz = fastZ<PC>(tab, __ldg(code + i), __ldg(r + i));
+    return fmaf(beta, __ldg(pOld + i), zz);
   };
   unsigned c = (unsigned)z0 * plane + (unsigned)y * (unsigned)R.x + (unsigned)x;
   float below = (in && z0 > 0) ? pn(c - plane) : 0.f;
   float cur = in ? pn(c) : 0.f;
+  float acc = 0.f;
   int buf = 0;
   for (int z = z0; z < z1; ++z, c += plane, buf ^= 1) {
     float above = (in && z + 1 < R.z) ? pn(c + plane) : 0.f;
     Code k = in ? __ldg(code + c) : (Code)0;
-    // halo ring of this plane (zero outside the grid; only read for fluid
-    // neighbours, which are inside by construction)
     float (*t)[TX + 2] = tile[buf];
     t[ty + 1][tx + 1] = cur;
     if (tx == 0) t[ty + 1][0] = (in && x > 0) ? pn(c - 1) : 0.f;
     if (tx == TX - 1 || x == R.x - 1) t[ty + 1][tx + 2] = (in && x + 1 < R.x) ? pn(c + 1) : 0.f;
-    if (ty == 0) t[0][tx + 1] = (x < R.x && y < R.y && y > 0) ? pn(c - R.x) : 0.f;
+    if (ty == 0) t[0][tx + 1] = (in && y > 0) ? pn(c - R.x) : 0.f;
     if (ty == TY - 1 || y == R.y - 1) t[ty + 2][tx + 1] = (in && y + 1 < R.y) ? pn(c + R.x) : 0.f;
     __syncthreads();
     if (in) {
-      float q = applyRow(k, sx, sy, sz, cur, t[ty + 1][tx], t[ty + 1][tx + 2], t[ty][tx + 1], t[ty + 2][tx + 1],
-                         below, above);
+      float q = fastRow(tab, k, sx, sy, sz, cur, t[ty + 1][tx], t[ty + 1][tx + 2], t[ty][tx + 1], t[ty + 2][tx + 1],
+                        below, above);
       pNew[c] = cur;
-      pq += (double)cur * (double)q;
+      acc = fmaf(cur, q, acc);
     }
     below = cur;
     cur = above;
   }
+  pq = (double)acc;
   if (gridSum2(pq, dummy, partials, &st->ticket) && flatTid() == 0) {
     st->pAp = pq;
     st->alpha = (float)(st->rz / pq);
@@ -303,7 +344,8 @@ __global__ void __launch_bounds__(TX* TY, 4) kCgDirection(Dim3i R, float sx, flo
 // through the same shared tile), z = M^-1 r, the reductions r.r and r.z; the
 // last block checks convergence and forms beta (CuMatrixFreePCG.cpp:49-63).
 // The |alpha| < FLT_EPSILON skip of CCuDenseVector::plusAlphaX
-// (CuDenseVector.cpp:178) is kept.
+// (CuDenseVector.cpp:178) is kept.  Per-thread partial sums run over one
+// z-column segment in FP32 and are combined in FP64.
 template <int PC>
 __global__ void __launch_bounds__(TX* TY, 4) kCgUpdate(Dim3i R, float sx, float sy, float sz,
                                                        const Code* __restrict__ code, const float* __restrict__ p,
@@ -311,9 +353,12 @@ __global__ void __launch_bounds__(TX* TY, 4) kCgUpdate(Dim3i R, float sx, float 
                                                        double* partials, CgState* st, int zPer) {
   if (st->done) return;
   __shared__ float tile[2][TY + 2][TX + 2];
+  __shared__ DiagTab tab;
+  buildDiagTab(tab, sx, sy, sz);
+  __syncthreads();
   const float alpha = st->alpha;
   const bool skip = fabsf(alpha) < FLT_EPSILON;
-  double rr = 0.0, rz = 0.0;
+  float arr = 0.f, arz = 0.f;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int x = blockIdx.x * TX + tx, y = blockIdx.y * TY + ty;
   const bool in = x < R.x && y < R.y;
@@ -332,30 +377,33 @@ __global__ void __launch_bounds__(TX* TY, 4) kCgUpdate(Dim3i R, float sx, float 
     t[ty + 1][tx + 1] = cur;
     if (tx == 0) t[ty + 1][0] = (in && x > 0) ? __ldg(p + c - 1) : 0.f;
     if (tx == TX - 1 || x == R.x - 1) t[ty + 1][tx + 2] = (in && x + 1 < R.x) ? __ldg(p + c + 1) : 0.f;
-    if (ty == 0) t[0][tx + 1] = (x < R.x && y < R.y && y > 0) ? __ldg(p + c - R.x) : 0.f;
+    if (ty == 0) t[0][tx + 1] = (in && y > 0) ? __ldg(p + c - R.x) : 0.f;
     if (ty == TY - 1 || y == R.y - 1) t[ty + 2][tx + 1] = (in && y + 1 < R.y) ? __ldg(p + c + R.x) : 0.f;
     __syncthreads();
     if (in) {
       if (!skip) {
-        float q = applyRow(k, sx, sy, sz, cur, t[ty + 1][tx], t[ty + 1][tx + 2], t[ty][tx + 1], t[ty + 2][tx + 1],
-                           below, above);
+        float q = fastRow(tab, k, sx, sy, sz, cur, t[ty + 1][tx], t[ty + 1][tx + 2], t[ty][tx + 1], t[ty + 2][tx + 1],
+                          below, above);
         xv[c] = fmaf(alpha, cur, xo);
         rv = fmaf(-alpha, q, rv);
         r[c] = rv;
       }
-      float zz = precondZ<PC>(k, rv, sx, sy, sz);
-      rr += (double)rv * (double)rv;
-      rz += (double)rv * (double)zz;
+      float zz = fastZ<PC>(tab, k, rv);
+      arr = fmaf(rv, rv, arr);
+      arz = fmaf(rv, zz, arz);
     }
     below = cur;
     cur = above;
   }
+  double rr = (double)arr, rz = (double)arz;
   if (gridSum2(rr, rz, partials, &st->ticket) && flatTid() == 0) {
     st->rr = rr;
     st->iter += 1;
     bool stop = cgStop(st, rr);
-    st->beta = (float)(rz / st->rz);
-    st->rz = rz;
+    if (PC != 2) {  // with multigrid the V-cycle's last sweep forms r.z and beta
+      st->beta = (float)(rz / st->rz);
+      st->rz = rz;
+    }
     st->done = stop || st->iter >= st->maxIter;
     st->ticket = 0;
   }
@@ -378,6 +426,20 @@ cudaError_t launchCgUpdate(const Dim3i& r, float sx, float sy, float sz, const C
     kCgUpdate<1><<<g.grid, g.block, 0, s>>>(r, sx, sy, sz, code, p, x, rr, partials, st, g.zPer);
   else
     kCgUpdate<0><<<g.grid, g.block, 0, s>>>(r, sx, sy, sz, code, p, x, rr, partials, st, g.zPer);
+  return cudaGetLastError();
+}
+
+// Multigrid flavour: z is read from memory (the V-cycle's output).
+cudaError_t launchCgDirectionZ(const Dim3i& r, float sx, float sy, float sz, const Code* code, const float* z,
+                               const float* pOld, float* pNew, double* partials, CgState* st, cudaStream_t s) {
+  CgGrid g = cgGrid(r);
+  kCgDirection<2><<<g.grid, g.block, 0, s>>>(r, sx, sy, sz, code, z, pOld, pNew, partials, st, g.zPer);
+  return cudaGetLastError();
+}
+cudaError_t launchCgUpdateNoZ(const Dim3i& r, float sx, float sy, float sz, const Code* code, const float* p,
+                              float* x, float* rr, double* partials, CgState* st, cudaStream_t s) {
+  CgGrid g = cgGrid(r);
+  kCgUpdate<2><<<g.grid, g.block, 0, s>>>(r, sx, sy, sz, code, p, x, rr, partials, st, g.zPer);
   return cudaGetLastError();
 }
 

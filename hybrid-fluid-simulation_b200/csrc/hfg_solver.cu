@@ -23,7 +23,8 @@ constexpr int kSubstepChunk = 4;   // CFL substeps launched between completion r
 // Multigrid preconditioner hooks (hfg_mg.cu).
 Multigrid* mgCreate(const Dim3i& r, int levels, int smooth, bool half);
 void mgDestroy(Multigrid* m);
-void mgSetup(Multigrid* m, const Code* code, float sx, float sy, float sz, cudaStream_t s, long long& launches);
+void mgSetup(Multigrid* m, const uint8_t* mk0, const Code* code, float sx, float sy, float sz, cudaStream_t s,
+             long long& launches);
 void mgRunCg(Multigrid* m, const Dim3i& r, float sx, float sy, float sz, const Code* code, float* x, float* rvec,
              double* partials, CgState* st, CgState* stHost, cudaStream_t s, long long& launches);
 
@@ -404,7 +405,7 @@ void GridSolver::computePressure() {
   launched(launchRhsInit(g_, cvel(ni), none, solidTable(), markers_.p, code_.p, sx, sy, sz, nullptr, cgr_.p, cgx_.p,
                          cgp_[0].p, partials_.p, cgState_.p, init.precond, stream_),
            "rhs");
-  if (opt_.precond == HFG_PRECOND_MG) mgSetup(mg_, code_.p, sx, sy, sz, stream_, launches_);
+  if (opt_.precond == HFG_PRECOND_MG) mgSetup(mg_, markers_.p, code_.p, sx, sy, sz, stream_, launches_);
   stageEnd(4);
   stageBegin(5);
   runCg();
