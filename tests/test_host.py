@@ -1,0 +1,135 @@
+"""Host-side logic on the CPU: the C ABI surface, error reporting without a
+GPU, scene construction, and the multi-rank plumbing (gloo, world size 2)."""
+import ctypes
+import os
+import re
+import socket
+
+import numpy as np
+import pytest
+
+import dist_util
+import hfgrid
+import scenes
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = []
+    for h in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if not h.endswith(".h"):
+            continue
+        src = open(os.path.join(ROOT, "include", h)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names += re.findall(r"(?:HFG_API|MPHYSICS_API)\s+[\w\s\*]+?\b(\w+)\s*\(", src)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(hfgrid.LIB_PATH)
+    names = declared_symbols()
+    assert len(names) >= 50
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_binding_covers_the_c_api():
+    """hfgrid.lib() binds a signature for every solver/operator entry point."""
+    lib = hfgrid.lib()
+    for n in declared_symbols():
+        if n.startswith("hfg_"):
+            assert getattr(lib, n).argtypes is not None, n
+
+
+def test_errors_cross_the_abi_as_status_codes():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("needs a host without a CUDA device")
+    lib = hfgrid.lib()
+    assert lib.hfg_init(0) != 0
+    assert "CUDA" in lib.hfg_last_error().decode() or "device" in lib.hfg_last_error().decode()
+    h = ctypes.c_void_p()
+    rc = lib.hfg_solver_create(ctypes.c_float(0.1), hfgrid._i3((4, 4, 4)), hfgrid._f3((0, 0, 0)),
+                               hfgrid._f3((1, 1, 1)), ctypes.byref(h))
+    assert rc < 0 and not h.value
+    # invalid arguments are rejected before any CUDA call
+    rc = lib.hfg_solver_create(ctypes.c_float(0.1), hfgrid._i3((0, 4, 4)), hfgrid._f3((0, 0, 0)),
+                               hfgrid._f3((1, 1, 1)), ctypes.byref(h))
+    assert rc == -1
+    assert lib.hfg_solver_update(None) == -1
+    assert lib.hfg_op_project(hfgrid._i3((4, 4, 4)), hfgrid._f3((1, 1, 1)), 0.1, None, None, None, None, None, None,
+                              None, 0, 0, 1e-3, -1, None, None, None) == -1
+
+
+def test_default_options_match_the_reference():
+    o = hfgrid.default_options()
+    assert o.precond == hfgrid.PRECOND_IDENTITY and o.tol_mode == hfgrid.TOL_REFERENCE
+    assert o.tol == pytest.approx(1e-3) and o.max_iter == -1      # CuMatrixFreePCG.h:28, PressureSolver.cpp:151
+    assert o.extrapolation_layers == 1000                           # GridFluidSolver.cpp:176
+    assert o.clamp_mode == 1
+
+
+def test_scene_sdfs():
+    sc = scenes.dam_break_64()
+    walls = scenes.sdf_walls(sc.res, sc.spacing)
+    # the outermost cell layer is wall, everything inside is not
+    assert (walls[0] < 0).all() and (walls[-1] < 0).all() and (walls[:, 0] < 0).all() and (walls[:, :, -1] < 0).all()
+    assert (walls[1:-1, 1:-1, 1:-1] > 0).all()
+    sph = scenes.solid_sdf(sc, sc.solids[0])
+    assert sph.min() < 0 < sph.max()
+    tot = scenes.total_solid(sc)
+    assert set(np.unique(tot)) <= {-1.0, -2.0, np.finfo(np.float32).max}
+    big = scenes.dam_break_256(n=32)
+    b = scenes.boundaries(big)
+    assert len(b) == 3 and all(s.dtype == np.float32 for s, _ in b)
+
+
+def test_scene_assignment_respects_budget():
+    fp = [100, 80, 60, 50, 40, 30, 20, 10, 500]
+    placed, rejected = dist_util.assign_scenes(fp, 2, 200)
+    assert rejected == [8]
+    loads = [sum(fp[i] for i in p) for p in placed]
+    assert all(l <= 200 for l in loads)
+    assert sorted(i for p in placed for i in p) == list(range(8))
+    assert dist_util.scene_bytes((256, 256, 256), 31_400_496) < 180e9
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _rank_main(rank, world, port, out):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        m = dist_util.max_over_ranks(10.0 + rank)
+        fp = [dist_util.scene_bytes((32 + 8 * i, 40, 48), 1000 * i) for i in range(7)]
+        placed, rejected = dist_util.assign_scenes(fp, world, 10**9)
+        same = dist_util.agree([i for p in placed for i in p] + [-1] + rejected)
+        out.put((rank, m, placed[rank], same))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_gloo():
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert res[0][1] == res[1][1] == 11.0          # max over ranks
+    assert res[0][3] and res[1][3]                 # identical assignment on both ranks
+    assert sorted(res[0][2] + res[1][2]) == list(range(7))
