@@ -308,6 +308,14 @@ HFG_API int hfg_solver_get_solid_vel_field(hfg_solver_t s, float* x, float* y, f
     return HFG_OK;
   });
 }
+HFG_API int hfg_solver_get_fluid_sdf(hfg_solver_t s, float* sdf) {
+  return guarded([&]() -> int {
+    SOLVER(s);
+    NEED(sdf, "null output");
+    S.getFluidSDF(sdf);
+    return HFG_OK;
+  });
+}
 HFG_API long long hfg_solver_num_particles(hfg_solver_t s) { return (s && s->s) ? s->s->numParticles() : -1; }
 HFG_API int hfg_solver_get_particles(hfg_solver_t s, float* pos, float* vel) {
   return guarded([&]() -> int {
@@ -686,6 +694,21 @@ HFG_API int hfg_op_sl_advect_cc(const int res[3], const float origin[3], const f
     check(launchSLCell(toGeom(res, origin, spacing), accuracy, dt, ConstFaceField{{vx, vy, vz}}, i1, o1, 1,
                        st(stream)),
           "sl");
+    return HFG_OK;
+  });
+}
+HFG_API int hfg_op_build_fluid_sdf(const int res[3], const float* domain, float* sdf, int layers, void* stream) {
+  return guarded([&]() -> int {
+    NEED(validRes(res) && domain && sdf && layers >= 1 && layers <= 100000, "invalid arguments");
+    Dim3i r = toRes(res);
+    cudaStream_t s = st(stream);
+    Scratch<unsigned int> fa(r.size(), s), fb(r.size(), s), cnt(2, s);
+    unsigned int* host = nullptr;
+    check(cudaMallocHost((void**)&host, sizeof(unsigned int)), "cudaMallocHost");
+    cudaError_t e = launchFluidSdf(r, domain, sdf, layers, fa.p, fb.p, cnt.p, host, s);
+    cudaFreeHost(host);
+    check(e, "fluid sdf");
+    check(cudaStreamSynchronize(s), "sync");
     return HFG_OK;
   });
 }

@@ -458,6 +458,82 @@ cudaError_t launchExtrapLayer(const Dim3i rc[3], float* const vals[3], const lon
 }
 
 // ===========================================================================
+// Fluid SDF of the fluid-domain field (buildFluidSDF, EulerSolverTool.cu:324-406,
+// :760-785; GridFluidSolver.cpp:571-591).  Layer 0 marks the cells on both
+// sides of the fluid surface (0.5 - 0.2 inside, 1.5 - 0.2 outside, +/-UNKNOWN
+// elsewhere); layer d then takes every still-UNKNOWN neighbour of a layer d-1
+// cell of the same side.  The reference sweeps the whole grid 1000 times;
+// here each layer visits only the previous layer's cells (frontier lists).
+// ===========================================================================
+namespace {
+constexpr double kSurf = 0.2;  // FluidSurfaceDensity (Common.h:244)
+__device__ __forceinline__ float outsideValue(int d) { return (float)((double)d + (1.5 - kSurf)); }
+__device__ __forceinline__ float insideValue(int d) { return d == 0 ? (float)(0.5 - kSurf) : (float)(-((double)d - (0.5 - kSurf))); }
+}  // namespace
+
+__global__ void kFluidSdfInit(Dim3i r, const float* __restrict__ dom, float* __restrict__ sdf,
+                              unsigned int* __restrict__ front, unsigned int* __restrict__ count) {
+  HFG_FOR(c, r.size()) {
+    int x, y, z;
+    cellCoord(c, r, x, y, z);
+    bool in = dom[c] < 0.f;
+    bool mixed = false;
+    const int dx[6] = {-1, 1, 0, 0, 0, 0}, dy[6] = {0, 0, -1, 1, 0, 0}, dz[6] = {0, 0, 0, 0, -1, 1};
+#pragma unroll
+    for (int k = 0; k < 6; ++k) mixed |= ((dom[linc(x + dx[k], y + dy[k], z + dz[k], r)] < 0.f) != in);
+    float v = in ? (mixed ? insideValue(0) : -kUnknown) : (mixed ? outsideValue(0) : kUnknown);
+    sdf[c] = v;
+    if (mixed) front[atomicAdd(count, 1u)] = (unsigned int)c;
+  }
+}
+
+__global__ void kFluidSdfLayer(Dim3i r, float* __restrict__ sdf, const unsigned int* __restrict__ front,
+                               unsigned int n, unsigned int* __restrict__ next, unsigned int* __restrict__ count, int d) {
+  HFG_FOR(i, (long long)n) {
+    long long c = front[i];
+    int x, y, z;
+    cellCoord(c, r, x, y, z);
+    bool inside = sdf[c] < 1.0f;  // inner values are <= 0.3, outer >= 1.3
+    float sentinel = inside ? -kUnknown : kUnknown;
+    float v = inside ? insideValue(d) : outsideValue(d);
+    const int dx[6] = {-1, 1, 0, 0, 0, 0}, dy[6] = {0, 0, -1, 1, 0, 0}, dz[6] = {0, 0, 0, 0, -1, 1};
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      long long nb = linc(x + dx[k], y + dy[k], z + dz[k], r);
+      int old = atomicCAS((int*)(sdf + nb), __float_as_int(sentinel), __float_as_int(v));
+      if (old == __float_as_int(sentinel)) next[atomicAdd(count, 1u)] = (unsigned int)nb;
+    }
+  }
+}
+
+cudaError_t launchFluidSdf(const Dim3i& r, const float* dom, float* sdf, int layers, unsigned int* frontA,
+                           unsigned int* frontB, unsigned int* counts, unsigned int* hostCount, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(counts, 0, sizeof(unsigned int) * 2, s);
+  if (e != cudaSuccess) return e;
+  kFluidSdfInit<<<gridFor(r.size()), kThreads, 0, s>>>(r, dom, sdf, frontA, counts);
+  unsigned int* cur = frontA;
+  unsigned int* nxt = frontB;
+  int slot = 0;
+  for (int d = 1; d < layers; ++d) {
+    e = cudaMemcpyAsync(hostCount, counts + slot, sizeof(unsigned int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return e;
+    unsigned int n = *hostCount;
+    if (n == 0) break;
+    e = cudaMemsetAsync(counts + (slot ^ 1), 0, sizeof(unsigned int), s);
+    if (e != cudaSuccess) return e;
+    kFluidSdfLayer<<<gridFor(n), kThreads, 0, s>>>(r, sdf, cur, n, nxt, counts + (slot ^ 1), d);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    unsigned int* t = cur;
+    cur = nxt;
+    nxt = t;
+    slot ^= 1;
+  }
+  return cudaGetLastError();
+}
+
+// ===========================================================================
 // Particles
 // ===========================================================================
 

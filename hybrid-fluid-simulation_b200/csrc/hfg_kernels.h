@@ -119,6 +119,11 @@ cudaError_t launchExtrapDistance(const Dim3i rc[3], float* const vals[3], long l
 cudaError_t launchExtrapLayer(const Dim3i rc[3], float* const vals[3], const long long off[3], ExtrapScratch sc,
                               unsigned int begin, unsigned int count, int d, cudaStream_t s);
 
+// ---- fluid SDF (buildFluidSDF); frontier buffers hold N cells each; counts 2;
+// hostCount pinned.  Blocks (one host read per layer).
+cudaError_t launchFluidSdf(const Dim3i& r, const float* dom, float* sdf, int layers, unsigned int* frontA,
+                           unsigned int* frontB, unsigned int* counts, unsigned int* hostCount, cudaStream_t s);
+
 // ---- particles -------------------------------------------------------------
 enum ParticleMode : int { MODE_PIC = 0, MODE_FLIP = 1, MODE_MIX = 2 };
 cudaError_t launchSeedCount(const Dim3i& r, const float* fluidSDF, const uint8_t* solidIdx, unsigned int* blockCounts,

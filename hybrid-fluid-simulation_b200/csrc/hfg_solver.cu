@@ -553,6 +553,20 @@ void GridSolver::getSolidVel(float* x, float* y, float* z) {
   synchronize();
 }
 
+// GridFluidSolver.cpp:571-591 generateCurFluidSDF on the current domain field
+void GridSolver::getFluidSDF(float* out) {
+  DArray<float> sdf;
+  DArray<unsigned int> fa, fb, cnt;
+  sdf.alloc(N_); fa.alloc(N_); fb.alloc(N_); cnt.alloc(2);
+  unsigned int* host = nullptr;
+  check(cudaMallocHost((void**)&host, sizeof(unsigned int)), "cudaMallocHost");
+  cudaError_t e = launchFluidSdf(g_.r, dom_[cur()].p, sdf.p, opt_.extrapolation_layers, fa.p, fb.p, cnt.p, host, stream_);
+  cudaFreeHost(host);
+  check(e, "fluid sdf");
+  check(cudaMemcpyAsync(out, sdf.p, N_ * 4, cudaMemcpyDeviceToHost, stream_), "download");
+  synchronize();
+}
+
 void GridSolver::getParticles(float* pos, float* vel) {
   if (P_ > 0) {
     if (pos) check(cudaMemcpyAsync(pos, ppos_.p, 12 * P_, cudaMemcpyDeviceToHost, stream_), "download");

@@ -98,6 +98,7 @@ def _signatures(lib):
         "hfg_solver_get_pressure": (C.c_int, [S, PF]),
         "hfg_solver_get_solid_sdf": (C.c_int, [S, PF]),
         "hfg_solver_get_solid_vel_field": (C.c_int, [S, PF, PF, PF]),
+        "hfg_solver_get_fluid_sdf": (C.c_int, [S, PF]),
         "hfg_solver_num_particles": (C.c_longlong, [S]),
         "hfg_solver_get_particles": (C.c_int, [S, PF, PF]),
         "hfg_solver_get_stats": (C.c_int, [S, C.POINTER(Stats)]),
@@ -127,6 +128,7 @@ def _signatures(lib):
         "hfg_op_sl_advect_fc": (C.c_int, [I3, F3, F3, VP, VP, VP, VP, VP, VP, C.c_float, C.c_int, VP, VP, VP, VP]),
         "hfg_op_sl_advect_cc": (C.c_int, [I3, F3, F3, VP, VP, VP, VP, C.c_float, C.c_int, VP, VP]),
         "hfg_op_fluid_domain_from_bbox": (C.c_int, [I3, F3, F3, F3, F3, VP, VP]),
+        "hfg_op_build_fluid_sdf": (C.c_int, [I3, VP, VP, C.c_int, VP]),
         "hfg_op_seed_particles": (C.c_int, [I3, F3, F3, VP, VP, C.c_int, C.c_ulonglong, VP, C.c_longlong,
                                             C.POINTER(C.c_longlong), VP]),
     }
@@ -191,10 +193,25 @@ class Solver:
         h = C.c_void_p()
         _check(lib().hfg_solver_create(C.c_float(dt), _i3(self.res), _f3(origin), _f3(spacing), C.byref(h)))
         self._h = h
+        self._owned = True
+
+    @classmethod
+    def attach(cls, handle: int, dt: float, res, origin, spacing) -> "Solver":
+        """Wrap a solver owned elsewhere (e.g. one a loaded MPhysics scene
+        holds, from mphysics_grid_solver); closing the wrapper leaves it alive."""
+        self = cls.__new__(cls)
+        self.res = tuple(int(r) for r in res)
+        self.origin = tuple(float(o) for o in origin)
+        self.spacing = tuple(float(h) for h in spacing)
+        self.dt = float(dt)
+        self._h = C.c_void_p(handle)
+        self._owned = False
+        return self
 
     def close(self):
         if getattr(self, "_h", None):
-            lib().hfg_solver_destroy(self._h)
+            if self._owned:
+                lib().hfg_solver_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -310,6 +327,11 @@ class Solver:
     def solid_vel_field(self):
         out = [np.empty(s, np.float32) for s in face_shapes(self.res)]
         _check(lib().hfg_solver_get_solid_vel_field(self._h, *[_fptr(o) for o in out]))
+        return out
+
+    def fluid_sdf(self):
+        out = np.empty(self.res[::-1], np.float32)
+        _check(lib().hfg_solver_get_fluid_sdf(self._h, _fptr(out)))
         return out
 
     @property
@@ -457,6 +479,10 @@ def op_sl_advect_cc(res, origin, spacing, field, vel, dt, accuracy, out, stream=
 def op_fluid_domain_from_bbox(res, origin, spacing, mn, mx, out, stream=None):
     _check(lib().hfg_op_fluid_domain_from_bbox(_i3(res), _f3(origin), _f3(spacing), _f3(mn), _f3(mx), _ptr(out),
                                                _stream(stream)))
+
+
+def op_build_fluid_sdf(res, domain, sdf, layers=1000, stream=None):
+    _check(lib().hfg_op_build_fluid_sdf(_i3(res), _ptr(domain), _ptr(sdf), layers, _stream(stream)))
 
 
 def op_seed_particles(res, origin, spacing, fluid_sdf, solid_sdf, per_cell, seed, pos=None, capacity=0, stream=None):

@@ -135,6 +135,9 @@ HFG_API int hfg_solver_get_pressure(hfg_solver_t s, float* p);
 /* getSolidSDFField (the total solid marker field)  GridFluidSolver.cpp:292-295 */
 HFG_API int hfg_solver_get_solid_sdf(hfg_solver_t s, float* sdf);
 HFG_API int hfg_solver_get_solid_vel_field(hfg_solver_t s, float* x, float* y, float* z);
+/* generateCurFluidSDF + getFluidSDFField: the layered fluid SDF of the current
+ * fluid-domain field (GridFluidSolver.cpp:571-591, EulerSolverTool.cu:324-406) */
+HFG_API int hfg_solver_get_fluid_sdf(hfg_solver_t s, float* sdf);
 HFG_API long long hfg_solver_num_particles(hfg_solver_t s);
 HFG_API int hfg_solver_get_particles(hfg_solver_t s, float* pos, float* vel);
 HFG_API int hfg_solver_get_stats(hfg_solver_t s, hfg_stats_t* st);
@@ -214,6 +217,9 @@ HFG_API int hfg_op_sl_advect_fc(const int res[3], const float origin[3], const f
 HFG_API int hfg_op_sl_advect_cc(const int res[3], const float origin[3], const float spacing[3], const float* in,
                                 const float* vx, const float* vy, const float* vz, float dt, int accuracy, float* out,
                                 void* stream);
+/* buildFluidSDFInvoker  EulerSolverTool.cu:760-785 (layers = the reference's
+ * vExtrapolationDistance; blocks) */
+HFG_API int hfg_op_build_fluid_sdf(const int res[3], const float* domain, float* sdf, int layers, void* stream);
 /* generateFluidDomainFromBBoxInvoker  EulerSolverTool.cu:989-1013 */
 HFG_API int hfg_op_fluid_domain_from_bbox(const int res[3], const float origin[3], const float spacing[3],
                                           const float mn[3], const float mx[3], float* out, void* stream);

@@ -975,6 +975,47 @@ long long orc_seed_particles(const int* res, const float* o, const float* h, con
   return n;
 }
 
+// EulerSolverTool.cu:324-406 buildFluidSDF, driven as buildFluidSDFInvoker
+// (:760-785): `layers` full-grid sweeps; layer d only reads values written by
+// layer d-1 (the reference's in-launch reads see either the old or the new
+// value of a cell, and a new value never equals the tested one).
+void orc_build_fluid_sdf(const int* res, const float* dom, int layers, float* sdf) {
+  Res r{res[0], res[1], res[2]};
+  const double FS = 0.2;  // FluidSurfaceDensity (Common.h:244)
+  const float U = FLT_MAX;
+  i64 N = r.size();
+  auto inside = [&](i64 c) { return dom[c] < 0; };
+  const int dx[6] = {-1, 1, 0, 0, 0, 0}, dy[6] = {0, 0, -1, 1, 0, 0}, dz[6] = {0, 0, 0, 0, -1, 1};
+  for (int z = 0; z < r.z; ++z)
+    for (int y = 0; y < r.y; ++y)
+      for (int x = 0; x < r.x; ++x) {
+        i64 c = lin(x, y, z, r);
+        bool in = inside(c), mixed = false;
+        for (int k = 0; k < 6; ++k) mixed |= inside(lin(x + dx[k], y + dy[k], z + dz[k], r)) != in;
+        sdf[c] = in ? (mixed ? (float)(0.5 - FS) : -U) : (mixed ? (float)(1.5 - FS) : U);
+      }
+  std::vector<float> prev(N);
+  for (int d = 1; d < layers; ++d) {
+    std::memcpy(prev.data(), sdf, N * sizeof(float));
+    float outT = (float)((double)d + (1.5 - FS) - 1), inT = (float)(-((double)d + FS - 1.5));
+    float outV = (float)((double)d + (1.5 - FS)), inV = (float)(-((double)d - (0.5 - FS)));
+    bool any = false;
+    for (int z = 0; z < r.z; ++z)
+      for (int y = 0; y < r.y; ++y)
+        for (int x = 0; x < r.x; ++x) {
+          i64 c = lin(x, y, z, r);
+          if (prev[c] == U) {
+            for (int k = 0; k < 6; ++k)
+              if (std::fabs(prev[lin(x + dx[k], y + dy[k], z + dz[k], r)] - outT) < FLT_MIN) { sdf[c] = outV; any = true; break; }
+          } else if (prev[c] == -U) {
+            for (int k = 0; k < 6; ++k)
+              if (std::fabs(prev[lin(x + dx[k], y + dy[k], z + dz[k], r)] - inT) < FLT_MIN) { sdf[c] = inV; any = true; break; }
+          }
+        }
+    if (!any) break;
+  }
+}
+
 // EulerSolverTool.cu:581-608 generateFluidDomainFromBBox (strict inequalities)
 void orc_fluid_domain_from_bbox(const int* res, const float* o, const float* h, const float* mn, const float* mx,
                                 float* out) {

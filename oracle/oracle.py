@@ -43,6 +43,7 @@ def lib():
             "orc_philox": (None, [PU32, C.c_uint32, C.c_uint32, PU32]),
             "orc_seed_particles": (C.c_longlong, [I3, F3, F3, PF, PF, C.c_int, C.c_ulonglong, PF]),
             "orc_fluid_domain_from_bbox": (None, [I3, F3, F3, F3, F3, PF]),
+            "orc_build_fluid_sdf": (None, [I3, PF, C.c_int, PF]),
             "orc_markers_from_particles": (None, [I3, F3, F3, PF, PF, C.c_longlong, PU8, PU32]),
             "orc_markers_from_sdf": (None, [I3, PF, PF, PU8]),
             "orc_build_matrix_a": (None, [C.c_int, I3, F3, C.c_float, PU8, PF]),
@@ -140,6 +141,12 @@ def philox(ctr, key):
 def fluid_domain_from_bbox(res, origin, spacing, mn, mx):
     out = np.empty(res[::-1], np.float32)
     lib().orc_fluid_domain_from_bbox(i3(res), f3(origin), f3(spacing), f3(mn), f3(mx), fp(out))
+    return out
+
+
+def build_fluid_sdf(res, domain, layers=1000):
+    out = np.empty(res[::-1], np.float32)
+    lib().orc_build_fluid_sdf(i3(res), fp(f32(domain).reshape(-1)), layers, fp(out))
     return out
 
 

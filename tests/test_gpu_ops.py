@@ -280,3 +280,16 @@ def test_fluid_domain_and_seeding_bit_exact(cuda):
     pref = oracle.seed_particles(res, o, h, dom, solid, 8, 1234)
     assert pref.shape[0] == n
     assert np.array_equal(host(pos), pref)
+
+
+def test_fluid_sdf_bit_exact(cuda):
+    """generateCurFluidSDF / buildFluidSDF (EulerSolverTool.cu:324-406): the
+    frontier BFS gives the reference's layered values exactly."""
+    rng = np.random.default_rng(60)
+    res = (23, 17, 13)
+    dom = np.where(rng.random(res[::-1]) < 0.3, -500.0, 500.0).astype(np.float32)
+    dom[:, :8, :10] = -500.0
+    for layers in (1000, 4):
+        out = torch.empty(res[::-1], dtype=torch.float32, device=cuda)
+        hfgrid.op_build_fluid_sdf(res, dev(dom), out, layers)
+        assert np.array_equal(host(out), oracle.build_fluid_sdf(res, dom, layers))
