@@ -313,6 +313,7 @@ template <class F> void guard(F&& f) {
 
 }  // namespace
 
+namespace MPhysicsAPI {
 extern "C" {
 
 MPHYSICS_API const char* mphysics_last_error(void) { return g_err.c_str(); }
@@ -465,3 +466,4 @@ MPHYSICS_API void copyCellDataToCPU(const char*, unsigned int*, unsigned int*) {
 }
 
 }  // extern "C"
+}  // namespace MPhysicsAPI

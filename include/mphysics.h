@@ -16,6 +16,10 @@
  * instances) is outside this library: those entry points exist so the symbol
  * set matches, report zero sizes and record "not supported".
  *
+ * In C++ the functions are declared in namespace MPhysicsAPI, as in the
+ * reference, so `MPhysicsAPI::update(dt)` compiles unchanged; their C
+ * linkage makes the symbol names the plain function names.
+ *
  * The reference returns nothing and prints on failure; these functions keep
  * the void signatures and record the failure for mphysics_last_error().
  * Calls are serialised by an internal mutex (the reference is single
@@ -26,6 +30,7 @@
 #define MPHYSICS_H
 
 #ifdef __cplusplus
+namespace MPhysicsAPI {
 extern "C" {
 #define MPHYSICS_REF(T) T&
 #else
@@ -84,6 +89,7 @@ MPHYSICS_API const char* mphysics_last_error(void);
 MPHYSICS_API void* mphysics_grid_solver(const char* vSimulatorName);
 
 #ifdef __cplusplus
-}
+}  /* extern "C" */
+}  /* namespace MPhysicsAPI */
 #endif
 #endif /* MPHYSICS_H */

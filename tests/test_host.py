@@ -133,3 +133,39 @@ def test_two_ranks_gloo():
     assert res[0][1] == res[1][1] == 11.0          # max over ranks
     assert res[0][3] and res[1][3]                 # identical assignment on both ranks
     assert sorted(res[0][2] + res[1][2]) == list(range(7))
+
+
+HOST_SRC = r"""
+#include "mphysics.h"
+#include "hfgrid.h"
+#include <stdio.h>
+int main(void) {
+  hfg_options_t o;
+  hfg_default_options(&o);
+  %(ns)sloadScene("{ \"HybridSimulator\": 3 }");
+  printf("%%s|%%d|%%u\n", %(ns)smphysics_last_error(), o.precond, %(ns)sgetParticleSize("none"));
+  return 0;
+}
+"""
+
+
+@pytest.mark.parametrize("cc,ns,ext", [("gcc", "", "c"), ("g++", "MPhysicsAPI::", "cpp")])
+def test_headers_compile_and_link_from_c_and_cpp(tmp_path, cc, ns, ext):
+    """A host written in C or C++ compiles against include/*.h and links
+    libhfgrid.so; the reference's call form MPhysicsAPI::f() works in C++."""
+    import shutil
+    import subprocess
+    if shutil.which(cc) is None:
+        pytest.skip(f"{cc} not installed")
+    src = tmp_path / f"host.{ext}"
+    src.write_text(HOST_SRC % {"ns": ns})
+    exe = tmp_path / "host"
+    libdir = os.path.dirname(hfgrid.LIB_PATH)
+    subprocess.run([cc, str(src), "-I", os.path.join(ROOT, "include"), "-L", libdir, "-lhfgrid",
+                    f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True)
+    env = dict(os.environ)
+    import torch  # libcudart.so ships with torch's CUDA wheels; make it findable
+    cudart = os.path.join(os.path.dirname(os.path.dirname(torch.__file__)), "nvidia", "cuda_runtime", "lib")
+    env["LD_LIBRARY_PATH"] = cudart + os.pathsep + env.get("LD_LIBRARY_PATH", "")
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True, env=env).stdout.strip()
+    assert out == "scene has no HybridSimulator array|0|0"
