@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 
 #include "hfg_solver.h"
@@ -747,6 +748,76 @@ HFG_API int hfg_op_seed_particles(const int res[3], const float origin[3], const
       check(launchSeedWrite(g, fluid_sdf, idx.p, counts.p, cpb, per_cell, seed, pos, s), "seed");
       check(cudaStreamSynchronize(s), "sync");
     }
+    return HFG_OK;
+  });
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// P2G onto the face grids with no device allocation (hfg_op_p2g_fc_static).
+//
+// hfg_op_p2g_fc takes its accumulators from the stream-ordered allocator on
+// every call.  Some callers may not allocate at call time: a host that runs
+// the transfer inside a fixed-memory real-time loop, or one whose own
+// allocator reserves the whole device and forbids other allocations.  For
+// them the accumulators live in one array that is part of the library image,
+// sized at build time.
+namespace {
+
+// Total faces (x + y + z face grids together) one call may cover: 2^20 float2
+// accumulators, 8 MiB of device memory (a 64 x 64 x 64 grid has 798,720 faces).
+constexpr long long kStaticP2GFaces = 1LL << 20;
+static __device__ __align__(256) float2 g_p2gStaticAcc[kStaticP2GFaces];
+
+constexpr int kMaxStaticDevices = 64;
+std::mutex g_p2gStaticMu;
+float2* g_p2gStaticPtr[kMaxStaticDevices] = {};
+
+// Address of the array on the current device, resolved once per device.
+float2* staticP2GAccumulators() {
+  int dev = 0;
+  check(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev < 0 || dev >= kMaxStaticDevices) throw CudaError("device index beyond the static table", HFG_ERR_UNSUPPORTED);
+  std::lock_guard<std::mutex> lk(g_p2gStaticMu);
+  if (!g_p2gStaticPtr[dev]) {
+    float2* p = nullptr;
+    check(cudaGetSymbolAddress((void**)&p, g_p2gStaticAcc), "cudaGetSymbolAddress");
+    g_p2gStaticPtr[dev] = p;
+  }
+  return g_p2gStaticPtr[dev];
+}
+
+}  // namespace
+
+extern "C" {
+
+HFG_API int hfg_op_p2g_fc_static(const int res[3], const float origin[3], const float spacing[3], const float* pos,
+                                 const float* vel, long long n, int alg, float* vx, float* vy, float* vz, float* wx,
+                                 float* wy, float* wz, void* stream) {
+  return guarded([&]() -> int {
+    NEED(validRes(res) && vx && vy && vz && n >= 0 && (n == 0 || (pos && vel)) && alg >= 0 && alg <= 4,
+         "invalid arguments");
+    long long F[3] = {(long long)(res[0] + 1) * res[1] * res[2], (long long)res[0] * (res[1] + 1) * res[2],
+                      (long long)res[0] * res[1] * (res[2] + 1)};
+    if (F[0] + F[1] + F[2] > kStaticP2GFaces)
+      return fail(HFG_ERR_INVALID, "hfg_op_p2g_fc_static: grid has " + std::to_string(F[0] + F[1] + F[2]) +
+                                       " faces, above the fixed limit of " + std::to_string(kStaticP2GFaces) +
+                                       " (use hfg_op_p2g_fc for larger grids)");
+    Geom g = toGeom(res, origin, spacing);
+    cudaStream_t s = st(stream);
+    float2* base = staticP2GAccumulators();
+    float2* acc[3] = {base, base + F[0], base + F[0] + F[1]};
+    // the scatter accumulates with atomics: every call zeroes the part it uses
+    check(cudaMemsetAsync(base, 0, sizeof(float2) * (F[0] + F[1] + F[2]), s), "memset");
+    check(launchP2GFace(g, alg, pos, vel, n, acc, s), "p2g");
+    float* out[3] = {vx, vy, vz};
+    float* w[3] = {wx, wy, wz};
+    for (int a = 0; a < 3; ++a) {
+      check(launchNormalize(F[a], acc[a], out[a], nullptr, 0.f, 0, 0.f, 0, s), "normalize");
+      if (w[a]) check(cudaMemcpy2DAsync(w[a], 4, (const char*)acc[a] + 4, 8, 4, F[a], cudaMemcpyDeviceToDevice, s), "w");
+    }
+    check(cudaStreamSynchronize(s), "sync");
     return HFG_OK;
   });
 }

@@ -122,6 +122,7 @@ def _signatures(lib):
         "hfg_op_g2p_fc": (C.c_int, [I3, F3, F3, VP, VP, VP, VP, C.c_longlong, C.c_int, VP, VP]),
         "hfg_op_g2p_cc": (C.c_int, [I3, F3, F3, VP, VP, C.c_longlong, C.c_int, VP, VP]),
         "hfg_op_p2g_fc": (C.c_int, [I3, F3, F3, VP, VP, C.c_longlong, C.c_int, VP, VP, VP, VP, VP, VP, VP]),
+        "hfg_op_p2g_fc_static": (C.c_int, [I3, F3, F3, VP, VP, C.c_longlong, C.c_int, VP, VP, VP, VP, VP, VP, VP]),
         "hfg_op_p2g_cc": (C.c_int, [I3, F3, F3, VP, VP, C.c_longlong, C.c_int, C.c_int, VP, VP, VP]),
         "hfg_op_advect_particles": (C.c_int, [I3, F3, F3, VP, VP, VP, VP, C.c_longlong, C.c_float, C.c_float,
                                               C.c_int, C.c_int, C.POINTER(C.c_int), VP]),
@@ -450,6 +451,14 @@ def op_g2p_cc(res, origin, spacing, f, pos, alg, out, stream=None):
 def op_p2g_fc(res, origin, spacing, pos, vel, alg, out, weights=(None, None, None), stream=None):
     _check(lib().hfg_op_p2g_fc(_i3(res), _f3(origin), _f3(spacing), _ptr(pos), _ptr(vel), pos.numel() // 3, alg,
                                *[_ptr(v) for v in out], *[_ptr(w) for w in weights], _stream(stream)))
+
+
+def op_p2g_fc_static(res, origin, spacing, pos, vel, alg, out, weights=(None, None, None), stream=None):
+    """op_p2g_fc with the accumulators in the library's fixed 8 MiB array
+    instead of freshly allocated device memory: at most 2**20 faces in total;
+    calls overlapping in time on one device race (hfgrid.h)."""
+    _check(lib().hfg_op_p2g_fc_static(_i3(res), _f3(origin), _f3(spacing), _ptr(pos), _ptr(vel), pos.numel() // 3,
+                                      alg, *[_ptr(v) for v in out], *[_ptr(w) for w in weights], _stream(stream)))
 
 
 def op_p2g_cc(res, origin, spacing, pos, val, alg, out, weights=None, normalize=True, stream=None):

@@ -229,6 +229,27 @@ HFG_API int hfg_op_seed_particles(const int res[3], const float origin[3], const
                                   unsigned long long seed, float* pos, long long capacity, long long* count,
                                   void* stream);
 
+/* hfg_op_p2g_fc without any device allocation.  This entry point has no
+ * counterpart in the reference.  It is for callers that may not allocate
+ * device memory at call time (a fixed-memory real-time loop, or a host whose
+ * own allocator reserves the whole device and forbids other allocations): the
+ * accumulators live in one 8 MiB array inside libhfgrid.so instead of coming
+ * from the stream-ordered allocator.
+ *   - Limit: the three face grids together hold at most 1,048,576 faces
+ *     ((nx+1)ny nz + nx(ny+1)nz + nx ny(nz+1); 64^3 cells fit).  Larger grids
+ *     return HFG_ERR_INVALID with a message; use hfg_op_p2g_fc for them.
+ *   - Every call, on every stream and thread of the process, uses the same
+ *     array on a device: calls that overlap in time on one device race and
+ *     give wrong results.  Serialise them.  Each call zeroes the accumulators
+ *     it uses before scattering, so nothing has to be cleared in advance.
+ *   - The first call on each device resolves the array's address on that
+ *     device (the caller's current device).  Make that first call before any
+ *     stream capture begins.
+ * Arguments, results and blocking behaviour are those of hfg_op_p2g_fc. */
+HFG_API int hfg_op_p2g_fc_static(const int res[3], const float origin[3], const float spacing[3], const float* pos,
+                                 const float* vel, long long n, int alg, float* vx, float* vy, float* vz, float* wx,
+                                 float* wy, float* wz, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
