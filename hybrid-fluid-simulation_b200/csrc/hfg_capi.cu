@@ -68,6 +68,10 @@ template <class T> struct Scratch {
 };
 }  // namespace
 
+namespace hfg {
+void setLastError(const std::string& msg) { g_lastError = msg; }
+}  // namespace hfg
+
 extern "C" {
 
 HFG_API const char* hfg_last_error(void) { return g_lastError.c_str(); }
@@ -138,6 +142,14 @@ HFG_API int hfg_solver_add_solid_boundary(hfg_solver_t s, const float* sdf, cons
     SOLVER(s);
     NEED(sdf, "null sdf");
     S.addBoundary(sdf, vel);
+    return HFG_OK;
+  });
+}
+HFG_API int hfg_solver_add_analytic_solid(hfg_solver_t s, int type, const double params[6], const float vel[3]) {
+  return guarded([&]() -> int {
+    SOLVER(s);
+    NEED(type == HFG_SOLID_WALLS || params, "null parameters");
+    S.addAnalyticBoundary(type, params, vel);
     return HFG_OK;
   });
 }
@@ -413,7 +425,7 @@ HFG_API int hfg_op_build_matrix_a(const int res[3], const float spacing[3], floa
     Scratch<Code> code(r.size(), st(stream));
     float sx, sy, sz;
     scalesA(spacing, dt, sx, sy, sz);
-    check(launchStencilCode(r, markers, code.p, st(stream)), "code");
+    check(launchStencilCode(r, r.x, markers, code.p, st(stream)), "code");
     check(launchMatrixA(r, sx, sy, sz, code.p, A, st(stream)), "matrix");
     return HFG_OK;
   });
@@ -426,7 +438,7 @@ HFG_API int hfg_op_apply_a(const int res[3], const float spacing[3], float dt, c
     Scratch<Code> code(r.size(), st(stream));
     float sx, sy, sz;
     scalesA(spacing, dt, sx, sy, sz);
-    check(launchStencilCode(r, markers, code.p, st(stream)), "code");
+    check(launchStencilCode(r, r.x, markers, code.p, st(stream)), "code");
     check(launchApplyA(r, sx, sy, sz, code.p, x, y, st(stream)), "apply");
     return HFG_OK;
   });
@@ -437,7 +449,8 @@ HFG_API int hfg_op_build_rhs(const int res[3], const float spacing[3], const flo
   return guarded([&]() -> int {
     NEED(validRes(res) && spacing && vx && vy && vz && svx && svy && svz && markers && b, "invalid arguments");
     Geom g = toGeom(res, nullptr, spacing);
-    long long N = g.r.size();
+    const Dim3i cg = cgDims(g.r);
+    long long N = cg.size();
     Scratch<Code> code(N, st(stream));
     Scratch<float> r(N, st(stream)), x(N, st(stream)), p(N, st(stream));
     Scratch<double> part(cgPartialsNeeded(g.r), st(stream));
@@ -446,7 +459,7 @@ HFG_API int hfg_op_build_rhs(const int res[3], const float spacing[3], const flo
     init.maxIter = 1;
     init.tol = 1e-3;
     check(cudaMemcpyAsync(cs.p, &init, sizeof(init), cudaMemcpyHostToDevice, st(stream)), "state");
-    check(launchStencilCode(g.r, markers, code.p, st(stream)), "code");
+    check(launchStencilCode(g.r, cg.x, markers, code.p, st(stream)), "code");
     ConstFaceField v{{vx, vy, vz}}, sv{{svx, svy, svz}};
     SolidVelTable none{};
     check(launchRhsInit(g, v, sv, none, markers, code.p, 1.f, 1.f, 1.f, b, r.p, x.p, p.p, part.p, cs.p, 0, st(stream)),
@@ -464,12 +477,15 @@ HFG_API int hfg_op_project(const int res[3], const float spacing[3], float dt, c
     NEED(precond == HFG_PRECOND_IDENTITY || precond == HFG_PRECOND_JACOBI, "operator projection supports identity/Jacobi");
     NEED(tol_mode == 0 || tol_mode == 1, "invalid tolerance mode");
     Geom g = toGeom(res, nullptr, spacing);
-    long long N = g.r.size();
+    const Dim3i cg = cgDims(g.r);
+    long long N = g.r.size(), NC = cg.size();
     cudaStream_t s = st(stream);
-    Scratch<Code> code(N, s);
-    Scratch<float> r(N, s), x(N, s), p0(N, s), p1(N, s);
+    Scratch<Code> code(NC, s);
+    Scratch<float> r(NC, s), x(NC, s), p0(NC, s), p1(NC, s);
     Scratch<double> part(cgPartialsNeeded(g.r), s);
     Scratch<CgState> cs(1, s);
+    CgMaps maps;
+    check(makeCgMaps(cg, code.p, r.p, x.p, p0.p, p1.p, &maps), "tensor maps");
     CgState init{};
     init.maxIter = (int)std::min<long long>(max_iter < 0 ? N : max_iter, 0x7fffffff);
     init.precond = precond == HFG_PRECOND_JACOBI ? 1 : 0;
@@ -478,7 +494,7 @@ HFG_API int hfg_op_project(const int res[3], const float spacing[3], float dt, c
     check(cudaMemcpyAsync(cs.p, &init, sizeof(init), cudaMemcpyHostToDevice, s), "state");
     float sx, sy, sz;
     scalesA(spacing, dt, sx, sy, sz);
-    check(launchStencilCode(g.r, markers, code.p, s), "code");
+    check(launchStencilCode(g.r, cg.x, markers, code.p, s), "code");
     ConstFaceField v{{vx, vy, vz}}, sv{{svx, svy, svz}};
     SolidVelTable none{};
     check(launchRhsInit(g, v, sv, none, markers, code.p, sx, sy, sz, nullptr, r.p, x.p, p0.p, part.p, cs.p,
@@ -489,21 +505,27 @@ HFG_API int hfg_op_project(const int res[3], const float spacing[3], float dt, c
     int it = 0;
     for (;;) {
       for (int k = 0; k < 16; ++k, ++it) {
-        check(launchCgDirection(g.r, sx, sy, sz, code.p, r.p, pb[it & 1], pb[(it + 1) & 1], part.p, cs.p,
-                                init.precond, s),
+        const int po = it & 1, pn = (it + 1) & 1;
+        check(launchCgDirection(cg, sx, sy, sz, maps.rH, maps.pH[po], maps.codeH, code.p, r.p, pb[po], pb[pn], part.p,
+                                cs.p, init.precond, s),
               "cg");
-        check(launchCgUpdate(g.r, sx, sy, sz, code.p, pb[(it + 1) & 1], x.p, r.p, part.p, cs.p, init.precond, s),
+        check(launchCgUpdate(cg, sx, sy, sz, maps.pH[pn], maps.rI, maps.xI, maps.codeI, pb[pn], x.p, r.p, part.p, cs.p,
+                             init.precond, s),
               "cg");
       }
       check(cudaMemcpyAsync(&host, cs.p, sizeof(host), cudaMemcpyDeviceToHost, s), "read state");
       check(cudaStreamSynchronize(s), "sync");
       if (host.done) break;
     }
+    if (host.error) return fail(HFG_ERR_TIMEOUT, "pressure CG: a stage load did not complete in time");
     FaceField vv{{vx, vy, vz}};
     check(launchGradient(g, dt / (1.0f * spacing[0]), dt / (1.0f * spacing[1]), dt / (1.0f * spacing[2]), markers,
                          x.p, vv, sv, none, s),
           "gradient");
-    if (pOut) check(cudaMemcpyAsync(pOut, x.p, N * 4, cudaMemcpyDeviceToDevice, s), "copy");
+    if (pOut)
+      check(cudaMemcpy2DAsync(pOut, (size_t)g.r.x * 4, x.p, (size_t)cg.x * 4, (size_t)g.r.x * 4,
+                              (size_t)g.r.y * g.r.z, cudaMemcpyDeviceToDevice, s),
+            "copy");
     check(cudaStreamSynchronize(s), "sync");
     if (stats) {
       stats[0] = host.iter;

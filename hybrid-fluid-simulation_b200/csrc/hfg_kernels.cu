@@ -82,6 +82,47 @@ cudaError_t launchSolidClassify(const Geom& g, const BoundarySet& b, uint8_t* so
 __global__ void kSolidFromSDF(long long n, const float* __restrict__ sdf, uint8_t* __restrict__ idx) {
   HFG_FOR(c, n) idx[c] = sdf[c] < 0.f ? 1 : 0;
 }
+__global__ void kAnalyticSdf(Geom g, int type, double p0, double p1, double p2, double p3, double p4, double p5,
+                             float* __restrict__ sdf) {
+  const Dim3i R = g.r;
+  HFG_FOR(c, R.size()) {
+    int x, y, z;
+    cellCoord(c, R, x, y, z);
+    const double P[3] = {(double)g.ox + (x + 0.5) * (double)g.hx, (double)g.oy + (y + 0.5) * (double)g.hy,
+                         (double)g.oz + (z + 0.5) * (double)g.hz};
+    double d;
+    if (type == 0) {
+      const double lo[3] = {(double)g.ox + g.hx, (double)g.oy + g.hy, (double)g.oz + g.hz};
+      const double hi[3] = {(double)g.ox + (R.x - 1) * (double)g.hx, (double)g.oy + (R.y - 1) * (double)g.hy,
+                            (double)g.oz + (R.z - 1) * (double)g.hz};
+      double in = 1e300, outsq = 0.0;
+      for (int a = 0; a < 3; ++a) {
+        double da = fmin(P[a] - lo[a], hi[a] - P[a]);
+        in = fmin(in, da);
+        if (da < 0.0) outsq += da * da;
+      }
+      d = in >= 0.0 ? in : -sqrt(outsq);
+    } else if (type == 1) {
+      const double dx = P[0] - p0, dy = P[1] - p1, dz = P[2] - p2;
+      d = sqrt(dx * dx + dy * dy + dz * dz) - p3;
+    } else {
+      const double c3[3] = {p0, p1, p2}, s3[3] = {p3, p4, p5};
+      double outsq = 0.0, mx = -1e300;
+      for (int a = 0; a < 3; ++a) {
+        double q = fabs(P[a] - c3[a]) - 0.5 * s3[a];
+        if (q > 0.0) outsq += q * q;
+        mx = fmax(mx, q);
+      }
+      d = sqrt(outsq) + fmin(mx, 0.0);
+    }
+    sdf[c] = (float)d;
+  }
+}
+cudaError_t launchAnalyticSdf(const Geom& g, int type, const double* p, float* sdf, cudaStream_t s) {
+  kAnalyticSdf<<<gridFor(g.r.size()), kThreads, 0, s>>>(g, type, p[0], p[1], p[2], p[3], p[4], p[5], sdf);
+  return cudaGetLastError();
+}
+
 cudaError_t launchSolidFromSDF(long long n, const float* solidSDF, uint8_t* solidIdx, cudaStream_t s) {
   kSolidFromSDF<<<gridFor(n), kThreads, 0, s>>>(n, solidSDF, solidIdx);
   return cudaGetLastError();
@@ -212,6 +253,9 @@ __global__ void kGradient(Geom g, float gx, float gy, float gz, const uint8_t* _
     cellCoord(c, R, x, y, z);
     long long sy = R.x, sz = (long long)R.x * R.y;
     long long cl = x > 0 ? c - 1 : c, cd = y > 0 ? c - sy : c, cb = z > 0 ? c - sz : c;
+    const long long px = cgPitch(R.x);
+    const long long pc = ((long long)z * R.y + y) * px + x;  // pressure is pitched
+    const long long po[3] = {x > 0 ? pc - 1 : pc, y > 0 ? pc - px : pc, z > 0 ? pc - px * R.y : pc};
     uint8_t mc = mk[c];
     long long fx = ((long long)z * rx.y + y) * rx.x + x;
     long long fy = ((long long)z * ry.y + y) * ry.x + x;
@@ -230,7 +274,7 @@ __global__ void kGradient(Geom g, float gx, float gy, float gz, const uint8_t* _
           else s = solidFaceVel(svTab, co[a] == c ? 0 : svTab.solidIdx[co[a]], svTab.solidIdx[c], a);
           vv[fo[a]] = s;
         } else {
-          vv[fo[a]] = __fsub_rn(vv[fo[a]], __fmul_rn(gs[a], __fsub_rn(p[c], p[co[a]])));
+          vv[fo[a]] = __fsub_rn(vv[fo[a]], __fmul_rn(gs[a], __fsub_rn(p[pc], p[po[a]])));
         }
       } else {
         vv[fo[a]] = kUnknown;

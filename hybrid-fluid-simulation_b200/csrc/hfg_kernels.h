@@ -3,6 +3,7 @@
 // cudaGetLastError() of its launch.
 #pragma once
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "hfg_device.cuh"
@@ -34,6 +35,7 @@ struct CgState {
   int precond;      // 0 identity, 1 Jacobi
   int tolMode;      // 0 reference rule sqrt(||r||) < tol, 1 ||r||/||b|| < tol
   double tol;
+  int error;        // nonzero: a kernel gave up (a stage load timed out); done is set too
   unsigned int ticket;  // last-block-done counter
 };
 
@@ -69,6 +71,11 @@ __device__ inline float solidFaceVel(const SolidVelTable& t, uint8_t lo, uint8_t
 cudaError_t launchSolidClassify(const Geom& g, const BoundarySet& b, uint8_t* solidIdx, float* const* curSDF,
                                 cudaStream_t s);
 cudaError_t launchSolidFromSDF(long long n, const float* solidSDF, uint8_t* solidIdx, cudaStream_t s);
+// Signed distance (negative inside the solid) of an analytic solid at every
+// cell centre, evaluated in FP64 and stored as FP32.  type 0: the walls, i.e.
+// everything outside the inner box [o + h, o + (n - 1) h]; 1: sphere
+// (cx, cy, cz, r); 2: axis-aligned box (cx, cy, cz, sx, sy, sz full sides).
+cudaError_t launchAnalyticSdf(const Geom& g, int type, const double* params, float* sdf, cudaStream_t s);
 cudaError_t launchTotalSolidSDF(long long n, int nb, const uint8_t* solidIdx, float* out, cudaStream_t s);
 cudaError_t launchSolidVelField(const Geom& g, const SolidVelTable& t, FaceField out, cudaStream_t s);
 cudaError_t launchMarkersInit(long long n, const uint8_t* solidIdx, uint8_t* markers, cudaStream_t s);
@@ -84,22 +91,43 @@ cudaError_t launchFluidDomainFromBBox(const Geom& g, const float mn[3], const fl
 // diagonal of buildPressureMatrixA, EulerSolverTool.cu:85-120); bits 7..12
 // that neighbour is inside the grid and fluid (the off-diagonals).
 typedef uint16_t Code;
-cudaError_t launchStencilCode(const Dim3i& r, const uint8_t* markers, Code* code, cudaStream_t s);
+// The pressure system lives on a pitched copy of the grid: rows of
+// px = cgPitch(nx) >= nx cells, px a multiple of 8 so that every row of FP32
+// values and of 16-bit codes starts on a 16-byte boundary (TMA tiles).  The
+// cells x >= nx are inert: code 0 and every CG vector 0 there.  Index of cell
+// (x, y, z): (z * ny + y) * px + x.
+__host__ __device__ inline int cgPitch(int nx) { return (nx + 7) & ~7; }
+__host__ __device__ inline Dim3i cgDims(const Dim3i& r) { return Dim3i{cgPitch(r.x), r.y, r.z}; }
+// Codes of grid `r` written with row pitch px (px = r.x: unpitched).
+cudaError_t launchStencilCode(const Dim3i& r, int px, const uint8_t* markers, Code* code, cudaStream_t s);
 cudaError_t launchMatrixA(const Dim3i& r, float sx, float sy, float sz, const Code* code, float* A, cudaStream_t s);
 cudaError_t launchApplyA(const Dim3i& r, float sx, float sy, float sz, const Code* code, const float* x, float* y,
                          cudaStream_t s);
 // RHS (divergence + solid terms) fused with CG set-up: r = b, x = 0, p = 0,
 // ||b||^2 and r.z into the state.  Solid face velocities come from `svArr`
-// when non-null, else from the per-solid table.
+// when non-null, else from the per-solid table.  `b` (optional) is unpitched;
+// code, r, x and p are pitched.
 cudaError_t launchRhsInit(const Geom& g, ConstFaceField v, ConstFaceField svArr, const SolidVelTable& svTab,
                           const uint8_t* markers, const Code* code, float ax, float ay, float az, float* b,
                           float* r, float* x, float* p, double* partials, CgState* st, int precond, cudaStream_t s);
-// precond: 0 identity, 1 Jacobi (must match CgState::precond)
-cudaError_t launchCgDirection(const Dim3i& r, float sx, float sy, float sz, const Code* code, const float* rr,
+// TMA descriptors of the CG vectors on the pitched grid cg = cgDims(r):
+// halo boxes (H) for the arrays read with neighbours, plain tiles (I) else.
+struct CgMaps {
+  CUtensorMap codeH, codeI, rH, rI, xI, pH[2];
+};
+cudaError_t makeCgMaps(const Dim3i& cg, const Code* code, const float* r, const float* x, const float* p0,
+                       const float* p1, CgMaps* m);
+cudaError_t makeHaloMap(const Dim3i& cg, const float* v, CUtensorMap* m);
+// precond: 0 identity, 1 Jacobi, 2 z read through mZ (must match CgState::precond);
+// mZ is the halo map of r (precond 0, 1) or of z (2); zr the same array.
+cudaError_t launchCgDirection(const Dim3i& cg, float sx, float sy, float sz, const CUtensorMap& mZ,
+                              const CUtensorMap& mPo, const CUtensorMap& mCode, const Code* code, const float* zr,
                               const float* pOld, float* pNew, double* partials, CgState* st, int precond,
                               cudaStream_t s);
-cudaError_t launchCgUpdate(const Dim3i& r, float sx, float sy, float sz, const Code* code, const float* p,
-                           float* x, float* rr, double* partials, CgState* st, int precond, cudaStream_t s);
+cudaError_t launchCgUpdate(const Dim3i& cg, float sx, float sy, float sz, const CUtensorMap& mP, const CUtensorMap& mR,
+                           const CUtensorMap& mX, const CUtensorMap& mCode, const float* p, float* x, float* r,
+                           double* partials, CgState* st, int precond, cudaStream_t s);
+// p pitched
 cudaError_t launchGradient(const Geom& g, float gx, float gy, float gz, const uint8_t* markers, const float* p,
                            FaceField v, ConstFaceField svArr, const SolidVelTable& svTab, cudaStream_t s);
 // doubles of reduction scratch the CG kernels need on grid `r`

@@ -133,14 +133,17 @@ __global__ void kJacobiFirst(Lvl L, const TB* __restrict__ b, TZ* __restrict__ z
 // post-smoothing sweep).
 template <class TB, class TZ, class TC, bool CORR, bool DOT>
 __global__ void kJacobi(Lvl L, Dim3i rc, const TB* __restrict__ b, const TZ* __restrict__ zi, TZ* __restrict__ zo,
-                        const TC* __restrict__ zc, const Code* __restrict__ code, double* partials, CgState* st) {
+                        const TC* __restrict__ zc, const Code* __restrict__ code, double* partials, CgState* st,
+                        int zPer) {
   if (st->done) return;
-  int x, y, z;
-  unsigned c;
   double rz = 0.0, dummy = 0.0;
-  bool in = cellOf(L.r, x, y, z, c);
-  if (in) {
-    const unsigned pl = (unsigned)L.r.x * L.r.y;
+  const int x = blockIdx.x * BX + threadIdx.x, y = blockIdx.y * BY + threadIdx.y;
+  const int zb0 = blockIdx.z * zPer;
+  const unsigned pl = (unsigned)L.r.x * L.r.y;
+  for (int zb = zb0; zb < zb0 + zPer; ++zb) {
+    const int z = zb * BZ + threadIdx.z;
+    if (x >= L.r.x || y >= L.r.y || z >= L.r.z) break;
+    const unsigned c = ((unsigned)z * L.r.y + y) * L.r.x + x;
     auto zAt = [&](int d) -> float {
       int dx, dy, dz;
       nbrOf(d, dx, dy, dz);
@@ -159,7 +162,7 @@ __global__ void kJacobi(Lvl L, Dim3i rc, const TB* __restrict__ b, const TZ* __r
       v = vc + kOmega * (bv - az) / diagOfC(k, L.sx, L.sy, L.sz);
     }
     zo[c] = cvt<TZ>(v);
-    if (DOT) rz = (double)bv * (double)v;
+    if (DOT) rz += (double)bv * (double)v;
   }
   if (DOT) {
     if (gridSum2(rz, dummy, partials, &st->ticket) && flatTid() == 0) {
@@ -174,6 +177,25 @@ __global__ void kJacobi(Lvl L, Dim3i rc, const TB* __restrict__ b, const TZ* __r
       st->ticket = 0;
     }
   }
+}
+
+// Launch shape of the sweeps: one z-block per thread block (zPer = 1), or for
+// the sweeps that end in a grid reduction a few thousand blocks each walking
+// several z-blocks, so that the last-block reduction stays short.
+struct SweepGrid {
+  dim3 grid;
+  int zPer;
+};
+SweepGrid sweepGrid(const Dim3i& r, bool reduce) {
+  dim3 g = gridOf(r);
+  int zPer = 1;
+  if (reduce) {
+    long long want = (long long)numSMs() * 8;
+    long long cols = (long long)g.x * g.y;
+    long long zc = std::max<long long>(1, want / std::max<long long>(1, cols));
+    zPer = (int)((g.z + zc - 1) / zc);
+  }
+  return SweepGrid{dim3(g.x, g.y, (g.z + zPer - 1) / zPer), zPer};
 }
 
 // Residual of level f restricted to level c: bc = mean over the children of
@@ -240,14 +262,9 @@ __global__ void kCoarseSolve(Lvl L, const TB* __restrict__ b, TZ* __restrict__ z
 }
 }  // namespace
 
-// Declared in the CG kernels file: the MG flavour of the two CG kernels.
-cudaError_t launchCgDirectionZ(const Dim3i& r, float sx, float sy, float sz, const Code* code, const float* z,
-                               const float* pOld, float* pNew, double* partials, CgState* st, cudaStream_t s);
-cudaError_t launchCgUpdateNoZ(const Dim3i& r, float sx, float sy, float sz, const Code* code, const float* p,
-                              float* x, float* rr, double* partials, CgState* st, cudaStream_t s);
-
 struct Multigrid {
-  Dim3i r0;
+  Dim3i r0;                          // level 0 = the pitched grid of the pressure system
+  Dim3i rLogical;                    // the solver's grid (level-0 markers are unpitched)
   int smooth = 2;
   bool half = true;
   std::vector<Dim3i> res;            // level resolutions, [0] = fine
@@ -258,6 +275,7 @@ struct Multigrid {
   DArray<float> z0a, z0b;            // level 0 iterate (FP32)
   DArray<float> p[2];
   DArray<double> partials;
+  CUtensorMap zH[2], pH[2];          // halo tensor maps of z0a / z0b and p[0] / p[1]
   const Code* code0 = nullptr;
   float s0[3] = {0, 0, 0};
   ~Multigrid() {
@@ -273,7 +291,7 @@ struct Multigrid {
   int levels() const { return (int)res.size(); }
 };
 
-Multigrid* mgCreate(const Dim3i& r, int levels, int smooth, bool half) {
+Multigrid* mgCreate(const Dim3i& r, int levels, int smooth, bool half, cudaStream_t s) {
   auto* m = new Multigrid();
   m->r0 = r;
   m->smooth = smooth > 0 ? smooth : 2;
@@ -291,27 +309,31 @@ Multigrid* mgCreate(const Dim3i& r, int levels, int smooth, bool half) {
     throw CudaError("multigrid: coarsest level too large; allow more levels", HFG_ERR_INVALID);
   }
   long long N = r.size();
-  m->z0a.alloc(N);
-  m->z0b.alloc(N);
-  m->p[0].alloc(N);
-  m->p[1].alloc(N);
-  m->partials.alloc(std::max(cgPartialsNeeded(r), 2 * (int)(gridOf(r).x * gridOf(r).y * gridOf(r).z)));
+  m->z0a.alloc(N, s);
+  m->z0b.alloc(N, s);
+  m->p[0].alloc(N, s);
+  m->p[1].alloc(N, s);
+  m->partials.alloc(std::max(cgPartialsNeeded(r), 2 * (int)(gridOf(r).x * gridOf(r).y * gridOf(r).z)), s);
+  check(makeHaloMap(r, m->z0a.p, &m->zH[0]), "multigrid tensor map");
+  check(makeHaloMap(r, m->z0b.p, &m->zH[1]), "multigrid tensor map");
+  check(makeHaloMap(r, m->p[0].p, &m->pH[0]), "multigrid tensor map");
+  check(makeHaloMap(r, m->p[1].p, &m->pH[1]), "multigrid tensor map");
   for (int l = 1; l < m->levels(); ++l) {
     long long n = m->res[l].size();
     auto* a = new DArray<uint8_t>();
-    a->alloc(n);
+    a->alloc(n, s);
     m->mk.push_back(a);
     auto* c = new DArray<Code>();
-    c->alloc(n);
+    c->alloc(n, s);
     m->code.push_back(c);
     if (half) {
-      auto* b = new DArray<uint16_t>(); b->alloc(n); m->b16.push_back(b);
-      auto* za = new DArray<uint16_t>(); za->alloc(n); m->z16a.push_back(za);
-      auto* zb = new DArray<uint16_t>(); zb->alloc(n); m->z16b.push_back(zb);
+      auto* b = new DArray<uint16_t>(); b->alloc(n, s); m->b16.push_back(b);
+      auto* za = new DArray<uint16_t>(); za->alloc(n, s); m->z16a.push_back(za);
+      auto* zb = new DArray<uint16_t>(); zb->alloc(n, s); m->z16b.push_back(zb);
     } else {
-      auto* b = new DArray<float>(); b->alloc(n); m->b32.push_back(b);
-      auto* za = new DArray<float>(); za->alloc(n); m->z32a.push_back(za);
-      auto* zb = new DArray<float>(); zb->alloc(n); m->z32b.push_back(zb);
+      auto* b = new DArray<float>(); b->alloc(n, s); m->b32.push_back(b);
+      auto* za = new DArray<float>(); za->alloc(n, s); m->z32a.push_back(za);
+      auto* zb = new DArray<float>(); zb->alloc(n, s); m->z32b.push_back(zb);
     }
   }
   return m;
@@ -326,10 +348,11 @@ void mgSetupLevels(Multigrid* m, const uint8_t* mk0, const Code* code0, float sx
   m->s0[0] = sx; m->s0[1] = sy; m->s0[2] = sz;
   const uint8_t* fine = mk0;
   for (int l = 1; l < m->levels(); ++l) {
-    Dim3i rf = m->res[l - 1], rc = m->res[l];
+    // level-0 markers are unpitched: children in the pitch padding are skipped
+    Dim3i rf = l == 1 ? m->rLogical : m->res[l - 1], rc = m->res[l];
     kCoarsenMarkers<<<gridOf(rc), dim3(BX, BY, BZ), 0, s>>>(rf, rc, fine, m->mk[l - 1]->p);
     check(cudaGetLastError(), "coarsen markers");
-    check(launchStencilCode(rc, m->mk[l - 1]->p, m->code[l - 1]->p, s), "level stencil code");
+    check(launchStencilCode(rc, rc.x, m->mk[l - 1]->p, m->code[l - 1]->p, s), "level stencil code");
     launches += 2;
     fine = m->mk[l - 1]->p;
   }
@@ -358,8 +381,8 @@ const float* vcycleT(Multigrid* m, const float* r0, CgState* st, cudaStream_t s,
       kJacobiFirst<float, float><<<gridOf(lv[0].r), blk, 0, s>>>(lv[0], r0, z0[0], codeOf(0), st);
       int cb = 0;
       for (int k = 1; k < nu; ++k, cb ^= 1)
-        kJacobi<float, float, float, false, false><<<gridOf(lv[0].r), blk, 0, s>>>(
-            lv[0], lv[0].r, r0, z0[cb], z0[cb ^ 1], nullptr, codeOf(0), nullptr, st);
+        kJacobi<float, float, float, false, false><<<sweepGrid(lv[0].r, false).grid, blk, 0, s>>>(
+            lv[0], lv[0].r, r0, z0[cb], z0[cb ^ 1], nullptr, codeOf(0), nullptr, st, sweepGrid(lv[0].r, false).zPer);
       curBuf[0] = cb;
       kResidualRestrict<float, float, TS><<<gridOf(lv[1].r), blk, 0, s>>>(lv[0], lv[1].r, r0, z0[cb], codeOf(0), bL[1],
                                                                            st);
@@ -369,8 +392,8 @@ const float* vcycleT(Multigrid* m, const float* r0, CgState* st, cudaStream_t s,
       kJacobiFirst<TS, TS><<<gridOf(lv[l].r), blk, 0, s>>>(lv[l], bL[l], zl[0], codeOf(l), st);
       int cb = 0;
       for (int k = 1; k < nu; ++k, cb ^= 1)
-        kJacobi<TS, TS, TS, false, false><<<gridOf(lv[l].r), blk, 0, s>>>(lv[l], lv[l].r, bL[l], zl[cb],
-                                                                           zl[cb ^ 1], nullptr, codeOf(l), nullptr, st);
+        kJacobi<TS, TS, TS, false, false><<<sweepGrid(lv[l].r, false).grid, blk, 0, s>>>(lv[l], lv[l].r, bL[l], zl[cb],
+                                                                           zl[cb ^ 1], nullptr, codeOf(l), nullptr, st, sweepGrid(lv[l].r, false).zPer);
       curBuf[l] = cb;
       kResidualRestrict<TS, TS, TS><<<gridOf(lv[l + 1].r), blk, 0, s>>>(lv[l], lv[l + 1].r, bL[l], zl[cb], codeOf(l),
                                                                          bL[l + 1], st);
@@ -397,17 +420,17 @@ const float* vcycleT(Multigrid* m, const float* r0, CgState* st, cudaStream_t s,
       for (int k = 0; k < nu; ++k, cb ^= 1) {
         bool last = k == nu - 1;
         if (k == 0 && last)
-          kJacobi<float, float, TS, true, true><<<gridOf(lv[0].r), blk, 0, s>>>(
-              lv[0], lv[1].r, r0, z0[cb], z0[cb ^ 1], zc, codeOf(0), m->partials.p, st);
+          kJacobi<float, float, TS, true, true><<<sweepGrid(lv[0].r, true).grid, blk, 0, s>>>(
+              lv[0], lv[1].r, r0, z0[cb], z0[cb ^ 1], zc, codeOf(0), m->partials.p, st, sweepGrid(lv[0].r, true).zPer);
         else if (k == 0)
-          kJacobi<float, float, TS, true, false><<<gridOf(lv[0].r), blk, 0, s>>>(
-              lv[0], lv[1].r, r0, z0[cb], z0[cb ^ 1], zc, codeOf(0), nullptr, st);
+          kJacobi<float, float, TS, true, false><<<sweepGrid(lv[0].r, false).grid, blk, 0, s>>>(
+              lv[0], lv[1].r, r0, z0[cb], z0[cb ^ 1], zc, codeOf(0), nullptr, st, sweepGrid(lv[0].r, false).zPer);
         else if (last)
-          kJacobi<float, float, float, false, true><<<gridOf(lv[0].r), blk, 0, s>>>(
-              lv[0], lv[0].r, r0, z0[cb], z0[cb ^ 1], nullptr, codeOf(0), m->partials.p, st);
+          kJacobi<float, float, float, false, true><<<sweepGrid(lv[0].r, true).grid, blk, 0, s>>>(
+              lv[0], lv[0].r, r0, z0[cb], z0[cb ^ 1], nullptr, codeOf(0), m->partials.p, st, sweepGrid(lv[0].r, true).zPer);
         else
-          kJacobi<float, float, float, false, false><<<gridOf(lv[0].r), blk, 0, s>>>(
-              lv[0], lv[0].r, r0, z0[cb], z0[cb ^ 1], nullptr, codeOf(0), nullptr, st);
+          kJacobi<float, float, float, false, false><<<sweepGrid(lv[0].r, false).grid, blk, 0, s>>>(
+              lv[0], lv[0].r, r0, z0[cb], z0[cb ^ 1], nullptr, codeOf(0), nullptr, st, sweepGrid(lv[0].r, false).zPer);
       }
       curBuf[0] = cb;
       launches += nu;
@@ -416,12 +439,12 @@ const float* vcycleT(Multigrid* m, const float* r0, CgState* st, cudaStream_t s,
       int cb = curBuf[l];
       for (int k = 0; k < nu; ++k, cb ^= 1) {
         if (k == 0)
-          kJacobi<TS, TS, TS, true, false><<<gridOf(lv[l].r), blk, 0, s>>>(lv[l], lv[l + 1].r, bL[l], zl[cb],
-                                                                            zl[cb ^ 1], zc, codeOf(l), nullptr, st);
+          kJacobi<TS, TS, TS, true, false><<<sweepGrid(lv[l].r, false).grid, blk, 0, s>>>(lv[l], lv[l + 1].r, bL[l], zl[cb],
+                                                                            zl[cb ^ 1], zc, codeOf(l), nullptr, st, sweepGrid(lv[l].r, false).zPer);
         else
-          kJacobi<TS, TS, TS, false, false><<<gridOf(lv[l].r), blk, 0, s>>>(lv[l], lv[l].r, bL[l], zl[cb],
+          kJacobi<TS, TS, TS, false, false><<<sweepGrid(lv[l].r, false).grid, blk, 0, s>>>(lv[l], lv[l].r, bL[l], zl[cb],
                                                                              zl[cb ^ 1], nullptr, codeOf(l), nullptr,
-                                                                             st);
+                                                                             st, sweepGrid(lv[l].r, false).zPer);
       }
       curBuf[l] = cb;
       launches += nu;
@@ -455,27 +478,31 @@ const float* mgVcycle(Multigrid* m, const float* r0, CgState* st, cudaStream_t s
   }
 }
 
-void mgSetup(Multigrid* m, const uint8_t* mk0, const Code* code, float sx, float sy, float sz, cudaStream_t s,
-             long long& launches) {
+void mgSetup(Multigrid* m, const Dim3i& r, const uint8_t* mk0, const Code* code, float sx, float sy, float sz,
+             cudaStream_t s, long long& launches) {
+  m->rLogical = r;
   mgSetupLevels(m, mk0, code, sx, sy, sz, s, launches);
 }
 
 // Preconditioned CG with the V-cycle: the RHS kernel already set r = b,
 // x = 0 and ||b||^2.  Iterations are launched in chunks; every kernel returns
 // immediately once the state says done.
-void mgRunCg(Multigrid* m, const Dim3i& r, float sx, float sy, float sz, const Code* code, float* x, float* rvec,
-             double* partials, CgState* st, CgState* stHost, cudaStream_t s, long long& launches) {
-  (void)partials;
+void mgRunCg(Multigrid* m, const Dim3i& cg, float sx, float sy, float sz, const CgMaps& maps, const Code* code, float* x,
+             float* rvec, CgState* st, CgState* stHost, cudaStream_t s, long long& launches) {
   check(cudaMemsetAsync(m->p[0].p, 0, m->p[0].bytes(), s), "memset");
   const float* z = mgVcycle(m, rvec, st, s, launches);  // z0 = V(b), rz = b.z0
   int it = 0;
   const int chunk = 4;
   for (;;) {
     for (int k = 0; k < chunk; ++k, ++it) {
-      float* pOld = m->p[it & 1].p;
-      float* pNew = m->p[(it + 1) & 1].p;
-      check(launchCgDirectionZ(r, sx, sy, sz, code, z, pOld, pNew, m->partials.p, st, s), "cg direction");
-      check(launchCgUpdateNoZ(r, sx, sy, sz, code, pNew, x, rvec, m->partials.p, st, s), "cg update");
+      const int po = it & 1, pn = (it + 1) & 1;
+      const int zi = z == m->z0a.p ? 0 : 1;
+      check(launchCgDirection(cg, sx, sy, sz, m->zH[zi], m->pH[po], maps.codeH, code, z, m->p[po].p, m->p[pn].p,
+                              m->partials.p, st, 2, s),
+            "cg direction");
+      check(launchCgUpdate(cg, sx, sy, sz, m->pH[pn], maps.rI, maps.xI, maps.codeI, m->p[pn].p, x, rvec,
+                           m->partials.p, st, 2, s),
+            "cg update");
       launches += 2;
       z = mgVcycle(m, rvec, st, s, launches);
     }

@@ -10,6 +10,8 @@
 // along z keeping the below / current / above planes in registers, so the z
 // neighbours cost no extra loads and no division is needed for indexing.
 #include <algorithm>
+#include <map>
+#include <mutex>
 
 #include "hfg_kernels.h"
 
@@ -83,38 +85,35 @@ __device__ __forceinline__ float applyRow(Code k, float sx, float sy, float sz, 
 }
 }  // namespace
 
-int cgPartialsNeeded(const Dim3i& r) {
-  CgGrid g = cgGrid(r);
-  return 2 * (int)(g.grid.x * g.grid.y * g.grid.z);
-}
 
 // ---------------------------------------------------------------------------
-__global__ void kStencilCode(Dim3i r, const uint8_t* __restrict__ mk, Code* __restrict__ code, int zPer) {
+__global__ void kStencilCode(Dim3i r, int px, const uint8_t* __restrict__ mk, Code* __restrict__ code, int zPer) {
   int x = blockIdx.x * TX + threadIdx.x, y = blockIdx.y * TY + threadIdx.y;
-  if (x >= r.x || y >= r.y) return;
+  if (x >= px || y >= r.y) return;
   int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, r.z);
   long long plane = (long long)r.x * r.y;
   for (int z = z0; z < z1; ++z) {
     long long c = (long long)z * plane + (long long)y * r.x + x;
+    long long o = ((long long)z * r.y + y) * px + x;
     Code k = 0;
-    if (mk[c] == kFluid) {
+    if (x < r.x && mk[c] == kFluid) {
       k = 1;
       const bool in[6] = {x > 0, x + 1 < r.x, y > 0, y + 1 < r.y, z > 0, z + 1 < r.z};
-      const long long o[6] = {-1, 1, -(long long)r.x, (long long)r.x, -plane, plane};
+      const long long d6[6] = {-1, 1, -(long long)r.x, (long long)r.x, -plane, plane};
 #pragma unroll
       for (int d = 0; d < 6; ++d) {
         if (!in[d]) continue;
-        uint8_t m = mk[c + o[d]];
+        uint8_t m = mk[c + d6[d]];
         if (m != kSolid) k |= (Code)(1u << (1 + d));
         if (m == kFluid) k |= (Code)(1u << (7 + d));
       }
     }
-    code[c] = k;
+    code[o] = k;
   }
 }
-cudaError_t launchStencilCode(const Dim3i& r, const uint8_t* markers, Code* code, cudaStream_t s) {
-  CgGrid g = cgGrid(r);
-  kStencilCode<<<g.grid, g.block, 0, s>>>(r, markers, code, g.zPer);
+cudaError_t launchStencilCode(const Dim3i& r, int px, const uint8_t* markers, Code* code, cudaStream_t s) {
+  CgGrid g = cgGrid(Dim3i{px, r.y, r.z});
+  kStencilCode<<<g.grid, g.block, 0, s>>>(r, px, markers, code, g.zPer);
   return cudaGetLastError();
 }
 
@@ -176,9 +175,19 @@ __global__ void __launch_bounds__(TX* TY) kRhsInit(Geom g, ConstFaceField v, Con
                                                    float* __restrict__ r, float* __restrict__ xv, float* __restrict__ p,
                                                    double* partials, CgState* st, int zPer) {
   const Dim3i R = g.r;
+  const int px = cgPitch(R.x);
   const float ix = 1.0f / g.hx, iy = 1.0f / g.hy, iz = 1.0f / g.hz;
   int x = blockIdx.x * TX + threadIdx.x, y = blockIdx.y * TY + threadIdx.y;
   double bb = 0.0, rzs = 0.0;
+  if (x >= R.x && x < px && y < R.y) {  // pitch padding: inert cells
+    int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, R.z);
+    for (int z = z0; z < z1; ++z) {
+      long long o = ((long long)z * R.y + y) * px + x;
+      r[o] = 0.f;
+      xv[o] = 0.f;
+      p[o] = 0.f;
+    }
+  }
   if (x < R.x && y < R.y) {
     int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, R.z);
     const long long plane = (long long)R.x * R.y;
@@ -212,10 +221,11 @@ __global__ void __launch_bounds__(TX* TY) kRhsInit(Geom g, ConstFaceField v, Con
         if (mk[cf] == kSolid) b = __fadd_rn(b, __fmul_rn(iz, __fsub_rn(F, sv(2, wF, cf, true))));
       }
       if (bOut) bOut[c] = b;
-      r[c] = b;
-      xv[c] = 0.f;
-      p[c] = 0.f;
-      float zz = precondZ<PC>(code[c], b, sAx, sAy, sAz);
+      long long o = ((long long)z * R.y + y) * px + x;
+      r[o] = b;
+      xv[o] = 0.f;
+      p[o] = 0.f;
+      float zz = precondZ<PC>(code[o], b, sAx, sAy, sAz);
       bb += (double)b * (double)b;
       rzs += (double)b * (double)zz;
     }
@@ -234,7 +244,7 @@ __global__ void __launch_bounds__(TX* TY) kRhsInit(Geom g, ConstFaceField v, Con
 cudaError_t launchRhsInit(const Geom& gm, ConstFaceField v, ConstFaceField svArr, const SolidVelTable& svTab,
                           const uint8_t* markers, const Code* code, float ax, float ay, float az, float* b, float* r,
                           float* x, float* p, double* partials, CgState* st, int precond, cudaStream_t s) {
-  CgGrid g = cgGrid(gm.r);
+  CgGrid g = cgGrid(cgDims(gm.r));
   if (precond == 1)
     kRhsInit<1><<<g.grid, g.block, 0, s>>>(gm, v, svArr, svTab, markers, code, ax, ay, az, b, r, x, p, partials, st,
                                            g.zPer);
@@ -244,6 +254,7 @@ cudaError_t launchRhsInit(const Geom& gm, ConstFaceField v, ConstFaceField svArr
   return cudaGetLastError();
 }
 
+namespace {
 // ---------------------------------------------------------------------------
 // Fast row of A for the CG: the diagonal and its reciprocal come from a
 // 64-entry table per launch (indexed by the six "not solid" bits; the entries
@@ -282,57 +293,233 @@ __device__ __forceinline__ float fastZ(const DiagTab& t, Code k, float rv) {
   return (k & 1) ? rv * t.inv[(k >> 1) & 63] : rv;
 }
 
+// ---------------------------------------------------------------------------
+// TMA plumbing.  Each CG block owns a 32 x 8 column of the pitched grid and
+// marches along z; one elected thread streams the planes ahead of the
+// consumers into a ring of shared-memory stages with cp.async.bulk.tensor,
+// completion tracked by one mbarrier per stage.  The halo boxes start 4
+// floats (8 codes) left of the tile so that every box starts on a 16-byte
+// boundary; boxes outside the grid arrive zero-filled.
+constexpr int CTX = 32, CTY = 8;     // tile (threads) per plane
+constexpr int HXF = 4, HXC = 8;      // left pad of the float / code halo boxes
+constexpr int FW = CTX + 2 * HXF;    // 40 floats
+constexpr int CW = CTX + 2 * HXC;    // 48 codes
+constexpr int FH = CTY + 2;          // 10 rows
+constexpr int kDirStages = 4, kUpdStages = 5;
+constexpr unsigned long long kWaitNs = 2000000000ull;  // a stage that takes 2 s to land is an error
+
+__device__ __forceinline__ uint32_t smemAddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ unsigned long long globalNs() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void mbarInit(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smemAddr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbarFenceInit() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbarExpectTx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smemAddr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbarTryWait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smemAddr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: false once the deadline has passed.
+__device__ __forceinline__ bool mbarWait(uint64_t* bar, unsigned parity, unsigned long long deadline) {
+  while (!mbarTryWait(bar, parity))
+    if (globalNs() > deadline) return false;
+  return true;
+}
+__device__ __forceinline__ void tmaLoad3(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smemAddr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smemAddr(bar))
+      : "memory");
+}
+
+// Marks the solve failed; the host sees `error` and stops.
+__device__ __forceinline__ void cgFail(CgState* st, int code) {
+  atomicExch(&st->error, code);
+  atomicExch(&st->done, 1);
+}
+
+// Blocks that gave up still drain every stage they issued (bounded) before
+// the shared memory is released.
+template <int S>
+__device__ void drainStages(uint64_t* bar, const int* issued, int waited) {
+  unsigned long long deadline = globalNs() + kWaitNs;
+  for (int i = waited; i < issued[0]; ++i)
+    if (!mbarWait(&bar[i % S], (unsigned)((i / S) & 1), deadline)) break;
+}
+
+struct __align__(128) DirStage {
+  alignas(128) float r[FH][FW];
+  alignas(128) float po[FH][FW];
+  alignas(128) Code code[FH][CW];
+};
+constexpr unsigned kDirStageBytes = sizeof(float) * FH * FW * 2 + sizeof(Code) * FH * CW;
+
+struct __align__(128) UpdStage {
+  alignas(128) float p[FH][FW];
+  alignas(128) float r[CTY][CTX];
+  alignas(128) float x[CTY][CTX];
+  alignas(128) Code code[CTY][CTX];
+};
+constexpr unsigned kUpdStageBytes = sizeof(float) * (FH * FW + 2 * CTY * CTX) + sizeof(Code) * CTY * CTX;
+
+struct CgLaunch {
+  dim3 grid, block;
+  int zPer;
+};
+
+// Tiles over (x, y), z split into chunks so that the blocks fill whole waves
+// of the resident slots (wave count x chunk length minimal).
+int residentBlocks(const void* kernel) {
+  static std::mutex mu;
+  static std::map<const void*, int> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(kernel);
+  if (it != cache.end()) return it->second;
+  int per = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, CTX * CTY, 0) != cudaSuccess || per <= 0) per = 1;
+  cache[kernel] = per;
+  return per;
+}
+
+template <class K>
+CgLaunch cgLaunch(const Dim3i& cg, K kernel) {
+  long long slots = (long long)numSMs() * residentBlocks((const void*)kernel);
+  CgLaunch L;
+  L.block = dim3(CTX, CTY, 1);
+  int bx = (cg.x + CTX - 1) / CTX, by = (cg.y + CTY - 1) / CTY;
+  long long tiles = (long long)bx * by;
+  long long best = -1;
+  int bestPer = cg.z;
+  for (int zPer = 1; zPer <= cg.z; ++zPer) {
+    long long zc = (cg.z + zPer - 1) / zPer;
+    long long waves = (tiles * zc + slots - 1) / slots;
+    long long cost = waves * (zPer + 2);  // +2: pipeline fill per block
+    if (best < 0 || cost < best) {
+      best = cost;
+      bestPer = zPer;
+    }
+  }
+  L.zPer = bestPer;
+  L.grid = dim3(bx, by, (cg.z + bestPer - 1) / bestPer);
+  return L;
+}
+
 // CG direction: p = z + beta p_old (scal then axpy with 1), q = A p and the
 // reduction p.q; the last block forms alpha = r.z / p.Ap
-// (CuMatrixFreePCG.cpp:40-47, :56-60).  p of the current plane (with a one-
-// cell halo) sits in a double-buffered shared tile, p below / above in
-// registers; every p value is formed once per cell plus the halo ring.
+// (CuMatrixFreePCG.cpp:40-47, :56-60).  Stage i of the ring holds raw (z or r,
+// p_old, code) of plane z0 + i with a one-cell halo; p of each plane (with
+// halo) is formed once into a double-buffered tile, p above / below the
+// current plane stay in registers.  PC: 0 identity, 1 Jacobi, 2 z from
+// memory (multigrid).
 template <int PC>
-__global__ void __launch_bounds__(TX* TY, 4) kCgDirection(Dim3i R, float sx, float sy, float sz,
-                                                          const Code* __restrict__ code, const float* __restrict__ r,
-                                                          const float* __restrict__ pOld, float* __restrict__ pNew,
-                                                          double* partials, CgState* st, int zPer) {
+__global__ void __launch_bounds__(CTX* CTY, 4)
+    kCgDirection(const __grid_constant__ CUtensorMap mZ, const __grid_constant__ CUtensorMap mPo,
+                 const __grid_constant__ CUtensorMap mCode, Dim3i P, float sx, float sy, float sz,
+                 const Code* __restrict__ code, const float* __restrict__ zr, const float* __restrict__ pOld,
+                 float* __restrict__ pNew, double* partials, CgState* st, int zPer) {
   if (st->done) return;
-  __shared__ float tile[2][TY + 2][TX + 2];
+  __shared__ DirStage stg[kDirStages];
+  __shared__ float pt[2][FH][CTX + 2];
   __shared__ DiagTab tab;
+  __shared__ __align__(8) uint64_t bar[kDirStages];
+  __shared__ int issued;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * CTX + tx;
+  const int x0 = blockIdx.x * CTX, y0 = blockIdx.y * CTY;
+  const int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, P.z);
+  const int nPlanes = z1 - z0, nLoad = nPlanes + 1;  // plane z1 is the last "above"
+  auto issue = [&](int i) {
+    DirStage& S = stg[i % kDirStages];
+    uint64_t* b = &bar[i % kDirStages];
+    mbarExpectTx(b, kDirStageBytes);
+    tmaLoad3(&S.r[0][0], &mZ, x0 - HXF, y0 - 1, z0 + i, b);
+    tmaLoad3(&S.po[0][0], &mPo, x0 - HXF, y0 - 1, z0 + i, b);
+    tmaLoad3(&S.code[0][0], &mCode, x0 - HXC, y0 - 1, z0 + i, b);
+  };
+  if (tid == 0) {
+    for (int s = 0; s < kDirStages; ++s) mbarInit(&bar[s], 1);
+    mbarFenceInit();
+  }
   buildDiagTab(tab, sx, sy, sz);
   __syncthreads();
+  if (tid == 0) {
+    int n = min(kDirStages, nLoad);
+    for (int i = 0; i < n; ++i) issue(i);
+    issued = n;
+  }
   const float beta = st->beta;
-  double pq = 0.0, dummy = 0.0;
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int x = blockIdx.x * TX + tx, y = blockIdx.y * TY + ty;
-  const bool in = x < R.x && y < R.y;
-  const int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, R.z);
-  const unsigned plane = (unsigned)R.x * (unsigned)R.y;
-  auto pn = [&](unsigned i) -> float {
-    float zz = fastZ<PC>(tab, __ldg(code + i), __ldg(r + i));
-    return fmaf(beta, __ldg(pOld + i), zz);
+  const unsigned long long deadline = globalNs() + kWaitNs;
+  const int x = x0 + tx, y = y0 + ty;
+  const bool in = x < P.x && y < P.y;
+  const unsigned plane = (unsigned)P.x * (unsigned)P.y;
+  unsigned c = (unsigned)z0 * plane + (unsigned)y * (unsigned)P.x + (unsigned)x;
+  // p of the plane below the chunk, own cell only
+  float below = 0.f;
+  if (in && z0 > 0) {
+    unsigned b = c - plane;
+    below = fmaf(beta, __ldg(pOld + b), fastZ<PC>(tab, __ldg(code + b), __ldg(zr + b)));
+  }
+  // p of stage i's plane into tile t (own cell and the halo ring); returns own p and code
+  auto formTile = [&](int i, float (*t)[CTX + 2], Code& kOwn) -> float {
+    const DirStage& S = stg[i % kDirStages];
+    auto pAt = [&](int row, int colF, int colC) {
+      return fmaf(beta, S.po[row][colF], fastZ<PC>(tab, S.code[row][colC], S.r[row][colF]));
+    };
+    float v = pAt(ty + 1, tx + HXF, tx + HXC);
+    kOwn = S.code[ty + 1][tx + HXC];
+    t[ty + 1][tx + 1] = v;
+    if (tx == 0) t[ty + 1][0] = pAt(ty + 1, HXF - 1, HXC - 1);
+    if (tx == CTX - 1) t[ty + 1][CTX + 1] = pAt(ty + 1, HXF + CTX, HXC + CTX);
+    if (ty == 0) t[0][tx + 1] = pAt(0, tx + HXF, tx + HXC);
+    if (ty == CTY - 1) t[CTY + 1][tx + 1] = pAt(CTY + 1, tx + HXF, tx + HXC);
+    return v;
   };
-  unsigned c = (unsigned)z0 * plane + (unsigned)y * (unsigned)R.x + (unsigned)x;
-  float below = (in && z0 > 0) ? pn(c - plane) : 0.f;
-  float cur = in ? pn(c) : 0.f;
+  bool ok = mbarWait(&bar[0], 0, deadline);
+  Code kCur = 0, kAbove = 0;
+  float cur = ok ? formTile(0, pt[0], kCur) : 0.f;
+  int waited = 1;
+  bool fail = __syncthreads_or(!ok);
+  if (!fail && tid == 0 && kDirStages < nLoad) issue(kDirStages), issued = kDirStages + 1;
   float acc = 0.f;
-  int buf = 0;
-  for (int z = z0; z < z1; ++z, c += plane, buf ^= 1) {
-    float above = (in && z + 1 < R.z) ? pn(c + plane) : 0.f;
-    Code k = in ? __ldg(code + c) : (Code)0;
-    float (*t)[TX + 2] = tile[buf];
-    t[ty + 1][tx + 1] = cur;
-    if (tx == 0) t[ty + 1][0] = (in && x > 0) ? pn(c - 1) : 0.f;
-    if (tx == TX - 1 || x == R.x - 1) t[ty + 1][tx + 2] = (in && x + 1 < R.x) ? pn(c + 1) : 0.f;
-    if (ty == 0) t[0][tx + 1] = (in && y > 0) ? pn(c - R.x) : 0.f;
-    if (ty == TY - 1 || y == R.y - 1) t[ty + 2][tx + 1] = (in && y + 1 < R.y) ? pn(c + R.x) : 0.f;
-    __syncthreads();
-    if (in) {
-      float q = fastRow(tab, k, sx, sy, sz, cur, t[ty + 1][tx], t[ty + 1][tx + 2], t[ty][tx + 1], t[ty + 2][tx + 1],
+  for (int i = 0; i < nPlanes && !fail; ++i, c += plane) {
+    ok = mbarWait(&bar[(i + 1) % kDirStages], (unsigned)(((i + 1) / kDirStages) & 1), deadline);
+    waited = i + 2;
+    float above = ok ? formTile(i + 1, pt[(i + 1) & 1], kAbove) : 0.f;
+    if (in && ok) {
+      float (*t)[CTX + 2] = pt[i & 1];
+      float q = fastRow(tab, kCur, sx, sy, sz, cur, t[ty + 1][tx], t[ty + 1][tx + 2], t[ty][tx + 1], t[ty + 2][tx + 1],
                         below, above);
       pNew[c] = cur;
       acc = fmaf(cur, q, acc);
     }
     below = cur;
     cur = above;
+    kCur = kAbove;
+    fail = __syncthreads_or(!ok);
+    if (!fail && tid == 0 && i + 1 + kDirStages < nLoad) issue(i + 1 + kDirStages), issued = i + 2 + kDirStages;
   }
-  pq = (double)acc;
+  if (fail) {
+    if (tid == 0) {
+      cgFail(st, 1);
+      drainStages<kDirStages>(bar, &issued, waited);
+    }
+    return;
+  }
+  double pq = (double)acc, dummy = 0.0;
   if (gridSum2(pq, dummy, partials, &st->ticket) && flatTid() == 0) {
     st->pAp = pq;
     st->alpha = (float)(st->rz / pq);
@@ -341,50 +528,71 @@ __global__ void __launch_bounds__(TX* TY, 4) kCgDirection(Dim3i R, float sx, flo
 }
 
 // CG update: x += alpha p, r -= alpha A p (A p recomputed from the stored p
-// through the same shared tile), z = M^-1 r, the reductions r.r and r.z; the
-// last block checks convergence and forms beta (CuMatrixFreePCG.cpp:49-63).
-// The |alpha| < FLT_EPSILON skip of CCuDenseVector::plusAlphaX
+// of the stage ring), z = M^-1 r, the reductions r.r and r.z; the last block
+// checks convergence and forms beta (CuMatrixFreePCG.cpp:49-63).  The
+// |alpha| < FLT_EPSILON skip of CCuDenseVector::plusAlphaX
 // (CuDenseVector.cpp:178) is kept.  Per-thread partial sums run over one
 // z-column segment in FP32 and are combined in FP64.
 template <int PC>
-__global__ void __launch_bounds__(TX* TY, 4) kCgUpdate(Dim3i R, float sx, float sy, float sz,
-                                                       const Code* __restrict__ code, const float* __restrict__ p,
-                                                       float* __restrict__ xv, float* __restrict__ r,
-                                                       double* partials, CgState* st, int zPer) {
+__global__ void __launch_bounds__(CTX* CTY, 4)
+    kCgUpdate(const __grid_constant__ CUtensorMap mP, const __grid_constant__ CUtensorMap mR,
+              const __grid_constant__ CUtensorMap mX, const __grid_constant__ CUtensorMap mCode, Dim3i P, float sx,
+              float sy, float sz, const float* __restrict__ p, float* __restrict__ xv, float* __restrict__ r,
+              double* partials, CgState* st, int zPer) {
   if (st->done) return;
-  __shared__ float tile[2][TY + 2][TX + 2];
+  __shared__ UpdStage stg[kUpdStages];
   __shared__ DiagTab tab;
+  __shared__ __align__(8) uint64_t bar[kUpdStages];
+  __shared__ int issued;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * CTX + tx;
+  const int x0 = blockIdx.x * CTX, y0 = blockIdx.y * CTY;
+  const int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, P.z);
+  const int nPlanes = z1 - z0, nLoad = nPlanes + 1;
+  auto issue = [&](int i) {
+    UpdStage& S = stg[i % kUpdStages];
+    uint64_t* b = &bar[i % kUpdStages];
+    mbarExpectTx(b, kUpdStageBytes);
+    tmaLoad3(&S.p[0][0], &mP, x0 - HXF, y0 - 1, z0 + i, b);
+    tmaLoad3(&S.r[0][0], &mR, x0, y0, z0 + i, b);
+    tmaLoad3(&S.x[0][0], &mX, x0, y0, z0 + i, b);
+    tmaLoad3(&S.code[0][0], &mCode, x0, y0, z0 + i, b);
+  };
+  if (tid == 0) {
+    for (int s = 0; s < kUpdStages; ++s) mbarInit(&bar[s], 1);
+    mbarFenceInit();
+  }
   buildDiagTab(tab, sx, sy, sz);
   __syncthreads();
+  if (tid == 0) {
+    int n = min(kUpdStages, nLoad);
+    for (int i = 0; i < n; ++i) issue(i);
+    issued = n;
+  }
   const float alpha = st->alpha;
   const bool skip = fabsf(alpha) < FLT_EPSILON;
-  float arr = 0.f, arz = 0.f;
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int x = blockIdx.x * TX + tx, y = blockIdx.y * TY + ty;
-  const bool in = x < R.x && y < R.y;
-  const int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, R.z);
-  const unsigned plane = (unsigned)R.x * (unsigned)R.y;
-  unsigned c = (unsigned)z0 * plane + (unsigned)y * (unsigned)R.x + (unsigned)x;
+  const unsigned long long deadline = globalNs() + kWaitNs;
+  const int x = x0 + tx, y = y0 + ty;
+  const bool in = x < P.x && y < P.y;
+  const unsigned plane = (unsigned)P.x * (unsigned)P.y;
+  unsigned c = (unsigned)z0 * plane + (unsigned)y * (unsigned)P.x + (unsigned)x;
   float below = (in && z0 > 0) ? __ldg(p + c - plane) : 0.f;
-  float cur = in ? __ldg(p + c) : 0.f;
-  int buf = 0;
-  for (int z = z0; z < z1; ++z, c += plane, buf ^= 1) {
-    float above = (in && z + 1 < R.z) ? __ldg(p + c + plane) : 0.f;
-    Code k = in ? __ldg(code + c) : (Code)0;
-    float rv = in ? r[c] : 0.f;
-    float xo = (in && !skip) ? xv[c] : 0.f;
-    float (*t)[TX + 2] = tile[buf];
-    t[ty + 1][tx + 1] = cur;
-    if (tx == 0) t[ty + 1][0] = (in && x > 0) ? __ldg(p + c - 1) : 0.f;
-    if (tx == TX - 1 || x == R.x - 1) t[ty + 1][tx + 2] = (in && x + 1 < R.x) ? __ldg(p + c + 1) : 0.f;
-    if (ty == 0) t[0][tx + 1] = (in && y > 0) ? __ldg(p + c - R.x) : 0.f;
-    if (ty == TY - 1 || y == R.y - 1) t[ty + 2][tx + 1] = (in && y + 1 < R.y) ? __ldg(p + c + R.x) : 0.f;
-    __syncthreads();
-    if (in) {
+  bool ok = mbarWait(&bar[0], 0, deadline);
+  float cur = ok ? stg[0].p[ty + 1][tx + HXF] : 0.f;
+  int waited = 1;
+  bool fail = __syncthreads_or(!ok);
+  float arr = 0.f, arz = 0.f;
+  for (int i = 0; i < nPlanes && !fail; ++i, c += plane) {
+    ok = mbarWait(&bar[(i + 1) % kUpdStages], (unsigned)(((i + 1) / kUpdStages) & 1), deadline);
+    waited = i + 2;
+    float above = ok ? stg[(i + 1) % kUpdStages].p[ty + 1][tx + HXF] : 0.f;
+    const UpdStage& S = stg[i % kUpdStages];
+    if (in && ok) {
+      Code k = S.code[ty][tx];
+      float rv = S.r[ty][tx];
       if (!skip) {
-        float q = fastRow(tab, k, sx, sy, sz, cur, t[ty + 1][tx], t[ty + 1][tx + 2], t[ty][tx + 1], t[ty + 2][tx + 1],
-                          below, above);
-        xv[c] = fmaf(alpha, cur, xo);
+        float q = fastRow(tab, k, sx, sy, sz, cur, S.p[ty + 1][tx + HXF - 1], S.p[ty + 1][tx + HXF + 1],
+                          S.p[ty][tx + HXF], S.p[ty + 2][tx + HXF], below, above);
+        xv[c] = fmaf(alpha, cur, S.x[ty][tx]);
         rv = fmaf(-alpha, q, rv);
         r[c] = rv;
       }
@@ -394,6 +602,15 @@ __global__ void __launch_bounds__(TX* TY, 4) kCgUpdate(Dim3i R, float sx, float 
     }
     below = cur;
     cur = above;
+    fail = __syncthreads_or(!ok);
+    if (!fail && tid == 0 && i + kUpdStages < nLoad) issue(i + kUpdStages), issued = i + 1 + kUpdStages;
+  }
+  if (fail) {
+    if (tid == 0) {
+      cgFail(st, 1);
+      drainStages<kUpdStages>(bar, &issued, waited);
+    }
+    return;
   }
   double rr = (double)arr, rz = (double)arz;
   if (gridSum2(rr, rz, partials, &st->ticket) && flatTid() == 0) {
@@ -404,42 +621,109 @@ __global__ void __launch_bounds__(TX* TY, 4) kCgUpdate(Dim3i R, float sx, float 
       st->beta = (float)(rz / st->rz);
       st->rz = rz;
     }
-    st->done = stop || st->iter >= st->maxIter;
+    st->done = st->error || stop || st->iter >= st->maxIter;
     st->ticket = 0;
   }
 }
 
-cudaError_t launchCgDirection(const Dim3i& r, float sx, float sy, float sz, const Code* code, const float* rr,
+// Tensor map of a pitched 3-D array (x fastest) with the given box.
+cudaError_t encodeMap(CUtensorMap* m, const void* base, CUtensorMapDataType type, unsigned esize, const Dim3i& cg,
+                      unsigned bx, unsigned by) {
+  using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                              const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static Encode encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+    if (e != cudaSuccess) return e;
+    if (q != cudaDriverEntryPointSuccess || !fn) return cudaErrorNotSupported;
+    encode = (Encode)fn;
+  }
+  cuuint64_t dims[3] = {(cuuint64_t)cg.x, (cuuint64_t)cg.y, (cuuint64_t)cg.z};
+  cuuint64_t strides[2] = {(cuuint64_t)cg.x * esize, (cuuint64_t)cg.x * cg.y * esize};
+  cuuint32_t box[3] = {bx, by, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = encode(m, type, 3, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+}  // namespace
+
+cudaError_t makeHaloMap(const Dim3i& cg, const float* v, CUtensorMap* m) {
+  return encodeMap(m, v, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cg, FW, FH);
+}
+
+cudaError_t makeCgMaps(const Dim3i& cg, const Code* code, const float* r, const float* x, const float* p0,
+                       const float* p1, CgMaps* m) {
+  if (cg.x % 8 != 0) return cudaErrorInvalidValue;  // rows must start on 16-byte boundaries
+  cudaError_t e;
+  if ((e = encodeMap(&m->codeH, code, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, cg, CW, FH)) != cudaSuccess) return e;
+  if ((e = encodeMap(&m->codeI, code, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, cg, CTX, CTY)) != cudaSuccess) return e;
+  if ((e = encodeMap(&m->rH, r, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cg, FW, FH)) != cudaSuccess) return e;
+  if ((e = encodeMap(&m->rI, r, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cg, CTX, CTY)) != cudaSuccess) return e;
+  if ((e = encodeMap(&m->xI, x, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cg, CTX, CTY)) != cudaSuccess) return e;
+  if ((e = encodeMap(&m->pH[0], p0, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cg, FW, FH)) != cudaSuccess) return e;
+  return encodeMap(&m->pH[1], p1, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cg, FW, FH);
+}
+
+int cgPartialsNeeded(const Dim3i& r) {
+  const Dim3i cg = cgDims(r);
+  CgGrid g = cgGrid(cg);
+  long long n = (long long)g.grid.x * g.grid.y * g.grid.z;
+  CgLaunch a = cgLaunch(cg, kCgDirection<1>), b = cgLaunch(cg, kCgUpdate<1>);
+  n = std::max(n, (long long)a.grid.x * a.grid.y * a.grid.z);
+  n = std::max(n, (long long)b.grid.x * b.grid.y * b.grid.z);
+  return 2 * (int)n;
+}
+
+cudaError_t launchCgDirection(const Dim3i& cg, float sx, float sy, float sz, const CUtensorMap& mZ,
+                              const CUtensorMap& mPo, const CUtensorMap& mCode, const Code* code, const float* zr,
                               const float* pOld, float* pNew, double* partials, CgState* st, int precond,
                               cudaStream_t s) {
-  CgGrid g = cgGrid(r);
-  if (precond == 1)
-    kCgDirection<1><<<g.grid, g.block, 0, s>>>(r, sx, sy, sz, code, rr, pOld, pNew, partials, st, g.zPer);
-  else
-    kCgDirection<0><<<g.grid, g.block, 0, s>>>(r, sx, sy, sz, code, rr, pOld, pNew, partials, st, g.zPer);
-  return cudaGetLastError();
-}
-cudaError_t launchCgUpdate(const Dim3i& r, float sx, float sy, float sz, const Code* code, const float* p, float* x,
-                           float* rr, double* partials, CgState* st, int precond, cudaStream_t s) {
-  CgGrid g = cgGrid(r);
-  if (precond == 1)
-    kCgUpdate<1><<<g.grid, g.block, 0, s>>>(r, sx, sy, sz, code, p, x, rr, partials, st, g.zPer);
-  else
-    kCgUpdate<0><<<g.grid, g.block, 0, s>>>(r, sx, sy, sz, code, p, x, rr, partials, st, g.zPer);
+  switch (precond) {
+    case 1: {
+      CgLaunch L = cgLaunch(cg, kCgDirection<1>);
+      kCgDirection<1><<<L.grid, L.block, 0, s>>>(mZ, mPo, mCode, cg, sx, sy, sz, code, zr, pOld, pNew, partials, st,
+                                                 L.zPer);
+      break;
+    }
+    case 2: {
+      CgLaunch L = cgLaunch(cg, kCgDirection<2>);
+      kCgDirection<2><<<L.grid, L.block, 0, s>>>(mZ, mPo, mCode, cg, sx, sy, sz, code, zr, pOld, pNew, partials, st,
+                                                 L.zPer);
+      break;
+    }
+    default: {
+      CgLaunch L = cgLaunch(cg, kCgDirection<0>);
+      kCgDirection<0><<<L.grid, L.block, 0, s>>>(mZ, mPo, mCode, cg, sx, sy, sz, code, zr, pOld, pNew, partials, st,
+                                                 L.zPer);
+    }
+  }
   return cudaGetLastError();
 }
 
-// Multigrid flavour: z is read from memory (the V-cycle's output).
-cudaError_t launchCgDirectionZ(const Dim3i& r, float sx, float sy, float sz, const Code* code, const float* z,
-                               const float* pOld, float* pNew, double* partials, CgState* st, cudaStream_t s) {
-  CgGrid g = cgGrid(r);
-  kCgDirection<2><<<g.grid, g.block, 0, s>>>(r, sx, sy, sz, code, z, pOld, pNew, partials, st, g.zPer);
-  return cudaGetLastError();
-}
-cudaError_t launchCgUpdateNoZ(const Dim3i& r, float sx, float sy, float sz, const Code* code, const float* p,
-                              float* x, float* rr, double* partials, CgState* st, cudaStream_t s) {
-  CgGrid g = cgGrid(r);
-  kCgUpdate<2><<<g.grid, g.block, 0, s>>>(r, sx, sy, sz, code, p, x, rr, partials, st, g.zPer);
+cudaError_t launchCgUpdate(const Dim3i& cg, float sx, float sy, float sz, const CUtensorMap& mP, const CUtensorMap& mR,
+                           const CUtensorMap& mX, const CUtensorMap& mCode, const float* p, float* x, float* r,
+                           double* partials, CgState* st, int precond, cudaStream_t s) {
+  switch (precond) {
+    case 1: {
+      CgLaunch L = cgLaunch(cg, kCgUpdate<1>);
+      kCgUpdate<1><<<L.grid, L.block, 0, s>>>(mP, mR, mX, mCode, cg, sx, sy, sz, p, x, r, partials, st, L.zPer);
+      break;
+    }
+    case 2: {
+      CgLaunch L = cgLaunch(cg, kCgUpdate<2>);
+      kCgUpdate<2><<<L.grid, L.block, 0, s>>>(mP, mR, mX, mCode, cg, sx, sy, sz, p, x, r, partials, st, L.zPer);
+      break;
+    }
+    default: {
+      CgLaunch L = cgLaunch(cg, kCgUpdate<0>);
+      kCgUpdate<0><<<L.grid, L.block, 0, s>>>(mP, mR, mX, mCode, cg, sx, sy, sz, p, x, r, partials, st, L.zPer);
+    }
+  }
   return cudaGetLastError();
 }
 

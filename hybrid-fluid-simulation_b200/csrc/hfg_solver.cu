@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 #include "hfg_solver.h"
 
@@ -16,17 +17,44 @@ void check(cudaError_t e, const char* what) {
 }
 
 namespace {
+constexpr size_t kPinnedBlock = 8192;
+std::mutex g_pinnedMu;
+std::vector<void*> g_pinnedFree;
+}  // namespace
+
+void* pinnedGet(size_t bytes) {
+  if (bytes > kPinnedBlock) throw CudaError("pinned block too large", HFG_ERR_INVALID);
+  {
+    std::lock_guard<std::mutex> lk(g_pinnedMu);
+    if (!g_pinnedFree.empty()) {
+      void* p = g_pinnedFree.back();
+      g_pinnedFree.pop_back();
+      return p;
+    }
+  }
+  void* p = nullptr;
+  check(cudaMallocHost(&p, kPinnedBlock), "cudaMallocHost");
+  return p;
+}
+
+void pinnedPut(void* p) {
+  if (!p) return;
+  std::lock_guard<std::mutex> lk(g_pinnedMu);
+  g_pinnedFree.push_back(p);
+}
+
+namespace {
 constexpr int kCgChunk = 16;       // CG iterations launched between convergence reads
 constexpr int kSubstepChunk = 4;   // CFL substeps launched between completion reads
 }  // namespace
 
 // Multigrid preconditioner hooks (hfg_mg.cu).
-Multigrid* mgCreate(const Dim3i& r, int levels, int smooth, bool half);
+Multigrid* mgCreate(const Dim3i& cg, int levels, int smooth, bool half, cudaStream_t s);
 void mgDestroy(Multigrid* m);
-void mgSetup(Multigrid* m, const uint8_t* mk0, const Code* code, float sx, float sy, float sz, cudaStream_t s,
-             long long& launches);
-void mgRunCg(Multigrid* m, const Dim3i& r, float sx, float sy, float sz, const Code* code, float* x, float* rvec,
-             double* partials, CgState* st, CgState* stHost, cudaStream_t s, long long& launches);
+void mgSetup(Multigrid* m, const Dim3i& r, const uint8_t* mk0, const Code* code, float sx, float sy, float sz,
+             cudaStream_t s, long long& launches);
+void mgRunCg(Multigrid* m, const Dim3i& cg, float sx, float sy, float sz, const CgMaps& maps, const Code* code, float* x,
+             float* rvec, CgState* st, CgState* stHost, cudaStream_t s, long long& launches);
 
 GridSolver::GridSolver(float dt, Dim3i res, const float origin[3], const float spacing[3]) {
   if (res.x <= 0 || res.y <= 0 || res.z <= 0) throw CudaError("resolution must be positive", HFG_ERR_INVALID);
@@ -43,23 +71,32 @@ GridSolver::GridSolver(float dt, Dim3i res, const float origin[3], const float s
   for (int a = 0; a < 3; ++a) { F_[a] = fr_[a].size(); Ftot_ += F_[a]; }
   hfg_default_options(&opt_);
   check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  own_.s = stream_;
   for (int b = 0; b < 2; ++b)
     for (int a = 0; a < 3; ++a) {
-      vel_[b][a].alloc(F_[a]);
-      color_[b][a].alloc(N_);
+      vel_[b][a].alloc(F_[a], stream_);
+      color_[b][a].alloc(N_, stream_);
     }
-  for (int b = 0; b < 2; ++b) dom_[b].alloc(N_);
-  for (int a = 0; a < 3; ++a) prev_[a].alloc(F_[a]);
-  solidIdx_.alloc(N_); markers_.alloc(N_); code_.alloc(N_);
-  cgx_.alloc(N_); cgr_.alloc(N_); cgp_[0].alloc(N_); cgp_[1].alloc(N_);
-  partials_.alloc(cgPartialsNeeded(res));
-  cgState_.alloc(1);
-  subState_.alloc(subSlots_ + 1);
-  dist_.alloc(Ftot_); list_.alloc(Ftot_);
-  hist_.alloc(kMaxLayers + 2); offsets_.alloc(kMaxLayers + 2); cursor_.alloc(kMaxLayers + 2);
-  check(cudaMallocHost((void**)&cgHost_, sizeof(CgState)), "cudaMallocHost");
-  check(cudaMallocHost((void**)&subHost_, sizeof(SubstepState)), "cudaMallocHost");
-  check(cudaMallocHost((void**)&offHost_, sizeof(unsigned int) * (kMaxLayers + 2)), "cudaMallocHost");
+  for (int b = 0; b < 2; ++b) dom_[b].alloc(N_, stream_);
+  for (int a = 0; a < 3; ++a) prev_[a].alloc(F_[a], stream_);
+  cg_ = cgDims(res);
+  NC_ = cg_.size();
+  solidIdx_.alloc(N_, stream_); markers_.alloc(N_, stream_); code_.alloc(NC_, stream_);
+  cgx_.alloc(NC_, stream_);
+  cgr_.alloc(NC_, stream_);
+  cgp_[0].alloc(NC_, stream_);
+  cgp_[1].alloc(NC_, stream_);
+  partials_.alloc(cgPartialsNeeded(res), stream_);
+  check(makeCgMaps(cg_, code_.p, cgr_.p, cgx_.p, cgp_[0].p, cgp_[1].p, &maps_), "CG tensor maps");
+  cgState_.alloc(1, stream_);
+  subState_.alloc(subSlots_ + 1, stream_);
+  dist_.alloc(Ftot_, stream_); list_.alloc(Ftot_, stream_);
+  hist_.alloc(kMaxLayers + 2, stream_);
+  offsets_.alloc(kMaxLayers + 2, stream_);
+  cursor_.alloc(kMaxLayers + 2, stream_);
+  cgHost_ = (CgState*)pinnedGet(sizeof(CgState));
+  subHost_ = (SubstepState*)pinnedGet(sizeof(SubstepState));
+  offHost_ = (unsigned int*)pinnedGet(sizeof(unsigned int) * (kMaxLayers + 2));
   // GridFluidSolver.cpp:179-195: every field starts at zero
   for (int b = 0; b < 2; ++b) {
     for (int a = 0; a < 3; ++a) {
@@ -81,12 +118,12 @@ GridSolver::~GridSolver() {
   if (stream_) cudaStreamSynchronize(stream_);
   for (auto* b : bsdf_) delete b;
   if (mg_) mgDestroy(mg_);
-  if (cgHost_) cudaFreeHost(cgHost_);
-  if (subHost_) cudaFreeHost(subHost_);
-  if (offHost_) cudaFreeHost(offHost_);
+  pinnedPut(cgHost_);
+  pinnedPut(subHost_);
+  pinnedPut(offHost_);
   for (int i = 0; i < 16; ++i)
     if (ev_[i]) cudaEventDestroy(ev_[i]);
-  if (stream_) cudaStreamDestroy(stream_);
+  // the stream itself goes with own_, after the member arrays are freed on it
 }
 
 void GridSolver::launched(cudaError_t e, const char* what, int count) {
@@ -106,11 +143,27 @@ void GridSolver::enableTiming(bool on) { timing_ = on; }
 void GridSolver::addBoundary(const float* sdfHost, const float vel[3]) {
   if ((int)bsdf_.size() >= kMaxBoundaries) throw CudaError("too many solid boundaries", HFG_ERR_INVALID);
   auto* b = new DArray<float>();
-  b->alloc(N_);
+  b->alloc(N_, stream_);
   check(cudaMemcpyAsync(b->p, sdfHost, N_ * sizeof(float), cudaMemcpyHostToDevice, stream_), "upload sdf");
   bsdf_.push_back(b);
   for (int a = 0; a < 3; ++a) { bvel_.push_back(vel ? vel[a] : 0.f); btrans_.push_back(0.f); }
   check(cudaStreamSynchronize(stream_), "sync");
+}
+
+void GridSolver::addAnalyticBoundary(int type, const double params[6], const float vel[3]) {
+  if ((int)bsdf_.size() >= kMaxBoundaries) throw CudaError("too many solid boundaries", HFG_ERR_INVALID);
+  if (type < 0 || type > 2) throw CudaError("unknown analytic solid type", HFG_ERR_INVALID);
+  const double zero[6] = {0, 0, 0, 0, 0, 0};
+  auto* b = new DArray<float>();
+  try {
+    b->alloc(N_, stream_);
+    check(launchAnalyticSdf(g_, type, params ? params : zero, b->p, stream_), "analytic sdf");
+  } catch (...) {
+    delete b;
+    throw;
+  }
+  bsdf_.push_back(b);
+  for (int a = 0; a < 3; ++a) { bvel_.push_back(vel ? vel[a] : 0.f); btrans_.push_back(0.f); }
 }
 
 void GridSolver::setBoundaryVelocity(int index, const float vel[3]) {
@@ -160,7 +213,11 @@ void GridSolver::setAdvection(int kind, int acc, int alg, float cfl, float mixin
 void GridSolver::setParticles(const float* pos, const float* vel, long long n) {
   if (n < 0) throw CudaError("negative particle count", HFG_ERR_INVALID);
   P_ = n;
-  ppos_.alloc(3 * n); pvel_.alloc(3 * n); pv0_.alloc(3 * n); pscalar_.alloc(n); pvector_.alloc(3 * n);
+  ppos_.alloc(3 * n, stream_);
+  pvel_.alloc(3 * n, stream_);
+  pv0_.alloc(3 * n, stream_);
+  pscalar_.alloc(n, stream_);
+  pvector_.alloc(3 * n, stream_);
   if (n > 0) {
     check(cudaMemcpyAsync(ppos_.p, pos, 12 * n, cudaMemcpyHostToDevice, stream_), "upload particles");
     if (vel) check(cudaMemcpyAsync(pvel_.p, vel, 12 * n, cudaMemcpyHostToDevice, stream_), "upload particles");
@@ -190,9 +247,9 @@ void GridSolver::seedParticles(int ppc, unsigned long long seed) {
   const int cellsPerBlock = 4096;
   int nb = (int)((N_ + cellsPerBlock - 1) / cellsPerBlock);
   DArray<unsigned int> counts;
-  counts.alloc(nb);
+  counts.alloc(nb, stream_);
   DArray<unsigned long long> total;
-  total.alloc(1);
+  total.alloc(1, stream_);
   const float* fsdf = dom_[cur()].p;
   launched(launchSeedCount(g_.r, fsdf, solidIdx_.p, counts.p, cellsPerBlock, stream_), "seed count");
   launched(launchSeedScan(counts.p, nb, total.p, stream_), "seed scan");
@@ -201,7 +258,11 @@ void GridSolver::seedParticles(int ppc, unsigned long long seed) {
   check(cudaStreamSynchronize(stream_), "sync");
   long long n = (long long)nf * ppc;
   P_ = n;
-  ppos_.alloc(3 * n); pvel_.alloc(3 * n); pv0_.alloc(3 * n); pscalar_.alloc(n); pvector_.alloc(3 * n);
+  ppos_.alloc(3 * n, stream_);
+  pvel_.alloc(3 * n, stream_);
+  pv0_.alloc(3 * n, stream_);
+  pscalar_.alloc(n, stream_);
+  pvector_.alloc(3 * n, stream_);
   if (n > 0) {
     launched(launchSeedWrite(g_, fsdf, solidIdx_.p, counts.p, cellsPerBlock, ppc, seed, ppos_.p, stream_), "seed write");
     check(cudaMemsetAsync(pvel_.p, 0, 12 * n, stream_), "memset");
@@ -222,7 +283,7 @@ void GridSolver::setOptions(const hfg_options_t& o) {
   opt_ = o;
   if (mgChanged) {
     if (mg_) mgDestroy(mg_);
-    mg_ = mgCreate(g_.r, o.mg_levels, o.mg_smooth, o.mg_half != 0);
+    mg_ = mgCreate(cg_, o.mg_levels, o.mg_smooth, o.mg_half != 0, stream_);
   }
 }
 
@@ -268,7 +329,7 @@ void GridSolver::forcesTerms(float gv[3], bool& doG, float ev[3], bool& doE) con
 void GridSolver::p2gFace(const float* vel, float* const out[3], float* const copy[3], const float add[3], bool doAdd,
                          const float add2[3], bool doAdd2) {
   for (int a = 0; a < 3; ++a) {
-    acc_[a].alloc(F_[a]);
+    acc_[a].alloc(F_[a], stream_);
     check(cudaMemsetAsync(acc_[a].p, 0, acc_[a].bytes(), stream_), "memset");
   }
   float2* acc[3] = {acc_[0].p, acc_[1].p, acc_[2].p};
@@ -280,7 +341,7 @@ void GridSolver::p2gFace(const float* vel, float* const out[3], float* const cop
 }
 
 void GridSolver::p2gCell(const float* vals, int span, int comp, float* out) {
-  cacc_.alloc(N_);
+  cacc_.alloc(N_, stream_);
   check(cudaMemsetAsync(cacc_.p, 0, cacc_.bytes(), stream_), "memset");
   launched(launchP2GCell(g_, alg_, ppos_.p, vals, span, comp, P_, cacc_.p, stream_), "p2g cell");
   launched(launchNormalize(N_, cacc_.p, out, nullptr, 0.f, 0, 0.f, 0, stream_), "normalize cell");
@@ -357,27 +418,31 @@ void GridSolver::computeAdvection() {
   stageEnd(1);
 }
 
+void GridSolver::cgIteration(int it, float sx, float sy, float sz, int pc) {
+  const int po = it & 1, pn = (it + 1) & 1;
+  launched(launchCgDirection(cg_, sx, sy, sz, maps_.rH, maps_.pH[po], maps_.codeH, code_.p, cgr_.p, cgp_[po].p,
+                             cgp_[pn].p, partials_.p, cgState_.p, pc, stream_),
+           "cg direction");
+  launched(launchCgUpdate(cg_, sx, sy, sz, maps_.pH[pn], maps_.rI, maps_.xI, maps_.codeI, cgp_[pn].p, cgx_.p, cgr_.p,
+                          partials_.p, cgState_.p, pc, stream_),
+           "cg update");
+}
+
 void GridSolver::runCg() {
   const float sx = dt_ / (1.0f * g_.hx * g_.hx), sy = dt_ / (1.0f * g_.hy * g_.hy), sz = dt_ / (1.0f * g_.hz * g_.hz);
   if (opt_.precond == HFG_PRECOND_MG) {
-    mgRunCg(mg_, g_.r, sx, sy, sz, code_.p, cgx_.p, cgr_.p, partials_.p, cgState_.p, cgHost_, stream_, launches_);
-    return;
-  }
-  int it = 0;
-  const int pc = opt_.precond == HFG_PRECOND_JACOBI ? 1 : 0;
-  for (;;) {
-    for (int k = 0; k < kCgChunk; ++k, ++it) {
-      float* pOld = cgp_[it & 1].p;
-      float* pNew = cgp_[(it + 1) & 1].p;
-      launched(launchCgDirection(g_.r, sx, sy, sz, code_.p, cgr_.p, pOld, pNew, partials_.p, cgState_.p, pc, stream_),
-               "cg direction");
-      launched(launchCgUpdate(g_.r, sx, sy, sz, code_.p, pNew, cgx_.p, cgr_.p, partials_.p, cgState_.p, pc, stream_),
-               "cg update");
+    mgRunCg(mg_, cg_, sx, sy, sz, maps_, code_.p, cgx_.p, cgr_.p, cgState_.p, cgHost_, stream_, launches_);
+  } else {
+    int it = 0;
+    const int pc = opt_.precond == HFG_PRECOND_JACOBI ? 1 : 0;
+    for (;;) {
+      for (int k = 0; k < kCgChunk; ++k, ++it) cgIteration(it, sx, sy, sz, pc);
+      check(cudaMemcpyAsync(cgHost_, cgState_.p, sizeof(CgState), cudaMemcpyDeviceToHost, stream_), "read cg state");
+      check(cudaStreamSynchronize(stream_), "cg sync");
+      if (cgHost_->done) break;
     }
-    check(cudaMemcpyAsync(cgHost_, cgState_.p, sizeof(CgState), cudaMemcpyDeviceToHost, stream_), "read cg state");
-    check(cudaStreamSynchronize(stream_), "cg sync");
-    if (cgHost_->done) break;
   }
+  if (cgHost_->error) throw CudaError("pressure CG: a stage load did not complete in time", HFG_ERR_TIMEOUT);
 }
 
 // PressureSolver.cpp:194-197 + GridFluidSolver.cpp:435-525
@@ -390,7 +455,7 @@ void GridSolver::computePressure() {
     launched(launchMarkersInit(N_, solidIdx_.p, markers_.p, stream_), "markers");
     launched(launchMarkersFromParticles(g_, ppos_.p, P_, markers_.p, stream_), "markers");
   }
-  launched(launchStencilCode(g_.r, markers_.p, code_.p, stream_), "stencil code");
+  launched(launchStencilCode(g_.r, cg_.x, markers_.p, code_.p, stream_), "stencil code");
   stageEnd(3);
   stageBegin(4);
   CgState init{};
@@ -405,7 +470,7 @@ void GridSolver::computePressure() {
   launched(launchRhsInit(g_, cvel(ni), none, solidTable(), markers_.p, code_.p, sx, sy, sz, nullptr, cgr_.p, cgx_.p,
                          cgp_[0].p, partials_.p, cgState_.p, init.precond, stream_),
            "rhs");
-  if (opt_.precond == HFG_PRECOND_MG) mgSetup(mg_, markers_.p, code_.p, sx, sy, sz, stream_, launches_);
+  if (opt_.precond == HFG_PRECOND_MG) mgSetup(mg_, g_.r, markers_.p, code_.p, sx, sy, sz, stream_, launches_);
   stageEnd(4);
   stageBegin(5);
   runCg();
@@ -490,18 +555,13 @@ float GridSolver::timeCg(int iters) {
   *cgHost_ = st;
   check(cudaMemcpyAsync(cgState_.p, cgHost_, sizeof(CgState), cudaMemcpyHostToDevice, stream_), "cg state");
   check(cudaEventRecord(ev_[14], stream_), "event");
-  for (int it = 0; it < iters; ++it) {
-    launched(launchCgDirection(g_.r, sx, sy, sz, code_.p, cgr_.p, cgp_[it & 1].p, cgp_[(it + 1) & 1].p, partials_.p,
-                               cgState_.p, st.precond, stream_),
-             "cg direction");
-    launched(launchCgUpdate(g_.r, sx, sy, sz, code_.p, cgp_[(it + 1) & 1].p, cgx_.p, cgr_.p, partials_.p,
-                            cgState_.p, st.precond, stream_),
-             "cg update");
-  }
+  for (int it = 0; it < iters; ++it) cgIteration(it, sx, sy, sz, st.precond);
   check(cudaEventRecord(ev_[15], stream_), "event");
   check(cudaEventSynchronize(ev_[15]), "event sync");
   float ms = 0.f;
   check(cudaEventElapsedTime(&ms, ev_[14], ev_[15]), "elapsed");
+  check(cudaMemcpy(cgHost_, cgState_.p, sizeof(CgState), cudaMemcpyDeviceToHost), "read cg state");
+  if (cgHost_->error) throw CudaError("pressure CG: a stage load did not complete in time", HFG_ERR_TIMEOUT);
   return ms / iters;
 }
 
@@ -531,13 +591,15 @@ void GridSolver::getMarkers(uint8_t* m) {
 }
 
 void GridSolver::getPressure(float* p) {
-  check(cudaMemcpyAsync(p, cgx_.p, N_ * 4, cudaMemcpyDeviceToHost, stream_), "download");
+  check(cudaMemcpy2DAsync(p, (size_t)g_.r.x * 4, cgx_.p, (size_t)cg_.x * 4, (size_t)g_.r.x * 4,
+                          (size_t)g_.r.y * g_.r.z, cudaMemcpyDeviceToHost, stream_),
+        "download");
   synchronize();
 }
 
 void GridSolver::getSolidSDF(float* s) {
   DArray<float> tmp;
-  tmp.alloc(N_);
+  tmp.alloc(N_, stream_);
   launched(launchTotalSolidSDF(N_, (int)bsdf_.size(), solidIdx_.p, tmp.p, stream_), "total sdf");
   check(cudaMemcpyAsync(s, tmp.p, N_ * 4, cudaMemcpyDeviceToHost, stream_), "download");
   synchronize();
@@ -545,7 +607,7 @@ void GridSolver::getSolidSDF(float* s) {
 
 void GridSolver::getSolidVel(float* x, float* y, float* z) {
   DArray<float> t[3];
-  for (int a = 0; a < 3; ++a) t[a].alloc(F_[a]);
+  for (int a = 0; a < 3; ++a) t[a].alloc(F_[a], stream_);
   FaceField f{{t[0].p, t[1].p, t[2].p}};
   launched(launchSolidVelField(g_, solidTable(), f, stream_), "solid vel");
   float* d[3] = {x, y, z};
@@ -557,11 +619,13 @@ void GridSolver::getSolidVel(float* x, float* y, float* z) {
 void GridSolver::getFluidSDF(float* out) {
   DArray<float> sdf;
   DArray<unsigned int> fa, fb, cnt;
-  sdf.alloc(N_); fa.alloc(N_); fb.alloc(N_); cnt.alloc(2);
-  unsigned int* host = nullptr;
-  check(cudaMallocHost((void**)&host, sizeof(unsigned int)), "cudaMallocHost");
+  sdf.alloc(N_, stream_);
+  fa.alloc(N_, stream_);
+  fb.alloc(N_, stream_);
+  cnt.alloc(2, stream_);
+  unsigned int* host = (unsigned int*)pinnedGet(sizeof(unsigned int));
   cudaError_t e = launchFluidSdf(g_.r, dom_[cur()].p, sdf.p, opt_.extrapolation_layers, fa.p, fb.p, cnt.p, host, stream_);
-  cudaFreeHost(host);
+  pinnedPut(host);
   check(e, "fluid sdf");
   check(cudaMemcpyAsync(out, sdf.p, N_ * 4, cudaMemcpyDeviceToHost, stream_), "download");
   synchronize();

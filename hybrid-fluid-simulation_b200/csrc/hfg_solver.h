@@ -25,31 +25,61 @@ struct CudaError : std::runtime_error {
 
 void check(cudaError_t e, const char* what);
 
-// Owning device array.
+// Owning device array.  With a stream the memory comes from the
+// stream-ordered allocator and is returned with cudaFreeAsync on the same
+// stream, so creating and destroying scenes never synchronises the device
+// (other scenes keep running); without one it is plain cudaMalloc / cudaFree.
 template <class T> struct DArray {
   T* p = nullptr;
   size_t n = 0;
+  cudaStream_t s = nullptr;
+  bool async = false;
   DArray() = default;
   DArray(const DArray&) = delete;
   DArray& operator=(const DArray&) = delete;
   ~DArray() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      if (async) cudaFreeAsync(p, s);
+      else cudaFree(p);
+    }
     p = nullptr;
     n = 0;
   }
-  void alloc(size_t count) {
+  void alloc(size_t count, cudaStream_t stream = nullptr) {
     if (count == n && p) return;
     release();
     if (count == 0) return;
-    cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T));
+    cudaError_t e;
+    if (stream) e = cudaMallocAsync((void**)&p, count * sizeof(T), stream);
+    else e = cudaMalloc((void**)&p, count * sizeof(T));
     if (e != cudaSuccess) {
       p = nullptr;
-      throw CudaError(std::string("cudaMalloc failed: ") + cudaGetErrorString(e), HFG_ERR_NOMEM);
+      throw CudaError(std::string("device allocation failed: ") + cudaGetErrorString(e), HFG_ERR_NOMEM);
     }
+    s = stream;
+    async = stream != nullptr;
     n = count;
   }
   size_t bytes() const { return n * sizeof(T); }
+};
+
+// Small pinned host blocks (state read-backs) from a process-wide free list:
+// cudaMallocHost / cudaFreeHost may synchronise the device, which a server
+// creating scenes while others run must avoid.
+void* pinnedGet(size_t bytes);
+void pinnedPut(void* p);
+
+// The solver's stream, destroyed after every member array has been freed
+// on it (declared first in GridSolver, so destroyed last).
+struct OwnedStream {
+  cudaStream_t s = nullptr;
+  ~OwnedStream() {
+    if (s) {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
+  }
 };
 
 struct Multigrid;  // hfg_mg.cu
@@ -61,6 +91,8 @@ class GridSolver {
 
   // ---- setters (GridFluidSolver.cpp:198-244) ----
   void addBoundary(const float* sdfHost, const float vel[3]);
+  // type/params as launchAnalyticSdf; the SDF is built on the device
+  void addAnalyticBoundary(int type, const double params[6], const float vel[3]);
   void addExternalForce(const float f[3]);
   void setBoundaryVelocity(int index, const float vel[3]);
   void setVelocity(const float* x, const float* y, const float* z);
@@ -94,6 +126,7 @@ class GridSolver {
 
   const Geom& geom() const { return g_; }
   cudaStream_t stream() const { return stream_; }
+  int numBoundaries() const { return (int)bsdf_.size(); }
   long long numParticles() const { return P_; }
   long long launches() const { return launches_; }
   const hfg_options_t& options() const { return opt_; }
@@ -107,6 +140,7 @@ class GridSolver {
   void p2gCell(const float* vals, int span, int comp, float* out);
   void computePressure();
   void runCg();
+  void cgIteration(int it, float sx, float sy, float sz, int pc);
   void extrapolate();
   void forcesTerms(float gv[3], bool& doG, float ev[3], bool& doE) const;
   int cur() const { return bufferFlag_ ? 1 : 0; }  // velocity/colour/domain "current" buffer
@@ -118,6 +152,7 @@ class GridSolver {
   void stageBegin(int i);
   void stageEnd(int i);
 
+  OwnedStream own_;  // first member: outlives every array below
   Geom g_;
   Dim3i fr_[3];
   long long N_, F_[3], Ftot_;
@@ -131,6 +166,9 @@ class GridSolver {
   DArray<float> vel_[2][3], prev_[3], color_[2][3], dom_[2], solidVel_[3];
   DArray<uint8_t> solidIdx_, markers_;
   DArray<Code> code_;
+  Dim3i cg_;       // pitched grid of the pressure system
+  long long NC_ = 0;
+  CgMaps maps_;
   DArray<float> cgx_, cgr_, cgp_[2];
   DArray<double> partials_;
   DArray<CgState> cgState_;

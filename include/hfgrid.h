@@ -229,6 +229,84 @@ HFG_API int hfg_op_seed_particles(const int res[3], const float origin[3], const
                                   unsigned long long seed, float* pos, long long capacity, long long* count,
                                   void* stream);
 
+/* ---- analytic solids and the scene server -------------------------------
+ * Neither has a counterpart in the reference, whose solids come from meshes
+ * voxelised by a D3D11 compute shader (BoundaryHelper.cpp:48-121) and whose
+ * simulators step one after another in one thread (MPhysics.cpp:19-25). */
+
+enum { HFG_SOLID_WALLS = 0, HFG_SOLID_SPHERE = 1, HFG_SOLID_BOX = 2 };
+/* addSolidBoundary with the SDF evaluated on the device at the cell centres
+ * (FP64, stored FP32): walls = everything outside the inner box
+ * [origin + h, origin + (n - 1) h]; sphere params (cx, cy, cz, r); box params
+ * (cx, cy, cz, sx, sy, sz) with full side lengths. */
+HFG_API int hfg_solver_add_analytic_solid(hfg_solver_t s, int type, const double params[6], const float vel[3]);
+
+/* A seeded dam break on the unit cube: walls, up to 4 static spheres, fluid
+ * in the cells whose centre lies below fluid_max on every axis, per_cell
+ * particles per fluid cell, PIC/FLIP mix, `steps` calls of update(). */
+typedef struct {
+  int res[3];
+  float dt;
+  float fluid_max[3];
+  int n_spheres;
+  float spheres[4][4];    /* centre x, y, z and radius */
+  int per_cell;
+  unsigned long long seed;
+  float cfl;
+  float mixing;           /* MixingCoefficient (PIC weight) */
+  int steps;
+  int keep_particles;     /* keep the final positions for hfg_server_particles */
+  hfg_options_t options;
+} hfg_scene_desc_t;
+
+typedef struct {
+  int status;             /* 0 queued, 1 running, 2 done, negative: the HFG_ERR_* it failed with */
+  int steps_done;
+  long long cells, particles, footprint_bytes;
+  double queue_ms;        /* submission -> admission */
+  double run_ms;          /* admission -> completion */
+  double step_ms_p50, step_ms_max;
+  hfg_stats_t last;       /* statistics of the last step */
+} hfg_request_info_t;
+
+typedef struct {
+  long long submitted, completed, failed, rejected;
+  double step_ms_p50, step_ms_p99;        /* over every step of every completed request */
+  double request_ms_p50, request_ms_p99;  /* submission -> completion */
+  double cell_steps;                      /* sum over completed requests of cells x steps */
+  double wall_s;                          /* first submission -> last completion */
+  long long peak_bytes, budget_bytes;
+  int peak_running, slots;
+} hfg_server_stats_t;
+
+typedef struct hfg_server_s* hfg_server_t;
+
+/* Device bytes a scene of this size holds while resident (the admission
+ * estimate of the server); host-only arithmetic. */
+HFG_API int hfg_scene_bytes(const int res[3], long long particles, int boundaries, int precond, long long* bytes);
+/* Upper bound of the particles a dam-break description seeds (fluid cells of
+ * the bbox, before solids are removed, x per_cell); host-only. */
+HFG_API int hfg_scene_particles_bound(const hfg_scene_desc_t* d, long long* particles);
+
+/* Continuous-batching server: `slots` worker threads on `device`, each owning
+ * the scene it runs (grids and particles resident on the device for all of
+ * its steps) on its own stream, so the steps of different scenes overlap on
+ * the GPU.  A queued request is admitted as soon as a slot is free and its
+ * footprint fits the remaining byte budget; smaller requests may pass a head
+ * that does not fit, unless the head has waited longer than 1 s.  A request
+ * whose footprint exceeds the whole budget is rejected at submission. */
+HFG_API int hfg_server_create(int device, int slots, long long budget_bytes, hfg_server_t* out);
+HFG_API int hfg_server_submit(hfg_server_t srv, const hfg_scene_desc_t* desc, long long* id);
+HFG_API int hfg_server_info(hfg_server_t srv, long long id, hfg_request_info_t* info);  /* non-blocking */
+HFG_API int hfg_server_wait(hfg_server_t srv, long long id, hfg_request_info_t* info);  /* until done */
+/* per-step latencies (ms) of a request; returns the count written */
+HFG_API int hfg_server_step_times(hfg_server_t srv, long long id, double* ms, int capacity);
+/* final particle positions (3n floats) of a done request with keep_particles */
+HFG_API int hfg_server_particles(hfg_server_t srv, long long id, float* pos, long long capacity);
+HFG_API int hfg_server_drain(hfg_server_t srv);  /* waits until every submitted request is done */
+HFG_API int hfg_server_stats(hfg_server_t srv, hfg_server_stats_t* st);
+HFG_API int hfg_server_destroy(hfg_server_t srv);  /* drains first */
+
 /* hfg_op_p2g_fc without any device allocation.  This entry point has no
  * counterpart in the reference.  It is for callers that may not allocate
  * device memory at call time (a fixed-memory real-time loop, or a host whose
