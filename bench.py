@@ -35,6 +35,7 @@ PKG = os.path.join(ROOT, "hybrid-fluid-simulation_b200")
 sys.path.insert(0, PKG)
 
 METRIC = "Mcell-steps/s at 256^3 (dam break, plain FP32 path)"
+CG_DRAM_BYTES_PER_CELL = (116.89e6 + 21.82e6 + 157.75e6 + 45.34e6) / 224 ** 3
 UNIT = "Mcell-steps/s"
 
 
@@ -48,6 +49,14 @@ def parse():
     ap.add_argument("--precond", default="jacobi", choices=["jacobi", "identity", "mg"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-sample-res", type=int, default=128)
+    ap.add_argument("--workload", default="dam-break", choices=["dam-break", "serve", "batch"],
+                    help="dam-break: the 256^3 headline line; serve: Poisson stream of mixed-size requests "
+                         "through the scene server vs each request run plain; batch: many uneven scenes at once")
+    ap.add_argument("--requests", type=int, default=100, help="serve/batch: number of scenes")
+    ap.add_argument("--rate", type=float, default=200.0, help="serve: arrivals per second")
+    ap.add_argument("--slots", type=int, default=16, help="serve/batch: concurrent scenes")
+    ap.add_argument("--scene-steps", type=int, default=10, help="serve/batch: steps per scene")
+    ap.add_argument("--no-plain", action="store_true", help="serve: skip the one-at-a-time comparison")
     return ap.parse_args()
 
 
@@ -174,10 +183,95 @@ def cpu_baseline_sample(n=64, steps=2):
             "sample": f"{steps} steps (after 1 warm-up) of the dam-break layout at {n}^3, FP64 oracle, {threads} threads"}
 
 
+def serve_requests(args, rng, batch=False):
+    """Request descriptions of the serving stream (C5) or the batch (C4)."""
+    import numpy as np
+    import hfgrid
+    out = []
+    for i in range(args.requests):
+        if batch:
+            # per-axis sizes U{32..128}, fluid fraction U(0.2, 0.5) as x < a, y < a with a = sqrt(frac)
+            res = tuple(int(v) for v in rng.integers(32, 129, 3))
+            a = float(np.sqrt(rng.uniform(0.2, 0.5)))
+            fluid, spheres = (a, a, 1.0), []
+        else:
+            # cubic, side log-uniform in [32, 256]; 0-3 spheres in the free region
+            n = int(round(float(np.exp(rng.uniform(np.log(32), np.log(256))))))
+            res = (n, n, n)
+            fluid = (0.4, 0.6, 1.0)
+            spheres = []
+            for _ in range(int(rng.integers(0, 4))):
+                r = float(rng.uniform(0.05, 0.15))
+                spheres.append((float(rng.uniform(0.45 + r, 0.95 - r)), float(rng.uniform(0.05 + r, 0.95 - r)),
+                                float(rng.uniform(0.05 + r, 0.95 - r)), r))
+        out.append(dict(res=res, spheres=spheres, fluid_max=fluid, seed=i))
+    return out
+
+
+def run_server(args, reqs, arrivals, slots, precond):
+    """Submit `reqs` at their arrival times (seconds from start) to a server
+    with `slots` concurrent scenes; returns its statistics."""
+    import hfgrid
+    srv = hfgrid.Server(slots=slots, budget_bytes=150 * 10**9)
+    t0 = time.perf_counter()
+    ids = []
+    for r, at in zip(reqs, arrivals):
+        dt = at - (time.perf_counter() - t0)
+        if dt > 0:
+            time.sleep(dt)
+        ids.append(srv.submit(hfgrid.scene_desc(r["res"], steps=args.scene_steps, spheres=r["spheres"],
+                                                fluid_max=r["fluid_max"], seed=r["seed"], precond=precond,
+                                                tol_mode=hfgrid.TOL_RELATIVE, tol=1e-6, max_iter=200)))
+    srv.drain()
+    st = srv.stats()
+    infos = [srv.info(i) for i in ids]
+    srv.close()
+    st["mcell_steps_per_s"] = st["cell_steps"] / max(st["wall_s"], 1e-9) / 1e6
+    st["failed_ids"] = [i for i, inf in zip(ids, infos) if inf["status"] != 2]
+    return st
+
+
+def run_serve(args):
+    """C5 (serve) or C4 (batch) through the scene server, one JSON line."""
+    import numpy as np
+    import hfgrid
+    hfgrid.init(0)
+    batch = args.workload == "batch"
+    rng = np.random.default_rng(2024)
+    reqs = serve_requests(args, rng, batch=batch)
+    if batch:
+        arrivals = [0.0] * len(reqs)
+    else:
+        arrivals = list(np.cumsum(rng.exponential(1.0 / args.rate, len(reqs))))
+    clocks = ClockSampler(0)
+    clocks.start()
+    mixed = run_server(args, reqs, arrivals, args.slots, hfgrid.PRECOND_MG)
+    clk = clocks.stop()
+    line = {
+        "metric": "Mcell-steps/s and step latency, " + ("batched uneven scenes" if batch else "served request stream"),
+        "value": mixed["mcell_steps_per_s"], "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
+        "dtype": "f32 (MG preconditioner with BF16 coarse levels, FP64 dots)", "data": "synthetic (seeded)",
+        "config": {"workload": ("C4 batch: %d scenes, axes U{32..128}, fluid fraction U(0.2,0.5), 8 ppc, %d steps"
+                                % (len(reqs), args.scene_steps)) if batch else
+                   ("C5 serve: %d requests, Poisson %.0f req/s, side log-uniform 32..256, 0-3 spheres, %d steps, "
+                    "150 GB budget" % (len(reqs), args.rate, args.scene_steps)),
+                   "slots": args.slots},
+        "served": mixed, "clocks": clk,
+    }
+    if not args.no_plain:
+        plain = run_server(args, reqs, arrivals, 1, hfgrid.PRECOND_JACOBI)
+        line["plain"] = plain
+        line["speedup_vs_plain"] = mixed["mcell_steps_per_s"] / max(plain["mcell_steps_per_s"], 1e-9)
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload != "dam-break":
+        run_serve(args)
         return
     import numpy as np
     import torch
@@ -280,6 +374,9 @@ def main():
         value = N * args.steps * world / (ms / 1e3) / 1e6
         algo_bytes = 25.0 * N  # compulsory bytes per CG iteration (d, x, r read + markers + x, r, d written)
         achieved = algo_bytes / (cg_ms / 1e3) / 1e9
+        # DRAM bytes per cell of one CG iteration (kCgDirection + kCgUpdate) from the ncu capture at 224^3
+        # (profiles/cg_kernels_224cubed_ncu.md), scaled by the cell count
+        traffic = CG_DRAM_BYTES_PER_CELL * N
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -291,7 +388,9 @@ def main():
                        "substeps_last": st["substeps"], "extrapolation_layers_last": st["extrapolation_layers"]},
             "roofline": {"bound": "hbm", "kernel": "CG iteration (kCgDirection + kCgUpdate)",
                          "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                         "traffic": None, "algorithmic_bytes_per_iter": algo_bytes, "ms_per_iter": cg_ms,
+                         "traffic": traffic, "traffic_source": "ncu dram__bytes_read+write at 224^3, per cell, "
+                                                                   "scaled to this grid",
+                         "algorithmic_bytes_per_iter": algo_bytes, "ms_per_iter": cg_ms,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback"},
             "clocks": clk,
             "gpu_launches": launches,

@@ -27,6 +27,7 @@ P2GSUM, G2PNEAREST, LINEAR, QUADRATIC, CUBIC = 0, 1, 2, 3, 4
 PRECOND_IDENTITY, PRECOND_JACOBI, PRECOND_MG = 0, 1, 2
 TOL_REFERENCE, TOL_RELATIVE = 0, 1
 HFG_OK, HFG_ERR_NOT_CONVERGED = 0, -5
+SOLID_WALLS, SOLID_SPHERE, SOLID_BOX = 0, 1, 2
 
 
 class HfgError(RuntimeError):
@@ -55,6 +56,41 @@ class Stats(C.Structure):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "stage_ms"}
         d["stage_ms"] = list(self.stage_ms)
         return d
+
+
+class SceneDesc(C.Structure):
+    """hfg_scene_desc_t: a seeded dam break on the unit cube."""
+    _fields_ = [
+        ("res", C.c_int * 3), ("dt", C.c_float), ("fluid_max", C.c_float * 3), ("n_spheres", C.c_int),
+        ("spheres", (C.c_float * 4) * 4), ("per_cell", C.c_int), ("seed", C.c_ulonglong), ("cfl", C.c_float),
+        ("mixing", C.c_float), ("steps", C.c_int), ("keep_particles", C.c_int), ("options", Options),
+    ]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [
+        ("status", C.c_int), ("steps_done", C.c_int), ("cells", C.c_longlong), ("particles", C.c_longlong),
+        ("footprint_bytes", C.c_longlong), ("queue_ms", C.c_double), ("run_ms", C.c_double),
+        ("step_ms_p50", C.c_double), ("step_ms_max", C.c_double), ("last", Stats),
+    ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_longlong), ("completed", C.c_longlong), ("failed", C.c_longlong),
+        ("rejected", C.c_longlong), ("step_ms_p50", C.c_double), ("step_ms_p99", C.c_double),
+        ("request_ms_p50", C.c_double), ("request_ms_p99", C.c_double), ("cell_steps", C.c_double),
+        ("wall_s", C.c_double), ("peak_bytes", C.c_longlong), ("budget_bytes", C.c_longlong),
+        ("peak_running", C.c_int), ("slots", C.c_int),
+    ]
+
+
+def _struct_dict(st) -> dict:
+    out = {}
+    for k, _ in st._fields_:
+        v = getattr(st, k)
+        out[k] = v.as_dict() if isinstance(v, Stats) else v
+    return out
 
 
 _lib = None
@@ -130,6 +166,18 @@ def _signatures(lib):
         "hfg_op_sl_advect_cc": (C.c_int, [I3, F3, F3, VP, VP, VP, VP, C.c_float, C.c_int, VP, VP]),
         "hfg_op_fluid_domain_from_bbox": (C.c_int, [I3, F3, F3, F3, F3, VP, VP]),
         "hfg_op_build_fluid_sdf": (C.c_int, [I3, VP, VP, C.c_int, VP]),
+        "hfg_solver_add_analytic_solid": (C.c_int, [S, C.c_int, C.POINTER(C.c_double), F3]),
+        "hfg_scene_bytes": (C.c_int, [I3, C.c_longlong, C.c_int, C.c_int, C.POINTER(C.c_longlong)]),
+        "hfg_scene_particles_bound": (C.c_int, [C.POINTER(SceneDesc), C.POINTER(C.c_longlong)]),
+        "hfg_server_create": (C.c_int, [C.c_int, C.c_int, C.c_longlong, C.POINTER(C.c_void_p)]),
+        "hfg_server_submit": (C.c_int, [VP, C.POINTER(SceneDesc), C.POINTER(C.c_longlong)]),
+        "hfg_server_info": (C.c_int, [VP, C.c_longlong, C.POINTER(RequestInfo)]),
+        "hfg_server_wait": (C.c_int, [VP, C.c_longlong, C.POINTER(RequestInfo)]),
+        "hfg_server_step_times": (C.c_int, [VP, C.c_longlong, C.POINTER(C.c_double), C.c_int]),
+        "hfg_server_particles": (C.c_int, [VP, C.c_longlong, PF, C.c_longlong]),
+        "hfg_server_drain": (C.c_int, [VP]),
+        "hfg_server_stats": (C.c_int, [VP, C.POINTER(ServerStats)]),
+        "hfg_server_destroy": (C.c_int, [VP]),
         "hfg_op_seed_particles": (C.c_int, [I3, F3, F3, VP, VP, C.c_int, C.c_ulonglong, VP, C.c_longlong,
                                             C.POINTER(C.c_longlong), VP]),
     }
@@ -230,6 +278,12 @@ class Solver:
         a = np.ascontiguousarray(sdf, dtype=np.float32).reshape(-1)
         assert a.size == self.n_cells
         _check(lib().hfg_solver_add_solid_boundary(self._h, _fptr(a), _f3(vel)))
+
+    def add_analytic_solid(self, kind: int, params=(0.0,) * 6, vel=(0.0, 0.0, 0.0)):
+        """SOLID_WALLS / SOLID_SPHERE (cx, cy, cz, r) / SOLID_BOX (cx, cy, cz,
+        sx, sy, sz): the SDF is evaluated on the device."""
+        p = (C.c_double * 6)(*(list(params) + [0.0] * (6 - len(params))))
+        _check(lib().hfg_solver_add_analytic_solid(self._h, kind, p, _f3(vel)))
 
     def set_boundary_velocity(self, index: int, vel):
         _check(lib().hfg_solver_set_boundary_velocity(self._h, index, _f3(vel)))
@@ -499,3 +553,84 @@ def op_seed_particles(res, origin, spacing, fluid_sdf, solid_sdf, per_cell, seed
     _check(lib().hfg_op_seed_particles(_i3(res), _f3(origin), _f3(spacing), _ptr(fluid_sdf), _ptr(solid_sdf),
                                        per_cell, seed, _ptr(pos), capacity, C.byref(n), _stream(stream)))
     return n.value
+
+
+# ---------------------------------------------------------------- server --
+def scene_desc(res, steps=10, spheres=(), fluid_max=(0.4, 0.6, 1.0), per_cell=8, seed=0, dt=1.0 / 60.0,
+               cfl=1.0, mixing=0.05, keep_particles=False, **options) -> SceneDesc:
+    """A dam-break request: walls, up to 4 static spheres (cx, cy, cz, r),
+    fluid below fluid_max; `options` fill hfg_options_t (precond, tol, ...)."""
+    d = SceneDesc()
+    d.res[:] = [int(r) for r in res]
+    d.dt = dt
+    d.fluid_max[:] = [float(f) for f in fluid_max]
+    d.n_spheres = len(spheres)
+    for i, sp in enumerate(spheres):
+        d.spheres[i][:] = [float(v) for v in sp]
+    d.per_cell, d.seed, d.cfl, d.mixing, d.steps = per_cell, seed, cfl, mixing, steps
+    d.keep_particles = int(keep_particles)
+    o = default_options()
+    for k, v in options.items():
+        setattr(o, k, v)
+    d.options = o
+    return d
+
+
+def scene_bytes(res, particles, boundaries=1, precond=PRECOND_JACOBI) -> int:
+    out = C.c_longlong()
+    _check(lib().hfg_scene_bytes(_i3(res), particles, boundaries, precond, C.byref(out)))
+    return out.value
+
+
+class Server:
+    """hfg_server_*: continuous batching of dam-break requests on one GPU."""
+
+    def __init__(self, slots: int = 8, budget_bytes: int = 150 * 10**9, device: int = 0):
+        h = C.c_void_p()
+        _check(lib().hfg_server_create(device, slots, budget_bytes, C.byref(h)))
+        self._h = h
+
+    def submit(self, desc: SceneDesc) -> int:
+        rid = C.c_longlong()
+        _check(lib().hfg_server_submit(self._h, C.byref(desc), C.byref(rid)))
+        return rid.value
+
+    def info(self, rid: int, wait: bool = False) -> dict:
+        inf = RequestInfo()
+        f = lib().hfg_server_wait if wait else lib().hfg_server_info
+        _check(f(self._h, rid, C.byref(inf)))
+        return _struct_dict(inf)
+
+    def wait(self, rid: int) -> dict:
+        return self.info(rid, wait=True)
+
+    def step_times(self, rid: int, cap: int = 4096):
+        buf = (C.c_double * cap)()
+        n = lib().hfg_server_step_times(self._h, rid, buf, cap)
+        if n < 0:
+            _check(n)
+        return list(buf[:n])
+
+    def particles(self, rid: int, n: int) -> np.ndarray:
+        out = np.empty((n, 3), np.float32)
+        _check(lib().hfg_server_particles(self._h, rid, _fptr(out), 3 * n))
+        return out
+
+    def drain(self):
+        _check(lib().hfg_server_drain(self._h))
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().hfg_server_stats(self._h, C.byref(st)))
+        return _struct_dict(st)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _check(lib().hfg_server_destroy(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
