@@ -127,9 +127,19 @@ cudaError_t launchCgDirection(const Dim3i& cg, float sx, float sy, float sz, con
 cudaError_t launchCgUpdate(const Dim3i& cg, float sx, float sy, float sz, const CUtensorMap& mP, const CUtensorMap& mR,
                            const CUtensorMap& mX, const CUtensorMap& mCode, const float* p, float* x, float* r,
                            double* partials, CgState* st, int precond, cudaStream_t s);
+// Divergence residual of the projected velocity over the fluid cells:
+// *sumOut = sum b^2 (FP64), ticketAndMax[1] = bits of max |b|.  `scratch`
+// holds 2 * divergenceBlocks() doubles.
+inline int divergenceBlocks() { return 1024; }
+cudaError_t launchDivergenceNorm(const Geom& g, ConstFaceField v, const SolidVelTable& svTab,
+                                 const uint8_t* markers, double* scratch, unsigned* ticketAndMax, double* sumOut,
+                                 cudaStream_t s);
 // p pitched
 cudaError_t launchGradient(const Geom& g, float gx, float gy, float gz, const uint8_t* markers, const float* p,
                            FaceField v, ConstFaceField svArr, const SolidVelTable& svTab, cudaStream_t s);
+// Resolves the launch shapes of every CG kernel variant (occupancy queries) so
+// that no query runs while a stream is being captured.
+void cgWarmLaunchCache();
 // doubles of reduction scratch the CG kernels need on grid `r`
 int cgPartialsNeeded(const Dim3i& r);
 

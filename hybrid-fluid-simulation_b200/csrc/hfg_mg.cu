@@ -24,6 +24,7 @@
 #include <algorithm>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+#include <functional>
 #include <vector>
 
 #include "hfg_solver.h"
@@ -276,6 +277,7 @@ struct Multigrid {
   DArray<float> p[2];
   DArray<double> partials;
   CUtensorMap zH[2], pH[2];          // halo tensor maps of z0a / z0b and p[0] / p[1]
+  long long chunkLaunches = 0;       // kernels in one captured chunk of CG iterations
   const Code* code0 = nullptr;
   float s0[3] = {0, 0, 0};
   ~Multigrid() {
@@ -488,13 +490,15 @@ void mgSetup(Multigrid* m, const Dim3i& r, const uint8_t* mk0, const Code* code,
 // x = 0 and ||b||^2.  Iterations are launched in chunks; every kernel returns
 // immediately once the state says done.
 void mgRunCg(Multigrid* m, const Dim3i& cg, float sx, float sy, float sz, const CgMaps& maps, const Code* code, float* x,
-             float* rvec, CgState* st, CgState* stHost, cudaStream_t s, long long& launches) {
+             float* rvec, CgState* st, CgState* stHost, cudaStream_t s, long long& launches,
+             const std::function<cudaGraphExec_t(const std::function<void()>&)>& capture, cudaGraphExec_t* chunk) {
   check(cudaMemsetAsync(m->p[0].p, 0, m->p[0].bytes(), s), "memset");
-  const float* z = mgVcycle(m, rvec, st, s, launches);  // z0 = V(b), rz = b.z0
-  int it = 0;
-  const int chunk = 4;
-  for (;;) {
-    for (int k = 0; k < chunk; ++k, ++it) {
+  const float* z0 = mgVcycle(m, rvec, st, s, launches);  // z0 = V(b), rz = b.z0
+  const int kChunk = 4;  // even: every chunk starts on p[0]
+  auto body = [&] {
+    const float* z = z0;
+    long long before = launches;
+    for (int it = 0; it < kChunk; ++it) {
       const int po = it & 1, pn = (it + 1) & 1;
       const int zi = z == m->z0a.p ? 0 : 1;
       check(launchCgDirection(cg, sx, sy, sz, m->zH[zi], m->pH[po], maps.codeH, code, z, m->p[po].p, m->p[pn].p,
@@ -506,6 +510,14 @@ void mgRunCg(Multigrid* m, const Dim3i& cg, float sx, float sy, float sz, const 
       launches += 2;
       z = mgVcycle(m, rvec, st, s, launches);
     }
+    m->chunkLaunches = launches - before;
+    // the V-cycle always leaves its result in the same level-0 buffer
+    if (z != z0) throw CudaError("multigrid: V-cycle output buffer changed between iterations", HFG_ERR_STATE);
+  };
+  if (!*chunk) *chunk = capture(body);
+  for (;;) {
+    check(cudaGraphLaunch(*chunk, s), "cg chunk");
+    launches += m->chunkLaunches;
     check(cudaMemcpyAsync(stHost, st, sizeof(CgState), cudaMemcpyDeviceToHost, s), "read cg state");
     check(cudaStreamSynchronize(s), "cg sync");
     if (stHost->done) break;

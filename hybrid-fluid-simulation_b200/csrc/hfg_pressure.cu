@@ -168,6 +168,68 @@ cudaError_t launchApplyA(const Dim3i& r, float sx, float sy, float sz, const Cod
 // RHS: divergence (FieldMathTool.cu:370-395) + solid terms
 // (EulerSolverTool.cu:128-197), fused with the CG set-up of
 // CuMatrixFreePCG.cpp:22-37 (x0 = 0 so r = b).
+// b of one cell: -div u plus the solid-face terms (FieldMathTool.cu:370-395,
+// EulerSolverTool.cu:128-197), in the reference's operation order; 0 for
+// non-fluid cells.
+__device__ __forceinline__ float rhsAt(const Geom& g, const ConstFaceField& v, const ConstFaceField& svArr,
+                                       const SolidVelTable& svTab, const uint8_t* __restrict__ mk, int x, int y,
+                                       int z) {
+  const Dim3i R = g.r;
+  const long long plane = (long long)R.x * R.y;
+  const long long c = (long long)z * plane + (long long)y * R.x + x;
+  if (mk[c] != kFluid) return 0.f;
+  const float ix = 1.0f / g.hx, iy = 1.0f / g.hy, iz = 1.0f / g.hz;
+  const long long fxRow = R.x + 1, fxPlane = (long long)(R.x + 1) * R.y;
+  const long long fyPlane = (long long)R.x * (R.y + 1);
+  long long uL = (long long)z * fxPlane + (long long)y * fxRow + x, uR = uL + 1;
+  long long vD = (long long)z * fyPlane + (long long)y * R.x + x, vU = vD + R.x;
+  long long wB = c, wF = c + plane;
+  float L = v.c[0][uL], Rr = v.c[0][uR], D = v.c[1][vD], U = v.c[1][vU], B = v.c[2][wB], F = v.c[2][wF];
+  float div = __fadd_rn(__fadd_rn(__fdiv_rn(__fsub_rn(Rr, L), g.hx), __fdiv_rn(__fsub_rn(U, D), g.hy)),
+                        __fdiv_rn(__fsub_rn(F, B), g.hz));
+  float b = -div;
+  uint8_t me = svTab.solidIdx ? svTab.solidIdx[c] : 0;
+  auto sv = [&](int axis, long long f, long long nb, bool nbIsHi) -> float {
+    if (svArr.c[0]) return svArr.c[axis][f];
+    uint8_t o = svTab.solidIdx[nb];
+    return nbIsHi ? solidFaceVel(svTab, me, o, axis) : solidFaceVel(svTab, o, me, axis);
+  };
+  long long cl = x > 0 ? c - 1 : c, cr = x + 1 < R.x ? c + 1 : c;
+  long long cd = y > 0 ? c - R.x : c, cu = y + 1 < R.y ? c + R.x : c;
+  long long cb = z > 0 ? c - plane : c, cf = z + 1 < R.z ? c + plane : c;
+  if (mk[cl] == kSolid) b = __fsub_rn(b, __fmul_rn(ix, __fsub_rn(L, sv(0, uL, cl, false))));
+  if (mk[cr] == kSolid) b = __fadd_rn(b, __fmul_rn(ix, __fsub_rn(Rr, sv(0, uR, cr, true))));
+  if (mk[cd] == kSolid) b = __fsub_rn(b, __fmul_rn(iy, __fsub_rn(D, sv(1, vD, cd, false))));
+  if (mk[cu] == kSolid) b = __fadd_rn(b, __fmul_rn(iy, __fsub_rn(U, sv(1, vU, cu, true))));
+  if (mk[cb] == kSolid) b = __fsub_rn(b, __fmul_rn(iz, __fsub_rn(B, sv(2, wB, cb, false))));
+  if (mk[cf] == kSolid) b = __fadd_rn(b, __fmul_rn(iz, __fsub_rn(F, sv(2, wF, cf, true))));
+  return b;
+}
+
+// Divergence residual of a projected field: sum of b^2 over the fluid cells
+// (FP64, last-block reduction) and max |b| (ordered-bits atomic max).
+__global__ void kDivergenceNorm(Geom g, ConstFaceField v, ConstFaceField svArr, SolidVelTable svTab,
+                                const uint8_t* __restrict__ mk, double* partials, unsigned* ticket,
+                                double* sumOut, unsigned* maxBits) {
+  double s2 = 0.0, dummy = 0.0;
+  float mx = 0.f;
+  const long long n = g.r.size();
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(c % g.r.x);
+    const long long t = c / g.r.x;
+    const int y = (int)(t % g.r.y), z = (int)(t / g.r.y);
+    float b = rhsAt(g, v, svArr, svTab, mk, x, y, z);
+    s2 += (double)b * (double)b;
+    mx = fmaxf(mx, fabsf(b));
+  }
+  mx = warpMaxF(mx);
+  if ((threadIdx.x & 31) == 0) atomicMax(maxBits, __float_as_uint(mx));
+  if (gridSum2(s2, dummy, partials, ticket) && flatTid() == 0) {
+    *sumOut = s2;
+    *ticket = 0;
+  }
+}
+
 template <int PC>
 __global__ void __launch_bounds__(TX* TY) kRhsInit(Geom g, ConstFaceField v, ConstFaceField svArr, SolidVelTable svTab,
                                                    const uint8_t* __restrict__ mk, const Code* __restrict__ code,
@@ -176,7 +238,6 @@ __global__ void __launch_bounds__(TX* TY) kRhsInit(Geom g, ConstFaceField v, Con
                                                    double* partials, CgState* st, int zPer) {
   const Dim3i R = g.r;
   const int px = cgPitch(R.x);
-  const float ix = 1.0f / g.hx, iy = 1.0f / g.hy, iz = 1.0f / g.hz;
   int x = blockIdx.x * TX + threadIdx.x, y = blockIdx.y * TY + threadIdx.y;
   double bb = 0.0, rzs = 0.0;
   if (x >= R.x && x < px && y < R.y) {  // pitch padding: inert cells
@@ -191,35 +252,9 @@ __global__ void __launch_bounds__(TX* TY) kRhsInit(Geom g, ConstFaceField v, Con
   if (x < R.x && y < R.y) {
     int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, R.z);
     const long long plane = (long long)R.x * R.y;
-    const long long fxRow = R.x + 1, fxPlane = (long long)(R.x + 1) * R.y;
-    const long long fyPlane = (long long)R.x * (R.y + 1);
     for (int z = z0; z < z1; ++z) {
       long long c = (long long)z * plane + (long long)y * R.x + x;
-      float b = 0.f;
-      if (mk[c] == kFluid) {
-        long long uL = (long long)z * fxPlane + (long long)y * fxRow + x, uR = uL + 1;
-        long long vD = (long long)z * fyPlane + (long long)y * R.x + x, vU = vD + R.x;
-        long long wB = c, wF = c + plane;
-        float L = v.c[0][uL], Rr = v.c[0][uR], D = v.c[1][vD], U = v.c[1][vU], B = v.c[2][wB], F = v.c[2][wF];
-        float div = __fadd_rn(__fadd_rn(__fdiv_rn(__fsub_rn(Rr, L), g.hx), __fdiv_rn(__fsub_rn(U, D), g.hy)),
-                              __fdiv_rn(__fsub_rn(F, B), g.hz));
-        b = -div;
-        uint8_t me = svTab.solidIdx ? svTab.solidIdx[c] : 0;
-        auto sv = [&](int axis, long long f, long long nb, bool nbIsHi) -> float {
-          if (svArr.c[0]) return svArr.c[axis][f];
-          uint8_t o = svTab.solidIdx[nb];
-          return nbIsHi ? solidFaceVel(svTab, me, o, axis) : solidFaceVel(svTab, o, me, axis);
-        };
-        long long cl = x > 0 ? c - 1 : c, cr = x + 1 < R.x ? c + 1 : c;
-        long long cd = y > 0 ? c - R.x : c, cu = y + 1 < R.y ? c + R.x : c;
-        long long cb = z > 0 ? c - plane : c, cf = z + 1 < R.z ? c + plane : c;
-        if (mk[cl] == kSolid) b = __fsub_rn(b, __fmul_rn(ix, __fsub_rn(L, sv(0, uL, cl, false))));
-        if (mk[cr] == kSolid) b = __fadd_rn(b, __fmul_rn(ix, __fsub_rn(Rr, sv(0, uR, cr, true))));
-        if (mk[cd] == kSolid) b = __fsub_rn(b, __fmul_rn(iy, __fsub_rn(D, sv(1, vD, cd, false))));
-        if (mk[cu] == kSolid) b = __fadd_rn(b, __fmul_rn(iy, __fsub_rn(U, sv(1, vU, cu, true))));
-        if (mk[cb] == kSolid) b = __fsub_rn(b, __fmul_rn(iz, __fsub_rn(B, sv(2, wB, cb, false))));
-        if (mk[cf] == kSolid) b = __fadd_rn(b, __fmul_rn(iz, __fsub_rn(F, sv(2, wF, cf, true))));
-      }
+      float b = rhsAt(g, v, svArr, svTab, mk, x, y, z);
       if (bOut) bOut[c] = b;
       long long o = ((long long)z * R.y + y) * px + x;
       r[o] = b;
@@ -251,6 +286,17 @@ cudaError_t launchRhsInit(const Geom& gm, ConstFaceField v, ConstFaceField svArr
   else
     kRhsInit<0><<<g.grid, g.block, 0, s>>>(gm, v, svArr, svTab, markers, code, ax, ay, az, b, r, x, p, partials, st,
                                            g.zPer);
+  return cudaGetLastError();
+}
+
+cudaError_t launchDivergenceNorm(const Geom& g, ConstFaceField v, const SolidVelTable& svTab,
+                                 const uint8_t* markers, double* scratch, unsigned* ticketAndMax, double* sumOut,
+                                 cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(ticketAndMax, 0, 2 * sizeof(unsigned), s);
+  if (e != cudaSuccess) return e;
+  ConstFaceField none{{nullptr, nullptr, nullptr}};
+  kDivergenceNorm<<<divergenceBlocks(), 256, 0, s>>>(g, v, none, svTab, markers, scratch, ticketAndMax, sumOut,
+                                                     ticketAndMax + 1);
   return cudaGetLastError();
 }
 
@@ -667,6 +713,15 @@ cudaError_t makeCgMaps(const Dim3i& cg, const Code* code, const float* r, const 
   if ((e = encodeMap(&m->xI, x, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cg, CTX, CTY)) != cudaSuccess) return e;
   if ((e = encodeMap(&m->pH[0], p0, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cg, FW, FH)) != cudaSuccess) return e;
   return encodeMap(&m->pH[1], p1, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cg, FW, FH);
+}
+
+void cgWarmLaunchCache() {
+  residentBlocks((const void*)kCgDirection<0>);
+  residentBlocks((const void*)kCgDirection<1>);
+  residentBlocks((const void*)kCgDirection<2>);
+  residentBlocks((const void*)kCgUpdate<0>);
+  residentBlocks((const void*)kCgUpdate<1>);
+  residentBlocks((const void*)kCgUpdate<2>);
 }
 
 int cgPartialsNeeded(const Dim3i& r) {

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <mutex>
 
 #include "hfg_solver.h"
@@ -54,7 +55,8 @@ void mgDestroy(Multigrid* m);
 void mgSetup(Multigrid* m, const Dim3i& r, const uint8_t* mk0, const Code* code, float sx, float sy, float sz,
              cudaStream_t s, long long& launches);
 void mgRunCg(Multigrid* m, const Dim3i& cg, float sx, float sy, float sz, const CgMaps& maps, const Code* code, float* x,
-             float* rvec, CgState* st, CgState* stHost, cudaStream_t s, long long& launches);
+             float* rvec, CgState* st, CgState* stHost, cudaStream_t s, long long& launches,
+             const std::function<cudaGraphExec_t(const std::function<void()>&)>& capture, cudaGraphExec_t* chunk);
 
 GridSolver::GridSolver(float dt, Dim3i res, const float origin[3], const float spacing[3]) {
   if (res.x <= 0 || res.y <= 0 || res.z <= 0) throw CudaError("resolution must be positive", HFG_ERR_INVALID);
@@ -117,6 +119,7 @@ GridSolver::GridSolver(float dt, Dim3i res, const float origin[3], const float s
 GridSolver::~GridSolver() {
   if (stream_) cudaStreamSynchronize(stream_);
   for (auto* b : bsdf_) delete b;
+  dropGraphs();
   if (mg_) mgDestroy(mg_);
   pinnedPut(cgHost_);
   pinnedPut(subHost_);
@@ -282,6 +285,7 @@ void GridSolver::setOptions(const hfg_options_t& o) {
                    (!mg_ || o.mg_levels != opt_.mg_levels || o.mg_smooth != opt_.mg_smooth || o.mg_half != opt_.mg_half);
   opt_ = o;
   if (mgChanged) {
+    dropGraphs();
     if (mg_) mgDestroy(mg_);
     mg_ = mgCreate(cg_, o.mg_levels, o.mg_smooth, o.mg_half != 0, stream_);
   }
@@ -428,15 +432,52 @@ void GridSolver::cgIteration(int it, float sx, float sy, float sz, int pc) {
            "cg update");
 }
 
+template <class F> cudaGraphExec_t GridSolver::capture(F&& f) {
+  cgWarmLaunchCache();  // launch-shape queries happen before the capture
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t e = nullptr;
+  const long long saved = launches_;
+  check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
+  try {
+    f();
+  } catch (...) {
+    cudaStreamEndCapture(stream_, &g);
+    if (g) cudaGraphDestroy(g);
+    launches_ = saved;
+    throw;
+  }
+  check(cudaStreamEndCapture(stream_, &g), "end capture");
+  launches_ = saved;
+  cudaError_t r = cudaGraphInstantiate(&e, g, 0);
+  cudaGraphDestroy(g);
+  check(r, "graph instantiate");
+  return e;
+}
+
+void GridSolver::dropGraphs() {
+  for (auto& g : cgGraph_)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+}
+
 void GridSolver::runCg() {
   const float sx = dt_ / (1.0f * g_.hx * g_.hx), sy = dt_ / (1.0f * g_.hy * g_.hy), sz = dt_ / (1.0f * g_.hz * g_.hz);
   if (opt_.precond == HFG_PRECOND_MG) {
-    mgRunCg(mg_, cg_, sx, sy, sz, maps_, code_.p, cgx_.p, cgr_.p, cgState_.p, cgHost_, stream_, launches_);
+    auto cap = [this](const std::function<void()>& f) { return capture(f); };
+    mgRunCg(mg_, cg_, sx, sy, sz, maps_, code_.p, cgx_.p, cgr_.p, cgState_.p, cgHost_, stream_, launches_, cap,
+            &cgGraph_[2]);
   } else {
-    int it = 0;
     const int pc = opt_.precond == HFG_PRECOND_JACOBI ? 1 : 0;
+    // kCgChunk is even, so every chunk starts on the same p buffer
+    if (!cgGraph_[pc])
+      cgGraph_[pc] = capture([&] {
+        for (int k = 0; k < kCgChunk; ++k) cgIteration(k, sx, sy, sz, pc);
+      });
     for (;;) {
-      for (int k = 0; k < kCgChunk; ++k, ++it) cgIteration(it, sx, sy, sz, pc);
+      check(cudaGraphLaunch(cgGraph_[pc], stream_), "cg chunk");
+      launches_ += 2 * kCgChunk;
       check(cudaMemcpyAsync(cgHost_, cgState_.p, sizeof(CgState), cudaMemcpyDeviceToHost, stream_), "read cg state");
       check(cudaStreamSynchronize(stream_), "cg sync");
       if (cgHost_->done) break;
@@ -484,6 +525,23 @@ void GridSolver::computePressure() {
   launched(launchGradient(g_, dt_ / (1.0f * g_.hx), dt_ / (1.0f * g_.hy), dt_ / (1.0f * g_.hz), markers_.p, cgx_.p,
                           mvel(ni), noneSv, solidTable(), stream_),
            "gradient");
+  if (opt_.report_divergence) {
+    const int nb = divergenceBlocks();
+    divScratch_.alloc(2 * nb + 1, stream_);
+    divTicket_.alloc(2, stream_);
+    launched(launchDivergenceNorm(g_, cvel(ni), solidTable(), markers_.p, divScratch_.p, divTicket_.p,
+                                  divScratch_.p + 2 * nb, stream_),
+             "divergence");
+    double sum = 0.0;
+    unsigned bits = 0;
+    check(cudaMemcpyAsync(&sum, divScratch_.p + 2 * nb, sizeof(double), cudaMemcpyDeviceToHost, stream_), "read");
+    check(cudaMemcpyAsync(&bits, divTicket_.p + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_), "read");
+    check(cudaStreamSynchronize(stream_), "sync");
+    divL2_ = std::sqrt(sum);
+    float mx;
+    std::memcpy(&mx, &bits, sizeof(mx));
+    divMax_ = mx;
+  }
   stageEnd(6);
 }
 
@@ -642,6 +700,8 @@ void GridSolver::getParticles(float* pos, float* vel) {
 void GridSolver::getStats(hfg_stats_t* st) {
   std::memset(st, 0, sizeof(*st));
   st->cg_iterations = cgIters_;
+  st->divergence_l2 = divL2_;
+  st->divergence_max = divMax_;
   st->cg_residual = cgResid_;
   st->cg_rhs_norm = cgBnorm_;
   st->cg_converged = cgConverged_;

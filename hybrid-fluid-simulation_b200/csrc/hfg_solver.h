@@ -141,6 +141,9 @@ class GridSolver {
   void computePressure();
   void runCg();
   void cgIteration(int it, float sx, float sy, float sz, int pc);
+  // Records what f() launches on the solver's stream as an executable graph.
+  template <class F> cudaGraphExec_t capture(F&& f);
+  void dropGraphs();
   void extrapolate();
   void forcesTerms(float gv[3], bool& doG, float ev[3], bool& doE) const;
   int cur() const { return bufferFlag_ ? 1 : 0; }  // velocity/colour/domain "current" buffer
@@ -197,9 +200,15 @@ class GridSolver {
   long long cgIters_ = 0;
   double cgResid_ = 0, cgBnorm_ = 0;
   int cgConverged_ = 0, substeps_ = 0, extrapDepth_ = 0;
+  double divL2_ = 0, divMax_ = 0;
+  DArray<double> divScratch_;     // with report_divergence: reduction partials + sum
+  DArray<unsigned> divTicket_;
   long long fluidCells_ = -1;
 
   Multigrid* mg_ = nullptr;
+  // one chunk of CG iterations as a CUDA graph, per preconditioner (identity,
+  // Jacobi, multigrid): replayed until the device-side state says done
+  cudaGraphExec_t cgGraph_[3] = {nullptr, nullptr, nullptr};
 
   bool timing_ = false;
   cudaEvent_t ev_[16] = {};

@@ -40,7 +40,7 @@ class Options(C.Structure):
     _fields_ = [
         ("precond", C.c_int), ("tol_mode", C.c_int), ("tol", C.c_double), ("max_iter", C.c_longlong),
         ("clamp_mode", C.c_int), ("advect_scalars", C.c_int), ("extrapolation_layers", C.c_int),
-        ("mg_levels", C.c_int), ("mg_smooth", C.c_int), ("mg_half", C.c_int),
+        ("mg_levels", C.c_int), ("mg_smooth", C.c_int), ("mg_half", C.c_int), ("report_divergence", C.c_int),
     ]
 
 
@@ -49,7 +49,7 @@ class Stats(C.Structure):
         ("cg_iterations", C.c_longlong), ("cg_residual", C.c_double), ("cg_rhs_norm", C.c_double),
         ("cg_converged", C.c_int), ("substeps", C.c_int), ("extrapolation_layers", C.c_int),
         ("sim_time", C.c_double), ("num_particles", C.c_longlong), ("fluid_cells", C.c_longlong),
-        ("stage_ms", C.c_float * 8),
+        ("stage_ms", C.c_float * 8), ("divergence_l2", C.c_double), ("divergence_max", C.c_double),
     ]
 
     def as_dict(self) -> dict:

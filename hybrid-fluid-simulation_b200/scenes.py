@@ -133,6 +133,43 @@ def dam_break_256(seed: int = 0, n: int = 256) -> Scene:
     return Scene(res=(n, n, n), solids=boxes, seed=seed, name=f"dam-break {n}^3, two boxes")
 
 
+@dataclasses.dataclass
+class SinePath:
+    """centre(t) = c + amp * sin(2 pi t / period + phase) * axis."""
+    c: Tuple[float, float, float]
+    phase: float
+    axis: Tuple[float, float, float]
+    amp: float = 0.1
+    period: float = 2.0
+
+    def centre(self, t: float):
+        s = self.amp * math.sin(2 * math.pi * t / self.period + self.phase)
+        return tuple(ci + s * ai for ci, ai in zip(self.c, self.axis))
+
+    def velocity(self, t: float):
+        w = 2 * math.pi / self.period
+        s = self.amp * w * math.cos(w * t + self.phase)
+        return tuple(s * ai for ai in self.axis)
+
+
+def moving_boxes(res=(512, 256, 512), seed: int = 0, n_boxes: int = 3):
+    """The moving-solid dam break: walls, the usual fluid block, and `n_boxes`
+    boxes of side 0.2 on the floor moving on seeded sinusoidal paths
+    (amplitude 0.1, period 2 s, axis x or z, phase U[0, 2 pi)).  Returns the
+    scene (boxes at their t = 0 positions) and the paths."""
+    rng = np.random.default_rng(seed)
+    h = 1.0 / res[1]
+    paths, solids = [], []
+    for _ in range(n_boxes):
+        c = (float(rng.uniform(0.6, 0.8)), 0.1 + h, float(rng.uniform(0.25, 0.75)))
+        axis = (1.0, 0.0, 0.0) if rng.random() < 0.5 else (0.0, 0.0, 1.0)
+        path = SinePath(c, float(rng.uniform(0.0, 2 * math.pi)), axis)
+        paths.append(path)
+        solids.append(Solid("box", path.centre(0.0), (0.2, 0.2, 0.2), path.velocity(0.0)))
+    sc = Scene(res=tuple(res), solids=solids, seed=seed, name=f"moving boxes {res[0]}x{res[1]}x{res[2]}")
+    return sc, paths
+
+
 def gpu_solver(scene: Scene, precond: int = 1, tol_mode: int = 1, tol: float = 1e-6, max_iter: int = 200,
                advect_scalars: bool = False, clamp_mode: int = 1, kind: int = 3, **extra):
     """Build the scene in an hfgrid.Solver: walls + solids, bbox fluid domain,

@@ -69,6 +69,7 @@ typedef struct {
   int mg_levels;          /* multigrid levels for HFG_PRECOND_MG (0 = auto) */
   int mg_smooth;          /* smoothing sweeps per level (0 = default) */
   int mg_half;            /* 1: multigrid smoothing stores in half precision */
+  int report_divergence;  /* 1: measure the divergence residual of every projection */
 } hfg_options_t;
 
 typedef struct {
@@ -83,6 +84,10 @@ typedef struct {
   long long fluid_cells;
   float stage_ms[8];        /* boundaries, advection, forces, markers, rhs,
                                cg, gradient, extrapolation (when timing on) */
+  double divergence_l2;     /* with report_divergence: ||b(u)||_2 over the fluid
+                               cells after the projection (b as the RHS: -div u
+                               plus the solid-face terms, 1/s) */
+  double divergence_max;    /* max |b(u)| over the fluid cells after the projection */
 } hfg_stats_t;
 
 /* ---- library ---------------------------------------------------------- */

@@ -1282,6 +1282,13 @@ template <class T> static void sAddBoundary(OrcSolver* S, const float* sdf, floa
   b.vel = V3<T>{(T)vx, (T)vy, (T)vz};
   s.bnd.push_back(b);
 }
+// The per-frame rigid-boundary update of the viewer loop: boundary `i` moves
+// with `v` from the next step on (Boundary.cpp:124-127 uses it as -dt * v).
+template <class T> static void sSetBoundaryVel(OrcSolver* S, int i, float vx, float vy, float vz) {
+  Solver<T>& s = pick<T>(S);
+  if (i < 0 || i >= (int)s.bnd.size()) return;
+  s.bnd[i].vel = V3<T>{(T)vx, (T)vy, (T)vz};
+}
 template <class T> static void sSetVel(OrcSolver* S, const float* x, const float* y, const float* z) {
   Solver<T>& s = pick<T>(S);
   s.vel1 = upFC<T>(s.g.r, x, y, z);
@@ -1385,6 +1392,9 @@ void* orc_solver_create(int dbl, float dt, const int* res, const float* o, const
 void orc_solver_destroy(void* p) { delete (OrcSolver*)p; }
 void orc_solver_add_boundary(void* p, const float* sdf, float vx, float vy, float vz) {
   ORC_CALL((OrcSolver*)p, sAddBoundary, sdf, vx, vy, vz);
+}
+void orc_solver_set_boundary_velocity(void* p, int i, float vx, float vy, float vz) {
+  ORC_CALL((OrcSolver*)p, sSetBoundaryVel, i, vx, vy, vz);
 }
 void orc_solver_set_velocity(void* p, const float* x, const float* y, const float* z) { ORC_CALL((OrcSolver*)p, sSetVel, x, y, z); }
 void orc_solver_set_fluid_domain(void* p, const float* d) { ORC_CALL((OrcSolver*)p, sSetDomain, d); }

@@ -65,6 +65,7 @@ def lib():
             "orc_solver_create": (vp, [C.c_int, C.c_float, I3, F3, F3]),
             "orc_solver_destroy": (None, [vp]),
             "orc_solver_add_boundary": (None, [vp, PF, C.c_float, C.c_float, C.c_float]),
+            "orc_solver_set_boundary_velocity": (None, [vp, C.c_int, C.c_float, C.c_float, C.c_float]),
             "orc_solver_set_velocity": (None, [vp, PF, PF, PF]),
             "orc_solver_set_fluid_domain": (None, [vp, PF]),
             "orc_solver_set_color": (None, [vp, PF, PF, PF]),
@@ -303,6 +304,9 @@ class Solver:
 
     def add_solid_boundary(self, sdf, vel=(0, 0, 0)):
         lib().orc_solver_add_boundary(self._h, fp(f32(sdf).reshape(-1)), *[float(v) for v in vel])
+
+    def set_boundary_velocity(self, index, vel):
+        lib().orc_solver_set_boundary_velocity(self._h, int(index), *[float(v) for v in vel])
 
     def set_velocity_field(self, x, y, z):
         lib().orc_solver_set_velocity(self._h, *[fp(f32(a).reshape(-1)) for a in (x, y, z)])
