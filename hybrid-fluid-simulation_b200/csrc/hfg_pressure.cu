@@ -346,11 +346,13 @@ __device__ __forceinline__ float fastZ(const DiagTab& t, Code k, float rv) {
 // completion tracked by one mbarrier per stage.  The halo boxes start 4
 // floats (8 codes) left of the tile so that every box starts on a 16-byte
 // boundary; boxes outside the grid arrive zero-filled.
-constexpr int CTX = 32, CTY = 8;     // tile (threads) per plane
+constexpr int CTX = 32, CTY = 8;     // threads per block (x, y)
+constexpr int RY = 2;                // rows per thread: thread (tx, ty) owns rows ty and ty + CTY
+constexpr int CTR = CTY * RY;        // 16 tile rows per plane
 constexpr int HXF = 4, HXC = 8;      // left pad of the float / code halo boxes
 constexpr int FW = CTX + 2 * HXF;    // 40 floats
 constexpr int CW = CTX + 2 * HXC;    // 48 codes
-constexpr int FH = CTY + 2;          // 10 rows
+constexpr int FH = CTR + 2;          // 18 rows
 constexpr int kDirStages = 4, kUpdStages = 5;
 constexpr unsigned long long kWaitNs = 2000000000ull;  // a stage that takes 2 s to land is an error
 
@@ -417,11 +419,11 @@ constexpr unsigned kDirStageBytes = sizeof(float) * FH * FW * 2 + sizeof(Code) *
 
 struct __align__(128) UpdStage {
   alignas(128) float p[FH][FW];
-  alignas(128) float r[CTY][CTX];
-  alignas(128) float x[CTY][CTX];
-  alignas(128) Code code[CTY][CTX];
+  alignas(128) float r[CTR][CTX];
+  alignas(128) float x[CTR][CTX];
+  alignas(128) Code code[CTR][CTX];
 };
-constexpr unsigned kUpdStageBytes = sizeof(float) * (FH * FW + 2 * CTY * CTX) + sizeof(Code) * CTY * CTX;
+constexpr unsigned kUpdStageBytes = sizeof(float) * (FH * FW + 2 * CTR * CTX) + sizeof(Code) * CTR * CTX;
 
 struct CgLaunch {
   dim3 grid, block;
@@ -447,7 +449,7 @@ CgLaunch cgLaunch(const Dim3i& cg, K kernel) {
   long long slots = (long long)numSMs() * residentBlocks((const void*)kernel);
   CgLaunch L;
   L.block = dim3(CTX, CTY, 1);
-  int bx = (cg.x + CTX - 1) / CTX, by = (cg.y + CTY - 1) / CTY;
+  int bx = (cg.x + CTX - 1) / CTX, by = (cg.y + CTR - 1) / CTR;
   long long tiles = (long long)bx * by;
   long long best = -1;
   int bestPer = cg.z;
@@ -485,7 +487,7 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
   __shared__ __align__(8) uint64_t bar[kDirStages];
   __shared__ int issued;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * CTX + tx;
-  const int x0 = blockIdx.x * CTX, y0 = blockIdx.y * CTY;
+  const int x0 = blockIdx.x * CTX, y0 = blockIdx.y * CTR;
   const int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, P.z);
   const int nPlanes = z1 - z0, nLoad = nPlanes + 1;  // plane z1 is the last "above"
   auto issue = [&](int i) {
@@ -509,52 +511,68 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
   }
   const float beta = st->beta;
   const unsigned long long deadline = globalNs() + kWaitNs;
-  const int x = x0 + tx, y = y0 + ty;
-  const bool in = x < P.x && y < P.y;
+  const int x = x0 + tx;
   const unsigned plane = (unsigned)P.x * (unsigned)P.y;
-  unsigned c = (unsigned)z0 * plane + (unsigned)y * (unsigned)P.x + (unsigned)x;
-  // p of the plane below the chunk, own cell only
-  float below = 0.f;
-  if (in && z0 > 0) {
-    unsigned b = c - plane;
-    below = fmaf(beta, __ldg(pOld + b), fastZ<PC>(tab, __ldg(code + b), __ldg(zr + b)));
+  bool in[RY];
+  unsigned c[RY];
+  float below[RY], cur[RY], above[RY];
+  Code kCur[RY], kAbove[RY];
+#pragma unroll
+  for (int j = 0; j < RY; ++j) {
+    const int y = y0 + ty + j * CTY;
+    in[j] = x < P.x && y < P.y;
+    c[j] = (unsigned)z0 * plane + (unsigned)y * (unsigned)P.x + (unsigned)x;
+    // p of the plane below the chunk, own cell only
+    below[j] = 0.f;
+    if (in[j] && z0 > 0) {
+      unsigned b = c[j] - plane;
+      below[j] = fmaf(beta, __ldg(pOld + b), fastZ<PC>(tab, __ldg(code + b), __ldg(zr + b)));
+    }
   }
-  // p of stage i's plane into tile t (own cell and the halo ring); returns own p and code
-  auto formTile = [&](int i, float (*t)[CTX + 2], Code& kOwn) -> float {
+  // p of stage i's plane into tile t: the thread's RY cells, the x halo of its
+  // rows and, for the edge warps, the y halo rows; own p and codes returned
+  auto formTile = [&](int i, float (*t)[CTX + 2], float* v, Code* kOwn) {
     const DirStage& S = stg[i % kDirStages];
     auto pAt = [&](int row, int colF, int colC) {
       return fmaf(beta, S.po[row][colF], fastZ<PC>(tab, S.code[row][colC], S.r[row][colF]));
     };
-    float v = pAt(ty + 1, tx + HXF, tx + HXC);
-    kOwn = S.code[ty + 1][tx + HXC];
-    t[ty + 1][tx + 1] = v;
-    if (tx == 0) t[ty + 1][0] = pAt(ty + 1, HXF - 1, HXC - 1);
-    if (tx == CTX - 1) t[ty + 1][CTX + 1] = pAt(ty + 1, HXF + CTX, HXC + CTX);
+#pragma unroll
+    for (int j = 0; j < RY; ++j) {
+      const int row = ty + 1 + j * CTY;
+      v[j] = pAt(row, tx + HXF, tx + HXC);
+      kOwn[j] = S.code[row][tx + HXC];
+      t[row][tx + 1] = v[j];
+      if (tx == 0) t[row][0] = pAt(row, HXF - 1, HXC - 1);
+      if (tx == CTX - 1) t[row][CTX + 1] = pAt(row, HXF + CTX, HXC + CTX);
+    }
     if (ty == 0) t[0][tx + 1] = pAt(0, tx + HXF, tx + HXC);
-    if (ty == CTY - 1) t[CTY + 1][tx + 1] = pAt(CTY + 1, tx + HXF, tx + HXC);
-    return v;
+    if (ty == CTY - 1) t[CTR + 1][tx + 1] = pAt(CTR + 1, tx + HXF, tx + HXC);
   };
   bool ok = mbarWait(&bar[0], 0, deadline);
-  Code kCur = 0, kAbove = 0;
-  float cur = ok ? formTile(0, pt[0], kCur) : 0.f;
+  if (ok) formTile(0, pt[0], cur, kCur);
   int waited = 1;
   bool fail = __syncthreads_or(!ok);
   if (!fail && tid == 0 && kDirStages < nLoad) issue(kDirStages), issued = kDirStages + 1;
   float acc = 0.f;
-  for (int i = 0; i < nPlanes && !fail; ++i, c += plane) {
+  for (int i = 0; i < nPlanes && !fail; ++i) {
     ok = mbarWait(&bar[(i + 1) % kDirStages], (unsigned)(((i + 1) / kDirStages) & 1), deadline);
     waited = i + 2;
-    float above = ok ? formTile(i + 1, pt[(i + 1) & 1], kAbove) : 0.f;
-    if (in && ok) {
-      float (*t)[CTX + 2] = pt[i & 1];
-      float q = fastRow(tab, kCur, sx, sy, sz, cur, t[ty + 1][tx], t[ty + 1][tx + 2], t[ty][tx + 1], t[ty + 2][tx + 1],
-                        below, above);
-      pNew[c] = cur;
-      acc = fmaf(cur, q, acc);
+    if (ok) formTile(i + 1, pt[(i + 1) & 1], above, kAbove);
+    float (*t)[CTX + 2] = pt[i & 1];
+#pragma unroll
+    for (int j = 0; j < RY; ++j) {
+      if (in[j] && ok) {
+        const int row = ty + 1 + j * CTY;
+        float q = fastRow(tab, kCur[j], sx, sy, sz, cur[j], t[row][tx], t[row][tx + 2], t[row - 1][tx + 1],
+                          t[row + 1][tx + 1], below[j], above[j]);
+        pNew[c[j]] = cur[j];
+        acc = fmaf(cur[j], q, acc);
+      }
+      below[j] = cur[j];
+      cur[j] = above[j];
+      kCur[j] = kAbove[j];
+      c[j] += plane;
     }
-    below = cur;
-    cur = above;
-    kCur = kAbove;
     fail = __syncthreads_or(!ok);
     if (!fail && tid == 0 && i + 1 + kDirStages < nLoad) issue(i + 1 + kDirStages), issued = i + 2 + kDirStages;
   }
@@ -591,7 +609,7 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
   __shared__ __align__(8) uint64_t bar[kUpdStages];
   __shared__ int issued;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * CTX + tx;
-  const int x0 = blockIdx.x * CTX, y0 = blockIdx.y * CTY;
+  const int x0 = blockIdx.x * CTX, y0 = blockIdx.y * CTR;
   const int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, P.z);
   const int nPlanes = z1 - z0, nLoad = nPlanes + 1;
   auto issue = [&](int i) {
@@ -617,37 +635,51 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
   const float alpha = st->alpha;
   const bool skip = fabsf(alpha) < FLT_EPSILON;
   const unsigned long long deadline = globalNs() + kWaitNs;
-  const int x = x0 + tx, y = y0 + ty;
-  const bool in = x < P.x && y < P.y;
+  const int x = x0 + tx;
   const unsigned plane = (unsigned)P.x * (unsigned)P.y;
-  unsigned c = (unsigned)z0 * plane + (unsigned)y * (unsigned)P.x + (unsigned)x;
-  float below = (in && z0 > 0) ? __ldg(p + c - plane) : 0.f;
+  bool in[RY];
+  unsigned c[RY];
+  float below[RY], cur[RY];
+#pragma unroll
+  for (int j = 0; j < RY; ++j) {
+    const int y = y0 + ty + j * CTY;
+    in[j] = x < P.x && y < P.y;
+    c[j] = (unsigned)z0 * plane + (unsigned)y * (unsigned)P.x + (unsigned)x;
+    below[j] = (in[j] && z0 > 0) ? __ldg(p + c[j] - plane) : 0.f;
+  }
   bool ok = mbarWait(&bar[0], 0, deadline);
-  float cur = ok ? stg[0].p[ty + 1][tx + HXF] : 0.f;
+#pragma unroll
+  for (int j = 0; j < RY; ++j) cur[j] = ok ? stg[0].p[ty + 1 + j * CTY][tx + HXF] : 0.f;
   int waited = 1;
   bool fail = __syncthreads_or(!ok);
   float arr = 0.f, arz = 0.f;
-  for (int i = 0; i < nPlanes && !fail; ++i, c += plane) {
+  for (int i = 0; i < nPlanes && !fail; ++i) {
     ok = mbarWait(&bar[(i + 1) % kUpdStages], (unsigned)(((i + 1) / kUpdStages) & 1), deadline);
     waited = i + 2;
-    float above = ok ? stg[(i + 1) % kUpdStages].p[ty + 1][tx + HXF] : 0.f;
+    const UpdStage& A = stg[(i + 1) % kUpdStages];
     const UpdStage& S = stg[i % kUpdStages];
-    if (in && ok) {
-      Code k = S.code[ty][tx];
-      float rv = S.r[ty][tx];
-      if (!skip) {
-        float q = fastRow(tab, k, sx, sy, sz, cur, S.p[ty + 1][tx + HXF - 1], S.p[ty + 1][tx + HXF + 1],
-                          S.p[ty][tx + HXF], S.p[ty + 2][tx + HXF], below, above);
-        xv[c] = fmaf(alpha, cur, S.x[ty][tx]);
-        rv = fmaf(-alpha, q, rv);
-        r[c] = rv;
+#pragma unroll
+    for (int j = 0; j < RY; ++j) {
+      const int row = ty + 1 + j * CTY, ir = ty + j * CTY;
+      float above = ok ? A.p[row][tx + HXF] : 0.f;
+      if (in[j] && ok) {
+        Code k = S.code[ir][tx];
+        float rv = S.r[ir][tx];
+        if (!skip) {
+          float q = fastRow(tab, k, sx, sy, sz, cur[j], S.p[row][tx + HXF - 1], S.p[row][tx + HXF + 1],
+                            S.p[row - 1][tx + HXF], S.p[row + 1][tx + HXF], below[j], above);
+          xv[c[j]] = fmaf(alpha, cur[j], S.x[ir][tx]);
+          rv = fmaf(-alpha, q, rv);
+          r[c[j]] = rv;
+        }
+        float zz = fastZ<PC>(tab, k, rv);
+        arr = fmaf(rv, rv, arr);
+        arz = fmaf(rv, zz, arz);
       }
-      float zz = fastZ<PC>(tab, k, rv);
-      arr = fmaf(rv, rv, arr);
-      arz = fmaf(rv, zz, arz);
+      below[j] = cur[j];
+      cur[j] = above;
+      c[j] += plane;
     }
-    below = cur;
-    cur = above;
     fail = __syncthreads_or(!ok);
     if (!fail && tid == 0 && i + kUpdStages < nLoad) issue(i + kUpdStages), issued = i + 1 + kUpdStages;
   }
@@ -707,10 +739,10 @@ cudaError_t makeCgMaps(const Dim3i& cg, const Code* code, const float* r, const 
   if (cg.x % 8 != 0) return cudaErrorInvalidValue;  // rows must start on 16-byte boundaries
   cudaError_t e;
   if ((e = encodeMap(&m->codeH, code, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, cg, CW, FH)) != cudaSuccess) return e;
-  if ((e = encodeMap(&m->codeI, code, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, cg, CTX, CTY)) != cudaSuccess) return e;
+  if ((e = encodeMap(&m->codeI, code, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, cg, CTX, CTR)) != cudaSuccess) return e;
   if ((e = encodeMap(&m->rH, r, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cg, FW, FH)) != cudaSuccess) return e;
-  if ((e = encodeMap(&m->rI, r, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cg, CTX, CTY)) != cudaSuccess) return e;
-  if ((e = encodeMap(&m->xI, x, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cg, CTX, CTY)) != cudaSuccess) return e;
+  if ((e = encodeMap(&m->rI, r, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cg, CTX, CTR)) != cudaSuccess) return e;
+  if ((e = encodeMap(&m->xI, x, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cg, CTX, CTR)) != cudaSuccess) return e;
   if ((e = encodeMap(&m->pH[0], p0, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cg, FW, FH)) != cudaSuccess) return e;
   return encodeMap(&m->pH[1], p1, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cg, FW, FH);
 }
