@@ -329,6 +329,14 @@ HFG_API int hfg_solver_get_fluid_sdf(hfg_solver_t s, float* sdf) {
     return HFG_OK;
   });
 }
+HFG_API int hfg_solver_get_fluid_density(hfg_solver_t s, float* out) {
+  return guarded([&]() -> int {
+    SOLVER(s);
+    NEED(out, "null output");
+    S.getFluidDensity(out);
+    return HFG_OK;
+  });
+}
 HFG_API long long hfg_solver_num_particles(hfg_solver_t s) { return (s && s->s) ? s->s->numParticles() : -1; }
 HFG_API int hfg_solver_get_particles(hfg_solver_t s, float* pos, float* vel) {
   return guarded([&]() -> int {
@@ -717,6 +725,67 @@ HFG_API int hfg_op_sl_advect_cc(const int res[3], const float origin[3], const f
     check(launchSLCell(toGeom(res, origin, spacing), accuracy, dt, ConstFaceField{{vx, vy, vz}}, i1, o1, 1,
                        st(stream)),
           "sl");
+    return HFG_OK;
+  });
+}
+HFG_API int hfg_op_sl_advect_fc_ex(const int res[3], const float origin[3], const float spacing[3], const float* ix,
+                                   const float* iy, const float* iz, const float* vx, const float* vy,
+                                   const float* vz, float dt, int accuracy, int sampling, float* ox, float* oy,
+                                   float* oz, void* stream) {
+  return guarded([&]() -> int {
+    NEED(validRes(res) && ix && iy && iz && vx && vy && vz && ox && oy && oz && accuracy >= 0 && accuracy <= 2 &&
+             sampling >= 0 && sampling <= 4,
+         "invalid arguments");
+    const float z3[3] = {0, 0, 0};
+    check(launchSLFace(toGeom(res, origin, spacing), accuracy, dt, ConstFaceField{{vx, vy, vz}},
+                       ConstFaceField{{ix, iy, iz}}, FaceField{{ox, oy, oz}}, z3, 0, z3, 0, st(stream), sampling),
+          "sl");
+    return HFG_OK;
+  });
+}
+HFG_API int hfg_op_sl_advect_cc_ex(const int res[3], const float origin[3], const float spacing[3], const float* in,
+                                   const float* vx, const float* vy, const float* vz, float dt, int accuracy,
+                                   int sampling, float* out, void* stream) {
+  return guarded([&]() -> int {
+    NEED(validRes(res) && in && vx && vy && vz && out && accuracy >= 0 && accuracy <= 2 && sampling >= 0 &&
+             sampling <= 4,
+         "invalid arguments");
+    const float* i1[1] = {in};
+    float* o1[1] = {out};
+    check(launchSLCell(toGeom(res, origin, spacing), accuracy, dt, ConstFaceField{{vx, vy, vz}}, i1, o1, 1,
+                       st(stream), sampling),
+          "sl");
+    return HFG_OK;
+  });
+}
+HFG_API int hfg_op_sample_cc_ex(const int res[3], const float origin[3], const float spacing[3], const float* f,
+                                const float* pos, long long n, int sampling, float* out, void* stream) {
+  return guarded([&]() -> int {
+    NEED(validRes(res) && f && n >= 0 && (n == 0 || (pos && out)) && sampling >= 0 && sampling <= 4,
+         "invalid arguments");
+    check(launchSampleAlg(toGeom(res, origin, spacing), 0, ConstFaceField{{f, nullptr, nullptr}}, pos, n, sampling,
+                          out, st(stream)),
+          "sample");
+    return HFG_OK;
+  });
+}
+HFG_API int hfg_op_sample_fc_ex(const int res[3], const float origin[3], const float spacing[3], const float* vx,
+                                const float* vy, const float* vz, const float* pos, long long n, int sampling,
+                                float* out, void* stream) {
+  return guarded([&]() -> int {
+    NEED(validRes(res) && vx && vy && vz && n >= 0 && (n == 0 || (pos && out)) && sampling >= 0 && sampling <= 4,
+         "invalid arguments");
+    check(launchSampleAlg(toGeom(res, origin, spacing), 1, ConstFaceField{{vx, vy, vz}}, pos, n, sampling, out,
+                          st(stream)),
+          "sample");
+    return HFG_OK;
+  });
+}
+HFG_API int hfg_op_build_fluid_density(const int res[3], const float* domain, const float* solid_sdf, float* out,
+                                       void* stream) {
+  return guarded([&]() -> int {
+    NEED(validRes(res) && domain && solid_sdf && out, "invalid arguments");
+    check(launchFluidDensity(toRes(res), domain, solid_sdf, nullptr, out, st(stream)), "fluid density");
     return HFG_OK;
   });
 }

@@ -183,6 +183,83 @@ __device__ __forceinline__ void sampleFaceFast(const ConstFaceField& v, const Ge
   for (int a = 0; a < 3; ++a) out[a] = s.sample(g, a, v.c[a]);
 }
 
+// Cubic samplers (MPhysics/EulerMathTool.cu:134-240, FieldMathTool.cu:106-173).
+// SAMP follows ESamplingAlgorithm (EnumType.h:3-10): 1 Catmull-Rom,
+// 2 monotonic Catmull-Rom, 3 Bridson cubic, 4 Bridson cubic clamped to the
+// two middle values.  The Bridson weights carry double literals in the
+// reference, so they are formed in FP64 (products of t alone in FP32) and the
+// sum is rounded to FP32 once; every operation is written out so that no
+// contraction changes the rounding.
+__device__ __forceinline__ float cubicBridson1(const float v[4], float t) {
+  const double td = (double)t;
+  const float t2 = __fmul_rn(t, t), t3 = __fmul_rn(t2, t);
+  double c0 = __dsub_rn(__dadd_rn(__dmul_rn(-1.0 / 3.0, td), __dmul_rn(__dmul_rn(0.5, td), td)),
+                        __dmul_rn(__dmul_rn(__dmul_rn(1.0 / 6.0, td), td), td));
+  double c1 = __dadd_rn(__dsub_rn(1.0, (double)t2), __dmul_rn(0.5, (double)__fsub_rn(t3, t)));
+  double c2 = __dadd_rn(td, __dmul_rn(0.5, (double)__fsub_rn(t2, t3)));
+  double c3 = __dmul_rn(1.0 / 6.0, (double)__fsub_rn(t3, t));
+  double s = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(c0, (double)v[0]), __dmul_rn(c1, (double)v[1])),
+                                 __dmul_rn(c2, (double)v[2])),
+                       __dmul_rn(c3, (double)v[3]));
+  return __double2float_rn(s);
+}
+__device__ __forceinline__ float catmullRom1(const float v[4], float t, bool monotonic) {
+  float d1 = __fdiv_rn(__fsub_rn(v[2], v[0]), 2.f), d2 = __fdiv_rn(__fsub_rn(v[3], v[1]), 2.f);
+  const float delta = __fsub_rn(v[2], v[1]);
+  if (monotonic) {
+    if (fabsf(delta) < FLT_EPSILON) { d1 = 0.f; d2 = 0.f; }
+    if (__fmul_rn(delta, d1) < 0.f) d1 = 0.f;
+    if (__fmul_rn(delta, d2) < 0.f) d2 = 0.f;
+  }
+  const float a3 = __fsub_rn(__fadd_rn(d1, d2), __fmul_rn(2.f, delta));
+  const float a2 = __fsub_rn(__fsub_rn(__fmul_rn(3.f, delta), __fmul_rn(2.f, d1)), d2);
+  float r = __fmul_rn(__fmul_rn(__fmul_rn(a3, t), t), t);
+  r = __fadd_rn(r, __fmul_rn(__fmul_rn(a2, t), t));
+  r = __fadd_rn(r, __fmul_rn(d1, t));
+  return __fadd_rn(r, v[1]);
+}
+template <int SAMP> __device__ __forceinline__ float cubic1(const float v[4], float t) {
+  if (SAMP == 1) return catmullRom1(v, t, false);
+  if (SAMP == 2) return catmullRom1(v, t, true);
+  if (SAMP == 3) return cubicBridson1(v, t);
+  float c = cubicBridson1(v, t);  // clampCUDA (EulerMathTool.cu:121-127)
+  return fmaxf(fminf(v[1], v[2]), fminf(c, fmaxf(v[1], v[2])));
+}
+// 4^3 clamp-to-edge neighbourhood, reduced along x, then y, then z.
+template <int SAMP>
+__device__ inline float cubicSample(const float* __restrict__ f, const Geom& g, float px, float py, float pz) {
+  const float rx = __fsub_rn(__fsub_rn(px, g.ox), __fdiv_rn(g.hx, 2.f));
+  const float ry = __fsub_rn(__fsub_rn(py, g.oy), __fdiv_rn(g.hy, 2.f));
+  const float rz = __fsub_rn(__fsub_rn(pz, g.oz), __fdiv_rn(g.hz, 2.f));
+  const int ix = floorRef(__fdiv_rn(rx, g.hx)), iy = floorRef(__fdiv_rn(ry, g.hy)), iz = floorRef(__fdiv_rn(rz, g.hz));
+  const float tx = __fdiv_rn(__fsub_rn(rx, __fmul_rn((float)ix, g.hx)), g.hx);
+  const float ty = __fdiv_rn(__fsub_rn(ry, __fmul_rn((float)iy, g.hy)), g.hy);
+  const float tz = __fdiv_rn(__fsub_rn(rz, __fmul_rn((float)iz, g.hz)), g.hz);
+  int xs[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) xs[k] = clampi(ix + k - 1, g.r.x);
+  float vz[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const long long zo = (long long)clampi(iz + i - 1, g.r.z) * g.r.y;
+    float vy[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float* row = f + (zo + clampi(iy + j - 1, g.r.y)) * g.r.x;
+      const float vx[4] = {__ldg(row + xs[0]), __ldg(row + xs[1]), __ldg(row + xs[2]), __ldg(row + xs[3])};
+      vy[j] = cubic1<SAMP>(vx, tx);
+    }
+    vz[i] = cubic1<SAMP>(vy, ty);
+  }
+  return cubic1<SAMP>(vz, tz);
+}
+// trilinear (SAMP 0) or cubic sample of one scalar grid
+template <int SAMP>
+__device__ __forceinline__ float sampleAlg(const float* __restrict__ f, const Geom& g, float px, float py, float pz) {
+  if (SAMP == 0) return trilerp(f, g, px, py, pz);
+  return cubicSample<SAMP>(f, g, px, py, pz);
+}
+
 // Transfer-kernel weights (MPhysics/EulerMathTool.cu:268-294).
 __device__ inline float kLinear(float o) {
   float a = fabsf(o);

@@ -550,6 +550,36 @@ __global__ void kFluidSdfLayer(Dim3i r, float* __restrict__ sdf, const unsigned 
   }
 }
 
+// buildFluidDensity (EulerSolverTool.cu:408-448): 1 inside the fluid, the
+// surface density 0.2 where a 6-neighbour (clamp-to-edge) is air, 0 outside
+// the fluid or inside a solid.  A cell is air when neither the fluid domain
+// nor the solid is negative there (isInsideAir, EulerMathTool.cu:344-348).
+__global__ void kFluidDensity(Dim3i r, const float* __restrict__ dom, const float* __restrict__ solidSdf,
+                              const uint8_t* __restrict__ solidIdx, float* __restrict__ out) {
+  HFG_FOR(c, r.size()) {
+    int x, y, z;
+    cellCoord(c, r, x, y, z);
+    auto solidAt = [&](long long i) { return solidSdf ? solidSdf[i] < 0.f : solidIdx[i] != 0; };
+    float v = 0.f;
+    if (dom[c] < 0.f && !solidAt(c)) {
+      const int dx[6] = {-1, 1, 0, 0, 0, 0}, dy[6] = {0, 0, -1, 1, 0, 0}, dz[6] = {0, 0, 0, 0, -1, 1};
+      bool air = false;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        long long nb = linc(x + dx[k], y + dy[k], z + dz[k], r);
+        air |= dom[nb] >= 0.f && !solidAt(nb);
+      }
+      v = air ? (float)0.2 : 1.f;  // FluidSurfaceDensity (Common.h:244)
+    }
+    out[c] = v;
+  }
+}
+cudaError_t launchFluidDensity(const Dim3i& r, const float* dom, const float* solidSdf, const uint8_t* solidIdx,
+                               float* out, cudaStream_t s) {
+  kFluidDensity<<<gridFor(r.size()), kThreads, 0, s>>>(r, dom, solidSdf, solidIdx, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launchFluidSdf(const Dim3i& r, const float* dom, float* sdf, int layers, unsigned int* frontA,
                            unsigned int* frontB, unsigned int* counts, unsigned int* hostCount, cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(counts, 0, sizeof(unsigned int) * 2, s);
@@ -1086,29 +1116,43 @@ __device__ inline void axpyPt(float a, const float v[3], float p[3]) {
   for (int k = 0; k < 3; ++k) p[k] = fmaf(a, v[k], p[k]);
 }
 
+template <int SAMP>
+__device__ inline void sampleVel(ConstFaceField vel, const Geom& g, float px, float py, float pz, float v[3]) {
+  if (SAMP == 0) {
+    sampleFaceFast(vel, g, px, py, pz, v);
+  } else {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) v[a] = cubicSample<SAMP>(vel.c[a], faceGeom(g, a), px, py, pz);
+  }
+}
+
+// CSemiLagrangian::backTrace (SemiLagrangian.cpp:188-347); every velocity
+// sample uses the advection's sampling algorithm.
+template <int SAMP>
 __device__ inline void backTrace(ConstFaceField vel, const Geom& g, float dt, int acc, const float in[3], float out[3]) {
   float v0[3], v1[3], v2[3], mid[3], tf[3];
   out[0] = in[0]; out[1] = in[1]; out[2] = in[2];
-  sampleFaceFast(vel, g, in[0], in[1], in[2], v0);
+  sampleVel<SAMP>(vel, g, in[0], in[1], in[2], v0);
   if (acc == 0) {
     axpyPt(-dt, v0, out);
     return;
   }
   mid[0] = in[0]; mid[1] = in[1]; mid[2] = in[2];
   axpyPt(-0.5f * dt, v0, mid);
-  sampleFaceFast(vel, g, mid[0], mid[1], mid[2], v1);
+  sampleVel<SAMP>(vel, g, mid[0], mid[1], mid[2], v1);
   if (acc == 1) {
     axpyPt(-dt, v1, out);
     return;
   }
   tf[0] = in[0]; tf[1] = in[1]; tf[2] = in[2];
   axpyPt(-0.75f * dt, v1, tf);
-  sampleFaceFast(vel, g, tf[0], tf[1], tf[2], v2);
+  sampleVel<SAMP>(vel, g, tf[0], tf[1], tf[2], v2);
   axpyPt(-(float)(2.0 / 9.0) * dt, v0, out);
   axpyPt(-(float)(3.0 / 9.0) * dt, v1, out);
   axpyPt(-(float)(4.0 / 9.0) * dt, v2, out);
 }
 
+template <int SAMP>
 __global__ void kSLFace(Geom g, int acc, float dt, ConstFaceField vel, ConstFaceField in, FaceField out, float ax,
                         float ay, float az, int doAdd, float bx, float by, float bz, int doAdd2) {
   const float add[3] = {ax, ay, az}, add2[3] = {bx, by, bz};
@@ -1125,8 +1169,8 @@ __global__ void kSLFace(Geom g, int acc, float dt, ConstFaceField vel, ConstFace
       if (a == 1) p[1] = __fadd_rn(__fmul_rn((float)y, g.hy), g.oy);
       if (a == 2) p[2] = __fadd_rn(__fmul_rn((float)z, g.hz), g.oz);
       float q[3];
-      backTrace(vel, g, dt, acc, p, q);
-      float v = trilerp(in.c[a], fg, q[0], q[1], q[2]);
+      backTrace<SAMP>(vel, g, dt, acc, p, q);
+      float v = sampleAlg<SAMP>(in.c[a], fg, q[0], q[1], q[2]);
       if (doAdd) v = __fadd_rn(add[a], v);
       if (doAdd2) v = __fadd_rn(add2[a], v);
       out.c[a][f] = v;
@@ -1134,9 +1178,19 @@ __global__ void kSLFace(Geom g, int acc, float dt, ConstFaceField vel, ConstFace
   }
 }
 cudaError_t launchSLFace(const Geom& g, int acc, float dt, ConstFaceField vel, ConstFaceField in, FaceField out,
-                         const float add[3], int doAdd, const float add2[3], int doAdd2, cudaStream_t s) {
-  kSLFace<<<gridFor(g.r.size()), kThreads, 0, s>>>(g, acc, dt, vel, in, out, add[0], add[1], add[2], doAdd, add2[0],
-                                                   add2[1], add2[2], doAdd2);
+                         const float add[3], int doAdd, const float add2[3], int doAdd2, cudaStream_t s,
+                         int sampling) {
+#define HFG_SL_FACE(S)                                                                                              \
+  kSLFace<S><<<gridFor(g.r.size()), kThreads, 0, s>>>(g, acc, dt, vel, in, out, add[0], add[1], add[2], doAdd,      \
+                                                      add2[0], add2[1], add2[2], doAdd2)
+  switch (sampling) {
+    case 1: HFG_SL_FACE(1); break;
+    case 2: HFG_SL_FACE(2); break;
+    case 3: HFG_SL_FACE(3); break;
+    case 4: HFG_SL_FACE(4); break;
+    default: HFG_SL_FACE(0);
+  }
+#undef HFG_SL_FACE
   return cudaGetLastError();
 }
 
@@ -1144,6 +1198,7 @@ struct CellFields {
   const float* in[4];
   float* out[4];
 };
+template <int SAMP>
 __global__ void kSLCell(Geom g, int acc, float dt, ConstFaceField vel, CellFields cf, int nf) {
   HFG_FOR(c, g.r.size()) {
     int x, y, z;
@@ -1152,15 +1207,50 @@ __global__ void kSLCell(Geom g, int acc, float dt, ConstFaceField vel, CellField
                   __fadd_rn(__fmul_rn(__fadd_rn((float)y, 0.5f), g.hy), g.oy),
                   __fadd_rn(__fmul_rn(__fadd_rn((float)z, 0.5f), g.hz), g.oz)};
     float q[3];
-    backTrace(vel, g, dt, acc, p, q);
-    for (int k = 0; k < nf; ++k) cf.out[k][c] = trilerp(cf.in[k], g, q[0], q[1], q[2]);
+    backTrace<SAMP>(vel, g, dt, acc, p, q);
+    for (int k = 0; k < nf; ++k) cf.out[k][c] = sampleAlg<SAMP>(cf.in[k], g, q[0], q[1], q[2]);
   }
 }
 cudaError_t launchSLCell(const Geom& g, int acc, float dt, ConstFaceField vel, const float* const* in, float* const* out,
-                         int nfields, cudaStream_t s) {
+                         int nfields, cudaStream_t s, int sampling) {
   CellFields cf{};
   for (int k = 0; k < nfields && k < 4; ++k) { cf.in[k] = in[k]; cf.out[k] = out[k]; }
-  kSLCell<<<gridFor(g.r.size()), kThreads, 0, s>>>(g, acc, dt, vel, cf, nfields < 4 ? nfields : 4);
+  const int nf = nfields < 4 ? nfields : 4;
+  switch (sampling) {
+    case 1: kSLCell<1><<<gridFor(g.r.size()), kThreads, 0, s>>>(g, acc, dt, vel, cf, nf); break;
+    case 2: kSLCell<2><<<gridFor(g.r.size()), kThreads, 0, s>>>(g, acc, dt, vel, cf, nf); break;
+    case 3: kSLCell<3><<<gridFor(g.r.size()), kThreads, 0, s>>>(g, acc, dt, vel, cf, nf); break;
+    case 4: kSLCell<4><<<gridFor(g.r.size()), kThreads, 0, s>>>(g, acc, dt, vel, cf, nf); break;
+    default: kSLCell<0><<<gridFor(g.r.size()), kThreads, 0, s>>>(g, acc, dt, vel, cf, nf);
+  }
+  return cudaGetLastError();
+}
+
+// Sampling of a cell-centred scalar grid (FieldMathTool.cu:470-573) or of
+// the three face grids (:783-1128) at n points with an ESamplingAlgorithm.
+template <int SAMP>
+__global__ void kSampleAlg(Geom g, int face, ConstFaceField f, const float* __restrict__ pos, long long n,
+                           float* __restrict__ out) {
+  HFG_FOR(i, n) {
+    const float px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
+    if (face) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) out[3 * i + a] = sampleAlg<SAMP>(f.c[a], faceGeom(g, a), px, py, pz);
+    } else {
+      out[i] = sampleAlg<SAMP>(f.c[0], g, px, py, pz);
+    }
+  }
+}
+cudaError_t launchSampleAlg(const Geom& g, int face, ConstFaceField f, const float* pos, long long n, int sampling,
+                            float* out, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  switch (sampling) {
+    case 1: kSampleAlg<1><<<gridFor(n), kThreads, 0, s>>>(g, face, f, pos, n, out); break;
+    case 2: kSampleAlg<2><<<gridFor(n), kThreads, 0, s>>>(g, face, f, pos, n, out); break;
+    case 3: kSampleAlg<3><<<gridFor(n), kThreads, 0, s>>>(g, face, f, pos, n, out); break;
+    case 4: kSampleAlg<4><<<gridFor(n), kThreads, 0, s>>>(g, face, f, pos, n, out); break;
+    default: kSampleAlg<0><<<gridFor(n), kThreads, 0, s>>>(g, face, f, pos, n, out);
+  }
   return cudaGetLastError();
 }
 

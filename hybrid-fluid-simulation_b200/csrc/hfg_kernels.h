@@ -161,6 +161,10 @@ cudaError_t launchExtrapLayer(const Dim3i rc[3], float* const vals[3], const lon
 // hostCount pinned.  Blocks (one host read per layer).
 cudaError_t launchFluidSdf(const Dim3i& r, const float* dom, float* sdf, int layers, unsigned int* frontA,
                            unsigned int* frontB, unsigned int* counts, unsigned int* hostCount, cudaStream_t s);
+// fluid density of buildFluidDensity; the solid is solidSdf < 0 when given,
+// else solidIdx != 0
+cudaError_t launchFluidDensity(const Dim3i& r, const float* dom, const float* solidSdf, const uint8_t* solidIdx,
+                               float* out, cudaStream_t s);
 
 // ---- particles -------------------------------------------------------------
 enum ParticleMode : int { MODE_PIC = 0, MODE_FLIP = 1, MODE_MIX = 2 };
@@ -192,10 +196,16 @@ cudaError_t launchSampleFace(const Geom& g, ConstFaceField f, const float* pos, 
 cudaError_t launchSampleCell(const Geom& g, const float* f, const float* pos, long long M, float* out, cudaStream_t s);
 
 // ---- semi-Lagrangian -------------------------------------------------------
+// sampling: ESamplingAlgorithm of every sample (0 trilinear .. 4 clamped Bridson)
 cudaError_t launchSLFace(const Geom& g, int acc, float dt, ConstFaceField vel, ConstFaceField in, FaceField out,
-                         const float add[3], int doAdd, const float add2[3], int doAdd2, cudaStream_t s);
+                         const float add[3], int doAdd, const float add2[3], int doAdd2, cudaStream_t s,
+                         int sampling = 0);
 cudaError_t launchSLCell(const Geom& g, int acc, float dt, ConstFaceField vel, const float* const* in, float* const* out,
-                         int nfields, cudaStream_t s);
+                         int nfields, cudaStream_t s, int sampling = 0);
+// n points (3n floats) sampled from one cell-centred grid (face = 0, f.c[0];
+// out n floats) or from the three face grids of `g` (face = 1; out 3n floats)
+cudaError_t launchSampleAlg(const Geom& g, int face, ConstFaceField f, const float* pos, long long n, int sampling,
+                            float* out, cudaStream_t s);
 
 // ---- external forces (unit-field axpy on every face) ------------------------
 cudaError_t launchAddConst(long long n, float* v, float a, cudaStream_t s);

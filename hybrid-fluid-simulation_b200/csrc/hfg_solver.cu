@@ -279,6 +279,7 @@ void GridSolver::seedParticles(int ppc, unsigned long long seed) {
 void GridSolver::setOptions(const hfg_options_t& o) {
   if (o.precond < 0 || o.precond > 2 || o.tol_mode < 0 || o.tol_mode > 1 || !(o.tol > 0))
     throw CudaError("invalid solver options", HFG_ERR_INVALID);
+  if (o.sampling < 0 || o.sampling > 4) throw CudaError("sampling algorithm must be in [0, 4]", HFG_ERR_INVALID);
   if (o.extrapolation_layers < 0 || o.extrapolation_layers > kMaxLayers)
     throw CudaError("extrapolation layers must be in [0, 1000]", HFG_ERR_INVALID);
   bool mgChanged = o.precond == HFG_PRECOND_MG &&
@@ -385,11 +386,12 @@ void GridSolver::computeAdvection() {
   float* vout[3] = {vel_[ni][0].p, vel_[ni][1].p, vel_[ni][2].p};
   if (adv_ == HFG_ADV_SEMI_LAGRANGIAN) {
     stageBegin(1);
-    launched(launchSLFace(g_, acc_rk_, dt_, cvel(ci), cvel(ci), mvel(ni), gv, doG, ev, doE, stream_), "sl face");
+    launched(launchSLFace(g_, acc_rk_, dt_, cvel(ci), cvel(ci), mvel(ni), gv, doG, ev, doE, stream_, opt_.sampling),
+             "sl face");
     if (opt_.advect_scalars) {
       const float* in[4] = {color_[ci][0].p, color_[ci][1].p, color_[ci][2].p, dom_[ci].p};
       float* out[4] = {color_[ni][0].p, color_[ni][1].p, color_[ni][2].p, dom_[ni].p};
-      launched(launchSLCell(g_, acc_rk_, dt_, cvel(ci), in, out, 4, stream_), "sl cell");
+      launched(launchSLCell(g_, acc_rk_, dt_, cvel(ci), in, out, 4, stream_, opt_.sampling), "sl cell");
     }
     stageEnd(1);
     return;
@@ -686,6 +688,16 @@ void GridSolver::getFluidSDF(float* out) {
   pinnedPut(host);
   check(e, "fluid sdf");
   check(cudaMemcpyAsync(out, sdf.p, N_ * 4, cudaMemcpyDeviceToHost, stream_), "download");
+  synchronize();
+}
+
+// GridFluidSolver.cpp:593-613 generateCurFluidDensity: the current fluid
+// domain against the total solid.
+void GridSolver::getFluidDensity(float* out) {
+  DArray<float> d;
+  d.alloc(N_, stream_);
+  check(launchFluidDensity(g_.r, dom_[cur()].p, nullptr, solidIdx_.p, d.p, stream_), "fluid density");
+  check(cudaMemcpyAsync(out, d.p, N_ * 4, cudaMemcpyDeviceToHost, stream_), "download");
   synchronize();
 }
 

@@ -119,6 +119,7 @@ class GridSolver {
   void getSolidSDF(float* s);
   void getSolidVel(float* x, float* y, float* z);
   void getFluidSDF(float* out);
+  void getFluidDensity(float* out);
   void getParticles(float* pos, float* vel);
   void getStats(hfg_stats_t* st);
   void synchronize();

@@ -28,6 +28,7 @@ PRECOND_IDENTITY, PRECOND_JACOBI, PRECOND_MG = 0, 1, 2
 TOL_REFERENCE, TOL_RELATIVE = 0, 1
 HFG_OK, HFG_ERR_NOT_CONVERGED = 0, -5
 SOLID_WALLS, SOLID_SPHERE, SOLID_BOX = 0, 1, 2
+SAMPLE_TRILINEAR, SAMPLE_CATMULLROM, SAMPLE_MONOCATMULLROM, SAMPLE_CUBICBRIDSON, SAMPLE_CLAMPCUBICBRIDSON = 0, 1, 2, 3, 4
 
 
 class HfgError(RuntimeError):
@@ -41,6 +42,7 @@ class Options(C.Structure):
         ("precond", C.c_int), ("tol_mode", C.c_int), ("tol", C.c_double), ("max_iter", C.c_longlong),
         ("clamp_mode", C.c_int), ("advect_scalars", C.c_int), ("extrapolation_layers", C.c_int),
         ("mg_levels", C.c_int), ("mg_smooth", C.c_int), ("mg_half", C.c_int), ("report_divergence", C.c_int),
+        ("sampling", C.c_int),
     ]
 
 
@@ -135,6 +137,7 @@ def _signatures(lib):
         "hfg_solver_get_solid_sdf": (C.c_int, [S, PF]),
         "hfg_solver_get_solid_vel_field": (C.c_int, [S, PF, PF, PF]),
         "hfg_solver_get_fluid_sdf": (C.c_int, [S, PF]),
+        "hfg_solver_get_fluid_density": (C.c_int, [S, PF]),
         "hfg_solver_num_particles": (C.c_longlong, [S]),
         "hfg_solver_get_particles": (C.c_int, [S, PF, PF]),
         "hfg_solver_get_stats": (C.c_int, [S, C.POINTER(Stats)]),
@@ -155,6 +158,11 @@ def _signatures(lib):
         "hfg_op_extrapolate_cc": (C.c_int, [I3, VP, C.c_int, VP]),
         "hfg_op_sample_fc": (C.c_int, [I3, F3, F3, VP, VP, VP, VP, C.c_longlong, VP, VP]),
         "hfg_op_sample_cc": (C.c_int, [I3, F3, F3, VP, VP, C.c_longlong, VP, VP]),
+        "hfg_op_sample_cc_ex": (C.c_int, [I3, F3, F3, VP, VP, C.c_longlong, C.c_int, VP, VP]),
+        "hfg_op_sample_fc_ex": (C.c_int, [I3, F3, F3, VP, VP, VP, VP, C.c_longlong, C.c_int, VP, VP]),
+        "hfg_op_sl_advect_fc_ex": (C.c_int, [I3, F3, F3, VP, VP, VP, VP, VP, VP, C.c_float, C.c_int, C.c_int, VP, VP,
+                                             VP, VP]),
+        "hfg_op_sl_advect_cc_ex": (C.c_int, [I3, F3, F3, VP, VP, VP, VP, C.c_float, C.c_int, C.c_int, VP, VP]),
         "hfg_op_g2p_fc": (C.c_int, [I3, F3, F3, VP, VP, VP, VP, C.c_longlong, C.c_int, VP, VP]),
         "hfg_op_g2p_cc": (C.c_int, [I3, F3, F3, VP, VP, C.c_longlong, C.c_int, VP, VP]),
         "hfg_op_p2g_fc": (C.c_int, [I3, F3, F3, VP, VP, C.c_longlong, C.c_int, VP, VP, VP, VP, VP, VP, VP]),
@@ -166,6 +174,7 @@ def _signatures(lib):
         "hfg_op_sl_advect_cc": (C.c_int, [I3, F3, F3, VP, VP, VP, VP, C.c_float, C.c_int, VP, VP]),
         "hfg_op_fluid_domain_from_bbox": (C.c_int, [I3, F3, F3, F3, F3, VP, VP]),
         "hfg_op_build_fluid_sdf": (C.c_int, [I3, VP, VP, C.c_int, VP]),
+        "hfg_op_build_fluid_density": (C.c_int, [I3, VP, VP, VP, VP]),
         "hfg_solver_add_analytic_solid": (C.c_int, [S, C.c_int, C.POINTER(C.c_double), F3]),
         "hfg_scene_bytes": (C.c_int, [I3, C.c_longlong, C.c_int, C.c_int, C.POINTER(C.c_longlong)]),
         "hfg_scene_particles_bound": (C.c_int, [C.POINTER(SceneDesc), C.POINTER(C.c_longlong)]),
@@ -389,6 +398,11 @@ class Solver:
         _check(lib().hfg_solver_get_fluid_sdf(self._h, _fptr(out)))
         return out
 
+    def fluid_density(self):
+        out = np.empty(self.res[::-1], np.float32)
+        _check(lib().hfg_solver_get_fluid_density(self._h, _fptr(out)))
+        return out
+
     @property
     def num_particles(self) -> int:
         return int(lib().hfg_solver_num_particles(self._h))
@@ -492,6 +506,16 @@ def op_sample_cc(res, origin, spacing, f, pos, out, stream=None):
                                   _ptr(out), _stream(stream)))
 
 
+def op_sample_cc_ex(res, origin, spacing, f, pos, sampling, out, stream=None):
+    _check(lib().hfg_op_sample_cc_ex(_i3(res), _f3(origin), _f3(spacing), _ptr(f), _ptr(pos), pos.numel() // 3,
+                                     sampling, _ptr(out), _stream(stream)))
+
+
+def op_sample_fc_ex(res, origin, spacing, vel, pos, sampling, out, stream=None):
+    _check(lib().hfg_op_sample_fc_ex(_i3(res), _f3(origin), _f3(spacing), *[_ptr(v) for v in vel], _ptr(pos),
+                                     pos.numel() // 3, sampling, _ptr(out), _stream(stream)))
+
+
 def op_g2p_fc(res, origin, spacing, vel, pos, alg, out, stream=None):
     _check(lib().hfg_op_g2p_fc(_i3(res), _f3(origin), _f3(spacing), *[_ptr(v) for v in vel], _ptr(pos),
                                pos.numel() // 3, alg, _ptr(out), _stream(stream)))
@@ -528,13 +552,23 @@ def op_advect_particles(res, origin, spacing, vel, pos, dt, cfl=1.0, accuracy=RK
     return n.value
 
 
-def op_sl_advect_fc(res, origin, spacing, field, vel, dt, accuracy, out, stream=None):
+def op_sl_advect_fc(res, origin, spacing, field, vel, dt, accuracy, out, stream=None, sampling=SAMPLE_TRILINEAR):
+    if sampling != SAMPLE_TRILINEAR:
+        _check(lib().hfg_op_sl_advect_fc_ex(_i3(res), _f3(origin), _f3(spacing), *[_ptr(v) for v in field],
+                                            *[_ptr(v) for v in vel], C.c_float(dt), accuracy, sampling,
+                                            *[_ptr(v) for v in out], _stream(stream)))
+        return
     _check(lib().hfg_op_sl_advect_fc(_i3(res), _f3(origin), _f3(spacing), *[_ptr(v) for v in field],
                                      *[_ptr(v) for v in vel], C.c_float(dt), accuracy, *[_ptr(v) for v in out],
                                      _stream(stream)))
 
 
-def op_sl_advect_cc(res, origin, spacing, field, vel, dt, accuracy, out, stream=None):
+def op_sl_advect_cc(res, origin, spacing, field, vel, dt, accuracy, out, stream=None, sampling=SAMPLE_TRILINEAR):
+    if sampling != SAMPLE_TRILINEAR:
+        _check(lib().hfg_op_sl_advect_cc_ex(_i3(res), _f3(origin), _f3(spacing), _ptr(field),
+                                            *[_ptr(v) for v in vel], C.c_float(dt), accuracy, sampling, _ptr(out),
+                                            _stream(stream)))
+        return
     _check(lib().hfg_op_sl_advect_cc(_i3(res), _f3(origin), _f3(spacing), _ptr(field), *[_ptr(v) for v in vel],
                                      C.c_float(dt), accuracy, _ptr(out), _stream(stream)))
 
@@ -542,6 +576,10 @@ def op_sl_advect_cc(res, origin, spacing, field, vel, dt, accuracy, out, stream=
 def op_fluid_domain_from_bbox(res, origin, spacing, mn, mx, out, stream=None):
     _check(lib().hfg_op_fluid_domain_from_bbox(_i3(res), _f3(origin), _f3(spacing), _f3(mn), _f3(mx), _ptr(out),
                                                _stream(stream)))
+
+
+def op_build_fluid_density(res, domain, solid_sdf, out, stream=None):
+    _check(lib().hfg_op_build_fluid_density(_i3(res), _ptr(domain), _ptr(solid_sdf), _ptr(out), _stream(stream)))
 
 
 def op_build_fluid_sdf(res, domain, sdf, layers=1000, stream=None):

@@ -53,6 +53,14 @@ enum { HFG_PRECOND_IDENTITY = 0, HFG_PRECOND_JACOBI = 1, HFG_PRECOND_MG = 2 };
 /* CG stopping rules: the reference's sqrt(||r||_2) < tol (CuMatrixFreePCG.cpp:28,51),
  * or the relative ||r||_2 / ||b||_2 < tol. */
 enum { HFG_TOL_REFERENCE = 0, HFG_TOL_RELATIVE = 1 };
+/* ESamplingAlgorithm (EnumType.h:3-10) */
+enum {
+  HFG_SAMPLE_TRILINEAR = 0,
+  HFG_SAMPLE_CATMULLROM = 1,
+  HFG_SAMPLE_MONOCATMULLROM = 2,
+  HFG_SAMPLE_CUBICBRIDSON = 3,
+  HFG_SAMPLE_CLAMPCUBICBRIDSON = 4
+};
 
 typedef struct hfg_solver_s* hfg_solver_t;
 
@@ -70,6 +78,8 @@ typedef struct {
   int mg_smooth;          /* smoothing sweeps per level (0 = default) */
   int mg_half;            /* 1: multigrid smoothing stores in half precision */
   int report_divergence;  /* 1: measure the divergence residual of every projection */
+  int sampling;           /* HFG_SAMPLE_* of the semi-Lagrangian advection (setSamplingAlg,
+                             AdvectionSolver.cpp:21-24; default trilinear) */
 } hfg_options_t;
 
 typedef struct {
@@ -143,6 +153,9 @@ HFG_API int hfg_solver_get_solid_vel_field(hfg_solver_t s, float* x, float* y, f
 /* generateCurFluidSDF + getFluidSDFField: the layered fluid SDF of the current
  * fluid-domain field (GridFluidSolver.cpp:571-591, EulerSolverTool.cu:324-406) */
 HFG_API int hfg_solver_get_fluid_sdf(hfg_solver_t s, float* sdf);
+/* generateCurFluidDensity + getFluidDensityField (N floats: 1 fluid, 0.2 at the
+ * surface, 0 elsewhere)  GridFluidSolver.cpp:297-300,593-613 */
+HFG_API int hfg_solver_get_fluid_density(hfg_solver_t s, float* density);
 HFG_API long long hfg_solver_num_particles(hfg_solver_t s);
 HFG_API int hfg_solver_get_particles(hfg_solver_t s, float* pos, float* vel);
 HFG_API int hfg_solver_get_stats(hfg_solver_t s, hfg_stats_t* st);
@@ -196,6 +209,15 @@ HFG_API int hfg_op_sample_fc(const int res[3], const float origin[3], const floa
 /* sampleCellCenteredScalarFieldInvoker at n points (trilinear)  FieldMathTool.cu:526-573 */
 HFG_API int hfg_op_sample_cc(const int res[3], const float origin[3], const float spacing[3], const float* f,
                              const float* pos, long long n, float* out, void* stream);
+/* sampleCellCenteredScalarFieldInvoker with an ESamplingAlgorithm (HFG_SAMPLE_*)
+ * FieldMathTool.cu:470-573 (cubic kernels :106-173, EulerMathTool.cu:134-240) */
+HFG_API int hfg_op_sample_cc_ex(const int res[3], const float origin[3], const float spacing[3], const float* f,
+                                const float* pos, long long n, int sampling, float* out, void* stream);
+/* sampleFaceCenteredVectorFieldInvoker with an ESamplingAlgorithm; out 3n floats
+ * FieldMathTool.cu:783-1128 */
+HFG_API int hfg_op_sample_fc_ex(const int res[3], const float origin[3], const float spacing[3], const float* vx,
+                                const float* vy, const float* vz, const float* pos, long long n, int sampling,
+                                float* out, void* stream);
 /* tranferFCVField2ParticlesInvoker  EulerParticlesTool.cu:805-868 */
 HFG_API int hfg_op_g2p_fc(const int res[3], const float origin[3], const float spacing[3], const float* vx,
                           const float* vy, const float* vz, const float* pos, long long n, int alg, float* out,
@@ -222,9 +244,21 @@ HFG_API int hfg_op_sl_advect_fc(const int res[3], const float origin[3], const f
 HFG_API int hfg_op_sl_advect_cc(const int res[3], const float origin[3], const float spacing[3], const float* in,
                                 const float* vx, const float* vy, const float* vz, float dt, int accuracy, float* out,
                                 void* stream);
+/* CSemiLagrangian::advect with the advection's ESamplingAlgorithm for every
+ * back-trace and final sample  SemiLagrangian.cpp:135-347 */
+HFG_API int hfg_op_sl_advect_fc_ex(const int res[3], const float origin[3], const float spacing[3], const float* ix,
+                                   const float* iy, const float* iz, const float* vx, const float* vy,
+                                   const float* vz, float dt, int accuracy, int sampling, float* ox, float* oy,
+                                   float* oz, void* stream);
+HFG_API int hfg_op_sl_advect_cc_ex(const int res[3], const float origin[3], const float spacing[3], const float* in,
+                                   const float* vx, const float* vy, const float* vz, float dt, int accuracy,
+                                   int sampling, float* out, void* stream);
 /* buildFluidSDFInvoker  EulerSolverTool.cu:760-785 (layers = the reference's
  * vExtrapolationDistance; blocks) */
 HFG_API int hfg_op_build_fluid_sdf(const int res[3], const float* domain, float* sdf, int layers, void* stream);
+/* buildFluidDensityInvoker  EulerSolverTool.cu:408-448,787-810; solid_sdf < 0 inside solids */
+HFG_API int hfg_op_build_fluid_density(const int res[3], const float* domain, const float* solid_sdf, float* out,
+                                       void* stream);
 /* generateFluidDomainFromBBoxInvoker  EulerSolverTool.cu:989-1013 */
 HFG_API int hfg_op_fluid_domain_from_bbox(const int res[3], const float origin[3], const float spacing[3],
                                           const float mn[3], const float mx[3], float* out, void* stream);

@@ -126,6 +126,75 @@ template <class T> static inline void sampleFC(const FC<T>& v, const GridGeom<T>
 }
 
 // ---------------------------------------------------------------------------
+// Cubic samplers (EulerMathTool.cu:134-240, FieldMathTool.cu:106-173).
+// ESamplingAlgorithm order (EnumType.h:3-10): 0 trilinear, 1 Catmull-Rom,
+// 2 monotonic Catmull-Rom, 3 Bridson cubic, 4 clamped Bridson cubic.  The
+// reference writes the Bridson weights with double literals, so for a float
+// Real they are evaluated in double (products of t alone stay in Real) and
+// the sum is rounded to Real; Catmull-Rom is all Real.
+// ---------------------------------------------------------------------------
+template <class T> static inline T cubicBridson1(const T* v, T t) {
+  double c0 = -1.0 / 3.0 * (double)t + 1.0 / 2.0 * (double)t * (double)t - 1.0 / 6.0 * (double)t * (double)t * (double)t;
+  double c1 = 1.0 - (double)(t * t) + 1.0 / 2.0 * (double)(t * t * t - t);
+  double c2 = (double)t + 1.0 / 2.0 * (double)(t * t - t * t * t);
+  double c3 = 1.0 / 6.0 * (double)(t * t * t - t);
+  return (T)(c0 * (double)v[0] + c1 * (double)v[1] + c2 * (double)v[2] + c3 * (double)v[3]);
+}
+template <class T> static inline T clampCUDA(T x, T a, T b) {  // EulerMathTool.cu:121-127
+  T mx = std::max(a, b), mn = std::min(a, b);
+  return std::max(mn, std::min(x, mx));
+}
+template <class T> static inline T catmullRom1(const T* v, T t, bool monotonic) {
+  T d1 = (v[2] - v[0]) / (T)2, d2 = (v[3] - v[1]) / (T)2, delta = v[2] - v[1];
+  if (monotonic) {
+    const T eps = std::numeric_limits<T>::epsilon();  // EPSILON (MMathExtra.h:43,55)
+    if (std::abs(delta) < eps) { d1 = 0; d2 = 0; }
+    if (delta * d1 < 0) d1 = 0;
+    if (delta * d2 < 0) d2 = 0;
+  }
+  T a3 = d1 + d2 - (T)2 * delta;
+  T a2 = (T)3 * delta - (T)2 * d1 - d2;
+  T a1 = d1, a0 = v[1];
+  return a3 * t * t * t + a2 * t * t + a1 * t + a0;
+}
+template <class T> static inline T cubic1(const T* v, T t, int alg) {
+  if (alg == 1) return catmullRom1(v, t, false);
+  if (alg == 2) return catmullRom1(v, t, true);
+  if (alg == 3) return cubicBridson1(v, t);
+  return clampCUDA(cubicBridson1(v, t), v[1], v[2]);
+}
+// sampleCellCenteredScalarFieldCubic (FieldMathTool.cu:106-173): the 4^3
+// clamp-to-edge neighbourhood around floor((p - o - h/2) / h), reduced along
+// x, then y, then z.
+template <class T> static inline T cubicSample(const T* f, const GridGeom<T>& g, T px, T py, T pz, int alg) {
+  T rx = px - g.o.x - g.h.x / 2;
+  T ry = py - g.o.y - g.h.y / 2;
+  T rz = pz - g.o.z - g.h.z / 2;
+  int ix = floorCUDA<T>(rx / g.h.x), iy = floorCUDA<T>(ry / g.h.y), iz = floorCUDA<T>(rz / g.h.z);
+  T tx = (rx - ((T)ix * g.h.x)) / g.h.x;
+  T ty = (ry - ((T)iy * g.h.y)) / g.h.y;
+  T tz = (rz - ((T)iz * g.h.z)) / g.h.z;
+  T vz[4];
+  for (int i = 0; i < 4; ++i) {
+    T vy[4];
+    for (int j = 0; j < 4; ++j) {
+      T vx[4];
+      for (int k = 0; k < 4; ++k) vx[k] = f[lin(ix + k - 1, iy + j - 1, iz + i - 1, g.r)];
+      vy[j] = cubic1(vx, tx, alg);
+    }
+    vz[i] = cubic1(vy, ty, alg);
+  }
+  return cubic1(vz, tz, alg);
+}
+template <class T> static inline T sampleAlg(const T* f, const GridGeom<T>& g, T px, T py, T pz, int alg) {
+  return alg == 0 ? trilerp(f, g, px, py, pz) : cubicSample(f, g, px, py, pz, alg);
+}
+template <class T>
+static inline void sampleFCAlg(const FC<T>& v, const GridGeom<T>& cc, T px, T py, T pz, int alg, T out[3]) {
+  for (int a = 0; a < 3; ++a) out[a] = sampleAlg(v.c[a].data(), faceGeom(cc, a), px, py, pz, alg);
+}
+
+// ---------------------------------------------------------------------------
 // Particle <-> grid transfers (EulerParticlesTool.cu:79-308)
 // ---------------------------------------------------------------------------
 
@@ -553,9 +622,11 @@ template <class T> static inline void axpy3(T a, const T v[3], T p[3]) {
 }
 
 template <class T>
-static inline void backTrace(const FC<T>& vel, const GridGeom<T>& cc, T dt, int acc, const T in[3], T out[3]) {
+static inline void backTrace(const FC<T>& vel, const GridGeom<T>& cc, T dt, int acc, const T in[3], T out[3],
+                             int samp = 0) {
   T v0[3], v1[3], v2[3], mid[3], tf[3];
   out[0] = in[0]; out[1] = in[1]; out[2] = in[2];
+  auto sampleFC = [&](const FC<T>& v, const GridGeom<T>& g, T x, T y, T z, T o[3]) { sampleFCAlg(v, g, x, y, z, samp, o); };
   sampleFC(vel, cc, in[0], in[1], in[2], v0);
   if (acc == 0) {
     axpy3(-dt, v0, out);
@@ -592,7 +663,8 @@ template <class T> static inline void fcPoint(const GridGeom<T>& g, int axis, in
 
 // CSemiLagrangian::advect (FC) SemiLagrangian.cpp:169-186
 template <class T>
-static void slAdvectFC(const GridGeom<T>& cc, const FC<T>& in, const FC<T>& vel, T dt, int acc, FC<T>& out) {
+static void slAdvectFC(const GridGeom<T>& cc, const FC<T>& in, const FC<T>& vel, T dt, int acc, FC<T>& out,
+                       int samp = 0) {
   for (int a = 0; a < 3; ++a) {
     GridGeom<T> fg = faceGeom(cc, a);
 #pragma omp parallel for collapse(2) schedule(static)
@@ -601,8 +673,8 @@ static void slAdvectFC(const GridGeom<T>& cc, const FC<T>& in, const FC<T>& vel,
         for (int x = 0; x < fg.r.x; ++x) {
           T p[3], q[3];
           fcPoint(cc, a, x, y, z, p);
-          backTrace(vel, cc, dt, acc, p, q);
-          out.c[a][lin(x, y, z, fg.r)] = trilerp(in.c[a].data(), fg, q[0], q[1], q[2]);
+          backTrace(vel, cc, dt, acc, p, q, samp);
+          out.c[a][lin(x, y, z, fg.r)] = sampleAlg(in.c[a].data(), fg, q[0], q[1], q[2], samp);
         }
   }
 }
@@ -610,15 +682,15 @@ static void slAdvectFC(const GridGeom<T>& cc, const FC<T>& in, const FC<T>& vel,
 // CSemiLagrangian::advect (CC scalar / vector) SemiLagrangian.cpp:135-167
 template <class T>
 static void slAdvectCC(const GridGeom<T>& cc, const std::vector<const T*>& in, const FC<T>& vel, T dt, int acc,
-                       const std::vector<T*>& out) {
+                       const std::vector<T*>& out, int samp = 0) {
 #pragma omp parallel for collapse(2) schedule(static)
   for (int z = 0; z < cc.r.z; ++z)
     for (int y = 0; y < cc.r.y; ++y)
       for (int x = 0; x < cc.r.x; ++x) {
         T p[3], q[3];
         ccPoint(cc, x, y, z, p);
-        backTrace(vel, cc, dt, acc, p, q);
-        for (size_t k = 0; k < in.size(); ++k) out[k][lin(x, y, z, cc.r)] = trilerp(in[k], cc, q[0], q[1], q[2]);
+        backTrace(vel, cc, dt, acc, p, q, samp);
+        for (size_t k = 0; k < in.size(); ++k) out[k][lin(x, y, z, cc.r)] = sampleAlg(in[k], cc, q[0], q[1], q[2], samp);
       }
 }
 
@@ -665,6 +737,7 @@ template <class T> struct Solver {
   V3<T> gravity{0, (T)-9.8, 0};  // ExternalForcesSolver.h:25
   // advection
   int adv = ADV_SL, acc = 2, alg = LINEAR, clampMode = 1;
+  int sampling = 0;  // ESamplingAlgorithm of the semi-Lagrangian samples (AdvectionSolver.h:50)
   T cfl = 1, mixing = 0.1f;
   bool sFlag = false, vFlag = false, velFlag = false;
   std::vector<T> ppos, pvel, pscalar, pvector;
@@ -784,10 +857,10 @@ template <class T> struct Solver {
     i64 N = g.r.size();
     if (adv == ADV_SL) {
       // SemiLagrangian.cpp:135-186
-      slAdvectFC(g, vin, vin, dt, acc, vout);
+      slAdvectFC(g, vin, vin, dt, acc, vout, sampling);
       if (advectScalars) {
         slAdvectCC<T>(g, {cIn[0].data(), cIn[1].data(), cIn[2].data(), dIn.data()}, vin, dt, acc,
-                      {cOut[0].data(), cOut[1].data(), cOut[2].data(), dOut.data()});
+                      {cOut[0].data(), cOut[1].data(), cOut[2].data(), dOut.data()}, sampling);
       }
       return;
     }
@@ -1016,6 +1089,29 @@ void orc_build_fluid_sdf(const int* res, const float* dom, int layers, float* sd
   }
 }
 
+// EulerSolverTool.cu:408-448 buildFluidDensity: 1 in the fluid, the surface
+// density 0.2 where a clamp-to-edge 6-neighbour is air (fluid domain and
+// solid both >= 0, isInsideAir EulerMathTool.cu:344-348), 0 elsewhere.
+void orc_build_fluid_density(const int* res, const float* dom, const float* solid, float* out) {
+  Res r{res[0], res[1], res[2]};
+  const int dx[6] = {-1, 1, 0, 0, 0, 0}, dy[6] = {0, 0, -1, 1, 0, 0}, dz[6] = {0, 0, 0, 0, -1, 1};
+  for (int z = 0; z < r.z; ++z)
+    for (int y = 0; y < r.y; ++y)
+      for (int x = 0; x < r.x; ++x) {
+        i64 c = lin(x, y, z, r);
+        float v = 0.f;
+        if (dom[c] < 0 && !(solid[c] < 0)) {
+          bool air = false;
+          for (int k = 0; k < 6; ++k) {
+            i64 nb = lin(x + dx[k], y + dy[k], z + dz[k], r);
+            air = air || (dom[nb] >= 0 && solid[nb] >= 0);
+          }
+          v = air ? (float)0.2 : 1.0f;
+        }
+        out[c] = v;
+      }
+}
+
 // EulerSolverTool.cu:581-608 generateFluidDomainFromBBox (strict inequalities)
 void orc_fluid_domain_from_bbox(const int* res, const float* o, const float* h, const float* mn, const float* mx,
                                 float* out) {
@@ -1150,6 +1246,30 @@ void orc_sample_fc(int dbl, const int* res, const float* o, const float* h, cons
   }
 }
 
+// Sampling of a cell-centred scalar field with an ESamplingAlgorithm
+// (FieldMathTool.cu:470-573), FP32 or FP64.
+void orc_sample_cc_alg(int dbl, const int* res, const float* o, const float* h, const float* f, const float* pos,
+                       long long M, int alg, float* out) {
+  if (dbl) {
+    GridGeom<double> g = mkGeom<double>(res, o, h);
+    std::vector<double> fd = up<double>(f, g.r.size());
+    for (i64 i = 0; i < M; ++i)
+      out[i] = (float)sampleAlg(fd.data(), g, (double)pos[3 * i], (double)pos[3 * i + 1], (double)pos[3 * i + 2], alg);
+  } else {
+    GridGeom<float> g = mkGeom<float>(res, o, h);
+    for (i64 i = 0; i < M; ++i) out[i] = sampleAlg(f, g, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], alg);
+  }
+}
+
+// Sampling of a face-centred field with an ESamplingAlgorithm
+// (FieldMathTool.cu:783-1128): out is 3 floats per point.
+void orc_sample_fc_alg(const int* res, const float* o, const float* h, const float* vx, const float* vy,
+                       const float* vz, const float* pos, long long M, int alg, float* out) {
+  GridGeom<float> g = mkGeom<float>(res, o, h);
+  FC<float> v = upFC<float>(g.r, vx, vy, vz);
+  for (i64 i = 0; i < M; ++i) sampleFCAlg(v, g, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], alg, &out[3 * i]);
+}
+
 // Trilinear sampling of a cell-centred scalar field.
 void orc_sample_cc(const int* res, const float* o, const float* h, const float* f, const float* pos, long long M,
                    float* out) {
@@ -1250,6 +1370,23 @@ void orc_sl_advect_fc(int dbl, const int* res, const float* o, const float* h, c
   }
 }
 
+// Semi-Lagrangian advection with an ESamplingAlgorithm for every sample.
+void orc_sl_advect_fc_alg(const int* res, const float* o, const float* h, const float* ix, const float* iy,
+                          const float* iz, const float* vx, const float* vy, const float* vz, float dt, int acc,
+                          int samp, float* ox, float* oy, float* oz) {
+  GridGeom<float> g = mkGeom<float>(res, o, h);
+  FC<float> in = upFC<float>(g.r, ix, iy, iz), v = upFC<float>(g.r, vx, vy, vz), out;
+  out.resize(g.r);
+  slAdvectFC<float>(g, in, v, dt, acc, out, samp);
+  downFC(out, ox, oy, oz);
+}
+void orc_sl_advect_cc_alg(const int* res, const float* o, const float* h, const float* in, const float* vx,
+                          const float* vy, const float* vz, float dt, int acc, int samp, float* out) {
+  GridGeom<float> g = mkGeom<float>(res, o, h);
+  FC<float> v = upFC<float>(g.r, vx, vy, vz);
+  slAdvectCC<float>(g, {in}, v, dt, acc, {out}, samp);
+}
+
 // Semi-Lagrangian advection of a cell-centred scalar field.
 void orc_sl_advect_cc(const int* res, const float* o, const float* h, const float* in, const float* vx,
                       const float* vy, const float* vz, float dt, int acc, float* out) {
@@ -1313,6 +1450,7 @@ static void sSetAdvection(OrcSolver* S, int kind, int acc, int alg, float cfl, f
   s.advectScalars = advectScalars != 0;
   s.sFlag = s.vFlag = s.velFlag = false;
 }
+template <class T> static void sSetSampling(OrcSolver* S, int samp) { pick<T>(S).sampling = samp; }
 template <class T> static void sSetParticles(OrcSolver* S, const float* pos, const float* vel, long long P) {
   Solver<T>& s = pick<T>(S);
   s.ppos = up<T>(pos, 3 * P);
@@ -1403,6 +1541,7 @@ void orc_solver_set_advection(void* p, int kind, int acc, int alg, float cfl, fl
                               int advectScalars) {
   ORC_CALL((OrcSolver*)p, sSetAdvection, kind, acc, alg, cfl, mixing, clampMode, advectScalars);
 }
+void orc_solver_set_sampling(void* p, int samp) { ORC_CALL((OrcSolver*)p, sSetSampling, samp); }
 void orc_solver_set_particles(void* p, const float* pos, const float* vel, long long P) {
   ORC_CALL((OrcSolver*)p, sSetParticles, pos, vel, P);
 }

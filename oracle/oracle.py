@@ -44,6 +44,7 @@ def lib():
             "orc_seed_particles": (C.c_longlong, [I3, F3, F3, PF, PF, C.c_int, C.c_ulonglong, PF]),
             "orc_fluid_domain_from_bbox": (None, [I3, F3, F3, F3, F3, PF]),
             "orc_build_fluid_sdf": (None, [I3, PF, C.c_int, PF]),
+            "orc_build_fluid_density": (None, [I3, PF, PF, PF]),
             "orc_markers_from_particles": (None, [I3, F3, F3, PF, PF, C.c_longlong, PU8, PU32]),
             "orc_markers_from_sdf": (None, [I3, PF, PF, PU8]),
             "orc_build_matrix_a": (None, [C.c_int, I3, F3, C.c_float, PU8, PF]),
@@ -53,6 +54,11 @@ def lib():
                                            C.c_double, C.c_longlong, PF, PD]),
             "orc_extrapolate": (None, [I3, PF, C.c_int, PF]),
             "orc_sample_fc": (None, [C.c_int, I3, F3, F3, PF, PF, PF, PF, C.c_longlong, PF]),
+            "orc_sample_cc_alg": (None, [C.c_int, I3, F3, F3, PF, PF, C.c_longlong, C.c_int, PF]),
+            "orc_sample_fc_alg": (None, [I3, F3, F3, PF, PF, PF, PF, C.c_longlong, C.c_int, PF]),
+            "orc_sl_advect_fc_alg": (None, [I3, F3, F3, PF, PF, PF, PF, PF, PF, C.c_float, C.c_int, C.c_int, PF, PF, PF]),
+            "orc_sl_advect_cc_alg": (None, [I3, F3, F3, PF, PF, PF, PF, C.c_float, C.c_int, C.c_int, PF]),
+            "orc_solver_set_sampling": (None, [vp, C.c_int]),
             "orc_sample_cc": (None, [I3, F3, F3, PF, PF, C.c_longlong, PF]),
             "orc_g2p_fc": (None, [I3, F3, F3, PF, PF, PF, PF, C.c_longlong, C.c_int, PF]),
             "orc_g2p_cc": (None, [I3, F3, F3, PF, PF, C.c_longlong, C.c_int, PF]),
@@ -151,6 +157,12 @@ def build_fluid_sdf(res, domain, layers=1000):
     return out
 
 
+def build_fluid_density(res, domain, solid_sdf):
+    out = np.empty(res[::-1], np.float32)
+    lib().orc_build_fluid_density(i3(res), fp(f32(domain).reshape(-1)), fp(f32(solid_sdf).reshape(-1)), fp(out))
+    return out
+
+
 def markers_from_particles(res, origin, spacing, solid_sdf, pos):
     ss = f32(solid_sdf).reshape(-1)
     p = f32(pos).reshape(-1)
@@ -224,11 +236,25 @@ def sample_fc(res, origin, spacing, vel, pos, dbl=0):
     return out.reshape(-1, 3)
 
 
-def sample_cc(res, origin, spacing, f, pos):
+def sample_cc(res, origin, spacing, f, pos, alg=0, dbl=0):
+    """alg: ESamplingAlgorithm (0 trilinear, 1 Catmull-Rom, 2 monotonic
+    Catmull-Rom, 3 Bridson cubic, 4 clamped Bridson cubic)."""
     p = f32(pos).reshape(-1)
     out = np.empty(p.size // 3, np.float32)
-    lib().orc_sample_cc(i3(res), f3(origin), f3(spacing), fp(f32(f).reshape(-1)), fp(p), p.size // 3, fp(out))
+    if alg == 0 and not dbl:
+        lib().orc_sample_cc(i3(res), f3(origin), f3(spacing), fp(f32(f).reshape(-1)), fp(p), p.size // 3, fp(out))
+    else:
+        lib().orc_sample_cc_alg(dbl, i3(res), f3(origin), f3(spacing), fp(f32(f).reshape(-1)), fp(p), p.size // 3,
+                                alg, fp(out))
     return out
+
+
+def sample_fc_alg(res, origin, spacing, vel, pos, alg):
+    p = f32(pos).reshape(-1)
+    out = np.empty(p.size, np.float32)
+    v = [f32(a).reshape(-1) for a in vel]
+    lib().orc_sample_fc_alg(i3(res), f3(origin), f3(spacing), *[fp(a) for a in v], fp(p), p.size // 3, alg, fp(out))
+    return out.reshape(-1, 3)
 
 
 def g2p_fc(res, origin, spacing, vel, pos, alg):
@@ -273,18 +299,26 @@ def advect_particles(res, origin, spacing, vel, pos, dt, cfl=1.0, accuracy=2, cl
     return p.reshape(-1, 3), n
 
 
-def sl_advect_fc(res, origin, spacing, field, vel, dt, accuracy, dbl=0):
+def sl_advect_fc(res, origin, spacing, field, vel, dt, accuracy, dbl=0, sampling=0):
     f = [f32(a).reshape(-1) for a in field]
     v = [f32(a).reshape(-1) for a in vel]
     out = [np.empty(s, np.float32) for s in face_shapes(res)]
+    if sampling:
+        lib().orc_sl_advect_fc_alg(i3(res), f3(origin), f3(spacing), *[fp(a) for a in f], *[fp(a) for a in v], dt,
+                                   accuracy, sampling, *[fp(a) for a in out])
+        return out
     lib().orc_sl_advect_fc(dbl, i3(res), f3(origin), f3(spacing), *[fp(a) for a in f], *[fp(a) for a in v], dt,
                            accuracy, *[fp(a) for a in out])
     return out
 
 
-def sl_advect_cc(res, origin, spacing, field, vel, dt, accuracy):
+def sl_advect_cc(res, origin, spacing, field, vel, dt, accuracy, sampling=0):
     v = [f32(a).reshape(-1) for a in vel]
     out = np.empty(res[::-1], np.float32)
+    if sampling:
+        lib().orc_sl_advect_cc_alg(i3(res), f3(origin), f3(spacing), fp(f32(field).reshape(-1)),
+                                   *[fp(a) for a in v], dt, accuracy, sampling, fp(out))
+        return out
     lib().orc_sl_advect_cc(i3(res), f3(origin), f3(spacing), fp(f32(field).reshape(-1)), *[fp(a) for a in v], dt,
                            accuracy, fp(out))
     return out
@@ -304,6 +338,9 @@ class Solver:
 
     def add_solid_boundary(self, sdf, vel=(0, 0, 0)):
         lib().orc_solver_add_boundary(self._h, fp(f32(sdf).reshape(-1)), *[float(v) for v in vel])
+
+    def set_sampling(self, alg):
+        lib().orc_solver_set_sampling(self._h, int(alg))
 
     def set_boundary_velocity(self, index, vel):
         lib().orc_solver_set_boundary_velocity(self._h, int(index), *[float(v) for v in vel])

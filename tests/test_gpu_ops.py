@@ -263,6 +263,66 @@ def test_semi_lagrangian(cuda, acc):
                                atol=1e-4)
 
 
+@pytest.mark.parametrize("samp", [1, 2, 3, 4])
+def test_cubic_sampling(cuda, samp):
+    """Catmull-Rom, monotonic Catmull-Rom, Bridson and clamped Bridson
+    sampling of a cell-centred grid and of the face grids against the FP32
+    oracle, points inside and outside the grid (clamp-to-edge)."""
+    rng = np.random.default_rng(80 + samp)
+    f = rng.standard_normal(RES[::-1]).astype(np.float32)
+    pos = random_particles(rng, 4000, margin=2.0)
+    out = torch.empty(4000, dtype=torch.float32, device=cuda)
+    hfgrid.op_sample_cc_ex(RES, ORIGIN, SPACING, dev(f), dev(pos), samp, out)
+    ref = oracle.sample_cc(RES, ORIGIN, SPACING, f, pos, alg=samp)
+    np.testing.assert_allclose(host(out), ref, rtol=1e-5, atol=1e-5)
+    v = face_arrays(RES, rng)
+    o3 = torch.empty((4000, 3), dtype=torch.float32, device=cuda)
+    hfgrid.op_sample_fc_ex(RES, ORIGIN, SPACING, [dev(a) for a in v], dev(pos), samp, o3)
+    np.testing.assert_allclose(host(o3), oracle.sample_fc_alg(RES, ORIGIN, SPACING, v, pos, samp), rtol=1e-5,
+                               atol=1e-5)
+
+
+def test_cubic_sampling_reference_cases(cuda):
+    """The reference's own cubic-sampling known answers
+    (UnitTest-CellCenteredScalarField.cu) through the GPU entry point."""
+    import json
+    import os
+    import test_oracle_golden as gold
+    cases = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "sampling_golden.json")))["cases"]
+    for case in cases:
+        res, dres = case["res"], case.get("res2", case["res"])
+        src = gold._grid_eval(case["src"], res)
+        pos = np.stack([gold._grid_eval(case["pos"][a], dres) for a in "XYZ"], axis=-1).reshape(-1, 3)
+        out = torch.empty(pos.shape[0], dtype=torch.float32, device=cuda)
+        hfgrid.op_sample_cc_ex(res, case["origin"], case["spacing"], dev(src), dev(pos),
+                               gold.SAMPLING_ALG[case["alg"]], out)
+        got = host(out)
+        for e in case["expect"]:
+            assert abs(got[e["index"]] - e["value"]) < 1e-4, (case["line"], e)
+        if "expect_formula" in case:
+            assert np.abs(got - gold._grid_eval(case["expect_formula"], dres).reshape(-1)).max() < 1e-4
+
+
+@pytest.mark.parametrize("samp", [1, 2, 3, 4])
+def test_semi_lagrangian_cubic(cuda, samp):
+    """Semi-Lagrangian RK3 advection with a cubic sampler for every back-trace
+    and final sample, against the FP32 oracle with the same sampler."""
+    rng = np.random.default_rng(90 + samp)
+    v = face_arrays(RES, rng, 0.2)
+    f = face_arrays(RES, rng)
+    out = [torch.empty(s, dtype=torch.float32, device=cuda) for s in oracle.face_shapes(RES)]
+    hfgrid.op_sl_advect_fc(RES, ORIGIN, SPACING, [dev(a) for a in f], [dev(a) for a in v], 0.05, 2, out,
+                           sampling=samp)
+    ref = oracle.sl_advect_fc(RES, ORIGIN, SPACING, f, v, 0.05, 2, sampling=samp)
+    for a in range(3):
+        np.testing.assert_allclose(host(out[a]), ref[a], rtol=1e-4, atol=1e-4)
+    c = rng.standard_normal(RES[::-1]).astype(np.float32)
+    o1 = torch.empty(RES[::-1], dtype=torch.float32, device=cuda)
+    hfgrid.op_sl_advect_cc(RES, ORIGIN, SPACING, dev(c), [dev(a) for a in v], 0.05, 2, o1, sampling=samp)
+    np.testing.assert_allclose(host(o1), oracle.sl_advect_cc(RES, ORIGIN, SPACING, c, v, 0.05, 2, sampling=samp),
+                               rtol=1e-4, atol=1e-4)
+
+
 def test_fluid_domain_and_seeding_bit_exact(cuda):
     res = (24, 20, 16)
     h = tuple(1.0 / r for r in res)
@@ -293,3 +353,17 @@ def test_fluid_sdf_bit_exact(cuda):
         out = torch.empty(res[::-1], dtype=torch.float32, device=cuda)
         hfgrid.op_build_fluid_sdf(res, dev(dom), out, layers)
         assert np.array_equal(host(out), oracle.build_fluid_sdf(res, dom, layers))
+
+
+def test_fluid_density_bit_exact(cuda):
+    """buildFluidDensity (EulerSolverTool.cu:408-448): 1 / 0.2 / 0 exactly."""
+    rng = np.random.default_rng(61)
+    res = (19, 15, 11)
+    dom = np.where(rng.random(res[::-1]) < 0.5, -500.0, 500.0).astype(np.float32)
+    dom[:, :6, :8] = -500.0
+    solid = np.where(rng.random(res[::-1]) < 0.1, -1.0, np.finfo(np.float32).max).astype(np.float32)
+    out = torch.empty(res[::-1], dtype=torch.float32, device=cuda)
+    hfgrid.op_build_fluid_density(res, dev(dom), dev(solid), out)
+    ref = oracle.build_fluid_density(res, dom, solid)
+    assert np.array_equal(host(out), ref)
+    assert set(np.unique(ref)) <= {0.0, np.float32(0.2), 1.0}

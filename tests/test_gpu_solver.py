@@ -213,3 +213,18 @@ def test_moving_boxes_multigrid_vs_fp64(cuda):
         # b(u) after the projection is the CG residual b - A p (rel 1e-6) plus
         # the FP32 rounding of the gradient update
         assert st["divergence_l2"] <= 1e-4 * st["cg_rhs_norm"]
+
+
+def test_semi_lagrangian_solver_catmull_rom(cuda):
+    """The solver in semi-Lagrangian mode with the Catmull-Rom sampler
+    (setSamplingAlg) against the FP64 oracle with the same sampler."""
+    sc = small_scene((16, 14, 12))
+    g = scenes.gpu_solver(sc, precond=1, tol_mode=1, tol=1e-7, max_iter=500, advect_scalars=True,
+                          kind=hfgrid.ADV_SEMI_LAGRANGIAN, sampling=hfgrid.SAMPLE_CATMULLROM)
+    o = oracle_twin(sc, g, 1, 1, 1, 1e-9, 2000, kind=hfgrid.ADV_SEMI_LAGRANGIAN)
+    o.set_sampling(hfgrid.SAMPLE_CATMULLROM)
+    for _ in range(3):
+        g.update()
+        o.update()
+    assert (g.markers() != o.markers()).mean() < 2e-3
+    assert vel_rel_l2(g.velocity_field(), o.velocity_field()) < 1e-3

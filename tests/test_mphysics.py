@@ -127,6 +127,9 @@ def test_loaded_scene_matches_oracle(cuda):
         for a, gr in zip((gz, gy, gx), ref):
             np.testing.assert_allclose(a, gr[1:-1, 1:-1, 1:-1], rtol=1e-5, atol=1e-3)
 
+        # generateCurFluidDensity on the same current domain and total solid
+        assert np.array_equal(g.fluid_density(), oracle.build_fluid_density(res, g.fluid_domain_field(), solid))
+
         # loading a name that exists stops the load and keeps the old simulator
         L.loadScene(scene_json(seed=9).encode())
         assert L.getEulerParticleSize(b"Water") == n

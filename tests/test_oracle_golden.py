@@ -199,3 +199,51 @@ def test_golden_fixture_coverage():
     """The fixture carries the reference's expectations for the hot path."""
     n = {s: sum(len(t["expect"]) for t in v["tests"].values()) for s, v in GOLDEN.items()}
     assert n["Extrapolation"] >= 200 and n["PressureSolver"] >= 200 and n["ParticlesAdvection"] >= 300
+
+
+# ------------------------------------------------- cubic samplers (DataStructure)
+SAMPLING = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "sampling_golden.json")))
+SAMPLING_ALG = {"CATMULLROM": 1, "MONOCATMULLROM": 2, "CUBICBRIDSON": 3, "CLAMPCUBICBRIDSON": 4}
+
+
+class _Res:
+    def __init__(self, r):
+        self.x, self.y, self.z = r
+
+
+def _grid_eval(expr, res, dtype=np.float32):
+    """Evaluate a formula of the reference test in i (z), j (y), k (x) over a
+    grid, with the test's C++ int division ((Int)(k / 2)) as truncation."""
+    py = expr.replace("(Int)", "int")
+    out = np.empty((res[2], res[1], res[0]), dtype)
+    env = {"Res": _Res(res), "Res2": _Res(res), "int": int}
+    for i in range(res[2]):
+        for j in range(res[1]):
+            for k in range(res[0]):
+                out[i, j, k] = eval(py, env, {"i": i, "j": j, "k": k})
+    return out
+
+
+@pytest.mark.parametrize("case", SAMPLING["cases"], ids=lambda c: f"{c['alg']}@{c['line']}")
+def test_cubic_sampling_golden(case):
+    """UnitTest-CellCenteredScalarField.cu: the oracle's Catmull-Rom,
+    monotonic Catmull-Rom, Bridson and clamped Bridson samplers reproduce
+    every expectation of the reference's own tests (tolerance 1e-4, the
+    tests' GRID_SOLVER_EPSILON), in FP32 and FP64."""
+    res = case["res"]
+    dres = case.get("res2", res)
+    src = _grid_eval(case["src"], res)
+    pos = np.stack([_grid_eval(case["pos"][a], dres) for a in "XYZ"], axis=-1).reshape(-1, 3)
+    for dbl in (0, 1):
+        out = oracle.sample_cc(res, case["origin"], case["spacing"], src, pos, alg=SAMPLING_ALG[case["alg"]], dbl=dbl)
+        for e in case["expect"]:
+            assert abs(out[e["index"]] - e["value"]) < 1e-4, (e, out[e["index"]])
+        if "expect_formula" in case:
+            ref = _grid_eval(case["expect_formula"], dres).reshape(-1)
+            assert np.abs(out - ref).max() < 1e-4
+
+
+def test_sampling_fixture_coverage():
+    algs = {c["alg"] for c in SAMPLING["cases"]}
+    assert algs == set(SAMPLING_ALG)
+    assert sum(len(c["expect"]) + ("expect_formula" in c) for c in SAMPLING["cases"]) >= 70
