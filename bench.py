@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--workload", default="dam-break", choices=["dam-break", "serve", "batch", "moving-boxes"],
                     help="dam-break: the 256^3 headline line; serve: Poisson stream of mixed-size requests "
                          "through the scene server vs each request run plain; batch: many uneven scenes at once")
+    ap.add_argument("--mg-smooth", type=int, default=0, help="multigrid smoothing sweeps per level (0: library default)")
+    ap.add_argument("--pressure-fp64", action="store_true",
+                    help="accumulate the pressure in FP64 (divergence follows the CG residual)")
     ap.add_argument("--requests", type=int, default=100, help="serve/batch: number of scenes")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: arrivals per second")
     ap.add_argument("--slots", type=int, default=16, help="serve/batch: concurrent scenes")
@@ -284,7 +287,7 @@ def run_moving_boxes(args):
     s.generate_fluid_domain_from_bbox(mn, mx)
     s.set_advection(hfgrid.ADV_MIX_PIC_FLIP, hfgrid.RK3, hfgrid.LINEAR, sc.cfl, sc.mixing)
     s.set_options(precond=hfgrid.PRECOND_MG, tol_mode=hfgrid.TOL_RELATIVE, tol=1e-6, max_iter=200,
-                  advect_scalars=0, report_divergence=1)
+                  advect_scalars=0, report_divergence=1, pressure_fp64=int(args.pressure_fp64))
     s.seed_particles(sc.per_cell, sc.seed)
     stream = torch.cuda.ExternalStream(s.stream)
     t = 0.0
@@ -325,6 +328,7 @@ def run_moving_boxes(args):
             "dtype": "f32 (MG preconditioner with BF16 coarse levels, FP64 dots)", "data": "synthetic (seeded)",
             "config": {"workload": "C3: 512x256x512 dam break, three boxes (side 0.2) on sinusoidal paths "
                                    "(amplitude 0.1, period 2 s), 8 ppc, MG-PCG rel 1e-6 max 200",
+                       "pressure": "fp64" if args.pressure_fp64 else "fp32",
                        "cells": N, "particles": s.num_particles},
             "per_step": per_step, "clocks": clk}
     print(json.dumps(line), flush=True)
@@ -359,7 +363,7 @@ def main():
     precond = {"jacobi": hfgrid.PRECOND_JACOBI, "identity": hfgrid.PRECOND_IDENTITY, "mg": hfgrid.PRECOND_MG}[args.precond]
     sc = scenes.dam_break_256(seed=rank, n=args.res)
     s = scenes.gpu_solver(sc, precond=precond, tol_mode=hfgrid.TOL_RELATIVE, tol=1e-6, max_iter=200,
-                          advect_scalars=False)
+                          advect_scalars=False, pressure_fp64=int(args.pressure_fp64), mg_smooth=args.mg_smooth)
     stream = torch.cuda.ExternalStream(s.stream)
 
     for _ in range(args.warmup):

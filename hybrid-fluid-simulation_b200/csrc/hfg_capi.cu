@@ -337,6 +337,24 @@ HFG_API int hfg_solver_get_fluid_density(hfg_solver_t s, float* out) {
     return HFG_OK;
   });
 }
+HFG_API int hfg_solver_mix_vel_field_with_others(hfg_solver_t s, const float* vx, const float* vy, const float* vz,
+                                                 const float* others_density, const float* fluid_density) {
+  return guarded([&]() -> int {
+    SOLVER(s);
+    NEED(vx && vy && vz && others_density && fluid_density, "null argument");
+    const float* o[3] = {vx, vy, vz};
+    S.mixVelFieldWithOthers(o, others_density, fluid_density);
+    return HFG_OK;
+  });
+}
+HFG_API int hfg_solver_transfer_vel_to_particles(hfg_solver_t s, const float* pos, long long n, int alg, float* vel) {
+  return guarded([&]() -> int {
+    SOLVER(s);
+    NEED(n >= 0 && (n == 0 || (pos && vel)) && alg >= 0 && alg <= 4, "invalid arguments");
+    S.transferVelToParticles(pos, n, alg, vel);
+    return HFG_OK;
+  });
+}
 HFG_API long long hfg_solver_num_particles(hfg_solver_t s) { return (s && s->s) ? s->s->numParticles() : -1; }
 HFG_API int hfg_solver_get_particles(hfg_solver_t s, float* pos, float* vel) {
   return guarded([&]() -> int {
@@ -470,7 +488,8 @@ HFG_API int hfg_op_build_rhs(const int res[3], const float spacing[3], const flo
     check(launchStencilCode(g.r, cg.x, markers, code.p, st(stream)), "code");
     ConstFaceField v{{vx, vy, vz}}, sv{{svx, svy, svz}};
     SolidVelTable none{};
-    check(launchRhsInit(g, v, sv, none, markers, code.p, 1.f, 1.f, 1.f, b, r.p, x.p, p.p, part.p, cs.p, 0, st(stream)),
+    check(launchRhsInit(g, v, sv, none, markers, code.p, 1.f, 1.f, 1.f, b, r.p, x.p, false, p.p, part.p, cs.p, 0,
+                        st(stream)),
           "rhs");
     check(cudaStreamSynchronize(st(stream)), "sync");
     return HFG_OK;
@@ -493,7 +512,7 @@ HFG_API int hfg_op_project(const int res[3], const float spacing[3], float dt, c
     Scratch<double> part(cgPartialsNeeded(g.r), s);
     Scratch<CgState> cs(1, s);
     CgMaps maps;
-    check(makeCgMaps(cg, code.p, r.p, x.p, p0.p, p1.p, &maps), "tensor maps");
+    check(makeCgMaps(cg, code.p, r.p, x.p, false, p0.p, p1.p, &maps), "tensor maps");
     CgState init{};
     init.maxIter = (int)std::min<long long>(max_iter < 0 ? N : max_iter, 0x7fffffff);
     init.precond = precond == HFG_PRECOND_JACOBI ? 1 : 0;
@@ -505,7 +524,7 @@ HFG_API int hfg_op_project(const int res[3], const float spacing[3], float dt, c
     check(launchStencilCode(g.r, cg.x, markers, code.p, s), "code");
     ConstFaceField v{{vx, vy, vz}}, sv{{svx, svy, svz}};
     SolidVelTable none{};
-    check(launchRhsInit(g, v, sv, none, markers, code.p, sx, sy, sz, nullptr, r.p, x.p, p0.p, part.p, cs.p,
+    check(launchRhsInit(g, v, sv, none, markers, code.p, sx, sy, sz, nullptr, r.p, x.p, false, p0.p, part.p, cs.p,
                         init.precond, s),
           "rhs");
     CgState host{};
@@ -517,8 +536,8 @@ HFG_API int hfg_op_project(const int res[3], const float spacing[3], float dt, c
         check(launchCgDirection(cg, sx, sy, sz, maps.rH, maps.pH[po], maps.codeH, code.p, r.p, pb[po], pb[pn], part.p,
                                 cs.p, init.precond, s),
               "cg");
-        check(launchCgUpdate(cg, sx, sy, sz, maps.pH[pn], maps.rI, maps.xI, maps.codeI, pb[pn], x.p, r.p, part.p, cs.p,
-                             init.precond, s),
+        check(launchCgUpdate(cg, sx, sy, sz, maps.pH[pn], maps.rI, maps.xI, maps.codeI, pb[pn], x.p, false, r.p, part.p,
+                             cs.p, init.precond, s),
               "cg");
       }
       check(cudaMemcpyAsync(&host, cs.p, sizeof(host), cudaMemcpyDeviceToHost, s), "read state");
@@ -528,7 +547,7 @@ HFG_API int hfg_op_project(const int res[3], const float spacing[3], float dt, c
     if (host.error) return fail(HFG_ERR_TIMEOUT, "pressure CG: a stage load did not complete in time");
     FaceField vv{{vx, vy, vz}};
     check(launchGradient(g, dt / (1.0f * spacing[0]), dt / (1.0f * spacing[1]), dt / (1.0f * spacing[2]), markers,
-                         x.p, vv, sv, none, s),
+                         x.p, false, vv, sv, none, s),
           "gradient");
     if (pOut)
       check(cudaMemcpy2DAsync(pOut, (size_t)g.r.x * 4, x.p, (size_t)cg.x * 4, (size_t)g.r.x * 4,
@@ -786,6 +805,40 @@ HFG_API int hfg_op_build_fluid_density(const int res[3], const float* domain, co
   return guarded([&]() -> int {
     NEED(validRes(res) && domain && solid_sdf && out, "invalid arguments");
     check(launchFluidDensity(toRes(res), domain, solid_sdf, nullptr, out, st(stream)), "fluid density");
+    return HFG_OK;
+  });
+}
+HFG_API int hfg_op_mix_field_with_density_cc(long long n, const float* a, float* b, const float* wa, const float* wb,
+                                             void* stream) {
+  return guarded([&]() -> int {
+    NEED(n >= 0 && (n == 0 || (a && b && wa && wb)), "invalid arguments");
+    if (n == 0) return HFG_OK;
+    const float* A[3] = {a, nullptr, nullptr};
+    float* B[3] = {b, nullptr, nullptr};
+    Dim3i r{(int)std::min<long long>(n, 1LL << 30), 1, 1};
+    NEED(n < (1LL << 30), "too many entries");
+    check(launchMixFieldWithDensity(r, 0, A, B, wa, wb, st(stream)), "mix");
+    return HFG_OK;
+  });
+}
+HFG_API int hfg_op_mix_field_with_density_fc(const int res[3], const float* ax, const float* ay, const float* az,
+                                             float* bx, float* by, float* bz, const float* wa, const float* wb,
+                                             void* stream) {
+  return guarded([&]() -> int {
+    NEED(validRes(res) && ax && ay && az && bx && by && bz && wa && wb, "invalid arguments");
+    const float* A[3] = {ax, ay, az};
+    float* B[3] = {bx, by, bz};
+    check(launchMixFieldWithDensity(toRes(res), 1, A, B, wa, wb, st(stream)), "mix");
+    return HFG_OK;
+  });
+}
+HFG_API int hfg_op_mix_particle_vel_pic_flip(const float* pic, const float* flip, const float* dist, long long n,
+                                             float cell, float g_rate, float gf_rate, float f_rate, float p_rate,
+                                             float* predict, void* stream) {
+  return guarded([&]() -> int {
+    NEED(n >= 0 && (n == 0 || (pic && flip && dist && predict)), "invalid arguments");
+    check(launchMixParticleVel(pic, flip, dist, n, cell, g_rate, gf_rate, f_rate, p_rate, predict, st(stream)),
+          "mix");
     return HFG_OK;
   });
 }

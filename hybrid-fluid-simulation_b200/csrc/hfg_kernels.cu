@@ -244,8 +244,9 @@ cudaError_t launchFluidDomainFromBBox(const Geom& g, const float mn[3], const fl
 // EulerSolverTool.cu:229-322 applyPressureGradient: faces with a fluid side
 // and a solid side take the solid velocity, fluid-fluid/fluid-air faces get
 // -dt/(rho h) * dp, all others and the far boundary faces become UNKNOWN.
+template <class TP>
 __global__ void kGradient(Geom g, float gx, float gy, float gz, const uint8_t* __restrict__ mk,
-                          const float* __restrict__ p, FaceField v, ConstFaceField svArr, SolidVelTable svTab) {
+                          const TP* __restrict__ p, FaceField v, ConstFaceField svArr, SolidVelTable svTab) {
   const Dim3i R = g.r;
   const Dim3i rx{R.x + 1, R.y, R.z}, ry{R.x, R.y + 1, R.z}, rz{R.x, R.y, R.z + 1};
   HFG_FOR(c, R.size()) {
@@ -274,7 +275,9 @@ __global__ void kGradient(Geom g, float gx, float gy, float gz, const uint8_t* _
           else s = solidFaceVel(svTab, co[a] == c ? 0 : svTab.solidIdx[co[a]], svTab.solidIdx[c], a);
           vv[fo[a]] = s;
         } else {
-          vv[fo[a]] = __fsub_rn(vv[fo[a]], __fmul_rn(gs[a], __fsub_rn(p[pc], p[po[a]])));
+          const float dp = sizeof(TP) == 8 ? __double2float_rn(__dsub_rn((double)p[pc], (double)p[po[a]]))
+                                           : __fsub_rn((float)p[pc], (float)p[po[a]]);
+          vv[fo[a]] = __fsub_rn(vv[fo[a]], __fmul_rn(gs[a], dp));
         }
       } else {
         vv[fo[a]] = kUnknown;
@@ -285,9 +288,15 @@ __global__ void kGradient(Geom g, float gx, float gy, float gz, const uint8_t* _
     if (z == R.z - 1) v.c[2][fz + (long long)rz.x * rz.y] = kUnknown;
   }
 }
-cudaError_t launchGradient(const Geom& g, float gx, float gy, float gz, const uint8_t* markers, const float* p,
-                           FaceField v, ConstFaceField svArr, const SolidVelTable& svTab, cudaStream_t s) {
-  kGradient<<<gridFor(g.r.size()), kThreads, 0, s>>>(g, gx, gy, gz, markers, p, v, svArr, svTab);
+cudaError_t launchGradient(const Geom& g, float gx, float gy, float gz, const uint8_t* markers, const void* p,
+                           bool pDouble, FaceField v, ConstFaceField svArr, const SolidVelTable& svTab,
+                           cudaStream_t s) {
+  if (pDouble)
+    kGradient<double><<<gridFor(g.r.size()), kThreads, 0, s>>>(g, gx, gy, gz, markers, (const double*)p, v, svArr,
+                                                               svTab);
+  else
+    kGradient<float><<<gridFor(g.r.size()), kThreads, 0, s>>>(g, gx, gy, gz, markers, (const float*)p, v, svArr,
+                                                              svTab);
   return cudaGetLastError();
 }
 
@@ -577,6 +586,78 @@ __global__ void kFluidDensity(Dim3i r, const float* __restrict__ dom, const floa
 cudaError_t launchFluidDensity(const Dim3i& r, const float* dom, const float* solidSdf, const uint8_t* solidIdx,
                                float* out, cudaStream_t s) {
   kFluidDensity<<<gridFor(r.size()), kThreads, 0, s>>>(r, dom, solidSdf, solidIdx, out);
+  return cudaGetLastError();
+}
+
+// Grid <-> particle mixing of the hybrid coupler.
+// HybridSimulatorMixFieldWithDensity.cu:6-265: B := (wA A + wB B) / (wA + wB)
+// where wA + wB > FLT_EPSILON; on a face grid the weights are the means of the
+// two adjacent cells (clamp to edge), scaled by the reference's double 0.5.
+__device__ __forceinline__ void mixOne(float a, float& b, float wa, float wb) {
+  float s = __fadd_rn(wa, wb);
+  if (s > FLT_EPSILON) b = __fdiv_rn(__fadd_rn(__fmul_rn(wa, a), __fmul_rn(wb, b)), s);
+}
+__global__ void kMixCell(long long n, const float* __restrict__ a, float* __restrict__ b, const float* __restrict__ wa,
+                         const float* __restrict__ wb) {
+  HFG_FOR(i, n) {
+    float v = b[i];
+    mixOne(a[i], v, wa[i], wb[i]);
+    b[i] = v;
+  }
+}
+__global__ void kMixFace(Dim3i r, int axis, const float* __restrict__ a, float* __restrict__ b,
+                         const float* __restrict__ wa, const float* __restrict__ wb) {
+  const Dim3i f{r.x + (axis == 0), r.y + (axis == 1), r.z + (axis == 2)};
+  HFG_FOR(c, f.size()) {
+    int x, y, z;
+    cellCoord(c, f, x, y, z);
+    long long lo = linc(x - (axis == 0), y - (axis == 1), z - (axis == 2), r), hi = linc(x, y, z, r);
+    float wA = __double2float_rn(__dmul_rn((double)__fadd_rn(wa[lo], wa[hi]), 0.5));
+    float wB = __double2float_rn(__dmul_rn((double)__fadd_rn(wb[lo], wb[hi]), 0.5));
+    float v = b[c];
+    mixOne(a[c], v, wA, wB);
+    b[c] = v;
+  }
+}
+cudaError_t launchMixFieldWithDensity(const Dim3i& r, int face, const float* const a[3], float* const b[3],
+                                      const float* wa, const float* wb, cudaStream_t s) {
+  if (!face) {
+    kMixCell<<<gridFor(r.size()), kThreads, 0, s>>>(r.size(), a[0], b[0], wa, wb);
+    return cudaGetLastError();
+  }
+  for (int axis = 0; axis < 3; ++axis) {
+    kMixFace<<<gridFor(r.size()), kThreads, 0, s>>>(r, axis, a[axis], b[axis], wa, wb);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+// HybridSimulatorMixParitcleVelWithPICAndFLIP.cu:5-57: by the particle's
+// distance d: PIC up to g cells, PIC -> predicted up to gf, FLIP up to f,
+// FLIP -> predicted up to p, predicted beyond (lerp(a, b, t) = a + t (b - a)).
+__global__ void kMixParticleVel(const float* __restrict__ pic, const float* __restrict__ flip,
+                                const float* __restrict__ dist, long long n, float cell, float g, float gf, float fr,
+                                float pr, float* __restrict__ predict) {
+  const float dg = __fmul_rn(g, cell), dgf = __fmul_rn(gf, cell), df = __fmul_rn(fr, cell), dp = __fmul_rn(pr, cell);
+  HFG_FOR(i, n) {
+    const float d = dist[i];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float P = pic[3 * i + a], F = flip[3 * i + a], Q = predict[3 * i + a];
+      float m;
+      if (d <= dg) m = P;
+      else if (d <= dgf) m = __fadd_rn(P, __fmul_rn(__fdiv_rn(__fsub_rn(d, dg), __fsub_rn(dgf, dg)), __fsub_rn(Q, P)));
+      else if (d <= df) m = F;
+      else if (d <= dp) m = __fadd_rn(F, __fmul_rn(__fdiv_rn(__fsub_rn(d, df), __fsub_rn(dp, df)), __fsub_rn(Q, F)));
+      else m = Q;
+      predict[3 * i + a] = m;
+    }
+  }
+}
+cudaError_t launchMixParticleVel(const float* pic, const float* flip, const float* dist, long long n, float cell,
+                                 float g, float gf, float f, float p, float* predict, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  kMixParticleVel<<<gridFor(n), kThreads, 0, s>>>(pic, flip, dist, n, cell, g, gf, f, p, predict);
   return cudaGetLastError();
 }
 
@@ -883,7 +964,11 @@ __global__ void __launch_bounds__(256, 4) kSubstep(Geom g, ConstFaceField vel, f
   float bmin[3] = {g.ox, g.oy, g.oz};
   float bmax[3] = {g.ox + (float)g.r.x * g.hx, g.oy + (float)g.r.y * g.hy, g.oz + (float)g.r.z * g.hz};
   float m = 0.f;
+  __shared__ float cacheVal[24 * kThreads];
+  __shared__ int cacheKey[9 * kThreads];
+  StencilCache sc{cacheVal, cacheKey, (int)threadIdx.x, kThreads};
   HFG_FOR(p, P) {
+    sc.reset();
     float q[3] = {pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]};
     float w0[3] = {v0[3 * p], v0[3 * p + 1], v0[3 * p + 2]};
     if (acc == 0) {
@@ -893,17 +978,17 @@ __global__ void __launch_bounds__(256, 4) kSubstep(Geom g, ConstFaceField vel, f
       float mid[3], w1[3];
 #pragma unroll
       for (int a = 0; a < 3; ++a) mid[a] = fmaf(half, w0[a], q[a]);
-      sampleFaceFast(vel, g, mid[0], mid[1], mid[2], w1);
+      sampleFaceCached(vel, g, mid[0], mid[1], mid[2], sc, w1);
 #pragma unroll
       for (int a = 0; a < 3; ++a) q[a] = fmaf(ds, w1[a], q[a]);
     } else {
       float mid[3], tf[3], w1[3], w2[3];
 #pragma unroll
       for (int a = 0; a < 3; ++a) mid[a] = fmaf(half, w0[a], q[a]);
-      sampleFaceFast(vel, g, mid[0], mid[1], mid[2], w1);
+      sampleFaceCached(vel, g, mid[0], mid[1], mid[2], sc, w1);
 #pragma unroll
       for (int a = 0; a < 3; ++a) tf[a] = fmaf(tq, w1[a], q[a]);
-      sampleFaceFast(vel, g, tf[0], tf[1], tf[2], w2);
+      sampleFaceCached(vel, g, tf[0], tf[1], tf[2], sc, w2);
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         q[a] = fmaf(a29, w0[a], q[a]);
@@ -918,7 +1003,7 @@ __global__ void __launch_bounds__(256, 4) kSubstep(Geom g, ConstFaceField vel, f
       }
     } else {
       float v[3];
-      sampleFaceFast(vel, g, q[0], q[1], q[2], v);
+      sampleFaceCached(vel, g, q[0], q[1], q[2], sc, v);
       v0[3 * p] = v[0]; v0[3 * p + 1] = v[1]; v0[3 * p + 2] = v[2];
       m = fmaxf(m, fmaxf(fabsf(v[0]), fmaxf(fabsf(v[1]), fabsf(v[2]))));
     }

@@ -109,14 +109,16 @@ cudaError_t launchApplyA(const Dim3i& r, float sx, float sy, float sz, const Cod
 // code, r, x and p are pitched.
 cudaError_t launchRhsInit(const Geom& g, ConstFaceField v, ConstFaceField svArr, const SolidVelTable& svTab,
                           const uint8_t* markers, const Code* code, float ax, float ay, float az, float* b,
-                          float* r, float* x, float* p, double* partials, CgState* st, int precond, cudaStream_t s);
+                          float* r, void* x, bool xDouble, float* p, double* partials, CgState* st, int precond,
+                          cudaStream_t s);
 // TMA descriptors of the CG vectors on the pitched grid cg = cgDims(r):
 // halo boxes (H) for the arrays read with neighbours, plain tiles (I) else.
 struct CgMaps {
   CUtensorMap codeH, codeI, rH, rI, xI, pH[2];
 };
-cudaError_t makeCgMaps(const Dim3i& cg, const Code* code, const float* r, const float* x, const float* p0,
-                       const float* p1, CgMaps* m);
+// x: the pressure iterate, FP32 or (xDouble) FP64
+cudaError_t makeCgMaps(const Dim3i& cg, const Code* code, const float* r, const void* x, bool xDouble,
+                       const float* p0, const float* p1, CgMaps* m);
 cudaError_t makeHaloMap(const Dim3i& cg, const float* v, CUtensorMap* m);
 // precond: 0 identity, 1 Jacobi, 2 z read through mZ (must match CgState::precond);
 // mZ is the halo map of r (precond 0, 1) or of z (2); zr the same array.
@@ -125,8 +127,8 @@ cudaError_t launchCgDirection(const Dim3i& cg, float sx, float sy, float sz, con
                               const float* pOld, float* pNew, double* partials, CgState* st, int precond,
                               cudaStream_t s);
 cudaError_t launchCgUpdate(const Dim3i& cg, float sx, float sy, float sz, const CUtensorMap& mP, const CUtensorMap& mR,
-                           const CUtensorMap& mX, const CUtensorMap& mCode, const float* p, float* x, float* r,
-                           double* partials, CgState* st, int precond, cudaStream_t s);
+                           const CUtensorMap& mX, const CUtensorMap& mCode, const float* p, void* x, bool xDouble,
+                           float* r, double* partials, CgState* st, int precond, cudaStream_t s);
 // Divergence residual of the projected velocity over the fluid cells:
 // *sumOut = sum b^2 (FP64), ticketAndMax[1] = bits of max |b|.  `scratch`
 // holds 2 * divergenceBlocks() doubles.
@@ -134,9 +136,10 @@ inline int divergenceBlocks() { return 1024; }
 cudaError_t launchDivergenceNorm(const Geom& g, ConstFaceField v, const SolidVelTable& svTab,
                                  const uint8_t* markers, double* scratch, unsigned* ticketAndMax, double* sumOut,
                                  cudaStream_t s);
-// p pitched
-cudaError_t launchGradient(const Geom& g, float gx, float gy, float gz, const uint8_t* markers, const float* p,
-                           FaceField v, ConstFaceField svArr, const SolidVelTable& svTab, cudaStream_t s);
+// p pitched, FP32 or (pDouble) FP64; the differences are rounded to FP32
+cudaError_t launchGradient(const Geom& g, float gx, float gy, float gz, const uint8_t* markers, const void* p,
+                           bool pDouble, FaceField v, ConstFaceField svArr, const SolidVelTable& svTab,
+                           cudaStream_t s);
 // Resolves the launch shapes of every CG kernel variant (occupancy queries) so
 // that no query runs while a stream is being captured.
 void cgWarmLaunchCache();
@@ -161,6 +164,12 @@ cudaError_t launchExtrapLayer(const Dim3i rc[3], float* const vals[3], const lon
 // hostCount pinned.  Blocks (one host read per layer).
 cudaError_t launchFluidSdf(const Dim3i& r, const float* dom, float* sdf, int layers, unsigned int* frontA,
                            unsigned int* frontB, unsigned int* counts, unsigned int* hostCount, cudaStream_t s);
+// mixFieldWithDensity of a cell grid (face = 0, a[0], b[0]) or of the three
+// face grids of r (face = 1); b is updated in place
+cudaError_t launchMixFieldWithDensity(const Dim3i& r, int face, const float* const a[3], float* const b[3],
+                                      const float* wa, const float* wb, cudaStream_t s);
+cudaError_t launchMixParticleVel(const float* pic, const float* flip, const float* dist, long long n, float cell,
+                                 float g, float gf, float f, float p, float* predict, cudaStream_t s);
 // fluid density of buildFluidDensity; the solid is solidSdf < 0 when given,
 // else solidIdx != 0
 cudaError_t launchFluidDensity(const Dim3i& r, const float* dom, const float* solidSdf, const uint8_t* solidIdx,

@@ -489,8 +489,8 @@ void mgSetup(Multigrid* m, const Dim3i& r, const uint8_t* mk0, const Code* code,
 // Preconditioned CG with the V-cycle: the RHS kernel already set r = b,
 // x = 0 and ||b||^2.  Iterations are launched in chunks; every kernel returns
 // immediately once the state says done.
-void mgRunCg(Multigrid* m, const Dim3i& cg, float sx, float sy, float sz, const CgMaps& maps, const Code* code, float* x,
-             float* rvec, CgState* st, CgState* stHost, cudaStream_t s, long long& launches,
+void mgRunCg(Multigrid* m, const Dim3i& cg, float sx, float sy, float sz, const CgMaps& maps, const Code* code, void* x,
+             bool xDouble, float* rvec, CgState* st, CgState* stHost, cudaStream_t s, long long& launches,
              const std::function<cudaGraphExec_t(const std::function<void()>&)>& capture, cudaGraphExec_t* chunk) {
   check(cudaMemsetAsync(m->p[0].p, 0, m->p[0].bytes(), s), "memset");
   const float* z0 = mgVcycle(m, rvec, st, s, launches);  // z0 = V(b), rz = b.z0
@@ -504,7 +504,7 @@ void mgRunCg(Multigrid* m, const Dim3i& cg, float sx, float sy, float sz, const 
       check(launchCgDirection(cg, sx, sy, sz, m->zH[zi], m->pH[po], maps.codeH, code, z, m->p[po].p, m->p[pn].p,
                               m->partials.p, st, 2, s),
             "cg direction");
-      check(launchCgUpdate(cg, sx, sy, sz, m->pH[pn], maps.rI, maps.xI, maps.codeI, m->p[pn].p, x, rvec,
+      check(launchCgUpdate(cg, sx, sy, sz, m->pH[pn], maps.rI, maps.xI, maps.codeI, m->p[pn].p, x, xDouble, rvec,
                            m->partials.p, st, 2, s),
             "cg update");
       launches += 2;

@@ -234,8 +234,8 @@ template <int PC>
 __global__ void __launch_bounds__(TX* TY) kRhsInit(Geom g, ConstFaceField v, ConstFaceField svArr, SolidVelTable svTab,
                                                    const uint8_t* __restrict__ mk, const Code* __restrict__ code,
                                                    float sAx, float sAy, float sAz, float* __restrict__ bOut,
-                                                   float* __restrict__ r, float* __restrict__ xv, float* __restrict__ p,
-                                                   double* partials, CgState* st, int zPer) {
+                                                   float* __restrict__ r, void* __restrict__ xv, int xDouble,
+                                                   float* __restrict__ p, double* partials, CgState* st, int zPer) {
   const Dim3i R = g.r;
   const int px = cgPitch(R.x);
   int x = blockIdx.x * TX + threadIdx.x, y = blockIdx.y * TY + threadIdx.y;
@@ -245,7 +245,8 @@ __global__ void __launch_bounds__(TX* TY) kRhsInit(Geom g, ConstFaceField v, Con
     for (int z = z0; z < z1; ++z) {
       long long o = ((long long)z * R.y + y) * px + x;
       r[o] = 0.f;
-      xv[o] = 0.f;
+      if (xDouble) ((double*)xv)[o] = 0.0;
+      else ((float*)xv)[o] = 0.f;
       p[o] = 0.f;
     }
   }
@@ -258,7 +259,8 @@ __global__ void __launch_bounds__(TX* TY) kRhsInit(Geom g, ConstFaceField v, Con
       if (bOut) bOut[c] = b;
       long long o = ((long long)z * R.y + y) * px + x;
       r[o] = b;
-      xv[o] = 0.f;
+      if (xDouble) ((double*)xv)[o] = 0.0;
+      else ((float*)xv)[o] = 0.f;
       p[o] = 0.f;
       float zz = precondZ<PC>(code[o], b, sAx, sAy, sAz);
       bb += (double)b * (double)b;
@@ -278,14 +280,16 @@ __global__ void __launch_bounds__(TX* TY) kRhsInit(Geom g, ConstFaceField v, Con
 }
 cudaError_t launchRhsInit(const Geom& gm, ConstFaceField v, ConstFaceField svArr, const SolidVelTable& svTab,
                           const uint8_t* markers, const Code* code, float ax, float ay, float az, float* b, float* r,
-                          float* x, float* p, double* partials, CgState* st, int precond, cudaStream_t s) {
+                          void* x, bool xDouble, float* p, double* partials, CgState* st, int precond,
+                          cudaStream_t s) {
   CgGrid g = cgGrid(cgDims(gm.r));
+  const int xd = xDouble ? 1 : 0;
   if (precond == 1)
-    kRhsInit<1><<<g.grid, g.block, 0, s>>>(gm, v, svArr, svTab, markers, code, ax, ay, az, b, r, x, p, partials, st,
-                                           g.zPer);
+    kRhsInit<1><<<g.grid, g.block, 0, s>>>(gm, v, svArr, svTab, markers, code, ax, ay, az, b, r, x, xd, p, partials,
+                                           st, g.zPer);
   else
-    kRhsInit<0><<<g.grid, g.block, 0, s>>>(gm, v, svArr, svTab, markers, code, ax, ay, az, b, r, x, p, partials, st,
-                                           g.zPer);
+    kRhsInit<0><<<g.grid, g.block, 0, s>>>(gm, v, svArr, svTab, markers, code, ax, ay, az, b, r, x, xd, p, partials,
+                                           st, g.zPer);
   return cudaGetLastError();
 }
 
@@ -417,13 +421,16 @@ struct __align__(128) DirStage {
 };
 constexpr unsigned kDirStageBytes = sizeof(float) * FH * FW * 2 + sizeof(Code) * FH * CW;
 
-struct __align__(128) UpdStage {
+// TX: the pressure iterate x in FP32 (the reference's Real) or FP64.
+template <class TX> struct __align__(128) UpdStage {
   alignas(128) float p[FH][FW];
   alignas(128) float r[CTR][CTX];
-  alignas(128) float x[CTR][CTX];
+  alignas(128) TX x[CTR][CTX];
   alignas(128) Code code[CTR][CTX];
 };
-constexpr unsigned kUpdStageBytes = sizeof(float) * (FH * FW + 2 * CTR * CTX) + sizeof(Code) * CTR * CTX;
+template <class TX>
+constexpr unsigned kUpdStageBytes = sizeof(float) * (FH * FW + CTR * CTX) + sizeof(TX) * CTR * CTX + sizeof(Code) * CTR * CTX;
+template <class TX> constexpr int kUpdStagesT = sizeof(TX) == 8 ? 4 : kUpdStages;  // keeps static shared memory < 48 KB
 
 struct CgLaunch {
   dim3 grid, block;
@@ -597,14 +604,16 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
 // |alpha| < FLT_EPSILON skip of CCuDenseVector::plusAlphaX
 // (CuDenseVector.cpp:178) is kept.  Per-thread partial sums run over one
 // z-column segment in FP32 and are combined in FP64.
-template <int PC>
+template <int PC, class TX>
 __global__ void __launch_bounds__(CTX* CTY, 4)
     kCgUpdate(const __grid_constant__ CUtensorMap mP, const __grid_constant__ CUtensorMap mR,
               const __grid_constant__ CUtensorMap mX, const __grid_constant__ CUtensorMap mCode, Dim3i P, float sx,
-              float sy, float sz, const float* __restrict__ p, float* __restrict__ xv, float* __restrict__ r,
+              float sy, float sz, const float* __restrict__ p, TX* __restrict__ xv, float* __restrict__ r,
               double* partials, CgState* st, int zPer) {
   if (st->done) return;
-  __shared__ UpdStage stg[kUpdStages];
+  constexpr int kUpdStages = kUpdStagesT<TX>;
+  using Stage = UpdStage<TX>;
+  __shared__ Stage stg[kUpdStages];
   __shared__ DiagTab tab;
   __shared__ __align__(8) uint64_t bar[kUpdStages];
   __shared__ int issued;
@@ -613,9 +622,9 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
   const int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, P.z);
   const int nPlanes = z1 - z0, nLoad = nPlanes + 1;
   auto issue = [&](int i) {
-    UpdStage& S = stg[i % kUpdStages];
+    Stage& S = stg[i % kUpdStages];
     uint64_t* b = &bar[i % kUpdStages];
-    mbarExpectTx(b, kUpdStageBytes);
+    mbarExpectTx(b, kUpdStageBytes<TX>);
     tmaLoad3(&S.p[0][0], &mP, x0 - HXF, y0 - 1, z0 + i, b);
     tmaLoad3(&S.r[0][0], &mR, x0, y0, z0 + i, b);
     tmaLoad3(&S.x[0][0], &mX, x0, y0, z0 + i, b);
@@ -656,8 +665,8 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
   for (int i = 0; i < nPlanes && !fail; ++i) {
     ok = mbarWait(&bar[(i + 1) % kUpdStages], (unsigned)(((i + 1) / kUpdStages) & 1), deadline);
     waited = i + 2;
-    const UpdStage& A = stg[(i + 1) % kUpdStages];
-    const UpdStage& S = stg[i % kUpdStages];
+    const Stage& A = stg[(i + 1) % kUpdStages];
+    const Stage& S = stg[i % kUpdStages];
 #pragma unroll
     for (int j = 0; j < RY; ++j) {
       const int row = ty + 1 + j * CTY, ir = ty + j * CTY;
@@ -668,7 +677,10 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
         if (!skip) {
           float q = fastRow(tab, k, sx, sy, sz, cur[j], S.p[row][tx + HXF - 1], S.p[row][tx + HXF + 1],
                             S.p[row - 1][tx + HXF], S.p[row + 1][tx + HXF], below[j], above);
-          xv[c[j]] = fmaf(alpha, cur[j], S.x[ir][tx]);
+          if (sizeof(TX) == 8)  // FP64 accumulation: x + alpha p, each operation rounded once
+            xv[c[j]] = (TX)__dadd_rn((double)S.x[ir][tx], __dmul_rn((double)alpha, (double)cur[j]));
+          else
+            xv[c[j]] = (TX)fmaf(alpha, cur[j], (float)S.x[ir][tx]);
           rv = fmaf(-alpha, q, rv);
           r[c[j]] = rv;
         }
@@ -734,15 +746,17 @@ cudaError_t makeHaloMap(const Dim3i& cg, const float* v, CUtensorMap* m) {
   return encodeMap(m, v, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cg, FW, FH);
 }
 
-cudaError_t makeCgMaps(const Dim3i& cg, const Code* code, const float* r, const float* x, const float* p0,
-                       const float* p1, CgMaps* m) {
+cudaError_t makeCgMaps(const Dim3i& cg, const Code* code, const float* r, const void* x, bool xDouble,
+                       const float* p0, const float* p1, CgMaps* m) {
   if (cg.x % 8 != 0) return cudaErrorInvalidValue;  // rows must start on 16-byte boundaries
   cudaError_t e;
   if ((e = encodeMap(&m->codeH, code, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, cg, CW, FH)) != cudaSuccess) return e;
   if ((e = encodeMap(&m->codeI, code, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, cg, CTX, CTR)) != cudaSuccess) return e;
   if ((e = encodeMap(&m->rH, r, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cg, FW, FH)) != cudaSuccess) return e;
   if ((e = encodeMap(&m->rI, r, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cg, CTX, CTR)) != cudaSuccess) return e;
-  if ((e = encodeMap(&m->xI, x, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cg, CTX, CTR)) != cudaSuccess) return e;
+  if ((e = encodeMap(&m->xI, x, xDouble ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                     xDouble ? 8 : 4, cg, CTX, CTR)) != cudaSuccess)
+    return e;
   if ((e = encodeMap(&m->pH[0], p0, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cg, FW, FH)) != cudaSuccess) return e;
   return encodeMap(&m->pH[1], p1, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cg, FW, FH);
 }
@@ -751,18 +765,23 @@ void cgWarmLaunchCache() {
   residentBlocks((const void*)kCgDirection<0>);
   residentBlocks((const void*)kCgDirection<1>);
   residentBlocks((const void*)kCgDirection<2>);
-  residentBlocks((const void*)kCgUpdate<0>);
-  residentBlocks((const void*)kCgUpdate<1>);
-  residentBlocks((const void*)kCgUpdate<2>);
+  residentBlocks((const void*)kCgUpdate<0, float>);
+  residentBlocks((const void*)kCgUpdate<1, float>);
+  residentBlocks((const void*)kCgUpdate<2, float>);
+  residentBlocks((const void*)kCgUpdate<0, double>);
+  residentBlocks((const void*)kCgUpdate<1, double>);
+  residentBlocks((const void*)kCgUpdate<2, double>);
 }
 
 int cgPartialsNeeded(const Dim3i& r) {
   const Dim3i cg = cgDims(r);
   CgGrid g = cgGrid(cg);
   long long n = (long long)g.grid.x * g.grid.y * g.grid.z;
-  CgLaunch a = cgLaunch(cg, kCgDirection<1>), b = cgLaunch(cg, kCgUpdate<1>);
+  CgLaunch a = cgLaunch(cg, kCgDirection<1>), b = cgLaunch(cg, kCgUpdate<1, float>),
+           d = cgLaunch(cg, kCgUpdate<1, double>);
   n = std::max(n, (long long)a.grid.x * a.grid.y * a.grid.z);
   n = std::max(n, (long long)b.grid.x * b.grid.y * b.grid.z);
+  n = std::max(n, (long long)d.grid.x * d.grid.y * d.grid.z);
   return 2 * (int)n;
 }
 
@@ -793,24 +812,24 @@ cudaError_t launchCgDirection(const Dim3i& cg, float sx, float sy, float sz, con
 }
 
 cudaError_t launchCgUpdate(const Dim3i& cg, float sx, float sy, float sz, const CUtensorMap& mP, const CUtensorMap& mR,
-                           const CUtensorMap& mX, const CUtensorMap& mCode, const float* p, float* x, float* r,
-                           double* partials, CgState* st, int precond, cudaStream_t s) {
-  switch (precond) {
-    case 1: {
-      CgLaunch L = cgLaunch(cg, kCgUpdate<1>);
-      kCgUpdate<1><<<L.grid, L.block, 0, s>>>(mP, mR, mX, mCode, cg, sx, sy, sz, p, x, r, partials, st, L.zPer);
-      break;
-    }
-    case 2: {
-      CgLaunch L = cgLaunch(cg, kCgUpdate<2>);
-      kCgUpdate<2><<<L.grid, L.block, 0, s>>>(mP, mR, mX, mCode, cg, sx, sy, sz, p, x, r, partials, st, L.zPer);
-      break;
-    }
-    default: {
-      CgLaunch L = cgLaunch(cg, kCgUpdate<0>);
-      kCgUpdate<0><<<L.grid, L.block, 0, s>>>(mP, mR, mX, mCode, cg, sx, sy, sz, p, x, r, partials, st, L.zPer);
-    }
+                           const CUtensorMap& mX, const CUtensorMap& mCode, const float* p, void* x, bool xDouble,
+                           float* r, double* partials, CgState* st, int precond, cudaStream_t s) {
+#define HFG_CG_UPDATE(PCV, TXV)                                                                                   \
+  {                                                                                                               \
+    CgLaunch L = cgLaunch(cg, kCgUpdate<PCV, TXV>);                                                             \
+    kCgUpdate<PCV, TXV><<<L.grid, L.block, 0, s>>>(mP, mR, mX, mCode, cg, sx, sy, sz, p, (TXV*)x, r, partials, st, \
+                                                   L.zPer);                                                     \
   }
+  if (xDouble) {
+    if (precond == 1) HFG_CG_UPDATE(1, double)
+    else if (precond == 2) HFG_CG_UPDATE(2, double)
+    else HFG_CG_UPDATE(0, double)
+  } else {
+    if (precond == 1) HFG_CG_UPDATE(1, float)
+    else if (precond == 2) HFG_CG_UPDATE(2, float)
+    else HFG_CG_UPDATE(0, float)
+  }
+#undef HFG_CG_UPDATE
   return cudaGetLastError();
 }
 

@@ -54,8 +54,8 @@ Multigrid* mgCreate(const Dim3i& cg, int levels, int smooth, bool half, cudaStre
 void mgDestroy(Multigrid* m);
 void mgSetup(Multigrid* m, const Dim3i& r, const uint8_t* mk0, const Code* code, float sx, float sy, float sz,
              cudaStream_t s, long long& launches);
-void mgRunCg(Multigrid* m, const Dim3i& cg, float sx, float sy, float sz, const CgMaps& maps, const Code* code, float* x,
-             float* rvec, CgState* st, CgState* stHost, cudaStream_t s, long long& launches,
+void mgRunCg(Multigrid* m, const Dim3i& cg, float sx, float sy, float sz, const CgMaps& maps, const Code* code, void* x,
+             bool xDouble, float* rvec, CgState* st, CgState* stHost, cudaStream_t s, long long& launches,
              const std::function<cudaGraphExec_t(const std::function<void()>&)>& capture, cudaGraphExec_t* chunk);
 
 GridSolver::GridSolver(float dt, Dim3i res, const float origin[3], const float spacing[3]) {
@@ -89,7 +89,7 @@ GridSolver::GridSolver(float dt, Dim3i res, const float origin[3], const float s
   cgp_[0].alloc(NC_, stream_);
   cgp_[1].alloc(NC_, stream_);
   partials_.alloc(cgPartialsNeeded(res), stream_);
-  check(makeCgMaps(cg_, code_.p, cgr_.p, cgx_.p, cgp_[0].p, cgp_[1].p, &maps_), "CG tensor maps");
+  check(makeCgMaps(cg_, code_.p, cgr_.p, cgx_.p, false, cgp_[0].p, cgp_[1].p, &maps_), "CG tensor maps");
   cgState_.alloc(1, stream_);
   subState_.alloc(subSlots_ + 1, stream_);
   dist_.alloc(Ftot_, stream_); list_.alloc(Ftot_, stream_);
@@ -284,7 +284,17 @@ void GridSolver::setOptions(const hfg_options_t& o) {
     throw CudaError("extrapolation layers must be in [0, 1000]", HFG_ERR_INVALID);
   bool mgChanged = o.precond == HFG_PRECOND_MG &&
                    (!mg_ || o.mg_levels != opt_.mg_levels || o.mg_smooth != opt_.mg_smooth || o.mg_half != opt_.mg_half);
+  const bool fp64Changed = (o.pressure_fp64 != 0) != (opt_.pressure_fp64 != 0);
   opt_ = o;
+  if (fp64Changed) {
+    // the pressure iterate changes type: new tensor map, recaptured graphs
+    dropGraphs();
+    if (o.pressure_fp64) {
+      cgx64_.alloc(NC_, stream_);
+      check(cudaMemsetAsync(cgx64_.p, 0, cgx64_.bytes(), stream_), "memset");
+    }
+    check(makeCgMaps(cg_, code_.p, cgr_.p, xPtr(), xDouble(), cgp_[0].p, cgp_[1].p, &maps_), "CG tensor maps");
+  }
   if (mgChanged) {
     dropGraphs();
     if (mg_) mgDestroy(mg_);
@@ -429,7 +439,8 @@ void GridSolver::cgIteration(int it, float sx, float sy, float sz, int pc) {
   launched(launchCgDirection(cg_, sx, sy, sz, maps_.rH, maps_.pH[po], maps_.codeH, code_.p, cgr_.p, cgp_[po].p,
                              cgp_[pn].p, partials_.p, cgState_.p, pc, stream_),
            "cg direction");
-  launched(launchCgUpdate(cg_, sx, sy, sz, maps_.pH[pn], maps_.rI, maps_.xI, maps_.codeI, cgp_[pn].p, cgx_.p, cgr_.p,
+  launched(launchCgUpdate(cg_, sx, sy, sz, maps_.pH[pn], maps_.rI, maps_.xI, maps_.codeI, cgp_[pn].p, xPtr(), xDouble(),
+                          cgr_.p,
                           partials_.p, cgState_.p, pc, stream_),
            "cg update");
 }
@@ -468,7 +479,7 @@ void GridSolver::runCg() {
   const float sx = dt_ / (1.0f * g_.hx * g_.hx), sy = dt_ / (1.0f * g_.hy * g_.hy), sz = dt_ / (1.0f * g_.hz * g_.hz);
   if (opt_.precond == HFG_PRECOND_MG) {
     auto cap = [this](const std::function<void()>& f) { return capture(f); };
-    mgRunCg(mg_, cg_, sx, sy, sz, maps_, code_.p, cgx_.p, cgr_.p, cgState_.p, cgHost_, stream_, launches_, cap,
+    mgRunCg(mg_, cg_, sx, sy, sz, maps_, code_.p, xPtr(), xDouble(), cgr_.p, cgState_.p, cgHost_, stream_, launches_, cap,
             &cgGraph_[2]);
   } else {
     const int pc = opt_.precond == HFG_PRECOND_JACOBI ? 1 : 0;
@@ -510,7 +521,8 @@ void GridSolver::computePressure() {
   check(cudaMemcpyAsync(cgState_.p, cgHost_, sizeof(CgState), cudaMemcpyHostToDevice, stream_), "cg state");
   const float sx = dt_ / (1.0f * g_.hx * g_.hx), sy = dt_ / (1.0f * g_.hy * g_.hy), sz = dt_ / (1.0f * g_.hz * g_.hz);
   ConstFaceField none{{nullptr, nullptr, nullptr}};
-  launched(launchRhsInit(g_, cvel(ni), none, solidTable(), markers_.p, code_.p, sx, sy, sz, nullptr, cgr_.p, cgx_.p,
+  launched(launchRhsInit(g_, cvel(ni), none, solidTable(), markers_.p, code_.p, sx, sy, sz, nullptr, cgr_.p, xPtr(),
+                         xDouble(),
                          cgp_[0].p, partials_.p, cgState_.p, init.precond, stream_),
            "rhs");
   if (opt_.precond == HFG_PRECOND_MG) mgSetup(mg_, g_.r, markers_.p, code_.p, sx, sy, sz, stream_, launches_);
@@ -524,7 +536,8 @@ void GridSolver::computePressure() {
   stageEnd(5);
   stageBegin(6);
   ConstFaceField noneSv{{nullptr, nullptr, nullptr}};
-  launched(launchGradient(g_, dt_ / (1.0f * g_.hx), dt_ / (1.0f * g_.hy), dt_ / (1.0f * g_.hz), markers_.p, cgx_.p,
+  launched(launchGradient(g_, dt_ / (1.0f * g_.hx), dt_ / (1.0f * g_.hy), dt_ / (1.0f * g_.hz), markers_.p, xPtr(),
+                          xDouble(),
                           mvel(ni), noneSv, solidTable(), stream_),
            "gradient");
   if (opt_.report_divergence) {
@@ -651,6 +664,15 @@ void GridSolver::getMarkers(uint8_t* m) {
 }
 
 void GridSolver::getPressure(float* p) {
+  if (xDouble()) {
+    std::vector<double> tmp((size_t)N_);
+    check(cudaMemcpy2DAsync(tmp.data(), (size_t)g_.r.x * 8, cgx64_.p, (size_t)cg_.x * 8, (size_t)g_.r.x * 8,
+                            (size_t)g_.r.y * g_.r.z, cudaMemcpyDeviceToHost, stream_),
+          "download");
+    synchronize();
+    for (long long i = 0; i < N_; ++i) p[i] = (float)tmp[i];
+    return;
+  }
   check(cudaMemcpy2DAsync(p, (size_t)g_.r.x * 4, cgx_.p, (size_t)cg_.x * 4, (size_t)g_.r.x * 4,
                           (size_t)g_.r.y * g_.r.z, cudaMemcpyDeviceToHost, stream_),
         "download");
@@ -698,6 +720,20 @@ void GridSolver::getFluidDensity(float* out) {
   d.alloc(N_, stream_);
   check(launchFluidDensity(g_.r, dom_[cur()].p, nullptr, solidIdx_.p, d.p, stream_), "fluid density");
   check(cudaMemcpyAsync(out, d.p, N_ * 4, cudaMemcpyDeviceToHost, stream_), "download");
+  synchronize();
+}
+
+// GridFluidSolver.cpp:615-642: into the velocity buffer the step in progress
+// writes (the reference's Field1 while its buffer flag is set, else Field2).
+void GridSolver::mixVelFieldWithOthers(const float* const other[3], const float* wOther, const float* wFluid) {
+  float* b[3] = {vel_[nxt()][0].p, vel_[nxt()][1].p, vel_[nxt()][2].p};
+  launched(launchMixFieldWithDensity(g_.r, 1, other, b, wOther, wFluid, stream_), "mix", 3);
+  synchronize();
+}
+
+// GridFluidSolver.cpp:644-670: G2P from the current velocity buffer.
+void GridSolver::transferVelToParticles(const float* pos, long long n, int alg, float* vel) {
+  if (n > 0) launched(launchG2PFace(g_, alg, cvel(cur()), pos, n, vel, stream_), "g2p");
   synchronize();
 }
 

@@ -120,6 +120,10 @@ class GridSolver {
   void getSolidVel(float* x, float* y, float* z);
   void getFluidSDF(float* out);
   void getFluidDensity(float* out);
+  // mixVelFieldWithOthers (device pointers)
+  void mixVelFieldWithOthers(const float* const other[3], const float* wOther, const float* wFluid);
+  // transferFluidVelField2Particles (device pointers)
+  void transferVelToParticles(const float* pos, long long n, int alg, float* vel);
   void getParticles(float* pos, float* vel);
   void getStats(hfg_stats_t* st);
   void synchronize();
@@ -174,6 +178,9 @@ class GridSolver {
   long long NC_ = 0;
   CgMaps maps_;
   DArray<float> cgx_, cgr_, cgp_[2];
+  DArray<double> cgx64_;  // the pressure iterate with pressure_fp64
+  bool xDouble() const { return opt_.pressure_fp64 != 0; }
+  void* xPtr() { return xDouble() ? (void*)cgx64_.p : (void*)cgx_.p; }
   DArray<double> partials_;
   DArray<CgState> cgState_;
   CgState* cgHost_ = nullptr;  // pinned

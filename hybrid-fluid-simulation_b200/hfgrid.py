@@ -42,7 +42,7 @@ class Options(C.Structure):
         ("precond", C.c_int), ("tol_mode", C.c_int), ("tol", C.c_double), ("max_iter", C.c_longlong),
         ("clamp_mode", C.c_int), ("advect_scalars", C.c_int), ("extrapolation_layers", C.c_int),
         ("mg_levels", C.c_int), ("mg_smooth", C.c_int), ("mg_half", C.c_int), ("report_divergence", C.c_int),
-        ("sampling", C.c_int),
+        ("sampling", C.c_int), ("pressure_fp64", C.c_int),
     ]
 
 
@@ -138,6 +138,8 @@ def _signatures(lib):
         "hfg_solver_get_solid_vel_field": (C.c_int, [S, PF, PF, PF]),
         "hfg_solver_get_fluid_sdf": (C.c_int, [S, PF]),
         "hfg_solver_get_fluid_density": (C.c_int, [S, PF]),
+        "hfg_solver_mix_vel_field_with_others": (C.c_int, [S, VP, VP, VP, VP, VP]),
+        "hfg_solver_transfer_vel_to_particles": (C.c_int, [S, VP, C.c_longlong, C.c_int, VP]),
         "hfg_solver_num_particles": (C.c_longlong, [S]),
         "hfg_solver_get_particles": (C.c_int, [S, PF, PF]),
         "hfg_solver_get_stats": (C.c_int, [S, C.POINTER(Stats)]),
@@ -175,6 +177,10 @@ def _signatures(lib):
         "hfg_op_fluid_domain_from_bbox": (C.c_int, [I3, F3, F3, F3, F3, VP, VP]),
         "hfg_op_build_fluid_sdf": (C.c_int, [I3, VP, VP, C.c_int, VP]),
         "hfg_op_build_fluid_density": (C.c_int, [I3, VP, VP, VP, VP]),
+        "hfg_op_mix_field_with_density_cc": (C.c_int, [C.c_longlong, VP, VP, VP, VP, VP]),
+        "hfg_op_mix_field_with_density_fc": (C.c_int, [I3, VP, VP, VP, VP, VP, VP, VP, VP, VP]),
+        "hfg_op_mix_particle_vel_pic_flip": (C.c_int, [VP, VP, VP, C.c_longlong, C.c_float, C.c_float, C.c_float,
+                                                       C.c_float, C.c_float, VP, VP]),
         "hfg_solver_add_analytic_solid": (C.c_int, [S, C.c_int, C.POINTER(C.c_double), F3]),
         "hfg_scene_bytes": (C.c_int, [I3, C.c_longlong, C.c_int, C.c_int, C.POINTER(C.c_longlong)]),
         "hfg_scene_particles_bound": (C.c_int, [C.POINTER(SceneDesc), C.POINTER(C.c_longlong)]),
@@ -398,6 +404,14 @@ class Solver:
         _check(lib().hfg_solver_get_fluid_sdf(self._h, _fptr(out)))
         return out
 
+    def mix_vel_field_with_others(self, other, w_other, w_fluid):
+        """torch CUDA tensors: the other face field (3), both cell densities."""
+        _check(lib().hfg_solver_mix_vel_field_with_others(self._h, *[_ptr(v) for v in other], _ptr(w_other),
+                                                          _ptr(w_fluid)))
+
+    def transfer_vel_to_particles(self, pos, alg, out):
+        _check(lib().hfg_solver_transfer_vel_to_particles(self._h, _ptr(pos), pos.numel() // 3, alg, _ptr(out)))
+
     def fluid_density(self):
         out = np.empty(self.res[::-1], np.float32)
         _check(lib().hfg_solver_get_fluid_density(self._h, _fptr(out)))
@@ -576,6 +590,21 @@ def op_sl_advect_cc(res, origin, spacing, field, vel, dt, accuracy, out, stream=
 def op_fluid_domain_from_bbox(res, origin, spacing, mn, mx, out, stream=None):
     _check(lib().hfg_op_fluid_domain_from_bbox(_i3(res), _f3(origin), _f3(spacing), _f3(mn), _f3(mx), _ptr(out),
                                                _stream(stream)))
+
+
+def op_mix_field_with_density_cc(a, b, wa, wb, stream=None):
+    _check(lib().hfg_op_mix_field_with_density_cc(b.numel(), _ptr(a), _ptr(b), _ptr(wa), _ptr(wb), _stream(stream)))
+
+
+def op_mix_field_with_density_fc(res, a, b, wa, wb, stream=None):
+    _check(lib().hfg_op_mix_field_with_density_fc(_i3(res), *[_ptr(v) for v in a], *[_ptr(v) for v in b], _ptr(wa),
+                                                  _ptr(wb), _stream(stream)))
+
+
+def op_mix_particle_vel_pic_flip(pic, flip, dist, cell, g_rate, gf_rate, f_rate, p_rate, predict, stream=None):
+    _check(lib().hfg_op_mix_particle_vel_pic_flip(_ptr(pic), _ptr(flip), _ptr(dist), dist.numel(), C.c_float(cell),
+                                                  C.c_float(g_rate), C.c_float(gf_rate), C.c_float(f_rate),
+                                                  C.c_float(p_rate), _ptr(predict), _stream(stream)))
 
 
 def op_build_fluid_density(res, domain, solid_sdf, out, stream=None):

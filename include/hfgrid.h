@@ -80,6 +80,10 @@ typedef struct {
   int report_divergence;  /* 1: measure the divergence residual of every projection */
   int sampling;           /* HFG_SAMPLE_* of the semi-Lagrangian advection (setSamplingAlg,
                              AdvectionSolver.cpp:21-24; default trilinear) */
+  int pressure_fp64;      /* 1: accumulate the pressure iterate in FP64 and take the
+                             gradient's differences in FP64 (the reference keeps
+                             it in FP32, which bounds the divergence of the
+                             projected field near 1e-4 of ||b|| on large grids) */
 } hfg_options_t;
 
 typedef struct {
@@ -156,6 +160,15 @@ HFG_API int hfg_solver_get_fluid_sdf(hfg_solver_t s, float* sdf);
 /* generateCurFluidDensity + getFluidDensityField (N floats: 1 fluid, 0.2 at the
  * surface, 0 elsewhere)  GridFluidSolver.cpp:297-300,593-613 */
 HFG_API int hfg_solver_get_fluid_density(hfg_solver_t s, float* density);
+/* mixVelFieldWithOthers  GridFluidSolver.cpp:615-642: blends another face
+ * velocity field into the buffer the step in progress writes (call it between
+ * hfg_solver_update_without_pressure and hfg_solver_solve_pressure), weighted by
+ * the two cell densities.  DEVICE pointers, like the reference's fields. */
+HFG_API int hfg_solver_mix_vel_field_with_others(hfg_solver_t s, const float* vx, const float* vy, const float* vz,
+                                                 const float* others_density, const float* fluid_density);
+/* transferFluidVelField2Particles  GridFluidSolver.cpp:644-670: G2P from the
+ * current velocity field; DEVICE pointers (pos, vel: 3n floats). */
+HFG_API int hfg_solver_transfer_vel_to_particles(hfg_solver_t s, const float* pos, long long n, int alg, float* vel);
 HFG_API long long hfg_solver_num_particles(hfg_solver_t s);
 HFG_API int hfg_solver_get_particles(hfg_solver_t s, float* pos, float* vel);
 HFG_API int hfg_solver_get_stats(hfg_solver_t s, hfg_stats_t* st);
@@ -256,6 +269,18 @@ HFG_API int hfg_op_sl_advect_cc_ex(const int res[3], const float origin[3], cons
 /* buildFluidSDFInvoker  EulerSolverTool.cu:760-785 (layers = the reference's
  * vExtrapolationDistance; blocks) */
 HFG_API int hfg_op_build_fluid_sdf(const int res[3], const float* domain, float* sdf, int layers, void* stream);
+/* mixFieldWithDensityInvoker (cell grid of n entries / face grids of res):
+ * b := (wa a + wb b) / (wa + wb) where wa + wb > FLT_EPSILON, in place
+ * HybridSimulatorMixFieldWithDensity.cu:6-265 */
+HFG_API int hfg_op_mix_field_with_density_cc(long long n, const float* a, float* b, const float* wa, const float* wb,
+                                             void* stream);
+HFG_API int hfg_op_mix_field_with_density_fc(const int res[3], const float* ax, const float* ay, const float* az,
+                                             float* bx, float* by, float* bz, const float* wa, const float* wb,
+                                             void* stream);
+/* mixParitcleVelWithPICAndFLIPInvoker  HybridSimulatorMixParitcleVelWithPICAndFLIP.cu:5-88 */
+HFG_API int hfg_op_mix_particle_vel_pic_flip(const float* pic, const float* flip, const float* dist, long long n,
+                                             float cell, float g_rate, float gf_rate, float f_rate, float p_rate,
+                                             float* predict, void* stream);
 /* buildFluidDensityInvoker  EulerSolverTool.cu:408-448,787-810; solid_sdf < 0 inside solids */
 HFG_API int hfg_op_build_fluid_density(const int res[3], const float* domain, const float* solid_sdf, float* out,
                                        void* stream);

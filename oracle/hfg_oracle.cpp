@@ -1112,6 +1112,55 @@ void orc_build_fluid_density(const int* res, const float* dom, const float* soli
       }
 }
 
+// HybridSimulatorMixFieldWithDensity.cu:6-265 mixFieldWithDensity: B := (wA A +
+// wB B) / (wA + wB) where wA + wB > FLT_EPSILON (B kept elsewhere).  On a
+// face grid the weights are the means of the two adjacent cells (clamp to
+// edge); the reference scales that sum by the double literal 0.5.
+static inline void mixOne(float a, float& b, float wa, float wb) {
+  if (wa + wb > std::numeric_limits<float>::epsilon()) b = (wa * a + wb * b) / (wa + wb);
+}
+void orc_mix_field_with_density_cc(long long n, const float* a, float* b, const float* wa, const float* wb) {
+  for (i64 i = 0; i < n; ++i) mixOne(a[i], b[i], wa[i], wb[i]);
+}
+void orc_mix_field_with_density_fc(const int* res, const float* ax, const float* ay, const float* az, float* bx,
+                                   float* by, float* bz, const float* wa, const float* wb) {
+  Res r{res[0], res[1], res[2]};
+  const float* A[3] = {ax, ay, az};
+  float* B[3] = {bx, by, bz};
+  for (int axis = 0; axis < 3; ++axis) {
+    Res f = r;
+    if (axis == 0) f.x += 1;
+    if (axis == 1) f.y += 1;
+    if (axis == 2) f.z += 1;
+    for (int z = 0; z < f.z; ++z)
+      for (int y = 0; y < f.y; ++y)
+        for (int x = 0; x < f.x; ++x) {
+          i64 lo = lin(x - (axis == 0), y - (axis == 1), z - (axis == 2), r), hi = lin(x, y, z, r);
+          float wA = (float)((double)(wa[lo] + wa[hi]) * 0.5), wB = (float)((double)(wb[lo] + wb[hi]) * 0.5);
+          i64 c = lin(x, y, z, f);
+          mixOne(A[axis][c], B[axis][c], wA, wB);
+        }
+  }
+}
+// HybridSimulatorMixParitcleVelWithPICAndFLIP.cu:5-57: blend by the particle's
+// distance (in cells) into PIC, then FLIP, then the predicted velocity.
+void orc_mix_particle_vel(const float* pic, const float* flip, const float* dist, long long n, float cell, float g,
+                          float gf, float f, float pr, float* predict) {
+  const float dg = g * cell, dgf = gf * cell, df = f * cell, dp = pr * cell;
+  for (i64 i = 0; i < n; ++i) {
+    float d = dist[i];
+    for (int a = 0; a < 3; ++a) {
+      float P = pic[3 * i + a], F = flip[3 * i + a], Q = predict[3 * i + a], m;
+      if (d <= dg) m = P;
+      else if (d <= dgf) m = P + ((d - dg) / (dgf - dg)) * (Q - P);
+      else if (d <= df) m = F;
+      else if (d <= dp) m = F + ((d - df) / (dp - df)) * (Q - F);
+      else m = Q;
+      predict[3 * i + a] = m;
+    }
+  }
+}
+
 // EulerSolverTool.cu:581-608 generateFluidDomainFromBBox (strict inequalities)
 void orc_fluid_domain_from_bbox(const int* res, const float* o, const float* h, const float* mn, const float* mx,
                                 float* out) {
@@ -1451,6 +1500,30 @@ static void sSetAdvection(OrcSolver* S, int kind, int acc, int alg, float cfl, f
   s.sFlag = s.vFlag = s.velFlag = false;
 }
 template <class T> static void sSetSampling(OrcSolver* S, int samp) { pick<T>(S).sampling = samp; }
+// GridFluidSolver.cpp:615-642 mixVelFieldWithOthers: into the buffer the step
+// in progress writes (Field1 while the flag is set, else Field2).
+template <class T>
+static void sMixVel(OrcSolver* S, const float* ox, const float* oy, const float* oz, const float* wo, const float* wf) {
+  Solver<T>& s = pick<T>(S);
+  FC<T>& b = s.velOut();
+  const float* O[3] = {ox, oy, oz};
+  const Res r = s.g.r;
+  for (int axis = 0; axis < 3; ++axis) {
+    Res f = r;
+    if (axis == 0) f.x += 1;
+    if (axis == 1) f.y += 1;
+    if (axis == 2) f.z += 1;
+    for (int z = 0; z < f.z; ++z)
+      for (int y = 0; y < f.y; ++y)
+        for (int x = 0; x < f.x; ++x) {
+          i64 lo = lin(x - (axis == 0), y - (axis == 1), z - (axis == 2), r), hi = lin(x, y, z, r);
+          T wA = (T)((double)((T)wo[lo] + (T)wo[hi]) * 0.5), wB = (T)((double)((T)wf[lo] + (T)wf[hi]) * 0.5);
+          i64 c = lin(x, y, z, f);
+          T& v = b.c[axis][c];
+          if (wA + wB > (T)std::numeric_limits<float>::epsilon()) v = (wA * (T)O[axis][c] + wB * v) / (wA + wB);
+        }
+  }
+}
 template <class T> static void sSetParticles(OrcSolver* S, const float* pos, const float* vel, long long P) {
   Solver<T>& s = pick<T>(S);
   s.ppos = up<T>(pos, 3 * P);
@@ -1542,6 +1615,9 @@ void orc_solver_set_advection(void* p, int kind, int acc, int alg, float cfl, fl
   ORC_CALL((OrcSolver*)p, sSetAdvection, kind, acc, alg, cfl, mixing, clampMode, advectScalars);
 }
 void orc_solver_set_sampling(void* p, int samp) { ORC_CALL((OrcSolver*)p, sSetSampling, samp); }
+void orc_solver_mix_vel(void* p, const float* ox, const float* oy, const float* oz, const float* wo, const float* wf) {
+  ORC_CALL((OrcSolver*)p, sMixVel, ox, oy, oz, wo, wf);
+}
 void orc_solver_set_particles(void* p, const float* pos, const float* vel, long long P) {
   ORC_CALL((OrcSolver*)p, sSetParticles, pos, vel, P);
 }

@@ -45,6 +45,11 @@ def lib():
             "orc_fluid_domain_from_bbox": (None, [I3, F3, F3, F3, F3, PF]),
             "orc_build_fluid_sdf": (None, [I3, PF, C.c_int, PF]),
             "orc_build_fluid_density": (None, [I3, PF, PF, PF]),
+            "orc_mix_field_with_density_cc": (None, [C.c_longlong, PF, PF, PF, PF]),
+            "orc_mix_field_with_density_fc": (None, [I3, PF, PF, PF, PF, PF, PF, PF, PF]),
+            "orc_mix_particle_vel": (None, [PF, PF, PF, C.c_longlong, C.c_float, C.c_float, C.c_float, C.c_float,
+                                            C.c_float, PF]),
+            "orc_solver_mix_vel": (None, [vp, PF, PF, PF, PF, PF]),
             "orc_markers_from_particles": (None, [I3, F3, F3, PF, PF, C.c_longlong, PU8, PU32]),
             "orc_markers_from_sdf": (None, [I3, PF, PF, PU8]),
             "orc_build_matrix_a": (None, [C.c_int, I3, F3, C.c_float, PU8, PF]),
@@ -160,6 +165,25 @@ def build_fluid_sdf(res, domain, layers=1000):
 def build_fluid_density(res, domain, solid_sdf):
     out = np.empty(res[::-1], np.float32)
     lib().orc_build_fluid_density(i3(res), fp(f32(domain).reshape(-1)), fp(f32(solid_sdf).reshape(-1)), fp(out))
+    return out
+
+
+def mix_field_with_density_cc(a, b, wa, wb):
+    out = f32(b).copy()
+    lib().orc_mix_field_with_density_cc(out.size, fp(f32(a)), fp(out), fp(f32(wa)), fp(f32(wb)))
+    return out
+
+
+def mix_field_with_density_fc(res, a, b, wa, wb):
+    out = [f32(x).copy() for x in b]
+    lib().orc_mix_field_with_density_fc(i3(res), *[fp(f32(x)) for x in a], *[fp(x) for x in out],
+                                        fp(f32(wa).reshape(-1)), fp(f32(wb).reshape(-1)))
+    return out
+
+
+def mix_particle_vel(pic, flip, dist, cell, g, gf, f, pr, predict):
+    out = f32(predict).copy()
+    lib().orc_mix_particle_vel(fp(f32(pic)), fp(f32(flip)), fp(f32(dist)), f32(dist).size, cell, g, gf, f, pr, fp(out))
     return out
 
 
@@ -338,6 +362,10 @@ class Solver:
 
     def add_solid_boundary(self, sdf, vel=(0, 0, 0)):
         lib().orc_solver_add_boundary(self._h, fp(f32(sdf).reshape(-1)), *[float(v) for v in vel])
+
+    def mix_vel_field_with_others(self, other, w_other, w_fluid):
+        lib().orc_solver_mix_vel(self._h, *[fp(f32(a).reshape(-1)) for a in other], fp(f32(w_other).reshape(-1)),
+                                 fp(f32(w_fluid).reshape(-1)))
 
     def set_sampling(self, alg):
         lib().orc_solver_set_sampling(self._h, int(alg))

@@ -367,3 +367,42 @@ def test_fluid_density_bit_exact(cuda):
     ref = oracle.build_fluid_density(res, dom, solid)
     assert np.array_equal(host(out), ref)
     assert set(np.unique(ref)) <= {0.0, np.float32(0.2), 1.0}
+
+
+def test_mix_field_with_density(cuda):
+    """mixFieldWithDensity (HybridSimulatorMixFieldWithDensity.cu): cell and
+    face grids, zero total weight leaves B unchanged."""
+    rng = np.random.default_rng(62)
+    n = int(np.prod(RES))
+    wa = rng.random(RES[::-1]).astype(np.float32)
+    wb = rng.random(RES[::-1]).astype(np.float32)
+    wa[0, 0, :4] = 0.0
+    wb[0, 0, :4] = 0.0
+    a = rng.standard_normal(RES[::-1]).astype(np.float32)
+    b = rng.standard_normal(RES[::-1]).astype(np.float32)
+    bd = dev(b)
+    hfgrid.op_mix_field_with_density_cc(dev(a), bd, dev(wa), dev(wb))
+    np.testing.assert_allclose(host(bd), oracle.mix_field_with_density_cc(a, b, wa, wb).reshape(RES[::-1]),
+                               rtol=1e-6, atol=1e-7)
+    A = face_arrays(RES, rng)
+    B = face_arrays(RES, rng)
+    Bd = [dev(x) for x in B]
+    hfgrid.op_mix_field_with_density_fc(RES, [dev(x) for x in A], Bd, dev(wa), dev(wb))
+    ref = oracle.mix_field_with_density_fc(RES, A, B, wa, wb)
+    for k in range(3):
+        np.testing.assert_allclose(host(Bd[k]), ref[k], rtol=1e-6, atol=1e-7)
+    assert n > 0
+
+
+def test_mix_particle_vel_pic_flip(cuda):
+    """mixParitcleVelWithPICAndFLIP: every distance band (PIC, PIC->predicted,
+    FLIP, FLIP->predicted, predicted)."""
+    rng = np.random.default_rng(63)
+    n = 5000
+    pic, flip, pred = (rng.standard_normal((n, 3)).astype(np.float32) for _ in range(3))
+    dist = (rng.random(n) * 6.0 - 0.5).astype(np.float32)
+    args = (0.1, 1.0, 2.0, 3.5, 5.0)
+    pd = dev(pred)
+    hfgrid.op_mix_particle_vel_pic_flip(dev(pic), dev(flip), dev(dist), *args, pd)
+    ref = oracle.mix_particle_vel(pic, flip, dist, *args, pred)
+    np.testing.assert_allclose(host(pd), ref, rtol=1e-6, atol=1e-6)

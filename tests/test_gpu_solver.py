@@ -228,3 +228,62 @@ def test_semi_lagrangian_solver_catmull_rom(cuda):
         o.update()
     assert (g.markers() != o.markers()).mean() < 2e-3
     assert vel_rel_l2(g.velocity_field(), o.velocity_field()) < 1e-3
+
+
+def test_mix_vel_field_and_transfer_to_particles(cuda):
+    """mixVelFieldWithOthers between updateWithoutPressure and solvePressure
+    (GridFluidSolver.cpp:615-642) against the FP64 oracle, and
+    transferFluidVelField2Particles (:644-670) as G2P of the current field."""
+    import torch
+    sc = small_scene((20, 16, 14))
+    g = scenes.gpu_solver(sc, precond=1, tol_mode=1, tol=1e-7, max_iter=500, advect_scalars=True)
+    o = oracle_twin(sc, g, 1, 1, 1, 1e-9, 2000)
+    rng = np.random.default_rng(64)
+    other = [(rng.standard_normal(s) * 0.2).astype(np.float32) for s in oracle.face_shapes(sc.res)]
+    w_other = rng.random(sc.res[::-1]).astype(np.float32)
+    w_fluid = rng.random(sc.res[::-1]).astype(np.float32)
+    for _ in range(2):
+        g.update_without_pressure()
+        o.update_without_pressure()
+        g.mix_vel_field_with_others([torch.from_numpy(a).cuda() for a in other], torch.from_numpy(w_other).cuda(),
+                                    torch.from_numpy(w_fluid).cuda())
+        o.mix_vel_field_with_others(other, w_other, w_fluid)
+        g.solve_pressure()
+        o.solve_pressure()
+    assert vel_rel_l2(g.velocity_field(), o.velocity_field()) < 2e-3
+    pos, _ = g.particles()
+    pt = torch.from_numpy(pos).cuda()
+    out = torch.empty_like(pt)
+    g.transfer_vel_to_particles(pt, hfgrid.LINEAR, out)
+    ref = torch.empty_like(pt)
+    hfgrid.op_g2p_fc(sc.res, sc.origin, sc.spacing, [torch.from_numpy(a).cuda() for a in g.velocity_field()], pt,
+                     hfgrid.LINEAR, ref)
+    torch.cuda.synchronize()
+    assert torch.equal(out, ref)
+
+
+def test_pressure_fp64_option(cuda):
+    """pressure_fp64: the pressure iterate accumulated in FP64 and its
+    gradient differences taken in FP64.  The divergence of the projected
+    field then follows the CG residual instead of the FP32 rounding of the
+    pressure, and the pressure moves closer to the FP64 oracle."""
+    sc, paths = scenes.moving_boxes((40, 20, 40), seed=5)
+    runs = {}
+    for fp64 in (0, 1):
+        g = scenes.gpu_solver(sc, precond=1, tol_mode=1, tol=1e-6, max_iter=400, report_divergence=1,
+                              pressure_fp64=fp64)
+        for step in range(3):
+            for i, p in enumerate(paths):
+                g.set_boundary_velocity(i + 1, p.velocity(step * sc.dt))
+            g.update()
+        runs[fp64] = (g.stats(), g.pressure(), g.velocity_field())
+    o = oracle_twin(sc, scenes.gpu_solver(sc), 1, 1, 1, 1e-6, 400)
+    for step in range(3):
+        for i, p in enumerate(paths):
+            o.set_boundary_velocity(i + 1, p.velocity(step * sc.dt))
+        o.update()
+    st32, p32, _ = runs[0]
+    st64, p64, v64 = runs[1]
+    assert st64["divergence_l2"] < st32["divergence_l2"]
+    assert st64["divergence_l2"] <= 1e-5 * st64["cg_rhs_norm"]
+    assert vel_rel_l2(v64, o.velocity_field()) < 2e-3
