@@ -583,11 +583,8 @@ int extrapolateGrids(int ngrids, const Dim3i* rc, float* const* vals, int layers
   std::vector<unsigned int> h(kMaxLayers + 2);
   check(cudaMemcpyAsync(h.data(), offs.p, sizeof(unsigned int) * (kMaxLayers + 2), cudaMemcpyDeviceToHost, s), "read");
   check(cudaStreamSynchronize(s), "sync");
-  for (int d = 1; d < layers; ++d) {
-    unsigned int b = h[d], e = h[d + 1];
-    if (e <= b) break;
-    check(launchExtrapLayer(r3, v3, off, sc, b, e - b, d, s), "extrapolation layer");
-  }
+  int depth = 0;
+  check(launchExtrapLayers(r3, v3, off, sc, h.data(), layers, s, &depth, nullptr), "extrapolation layers");
   check(cudaStreamSynchronize(s), "sync");
   return HFG_OK;
 }

@@ -176,51 +176,6 @@ struct FaceSampler {
   }
 };
 
-// sampleFaceFast with a per-thread cache of the last 8 corner values of each
-// component, kept in shared memory ([slot][thread], conflict-free).  Points
-// that share a component's stencil cell (same clamped corner indices on every
-// axis) reuse the cached values: identical inputs, weights and summation
-// order, so the result equals sampleFaceFast bit for bit.  The substeps of a
-// particle sample three nearby points (CFL <= 1 cell per substep), which
-// mostly share their stencil cells.
-struct StencilCache {
-  float* val;  // [24][nthreads]: component a, corner k at (8a + k) * n + t
-  int* key;    // [9][nthreads]: component a, axis d at (3a + d) * n + t
-  int t, n;
-  __device__ __forceinline__ void reset() {
-#pragma unroll
-    for (int i = 0; i < 9; ++i) key[i * n + t] = -1;
-  }
-};
-__device__ __forceinline__ int axisKey(const AxisW& w) { return (w.i0 << 1) | (w.i1 - w.i0); }
-__device__ __forceinline__ void sampleFaceCached(const ConstFaceField& v, const Geom& g, float px, float py, float pz,
-                                                 StencilCache& c, float out[3]) {
-  FaceSampler s(g, px, py, pz);
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const AxisW& X = a == 0 ? s.fc[0] : s.cc[0];
-    const AxisW& Y = a == 1 ? s.fc[1] : s.cc[1];
-    const AxisW& Z = a == 2 ? s.fc[2] : s.cc[2];
-    const int kx = axisKey(X), ky = axisKey(Y), kz = axisKey(Z);
-    int* K = c.key + 3 * a * c.n + c.t;
-    float* V = c.val + 8 * a * c.n + c.t;
-    unsigned idx[8];
-    float w[8];
-    s.corners(g, a, idx, w);
-    if (K[0] != kx || K[c.n] != ky || K[2 * c.n] != kz) {
-#pragma unroll
-      for (int k = 0; k < 8; ++k) V[k * c.n] = __ldg(v.c[a] + idx[k]);
-      K[0] = kx;
-      K[c.n] = ky;
-      K[2 * c.n] = kz;
-    }
-    float r = 0.f;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) r = fmaf(w[k], V[k * c.n], r);
-    out[a] = r;
-  }
-}
-
 __device__ __forceinline__ void sampleFaceFast(const ConstFaceField& v, const Geom& g, float px, float py, float pz,
                                                float out[3]) {
   FaceSampler s(g, px, py, pz);

@@ -472,41 +472,102 @@ cudaError_t launchExtrapDistance(const Dim3i rc[3], float* const vals[3], long l
   return cudaGetLastError();
 }
 
-// One layer: mean of the neighbours with a smaller layer, summed in the fixed
-// order left, right, down, up, back, front (extrapolatingData).
-__global__ void kExtrapLayer(Dim3i r0, Dim3i r1, Dim3i r2, float* v0, float* v1, float* v2, long long off1,
-                             long long off2, const uint16_t* __restrict__ dist, const unsigned int* __restrict__ list,
-                             unsigned int begin, unsigned int count, int d) {
-  HFG_FOR(k, (long long)count) {
-    long long id = list[begin + k];
-    int a = id >= off2 ? 2 : (id >= off1 ? 1 : 0);
-    long long base = a == 2 ? off2 : (a == 1 ? off1 : 0);
-    long long i = id - base;
-    Dim3i r = a == 2 ? r2 : (a == 1 ? r1 : r0);
-    float* v = a == 2 ? v2 : (a == 1 ? v1 : v0);
-    const uint16_t* dd = dist + base;
-    int x, y, z;
-    cellCoord(i, r, x, y, z);
-    long long nb[6] = {linc(x - 1, y, z, r), linc(x + 1, y, z, r), linc(x, y - 1, z, r),
-                       linc(x, y + 1, z, r), linc(x, y, z - 1, r), linc(x, y, z + 1, r)};
-    float acc = 0.f, cnt = 0.f;
+// One entry of layer d: mean of the neighbours with a smaller layer, summed in
+// the fixed order left, right, down, up, back, front (extrapolatingData).
+// 32-bit index arithmetic: every face grid holds fewer than 2^31 entries.
+__device__ __forceinline__ void extrapEntry(const Dim3i& r0, const Dim3i& r1, const Dim3i& r2, float* v0, float* v1,
+                                            float* v2, unsigned off1, unsigned off2, const uint16_t* __restrict__ dist,
+                                            unsigned id, int d) {
+  const int a = id >= off2 ? 2 : (id >= off1 ? 1 : 0);
+  const unsigned base = a == 2 ? off2 : (a == 1 ? off1 : 0u);
+  const unsigned i = id - base;
+  const Dim3i r = a == 2 ? r2 : (a == 1 ? r1 : r0);
+  float* v = a == 2 ? v2 : (a == 1 ? v1 : v0);
+  const uint16_t* dd = dist + base;
+  const unsigned nx = (unsigned)r.x, ny = (unsigned)r.y, t = i / nx;
+  const int x = (int)(i - t * nx), y = (int)(t % ny), z = (int)(t / ny);
+  const unsigned plane = nx * ny;
+  const unsigned nb[6] = {x > 0 ? i - 1 : i, x + 1 < r.x ? i + 1 : i, y > 0 ? i - nx : i, y + 1 < r.y ? i + nx : i,
+                          z > 0 ? i - plane : i, z + 1 < r.z ? i + plane : i};
+  float acc = 0.f, cnt = 0.f;
 #pragma unroll
-    for (int q = 0; q < 6; ++q) {
-      if ((int)dd[nb[q]] < d) {
-        acc = __fadd_rn(acc, v[nb[q]]);
-        cnt = __fadd_rn(cnt, 1.f);
-      }
+  for (int q = 0; q < 6; ++q) {
+    if ((int)dd[nb[q]] < d) {
+      acc = __fadd_rn(acc, v[nb[q]]);
+      cnt = __fadd_rn(cnt, 1.f);
     }
-    if (cnt != 0.f) acc = __fdiv_rn(acc, cnt);
-    v[i] = acc;
+  }
+  if (cnt != 0.f) acc = __fdiv_rn(acc, cnt);
+  v[i] = acc;
+}
+
+__global__ void kExtrapLayer(Dim3i r0, Dim3i r1, Dim3i r2, float* v0, float* v1, float* v2, unsigned off1,
+                             unsigned off2, const uint16_t* __restrict__ dist, const unsigned int* __restrict__ list,
+                             unsigned int begin, unsigned int count, int d) {
+  HFG_FOR(k, (long long)count) extrapEntry(r0, r1, r2, v0, v1, v2, off1, off2, dist, list[begin + k], d);
+}
+
+// A run of small consecutive layers [dFirst, dLast] in one block: the block
+// barrier between layers orders layer d's writes before layer d+1's reads.
+__global__ void __launch_bounds__(1024) kExtrapLayerRun(Dim3i r0, Dim3i r1, Dim3i r2, float* v0, float* v1, float* v2,
+                                                        unsigned off1, unsigned off2,
+                                                        const uint16_t* __restrict__ dist,
+                                                        const unsigned int* __restrict__ list,
+                                                        const unsigned int* __restrict__ offsets, int dFirst,
+                                                        int dLast) {
+  for (int d = dFirst; d <= dLast; ++d) {
+    const unsigned b = offsets[d], e = offsets[d + 1];
+    for (unsigned k = b + threadIdx.x; k < e; k += blockDim.x)
+      extrapEntry(r0, r1, r2, v0, v1, v2, off1, off2, dist, list[k], d);
+    __syncthreads();
   }
 }
 
 cudaError_t launchExtrapLayer(const Dim3i rc[3], float* const vals[3], const long long off[3], ExtrapScratch sc,
                               unsigned int begin, unsigned int count, int d, cudaStream_t s) {
   if (count == 0) return cudaSuccess;
-  kExtrapLayer<<<gridFor(count), kThreads, 0, s>>>(rc[0], rc[1], rc[2], vals[0], vals[1], vals[2], off[1], off[2],
-                                                    sc.dist, sc.list, begin, count, d);
+  kExtrapLayer<<<gridFor(count), kThreads, 0, s>>>(rc[0], rc[1], rc[2], vals[0], vals[1], vals[2],
+                                                    (unsigned)off[1], (unsigned)off[2], sc.dist, sc.list, begin,
+                                                    count, d);
+  return cudaGetLastError();
+}
+
+// Layers 1 .. nums-1 from the host copy of the layer offsets: a layer larger
+// than kExtrapSmallLayer gets a grid-wide launch, runs of smaller consecutive
+// layers share one single-block launch.  Stops at the first empty layer.
+cudaError_t launchExtrapLayers(const Dim3i rc[3], float* const vals[3], const long long off[3], ExtrapScratch sc,
+                               const unsigned int* hostOffsets, int nums, cudaStream_t s, int* depth,
+                               long long* launches) {
+  int d = 1;
+  *depth = 0;
+  while (d < nums && d <= kMaxLayers) {
+    unsigned int b = hostOffsets[d], e = hostOffsets[d + 1];
+    if (e <= b) break;
+    cudaError_t err;
+    if (e - b > kExtrapSmallLayer) {
+      err = launchExtrapLayer(rc, vals, off, sc, b, e - b, d, s);
+      *depth = d++;
+    } else {
+      int last = d;
+      while (last + 1 < nums && last + 1 <= kMaxLayers) {
+        unsigned int nb = hostOffsets[last + 1], ne = hostOffsets[last + 2];
+        if (ne <= nb || ne - nb > kExtrapSmallLayer) break;
+        ++last;
+      }
+      err = launchExtrapLayerRun(rc, vals, off, sc, d, last, s);
+      *depth = last;
+      d = last + 1;
+    }
+    if (err != cudaSuccess) return err;
+    if (launches) ++*launches;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launchExtrapLayerRun(const Dim3i rc[3], float* const vals[3], const long long off[3], ExtrapScratch sc,
+                                 int dFirst, int dLast, cudaStream_t s) {
+  kExtrapLayerRun<<<1, 1024, 0, s>>>(rc[0], rc[1], rc[2], vals[0], vals[1], vals[2], (unsigned)off[1],
+                                     (unsigned)off[2], sc.dist, sc.list, sc.offsets, dFirst, dLast);
   return cudaGetLastError();
 }
 
@@ -964,11 +1025,7 @@ __global__ void __launch_bounds__(256, 4) kSubstep(Geom g, ConstFaceField vel, f
   float bmin[3] = {g.ox, g.oy, g.oz};
   float bmax[3] = {g.ox + (float)g.r.x * g.hx, g.oy + (float)g.r.y * g.hy, g.oz + (float)g.r.z * g.hz};
   float m = 0.f;
-  __shared__ float cacheVal[24 * kThreads];
-  __shared__ int cacheKey[9 * kThreads];
-  StencilCache sc{cacheVal, cacheKey, (int)threadIdx.x, kThreads};
   HFG_FOR(p, P) {
-    sc.reset();
     float q[3] = {pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]};
     float w0[3] = {v0[3 * p], v0[3 * p + 1], v0[3 * p + 2]};
     if (acc == 0) {
@@ -978,17 +1035,17 @@ __global__ void __launch_bounds__(256, 4) kSubstep(Geom g, ConstFaceField vel, f
       float mid[3], w1[3];
 #pragma unroll
       for (int a = 0; a < 3; ++a) mid[a] = fmaf(half, w0[a], q[a]);
-      sampleFaceCached(vel, g, mid[0], mid[1], mid[2], sc, w1);
+      sampleFaceFast(vel, g, mid[0], mid[1], mid[2], w1);
 #pragma unroll
       for (int a = 0; a < 3; ++a) q[a] = fmaf(ds, w1[a], q[a]);
     } else {
       float mid[3], tf[3], w1[3], w2[3];
 #pragma unroll
       for (int a = 0; a < 3; ++a) mid[a] = fmaf(half, w0[a], q[a]);
-      sampleFaceCached(vel, g, mid[0], mid[1], mid[2], sc, w1);
+      sampleFaceFast(vel, g, mid[0], mid[1], mid[2], w1);
 #pragma unroll
       for (int a = 0; a < 3; ++a) tf[a] = fmaf(tq, w1[a], q[a]);
-      sampleFaceCached(vel, g, tf[0], tf[1], tf[2], sc, w2);
+      sampleFaceFast(vel, g, tf[0], tf[1], tf[2], w2);
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         q[a] = fmaf(a29, w0[a], q[a]);
@@ -1003,7 +1060,7 @@ __global__ void __launch_bounds__(256, 4) kSubstep(Geom g, ConstFaceField vel, f
       }
     } else {
       float v[3];
-      sampleFaceCached(vel, g, q[0], q[1], q[2], sc, v);
+      sampleFaceFast(vel, g, q[0], q[1], q[2], v);
       v0[3 * p] = v[0]; v0[3 * p + 1] = v[1]; v0[3 * p + 2] = v[2];
       m = fmaxf(m, fmaxf(fabsf(v[0]), fmaxf(fabsf(v[1]), fabsf(v[2]))));
     }

@@ -159,6 +159,16 @@ cudaError_t launchExtrapDistance(const Dim3i rc[3], float* const vals[3], long l
                                  ExtrapScratch sc, cudaStream_t s);
 cudaError_t launchExtrapLayer(const Dim3i rc[3], float* const vals[3], const long long off[3], ExtrapScratch sc,
                               unsigned int begin, unsigned int count, int d, cudaStream_t s);
+// layers dFirst..dLast (each small) in one single-block launch; the layer
+// bounds come from sc.offsets on the device
+constexpr unsigned kExtrapSmallLayer = 4096;
+cudaError_t launchExtrapLayerRun(const Dim3i rc[3], float* const vals[3], const long long off[3], ExtrapScratch sc,
+                                 int dFirst, int dLast, cudaStream_t s);
+// every layer 1 .. nums-1 (host copy of the offsets), large layers one launch
+// each, runs of small ones together; *depth = deepest layer filled
+cudaError_t launchExtrapLayers(const Dim3i rc[3], float* const vals[3], const long long off[3], ExtrapScratch sc,
+                               const unsigned int* hostOffsets, int nums, cudaStream_t s, int* depth,
+                               long long* launches);
 
 // ---- fluid SDF (buildFluidSDF); frontier buffers hold N cells each; counts 2;
 // hostCount pinned.  Blocks (one host read per layer).

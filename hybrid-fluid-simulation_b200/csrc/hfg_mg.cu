@@ -296,7 +296,7 @@ struct Multigrid {
 Multigrid* mgCreate(const Dim3i& r, int levels, int smooth, bool half, cudaStream_t s) {
   auto* m = new Multigrid();
   m->r0 = r;
-  m->smooth = smooth > 0 ? smooth : 2;
+  m->smooth = smooth > 0 ? smooth : 3;  // 3 sweeps: fewest ms per solve at 256^3 (2: 67.3, 3: 65.6, 4: 66.9 ms per step)
   m->half = half;
   m->res.push_back(r);
   Dim3i cur = r;

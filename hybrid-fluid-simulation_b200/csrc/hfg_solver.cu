@@ -575,12 +575,8 @@ void GridSolver::extrapolate() {
                           stream_),
           "read layer offsets");
     check(cudaStreamSynchronize(stream_), "extrapolation sync");
-    for (int d = 1; d < nums && d <= kMaxLayers; ++d) {
-      unsigned int b = offHost_[d], e = offHost_[d + 1];
-      if (e <= b) break;
-      launched(launchExtrapLayer(fr_, vals, off, sc, b, e - b, d, stream_), "extrapolation layer");
-      extrapDepth_ = d;
-    }
+    check(launchExtrapLayers(fr_, vals, off, sc, offHost_, nums, stream_, &extrapDepth_, &launches_),
+          "extrapolation layers");
   }
   stageEnd(7);
 }
