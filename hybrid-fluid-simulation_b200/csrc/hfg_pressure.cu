@@ -309,7 +309,7 @@ namespace {
 // Fast row of A for the CG: the diagonal and its reciprocal come from a
 // 64-entry table per launch (indexed by the six "not solid" bits; the entries
 // are summed in the reference's order), the six off-diagonal terms are FP32
-// FMAs on masked neighbour values.
+// FMAs on the neighbour values.
 struct DiagTab {
   float d[64], inv[64];
 };
@@ -324,17 +324,20 @@ __device__ __forceinline__ void buildDiagTab(DiagTab& t, float sx, float sy, flo
   }
 }
 
+// The neighbour values need no masks here.  The CG vectors p, r and z are
+// zero at every cell that is not fluid: b is zero there, the row of A is the
+// identity, and the Jacobi and multigrid preconditioners write zero there, so
+// r -= alpha A p and p = z + beta p keep them zero.  The halo outside the
+// grid arrives zero-filled and the pitch padding is zero too.  So the only
+// neighbours that add anything are the fluid ones, as in the reference's
+// off-diagonal terms, and the sum is the masked sum up to the sign of a zero.
 __device__ __forceinline__ float fastRow(const DiagTab& t, Code k, float sx, float sy, float sz, float vc, float vl,
                                          float vr, float vd, float vu, float vb, float vf) {
-  if (!(k & 1)) return vc;
-  float nx = ((k >> 7) & 1 ? vl : 0.f) + ((k >> 8) & 1 ? vr : 0.f);
-  float ny = ((k >> 9) & 1 ? vd : 0.f) + ((k >> 10) & 1 ? vu : 0.f);
-  float nz = ((k >> 11) & 1 ? vb : 0.f) + ((k >> 12) & 1 ? vf : 0.f);
   float q = t.d[(k >> 1) & 63] * vc;
-  q = fmaf(-sx, nx, q);
-  q = fmaf(-sy, ny, q);
-  q = fmaf(-sz, nz, q);
-  return q;
+  q = fmaf(-sx, vl + vr, q);
+  q = fmaf(-sy, vd + vu, q);
+  q = fmaf(-sz, vb + vf, q);
+  return (k & 1) ? q : vc;
 }
 
 template <int PC>
@@ -353,6 +356,7 @@ __device__ __forceinline__ float fastZ(const DiagTab& t, Code k, float rv) {
 constexpr int CTX = 32, CTY = 8;     // threads per block (x, y)
 constexpr int RY = 2;                // rows per thread: thread (tx, ty) owns rows ty and ty + CTY
 constexpr int CTR = CTY * RY;        // 16 tile rows per plane
+static_assert(2 * CTR == CTX, "one warp computes both halo columns (one lane per halo cell)");
 constexpr int HXF = 4, HXC = 8;      // left pad of the float / code halo boxes
 constexpr int FW = CTX + 2 * HXF;    // 40 floats
 constexpr int CW = CTX + 2 * HXC;    // 48 codes
@@ -549,11 +553,17 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
       v[j] = pAt(row, tx + HXF, tx + HXC);
       kOwn[j] = S.code[row][tx + HXC];
       t[row][tx + 1] = v[j];
-      if (tx == 0) t[row][0] = pAt(row, HXF - 1, HXC - 1);
-      if (tx == CTX - 1) t[row][CTX + 1] = pAt(row, HXF + CTX, HXC + CTX);
     }
+    // the halo ring, one warp-wide pass per side: warps 0 and CTY-1 take the
+    // rows below and above; warp 3 takes both columns, lane l -> row
+    // 1 + (l & 15), left for l < 16, right otherwise
     if (ty == 0) t[0][tx + 1] = pAt(0, tx + HXF, tx + HXC);
     if (ty == CTY - 1) t[CTR + 1][tx + 1] = pAt(CTR + 1, tx + HXF, tx + HXC);
+    if (ty == 3) {
+      const int row = 1 + (tx & (CTR - 1));
+      const bool right = tx >= CTR;
+      t[row][right ? CTX + 1 : 0] = pAt(row, right ? HXF + CTX : HXF - 1, right ? HXC + CTX : HXC - 1);
+    }
   };
   bool ok = mbarWait(&bar[0], 0, deadline);
   if (ok) formTile(0, pt[0], cur, kCur);

@@ -59,7 +59,8 @@ long long sceneBytes(const int res[3], long long particles, int boundaries, int 
   b += N * 4 * (6 + 2);        // colour x2 x3, domain x2
   b += N * 2;                  // markers, solid index
   b += NC * (2 + 4 * 4);       // code, x, r, p x2
-  b += F * 8 + N * 8;          // P2G accumulators (faces, cells)
+  b += (F + ny * nz + (ny + 1) * nz + ny * (nz + 1)) * 8;  // P2G accumulators / x-pair tables (faces)
+  b += N * 8;                  // P2G accumulator (cells)
   b += F * (2 + 4);            // extrapolation distance + list
   b += N * 4 * (long long)boundaries;
   b += particles * (4 * 3 * 4 + 4);  // pos, vel, v0, vector scalars, scalar

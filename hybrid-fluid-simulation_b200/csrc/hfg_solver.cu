@@ -341,10 +341,12 @@ void GridSolver::forcesTerms(float gv[3], bool& doG, float ev[3], bool& doE) con
   doE = !tiny(ev);
 }
 
+size_t GridSolver::accCount(int a) const { return (size_t)std::max(F_[a], facePairCount(g_.r, a)); }
+
 void GridSolver::p2gFace(const float* vel, float* const out[3], float* const copy[3], const float add[3], bool doAdd,
                          const float add2[3], bool doAdd2) {
   for (int a = 0; a < 3; ++a) {
-    acc_[a].alloc(F_[a], stream_);
+    acc_[a].alloc(accCount(a), stream_);
     check(cudaMemsetAsync(acc_[a].p, 0, acc_[a].bytes(), stream_), "memset");
   }
   float2* acc[3] = {acc_[0].p, acc_[1].p, acc_[2].p};
@@ -365,7 +367,13 @@ void GridSolver::p2gCell(const float* vals, int span, int comp, float* out) {
 // EulerParticles.cpp:231-325.  Substeps are launched speculatively in chunks;
 // a launch whose slot is already finished does nothing.
 void GridSolver::advectParticles(const float* const vin[3]) {
-  ConstFaceField v{{vin[0], vin[1], vin[2]}};
+  float2* pairs[3];
+  for (int a = 0; a < 3; ++a) {
+    acc_[a].alloc(accCount(a), stream_);
+    pairs[a] = acc_[a].p;
+  }
+  launched(launchFacePairs(g_.r, ConstFaceField{{vin[0], vin[1], vin[2]}}, pairs, stream_), "face pairs");
+  FacePairs v{{pairs[0], pairs[1], pairs[2]}};
   check(cudaMemsetAsync(subState_.p, 0, sizeof(SubstepState) * (subSlots_ + 1), stream_), "memset");
   launched(launchSubstepBegin(g_, v, ppos_.p, pv0_.p, P_, subState_.p, stream_), "substep begin");
   long long nclamp = opt_.clamp_mode == 1 ? std::min<long long>(P_, N_) : P_;
