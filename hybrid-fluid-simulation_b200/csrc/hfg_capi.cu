@@ -701,10 +701,10 @@ HFG_API int hfg_op_advect_particles(const int res[3], const float origin[3], con
     Scratch<SubstepState> ss(slots + 1, s);
     Scratch<float> v0(3 * (n > 0 ? n : 1), s);
     check(cudaMemsetAsync(ss.p, 0, sizeof(SubstepState) * (slots + 1), s), "memset");
-    Scratch<float2> p0(facePairCount(g.r, 0), s), p1(facePairCount(g.r, 1), s), p2(facePairCount(g.r, 2), s);
-    float2* pairs[3] = {p0.p, p1.p, p2.p};
-    check(launchFacePairs(g.r, ConstFaceField{{vx, vy, vz}}, pairs, s), "face pairs");
-    FacePairs v{{p0.p, p1.p, p2.p}};
+    Scratch<float4> q0(faceQuadCount(g.r, 0), s), q1(faceQuadCount(g.r, 1), s), q2(faceQuadCount(g.r, 2), s);
+    float4* quads[3] = {q0.p, q1.p, q2.p};
+    check(launchFaceQuads(g.r, ConstFaceField{{vx, vy, vz}}, quads, s), "face corner tables");
+    FaceQuads v{{q0.p, q1.p, q2.p}};
     check(launchSubstepBegin(g, v, pos, v0.p, n, ss.p, s), "substep");
     long long nclamp = clamp_mode == 1 ? std::min<long long>(n, g.r.size()) : n;
     SubstepState host{};

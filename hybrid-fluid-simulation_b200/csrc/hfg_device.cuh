@@ -117,7 +117,7 @@ __device__ inline void sampleFace(const ConstFaceField& v, const Geom& cc, float
 // (EulerParticlesTool.cu:113-115); rounding differs in the last bits.
 struct AxisW {
   int i0, i1;
-  int j;  // x-pair entry: the floor index clamped to [-1, n - 1], plus one
+  int j;  // corner-table entry: the floor index clamped to [-1, n - 1], plus one
   float w1;
 };
 
@@ -130,11 +130,14 @@ __device__ __forceinline__ void axisWeights(float t, int n, AxisW& a) {
   a.j = min(max(i, -1), n - 1) + 1;
 }
 
-// x-pair table of a face grid with rows of n entries: rows of n + 1 float2,
-// entry j = (f[clamp(j - 1)], f[clamp(j)]), so entry AxisW::j of a sample holds
-// its two x corners (f[i0], f[i1]) and one 8-byte load serves both.
-struct FacePairs {
-  const float2* c[3];
+// Corner table of a face grid of nx x ny x nz values: (nx + 1) x (ny + 1) x nz
+// float4, entry (z, jy, jx) = (f[z][y0][x0], f[z][y0][x1], f[z][y1][x0],
+// f[z][y1][x1]) with x0 = clamp(jx - 1), x1 = clamp(jx), y0 = clamp(jy - 1),
+// y1 = clamp(jy).  Entry (AxisW::j of y, AxisW::j of x) of a sample holds the
+// four corners of one z layer of its trilinear stencil, so one 16-byte load
+// serves four corners.
+struct FaceQuads {
+  const float4* c[3];
 };
 
 struct FaceSampler {
@@ -172,26 +175,25 @@ struct FaceSampler {
     for (int k = 0; k < 8; ++k) v = fmaf(w[k], __ldg(f + idx[k]), v);
     return v;
   }
-  // the same sample from the x-pair table of the component: four 8-byte
+  // the same sample from the corner table of the component: two 16-byte
   // loads instead of eight 4-byte ones, same values and the same FMA chain
-  __device__ __forceinline__ float samplePairs(const Geom& g, int a, const float2* __restrict__ P) const {
+  __device__ __forceinline__ float sampleQuads(const Geom& g, int a, const float4* __restrict__ Q) const {
     const AxisW& X = a == 0 ? fc[0] : cc[0];
     const AxisW& Y = a == 1 ? fc[1] : cc[1];
     const AxisW& Z = a == 2 ? fc[2] : cc[2];
-    unsigned nx = (unsigned)(g.r.x + (a == 0) + 1), ny = (unsigned)(g.r.y + (a == 1));
-    unsigned r0 = (unsigned)Z.i0 * ny, r1 = (unsigned)Z.i1 * ny, j = (unsigned)X.j;
-    float2 q00 = __ldg(P + (r0 + Y.i0) * nx + j), q01 = __ldg(P + (r0 + Y.i1) * nx + j);
-    float2 q10 = __ldg(P + (r1 + Y.i0) * nx + j), q11 = __ldg(P + (r1 + Y.i1) * nx + j);
+    unsigned lx = (unsigned)(g.r.x + (a == 0) + 1), ly = (unsigned)(g.r.y + (a == 1) + 1);
+    unsigned row = (unsigned)Y.j * lx + (unsigned)X.j, pl = lx * ly;
+    float4 q0 = __ldg(Q + (unsigned)Z.i0 * pl + row), q1 = __ldg(Q + (unsigned)Z.i1 * pl + row);
     float x0 = 1.f - X.w1, x1 = X.w1, y0 = 1.f - Y.w1, y1 = Y.w1, z0 = 1.f - Z.w1, z1 = Z.w1;
     float v = 0.f;
-    v = fmaf(x0 * y0 * z0, q00.x, v);
-    v = fmaf(x1 * y0 * z0, q00.y, v);
-    v = fmaf(x0 * y1 * z0, q01.x, v);
-    v = fmaf(x1 * y1 * z0, q01.y, v);
-    v = fmaf(x0 * y0 * z1, q10.x, v);
-    v = fmaf(x1 * y0 * z1, q10.y, v);
-    v = fmaf(x0 * y1 * z1, q11.x, v);
-    v = fmaf(x1 * y1 * z1, q11.y, v);
+    v = fmaf(x0 * y0 * z0, q0.x, v);
+    v = fmaf(x1 * y0 * z0, q0.y, v);
+    v = fmaf(x0 * y1 * z0, q0.z, v);
+    v = fmaf(x1 * y1 * z0, q0.w, v);
+    v = fmaf(x0 * y0 * z1, q1.x, v);
+    v = fmaf(x1 * y0 * z1, q1.y, v);
+    v = fmaf(x0 * y1 * z1, q1.z, v);
+    v = fmaf(x1 * y1 * z1, q1.w, v);
     return v;
   }
   // sample of the difference field f - h at the same point
@@ -213,11 +215,11 @@ __device__ __forceinline__ void sampleFaceFast(const ConstFaceField& v, const Ge
 #pragma unroll
   for (int a = 0; a < 3; ++a) out[a] = s.sample(g, a, v.c[a]);
 }
-__device__ __forceinline__ void sampleFacePairs(const FacePairs& v, const Geom& g, float px, float py, float pz,
+__device__ __forceinline__ void sampleFaceQuads(const FaceQuads& v, const Geom& g, float px, float py, float pz,
                                                 float out[3]) {
   FaceSampler s(g, px, py, pz);
 #pragma unroll
-  for (int a = 0; a < 3; ++a) out[a] = s.samplePairs(g, a, v.c[a]);
+  for (int a = 0; a < 3; ++a) out[a] = s.sampleQuads(g, a, v.c[a]);
 }
 
 // Cubic samplers (MPhysics/EulerMathTool.cu:134-240, FieldMathTool.cu:106-173).

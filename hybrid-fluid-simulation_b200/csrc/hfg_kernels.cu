@@ -970,46 +970,48 @@ __device__ inline void blockMaxToGlobal(float m, unsigned int* dst) {
   }
 }
 
-// x-pair tables of the three face grids (FacePairs), one component per
-// blockIdx.y: entry (z, y, j) = (f[z][y][clamp(j - 1)], f[z][y][clamp(j)]).
-__global__ void kFacePairs(Dim3i r, ConstFaceField v, float2* p0, float2* p1, float2* p2) {
+// Corner tables of the three face grids (FaceQuads), one component per
+// blockIdx.y; consecutive threads take consecutive jx.
+__global__ void kFaceQuads(Dim3i r, ConstFaceField v, float4* q0, float4* q1, float4* q2) {
   const int a = blockIdx.y;
   const unsigned nx = (unsigned)(r.x + (a == 0)), ny = (unsigned)(r.y + (a == 1)), nz = (unsigned)(r.z + (a == 2));
-  const unsigned L = nx + 1;
-  const long long n = (long long)L * ny * nz;
+  const unsigned lx = nx + 1, ly = ny + 1;
+  const long long n = (long long)lx * ly * nz;
   const float* __restrict__ f = a == 0 ? v.c[0] : (a == 1 ? v.c[1] : v.c[2]);
-  float2* __restrict__ out = a == 0 ? p0 : (a == 1 ? p1 : p2);
+  float4* __restrict__ out = a == 0 ? q0 : (a == 1 ? q1 : q2);
   HFG_FOR(e, n) {
-    const unsigned row = (unsigned)(e / L), j = (unsigned)(e - (long long)row * L);
-    const unsigned base = row * nx;
-    const unsigned lo = j > 0 ? j - 1 : 0, hi = j < nx ? j : nx - 1;
-    out[e] = make_float2(__ldg(f + base + lo), __ldg(f + base + hi));
+    const unsigned t = (unsigned)(e / lx), jx = (unsigned)(e - (long long)t * lx);
+    const unsigned z = t / ly, jy = t - z * ly;
+    const unsigned x0 = jx > 0 ? jx - 1 : 0, x1 = jx < nx ? jx : nx - 1;
+    const unsigned y0 = jy > 0 ? jy - 1 : 0, y1 = jy < ny ? jy : ny - 1;
+    const unsigned b0 = (z * ny + y0) * nx, b1 = (z * ny + y1) * nx;
+    out[e] = make_float4(__ldg(f + b0 + x0), __ldg(f + b0 + x1), __ldg(f + b1 + x0), __ldg(f + b1 + x1));
   }
 }
-long long facePairCount(const Dim3i& r, int a) {
-  return (long long)(r.x + (a == 0) + 1) * (r.y + (a == 1)) * (r.z + (a == 2));
+long long faceQuadCount(const Dim3i& r, int a) {
+  return (long long)(r.x + (a == 0) + 1) * (r.y + (a == 1) + 1) * (r.z + (a == 2));
 }
-cudaError_t launchFacePairs(const Dim3i& r, ConstFaceField v, float2* const out[3], cudaStream_t s) {
-  long long n = facePairCount(r, 0);
+cudaError_t launchFaceQuads(const Dim3i& r, ConstFaceField v, float4* const out[3], cudaStream_t s) {
+  long long n = faceQuadCount(r, 0);
   dim3 grid(gridFor(n), 3);
-  kFacePairs<<<grid, kThreads, 0, s>>>(r, v, out[0], out[1], out[2]);
+  kFaceQuads<<<grid, kThreads, 0, s>>>(r, v, out[0], out[1], out[2]);
   return cudaGetLastError();
 }
 
 // First velocity sample of the substep loop (EulerParticles.cpp:249-251):
 // v0 = trilinear(vel, pos) and max |v0| over every component.
-__global__ void kSubstepBegin(Geom g, FacePairs vel, const float* __restrict__ pos, float* __restrict__ v0,
+__global__ void kSubstepBegin(Geom g, FaceQuads vel, const float* __restrict__ pos, float* __restrict__ v0,
                               long long P, SubstepState* st) {
   float m = 0.f;
   HFG_FOR(p, P) {
     float v[3];
-    sampleFacePairs(vel, g, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2], v);
+    sampleFaceQuads(vel, g, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2], v);
     v0[3 * p] = v[0]; v0[3 * p + 1] = v[1]; v0[3 * p + 2] = v[2];
     m = fmaxf(m, fmaxf(fabsf(v[0]), fmaxf(fabsf(v[1]), fabsf(v[2]))));
   }
   blockMaxToGlobal(m, &st[0].maxAbsBits);
 }
-cudaError_t launchSubstepBegin(const Geom& g, FacePairs vel, const float* pos, float* v0, long long P,
+cudaError_t launchSubstepBegin(const Geom& g, FaceQuads vel, const float* pos, float* v0, long long P,
                                SubstepState* st, cudaStream_t s) {
   kSubstepBegin<<<gridFor(P > 0 ? P : 1), kThreads, 0, s>>>(g, vel, pos, v0, P, st);
   return cudaGetLastError();
@@ -1034,7 +1036,7 @@ __device__ inline float substepSize(const SubstepState& s, float dt, float cfl, 
 // box clamp of fixParticlesPosWithBoundarys (EulerParticlesTool.cu:310-333) is
 // applied to the first `nclamp` particles; otherwise the next v0 and its max
 // are produced for slot+1.
-__global__ void __launch_bounds__(256, 4) kSubstep(Geom g, FacePairs vel, float* __restrict__ pos,
+__global__ void __launch_bounds__(256, 4) kSubstep(Geom g, FaceQuads vel, float* __restrict__ pos,
                                                   float* __restrict__ v0, long long P,
                          int acc, float dt, float cfl, long long nclamp, SubstepState* st, int slot) {
   const SubstepState cur = st[slot];
@@ -1061,23 +1063,27 @@ __global__ void __launch_bounds__(256, 4) kSubstep(Geom g, FacePairs vel, float*
       float mid[3], w1[3];
 #pragma unroll
       for (int a = 0; a < 3; ++a) mid[a] = fmaf(half, w0[a], q[a]);
-      sampleFacePairs(vel, g, mid[0], mid[1], mid[2], w1);
+      sampleFaceQuads(vel, g, mid[0], mid[1], mid[2], w1);
 #pragma unroll
       for (int a = 0; a < 3; ++a) q[a] = fmaf(ds, w1[a], q[a]);
     } else {
-      float mid[3], tf[3], w1[3], w2[3];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) mid[a] = fmaf(half, w0[a], q[a]);
-      sampleFacePairs(vel, g, mid[0], mid[1], mid[2], w1);
-#pragma unroll
-      for (int a = 0; a < 3; ++a) tf[a] = fmaf(tq, w1[a], q[a]);
-      sampleFacePairs(vel, g, tf[0], tf[1], tf[2], w2);
+      // q + a29 w0 + a39 w1 + a49 w2, in that order, accumulated as soon as
+      // each sample is known so that fewer values stay live across a sample
+      float mid[3], tf[3], acc3[3], w[3];
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        q[a] = fmaf(a29, w0[a], q[a]);
-        q[a] = fmaf(a39, w1[a], q[a]);
-        q[a] = fmaf(a49, w2[a], q[a]);
+        mid[a] = fmaf(half, w0[a], q[a]);
+        acc3[a] = fmaf(a29, w0[a], q[a]);
       }
+      sampleFaceQuads(vel, g, mid[0], mid[1], mid[2], w);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        tf[a] = fmaf(tq, w[a], q[a]);
+        acc3[a] = fmaf(a39, w[a], acc3[a]);
+      }
+      sampleFaceQuads(vel, g, tf[0], tf[1], tf[2], w);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) q[a] = fmaf(a49, w[a], acc3[a]);
     }
     if (last) {
       if (p < nclamp) {
@@ -1086,7 +1092,7 @@ __global__ void __launch_bounds__(256, 4) kSubstep(Geom g, FacePairs vel, float*
       }
     } else {
       float v[3];
-      sampleFacePairs(vel, g, q[0], q[1], q[2], v);
+      sampleFaceQuads(vel, g, q[0], q[1], q[2], v);
       v0[3 * p] = v[0]; v0[3 * p + 1] = v[1]; v0[3 * p + 2] = v[2];
       m = fmaxf(m, fmaxf(fabsf(v[0]), fmaxf(fabsf(v[1]), fabsf(v[2]))));
     }
@@ -1099,7 +1105,7 @@ __global__ void __launch_bounds__(256, 4) kSubstep(Geom g, FacePairs vel, float*
     st[slot + 1].count = cur.count + 1;
   }
 }
-cudaError_t launchSubstep(const Geom& g, FacePairs vel, float* pos, float* v0, long long P, int acc, float dt,
+cudaError_t launchSubstep(const Geom& g, FaceQuads vel, float* pos, float* v0, long long P, int acc, float dt,
                           float cfl, long long nclamp, SubstepState* st, int slot, cudaStream_t s) {
   kSubstep<<<gridFor(P > 0 ? P : 1), kThreads, 0, s>>>(g, vel, pos, v0, P, acc, dt, cfl, nclamp, st, slot);
   return cudaGetLastError();

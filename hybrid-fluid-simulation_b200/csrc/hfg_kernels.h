@@ -196,13 +196,13 @@ cudaError_t launchSeedWrite(const Geom& g, const float* fluidSDF, const uint8_t*
 cudaError_t launchParticleVelUpdate(const Geom& g, int mode, int alg, ConstFaceField vin, ConstFaceField prev,
                                     int firstFlip, float mixing, const float* pos, float* vel, long long P,
                                     cudaStream_t s);
-// x-pair tables of the face grids for the substep kernels; component a has
-// facePairCount(r, a) entries.
-long long facePairCount(const Dim3i& r, int a);
-cudaError_t launchFacePairs(const Dim3i& r, ConstFaceField v, float2* const out[3], cudaStream_t s);
-cudaError_t launchSubstepBegin(const Geom& g, FacePairs vel, const float* pos, float* v0, long long P,
+// Corner tables of the face grids for the substep kernels; component a has
+// faceQuadCount(r, a) entries.
+long long faceQuadCount(const Dim3i& r, int a);
+cudaError_t launchFaceQuads(const Dim3i& r, ConstFaceField v, float4* const out[3], cudaStream_t s);
+cudaError_t launchSubstepBegin(const Geom& g, FaceQuads vel, const float* pos, float* v0, long long P,
                                SubstepState* st, cudaStream_t s);
-cudaError_t launchSubstep(const Geom& g, FacePairs vel, float* pos, float* v0, long long P, int acc, float dt,
+cudaError_t launchSubstep(const Geom& g, FaceQuads vel, float* pos, float* v0, long long P, int acc, float dt,
                           float cfl, long long nclamp, SubstepState* st, int slot, cudaStream_t s);
 cudaError_t launchP2GFace(const Geom& g, int alg, const float* pos, const float* vel, long long P, float2* acc[3],
                           cudaStream_t s);

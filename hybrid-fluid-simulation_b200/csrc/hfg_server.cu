@@ -48,7 +48,8 @@ double percentile(std::vector<double> v, double q) {
 // Device bytes of one resident scene: the GridSolver allocations (face
 // velocities x2 + FLIP copy, colour / domain double buffers, markers, solid
 // index, stencil code and CG vectors on the pitched grid, P2G accumulators,
-// extrapolation scratch, boundary SDFs, particles) plus the multigrid levels.
+// face corner tables, extrapolation scratch, boundary SDFs, particles) plus
+// the multigrid levels.
 long long sceneBytes(const int res[3], long long particles, int boundaries, int precond) {
   const long long nx = res[0], ny = res[1], nz = res[2];
   const long long N = nx * ny * nz;
@@ -59,8 +60,8 @@ long long sceneBytes(const int res[3], long long particles, int boundaries, int 
   b += N * 4 * (6 + 2);        // colour x2 x3, domain x2
   b += N * 2;                  // markers, solid index
   b += NC * (2 + 4 * 4);       // code, x, r, p x2
-  b += (F + ny * nz + (ny + 1) * nz + ny * (nz + 1)) * 8;  // P2G accumulators / x-pair tables (faces)
-  b += N * 8;                  // P2G accumulator (cells)
+  b += F * 8 + N * 8;          // P2G accumulators (faces, cells)
+  b += ((nx + 2) * (ny + 1) * nz + (nx + 1) * (ny + 2) * nz + (nx + 1) * (ny + 1) * (nz + 1)) * 16;  // corner tables
   b += F * (2 + 4);            // extrapolation distance + list
   b += N * 4 * (long long)boundaries;
   b += particles * (4 * 3 * 4 + 4);  // pos, vel, v0, vector scalars, scalar

@@ -341,12 +341,10 @@ void GridSolver::forcesTerms(float gv[3], bool& doG, float ev[3], bool& doE) con
   doE = !tiny(ev);
 }
 
-size_t GridSolver::accCount(int a) const { return (size_t)std::max(F_[a], facePairCount(g_.r, a)); }
-
 void GridSolver::p2gFace(const float* vel, float* const out[3], float* const copy[3], const float add[3], bool doAdd,
                          const float add2[3], bool doAdd2) {
   for (int a = 0; a < 3; ++a) {
-    acc_[a].alloc(accCount(a), stream_);
+    acc_[a].alloc(F_[a], stream_);
     check(cudaMemsetAsync(acc_[a].p, 0, acc_[a].bytes(), stream_), "memset");
   }
   float2* acc[3] = {acc_[0].p, acc_[1].p, acc_[2].p};
@@ -367,13 +365,13 @@ void GridSolver::p2gCell(const float* vals, int span, int comp, float* out) {
 // EulerParticles.cpp:231-325.  Substeps are launched speculatively in chunks;
 // a launch whose slot is already finished does nothing.
 void GridSolver::advectParticles(const float* const vin[3]) {
-  float2* pairs[3];
+  float4* quads[3];
   for (int a = 0; a < 3; ++a) {
-    acc_[a].alloc(accCount(a), stream_);
-    pairs[a] = acc_[a].p;
+    quads_[a].alloc(faceQuadCount(g_.r, a), stream_);
+    quads[a] = quads_[a].p;
   }
-  launched(launchFacePairs(g_.r, ConstFaceField{{vin[0], vin[1], vin[2]}}, pairs, stream_), "face pairs");
-  FacePairs v{{pairs[0], pairs[1], pairs[2]}};
+  launched(launchFaceQuads(g_.r, ConstFaceField{{vin[0], vin[1], vin[2]}}, quads, stream_), "face corner tables");
+  FaceQuads v{{quads[0], quads[1], quads[2]}};
   check(cudaMemsetAsync(subState_.p, 0, sizeof(SubstepState) * (subSlots_ + 1), stream_), "memset");
   launched(launchSubstepBegin(g_, v, ppos_.p, pv0_.p, P_, subState_.p, stream_), "substep begin");
   long long nclamp = opt_.clamp_mode == 1 ? std::min<long long>(P_, N_) : P_;

@@ -187,10 +187,8 @@ class GridSolver {
   DArray<SubstepState> subState_;
   SubstepState* subHost_ = nullptr;  // pinned
   int subSlots_ = 4096;
-  // P2G accumulators of the face grids; during the particle substeps the same
-  // buffers hold the x-pair tables of the advecting velocity
   DArray<float2> acc_[3], cacc_;
-  size_t accCount(int a) const;
+  DArray<float4> quads_[3];  // corner tables of the advecting velocity (particle substeps)
   DArray<uint16_t> dist_;
   DArray<unsigned int> list_, hist_, offsets_, cursor_;
   unsigned int* offHost_ = nullptr;  // pinned
