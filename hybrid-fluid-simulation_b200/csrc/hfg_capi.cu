@@ -508,11 +508,12 @@ HFG_API int hfg_op_project(const int res[3], const float spacing[3], float dt, c
     long long N = g.r.size(), NC = cg.size();
     cudaStream_t s = st(stream);
     Scratch<Code> code(NC, s);
+    Scratch<CgCode> cgc(NC, s);
     Scratch<float> r(NC, s), x(NC, s), p0(NC, s), p1(NC, s);
     Scratch<double> part(cgPartialsNeeded(g.r), s);
     Scratch<CgState> cs(1, s);
     CgMaps maps;
-    check(makeCgMaps(cg, code.p, r.p, x.p, false, p0.p, p1.p, &maps), "tensor maps");
+    check(makeCgMaps(cg, cgc.p, r.p, x.p, false, p0.p, p1.p, &maps), "tensor maps");
     CgState init{};
     init.maxIter = (int)std::min<long long>(max_iter < 0 ? N : max_iter, 0x7fffffff);
     init.precond = precond == HFG_PRECOND_JACOBI ? 1 : 0;
@@ -521,7 +522,7 @@ HFG_API int hfg_op_project(const int res[3], const float spacing[3], float dt, c
     check(cudaMemcpyAsync(cs.p, &init, sizeof(init), cudaMemcpyHostToDevice, s), "state");
     float sx, sy, sz;
     scalesA(spacing, dt, sx, sy, sz);
-    check(launchStencilCode(g.r, cg.x, markers, code.p, s), "code");
+    check(launchStencilCode(g.r, cg.x, markers, code.p, s, cgc.p), "code");
     ConstFaceField v{{vx, vy, vz}}, sv{{svx, svy, svz}};
     SolidVelTable none{};
     check(launchRhsInit(g, v, sv, none, markers, code.p, sx, sy, sz, nullptr, r.p, x.p, false, p0.p, part.p, cs.p,
@@ -533,7 +534,7 @@ HFG_API int hfg_op_project(const int res[3], const float spacing[3], float dt, c
     for (;;) {
       for (int k = 0; k < 16; ++k, ++it) {
         const int po = it & 1, pn = (it + 1) & 1;
-        check(launchCgDirection(cg, sx, sy, sz, maps.rH, maps.pH[po], maps.codeH, code.p, r.p, pb[po], pb[pn], part.p,
+        check(launchCgDirection(cg, sx, sy, sz, maps.rH, maps.pH[po], maps.codeH, cgc.p, r.p, pb[po], pb[pn], part.p,
                                 cs.p, init.precond, s),
               "cg");
         check(launchCgUpdate(cg, sx, sy, sz, maps.pH[pn], maps.rI, maps.xI, maps.codeI, pb[pn], x.p, false, r.p, part.p,

@@ -1050,8 +1050,6 @@ __global__ void __launch_bounds__(256, 4) kSubstep(Geom g, FaceQuads vel, float*
   float ds = substepSize(cur, dt, cfl, minH, last);
   float half = (float)(0.5 * (double)ds), tq = (float)(0.75 * (double)ds);
   float a29 = (float)(2.0 / 9.0 * (double)ds), a39 = (float)(3.0 / 9.0 * (double)ds), a49 = (float)(4.0 / 9.0 * (double)ds);
-  float bmin[3] = {g.ox, g.oy, g.oz};
-  float bmax[3] = {g.ox + (float)g.r.x * g.hx, g.oy + (float)g.r.y * g.hy, g.oz + (float)g.r.z * g.hz};
   float m = 0.f;
   HFG_FOR(p, P) {
     float q[3] = {pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]};
@@ -1086,7 +1084,9 @@ __global__ void __launch_bounds__(256, 4) kSubstep(Geom g, FaceQuads vel, float*
       for (int a = 0; a < 3; ++a) q[a] = fmaf(a49, w[a], acc3[a]);
     }
     if (last) {
-      if (p < nclamp) {
+      if (p < nclamp) {  // the box bounds are formed here, from the kernel parameters
+        const float bmin[3] = {g.ox, g.oy, g.oz};
+        const float bmax[3] = {g.ox + (float)g.r.x * g.hx, g.oy + (float)g.r.y * g.hy, g.oz + (float)g.r.z * g.hz};
 #pragma unroll
         for (int a = 0; a < 3; ++a) q[a] = fmaxf(bmin[a], fminf(q[a], bmax[a]));
       }

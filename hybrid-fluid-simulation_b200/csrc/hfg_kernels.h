@@ -91,15 +91,21 @@ cudaError_t launchFluidDomainFromBBox(const Geom& g, const float mn[3], const fl
 // diagonal of buildPressureMatrixA, EulerSolverTool.cu:85-120); bits 7..12
 // that neighbour is inside the grid and fluid (the off-diagonals).
 typedef uint16_t Code;
+// Bits 0..6 of the code (fluid, the six "not solid" neighbours): all the CG
+// kernels read.  The neighbour-is-fluid bits are not needed there because
+// every CG vector is zero off the fluid.
+typedef uint8_t CgCode;
 // The pressure system lives on a pitched copy of the grid: rows of
-// px = cgPitch(nx) >= nx cells, px a multiple of 8 so that every row of FP32
-// values and of 16-bit codes starts on a 16-byte boundary (TMA tiles).  The
+// px = cgPitch(nx) >= nx cells, px a multiple of 16 so that every row of FP32
+// values and of 8-bit CG codes starts on a 16-byte boundary (TMA tiles).  The
 // cells x >= nx are inert: code 0 and every CG vector 0 there.  Index of cell
 // (x, y, z): (z * ny + y) * px + x.
-__host__ __device__ inline int cgPitch(int nx) { return (nx + 7) & ~7; }
+__host__ __device__ inline int cgPitch(int nx) { return (nx + 15) & ~15; }
 __host__ __device__ inline Dim3i cgDims(const Dim3i& r) { return Dim3i{cgPitch(r.x), r.y, r.z}; }
 // Codes of grid `r` written with row pitch px (px = r.x: unpitched).
-cudaError_t launchStencilCode(const Dim3i& r, int px, const uint8_t* markers, Code* code, cudaStream_t s);
+// With `cgc`, the CG codes too (same pitch).
+cudaError_t launchStencilCode(const Dim3i& r, int px, const uint8_t* markers, Code* code, cudaStream_t s,
+                              CgCode* cgc = nullptr);
 cudaError_t launchMatrixA(const Dim3i& r, float sx, float sy, float sz, const Code* code, float* A, cudaStream_t s);
 cudaError_t launchApplyA(const Dim3i& r, float sx, float sy, float sz, const Code* code, const float* x, float* y,
                          cudaStream_t s);
@@ -117,13 +123,13 @@ struct CgMaps {
   CUtensorMap codeH, codeI, rH, rI, xI, pH[2];
 };
 // x: the pressure iterate, FP32 or (xDouble) FP64
-cudaError_t makeCgMaps(const Dim3i& cg, const Code* code, const float* r, const void* x, bool xDouble,
+cudaError_t makeCgMaps(const Dim3i& cg, const CgCode* code, const float* r, const void* x, bool xDouble,
                        const float* p0, const float* p1, CgMaps* m);
 cudaError_t makeHaloMap(const Dim3i& cg, const float* v, CUtensorMap* m);
 // precond: 0 identity, 1 Jacobi, 2 z read through mZ (must match CgState::precond);
 // mZ is the halo map of r (precond 0, 1) or of z (2); zr the same array.
 cudaError_t launchCgDirection(const Dim3i& cg, float sx, float sy, float sz, const CUtensorMap& mZ,
-                              const CUtensorMap& mPo, const CUtensorMap& mCode, const Code* code, const float* zr,
+                              const CUtensorMap& mPo, const CUtensorMap& mCode, const CgCode* code, const float* zr,
                               const float* pOld, float* pNew, double* partials, CgState* st, int precond,
                               cudaStream_t s);
 cudaError_t launchCgUpdate(const Dim3i& cg, float sx, float sy, float sz, const CUtensorMap& mP, const CUtensorMap& mR,

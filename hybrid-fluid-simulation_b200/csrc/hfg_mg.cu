@@ -489,7 +489,7 @@ void mgSetup(Multigrid* m, const Dim3i& r, const uint8_t* mk0, const Code* code,
 // Preconditioned CG with the V-cycle: the RHS kernel already set r = b,
 // x = 0 and ||b||^2.  Iterations are launched in chunks; every kernel returns
 // immediately once the state says done.
-void mgRunCg(Multigrid* m, const Dim3i& cg, float sx, float sy, float sz, const CgMaps& maps, const Code* code, void* x,
+void mgRunCg(Multigrid* m, const Dim3i& cg, float sx, float sy, float sz, const CgMaps& maps, const CgCode* code, void* x,
              bool xDouble, float* rvec, CgState* st, CgState* stHost, cudaStream_t s, long long& launches,
              const std::function<cudaGraphExec_t(const std::function<void()>&)>& capture, cudaGraphExec_t* chunk) {
   check(cudaMemsetAsync(m->p[0].p, 0, m->p[0].bytes(), s), "memset");

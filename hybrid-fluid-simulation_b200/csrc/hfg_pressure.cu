@@ -87,7 +87,8 @@ __device__ __forceinline__ float applyRow(Code k, float sx, float sy, float sz, 
 
 
 // ---------------------------------------------------------------------------
-__global__ void kStencilCode(Dim3i r, int px, const uint8_t* __restrict__ mk, Code* __restrict__ code, int zPer) {
+__global__ void kStencilCode(Dim3i r, int px, const uint8_t* __restrict__ mk, Code* __restrict__ code,
+                             CgCode* __restrict__ cgc, int zPer) {
   int x = blockIdx.x * TX + threadIdx.x, y = blockIdx.y * TY + threadIdx.y;
   if (x >= px || y >= r.y) return;
   int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, r.z);
@@ -109,11 +110,13 @@ __global__ void kStencilCode(Dim3i r, int px, const uint8_t* __restrict__ mk, Co
       }
     }
     code[o] = k;
+    if (cgc) cgc[o] = (CgCode)(k & 0x7f);
   }
 }
-cudaError_t launchStencilCode(const Dim3i& r, int px, const uint8_t* markers, Code* code, cudaStream_t s) {
+cudaError_t launchStencilCode(const Dim3i& r, int px, const uint8_t* markers, Code* code, cudaStream_t s,
+                              CgCode* cgc) {
   CgGrid g = cgGrid(Dim3i{px, r.y, r.z});
-  kStencilCode<<<g.grid, g.block, 0, s>>>(r, px, markers, code, g.zPer);
+  kStencilCode<<<g.grid, g.block, 0, s>>>(r, px, markers, code, cgc, g.zPer);
   return cudaGetLastError();
 }
 
@@ -331,7 +334,7 @@ __device__ __forceinline__ void buildDiagTab(DiagTab& t, float sx, float sy, flo
 // grid arrives zero-filled and the pitch padding is zero too.  So the only
 // neighbours that add anything are the fluid ones, as in the reference's
 // off-diagonal terms, and the sum is the masked sum up to the sign of a zero.
-__device__ __forceinline__ float fastRow(const DiagTab& t, Code k, float sx, float sy, float sz, float vc, float vl,
+__device__ __forceinline__ float fastRow(const DiagTab& t, CgCode k, float sx, float sy, float sz, float vc, float vl,
                                          float vr, float vd, float vu, float vb, float vf) {
   float q = t.d[(k >> 1) & 63] * vc;
   q = fmaf(-sx, vl + vr, q);
@@ -341,7 +344,7 @@ __device__ __forceinline__ float fastRow(const DiagTab& t, Code k, float sx, flo
 }
 
 template <int PC>
-__device__ __forceinline__ float fastZ(const DiagTab& t, Code k, float rv) {
+__device__ __forceinline__ float fastZ(const DiagTab& t, CgCode k, float rv) {
   if (PC != 1) return rv;
   return (k & 1) ? rv * t.inv[(k >> 1) & 63] : rv;
 }
@@ -357,9 +360,9 @@ constexpr int CTX = 32, CTY = 8;     // threads per block (x, y)
 constexpr int RY = 2;                // rows per thread: thread (tx, ty) owns rows ty and ty + CTY
 constexpr int CTR = CTY * RY;        // 16 tile rows per plane
 static_assert(2 * CTR == CTX, "one warp computes both halo columns (one lane per halo cell)");
-constexpr int HXF = 4, HXC = 8;      // left pad of the float / code halo boxes
+constexpr int HXF = 4, HXC = 16;     // left pad of the float / code halo boxes (16 bytes)
 constexpr int FW = CTX + 2 * HXF;    // 40 floats
-constexpr int CW = CTX + 2 * HXC;    // 48 codes
+constexpr int CW = CTX + 2 * HXC;    // 64 codes
 constexpr int FH = CTR + 2;          // 18 rows
 constexpr int kDirStages = 4, kUpdStages = 5;
 constexpr unsigned long long kWaitNs = 2000000000ull;  // a stage that takes 2 s to land is an error
@@ -421,19 +424,19 @@ __device__ void drainStages(uint64_t* bar, const int* issued, int waited) {
 struct __align__(128) DirStage {
   alignas(128) float r[FH][FW];
   alignas(128) float po[FH][FW];
-  alignas(128) Code code[FH][CW];
+  alignas(128) CgCode code[FH][CW];
 };
-constexpr unsigned kDirStageBytes = sizeof(float) * FH * FW * 2 + sizeof(Code) * FH * CW;
+constexpr unsigned kDirStageBytes = sizeof(float) * FH * FW * 2 + sizeof(CgCode) * FH * CW;
 
 // TX: the pressure iterate x in FP32 (the reference's Real) or FP64.
 template <class TX> struct __align__(128) UpdStage {
   alignas(128) float p[FH][FW];
   alignas(128) float r[CTR][CTX];
   alignas(128) TX x[CTR][CTX];
-  alignas(128) Code code[CTR][CTX];
+  alignas(128) CgCode code[CTR][CTX];
 };
 template <class TX>
-constexpr unsigned kUpdStageBytes = sizeof(float) * (FH * FW + CTR * CTX) + sizeof(TX) * CTR * CTX + sizeof(Code) * CTR * CTX;
+constexpr unsigned kUpdStageBytes = sizeof(float) * (FH * FW + CTR * CTX) + sizeof(TX) * CTR * CTX + sizeof(CgCode) * CTR * CTX;
 template <class TX> constexpr int kUpdStagesT = sizeof(TX) == 8 ? 4 : kUpdStages;  // keeps static shared memory < 48 KB
 
 struct CgLaunch {
@@ -489,7 +492,7 @@ template <int PC>
 __global__ void __launch_bounds__(CTX* CTY, 4)
     kCgDirection(const __grid_constant__ CUtensorMap mZ, const __grid_constant__ CUtensorMap mPo,
                  const __grid_constant__ CUtensorMap mCode, Dim3i P, float sx, float sy, float sz,
-                 const Code* __restrict__ code, const float* __restrict__ zr, const float* __restrict__ pOld,
+                 const CgCode* __restrict__ code, const float* __restrict__ zr, const float* __restrict__ pOld,
                  float* __restrict__ pNew, double* partials, CgState* st, int zPer) {
   if (st->done) return;
   __shared__ DirStage stg[kDirStages];
@@ -527,7 +530,7 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
   bool in[RY];
   unsigned c[RY];
   float below[RY], cur[RY], above[RY];
-  Code kCur[RY], kAbove[RY];
+  CgCode kCur[RY], kAbove[RY];
 #pragma unroll
   for (int j = 0; j < RY; ++j) {
     const int y = y0 + ty + j * CTY;
@@ -542,7 +545,7 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
   }
   // p of stage i's plane into tile t: the thread's RY cells, the x halo of its
   // rows and, for the edge warps, the y halo rows; own p and codes returned
-  auto formTile = [&](int i, float (*t)[CTX + 2], float* v, Code* kOwn) {
+  auto formTile = [&](int i, float (*t)[CTX + 2], float* v, CgCode* kOwn) {
     const DirStage& S = stg[i % kDirStages];
     auto pAt = [&](int row, int colF, int colC) {
       return fmaf(beta, S.po[row][colF], fastZ<PC>(tab, S.code[row][colC], S.r[row][colF]));
@@ -682,7 +685,7 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
       const int row = ty + 1 + j * CTY, ir = ty + j * CTY;
       float above = ok ? A.p[row][tx + HXF] : 0.f;
       if (in[j] && ok) {
-        Code k = S.code[ir][tx];
+        CgCode k = S.code[ir][tx];
         float rv = S.r[ir][tx];
         if (!skip) {
           float q = fastRow(tab, k, sx, sy, sz, cur[j], S.p[row][tx + HXF - 1], S.p[row][tx + HXF + 1],
@@ -756,12 +759,12 @@ cudaError_t makeHaloMap(const Dim3i& cg, const float* v, CUtensorMap* m) {
   return encodeMap(m, v, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cg, FW, FH);
 }
 
-cudaError_t makeCgMaps(const Dim3i& cg, const Code* code, const float* r, const void* x, bool xDouble,
+cudaError_t makeCgMaps(const Dim3i& cg, const CgCode* code, const float* r, const void* x, bool xDouble,
                        const float* p0, const float* p1, CgMaps* m) {
   if (cg.x % 8 != 0) return cudaErrorInvalidValue;  // rows must start on 16-byte boundaries
   cudaError_t e;
-  if ((e = encodeMap(&m->codeH, code, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, cg, CW, FH)) != cudaSuccess) return e;
-  if ((e = encodeMap(&m->codeI, code, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, cg, CTX, CTR)) != cudaSuccess) return e;
+  if ((e = encodeMap(&m->codeH, code, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, cg, CW, FH)) != cudaSuccess) return e;
+  if ((e = encodeMap(&m->codeI, code, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, cg, CTX, CTR)) != cudaSuccess) return e;
   if ((e = encodeMap(&m->rH, r, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cg, FW, FH)) != cudaSuccess) return e;
   if ((e = encodeMap(&m->rI, r, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cg, CTX, CTR)) != cudaSuccess) return e;
   if ((e = encodeMap(&m->xI, x, xDouble ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
@@ -796,7 +799,7 @@ int cgPartialsNeeded(const Dim3i& r) {
 }
 
 cudaError_t launchCgDirection(const Dim3i& cg, float sx, float sy, float sz, const CUtensorMap& mZ,
-                              const CUtensorMap& mPo, const CUtensorMap& mCode, const Code* code, const float* zr,
+                              const CUtensorMap& mPo, const CUtensorMap& mCode, const CgCode* code, const float* zr,
                               const float* pOld, float* pNew, double* partials, CgState* st, int precond,
                               cudaStream_t s) {
   switch (precond) {

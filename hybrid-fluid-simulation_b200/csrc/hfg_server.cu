@@ -54,12 +54,12 @@ long long sceneBytes(const int res[3], long long particles, int boundaries, int 
   const long long nx = res[0], ny = res[1], nz = res[2];
   const long long N = nx * ny * nz;
   const long long F = (nx + 1) * ny * nz + nx * (ny + 1) * nz + nx * ny * (nz + 1);
-  const long long NC = ((nx + 7) & ~7LL) * ny * nz;
+  const long long NC = ((nx + 15) & ~15LL) * ny * nz;
   long long b = 0;
   b += F * 4 * 3;              // velocity x2 + previous
   b += N * 4 * (6 + 2);        // colour x2 x3, domain x2
   b += N * 2;                  // markers, solid index
-  b += NC * (2 + 4 * 4);       // code, x, r, p x2
+  b += NC * (2 + 1 + 4 * 4);   // code, CG code, x, r, p x2
   b += F * 8 + N * 8;          // P2G accumulators (faces, cells)
   b += ((nx + 2) * (ny + 1) * nz + (nx + 1) * (ny + 2) * nz + (nx + 1) * (ny + 1) * (nz + 1)) * 16;  // corner tables
   b += F * (2 + 4);            // extrapolation distance + list

@@ -54,7 +54,7 @@ Multigrid* mgCreate(const Dim3i& cg, int levels, int smooth, bool half, cudaStre
 void mgDestroy(Multigrid* m);
 void mgSetup(Multigrid* m, const Dim3i& r, const uint8_t* mk0, const Code* code, float sx, float sy, float sz,
              cudaStream_t s, long long& launches);
-void mgRunCg(Multigrid* m, const Dim3i& cg, float sx, float sy, float sz, const CgMaps& maps, const Code* code, void* x,
+void mgRunCg(Multigrid* m, const Dim3i& cg, float sx, float sy, float sz, const CgMaps& maps, const CgCode* code, void* x,
              bool xDouble, float* rvec, CgState* st, CgState* stHost, cudaStream_t s, long long& launches,
              const std::function<cudaGraphExec_t(const std::function<void()>&)>& capture, cudaGraphExec_t* chunk);
 
@@ -83,13 +83,13 @@ GridSolver::GridSolver(float dt, Dim3i res, const float origin[3], const float s
   for (int a = 0; a < 3; ++a) prev_[a].alloc(F_[a], stream_);
   cg_ = cgDims(res);
   NC_ = cg_.size();
-  solidIdx_.alloc(N_, stream_); markers_.alloc(N_, stream_); code_.alloc(NC_, stream_);
+  solidIdx_.alloc(N_, stream_); markers_.alloc(N_, stream_); code_.alloc(NC_, stream_); cgc_.alloc(NC_, stream_);
   cgx_.alloc(NC_, stream_);
   cgr_.alloc(NC_, stream_);
   cgp_[0].alloc(NC_, stream_);
   cgp_[1].alloc(NC_, stream_);
   partials_.alloc(cgPartialsNeeded(res), stream_);
-  check(makeCgMaps(cg_, code_.p, cgr_.p, cgx_.p, false, cgp_[0].p, cgp_[1].p, &maps_), "CG tensor maps");
+  check(makeCgMaps(cg_, cgc_.p, cgr_.p, cgx_.p, false, cgp_[0].p, cgp_[1].p, &maps_), "CG tensor maps");
   cgState_.alloc(1, stream_);
   subState_.alloc(subSlots_ + 1, stream_);
   dist_.alloc(Ftot_, stream_); list_.alloc(Ftot_, stream_);
@@ -293,7 +293,7 @@ void GridSolver::setOptions(const hfg_options_t& o) {
       cgx64_.alloc(NC_, stream_);
       check(cudaMemsetAsync(cgx64_.p, 0, cgx64_.bytes(), stream_), "memset");
     }
-    check(makeCgMaps(cg_, code_.p, cgr_.p, xPtr(), xDouble(), cgp_[0].p, cgp_[1].p, &maps_), "CG tensor maps");
+    check(makeCgMaps(cg_, cgc_.p, cgr_.p, xPtr(), xDouble(), cgp_[0].p, cgp_[1].p, &maps_), "CG tensor maps");
   }
   if (mgChanged) {
     dropGraphs();
@@ -442,7 +442,7 @@ void GridSolver::computeAdvection() {
 
 void GridSolver::cgIteration(int it, float sx, float sy, float sz, int pc) {
   const int po = it & 1, pn = (it + 1) & 1;
-  launched(launchCgDirection(cg_, sx, sy, sz, maps_.rH, maps_.pH[po], maps_.codeH, code_.p, cgr_.p, cgp_[po].p,
+  launched(launchCgDirection(cg_, sx, sy, sz, maps_.rH, maps_.pH[po], maps_.codeH, cgc_.p, cgr_.p, cgp_[po].p,
                              cgp_[pn].p, partials_.p, cgState_.p, pc, stream_),
            "cg direction");
   launched(launchCgUpdate(cg_, sx, sy, sz, maps_.pH[pn], maps_.rI, maps_.xI, maps_.codeI, cgp_[pn].p, xPtr(), xDouble(),
@@ -485,7 +485,7 @@ void GridSolver::runCg() {
   const float sx = dt_ / (1.0f * g_.hx * g_.hx), sy = dt_ / (1.0f * g_.hy * g_.hy), sz = dt_ / (1.0f * g_.hz * g_.hz);
   if (opt_.precond == HFG_PRECOND_MG) {
     auto cap = [this](const std::function<void()>& f) { return capture(f); };
-    mgRunCg(mg_, cg_, sx, sy, sz, maps_, code_.p, xPtr(), xDouble(), cgr_.p, cgState_.p, cgHost_, stream_, launches_, cap,
+    mgRunCg(mg_, cg_, sx, sy, sz, maps_, cgc_.p, xPtr(), xDouble(), cgr_.p, cgState_.p, cgHost_, stream_, launches_, cap,
             &cgGraph_[2]);
   } else {
     const int pc = opt_.precond == HFG_PRECOND_JACOBI ? 1 : 0;
@@ -515,7 +515,7 @@ void GridSolver::computePressure() {
     launched(launchMarkersInit(N_, solidIdx_.p, markers_.p, stream_), "markers");
     launched(launchMarkersFromParticles(g_, ppos_.p, P_, markers_.p, stream_), "markers");
   }
-  launched(launchStencilCode(g_.r, cg_.x, markers_.p, code_.p, stream_), "stencil code");
+  launched(launchStencilCode(g_.r, cg_.x, markers_.p, code_.p, stream_, cgc_.p), "stencil code");
   stageEnd(3);
   stageBegin(4);
   CgState init{};

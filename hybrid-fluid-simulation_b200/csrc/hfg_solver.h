@@ -174,6 +174,7 @@ class GridSolver {
   DArray<float> vel_[2][3], prev_[3], color_[2][3], dom_[2], solidVel_[3];
   DArray<uint8_t> solidIdx_, markers_;
   DArray<Code> code_;
+  DArray<CgCode> cgc_;
   Dim3i cg_;       // pitched grid of the pressure system
   long long NC_ = 0;
   CgMaps maps_;
