@@ -35,7 +35,7 @@ PKG = os.path.join(ROOT, "hybrid-fluid-simulation_b200")
 sys.path.insert(0, PKG)
 
 METRIC = "Mcell-steps/s at 256^3 (dam break, plain FP32 path)"
-CG_DRAM_BYTES_PER_CELL = (116.89e6 + 21.82e6 + 157.75e6 + 45.34e6) / 224 ** 3
+CG_DRAM_BYTES_PER_CELL = (107.12e6 + 18.07e6 + 146.51e6 + 38.64e6) / 224 ** 3
 UNIT = "Mcell-steps/s"
 
 
