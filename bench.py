@@ -421,6 +421,14 @@ def main():
     # back-to-back on the last system
     cg_ms = s.time_cg(40)
 
+    # per-stage device times of one more step (CUDA events around each stage;
+    # outside the timed region)
+    s.enable_timing(True)
+    s.update()
+    stage_ms = dict(zip(("boundaries", "advection", "forces", "markers", "rhs", "cg", "gradient", "extrapolation"),
+                        (round(float(v), 3) for v in s.stats()["stage_ms"])))
+    s.enable_timing(False)
+
     def max_over_ranks(v):
         if pg is None:
             return v
@@ -457,7 +465,8 @@ def main():
                                    f"{args.precond}-PCG rel 1e-6 max 200", "res": [args.res] * 3,
                        "cells": N, "particles": s.num_particles, "l2": "state > L2 (no flush needed)",
                        "parallelism": f"replicas x{world}", "cg_iterations_last": st["cg_iterations"],
-                       "substeps_last": st["substeps"], "extrapolation_layers_last": st["extrapolation_layers"]},
+                       "substeps_last": st["substeps"], "extrapolation_layers_last": st["extrapolation_layers"],
+                       "stage_ms_one_more_step": stage_ms},
             "roofline": {"bound": "hbm", "kernel": "CG iteration (kCgDirection + kCgUpdate)",
                          "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": traffic, "traffic_source": "ncu dram__bytes_read+write at 224^3, per cell, "

@@ -575,18 +575,21 @@ int extrapolateGrids(int ngrids, const Dim3i* rc, float* const* vals, int layers
   for (int a = 0; a < ngrids; ++a) { off[a] = total; total += rc[a].size(); r3[a] = rc[a]; v3[a] = vals[a]; }
   for (int a = ngrids; a < 3; ++a) { off[a] = total; r3[a] = Dim3i{1, 1, 0}; }
   Scratch<uint16_t> dist(total, s);
-  Scratch<unsigned int> list(total, s), hist(kMaxLayers + 2, s), offs(kMaxLayers + 2, s), cur(kMaxLayers + 2, s);
+  Scratch<unsigned int> list(total, s), hist(kExtrapHistWords, s), offs(kMaxLayers + 2, s), cur(kMaxLayers + 2, s);
   ExtrapScratch sc{dist.p, list.p, hist.p, offs.p, cur.p};
   if (layers > kMaxLayers) layers = kMaxLayers;
   if (layers <= 1) return HFG_OK;
   // grids with zero size contribute nothing
   check(launchExtrapDistance(r3, v3, off, layers, sc, s), "extrapolation distance");
-  std::vector<unsigned int> h(kMaxLayers + 2);
-  check(cudaMemcpyAsync(h.data(), offs.p, sizeof(unsigned int) * (kMaxLayers + 2), cudaMemcpyDeviceToHost, s), "read");
+  struct User {
+    User() { extrapUsers(+1); }
+    ~User() { extrapUsers(-1); }
+  } user;
+  check(launchExtrapLayers(r3, v3, off, sc, layers, s, nullptr), "extrapolation layers");
+  unsigned int words[4] = {0, 0, 0, 0};
+  check(cudaMemcpyAsync(words, extrapBarWords(sc), sizeof(words), cudaMemcpyDeviceToHost, s), "read");
   check(cudaStreamSynchronize(s), "sync");
-  int depth = 0;
-  check(launchExtrapLayers(r3, v3, off, sc, h.data(), layers, s, &depth, nullptr), "extrapolation layers");
-  check(cudaStreamSynchronize(s), "sync");
+  if (words[2] != 0u) return fail(HFG_ERR_TIMEOUT, "extrapolation: a grid barrier timed out");
   return HFG_OK;
 }
 }  // namespace

@@ -175,26 +175,22 @@ struct FaceSampler {
     for (int k = 0; k < 8; ++k) v = fmaf(w[k], __ldg(f + idx[k]), v);
     return v;
   }
-  // the same sample from the corner table of the component: two 16-byte
-  // loads instead of eight 4-byte ones, same values and the same FMA chain
+  // the same trilinear sample from the corner table of the component: two
+  // 16-byte loads instead of eight 4-byte ones, reduced by lerps along x,
+  // then y, then z (seven FMAs; rounding differs from the weighted sum in the
+  // last bits, and equal corners return their value exactly)
   __device__ __forceinline__ float sampleQuads(const Geom& g, int a, const float4* __restrict__ Q) const {
     const AxisW& X = a == 0 ? fc[0] : cc[0];
     const AxisW& Y = a == 1 ? fc[1] : cc[1];
     const AxisW& Z = a == 2 ? fc[2] : cc[2];
     unsigned lx = (unsigned)(g.r.x + (a == 0) + 1), ly = (unsigned)(g.r.y + (a == 1) + 1);
     unsigned row = (unsigned)Y.j * lx + (unsigned)X.j, pl = lx * ly;
-    float4 q0 = __ldg(Q + (unsigned)Z.i0 * pl + row), q1 = __ldg(Q + (unsigned)Z.i1 * pl + row);
-    float x0 = 1.f - X.w1, x1 = X.w1, y0 = 1.f - Y.w1, y1 = Y.w1, z0 = 1.f - Z.w1, z1 = Z.w1;
-    float v = 0.f;
-    v = fmaf(x0 * y0 * z0, q0.x, v);
-    v = fmaf(x1 * y0 * z0, q0.y, v);
-    v = fmaf(x0 * y1 * z0, q0.z, v);
-    v = fmaf(x1 * y1 * z0, q0.w, v);
-    v = fmaf(x0 * y0 * z1, q1.x, v);
-    v = fmaf(x1 * y0 * z1, q1.y, v);
-    v = fmaf(x0 * y1 * z1, q1.z, v);
-    v = fmaf(x1 * y1 * z1, q1.w, v);
-    return v;
+    const float4 q0 = __ldg(Q + (unsigned)Z.i0 * pl + row), q1 = __ldg(Q + (unsigned)Z.i1 * pl + row);
+    const float wx = X.w1, wy = Y.w1, wz = Z.w1;
+    const float a00 = fmaf(wx, q0.y - q0.x, q0.x), a01 = fmaf(wx, q0.w - q0.z, q0.z);
+    const float a10 = fmaf(wx, q1.y - q1.x, q1.x), a11 = fmaf(wx, q1.w - q1.z, q1.z);
+    const float b0 = fmaf(wy, a01 - a00, a00), b1 = fmaf(wy, a11 - a10, a10);
+    return fmaf(wz, b1 - b0, b0);
   }
   // sample of the difference field f - h at the same point
   __device__ __forceinline__ float sampleDiff(const Geom& g, int a, const float* __restrict__ f,

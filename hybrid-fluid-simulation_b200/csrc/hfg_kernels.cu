@@ -6,6 +6,7 @@
 // markers, FP64 deterministic reductions and device-resident solver scalars.
 // The reference line each kernel follows is cited beside it.
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 
 #include "hfg_kernels.h"
@@ -456,7 +457,7 @@ cudaError_t launchExtrapDistance(const Dim3i rc[3], float* const vals[3], long l
     kDistCols<<<gridFor((long long)rc[a].x * rc[a].z), kThreads, 0, s>>>(rc[a], 1, d);
     kDistCols<<<gridFor((long long)rc[a].x * rc[a].y), kThreads, 0, s>>>(rc[a], 2, d);
   }
-  cudaError_t e = cudaMemsetAsync(sc.hist, 0, sizeof(unsigned int) * (kMaxLayers + 2), s);
+  cudaError_t e = cudaMemsetAsync(sc.hist, 0, sizeof(unsigned int) * kExtrapHistWords, s);
   if (e != cudaSuccess) return e;
   for (int a = 0; a < 3; ++a) {
     long long n = rc[a].size();
@@ -474,6 +475,8 @@ cudaError_t launchExtrapDistance(const Dim3i rc[3], float* const vals[3], long l
 
 // One entry of layer d: mean of the neighbours with a smaller layer, summed in
 // the fixed order left, right, down, up, back, front (extrapolatingData).
+// The values of earlier layers were written by other blocks of the same
+// launch, so they are read from L2 (ld.cg), never from a stale L1 line.
 // 32-bit index arithmetic: every face grid holds fewer than 2^31 entries.
 __device__ __forceinline__ void extrapEntry(const Dim3i& r0, const Dim3i& r1, const Dim3i& r2, float* v0, float* v1,
                                             float* v2, unsigned off1, unsigned off2, const uint16_t* __restrict__ dist,
@@ -492,8 +495,8 @@ __device__ __forceinline__ void extrapEntry(const Dim3i& r0, const Dim3i& r1, co
   float acc = 0.f, cnt = 0.f;
 #pragma unroll
   for (int q = 0; q < 6; ++q) {
-    if ((int)dd[nb[q]] < d) {
-      acc = __fadd_rn(acc, v[nb[q]]);
+    if ((int)__ldg(dd + nb[q]) < d) {
+      acc = __fadd_rn(acc, __ldcg(v + nb[q]));
       cnt = __fadd_rn(cnt, 1.f);
     }
   }
@@ -501,74 +504,128 @@ __device__ __forceinline__ void extrapEntry(const Dim3i& r0, const Dim3i& r1, co
   v[i] = acc;
 }
 
-__global__ void kExtrapLayer(Dim3i r0, Dim3i r1, Dim3i r2, float* v0, float* v1, float* v2, unsigned off1,
-                             unsigned off2, const uint16_t* __restrict__ dist, const unsigned int* __restrict__ list,
-                             unsigned int begin, unsigned int count, int d) {
-  HFG_FOR(k, (long long)count) extrapEntry(r0, r1, r2, v0, v1, v2, off1, off2, dist, list[begin + k], d);
+__device__ __forceinline__ unsigned long long globalNs() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ unsigned ldAcquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
 }
 
-// A run of small consecutive layers [dFirst, dLast] in one block: the block
-// barrier between layers orders layer d's writes before layer d+1's reads.
-__global__ void __launch_bounds__(1024) kExtrapLayerRun(Dim3i r0, Dim3i r1, Dim3i r2, float* v0, float* v1, float* v2,
-                                                        unsigned off1, unsigned off2,
-                                                        const uint16_t* __restrict__ dist,
-                                                        const unsigned int* __restrict__ list,
-                                                        const unsigned int* __restrict__ offsets, int dFirst,
-                                                        int dLast) {
-  for (int d = dFirst; d <= dLast; ++d) {
-    const unsigned b = offsets[d], e = offsets[d + 1];
-    for (unsigned k = b + threadIdx.x; k < e; k += blockDim.x)
-      extrapEntry(r0, r1, r2, v0, v1, v2, off1, off2, dist, list[k], d);
-    __syncthreads();
+// Grid barrier of a cooperative launch (generation counting).  The wait is
+// bounded: past the deadline, or once another block has given up, the error
+// word is set and false returned, and the caller stops.
+__device__ bool gridBarrier(unsigned* count, unsigned* gen, unsigned* err, unsigned nblocks) {
+  __shared__ int okS;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned g = ldAcquire(gen);
+    __threadfence();  // this block's layer writes before its arrival
+    if (atomicAdd(count, 1u) == nblocks - 1) {
+      atomicExch(count, 0u);
+      __threadfence();
+      atomicAdd(gen, 1u);
+    } else {
+      const unsigned long long deadline = globalNs() + 1000000000ull;  // 1 s
+      while (ldAcquire(gen) == g) {
+        if (ldAcquire(err) != 0u || globalNs() > deadline) {
+          atomicExch(err, 1u);
+          ok = 0;
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+    okS = ok;
   }
+  __syncthreads();
+  return okS != 0;
 }
 
-cudaError_t launchExtrapLayer(const Dim3i rc[3], float* const vals[3], const long long off[3], ExtrapScratch sc,
-                              unsigned int begin, unsigned int count, int d, cudaStream_t s) {
-  if (count == 0) return cudaSuccess;
-  kExtrapLayer<<<gridFor(count), kThreads, 0, s>>>(rc[0], rc[1], rc[2], vals[0], vals[1], vals[2],
-                                                    (unsigned)off[1], (unsigned)off[2], sc.dist, sc.list, begin,
-                                                    count, d);
-  return cudaGetLastError();
-}
-
-// Layers 1 .. nums-1 from the host copy of the layer offsets: a layer larger
-// than kExtrapSmallLayer gets a grid-wide launch, runs of smaller consecutive
-// layers share one single-block launch.  Stops at the first empty layer.
-cudaError_t launchExtrapLayers(const Dim3i rc[3], float* const vals[3], const long long off[3], ExtrapScratch sc,
-                               const unsigned int* hostOffsets, int nums, cudaStream_t s, int* depth,
-                               long long* launches) {
+// Layers 1 .. nums-1, persistent: a layer with more than kExtrapSmallLayer
+// faces is spread over the grid; a run of smaller consecutive layers is filled
+// by block 0 alone with block barriers between them.  Every block walks the
+// same layer bounds (sc.offsets), so all meet at the same grid barriers.
+// barWords: count, generation, error, deepest layer filled.
+__global__ void __launch_bounds__(256) kExtrapLayers(Dim3i r0, Dim3i r1, Dim3i r2, float* v0, float* v1, float* v2,
+                                                     unsigned off1, unsigned off2, const uint16_t* __restrict__ dist,
+                                                     const unsigned int* __restrict__ list,
+                                                     const unsigned int* __restrict__ offsets, int nums,
+                                                     unsigned* barWords) {
+  unsigned* count = barWords;
+  unsigned* gen = barWords + 1;
+  unsigned* err = barWords + 2;
+  const unsigned stride = gridDim.x * blockDim.x, gtid = blockIdx.x * blockDim.x + threadIdx.x;
   int d = 1;
-  *depth = 0;
   while (d < nums && d <= kMaxLayers) {
-    unsigned int b = hostOffsets[d], e = hostOffsets[d + 1];
+    if (blockIdx.x == 0 && threadIdx.x == 0) barWords[3] = (unsigned)(d - 1);
+    const unsigned b = __ldg(offsets + d), e = __ldg(offsets + d + 1);
     if (e <= b) break;
-    cudaError_t err;
     if (e - b > kExtrapSmallLayer) {
-      err = launchExtrapLayer(rc, vals, off, sc, b, e - b, d, s);
-      *depth = d++;
+      for (unsigned k = b + gtid; k < e; k += stride) extrapEntry(r0, r1, r2, v0, v1, v2, off1, off2, dist, list[k], d);
+      ++d;
     } else {
       int last = d;
       while (last + 1 < nums && last + 1 <= kMaxLayers) {
-        unsigned int nb = hostOffsets[last + 1], ne = hostOffsets[last + 2];
+        const unsigned nb = __ldg(offsets + last + 1), ne = __ldg(offsets + last + 2);
         if (ne <= nb || ne - nb > kExtrapSmallLayer) break;
         ++last;
       }
-      err = launchExtrapLayerRun(rc, vals, off, sc, d, last, s);
-      *depth = last;
+      if (blockIdx.x == 0) {
+        for (int l = d; l <= last; ++l) {
+          const unsigned lb = __ldg(offsets + l), le = __ldg(offsets + l + 1);
+          for (unsigned k = lb + threadIdx.x; k < le; k += blockDim.x)
+            extrapEntry(r0, r1, r2, v0, v1, v2, off1, off2, dist, list[k], l);
+          __syncthreads();
+        }
+      }
       d = last + 1;
     }
-    if (err != cudaSuccess) return err;
-    if (launches) ++*launches;
+    if (gridDim.x > 1 && !gridBarrier(count, gen, err, gridDim.x)) return;
   }
-  return cudaSuccess;
+  if (blockIdx.x == 0 && threadIdx.x == 0) barWords[3] = (unsigned)(d - 1);
 }
 
-cudaError_t launchExtrapLayerRun(const Dim3i rc[3], float* const vals[3], const long long off[3], ExtrapScratch sc,
-                                 int dFirst, int dLast, cudaStream_t s) {
-  kExtrapLayerRun<<<1, 1024, 0, s>>>(rc[0], rc[1], rc[2], vals[0], vals[1], vals[2], (unsigned)off[1],
-                                     (unsigned)off[2], sc.dist, sc.list, sc.offsets, dFirst, dLast);
-  return cudaGetLastError();
+namespace {
+std::atomic<int> g_extrapUsers{0};
+}
+void extrapUsers(int delta) { g_extrapUsers.fetch_add(delta); }
+
+// Layers 1 .. nums-1 in one cooperative launch: about one block per 8192
+// faces of the grids, at most two per SM, and at most an equal share of the
+// GPU's resident slots for this kernel among the registered users, so that the
+// grids of concurrent scenes always fit on the GPU together.
+cudaError_t launchExtrapLayers(const Dim3i rc[3], float* const vals[3], const long long off[3], ExtrapScratch sc,
+                               int nums, cudaStream_t s, long long* launches) {
+  if (nums <= 1) return cudaSuccess;
+  static std::atomic<int> perSM{0};
+  if (perSM.load() == 0) {
+    int v = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kExtrapLayers, kThreads, 0);
+    if (e != cudaSuccess) return e;
+    perSM.store(std::max(1, v));
+  }
+  const long long slots = (long long)numSMs() * perSM.load();
+  const long long share = std::max(1LL, slots / std::max(1, g_extrapUsers.load()));
+  const long long faces = rc[0].size() + rc[1].size() + rc[2].size();
+  const int blocks = (int)std::max(
+      1LL, std::min({(faces + 8191) / 8192, (long long)numSMs() * std::min(perSM.load(), 2), share}));
+  Dim3i r0 = rc[0], r1 = rc[1], r2 = rc[2];
+  float *v0 = vals[0], *v1 = vals[1], *v2 = vals[2];
+  unsigned o1 = (unsigned)off[1], o2 = (unsigned)off[2];
+  const uint16_t* dist = sc.dist;
+  const unsigned int* list = sc.list;
+  const unsigned int* offs = sc.offsets;
+  unsigned* bar = extrapBarWords(sc);
+  void* args[] = {&r0, &r1, &r2, &v0, &v1, &v2, &o1, &o2, &dist, &list, &offs, &nums, &bar};
+  cudaError_t e = cudaLaunchCooperativeKernel((const void*)kExtrapLayers, dim3(blocks), dim3(kThreads), args, 0, s);
+  if (e == cudaSuccess && launches) ++*launches;
+  return e;
 }
 
 // ===========================================================================

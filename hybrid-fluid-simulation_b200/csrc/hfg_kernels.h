@@ -156,25 +156,29 @@ int cgPartialsNeeded(const Dim3i& r);
 struct ExtrapScratch {
   uint16_t* dist;          // total faces
   unsigned int* list;      // total faces
-  unsigned int* hist;      // kMaxLayers + 2
+  unsigned int* hist;      // kExtrapHistWords: the layer histogram, then the grid-barrier words
   unsigned int* offsets;   // kMaxLayers + 2
   unsigned int* cursor;    // kMaxLayers + 2
 };
 constexpr int kMaxLayers = 1000;
+// hist[0 .. kMaxLayers + 1] is the histogram; hist[kMaxLayers + 2 ..] the
+// barrier count, generation and error word of the layer kernel
+constexpr int kExtrapHistWords = kMaxLayers + 2 + 4;
 cudaError_t launchExtrapDistance(const Dim3i rc[3], float* const vals[3], long long off[3], int nums,
                                  ExtrapScratch sc, cudaStream_t s);
-cudaError_t launchExtrapLayer(const Dim3i rc[3], float* const vals[3], const long long off[3], ExtrapScratch sc,
-                              unsigned int begin, unsigned int count, int d, cudaStream_t s);
-// layers dFirst..dLast (each small) in one single-block launch; the layer
-// bounds come from sc.offsets on the device
+// a layer of at most this many faces is filled by one block (runs of such
+// layers without grid barriers between them)
 constexpr unsigned kExtrapSmallLayer = 4096;
-cudaError_t launchExtrapLayerRun(const Dim3i rc[3], float* const vals[3], const long long off[3], ExtrapScratch sc,
-                                 int dFirst, int dLast, cudaStream_t s);
-// every layer 1 .. nums-1 (host copy of the offsets), large layers one launch
-// each, runs of small ones together; *depth = deepest layer filled
+// Every layer 1 .. nums-1 in one cooperative launch, with a grid barrier
+// between layers.  The barrier waits are bounded.  Afterwards the four words
+// at extrapBarWords() hold: count, generation, error (nonzero: a barrier timed
+// out and the layers are incomplete), deepest layer filled.
 cudaError_t launchExtrapLayers(const Dim3i rc[3], float* const vals[3], const long long off[3], ExtrapScratch sc,
-                               const unsigned int* hostOffsets, int nums, cudaStream_t s, int* depth,
-                               long long* launches);
+                               int nums, cudaStream_t s, long long* launches);
+inline unsigned int* extrapBarWords(const ExtrapScratch& sc) { return sc.hist + kMaxLayers + 2; }
+// Registers (+1) or drops (-1) a user of launchExtrapLayers (a solver, an
+// operator call); the launch sizes its grid to a share of the GPU per user.
+void extrapUsers(int delta);
 
 // ---- fluid SDF (buildFluidSDF); frontier buffers hold N cells each; counts 2;
 // hostCount pinned.  Blocks (one host read per layer).

@@ -93,12 +93,12 @@ GridSolver::GridSolver(float dt, Dim3i res, const float origin[3], const float s
   cgState_.alloc(1, stream_);
   subState_.alloc(subSlots_ + 1, stream_);
   dist_.alloc(Ftot_, stream_); list_.alloc(Ftot_, stream_);
-  hist_.alloc(kMaxLayers + 2, stream_);
+  hist_.alloc(kExtrapHistWords, stream_);
   offsets_.alloc(kMaxLayers + 2, stream_);
   cursor_.alloc(kMaxLayers + 2, stream_);
   cgHost_ = (CgState*)pinnedGet(sizeof(CgState));
   subHost_ = (SubstepState*)pinnedGet(sizeof(SubstepState));
-  offHost_ = (unsigned int*)pinnedGet(sizeof(unsigned int) * (kMaxLayers + 2));
+  extrapHost_ = (unsigned int*)pinnedGet(sizeof(unsigned int) * 4);
   // GridFluidSolver.cpp:179-195: every field starts at zero
   for (int b = 0; b < 2; ++b) {
     for (int a = 0; a < 3; ++a) {
@@ -114,16 +114,18 @@ GridSolver::GridSolver(float dt, Dim3i res, const float origin[3], const float s
   check(cudaMemsetAsync(cgState_.p, 0, sizeof(CgState), stream_), "memset");
   for (int i = 0; i < 16; ++i) check(cudaEventCreate(&ev_[i]), "cudaEventCreate");
   check(cudaStreamSynchronize(stream_), "sync");
+  extrapUsers(+1);  // last: a constructor that throws registers nothing
 }
 
 GridSolver::~GridSolver() {
   if (stream_) cudaStreamSynchronize(stream_);
+  extrapUsers(-1);
   for (auto* b : bsdf_) delete b;
   dropGraphs();
   if (mg_) mgDestroy(mg_);
   pinnedPut(cgHost_);
   pinnedPut(subHost_);
-  pinnedPut(offHost_);
+  pinnedPut(extrapHost_);
   for (int i = 0; i < 16; ++i)
     if (ev_[i]) cudaEventDestroy(ev_[i]);
   // the stream itself goes with own_, after the member arrays are freed on it
@@ -577,12 +579,12 @@ void GridSolver::extrapolate() {
     long long off[3] = {0, F_[0], F_[0] + F_[1]};
     ExtrapScratch sc{dist_.p, list_.p, hist_.p, offsets_.p, cursor_.p};
     launched(launchExtrapDistance(fr_, vals, off, nums, sc, stream_), "extrapolation distance", 17);
-    check(cudaMemcpyAsync(offHost_, offsets_.p, sizeof(unsigned int) * (kMaxLayers + 2), cudaMemcpyDeviceToHost,
-                          stream_),
-          "read layer offsets");
+    check(launchExtrapLayers(fr_, vals, off, sc, nums, stream_, &launches_), "extrapolation layers");
+    check(cudaMemcpyAsync(extrapHost_, extrapBarWords(sc), sizeof(unsigned int) * 4, cudaMemcpyDeviceToHost, stream_),
+          "read extrapolation state");
     check(cudaStreamSynchronize(stream_), "extrapolation sync");
-    check(launchExtrapLayers(fr_, vals, off, sc, offHost_, nums, stream_, &extrapDepth_, &launches_),
-          "extrapolation layers");
+    if (extrapHost_[2] != 0u) throw CudaError("extrapolation: a grid barrier timed out", HFG_ERR_TIMEOUT);
+    extrapDepth_ = (int)extrapHost_[3];
   }
   stageEnd(7);
 }

@@ -192,7 +192,7 @@ class GridSolver {
   DArray<float4> quads_[3];  // corner tables of the advecting velocity (particle substeps)
   DArray<uint16_t> dist_;
   DArray<unsigned int> list_, hist_, offsets_, cursor_;
-  unsigned int* offHost_ = nullptr;  // pinned
+  unsigned int* extrapHost_ = nullptr;  // pinned
 
   long long P_ = 0;
   DArray<float> ppos_, pvel_, pv0_, pscalar_, pvector_;
