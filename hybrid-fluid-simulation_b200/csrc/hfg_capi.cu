@@ -576,7 +576,8 @@ int extrapolateGrids(int ngrids, const Dim3i* rc, float* const* vals, int layers
   for (int a = ngrids; a < 3; ++a) { off[a] = total; r3[a] = Dim3i{1, 1, 0}; }
   Scratch<uint16_t> dist(total, s);
   Scratch<unsigned int> list(total, s), hist(kExtrapHistWords, s), offs(kMaxLayers + 2, s), cur(kMaxLayers + 2, s);
-  ExtrapScratch sc{dist.p, list.p, hist.p, offs.p, cur.p};
+  Scratch<uint8_t> mask(total, s);
+  ExtrapScratch sc{dist.p, list.p, hist.p, offs.p, cur.p, mask.p};
   if (layers > kMaxLayers) layers = kMaxLayers;
   if (layers <= 1) return HFG_OK;
   // grids with zero size contribute nothing

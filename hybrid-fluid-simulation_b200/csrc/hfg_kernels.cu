@@ -416,12 +416,29 @@ __global__ void kExclusiveScanSmall(const unsigned int* __restrict__ hist, unsig
   }
 }
 
+// Neighbours of entry i of grid r in the order left, right, down, up, back,
+// front, clamped to the grid (an edge entry is its own neighbour there).
+__device__ __forceinline__ void extrapNeighbours(const Dim3i& r, unsigned i, unsigned nb[6]) {
+  const unsigned nx = (unsigned)r.x, ny = (unsigned)r.y, t = i / nx;
+  const int x = (int)(i - t * nx), y = (int)(t % ny), z = (int)(t / ny);
+  const unsigned plane = nx * ny;
+  nb[0] = x > 0 ? i - 1 : i;
+  nb[1] = x + 1 < r.x ? i + 1 : i;
+  nb[2] = y > 0 ? i - nx : i;
+  nb[3] = y + 1 < r.y ? i + nx : i;
+  nb[4] = z > 0 ? i - plane : i;
+  nb[5] = z + 1 < r.z ? i + plane : i;
+}
+
 // Bucket the entries by layer: a block counts its chunk per layer in shared
 // memory, reserves one global range per (block, layer) and hands out slots
-// with shared-memory atomics.
+// with shared-memory atomics.  Each entry also gets the mask of its
+// neighbours in earlier layers, so that the layer pass reads no distances.
 constexpr int kScatterChunk = 4096;
-__global__ void kDistScatter(long long n, long long base, const uint16_t* __restrict__ d, int nums,
-                             unsigned int* __restrict__ cursor, unsigned int* __restrict__ list) {
+__global__ void kDistScatter(Dim3i r, long long base, const uint16_t* __restrict__ d, int nums,
+                             unsigned int* __restrict__ cursor, unsigned int* __restrict__ list,
+                             uint8_t* __restrict__ mask) {
+  const long long n = r.size();
   __shared__ unsigned int cnt[kMaxLayers + 1], start[kMaxLayers + 1];
   for (long long c0 = (long long)blockIdx.x * kScatterChunk; c0 < n; c0 += (long long)gridDim.x * kScatterChunk) {
     long long c1 = c0 + kScatterChunk < n ? c0 + kScatterChunk : n;
@@ -440,7 +457,16 @@ __global__ void kDistScatter(long long n, long long base, const uint16_t* __rest
     __syncthreads();
     for (long long i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
       unsigned int v = d[i];
-      if (v >= 1 && (int)v < nums) list[start[v] + atomicAdd(&cnt[v], 1u)] = (unsigned int)(base + i);
+      if (v >= 1 && (int)v < nums) {
+        unsigned nb[6];
+        extrapNeighbours(r, (unsigned)i, nb);
+        unsigned m = 0;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) m |= (unsigned)(d[nb[q]] < v) << q;
+        const unsigned slot = start[v] + atomicAdd(&cnt[v], 1u);
+        list[slot] = (unsigned int)(base + i);
+        mask[slot] = (uint8_t)m;
+      }
     }
     __syncthreads();
   }
@@ -468,34 +494,30 @@ cudaError_t launchExtrapDistance(const Dim3i rc[3], float* const vals[3], long l
     long long n = rc[a].size();
     int blocks = (int)std::min<long long>((n + kScatterChunk - 1) / kScatterChunk, (long long)numSMs() * 8);
     if (blocks < 1) blocks = 1;
-    kDistScatter<<<blocks, kThreads, 0, s>>>(n, off[a], sc.dist + off[a], nums, sc.cursor, sc.list);
+    kDistScatter<<<blocks, kThreads, 0, s>>>(rc[a], off[a], sc.dist + off[a], nums, sc.cursor, sc.list, sc.mask);
   }
   return cudaGetLastError();
 }
 
-// One entry of layer d: mean of the neighbours with a smaller layer, summed in
-// the fixed order left, right, down, up, back, front (extrapolatingData).
+// One entry of layer d: mean of the neighbours with a smaller layer (mask m),
+// summed in the fixed order left, right, down, up, back, front
+// (extrapolatingData).
 // The values of earlier layers were written by other blocks of the same
 // launch, so they are read from L2 (ld.cg), never from a stale L1 line.
 // 32-bit index arithmetic: every face grid holds fewer than 2^31 entries.
 __device__ __forceinline__ void extrapEntry(const Dim3i& r0, const Dim3i& r1, const Dim3i& r2, float* v0, float* v1,
-                                            float* v2, unsigned off1, unsigned off2, const uint16_t* __restrict__ dist,
-                                            unsigned id, int d) {
+                                            float* v2, unsigned off1, unsigned off2, unsigned id, unsigned m) {
   const int a = id >= off2 ? 2 : (id >= off1 ? 1 : 0);
   const unsigned base = a == 2 ? off2 : (a == 1 ? off1 : 0u);
   const unsigned i = id - base;
   const Dim3i r = a == 2 ? r2 : (a == 1 ? r1 : r0);
   float* v = a == 2 ? v2 : (a == 1 ? v1 : v0);
-  const uint16_t* dd = dist + base;
-  const unsigned nx = (unsigned)r.x, ny = (unsigned)r.y, t = i / nx;
-  const int x = (int)(i - t * nx), y = (int)(t % ny), z = (int)(t / ny);
-  const unsigned plane = nx * ny;
-  const unsigned nb[6] = {x > 0 ? i - 1 : i, x + 1 < r.x ? i + 1 : i, y > 0 ? i - nx : i, y + 1 < r.y ? i + nx : i,
-                          z > 0 ? i - plane : i, z + 1 < r.z ? i + plane : i};
+  unsigned nb[6];
+  extrapNeighbours(r, i, nb);
   float acc = 0.f, cnt = 0.f;
 #pragma unroll
   for (int q = 0; q < 6; ++q) {
-    if ((int)__ldg(dd + nb[q]) < d) {
+    if ((m >> q) & 1u) {
       acc = __fadd_rn(acc, __ldcg(v + nb[q]));
       cnt = __fadd_rn(cnt, 1.f);
     }
@@ -553,7 +575,7 @@ __device__ bool gridBarrier(unsigned* count, unsigned* gen, unsigned* err, unsig
 // same layer bounds (sc.offsets), so all meet at the same grid barriers.
 // barWords: count, generation, error, deepest layer filled.
 __global__ void __launch_bounds__(256) kExtrapLayers(Dim3i r0, Dim3i r1, Dim3i r2, float* v0, float* v1, float* v2,
-                                                     unsigned off1, unsigned off2, const uint16_t* __restrict__ dist,
+                                                     unsigned off1, unsigned off2, const uint8_t* __restrict__ mask,
                                                      const unsigned int* __restrict__ list,
                                                      const unsigned int* __restrict__ offsets, int nums,
                                                      unsigned* barWords) {
@@ -567,7 +589,7 @@ __global__ void __launch_bounds__(256) kExtrapLayers(Dim3i r0, Dim3i r1, Dim3i r
     const unsigned b = __ldg(offsets + d), e = __ldg(offsets + d + 1);
     if (e <= b) break;
     if (e - b > kExtrapSmallLayer) {
-      for (unsigned k = b + gtid; k < e; k += stride) extrapEntry(r0, r1, r2, v0, v1, v2, off1, off2, dist, list[k], d);
+      for (unsigned k = b + gtid; k < e; k += stride) extrapEntry(r0, r1, r2, v0, v1, v2, off1, off2, list[k], mask[k]);
       ++d;
     } else {
       int last = d;
@@ -580,7 +602,7 @@ __global__ void __launch_bounds__(256) kExtrapLayers(Dim3i r0, Dim3i r1, Dim3i r
         for (int l = d; l <= last; ++l) {
           const unsigned lb = __ldg(offsets + l), le = __ldg(offsets + l + 1);
           for (unsigned k = lb + threadIdx.x; k < le; k += blockDim.x)
-            extrapEntry(r0, r1, r2, v0, v1, v2, off1, off2, dist, list[k], l);
+            extrapEntry(r0, r1, r2, v0, v1, v2, off1, off2, list[k], mask[k]);
           __syncthreads();
         }
       }
@@ -618,11 +640,11 @@ cudaError_t launchExtrapLayers(const Dim3i rc[3], float* const vals[3], const lo
   Dim3i r0 = rc[0], r1 = rc[1], r2 = rc[2];
   float *v0 = vals[0], *v1 = vals[1], *v2 = vals[2];
   unsigned o1 = (unsigned)off[1], o2 = (unsigned)off[2];
-  const uint16_t* dist = sc.dist;
+  const uint8_t* mask = sc.mask;
   const unsigned int* list = sc.list;
   const unsigned int* offs = sc.offsets;
   unsigned* bar = extrapBarWords(sc);
-  void* args[] = {&r0, &r1, &r2, &v0, &v1, &v2, &o1, &o2, &dist, &list, &offs, &nums, &bar};
+  void* args[] = {&r0, &r1, &r2, &v0, &v1, &v2, &o1, &o2, &mask, &list, &offs, &nums, &bar};
   cudaError_t e = cudaLaunchCooperativeKernel((const void*)kExtrapLayers, dim3(blocks), dim3(kThreads), args, 0, s);
   if (e == cudaSuccess && launches) ++*launches;
   return e;
@@ -921,34 +943,6 @@ cudaError_t launchSeedWrite(const Geom& g, const float* fluidSDF, const uint8_t*
 //   FLIP (FluidImplicitParticle.cpp:107-119): v += G2P(vin - prev)
 //   MIX  (MixPICAndFLIP.cpp:112-129):        v = (1-m)(v + G2P(vin - prev)) + m G2P(vin)
 // with prev = the previous step's P2G output, or prev = 0 on the first FLIP step.
-// LINEAR transfers through the shared per-axis weights (the configuration of
-// every benchmark scene): one sampler per particle serves PIC, the FLIP
-// difference and all three components.
-__global__ void kParticleVelUpdateLinear(Geom g, int mode, ConstFaceField vin, ConstFaceField prev, int first,
-                                         float mixing, const float* __restrict__ pos, float* __restrict__ vel,
-                                         long long P) {
-  const float keep = (float)(1.0 - (double)mixing);
-  HFG_FOR(p, P) {
-    FaceSampler fs(g, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]);
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      float v = vel[3 * p + a];
-      if (mode == MODE_PIC) {
-        v = fs.sample(g, a, vin.c[a]);
-      } else {
-        float pic = (mode == MODE_MIX || first) ? fs.sample(g, a, vin.c[a]) : 0.f;
-        float dv = first ? pic : fs.sampleDiff(g, a, vin.c[a], prev.c[a]);
-        v = __fadd_rn(dv, v);
-        if (mode == MODE_MIX) {
-          v = __fmul_rn(v, keep);
-          v = fmaf(mixing, pic, v);
-        }
-      }
-      vel[3 * p + a] = v;
-    }
-  }
-}
-
 template <int ALG>
 __global__ void kParticleVelUpdate(Geom g, int mode, ConstFaceField vin, ConstFaceField prev, int first, float mixing,
                                    const float* __restrict__ pos, float* __restrict__ vel, long long P) {
@@ -999,13 +993,58 @@ __global__ void kParticleVelUpdate(Geom g, int mode, ConstFaceField vin, ConstFa
   }
 }
 
+__device__ inline void blockMaxToGlobal(float m, unsigned int* dst);
+
+// LINEAR transfers (the configuration of every benchmark scene), fused with the
+// first velocity sample of the substep loop that follows
+// (EulerParticles.cpp:249-251): one sampler per particle serves the PIC sample,
+// the FLIP difference and all three components.  The PIC sample comes from the
+// corner tables of vin and is also v0 of the substeps, with max |v0|.
+__global__ void kParticleVelUpdateLinear(Geom g, int mode, FaceQuads vinQ, ConstFaceField vin, ConstFaceField prev,
+                                         int first, float mixing, const float* __restrict__ pos,
+                                         float* __restrict__ vel, long long P, float* __restrict__ v0,
+                                         SubstepState* st) {
+  const float keep = (float)(1.0 - (double)mixing);
+  float m = 0.f;
+  HFG_FOR(p, P) {
+    FaceSampler fs(g, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]);
+    float pic[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      pic[a] = fs.sampleQuads(g, a, vinQ.c[a]);
+      v0[3 * p + a] = pic[a];
+      m = fmaxf(m, fabsf(pic[a]));
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      float v = vel[3 * p + a];
+      if (mode == MODE_PIC) {
+        v = pic[a];
+      } else {
+        float dv = first ? pic[a] : fs.sampleDiff(g, a, vin.c[a], prev.c[a]);
+        v = __fadd_rn(dv, v);
+        if (mode == MODE_MIX) {
+          v = __fmul_rn(v, keep);
+          v = fmaf(mixing, pic[a], v);
+        }
+      }
+      vel[3 * p + a] = v;
+    }
+  }
+  blockMaxToGlobal(m, &st[0].maxAbsBits);
+}
+
 cudaError_t launchParticleVelUpdate(const Geom& g, int mode, int alg, ConstFaceField vin, ConstFaceField prev,
                                     int firstFlip, float mixing, const float* pos, float* vel, long long P,
-                                    cudaStream_t s) {
+                                    cudaStream_t s, const FaceQuads* vinQ, float* v0, SubstepState* st) {
   if (P <= 0) return cudaSuccess;
   int gr = gridFor(P);
   switch (alg) {
-    case LINEAR: kParticleVelUpdateLinear<<<gr, kThreads, 0, s>>>(g, mode, vin, prev, firstFlip, mixing, pos, vel, P); break;
+    case LINEAR:
+      if (!vinQ || !v0 || !st) return cudaErrorInvalidValue;
+      kParticleVelUpdateLinear<<<gr, kThreads, 0, s>>>(g, mode, *vinQ, vin, prev, firstFlip, mixing, pos, vel, P, v0,
+                                                       st);
+      break;
     case QUADRATIC: kParticleVelUpdate<QUADRATIC><<<gr, kThreads, 0, s>>>(g, mode, vin, prev, firstFlip, mixing, pos, vel, P); break;
     case CUBIC: kParticleVelUpdate<CUBIC><<<gr, kThreads, 0, s>>>(g, mode, vin, prev, firstFlip, mixing, pos, vel, P); break;
     case G2PNEAREST: kParticleVelUpdate<G2PNEAREST><<<gr, kThreads, 0, s>>>(g, mode, vin, prev, firstFlip, mixing, pos, vel, P); break;
@@ -1014,6 +1053,7 @@ cudaError_t launchParticleVelUpdate(const Geom& g, int mode, int alg, ConstFaceF
   return cudaGetLastError();
 }
 
+// max of m over the block, then atomically into *dst (bits of a float >= 0)
 __device__ inline void blockMaxToGlobal(float m, unsigned int* dst) {
   __shared__ float s[32];
   m = warpMaxF(m);

@@ -159,6 +159,8 @@ struct ExtrapScratch {
   unsigned int* hist;      // kExtrapHistWords: the layer histogram, then the grid-barrier words
   unsigned int* offsets;   // kMaxLayers + 2
   unsigned int* cursor;    // kMaxLayers + 2
+  uint8_t* mask;           // total faces: per list entry, the neighbours (bit q in the order left, right,
+                           // down, up, back, front) that lie in an earlier layer
 };
 constexpr int kMaxLayers = 1000;
 // hist[0 .. kMaxLayers + 1] is the histogram; hist[kMaxLayers + 2 ..] the
@@ -203,9 +205,12 @@ cudaError_t launchSeedScan(unsigned int* blockCounts, int nBlocks, unsigned long
 cudaError_t launchSeedWrite(const Geom& g, const float* fluidSDF, const uint8_t* solidIdx,
                             const unsigned int* blockOffsets, int cellsPerBlock, int ppc, unsigned long long seed,
                             float* pos, cudaStream_t s);
+// LINEAR (alg 2) also writes v0 = the PIC sample of vinQ (the corner tables of
+// vin) and max |v0| into st[0], the start of the substep loop, which then
+// needs no launchSubstepBegin; the other transfer kernels leave both alone.
 cudaError_t launchParticleVelUpdate(const Geom& g, int mode, int alg, ConstFaceField vin, ConstFaceField prev,
                                     int firstFlip, float mixing, const float* pos, float* vel, long long P,
-                                    cudaStream_t s);
+                                    cudaStream_t s, const FaceQuads* vinQ, float* v0, SubstepState* st);
 // Corner tables of the face grids for the substep kernels; component a has
 // faceQuadCount(r, a) entries.
 long long faceQuadCount(const Dim3i& r, int a);

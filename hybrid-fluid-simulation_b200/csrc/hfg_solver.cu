@@ -92,7 +92,7 @@ GridSolver::GridSolver(float dt, Dim3i res, const float origin[3], const float s
   check(makeCgMaps(cg_, cgc_.p, cgr_.p, cgx_.p, false, cgp_[0].p, cgp_[1].p, &maps_), "CG tensor maps");
   cgState_.alloc(1, stream_);
   subState_.alloc(subSlots_ + 1, stream_);
-  dist_.alloc(Ftot_, stream_); list_.alloc(Ftot_, stream_);
+  dist_.alloc(Ftot_, stream_); list_.alloc(Ftot_, stream_); mask_.alloc(Ftot_, stream_);
   hist_.alloc(kExtrapHistWords, stream_);
   offsets_.alloc(kMaxLayers + 2, stream_);
   cursor_.alloc(kMaxLayers + 2, stream_);
@@ -364,18 +364,24 @@ void GridSolver::p2gCell(const float* vals, int span, int comp, float* out) {
   launched(launchNormalize(N_, cacc_.p, out, nullptr, 0.f, 0, 0.f, 0, stream_), "normalize cell");
 }
 
-// EulerParticles.cpp:231-325.  Substeps are launched speculatively in chunks;
-// a launch whose slot is already finished does nothing.
-void GridSolver::advectParticles(const float* const vin[3]) {
+// Corner tables of the advecting velocity (G2P and every substep sample read
+// them) and a cleared substep state.
+FaceQuads GridSolver::beginParticleStep(ConstFaceField vin) {
   float4* quads[3];
   for (int a = 0; a < 3; ++a) {
     quads_[a].alloc(faceQuadCount(g_.r, a), stream_);
     quads[a] = quads_[a].p;
   }
-  launched(launchFaceQuads(g_.r, ConstFaceField{{vin[0], vin[1], vin[2]}}, quads, stream_), "face corner tables");
-  FaceQuads v{{quads[0], quads[1], quads[2]}};
+  launched(launchFaceQuads(g_.r, vin, quads, stream_), "face corner tables");
   check(cudaMemsetAsync(subState_.p, 0, sizeof(SubstepState) * (subSlots_ + 1), stream_), "memset");
-  launched(launchSubstepBegin(g_, v, ppos_.p, pv0_.p, P_, subState_.p, stream_), "substep begin");
+  return FaceQuads{{quads[0], quads[1], quads[2]}};
+}
+
+// EulerParticles.cpp:231-325.  Substeps are launched speculatively in chunks;
+// a launch whose slot is already finished does nothing.  With haveV0 the
+// first sample (v0 and its max) is already in place, from the LINEAR G2P.
+void GridSolver::advectParticles(const FaceQuads& v, bool haveV0) {
+  if (!haveV0) launched(launchSubstepBegin(g_, v, ppos_.p, pv0_.p, P_, subState_.p, stream_), "substep begin");
   long long nclamp = opt_.clamp_mode == 1 ? std::min<long long>(P_, N_) : P_;
   int slot = 0;
   for (;;) {
@@ -400,7 +406,6 @@ void GridSolver::computeAdvection() {
   float gv[3], ev[3];
   bool doG, doE;
   forcesTerms(gv, doG, ev, doE);
-  const float* vin[3] = {vel_[ci][0].p, vel_[ci][1].p, vel_[ci][2].p};
   float* vout[3] = {vel_[ni][0].p, vel_[ni][1].p, vel_[ni][2].p};
   if (adv_ == HFG_ADV_SEMI_LAGRANGIAN) {
     stageBegin(1);
@@ -419,10 +424,12 @@ void GridSolver::computeAdvection() {
   ConstFaceField prev{{prev_[0].p, prev_[1].p, prev_[2].p}};
   int mode = adv_ == HFG_ADV_PIC ? MODE_PIC : (adv_ == HFG_ADV_FLIP ? MODE_FLIP : MODE_MIX);
   int first = (mode != MODE_PIC && !velFlag_) ? 1 : 0;
-  launched(launchParticleVelUpdate(g_, mode, alg_, cvel(ci), prev, first, mixing_, ppos_.p, pvel_.p, P_, stream_),
+  FaceQuads vq = beginParticleStep(cvel(ci));
+  launched(launchParticleVelUpdate(g_, mode, alg_, cvel(ci), prev, first, mixing_, ppos_.p, pvel_.p, P_, stream_,
+                                   &vq, pv0_.p, subState_.p),
            "particle velocity");
   if (mode != MODE_PIC) velFlag_ = true;
-  advectParticles(vin);
+  advectParticles(vq, alg_ == HFG_LINEAR);
   float* copy[3] = {prev_[0].p, prev_[1].p, prev_[2].p};
   p2gFace(pvel_.p, vout, mode == MODE_PIC ? nullptr : copy, gv, doG, ev, doE);
   if (opt_.advect_scalars) {
@@ -577,7 +584,7 @@ void GridSolver::extrapolate() {
   if (nums > 1) {
     float* vals[3] = {vel_[ni][0].p, vel_[ni][1].p, vel_[ni][2].p};
     long long off[3] = {0, F_[0], F_[0] + F_[1]};
-    ExtrapScratch sc{dist_.p, list_.p, hist_.p, offsets_.p, cursor_.p};
+    ExtrapScratch sc{dist_.p, list_.p, hist_.p, offsets_.p, cursor_.p, mask_.p};
     launched(launchExtrapDistance(fr_, vals, off, nums, sc, stream_), "extrapolation distance", 17);
     check(launchExtrapLayers(fr_, vals, off, sc, nums, stream_, &launches_), "extrapolation layers");
     check(cudaMemcpyAsync(extrapHost_, extrapBarWords(sc), sizeof(unsigned int) * 4, cudaMemcpyDeviceToHost, stream_),

@@ -139,7 +139,8 @@ class GridSolver {
  private:
   void updateBoundarys();
   void computeAdvection();
-  void advectParticles(const float* const vin[3]);
+  FaceQuads beginParticleStep(ConstFaceField vin);
+  void advectParticles(const FaceQuads& v, bool haveV0);
   void p2gFace(const float* vel, float* const out[3], float* const copy[3], const float add[3], bool doAdd,
                const float add2[3], bool doAdd2);
   void p2gCell(const float* vals, int span, int comp, float* out);
@@ -191,6 +192,7 @@ class GridSolver {
   DArray<float2> acc_[3], cacc_;
   DArray<float4> quads_[3];  // corner tables of the advecting velocity (particle substeps)
   DArray<uint16_t> dist_;
+  DArray<uint8_t> mask_;
   DArray<unsigned int> list_, hist_, offsets_, cursor_;
   unsigned int* extrapHost_ = nullptr;  // pinned
 
