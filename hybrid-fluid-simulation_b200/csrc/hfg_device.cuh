@@ -429,4 +429,48 @@ __device__ inline bool gridSum2(double& a, double& b, double* partials, unsigned
   return true;
 }
 
+// Device clock in ns (globaltimer), for bounded waits.
+__device__ __forceinline__ unsigned long long globalNs() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ unsigned ldAcquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Grid barrier of a cooperative launch (generation counting).  The wait is
+// bounded: past the deadline, or once another block has given up, the error
+// word is set and false returned, and the caller stops.
+__device__ inline bool gridBarrier(unsigned* count, unsigned* gen, unsigned* err, unsigned nblocks) {
+  __shared__ int okS;
+  __syncthreads();
+  if (flatTid() == 0) {
+    int ok = 1;
+    const unsigned g = ldAcquire(gen);
+    __threadfence();  // this block's writes before its arrival
+    if (atomicAdd(count, 1u) == nblocks - 1) {
+      atomicExch(count, 0u);
+      __threadfence();
+      atomicAdd(gen, 1u);
+    } else {
+      const unsigned long long deadline = globalNs() + 1000000000ull;  // 1 s
+      while (ldAcquire(gen) == g) {
+        if (ldAcquire(err) != 0u || globalNs() > deadline) {
+          atomicExch(err, 1u);
+          ok = 0;
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+    okS = ok;
+  }
+  __syncthreads();
+  return okS != 0;
+}
+
 }  // namespace hfg

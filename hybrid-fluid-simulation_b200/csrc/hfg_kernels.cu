@@ -526,49 +526,6 @@ __device__ __forceinline__ void extrapEntry(const Dim3i& r0, const Dim3i& r1, co
   v[i] = acc;
 }
 
-__device__ __forceinline__ unsigned long long globalNs() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-__device__ __forceinline__ unsigned ldAcquire(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
-// Grid barrier of a cooperative launch (generation counting).  The wait is
-// bounded: past the deadline, or once another block has given up, the error
-// word is set and false returned, and the caller stops.
-__device__ bool gridBarrier(unsigned* count, unsigned* gen, unsigned* err, unsigned nblocks) {
-  __shared__ int okS;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int ok = 1;
-    const unsigned g = ldAcquire(gen);
-    __threadfence();  // this block's layer writes before its arrival
-    if (atomicAdd(count, 1u) == nblocks - 1) {
-      atomicExch(count, 0u);
-      __threadfence();
-      atomicAdd(gen, 1u);
-    } else {
-      const unsigned long long deadline = globalNs() + 1000000000ull;  // 1 s
-      while (ldAcquire(gen) == g) {
-        if (ldAcquire(err) != 0u || globalNs() > deadline) {
-          atomicExch(err, 1u);
-          ok = 0;
-          break;
-        }
-        __nanosleep(32);
-      }
-    }
-    __threadfence();
-    okS = ok;
-  }
-  __syncthreads();
-  return okS != 0;
-}
-
 // Layers 1 .. nums-1, persistent: a layer with more than kExtrapSmallLayer
 // faces is spread over the grid; a run of smaller consecutive layers is filled
 // by block 0 alone with block barriers between them.  Every block walks the

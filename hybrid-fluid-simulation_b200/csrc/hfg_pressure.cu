@@ -368,11 +368,6 @@ constexpr int kDirStages = 4, kUpdStages = 5;
 constexpr unsigned long long kWaitNs = 2000000000ull;  // a stage that takes 2 s to land is an error
 
 __device__ __forceinline__ uint32_t smemAddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ unsigned long long globalNs() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
 __device__ __forceinline__ void mbarInit(uint64_t* bar, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smemAddr(bar)), "r"(count) : "memory");
 }
@@ -761,7 +756,7 @@ cudaError_t makeHaloMap(const Dim3i& cg, const float* v, CUtensorMap* m) {
 
 cudaError_t makeCgMaps(const Dim3i& cg, const CgCode* code, const float* r, const void* x, bool xDouble,
                        const float* p0, const float* p1, CgMaps* m) {
-  if (cg.x % 8 != 0) return cudaErrorInvalidValue;  // rows must start on 16-byte boundaries
+  if (cg.x % 16 != 0) return cudaErrorInvalidValue;  // rows of 8-bit codes must start on 16-byte boundaries
   cudaError_t e;
   if ((e = encodeMap(&m->codeH, code, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, cg, CW, FH)) != cudaSuccess) return e;
   if ((e = encodeMap(&m->codeI, code, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, cg, CTX, CTR)) != cudaSuccess) return e;
