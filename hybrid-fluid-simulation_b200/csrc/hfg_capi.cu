@@ -363,6 +363,14 @@ HFG_API int hfg_solver_get_particles(hfg_solver_t s, float* pos, float* vel) {
     return HFG_OK;
   });
 }
+HFG_API int hfg_solver_set_particle_mirror(hfg_solver_t s, float* pos, float* vel, long long capacity) {
+  return guarded([&]() -> int {
+    SOLVER(s);
+    NEED(capacity >= 0 && (capacity == 0 || pos || vel || (!pos && !vel)), "invalid arguments");
+    S.setParticleMirror(pos, vel, capacity);
+    return HFG_OK;
+  });
+}
 HFG_API int hfg_solver_get_stats(hfg_solver_t s, hfg_stats_t* out) {
   return guarded([&]() -> int {
     SOLVER(s);

@@ -118,7 +118,10 @@ GridSolver::GridSolver(float dt, Dim3i res, const float origin[3], const float s
 }
 
 GridSolver::~GridSolver() {
+  if (copy_.s) cudaStreamSynchronize(copy_.s);
   if (stream_) cudaStreamSynchronize(stream_);
+  if (advDone_) cudaEventDestroy(advDone_);
+  if (copyDone_) cudaEventDestroy(copyDone_);
   extrapUsers(-1);
   for (auto* b : bsdf_) delete b;
   dropGraphs();
@@ -216,6 +219,7 @@ void GridSolver::setAdvection(int kind, int acc, int alg, float cfl, float mixin
 }
 
 void GridSolver::setParticles(const float* pos, const float* vel, long long n) {
+  finishMirrorCopy();
   if (n < 0) throw CudaError("negative particle count", HFG_ERR_INVALID);
   P_ = n;
   ppos_.alloc(3 * n, stream_);
@@ -237,6 +241,7 @@ void GridSolver::setParticles(const float* pos, const float* vel, long long n) {
 // EulerParticles.cpp:140-179 on the device: the fluid cells of the current
 // fluid-domain field that are not inside a solid get `ppc` particles each.
 void GridSolver::seedParticles(int ppc, unsigned long long seed) {
+  finishMirrorCopy();
   if (ppc <= 0) throw CudaError("particles per cell must be positive", HFG_ERR_INVALID);
   // Cells inside a solid get no particles (findFluidGrid,
   // EulerParticlesTool.cu:20).  The solids are classified at their current
@@ -402,6 +407,7 @@ void GridSolver::advectParticles(const FaceQuads& v, bool haveV0) {
 // forces of ExternalForcesSolver.cpp:50-58 are folded into the pass that
 // writes the advected velocity.
 void GridSolver::computeAdvection() {
+  finishMirrorCopy();
   int ci = cur(), ni = nxt();
   float gv[3], ev[3];
   bool doG, doE;
@@ -429,7 +435,9 @@ void GridSolver::computeAdvection() {
                                    &vq, pv0_.p, subState_.p),
            "particle velocity");
   if (mode != MODE_PIC) velFlag_ = true;
+  startMirrorCopy(false);
   advectParticles(vq, alg_ == HFG_LINEAR);
+  startMirrorCopy(true);
   float* copy[3] = {prev_[0].p, prev_[1].p, prev_[2].p};
   p2gFace(pvel_.p, vout, mode == MODE_PIC ? nullptr : copy, gv, doG, ev, doE);
   if (opt_.advect_scalars) {
@@ -606,6 +614,7 @@ void GridSolver::updateWithoutPressure() {
 void GridSolver::solvePressure() {
   computePressure();
   extrapolate();
+  finishMirrorCopy();
   bufferFlag_ = !bufferFlag_;  // GridFluidSolver.cpp:393-397
   time_ += dt_;
 }
@@ -746,6 +755,44 @@ void GridSolver::mixVelFieldWithOthers(const float* const other[3], const float*
 void GridSolver::transferVelToParticles(const float* pos, long long n, int alg, float* vel) {
   if (n > 0) launched(launchG2PFace(g_, alg, cvel(cur()), pos, n, vel, stream_), "g2p");
   synchronize();
+}
+
+void GridSolver::setParticleMirror(float* pos, float* vel, long long capacity) {
+  finishMirrorCopy();
+  if (!pos && !vel) {
+    mirrorPos_ = mirrorVel_ = nullptr;
+    mirrorCap_ = 0;
+    return;
+  }
+  if (!copy_.s) check(cudaStreamCreateWithFlags(&copy_.s, cudaStreamNonBlocking), "cudaStreamCreate");
+  if (!advDone_) check(cudaEventCreateWithFlags(&advDone_, cudaEventDisableTiming), "cudaEventCreate");
+  if (!copyDone_) check(cudaEventCreateWithFlags(&copyDone_, cudaEventDisableTiming), "cudaEventCreate");
+  mirrorPos_ = pos;
+  mirrorVel_ = vel;
+  mirrorCap_ = capacity;
+}
+
+// The particle velocities hold their values for the rest of the step once the
+// G2P update has run, the positions once the substeps have: each copy to the
+// mirror starts on the copy stream at that point, the velocities while the
+// substeps run and the positions while the pressure solve runs.  Every writer
+// of the particles (setParticles, seedParticles, the next advection) first
+// waits for both (finishMirrorCopy), and so does the end of the step.
+void GridSolver::startMirrorCopy(bool positions) {
+  float* dst = positions ? mirrorPos_ : mirrorVel_;
+  if (!dst || P_ <= 0) return;
+  if (P_ > mirrorCap_) throw CudaError("particle mirror smaller than the particle count", HFG_ERR_INVALID);
+  check(cudaEventRecord(advDone_, stream_), "event");
+  check(cudaStreamWaitEvent(copy_.s, advDone_, 0), "wait");
+  check(cudaMemcpyAsync(dst, positions ? ppos_.p : pvel_.p, 12 * P_, cudaMemcpyDeviceToHost, copy_.s), "mirror");
+  check(cudaEventRecord(copyDone_, copy_.s), "event");
+  copyPending_ = true;
+}
+
+void GridSolver::finishMirrorCopy() {
+  if (!copyPending_) return;
+  copyPending_ = false;
+  check(cudaEventSynchronize(copyDone_), "mirror copy");
 }
 
 void GridSolver::getParticles(float* pos, float* vel) {

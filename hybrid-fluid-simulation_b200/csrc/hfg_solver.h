@@ -125,6 +125,8 @@ class GridSolver {
   // transferFluidVelField2Particles (device pointers)
   void transferVelToParticles(const float* pos, long long n, int alg, float* vel);
   void getParticles(float* pos, float* vel);
+  // host mirror filled by every update (hfg_solver_set_particle_mirror)
+  void setParticleMirror(float* pos, float* vel, long long capacity);
   void getStats(hfg_stats_t* st);
   void synchronize();
   float timeCg(int iters);
@@ -162,6 +164,7 @@ class GridSolver {
   void stageEnd(int i);
 
   OwnedStream own_;  // first member: outlives every array below
+  OwnedStream copy_;  // the particle-mirror copies
   Geom g_;
   Dim3i fr_[3];
   long long N_, F_[3], Ftot_;
@@ -176,6 +179,13 @@ class GridSolver {
   DArray<uint8_t> solidIdx_, markers_;
   DArray<Code> code_;
   DArray<CgCode> cgc_;
+  float* mirrorPos_ = nullptr;
+  float* mirrorVel_ = nullptr;
+  long long mirrorCap_ = 0;
+  cudaEvent_t advDone_ = nullptr, copyDone_ = nullptr;
+  bool copyPending_ = false;
+  void startMirrorCopy(bool positions);
+  void finishMirrorCopy();
   Dim3i cg_;       // pitched grid of the pressure system
   long long NC_ = 0;
   CgMaps maps_;

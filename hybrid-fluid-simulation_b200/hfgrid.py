@@ -142,6 +142,7 @@ def _signatures(lib):
         "hfg_solver_transfer_vel_to_particles": (C.c_int, [S, VP, C.c_longlong, C.c_int, VP]),
         "hfg_solver_num_particles": (C.c_longlong, [S]),
         "hfg_solver_get_particles": (C.c_int, [S, PF, PF]),
+        "hfg_solver_set_particle_mirror": (C.c_int, [S, PF, PF, C.c_longlong]),
         "hfg_solver_get_stats": (C.c_int, [S, C.POINTER(Stats)]),
         "hfg_solver_get_grid": (C.c_int, [S, I3, F3, F3]),
         "hfg_solver_stream": (C.c_void_p, [S]),
@@ -430,6 +431,18 @@ class Solver:
 
     def copy_particles_into(self, pos: np.ndarray, vel: Optional[np.ndarray] = None):
         _check(lib().hfg_solver_get_particles(self._h, _fptr(pos), None if vel is None else _fptr(vel)))
+
+    def set_particle_mirror(self, pos: Optional[np.ndarray], vel: Optional[np.ndarray] = None):
+        """hfg_solver_set_particle_mirror: every update() also fills pos / vel
+        ((capacity, 3) float32 host arrays, pinned for overlap) with the
+        particles; None, None removes the mirror."""
+        arrays = [a for a in (pos, vel) if a is not None]
+        cap = min(a.shape[0] for a in arrays) if arrays else 0
+        for a in arrays:
+            assert a.ndim == 2 and a.shape[1] == 3
+        _check(lib().hfg_solver_set_particle_mirror(self._h, None if pos is None else _fptr(pos),
+                                                    None if vel is None else _fptr(vel), cap))
+        self._mirror = (pos, vel)  # the library writes into them: keep them alive
 
     def stats(self) -> dict:
         s = Stats()

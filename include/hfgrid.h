@@ -171,6 +171,19 @@ HFG_API int hfg_solver_mix_vel_field_with_others(hfg_solver_t s, const float* vx
 HFG_API int hfg_solver_transfer_vel_to_particles(hfg_solver_t s, const float* pos, long long n, int alg, float* vel);
 HFG_API long long hfg_solver_num_particles(hfg_solver_t s);
 HFG_API int hfg_solver_get_particles(hfg_solver_t s, float* pos, float* vel);
+/* Host mirror of the particles (an extension; the reference's viewer calls
+ * copyEulerParticlesPos/VelToCPU after every update, MPhysicsAPI.h).  While a
+ * mirror is set, every update also copies the particle positions and
+ * velocities into pos and vel (HOST buffers of 3 * capacity floats, either may
+ * be NULL), as the step leaves them: each copy runs on a second stream from
+ * the point where the step is done with that array (the velocities after the
+ * grid-to-particle update, the positions after the substeps), overlapped with
+ * the rest of the step; the update returns after both have landed.  Buffers allocated with
+ * cudaHostAlloc or registered with cudaHostRegister let the copy overlap; other
+ * host memory is copied correctly but not overlapped.  An update with more
+ * particles than capacity fails with HFG_ERR_INVALID.  pos = vel = NULL
+ * removes the mirror. */
+HFG_API int hfg_solver_set_particle_mirror(hfg_solver_t s, float* pos, float* vel, long long capacity);
 HFG_API int hfg_solver_get_stats(hfg_solver_t s, hfg_stats_t* st);
 HFG_API int hfg_solver_get_grid(hfg_solver_t s, int res[3], float origin[3], float spacing[3]);
 /* The CUDA stream every kernel of this solver runs on (cudaStream_t). */

@@ -287,3 +287,30 @@ def test_pressure_fp64_option(cuda):
     assert st64["divergence_l2"] < st32["divergence_l2"]
     assert st64["divergence_l2"] <= 1e-5 * st64["cg_rhs_norm"]
     assert vel_rel_l2(v64, o.velocity_field()) < 2e-3
+
+
+def test_particle_mirror(cuda):
+    """hfg_solver_set_particle_mirror: after every update the host mirror
+    (pinned, and plain pageable memory) holds exactly the particles that
+    hfg_solver_get_particles returns; a mirror smaller than the particle count
+    makes the update fail; removing it stops the copies."""
+    import torch
+    sc = small_scene()
+    g = scenes.gpu_solver(sc, precond=1, tol_mode=1, tol=1e-6, max_iter=400)
+    n = g.num_particles
+    mpos = torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy()
+    mvel = np.empty((n, 3), np.float32)  # pageable: correct, not overlapped
+    g.set_particle_mirror(mpos, mvel)
+    for _ in range(3):
+        g.update()
+        pos, vel = g.particles()
+        assert np.array_equal(mpos, pos)
+        assert np.array_equal(mvel, vel)
+    g.set_particle_mirror(None, None)
+    before = mpos.copy()
+    g.update()
+    assert np.array_equal(mpos, before)
+    small = np.empty((n - 1, 3), np.float32)
+    g.set_particle_mirror(small)
+    with pytest.raises(hfgrid.HfgError):
+        g.update()
