@@ -252,8 +252,7 @@ void GridSolver::seedParticles(int ppc, unsigned long long seed) {
     bs.sdf[i] = bsdf_[i]->p;
     bs.tx[i] = btrans_[3 * i]; bs.ty[i] = btrans_[3 * i + 1]; bs.tz[i] = btrans_[3 * i + 2];
   }
-  if (bs.n > 0) launched(launchSolidClassify(g_, bs, solidIdx_.p, nullptr, stream_), "solid classify");
-  else check(cudaMemsetAsync(solidIdx_.p, 0, N_, stream_), "memset");
+  classifySolids(bs);
   const int cellsPerBlock = 4096;
   int nb = (int)((N_ + cellsPerBlock - 1) / cellsPerBlock);
   DArray<unsigned int> counts;
@@ -330,11 +329,28 @@ void GridSolver::updateBoundarys() {
     b.tx[i] = btrans_[3 * i]; b.ty[i] = btrans_[3 * i + 1]; b.tz[i] = btrans_[3 * i + 2];
     b.vx[i] = bvel_[3 * i]; b.vy[i] = bvel_[3 * i + 1]; b.vz[i] = bvel_[3 * i + 2];
   }
-  if (b.n == 0) {
-    check(cudaMemsetAsync(solidIdx_.p, 0, N_, stream_), "memset");
-    return;
+  classifySolids(b);
+}
+
+// solidIdx_ from the boundaries at their current placement.  A placement
+// equal to the one solidIdx_ already holds (same SDF arrays, same
+// translations: solids at rest) needs no new classification.
+void GridSolver::classifySolids(const BoundarySet& b) {
+  std::vector<float> key;
+  key.reserve(4 * b.n + 1);
+  key.push_back((float)b.n);
+  for (int i = 0; i < b.n; ++i) {
+    key.push_back(b.tx[i]);
+    key.push_back(b.ty[i]);
+    key.push_back(b.tz[i]);
   }
-  launched(launchSolidClassify(g_, b, solidIdx_.p, nullptr, stream_), "solid classify");
+  std::vector<const float*> ptrs(b.sdf, b.sdf + b.n);
+  if (classified_ && key == classKey_ && ptrs == classSdf_) return;
+  if (b.n == 0) check(cudaMemsetAsync(solidIdx_.p, 0, N_, stream_), "memset");
+  else launched(launchSolidClassify(g_, b, solidIdx_.p, nullptr, stream_), "solid classify");
+  classified_ = true;
+  classKey_ = std::move(key);
+  classSdf_ = std::move(ptrs);
 }
 
 // ExternalForcesSolver.cpp:50-58: two unit-field axpys, each skipped when all

@@ -211,6 +211,11 @@ class GridSolver {
 
   std::vector<DArray<float>*> bsdf_;
   std::vector<float> bvel_, btrans_;
+  // the placement solidIdx_ was last classified at (classifySolids)
+  bool classified_ = false;
+  std::vector<float> classKey_;
+  std::vector<const float*> classSdf_;
+  void classifySolids(const BoundarySet& b);
   float ext_[3] = {0, 0, 0};
   float gravity_[3] = {0.f, -9.8f, 0.f};  // ExternalForcesSolver.h:25
 
