@@ -376,19 +376,43 @@ __global__ void kDistCols(Dim3i r, int axis, uint16_t* __restrict__ d) {
     } else {
       base = l;
     }
+    // the column in batches of B: the B loads of a batch are in flight
+    // together, then the batch is relaxed in order
+    constexpr int B = 8;
+    uint16_t* col = d + base;
     uint16_t prev = kFar;
-    for (int i = 0; i < len; ++i) {
-      uint16_t v = d[base + i * stride];
-      uint16_t cand = satInc(prev);
-      if (cand < v) { v = cand; d[base + i * stride] = v; }
-      prev = v;
+    for (int i0 = 0; i0 < len; i0 += B) {
+      uint16_t v[B];
+#pragma unroll
+      for (int k = 0; k < B; ++k) v[k] = i0 + k < len ? col[(long long)(i0 + k) * stride] : kFar;
+#pragma unroll
+      for (int k = 0; k < B; ++k) {
+        if (i0 + k < len) {
+          const uint16_t cand = satInc(prev);
+          if (cand < v[k]) {
+            v[k] = cand;
+            col[(long long)(i0 + k) * stride] = cand;
+          }
+          prev = v[k];
+        }
+      }
     }
     prev = kFar;
-    for (int i = len - 1; i >= 0; --i) {
-      uint16_t v = d[base + i * stride];
-      uint16_t cand = satInc(prev);
-      if (cand < v) { v = cand; d[base + i * stride] = v; }
-      prev = v;
+    for (int i0 = len - 1; i0 >= 0; i0 -= B) {
+      uint16_t v[B];
+#pragma unroll
+      for (int k = 0; k < B; ++k) v[k] = i0 - k >= 0 ? col[(long long)(i0 - k) * stride] : kFar;
+#pragma unroll
+      for (int k = 0; k < B; ++k) {
+        if (i0 - k >= 0) {
+          const uint16_t cand = satInc(prev);
+          if (cand < v[k]) {
+            v[k] = cand;
+            col[(long long)(i0 - k) * stride] = cand;
+          }
+          prev = v[k];
+        }
+      }
     }
   }
 }
