@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <map>
 #include <mutex>
+#include <utility>
 
 #include "hfg_kernels.h"
 
@@ -368,6 +369,14 @@ constexpr int kDirStages = 4, kUpdStages = 5;
 constexpr unsigned long long kWaitNs = 2000000000ull;  // a stage that takes 2 s to land is an error
 
 __device__ __forceinline__ uint32_t smemAddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+// Programmatic dependent launch: the CG kernels are launched so that they may
+// start while the kernel before them finishes; this wait (griddepcontrol.wait)
+// returns once that kernel has completed and its writes are visible, and
+// comes before the first read of anything it wrote.
+__device__ __forceinline__ void waitPrevGrid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// Lets the next kernel of the stream be scheduled once every block of this one
+// has issued it (its blocks then wait in waitPrevGrid for this one to finish).
+__device__ __forceinline__ void allowNextGrid() { asm volatile("griddepcontrol.launch_dependents;" :::); }
 __device__ __forceinline__ void mbarInit(uint64_t* bar, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smemAddr(bar)), "r"(count) : "memory");
 }
@@ -476,6 +485,23 @@ CgLaunch cgLaunch(const Dim3i& cg, K kernel) {
   return L;
 }
 
+// Launch with programmatic stream serialization (the kernel calls
+// waitPrevGrid before reading what earlier work wrote).
+template <class... KP, class... A>
+cudaError_t launchPdl(void (*kernel)(KP...), dim3 grid, dim3 block, cudaStream_t s, A&&... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+}
+
 // CG direction: p = z + beta p_old (scal then axpy with 1), q = A p and the
 // reduction p.q; the last block forms alpha = r.z / p.Ap
 // (CuMatrixFreePCG.cpp:40-47, :56-60).  Stage i of the ring holds raw (z or r,
@@ -489,7 +515,6 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
                  const __grid_constant__ CUtensorMap mCode, Dim3i P, float sx, float sy, float sz,
                  const CgCode* __restrict__ code, const float* __restrict__ zr, const float* __restrict__ pOld,
                  float* __restrict__ pNew, double* partials, CgState* st, int zPer) {
-  if (st->done) return;
   __shared__ DirStage stg[kDirStages];
   __shared__ float pt[2][FH][CTX + 2];
   __shared__ DiagTab tab;
@@ -513,6 +538,9 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
   }
   buildDiagTab(tab, sx, sy, sz);
   __syncthreads();
+  waitPrevGrid();
+  if (st->done) return;  // the same value in every thread
+  allowNextGrid();
   if (tid == 0) {
     int n = min(kDirStages, nLoad);
     for (int i = 0; i < n; ++i) issue(i);
@@ -618,7 +646,6 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
               const __grid_constant__ CUtensorMap mX, const __grid_constant__ CUtensorMap mCode, Dim3i P, float sx,
               float sy, float sz, const float* __restrict__ p, TX* __restrict__ xv, float* __restrict__ r,
               double* partials, CgState* st, int zPer) {
-  if (st->done) return;
   constexpr int kUpdStages = kUpdStagesT<TX>;
   using Stage = UpdStage<TX>;
   __shared__ Stage stg[kUpdStages];
@@ -644,6 +671,9 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
   }
   buildDiagTab(tab, sx, sy, sz);
   __syncthreads();
+  waitPrevGrid();
+  if (st->done) return;  // the same value in every thread
+  allowNextGrid();
   if (tid == 0) {
     int n = min(kUpdStages, nLoad);
     for (int i = 0; i < n; ++i) issue(i);
@@ -800,20 +830,23 @@ cudaError_t launchCgDirection(const Dim3i& cg, float sx, float sy, float sz, con
   switch (precond) {
     case 1: {
       CgLaunch L = cgLaunch(cg, kCgDirection<1>);
-      kCgDirection<1><<<L.grid, L.block, 0, s>>>(mZ, mPo, mCode, cg, sx, sy, sz, code, zr, pOld, pNew, partials, st,
-                                                 L.zPer);
+      cudaError_t e = launchPdl(kCgDirection<1>, L.grid, L.block, s, mZ, mPo, mCode, cg, sx, sy, sz, code, zr, pOld,
+                                pNew, partials, st, L.zPer);
+      if (e != cudaSuccess) return e;
       break;
     }
     case 2: {
       CgLaunch L = cgLaunch(cg, kCgDirection<2>);
-      kCgDirection<2><<<L.grid, L.block, 0, s>>>(mZ, mPo, mCode, cg, sx, sy, sz, code, zr, pOld, pNew, partials, st,
-                                                 L.zPer);
+      cudaError_t e = launchPdl(kCgDirection<2>, L.grid, L.block, s, mZ, mPo, mCode, cg, sx, sy, sz, code, zr, pOld,
+                                pNew, partials, st, L.zPer);
+      if (e != cudaSuccess) return e;
       break;
     }
     default: {
       CgLaunch L = cgLaunch(cg, kCgDirection<0>);
-      kCgDirection<0><<<L.grid, L.block, 0, s>>>(mZ, mPo, mCode, cg, sx, sy, sz, code, zr, pOld, pNew, partials, st,
-                                                 L.zPer);
+      cudaError_t e = launchPdl(kCgDirection<0>, L.grid, L.block, s, mZ, mPo, mCode, cg, sx, sy, sz, code, zr, pOld,
+                                pNew, partials, st, L.zPer);
+      if (e != cudaSuccess) return e;
     }
   }
   return cudaGetLastError();
@@ -825,8 +858,9 @@ cudaError_t launchCgUpdate(const Dim3i& cg, float sx, float sy, float sz, const 
 #define HFG_CG_UPDATE(PCV, TXV)                                                                                   \
   {                                                                                                               \
     CgLaunch L = cgLaunch(cg, kCgUpdate<PCV, TXV>);                                                             \
-    kCgUpdate<PCV, TXV><<<L.grid, L.block, 0, s>>>(mP, mR, mX, mCode, cg, sx, sy, sz, p, (TXV*)x, r, partials, st, \
-                                                   L.zPer);                                                     \
+    cudaError_t e = launchPdl(kCgUpdate<PCV, TXV>, L.grid, L.block, s, mP, mR, mX, mCode, cg, sx, sy, sz, p,      \
+                              (TXV*)x, r, partials, st, L.zPer);                                              \
+    if (e != cudaSuccess) return e;                                                                             \
   }
   if (xDouble) {
     if (precond == 1) HFG_CG_UPDATE(1, double)
