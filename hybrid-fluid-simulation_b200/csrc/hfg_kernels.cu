@@ -631,6 +631,16 @@ cudaError_t launchExtrapLayers(const Dim3i rc[3], float* const vals[3], const lo
   return e;
 }
 
+// One warp copies `words` 32-bit words (small state read-backs into mapped
+// host memory).
+__global__ void kCopyWords(const unsigned* __restrict__ src, unsigned* __restrict__ dst, int words) {
+  for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+}
+cudaError_t launchCopyWords(const unsigned* src, unsigned* dst, int words, cudaStream_t s) {
+  kCopyWords<<<1, 32, 0, s>>>(src, dst, words);
+  return cudaGetLastError();
+}
+
 // ===========================================================================
 // Fluid SDF of the fluid-domain field (buildFluidSDF, EulerSolverTool.cu:324-406,
 // :760-785; GridFluidSolver.cpp:571-591).  Layer 0 marks the cells on both

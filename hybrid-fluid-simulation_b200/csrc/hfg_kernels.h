@@ -152,6 +152,9 @@ void cgWarmLaunchCache();
 // doubles of reduction scratch the CG kernels need on grid `r`
 int cgPartialsNeeded(const Dim3i& r);
 
+// dst[0 .. words) = src[...] by one warp (dst may be mapped host memory)
+cudaError_t launchCopyWords(const unsigned* src, unsigned* dst, int words, cudaStream_t s);
+
 // ---- extrapolation ---------------------------------------------------------
 struct ExtrapScratch {
   uint16_t* dist;          // total faces

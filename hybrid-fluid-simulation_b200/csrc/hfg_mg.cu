@@ -518,7 +518,7 @@ void mgRunCg(Multigrid* m, const Dim3i& cg, float sx, float sy, float sz, const 
   for (;;) {
     check(cudaGraphLaunch(*chunk, s), "cg chunk");
     launches += m->chunkLaunches;
-    check(cudaMemcpyAsync(stHost, st, sizeof(CgState), cudaMemcpyDeviceToHost, s), "read cg state");
+    readBack(stHost, st, sizeof(CgState), s);
     check(cudaStreamSynchronize(s), "cg sync");
     if (stHost->done) break;
   }

@@ -34,7 +34,8 @@ void* pinnedGet(size_t bytes) {
     }
   }
   void* p = nullptr;
-  check(cudaMallocHost(&p, kPinnedBlock), "cudaMallocHost");
+  // mapped: kernels write the read-backs straight into these blocks
+  check(cudaHostAlloc(&p, kPinnedBlock, cudaHostAllocMapped | cudaHostAllocPortable), "cudaHostAlloc");
   return p;
 }
 
@@ -42,6 +43,17 @@ void pinnedPut(void* p) {
   if (!p) return;
   std::lock_guard<std::mutex> lk(g_pinnedMu);
   g_pinnedFree.push_back(p);
+}
+
+// A small device-to-host read that does not use a copy engine: a one-warp
+// kernel stores the words into the mapped pinned block over the bus.  A large
+// copy on another stream (the particle mirror) occupies the copy engine for
+// milliseconds, and a small cudaMemcpyAsync queued behind it would wait that
+// long.  The caller synchronises the stream before reading `host`.
+void readBack(void* host, const void* dev, size_t bytes, cudaStream_t s) {
+  void* d = nullptr;
+  check(cudaHostGetDevicePointer(&d, host, 0), "cudaHostGetDevicePointer");
+  check(launchCopyWords((const unsigned*)dev, (unsigned*)d, (int)((bytes + 3) / 4), s), "read back");
 }
 
 namespace {
@@ -409,8 +421,7 @@ void GridSolver::advectParticles(const FaceQuads& v, bool haveV0) {
     for (int k = 0; k < kSubstepChunk && slot < subSlots_; ++k, ++slot)
       launched(launchSubstep(g_, v, ppos_.p, pv0_.p, P_, acc_rk_, dt_, cfl_, nclamp, subState_.p, slot, stream_),
                "substep");
-    check(cudaMemcpyAsync(subHost_, subState_.p + slot, sizeof(SubstepState), cudaMemcpyDeviceToHost, stream_),
-          "read substep state");
+    readBack(subHost_, subState_.p + slot, sizeof(SubstepState), stream_);
     check(cudaStreamSynchronize(stream_), "substep sync");
     if (subHost_->finished) { substeps_ = subHost_->count; break; }
     if (slot >= subSlots_) throw CudaError("CFL substep limit reached", HFG_ERR_STATE);
@@ -530,7 +541,7 @@ void GridSolver::runCg() {
     for (;;) {
       check(cudaGraphLaunch(cgGraph_[pc], stream_), "cg chunk");
       launches_ += 2 * kCgChunk;
-      check(cudaMemcpyAsync(cgHost_, cgState_.p, sizeof(CgState), cudaMemcpyDeviceToHost, stream_), "read cg state");
+      readBack(cgHost_, cgState_.p, sizeof(CgState), stream_);
       check(cudaStreamSynchronize(stream_), "cg sync");
       if (cgHost_->done) break;
     }
@@ -611,8 +622,7 @@ void GridSolver::extrapolate() {
     ExtrapScratch sc{dist_.p, list_.p, hist_.p, offsets_.p, cursor_.p, mask_.p};
     launched(launchExtrapDistance(fr_, vals, off, nums, sc, stream_), "extrapolation distance", 17);
     check(launchExtrapLayers(fr_, vals, off, sc, nums, stream_, &launches_), "extrapolation layers");
-    check(cudaMemcpyAsync(extrapHost_, extrapBarWords(sc), sizeof(unsigned int) * 4, cudaMemcpyDeviceToHost, stream_),
-          "read extrapolation state");
+    readBack(extrapHost_, extrapBarWords(sc), sizeof(unsigned int) * 4, stream_);
     check(cudaStreamSynchronize(stream_), "extrapolation sync");
     if (extrapHost_[2] != 0u) throw CudaError("extrapolation: a grid barrier timed out", HFG_ERR_TIMEOUT);
     extrapDepth_ = (int)extrapHost_[3];

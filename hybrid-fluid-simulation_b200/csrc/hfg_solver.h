@@ -69,6 +69,9 @@ template <class T> struct DArray {
 // creating scenes while others run must avoid.
 void* pinnedGet(size_t bytes);
 void pinnedPut(void* p);
+// `bytes` from device memory into a pinned block of pinnedGet, by a kernel
+// on stream s (no copy engine); valid on the host once s is synchronised.
+void readBack(void* host, const void* dev, size_t bytes, cudaStream_t s);
 
 // The solver's stream, destroyed after every member array has been freed
 // on it (declared first in GridSolver, so destroyed last).
