@@ -234,6 +234,34 @@ def test_p2g(cuda, alg):
     np.testing.assert_allclose(host(w), wr, rtol=1e-4, atol=1e-4)
 
 
+def test_p2g_linear_grouped_particles(cuda):
+    """LINEAR face P2G with particles in seeding order (eight per cell, next
+    to each other), the layout where lanes of a warp share corners and sum by
+    shuffles first.  Cells near every wall (the clamped-corner cases), cells
+    with fewer than eight particles and a ragged tail cover full octets,
+    quads, pairs and single lanes; the result must match the FP64 oracle as
+    for unordered particles."""
+    rng = np.random.default_rng(77)
+    nx, ny, nz = RES
+    cells = [(x, y, z) for z in range(nz) for y in range(ny) for x in range(nx)]
+    pos = []
+    for i, (x, y, z) in enumerate(cells):
+        k = 8 if i % 5 else (i % 8)  # every fifth cell holds fewer than eight
+        for _ in range(k):
+            jitter = rng.random(3)
+            pos.append([ORIGIN[0] + (x + jitter[0]) * SPACING[0], ORIGIN[1] + (y + jitter[1]) * SPACING[1],
+                        ORIGIN[2] + (z + jitter[2]) * SPACING[2]])
+    pos = np.array(pos[: len(pos) - 3], np.float32)  # ragged tail
+    vel = rng.standard_normal((len(pos), 3)).astype(np.float32)
+    outs = [torch.empty(sh, dtype=torch.float32, device=cuda) for sh in oracle.face_shapes(RES)]
+    ws = [torch.empty(sh, dtype=torch.float32, device=cuda) for sh in oracle.face_shapes(RES)]
+    hfgrid.op_p2g_fc(RES, ORIGIN, SPACING, dev(pos), dev(vel), hfgrid.LINEAR, outs, ws)
+    ref, wref = oracle.p2g_fc(RES, ORIGIN, SPACING, pos, vel, hfgrid.LINEAR, dbl=1)
+    for a in range(3):
+        np.testing.assert_allclose(host(outs[a]), ref[a], rtol=1e-4, atol=1e-4)
+        np.testing.assert_allclose(host(ws[a]), wref[a], rtol=1e-5, atol=1e-4)
+
+
 @pytest.mark.parametrize("acc", [0, 1, 2])
 def test_advect_particles(cuda, acc):
     rng = np.random.default_rng(30 + acc)
