@@ -11,6 +11,7 @@
 #include <cfloat>
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <utility>
 
 namespace hfg {
 
@@ -471,6 +472,30 @@ __device__ inline bool gridBarrier(unsigned* count, unsigned* gen, unsigned* err
   }
   __syncthreads();
   return okS != 0;
+}
+
+// Programmatic dependent launch.  A kernel launched with launchPdl may start
+// while the kernel before it in the stream finishes: waitPrevGrid
+// (griddepcontrol.wait) returns once that kernel has completed and its writes
+// are visible, and must come before the first read of anything earlier work
+// wrote.  allowNextGrid lets the next such kernel be scheduled once every
+// block of this one has issued it.
+__device__ __forceinline__ void waitPrevGrid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void allowNextGrid() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+
+template <class... KP, class... A>
+inline cudaError_t launchPdl(void (*kernel)(KP...), dim3 grid, dim3 block, cudaStream_t s, A&&... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
 }
 
 }  // namespace hfg

@@ -119,7 +119,9 @@ __global__ void kCoarsenMarkers(Dim3i rf, Dim3i rc, const uint8_t* __restrict__ 
 template <class TB, class TZ>
 __global__ void kJacobiFirst(Lvl L, const TB* __restrict__ b, TZ* __restrict__ z, const Code* __restrict__ code,
                              const CgState* st) {
+  waitPrevGrid();
   if (st->done) return;
+  allowNextGrid();
   int x, y, zz;
   unsigned c;
   if (!cellOf(L.r, x, y, zz, c)) return;
@@ -136,7 +138,9 @@ template <class TB, class TZ, class TC, bool CORR, bool DOT>
 __global__ void kJacobi(Lvl L, Dim3i rc, const TB* __restrict__ b, const TZ* __restrict__ zi, TZ* __restrict__ zo,
                         const TC* __restrict__ zc, const Code* __restrict__ code, double* partials, CgState* st,
                         int zPer) {
+  waitPrevGrid();
   if (st->done) return;
+  allowNextGrid();
   double rz = 0.0, dummy = 0.0;
   const int x = blockIdx.x * BX + threadIdx.x, y = blockIdx.y * BY + threadIdx.y;
   const int zb0 = blockIdx.z * zPer;
@@ -204,7 +208,9 @@ SweepGrid sweepGrid(const Dim3i& r, bool reduce) {
 template <class TB, class TZ, class TBC>
 __global__ void kResidualRestrict(Lvl Lf, Dim3i rc, const TB* __restrict__ b, const TZ* __restrict__ zf,
                                   const Code* __restrict__ code, TBC* __restrict__ bc, const CgState* st) {
+  waitPrevGrid();
   if (st->done) return;
+  allowNextGrid();
   int X, Y, Z;
   unsigned C;
   if (!cellOf(rc, X, Y, Z, C)) return;
@@ -232,7 +238,9 @@ __global__ void kResidualRestrict(Lvl Lf, Dim3i rc, const TB* __restrict__ b, co
 template <class TB, class TZ>
 __global__ void kCoarseSolve(Lvl L, const TB* __restrict__ b, TZ* __restrict__ z, const Code* __restrict__ code,
                              const CgState* st) {
+  waitPrevGrid();
   if (st->done) return;
+  allowNextGrid();
   __shared__ float za[kCoarseMax], zb[kCoarseMax];
   unsigned n = (unsigned)L.r.size();
   for (unsigned c = threadIdx.x; c < n; c += blockDim.x) za[c] = 0.f;
@@ -372,47 +380,53 @@ const float* vcycleT(Multigrid* m, const float* r0, CgState* st, cudaStream_t s,
     lv[l] = Lvl{m->res[l], m->s0[0] * f, m->s0[1] * f, m->s0[2] * f};
   }
   auto codeOf = [&](int l) -> const Code* { return l == 0 ? m->code0 : m->code[l - 1]->p; };
-  dim3 blk(BX, BY, BZ);
+  const dim3 blk(BX, BY, BZ);
   const int nu = m->smooth;
+  // every kernel of the V-cycle is a programmatic dependent launch: the launch
+  // of the next one overlaps the tail of this one
+  auto run = [&](auto kernel, dim3 grid, dim3 block, auto... args) {
+    check(launchPdl(kernel, grid, block, s, args...), "multigrid");
+    ++launches;
+  };
+  // a smoothing sweep (with the grid reduction of the CG's r.z when dot)
+  auto sweep = [&](auto kernel, const Dim3i& r, bool dot, auto... args) {
+    const SweepGrid g = sweepGrid(r, dot);
+    run(kernel, g.grid, blk, args..., g.zPer);
+  };
   // which ping-pong buffer holds the current iterate of each level
   std::vector<int> curBuf(L, 0);
   float* z0[2] = {m->z0a.p, m->z0b.p};
   // downward sweep
   for (int l = 0; l < L - 1; ++l) {
     if (l == 0) {
-      kJacobiFirst<float, float><<<gridOf(lv[0].r), blk, 0, s>>>(lv[0], r0, z0[0], codeOf(0), st);
+      run(kJacobiFirst<float, float>, gridOf(lv[0].r), blk, lv[0], r0, z0[0], codeOf(0), (const CgState*)st);
       int cb = 0;
       for (int k = 1; k < nu; ++k, cb ^= 1)
-        kJacobi<float, float, float, false, false><<<sweepGrid(lv[0].r, false).grid, blk, 0, s>>>(
-            lv[0], lv[0].r, r0, z0[cb], z0[cb ^ 1], nullptr, codeOf(0), nullptr, st, sweepGrid(lv[0].r, false).zPer);
+        sweep(kJacobi<float, float, float, false, false>, lv[0].r, false, lv[0], lv[0].r, r0, (const float*)z0[cb],
+              z0[cb ^ 1], (const float*)nullptr, codeOf(0), (double*)nullptr, st);
       curBuf[0] = cb;
-      kResidualRestrict<float, float, TS><<<gridOf(lv[1].r), blk, 0, s>>>(lv[0], lv[1].r, r0, z0[cb], codeOf(0), bL[1],
-                                                                           st);
-      launches += nu + 1;
+      run(kResidualRestrict<float, float, TS>, gridOf(lv[1].r), blk, lv[0], lv[1].r, r0, (const float*)z0[cb],
+          codeOf(0), bL[1], (const CgState*)st);
     } else {
       TS* zl[2] = {zaL[l], zbL[l]};
-      kJacobiFirst<TS, TS><<<gridOf(lv[l].r), blk, 0, s>>>(lv[l], bL[l], zl[0], codeOf(l), st);
+      run(kJacobiFirst<TS, TS>, gridOf(lv[l].r), blk, lv[l], (const TS*)bL[l], zl[0], codeOf(l), (const CgState*)st);
       int cb = 0;
       for (int k = 1; k < nu; ++k, cb ^= 1)
-        kJacobi<TS, TS, TS, false, false><<<sweepGrid(lv[l].r, false).grid, blk, 0, s>>>(lv[l], lv[l].r, bL[l], zl[cb],
-                                                                           zl[cb ^ 1], nullptr, codeOf(l), nullptr, st, sweepGrid(lv[l].r, false).zPer);
+        sweep(kJacobi<TS, TS, TS, false, false>, lv[l].r, false, lv[l], lv[l].r, (const TS*)bL[l], (const TS*)zl[cb],
+              zl[cb ^ 1], (const TS*)nullptr, codeOf(l), (double*)nullptr, st);
       curBuf[l] = cb;
-      kResidualRestrict<TS, TS, TS><<<gridOf(lv[l + 1].r), blk, 0, s>>>(lv[l], lv[l + 1].r, bL[l], zl[cb], codeOf(l),
-                                                                         bL[l + 1], st);
-      launches += nu + 1;
+      run(kResidualRestrict<TS, TS, TS>, gridOf(lv[l + 1].r), blk, lv[l], lv[l + 1].r, (const TS*)bL[l],
+          (const TS*)zl[cb], codeOf(l), bL[l + 1], (const CgState*)st);
     }
   }
   // coarsest
   {
     int l = L - 1;
-    if (l == 0) {
-      kCoarseSolve<float, float><<<1, 1024, 0, s>>>(lv[0], r0, z0[0], codeOf(0), st);
-      curBuf[0] = 0;
-    } else {
-      kCoarseSolve<TS, TS><<<1, 1024, 0, s>>>(lv[l], bL[l], zaL[l], codeOf(l), st);
-      curBuf[l] = 0;
-    }
-    launches += 1;
+    if (l == 0)
+      run(kCoarseSolve<float, float>, dim3(1), dim3(1024), lv[0], r0, z0[0], codeOf(0), (const CgState*)st);
+    else
+      run(kCoarseSolve<TS, TS>, dim3(1), dim3(1024), lv[l], (const TS*)bL[l], zaL[l], codeOf(l), (const CgState*)st);
+    curBuf[l] = 0;
   }
   // upward sweep: prolongation fused into the first post-smoothing sweep
   for (int l = L - 2; l >= 0; --l) {
@@ -420,39 +434,36 @@ const float* vcycleT(Multigrid* m, const float* r0, CgState* st, cudaStream_t s,
     if (l == 0) {
       int cb = curBuf[0];
       for (int k = 0; k < nu; ++k, cb ^= 1) {
-        bool last = k == nu - 1;
+        const bool last = k == nu - 1;
+        const float* zi = z0[cb];
         if (k == 0 && last)
-          kJacobi<float, float, TS, true, true><<<sweepGrid(lv[0].r, true).grid, blk, 0, s>>>(
-              lv[0], lv[1].r, r0, z0[cb], z0[cb ^ 1], zc, codeOf(0), m->partials.p, st, sweepGrid(lv[0].r, true).zPer);
+          sweep(kJacobi<float, float, TS, true, true>, lv[0].r, true, lv[0], lv[1].r, r0, zi, z0[cb ^ 1], zc,
+                codeOf(0), m->partials.p, st);
         else if (k == 0)
-          kJacobi<float, float, TS, true, false><<<sweepGrid(lv[0].r, false).grid, blk, 0, s>>>(
-              lv[0], lv[1].r, r0, z0[cb], z0[cb ^ 1], zc, codeOf(0), nullptr, st, sweepGrid(lv[0].r, false).zPer);
+          sweep(kJacobi<float, float, TS, true, false>, lv[0].r, false, lv[0], lv[1].r, r0, zi, z0[cb ^ 1], zc,
+                codeOf(0), (double*)nullptr, st);
         else if (last)
-          kJacobi<float, float, float, false, true><<<sweepGrid(lv[0].r, true).grid, blk, 0, s>>>(
-              lv[0], lv[0].r, r0, z0[cb], z0[cb ^ 1], nullptr, codeOf(0), m->partials.p, st, sweepGrid(lv[0].r, true).zPer);
+          sweep(kJacobi<float, float, float, false, true>, lv[0].r, true, lv[0], lv[0].r, r0, zi, z0[cb ^ 1],
+                (const float*)nullptr, codeOf(0), m->partials.p, st);
         else
-          kJacobi<float, float, float, false, false><<<sweepGrid(lv[0].r, false).grid, blk, 0, s>>>(
-              lv[0], lv[0].r, r0, z0[cb], z0[cb ^ 1], nullptr, codeOf(0), nullptr, st, sweepGrid(lv[0].r, false).zPer);
+          sweep(kJacobi<float, float, float, false, false>, lv[0].r, false, lv[0], lv[0].r, r0, zi, z0[cb ^ 1],
+                (const float*)nullptr, codeOf(0), (double*)nullptr, st);
       }
       curBuf[0] = cb;
-      launches += nu;
     } else {
       TS* zl[2] = {zaL[l], zbL[l]};
       int cb = curBuf[l];
       for (int k = 0; k < nu; ++k, cb ^= 1) {
         if (k == 0)
-          kJacobi<TS, TS, TS, true, false><<<sweepGrid(lv[l].r, false).grid, blk, 0, s>>>(lv[l], lv[l + 1].r, bL[l], zl[cb],
-                                                                            zl[cb ^ 1], zc, codeOf(l), nullptr, st, sweepGrid(lv[l].r, false).zPer);
+          sweep(kJacobi<TS, TS, TS, true, false>, lv[l].r, false, lv[l], lv[l + 1].r, (const TS*)bL[l],
+                (const TS*)zl[cb], zl[cb ^ 1], zc, codeOf(l), (double*)nullptr, st);
         else
-          kJacobi<TS, TS, TS, false, false><<<sweepGrid(lv[l].r, false).grid, blk, 0, s>>>(lv[l], lv[l].r, bL[l], zl[cb],
-                                                                             zl[cb ^ 1], nullptr, codeOf(l), nullptr,
-                                                                             st, sweepGrid(lv[l].r, false).zPer);
+          sweep(kJacobi<TS, TS, TS, false, false>, lv[l].r, false, lv[l], lv[l].r, (const TS*)bL[l],
+                (const TS*)zl[cb], zl[cb ^ 1], (const TS*)nullptr, codeOf(l), (double*)nullptr, st);
       }
       curBuf[l] = cb;
-      launches += nu;
     }
   }
-  check(cudaGetLastError(), "v-cycle");
   return z0[curBuf[0]];
 }
 }  // namespace

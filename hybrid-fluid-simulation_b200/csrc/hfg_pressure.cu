@@ -369,14 +369,7 @@ constexpr int kDirStages = 4, kUpdStages = 5;
 constexpr unsigned long long kWaitNs = 2000000000ull;  // a stage that takes 2 s to land is an error
 
 __device__ __forceinline__ uint32_t smemAddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-// Programmatic dependent launch: the CG kernels are launched so that they may
-// start while the kernel before them finishes; this wait (griddepcontrol.wait)
-// returns once that kernel has completed and its writes are visible, and
-// comes before the first read of anything it wrote.
-__device__ __forceinline__ void waitPrevGrid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-// Lets the next kernel of the stream be scheduled once every block of this one
-// has issued it (its blocks then wait in waitPrevGrid for this one to finish).
-__device__ __forceinline__ void allowNextGrid() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+
 __device__ __forceinline__ void mbarInit(uint64_t* bar, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smemAddr(bar)), "r"(count) : "memory");
 }
@@ -483,23 +476,6 @@ CgLaunch cgLaunch(const Dim3i& cg, K kernel) {
   L.zPer = bestPer;
   L.grid = dim3(bx, by, (cg.z + bestPer - 1) / bestPer);
   return L;
-}
-
-// Launch with programmatic stream serialization (the kernel calls
-// waitPrevGrid before reading what earlier work wrote).
-template <class... KP, class... A>
-cudaError_t launchPdl(void (*kernel)(KP...), dim3 grid, dim3 block, cudaStream_t s, A&&... args) {
-  cudaLaunchConfig_t cfg{};
-  cfg.gridDim = grid;
-  cfg.blockDim = block;
-  cfg.dynamicSmemBytes = 0;
-  cfg.stream = s;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
 }
 
 // CG direction: p = z + beta p_old (scal then axpy with 1), q = A p and the
