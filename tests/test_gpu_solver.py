@@ -314,3 +314,26 @@ def test_particle_mirror(cuda):
     g.set_particle_mirror(small)
     with pytest.raises(hfgrid.HfgError):
         g.update()
+
+
+@pytest.mark.parametrize("precond", [hfgrid.PRECOND_JACOBI, hfgrid.PRECOND_MG])
+def test_tiny_grid_few_particles(cuda, precond):
+    """Edge sizes for the warp- and cluster-level paths: a 6x5x7 grid (one
+    partial CG tile, a pitch of 16 with 10 padding columns, at most a couple
+    of multigrid levels) and a fluid box of a few cells with 2 particles per
+    cell, so particle arrays end inside the first warp.  Three steps must match
+    the FP64 oracle as the larger scenes do."""
+    sc = scenes.Scene(res=(6, 5, 7), fluid_max=(0.6, 0.6, 0.5), per_cell=2, seed=11)  # 24 particles
+    g = scenes.gpu_solver(sc, precond=precond, tol_mode=1, tol=1e-6, max_iter=400, advect_scalars=True)
+    assert 0 < g.num_particles < 32
+    o = oracle_twin(sc, g, 1, 1, 1, 1e-10, 5000)  # Jacobi-PCG in FP64, solved tighter
+    for _ in range(3):
+        g.update()
+        o.update()
+    gs, os_ = g.stats(), o.stats()
+    assert gs["substeps"] == os_["substeps"]
+    gp, gv = g.particles()
+    op, ov = o.particles()
+    assert np.abs(gp - op).max() < 3e-4
+    assert rel_l2(gv, ov) < 2e-3
+    assert vel_rel_l2(g.velocity_field(), o.velocity_field()) < 2e-3
