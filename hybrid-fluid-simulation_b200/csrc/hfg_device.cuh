@@ -131,12 +131,14 @@ __device__ __forceinline__ void axisWeights(float t, int n, AxisW& a) {
   a.j = min(max(i, -1), n - 1) + 1;
 }
 
-// Corner table of a face grid of nx x ny x nz values: (nx + 1) x (ny + 1) x nz
-// float4, entry (z, jy, jx) = (f[z][y0][x0], f[z][y0][x1], f[z][y1][x0],
-// f[z][y1][x1]) with x0 = clamp(jx - 1), x1 = clamp(jx), y0 = clamp(jy - 1),
-// y1 = clamp(jy).  Entry (AxisW::j of y, AxisW::j of x) of a sample holds the
-// four corners of one z layer of its trilinear stencil, so one 16-byte load
-// serves four corners.
+// Corner table of a face grid of nx x ny x nz values: (nx + 1) x (ny + 1) x
+// (nz + 2) float4, entry (L, jy, jx) = (f[z][y0][x0], f[z][y0][x1],
+// f[z][y1][x0], f[z][y1][x1]) with z = clamp(L - 1), x0 = clamp(jx - 1),
+// x1 = clamp(jx), y0 = clamp(jy - 1), y1 = clamp(jy).  Entry (AxisW::j of y,
+// AxisW::j of x) of a sample holds the four corners of one z layer of its
+// trilinear stencil, so one 16-byte load serves four corners; layers
+// AxisW::j and AxisW::j + 1 of z are the stencil's clamp(i) and clamp(i + 1),
+// because the padding layers 0 and nz + 1 repeat the end layers.
 struct FaceQuads {
   const float4* c[3];
 };
@@ -185,8 +187,9 @@ struct FaceSampler {
     const AxisW& Y = a == 1 ? fc[1] : cc[1];
     const AxisW& Z = a == 2 ? fc[2] : cc[2];
     unsigned lx = (unsigned)(g.r.x + (a == 0) + 1), ly = (unsigned)(g.r.y + (a == 1) + 1);
-    unsigned row = (unsigned)Y.j * lx + (unsigned)X.j, pl = lx * ly;
-    const float4 q0 = __ldg(Q + (unsigned)Z.i0 * pl + row), q1 = __ldg(Q + (unsigned)Z.i1 * pl + row);
+    unsigned pl = lx * ly;
+    const float4* q = Q + ((unsigned)Z.j * ly + (unsigned)Y.j) * lx + (unsigned)X.j;
+    const float4 q0 = __ldg(q), q1 = __ldg(q + pl);
     const float wx = X.w1, wy = Y.w1, wz = Z.w1;
     const float a00 = fmaf(wx, q0.y - q0.x, q0.x), a01 = fmaf(wx, q0.w - q0.z, q0.z);
     const float a10 = fmaf(wx, q1.y - q1.x, q1.x), a11 = fmaf(wx, q1.w - q1.z, q1.z);

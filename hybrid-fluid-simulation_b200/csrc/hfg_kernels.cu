@@ -29,6 +29,15 @@ inline int gridFor(long long n, int threads = kThreads, int perSM = 16) {
 #define HFG_FOR(i, n) \
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += (long long)gridDim.x * blockDim.x)
 
+// The same loop with an index of type I.  The particle kernels take I = int
+// when 3 n and n + the grid's thread count stay below 2^31, which saves the
+// 64-bit index and address arithmetic of every iteration.
+#define HFG_FOR_T(I, i, n) \
+  for (I i = (I)blockIdx.x * blockDim.x + threadIdx.x; i < (I)(n); i += (I)gridDim.x * blockDim.x)
+
+// True when a particle kernel over n particles may index in 32 bits.
+inline bool index32(long long n) { return 3 * n + (long long)numSMs() * 16 * kThreads < (1ll << 31); }
+
 __device__ inline void cellCoord(long long c, const Dim3i& r, int& x, int& y, int& z) {
   x = (int)(c % r.x);
   long long t = c / r.x;
@@ -991,13 +1000,14 @@ __device__ inline void blockMaxToGlobal(float m, unsigned int* dst);
 // (EulerParticles.cpp:249-251): one sampler per particle serves the PIC sample,
 // the FLIP difference and all three components.  The PIC sample comes from the
 // corner tables of vin and is also v0 of the substeps, with max |v0|.
+template <typename I>
 __global__ void kParticleVelUpdateLinear(Geom g, int mode, FaceQuads vinQ, ConstFaceField vin, ConstFaceField prev,
                                          int first, float mixing, const float* __restrict__ pos,
                                          float* __restrict__ vel, long long P, float* __restrict__ v0,
                                          SubstepState* st) {
   const float keep = (float)(1.0 - (double)mixing);
   float m = 0.f;
-  HFG_FOR(p, P) {
+  HFG_FOR_T(I, p, P) {
     FaceSampler fs(g, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]);
     float pic[3];
 #pragma unroll
@@ -1033,8 +1043,12 @@ cudaError_t launchParticleVelUpdate(const Geom& g, int mode, int alg, ConstFaceF
   switch (alg) {
     case LINEAR:
       if (!vinQ || !v0 || !st) return cudaErrorInvalidValue;
-      kParticleVelUpdateLinear<<<gr, kThreads, 0, s>>>(g, mode, *vinQ, vin, prev, firstFlip, mixing, pos, vel, P, v0,
-                                                       st);
+      if (index32(P))
+        kParticleVelUpdateLinear<int><<<gr, kThreads, 0, s>>>(g, mode, *vinQ, vin, prev, firstFlip, mixing, pos, vel,
+                                                              P, v0, st);
+      else
+        kParticleVelUpdateLinear<long long><<<gr, kThreads, 0, s>>>(g, mode, *vinQ, vin, prev, firstFlip, mixing, pos,
+                                                                    vel, P, v0, st);
       break;
     case QUADRATIC: kParticleVelUpdate<QUADRATIC><<<gr, kThreads, 0, s>>>(g, mode, vin, prev, firstFlip, mixing, pos, vel, P); break;
     case CUBIC: kParticleVelUpdate<CUBIC><<<gr, kThreads, 0, s>>>(g, mode, vin, prev, firstFlip, mixing, pos, vel, P); break;
@@ -1064,12 +1078,13 @@ __global__ void kFaceQuads(Dim3i r, ConstFaceField v, float4* q0, float4* q1, fl
   const int a = blockIdx.y;
   const unsigned nx = (unsigned)(r.x + (a == 0)), ny = (unsigned)(r.y + (a == 1)), nz = (unsigned)(r.z + (a == 2));
   const unsigned lx = nx + 1, ly = ny + 1;
-  const long long n = (long long)lx * ly * nz;
+  const long long n = (long long)lx * ly * (nz + 2);
   const float* __restrict__ f = a == 0 ? v.c[0] : (a == 1 ? v.c[1] : v.c[2]);
   float4* __restrict__ out = a == 0 ? q0 : (a == 1 ? q1 : q2);
   HFG_FOR(e, n) {
     const unsigned t = (unsigned)(e / lx), jx = (unsigned)(e - (long long)t * lx);
-    const unsigned z = t / ly, jy = t - z * ly;
+    const unsigned L = t / ly, jy = t - L * ly;
+    const unsigned z = L == 0 ? 0 : (L > nz ? nz - 1 : L - 1);
     const unsigned x0 = jx > 0 ? jx - 1 : 0, x1 = jx < nx ? jx : nx - 1;
     const unsigned y0 = jy > 0 ? jy - 1 : 0, y1 = jy < ny ? jy : ny - 1;
     const unsigned b0 = (z * ny + y0) * nx, b1 = (z * ny + y1) * nx;
@@ -1077,7 +1092,7 @@ __global__ void kFaceQuads(Dim3i r, ConstFaceField v, float4* q0, float4* q1, fl
   }
 }
 long long faceQuadCount(const Dim3i& r, int a) {
-  return (long long)(r.x + (a == 0) + 1) * (r.y + (a == 1) + 1) * (r.z + (a == 2));
+  return (long long)(r.x + (a == 0) + 1) * (r.y + (a == 1) + 1) * (r.z + (a == 2) + 2);
 }
 cudaError_t launchFaceQuads(const Dim3i& r, ConstFaceField v, float4* const out[3], cudaStream_t s) {
   long long n = faceQuadCount(r, 0);
@@ -1088,10 +1103,11 @@ cudaError_t launchFaceQuads(const Dim3i& r, ConstFaceField v, float4* const out[
 
 // First velocity sample of the substep loop (EulerParticles.cpp:249-251):
 // v0 = trilinear(vel, pos) and max |v0| over every component.
+template <typename I>
 __global__ void kSubstepBegin(Geom g, FaceQuads vel, const float* __restrict__ pos, float* __restrict__ v0,
                               long long P, SubstepState* st) {
   float m = 0.f;
-  HFG_FOR(p, P) {
+  HFG_FOR_T(I, p, P) {
     float v[3];
     sampleFaceQuads(vel, g, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2], v);
     v0[3 * p] = v[0]; v0[3 * p + 1] = v[1]; v0[3 * p + 2] = v[2];
@@ -1101,7 +1117,10 @@ __global__ void kSubstepBegin(Geom g, FaceQuads vel, const float* __restrict__ p
 }
 cudaError_t launchSubstepBegin(const Geom& g, FaceQuads vel, const float* pos, float* v0, long long P,
                                SubstepState* st, cudaStream_t s) {
-  kSubstepBegin<<<gridFor(P > 0 ? P : 1), kThreads, 0, s>>>(g, vel, pos, v0, P, st);
+  if (index32(P))
+    kSubstepBegin<int><<<gridFor(P > 0 ? P : 1), kThreads, 0, s>>>(g, vel, pos, v0, P, st);
+  else
+    kSubstepBegin<long long><<<gridFor(P > 0 ? P : 1), kThreads, 0, s>>>(g, vel, pos, v0, P, st);
   return cudaGetLastError();
 }
 
@@ -1124,6 +1143,7 @@ __device__ inline float substepSize(const SubstepState& s, float dt, float cfl, 
 // box clamp of fixParticlesPosWithBoundarys (EulerParticlesTool.cu:310-333) is
 // applied to the first `nclamp` particles; otherwise the next v0 and its max
 // are produced for slot+1.
+template <typename I>
 __global__ void __launch_bounds__(256, 4) kSubstep(Geom g, FaceQuads vel, float* __restrict__ pos,
                                                   float* __restrict__ v0, long long P,
                          int acc, float dt, float cfl, long long nclamp, SubstepState* st, int slot) {
@@ -1139,7 +1159,7 @@ __global__ void __launch_bounds__(256, 4) kSubstep(Geom g, FaceQuads vel, float*
   float half = (float)(0.5 * (double)ds), tq = (float)(0.75 * (double)ds);
   float a29 = (float)(2.0 / 9.0 * (double)ds), a39 = (float)(3.0 / 9.0 * (double)ds), a49 = (float)(4.0 / 9.0 * (double)ds);
   float m = 0.f;
-  HFG_FOR(p, P) {
+  HFG_FOR_T(I, p, P) {
     float q[3] = {pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]};
     float w0[3] = {v0[3 * p], v0[3 * p + 1], v0[3 * p + 2]};
     if (acc == 0) {
@@ -1172,7 +1192,7 @@ __global__ void __launch_bounds__(256, 4) kSubstep(Geom g, FaceQuads vel, float*
       for (int a = 0; a < 3; ++a) q[a] = fmaf(a49, w[a], acc3[a]);
     }
     if (last) {
-      if (p < nclamp) {  // the box bounds are formed here, from the kernel parameters
+      if ((long long)p < nclamp) {  // the box bounds are formed here, from the kernel parameters
         const float bmin[3] = {g.ox, g.oy, g.oz};
         const float bmax[3] = {g.ox + (float)g.r.x * g.hx, g.oy + (float)g.r.y * g.hy, g.oz + (float)g.r.z * g.hz};
 #pragma unroll
@@ -1195,7 +1215,11 @@ __global__ void __launch_bounds__(256, 4) kSubstep(Geom g, FaceQuads vel, float*
 }
 cudaError_t launchSubstep(const Geom& g, FaceQuads vel, float* pos, float* v0, long long P, int acc, float dt,
                           float cfl, long long nclamp, SubstepState* st, int slot, cudaStream_t s) {
-  kSubstep<<<gridFor(P > 0 ? P : 1), kThreads, 0, s>>>(g, vel, pos, v0, P, acc, dt, cfl, nclamp, st, slot);
+  if (index32(P))
+    kSubstep<int><<<gridFor(P > 0 ? P : 1), kThreads, 0, s>>>(g, vel, pos, v0, P, acc, dt, cfl, nclamp, st, slot);
+  else
+    kSubstep<long long><<<gridFor(P > 0 ? P : 1), kThreads, 0, s>>>(g, vel, pos, v0, P, acc, dt, cfl, nclamp, st,
+                                                                     slot);
   return cudaGetLastError();
 }
 

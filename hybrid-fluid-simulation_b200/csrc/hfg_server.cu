@@ -61,7 +61,7 @@ long long sceneBytes(const int res[3], long long particles, int boundaries, int 
   b += N * 2;                  // markers, solid index
   b += NC * (2 + 1 + 4 * 4);   // code, CG code, x, r, p x2
   b += F * 8 + N * 8;          // P2G accumulators (faces, cells)
-  b += ((nx + 2) * (ny + 1) * nz + (nx + 1) * (ny + 2) * nz + (nx + 1) * (ny + 1) * (nz + 1)) * 16;  // corner tables
+  b += ((nx + 2) * (ny + 1) * (nz + 2) + (nx + 1) * (ny + 2) * (nz + 2) + (nx + 1) * (ny + 1) * (nz + 3)) * 16;  // corner tables
   b += F * (2 + 4 + 1);        // extrapolation distance, list, neighbour masks
   b += N * 4 * (long long)boundaries;
   b += particles * (4 * 3 * 4 + 4);  // pos, vel, v0, vector scalars, scalar
