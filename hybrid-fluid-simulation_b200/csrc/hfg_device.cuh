@@ -477,16 +477,16 @@ __device__ inline bool gridBarrier(unsigned* count, unsigned* gen, unsigned* err
   return okS != 0;
 }
 
+// Asks L2 for the line holding *p ahead of its load (no register is held
+// while the line is fetched); p must lie inside an allocation.
+__device__ __forceinline__ void prefetchL2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 // Programmatic dependent launch.  A kernel launched with launchPdl may start
 // while the kernel before it in the stream finishes: waitPrevGrid
 // (griddepcontrol.wait) returns once that kernel has completed and its writes
 // are visible, and must come before the first read of anything earlier work
 // wrote.  allowNextGrid lets the next such kernel be scheduled once every
 // block of this one has issued it.
-// Asks L2 for the line holding *p ahead of its load (no register is held
-// while the line is fetched); p must lie inside an allocation.
-__device__ __forceinline__ void prefetchL2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
-
 __device__ __forceinline__ void waitPrevGrid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void allowNextGrid() { asm volatile("griddepcontrol.launch_dependents;" :::); }
 

@@ -564,16 +564,19 @@ __device__ __forceinline__ void extrapEntry(const Dim3i& r0, const Dim3i& r1, co
   v[i] = acc;
 }
 
+// Block shape of the layer pass: 512 threads, at most two blocks per SM
+// (fewer, larger blocks than 256 x 4 meet at the grid barriers sooner).
+constexpr int kExtrapThreads = 512, kExtrapPerSM = 2;
+
 // Layers 1 .. nums-1, persistent: a layer with more than kExtrapSmallLayer
 // faces is spread over the grid; a run of smaller consecutive layers is filled
 // by block 0 alone with block barriers between them.  Every block walks the
 // same layer bounds (sc.offsets), so all meet at the same grid barriers.
 // barWords: count, generation, error, deepest layer filled.
-__global__ void __launch_bounds__(256) kExtrapLayers(Dim3i r0, Dim3i r1, Dim3i r2, float* v0, float* v1, float* v2,
-                                                     unsigned off1, unsigned off2, const uint8_t* __restrict__ mask,
-                                                     const unsigned int* __restrict__ list,
-                                                     const unsigned int* __restrict__ offsets, int nums,
-                                                     unsigned* barWords) {
+__global__ void __launch_bounds__(kExtrapThreads)
+    kExtrapLayers(Dim3i r0, Dim3i r1, Dim3i r2, float* v0, float* v1, float* v2, unsigned off1, unsigned off2,
+                  const uint8_t* __restrict__ mask, const unsigned int* __restrict__ list,
+                  const unsigned int* __restrict__ offsets, int nums, unsigned* barWords) {
   unsigned* count = barWords;
   unsigned* gen = barWords + 1;
   unsigned* err = barWords + 2;
@@ -614,16 +617,17 @@ std::atomic<int> g_extrapUsers{0};
 void extrapUsers(int delta) { g_extrapUsers.fetch_add(delta); }
 
 // Layers 1 .. nums-1 in one cooperative launch: about one block per 8192
-// faces of the grids, at most two per SM, and at most an equal share of the
-// GPU's resident slots for this kernel among the registered users, so that the
-// grids of concurrent scenes always fit on the GPU together.
+// faces of the grids, at most kExtrapPerSM per SM, and at most an equal
+// share of the GPU's resident slots for this kernel among the registered
+// users, so that the grids of concurrent scenes always fit on the GPU
+// together.
 cudaError_t launchExtrapLayers(const Dim3i rc[3], float* const vals[3], const long long off[3], ExtrapScratch sc,
                                int nums, cudaStream_t s, long long* launches) {
   if (nums <= 1) return cudaSuccess;
   static std::atomic<int> perSM{0};
   if (perSM.load() == 0) {
     int v = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kExtrapLayers, kThreads, 0);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kExtrapLayers, kExtrapThreads, 0);
     if (e != cudaSuccess) return e;
     perSM.store(std::max(1, v));
   }
@@ -631,7 +635,8 @@ cudaError_t launchExtrapLayers(const Dim3i rc[3], float* const vals[3], const lo
   const long long share = std::max(1LL, slots / std::max(1, g_extrapUsers.load()));
   const long long faces = rc[0].size() + rc[1].size() + rc[2].size();
   const int blocks = (int)std::max(
-      1LL, std::min({(faces + 8191) / 8192, (long long)numSMs() * std::min(perSM.load(), 2), share}));
+      1LL,
+      std::min({(faces + 8191) / 8192, (long long)numSMs() * std::min(perSM.load(), kExtrapPerSM), share}));
   Dim3i r0 = rc[0], r1 = rc[1], r2 = rc[2];
   float *v0 = vals[0], *v1 = vals[1], *v2 = vals[2];
   unsigned o1 = (unsigned)off[1], o2 = (unsigned)off[2];
@@ -640,7 +645,8 @@ cudaError_t launchExtrapLayers(const Dim3i rc[3], float* const vals[3], const lo
   const unsigned int* offs = sc.offsets;
   unsigned* bar = extrapBarWords(sc);
   void* args[] = {&r0, &r1, &r2, &v0, &v1, &v2, &o1, &o2, &mask, &list, &offs, &nums, &bar};
-  cudaError_t e = cudaLaunchCooperativeKernel((const void*)kExtrapLayers, dim3(blocks), dim3(kThreads), args, 0, s);
+  cudaError_t e =
+      cudaLaunchCooperativeKernel((const void*)kExtrapLayers, dim3(blocks), dim3(kExtrapThreads), args, 0, s);
   if (e == cudaSuccess && launches) ++*launches;
   return e;
 }
