@@ -10,7 +10,8 @@
 //    children is air, else fluid if any child is fluid, else solid;
 //  * level operators: the same matrix-free 7-point stencil rebuilt from each
 //    level's markers with the scales dt / (rho h^2) of that level (h doubles);
-//  * smoothing: damped Jacobi (omega = 2/3), nu sweeps before and after;
+//  * smoothing: damped Jacobi (omega = 2/3), nu sweeps before and after; on
+//    level 0 each thread marches along z with the z neighbours in registers;
 //  * transfers: restriction = mean of the children's residuals, prolongation =
 //    piecewise-constant injection (the scaled transpose), so the V-cycle is a
 //    symmetric operator and plain CG applies;
@@ -203,6 +204,109 @@ SweepGrid sweepGrid(const Dim3i& r, bool reduce) {
   return SweepGrid{dim3(g.x, g.y, (g.z + zPer - 1) / zPer), zPer};
 }
 
+// The same sweep on level 0, marching along z: a 32 x 8 tile of threads
+// walks zLen planes, and the z neighbours come from registers (the value of
+// the plane below is the one just used as the centre, the plane above is
+// loaded one plane ahead and its stencil code two planes ahead).  The values
+// and the arithmetic are those of kJacobi, so the sweeps agree bit for bit;
+// only the order of the r.z partial sums differs.
+constexpr int MX = 32, MY = 8;
+template <class TC, bool CORR, bool DOT>
+__global__ void __launch_bounds__(MX* MY)
+    kJacobiZ(Lvl L, Dim3i rc, const float* __restrict__ b, const float* __restrict__ zi, float* __restrict__ zo,
+             const TC* __restrict__ zc, const Code* __restrict__ code, double* partials, CgState* st, int zLen) {
+  waitPrevGrid();
+  if (st->done) return;
+  allowNextGrid();
+  double rz = 0.0, dummy = 0.0;
+  const int x = blockIdx.x * MX + threadIdx.x, y = blockIdx.y * MY + threadIdx.y;
+  const int z0 = blockIdx.z * zLen, z1 = min(z0 + zLen, L.r.z);
+  if (x < L.r.x && y < L.r.y && z0 < z1) {
+    const unsigned pl = (unsigned)L.r.x * L.r.y;
+    auto par = [&](int i, int j, int k) { return ((unsigned)(k >> 1) * rc.y + (j >> 1)) * rc.x + (i >> 1); };
+    // iterate (with the coarse correction) at cell i of plane zz, 0 off the fluid
+    auto value = [&](unsigned i, int zz, Code ki) -> float {
+      if (!(ki & 1)) return 0.f;
+      float v = __ldg(zi + i);
+      if (CORR) v += ld(zc, par(x, y, zz));
+      return v;
+    };
+    unsigned c = ((unsigned)z0 * L.r.y + y) * L.r.x + x;
+    const Code kb0 = z0 > 0 ? code[c - pl] : (Code)0;
+    float vb = value(c - pl, z0 - 1, kb0);
+    Code k = code[c];
+    float vc = value(c, z0, k);
+    Code ka = z0 + 1 < L.r.z ? code[c + pl] : (Code)0;
+    for (int z = z0; z < z1; ++z, c += pl) {
+      const Code kaa = z + 2 < L.r.z ? code[c + 2 * pl] : (Code)0;
+      const float va = value(c + pl, z + 1, ka);
+      const float bv = __ldg(b + c);
+      float v = 0.f;
+      if (k & 1) {
+        auto zAt = [&](int d) -> float {
+          if (d == 4) return vb;
+          if (d == 5) return va;
+          int dx, dy, dz;
+          nbrOf(d, dx, dy, dz);
+          float w = __ldg(zi + c + dx + dy * L.r.x);
+          if (CORR) w += ld(zc, par(x + dx, y + dy, z));
+          return w;
+        };
+        float az = applyA(L, k, vc, zAt);
+        v = vc + kOmega * (bv - az) / diagOfC(k, L.sx, L.sy, L.sz);
+      }
+      zo[c] = v;
+      if (DOT) rz += (double)bv * (double)v;
+      vb = vc;
+      k = ka;
+      vc = va;
+      ka = kaa;
+    }
+  }
+  if (DOT) {
+    if (gridSum2(rz, dummy, partials, &st->ticket) && flatTid() == 0) {
+      if (st->iter == 0) {
+        st->rz = rz;
+        st->beta = 0.f;
+      } else {
+        st->beta = (float)(rz / st->rz);
+        st->rz = rz;
+      }
+      st->ticket = 0;
+    }
+  }
+}
+
+// kJacobiFirst on level 0 with the launch shape of kJacobiZ: z = omega b /
+// diag along a column of zLen planes.
+__global__ void __launch_bounds__(MX* MY)
+    kJacobiFirstZ(Lvl L, const float* __restrict__ b, float* __restrict__ z, const Code* __restrict__ code,
+                  const CgState* st, int zLen) {
+  waitPrevGrid();
+  if (st->done) return;
+  allowNextGrid();
+  const int x = blockIdx.x * MX + threadIdx.x, y = blockIdx.y * MY + threadIdx.y;
+  const int z0 = blockIdx.z * zLen, z1 = min(z0 + zLen, L.r.z);
+  if (x >= L.r.x || y >= L.r.y) return;
+  const unsigned pl = (unsigned)L.r.x * L.r.y;
+  unsigned c = ((unsigned)z0 * L.r.y + y) * L.r.x + x;
+#pragma unroll 4
+  for (int zz = z0; zz < z1; ++zz, c += pl) {
+    const Code k = code[c];
+    z[c] = (k & 1) ? kOmega * __ldg(b + c) / diagOfC(k, L.sx, L.sy, L.sz) : 0.f;
+  }
+}
+
+// Launch shape of the level-0 marching sweeps: enough z chunks for about 32
+// blocks per SM (8 or 64 per SM, and 128, were slower at 256^3).
+SweepGrid marchGrid(const Dim3i& r) {
+  const long long cols = (long long)((r.x + MX - 1) / MX) * ((r.y + MY - 1) / MY);
+  const long long want = (long long)numSMs() * 32;
+  const long long chunks = std::min<long long>(r.z, std::max<long long>(1, (want + cols - 1) / cols));
+  const int zLen = (int)((r.z + chunks - 1) / chunks);
+  return SweepGrid{dim3((r.x + MX - 1) / MX, (r.y + MY - 1) / MY, (r.z + zLen - 1) / zLen), zLen};
+}
+
 // Residual of level f restricted to level c: bc = mean over the children of
 // (b - A z).
 template <class TB, class TZ, class TBC>
@@ -323,7 +427,10 @@ Multigrid* mgCreate(const Dim3i& r, int levels, int smooth, bool half, cudaStrea
   m->z0b.alloc(N, s);
   m->p[0].alloc(N, s);
   m->p[1].alloc(N, s);
-  m->partials.alloc(std::max(cgPartialsNeeded(r), 2 * (int)(gridOf(r).x * gridOf(r).y * gridOf(r).z)), s);
+  const dim3 mg = marchGrid(r).grid;
+  m->partials.alloc(std::max({cgPartialsNeeded(r), 2 * (int)(gridOf(r).x * gridOf(r).y * gridOf(r).z),
+                              2 * (int)(mg.x * mg.y * mg.z)}),
+                    s);
   check(makeHaloMap(r, m->z0a.p, &m->zH[0]), "multigrid tensor map");
   check(makeHaloMap(r, m->z0b.p, &m->zH[1]), "multigrid tensor map");
   check(makeHaloMap(r, m->p[0].p, &m->pH[0]), "multigrid tensor map");
@@ -393,17 +500,20 @@ const float* vcycleT(Multigrid* m, const float* r0, CgState* st, cudaStream_t s,
     const SweepGrid g = sweepGrid(r, dot);
     run(kernel, g.grid, blk, args..., g.zPer);
   };
+  // a level-0 sweep marching along z
+  const SweepGrid mg0 = marchGrid(lv[0].r);
+  auto march = [&](auto kernel, auto... args) { run(kernel, mg0.grid, dim3(MX, MY), args..., mg0.zPer); };
   // which ping-pong buffer holds the current iterate of each level
   std::vector<int> curBuf(L, 0);
   float* z0[2] = {m->z0a.p, m->z0b.p};
   // downward sweep
   for (int l = 0; l < L - 1; ++l) {
     if (l == 0) {
-      run(kJacobiFirst<float, float>, gridOf(lv[0].r), blk, lv[0], r0, z0[0], codeOf(0), (const CgState*)st);
+      march(kJacobiFirstZ, lv[0], r0, z0[0], codeOf(0), (const CgState*)st);
       int cb = 0;
       for (int k = 1; k < nu; ++k, cb ^= 1)
-        sweep(kJacobi<float, float, float, false, false>, lv[0].r, false, lv[0], lv[0].r, r0, (const float*)z0[cb],
-              z0[cb ^ 1], (const float*)nullptr, codeOf(0), (double*)nullptr, st);
+        march(kJacobiZ<float, false, false>, lv[0], lv[0].r, r0, (const float*)z0[cb], z0[cb ^ 1],
+              (const float*)nullptr, codeOf(0), (double*)nullptr, st);
       curBuf[0] = cb;
       run(kResidualRestrict<float, float, TS>, gridOf(lv[1].r), blk, lv[0], lv[1].r, r0, (const float*)z0[cb],
           codeOf(0), bL[1], (const CgState*)st);
@@ -437,17 +547,15 @@ const float* vcycleT(Multigrid* m, const float* r0, CgState* st, cudaStream_t s,
         const bool last = k == nu - 1;
         const float* zi = z0[cb];
         if (k == 0 && last)
-          sweep(kJacobi<float, float, TS, true, true>, lv[0].r, true, lv[0], lv[1].r, r0, zi, z0[cb ^ 1], zc,
-                codeOf(0), m->partials.p, st);
+          march(kJacobiZ<TS, true, true>, lv[0], lv[1].r, r0, zi, z0[cb ^ 1], zc, codeOf(0), m->partials.p, st);
         else if (k == 0)
-          sweep(kJacobi<float, float, TS, true, false>, lv[0].r, false, lv[0], lv[1].r, r0, zi, z0[cb ^ 1], zc,
-                codeOf(0), (double*)nullptr, st);
+          march(kJacobiZ<TS, true, false>, lv[0], lv[1].r, r0, zi, z0[cb ^ 1], zc, codeOf(0), (double*)nullptr, st);
         else if (last)
-          sweep(kJacobi<float, float, float, false, true>, lv[0].r, true, lv[0], lv[0].r, r0, zi, z0[cb ^ 1],
-                (const float*)nullptr, codeOf(0), m->partials.p, st);
+          march(kJacobiZ<float, false, true>, lv[0], lv[0].r, r0, zi, z0[cb ^ 1], (const float*)nullptr, codeOf(0),
+                m->partials.p, st);
         else
-          sweep(kJacobi<float, float, float, false, false>, lv[0].r, false, lv[0], lv[0].r, r0, zi, z0[cb ^ 1],
-                (const float*)nullptr, codeOf(0), (double*)nullptr, st);
+          march(kJacobiZ<float, false, false>, lv[0], lv[0].r, r0, zi, z0[cb ^ 1], (const float*)nullptr, codeOf(0),
+                (double*)nullptr, st);
       }
       curBuf[0] = cb;
     } else {
