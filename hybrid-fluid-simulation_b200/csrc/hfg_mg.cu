@@ -298,13 +298,23 @@ __global__ void __launch_bounds__(MX* MY)
 }
 
 // Launch shape of the level-0 marching sweeps: enough z chunks for about 32
-// blocks per SM (8 or 64 per SM, and 128, were slower at 256^3).
+// blocks per SM (8 or 64 per SM, and 128, were slower at 256^3), but columns
+// of at least 4 planes (shorter ones re-load more of their neighbours than
+// they save; with concurrent scenes every load counts).
 SweepGrid marchGrid(const Dim3i& r) {
   const long long cols = (long long)((r.x + MX - 1) / MX) * ((r.y + MY - 1) / MY);
   const long long want = (long long)numSMs() * 32;
-  const long long chunks = std::min<long long>(r.z, std::max<long long>(1, (want + cols - 1) / cols));
+  const long long chunks = std::min<long long>((r.z + 3) / 4, std::max<long long>(1, (want + cols - 1) / cols));
   const int zLen = (int)((r.z + chunks - 1) / chunks);
   return SweepGrid{dim3((r.x + MX - 1) / MX, (r.y + MY - 1) / MY, (r.z + zLen - 1) / zLen), zLen};
+}
+
+// Level 0 marches when that still gives two blocks per SM; smaller grids (64^3
+// and below) keep the per-cell sweeps, whose many short blocks hide latency
+// better there.
+bool marchLevel0(const Dim3i& r) {
+  const dim3 g = marchGrid(r).grid;
+  return (long long)g.x * g.y * g.z >= 2LL * numSMs();
 }
 
 // Residual of level f restricted to level c: bc = mean over the children of
@@ -502,6 +512,7 @@ const float* vcycleT(Multigrid* m, const float* r0, CgState* st, cudaStream_t s,
   };
   // a level-0 sweep marching along z
   const SweepGrid mg0 = marchGrid(lv[0].r);
+  const bool marching = marchLevel0(lv[0].r);
   auto march = [&](auto kernel, auto... args) { run(kernel, mg0.grid, dim3(MX, MY), args..., mg0.zPer); };
   // which ping-pong buffer holds the current iterate of each level
   std::vector<int> curBuf(L, 0);
@@ -509,11 +520,19 @@ const float* vcycleT(Multigrid* m, const float* r0, CgState* st, cudaStream_t s,
   // downward sweep
   for (int l = 0; l < L - 1; ++l) {
     if (l == 0) {
-      march(kJacobiFirstZ, lv[0], r0, z0[0], codeOf(0), (const CgState*)st);
+      if (marching)
+        march(kJacobiFirstZ, lv[0], r0, z0[0], codeOf(0), (const CgState*)st);
+      else
+        run(kJacobiFirst<float, float>, gridOf(lv[0].r), blk, lv[0], r0, z0[0], codeOf(0), (const CgState*)st);
       int cb = 0;
-      for (int k = 1; k < nu; ++k, cb ^= 1)
-        march(kJacobiZ<float, false, false>, lv[0], lv[0].r, r0, (const float*)z0[cb], z0[cb ^ 1],
-              (const float*)nullptr, codeOf(0), (double*)nullptr, st);
+      for (int k = 1; k < nu; ++k, cb ^= 1) {
+        if (marching)
+          march(kJacobiZ<float, false, false>, lv[0], lv[0].r, r0, (const float*)z0[cb], z0[cb ^ 1],
+                (const float*)nullptr, codeOf(0), (double*)nullptr, st);
+        else
+          sweep(kJacobi<float, float, float, false, false>, lv[0].r, false, lv[0], lv[0].r, r0, (const float*)z0[cb],
+                z0[cb ^ 1], (const float*)nullptr, codeOf(0), (double*)nullptr, st);
+      }
       curBuf[0] = cb;
       run(kResidualRestrict<float, float, TS>, gridOf(lv[1].r), blk, lv[0], lv[1].r, r0, (const float*)z0[cb],
           codeOf(0), bL[1], (const CgState*)st);
@@ -546,7 +565,20 @@ const float* vcycleT(Multigrid* m, const float* r0, CgState* st, cudaStream_t s,
       for (int k = 0; k < nu; ++k, cb ^= 1) {
         const bool last = k == nu - 1;
         const float* zi = z0[cb];
-        if (k == 0 && last)
+        if (!marching) {
+          if (k == 0 && last)
+            sweep(kJacobi<float, float, TS, true, true>, lv[0].r, true, lv[0], lv[1].r, r0, zi, z0[cb ^ 1], zc,
+                  codeOf(0), m->partials.p, st);
+          else if (k == 0)
+            sweep(kJacobi<float, float, TS, true, false>, lv[0].r, false, lv[0], lv[1].r, r0, zi, z0[cb ^ 1], zc,
+                  codeOf(0), (double*)nullptr, st);
+          else if (last)
+            sweep(kJacobi<float, float, float, false, true>, lv[0].r, true, lv[0], lv[0].r, r0, zi, z0[cb ^ 1],
+                  (const float*)nullptr, codeOf(0), m->partials.p, st);
+          else
+            sweep(kJacobi<float, float, float, false, false>, lv[0].r, false, lv[0], lv[0].r, r0, zi, z0[cb ^ 1],
+                  (const float*)nullptr, codeOf(0), (double*)nullptr, st);
+        } else if (k == 0 && last)
           march(kJacobiZ<TS, true, true>, lv[0], lv[1].r, r0, zi, z0[cb ^ 1], zc, codeOf(0), m->partials.p, st);
         else if (k == 0)
           march(kJacobiZ<TS, true, false>, lv[0], lv[1].r, r0, zi, z0[cb ^ 1], zc, codeOf(0), (double*)nullptr, st);

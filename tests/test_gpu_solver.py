@@ -130,6 +130,25 @@ def test_multigrid_pcg(cuda, half):
     assert vel_rel_l2(g.velocity_field(), o.velocity_field()) < 1e-3
 
 
+@pytest.mark.parametrize("half", [1, 0])
+def test_multigrid_marching_sweeps(cuda, half):
+    """Level-0 sweeps that march along z (a grid with enough tile columns for
+    two blocks per SM: 72 x 44 x 78, so partial tiles in x and y, x padding
+    and a short last z chunk) against the Jacobi-PCG solve of the same step,
+    both to rel 1e-6: markers equal, projected velocity within 1e-4, and the
+    multigrid CG converging in few iterations."""
+    sc = small_scene((72, 44, 78))
+    g = scenes.gpu_solver(sc, precond=hfgrid.PRECOND_MG, tol_mode=1, tol=1e-6, max_iter=200, mg_half=half)
+    j = scenes.gpu_solver(sc, precond=hfgrid.PRECOND_JACOBI, tol_mode=1, tol=1e-6, max_iter=3000)
+    g.update()
+    j.update()
+    sg, sj = g.stats(), j.stats()
+    assert sg["cg_converged"] == 1 and sj["cg_converged"] == 1
+    assert sg["cg_iterations"] < 30
+    assert np.array_equal(g.markers(), j.markers())
+    assert vel_rel_l2(g.velocity_field(), j.velocity_field()) < 1e-4
+
+
 def test_semi_lagrangian_solver(cuda):
     sc = small_scene((16, 14, 12))
     g = scenes.gpu_solver(sc, precond=1, tol_mode=1, tol=1e-7, max_iter=500, advect_scalars=True,
