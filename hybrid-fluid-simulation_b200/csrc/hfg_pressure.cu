@@ -311,20 +311,25 @@ cudaError_t launchDivergenceNorm(const Geom& g, ConstFaceField v, const SolidVel
 namespace {
 // ---------------------------------------------------------------------------
 // Fast row of A for the CG: the diagonal and its reciprocal come from a
-// 64-entry table per launch (indexed by the six "not solid" bits; the entries
-// are summed in the reference's order), the six off-diagonal terms are FP32
-// FMAs on the neighbour values.
+// 128-entry table per launch, indexed by the whole 7-bit CG code (fluid bit
+// and the six "not solid" bits; the entries are summed in the reference's
+// order), and the six off-diagonal terms are FP32 FMAs on the neighbour
+// values.  The entries of the non-fluid codes are 1, so that the Jacobi
+// preconditioner needs no test of the fluid bit (r * 1 = r).
 struct DiagTab {
-  float d[64], inv[64];
+  float d[128], inv[128];
 };
 
 __device__ __forceinline__ void buildDiagTab(DiagTab& t, float sx, float sy, float sz) {
   const int tid = flatTid();
-  if (tid < 64) {
-    Code k = (Code)(1 | (tid << 1));
-    float d = diagOf(k, sx, sy, sz);
+  if (tid < 128) {
+    float d = 1.f, inv = 1.f;
+    if (tid & 1) {
+      d = diagOf((Code)tid, sx, sy, sz);
+      inv = d != 0.f ? 1.0f / d : 0.f;
+    }
     t.d[tid] = d;
-    t.inv[tid] = d != 0.f ? 1.0f / d : 0.f;
+    t.inv[tid] = inv;
   }
 }
 
@@ -337,7 +342,7 @@ __device__ __forceinline__ void buildDiagTab(DiagTab& t, float sx, float sy, flo
 // off-diagonal terms, and the sum is the masked sum up to the sign of a zero.
 __device__ __forceinline__ float fastRow(const DiagTab& t, CgCode k, float sx, float sy, float sz, float vc, float vl,
                                          float vr, float vd, float vu, float vb, float vf) {
-  float q = t.d[(k >> 1) & 63] * vc;
+  float q = t.d[k] * vc;
   q = fmaf(-sx, vl + vr, q);
   q = fmaf(-sy, vd + vu, q);
   q = fmaf(-sz, vb + vf, q);
@@ -347,7 +352,7 @@ __device__ __forceinline__ float fastRow(const DiagTab& t, CgCode k, float sx, f
 template <int PC>
 __device__ __forceinline__ float fastZ(const DiagTab& t, CgCode k, float rv) {
   if (PC != 1) return rv;
-  return (k & 1) ? rv * t.inv[(k >> 1) & 63] : rv;
+  return rv * t.inv[k];
 }
 
 // ---------------------------------------------------------------------------
