@@ -317,7 +317,7 @@ namespace {
 // values.  The entries of the non-fluid codes are 1, so that the Jacobi
 // preconditioner needs no test of the fluid bit (r * 1 = r).
 struct DiagTab {
-  float d[128], inv[128];
+  float2 e[128];  // (diagonal, its reciprocal)
 };
 
 __device__ __forceinline__ void buildDiagTab(DiagTab& t, float sx, float sy, float sz) {
@@ -328,31 +328,34 @@ __device__ __forceinline__ void buildDiagTab(DiagTab& t, float sx, float sy, flo
       d = diagOf((Code)tid, sx, sy, sz);
       inv = d != 0.f ? 1.0f / d : 0.f;
     }
-    t.d[tid] = d;
-    t.inv[tid] = inv;
+    t.e[tid] = make_float2(d, inv);
   }
 }
 
-// The neighbour values need no masks here.  The CG vectors p, r and z are
-// zero at every cell that is not fluid: b is zero there, the row of A is the
-// identity, and the Jacobi and multigrid preconditioners write zero there, so
-// r -= alpha A p and p = z + beta p keep them zero.  The halo outside the
-// grid arrives zero-filled and the pitch padding is zero too.  So the only
-// neighbours that add anything are the fluid ones, as in the reference's
-// off-diagonal terms, and the sum is the masked sum up to the sign of a zero.
-__device__ __forceinline__ float fastRow(const DiagTab& t, CgCode k, float sx, float sy, float sz, float vc, float vl,
-                                         float vr, float vd, float vu, float vb, float vf) {
-  float q = t.d[k] * vc;
+// Row sum of A at a fluid cell: d vc minus the six off-diagonal terms, d the
+// diagonal of the cell's code.  The neighbour values need no masks here.  The
+// CG vectors p, r and z are zero at every cell that is not fluid: b is zero
+// there, the row of A is the identity, and the Jacobi and multigrid
+// preconditioners write zero there, so r -= alpha A p and p = z + beta p keep
+// them zero.  The halo outside the grid arrives zero-filled and the pitch
+// padding is zero too.  So the only neighbours that add anything are the
+// fluid ones, as in the reference's off-diagonal terms, and the sum is the
+// masked sum up to the sign of a zero.  At a non-fluid cell (d = 1) the sum
+// is not the identity row: kCgUpdate selects vc there, and kCgDirection only
+// uses the row times vc, which is zero there.
+__device__ __forceinline__ float rowSum(float d, float sx, float sy, float sz, float vc, float vl, float vr, float vd,
+                                        float vu, float vb, float vf) {
+  float q = d * vc;
   q = fmaf(-sx, vl + vr, q);
   q = fmaf(-sy, vd + vu, q);
   q = fmaf(-sz, vb + vf, q);
-  return (k & 1) ? q : vc;
+  return q;
 }
 
 template <int PC>
-__device__ __forceinline__ float fastZ(const DiagTab& t, CgCode k, float rv) {
+__device__ __forceinline__ float fastZ(float inv, float rv) {
   if (PC != 1) return rv;
-  return rv * t.inv[k];
+  return rv * inv;
 }
 
 // ---------------------------------------------------------------------------
@@ -534,7 +537,7 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
   bool in[RY];
   unsigned c[RY];
   float below[RY], cur[RY], above[RY];
-  CgCode kCur[RY], kAbove[RY];
+  float dCur[RY], dAbove[RY];
 #pragma unroll
   for (int j = 0; j < RY; ++j) {
     const int y = y0 + ty + j * CTY;
@@ -544,21 +547,22 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
     below[j] = 0.f;
     if (in[j] && z0 > 0) {
       unsigned b = c[j] - plane;
-      below[j] = fmaf(beta, __ldg(pOld + b), fastZ<PC>(tab, __ldg(code + b), __ldg(zr + b)));
+      below[j] = fmaf(beta, __ldg(pOld + b), fastZ<PC>(tab.e[__ldg(code + b)].y, __ldg(zr + b)));
     }
   }
   // p of stage i's plane into tile t: the thread's RY cells, the x halo of its
-  // rows and, for the edge warps, the y halo rows; own p and codes returned
-  auto formTile = [&](int i, float (*t)[CTX + 2], float* v, CgCode* kOwn) {
+  // rows and, for the edge warps, the y halo rows; own p and diagonals returned
+  auto formTile = [&](int i, float (*t)[CTX + 2], float* v, float* dOwn) {
     const DirStage& S = stg[i % kDirStages];
     auto pAt = [&](int row, int colF, int colC) {
-      return fmaf(beta, S.po[row][colF], fastZ<PC>(tab, S.code[row][colC], S.r[row][colF]));
+      return fmaf(beta, S.po[row][colF], fastZ<PC>(tab.e[S.code[row][colC]].y, S.r[row][colF]));
     };
 #pragma unroll
     for (int j = 0; j < RY; ++j) {
       const int row = ty + 1 + j * CTY;
-      v[j] = pAt(row, tx + HXF, tx + HXC);
-      kOwn[j] = S.code[row][tx + HXC];
+      const float2 e = tab.e[S.code[row][tx + HXC]];
+      v[j] = fmaf(beta, S.po[row][tx + HXF], fastZ<PC>(e.y, S.r[row][tx + HXF]));
+      dOwn[j] = e.x;
       t[row][tx + 1] = v[j];
     }
     // the halo ring, one warp-wide pass per side: warps 0 and CTY-1 take the
@@ -573,7 +577,7 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
     }
   };
   bool ok = mbarWait(&bar[0], 0, deadline);
-  if (ok) formTile(0, pt[0], cur, kCur);
+  if (ok) formTile(0, pt[0], cur, dCur);
   int waited = 1;
   bool fail = __syncthreads_or(!ok);
   if (!fail && tid == 0 && kDirStages < nLoad) issue(kDirStages), issued = kDirStages + 1;
@@ -581,20 +585,21 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
   for (int i = 0; i < nPlanes && !fail; ++i) {
     ok = mbarWait(&bar[(i + 1) % kDirStages], (unsigned)(((i + 1) / kDirStages) & 1), deadline);
     waited = i + 2;
-    if (ok) formTile(i + 1, pt[(i + 1) & 1], above, kAbove);
+    if (ok) formTile(i + 1, pt[(i + 1) & 1], above, dAbove);
     float (*t)[CTX + 2] = pt[i & 1];
 #pragma unroll
     for (int j = 0; j < RY; ++j) {
       if (in[j] && ok) {
         const int row = ty + 1 + j * CTY;
-        float q = fastRow(tab, kCur[j], sx, sy, sz, cur[j], t[row][tx], t[row][tx + 2], t[row - 1][tx + 1],
-                          t[row + 1][tx + 1], below[j], above[j]);
+        // cur is zero off the fluid, so cur * q adds nothing there whatever q is
+        float q = rowSum(dCur[j], sx, sy, sz, cur[j], t[row][tx], t[row][tx + 2], t[row - 1][tx + 1],
+                         t[row + 1][tx + 1], below[j], above[j]);
         pNew[c[j]] = cur[j];
         acc = fmaf(cur[j], q, acc);
       }
       below[j] = cur[j];
       cur[j] = above[j];
-      kCur[j] = kAbove[j];
+      dCur[j] = dAbove[j];
       c[j] += plane;
     }
     fail = __syncthreads_or(!ok);
@@ -692,10 +697,12 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
       float above = ok ? A.p[row][tx + HXF] : 0.f;
       if (in[j] && ok) {
         CgCode k = S.code[ir][tx];
+        const float2 e = tab.e[k];
         float rv = S.r[ir][tx];
         if (!skip) {
-          float q = fastRow(tab, k, sx, sy, sz, cur[j], S.p[row][tx + HXF - 1], S.p[row][tx + HXF + 1],
-                            S.p[row - 1][tx + HXF], S.p[row + 1][tx + HXF], below[j], above);
+          float q = rowSum(e.x, sx, sy, sz, cur[j], S.p[row][tx + HXF - 1], S.p[row][tx + HXF + 1],
+                           S.p[row - 1][tx + HXF], S.p[row + 1][tx + HXF], below[j], above);
+          q = (k & 1) ? q : cur[j];
           if (sizeof(TX) == 8)  // FP64 accumulation: x + alpha p, each operation rounded once
             xv[c[j]] = (TX)__dadd_rn((double)S.x[ir][tx], __dmul_rn((double)alpha, (double)cur[j]));
           else
@@ -703,7 +710,7 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
           rv = fmaf(-alpha, q, rv);
           r[c[j]] = rv;
         }
-        float zz = fastZ<PC>(tab, k, rv);
+        float zz = fastZ<PC>(e.y, rv);
         arr = fmaf(rv, rv, arr);
         arz = fmaf(rv, zz, arz);
       }
