@@ -451,7 +451,7 @@ struct CgLaunch {
 
 // Tiles over (x, y), z split into chunks so that the blocks fill whole waves
 // of the resident slots (wave count x chunk length minimal, chunks of at
-// least 4 planes).
+// least 3 planes).
 int residentBlocks(const void* kernel) {
   static std::mutex mu;
   static std::map<const void*, int> cache;
@@ -473,10 +473,11 @@ CgLaunch cgLaunch(const Dim3i& cg, K kernel) {
   long long tiles = (long long)bx * by;
   long long best = -1;
   int bestPer = cg.z;
-  // chunks of at least 4 planes: on small grids (64^3) one-plane chunks pay
-  // the ring's fill and a block's set-up for every plane (16.1 against 15.3
-  // us per iteration at 64^3; 8 planes: 19.2)
-  for (int zPer = std::min(4, cg.z); zPer <= cg.z; ++zPer) {
+  // chunks of at least 3 planes: on small grids one-plane chunks pay the
+  // ring's fill and a block's set-up for every plane (64^3: 16.1 us per
+  // iteration with 1 plane, 15.2 with 3, 15.3 with 4, 19.2 with 8; 96^3:
+  // 22.3 with 3, 24.1 with 4)
+  for (int zPer = std::min(3, cg.z); zPer <= cg.z; ++zPer) {
     long long zc = (cg.z + zPer - 1) / zPer;
     long long waves = (tiles * zc + slots - 1) / slots;
     long long cost = waves * (zPer + 2);  // +2: pipeline fill per block
