@@ -35,10 +35,6 @@ inline int gridFor(long long n, int threads = kThreads, int perSM = 16) {
 #define HFG_FOR_T(I, i, n) \
   for (I i = (I)blockIdx.x * blockDim.x + threadIdx.x; i < (I)(n); i += (I)gridDim.x * blockDim.x)
 
-// Iterations ahead at which the particle kernels prefetch their streams.
-#ifndef HFG_PF_AHEAD
-#define HFG_PF_AHEAD 1
-#endif
 
 // True when a particle kernel over n particles may index in 32 bits.
 inline bool index32(long long n) { return 3 * n + (long long)numSMs() * 16 * kThreads < (1ll << 31); }
@@ -1020,9 +1016,9 @@ __global__ void kParticleVelUpdateLinear(Geom g, int mode, FaceQuads vinQ, Const
   const I stride = (I)gridDim.x * blockDim.x;
   float m = 0.f;
   HFG_FOR_T(I, p, P) {
-    if (p + HFG_PF_AHEAD * stride < (I)P) {
-      prefetchL2(pos + 3 * (p + HFG_PF_AHEAD * stride));
-      prefetchL2(vel + 3 * (p + HFG_PF_AHEAD * stride));
+    if (p + stride < (I)P) {  // the next iteration's lines (two or four ahead gained less)
+      prefetchL2(pos + 3 * (p + stride));
+      prefetchL2(vel + 3 * (p + stride));
     }
     FaceSampler fs(g, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]);
     float pic[3];
@@ -1179,9 +1175,9 @@ __global__ void __launch_bounds__(256, 4) kSubstep(Geom g, FaceQuads vel, float*
   HFG_FOR_T(I, p, P) {
     // the stream loads of a later iteration are DRAM misses; ask for them now
     // so that the chain of samples below does not start with one
-    if (p + HFG_PF_AHEAD * stride < (I)P) {
-      prefetchL2(pos + 3 * (p + HFG_PF_AHEAD * stride));
-      prefetchL2(v0 + 3 * (p + HFG_PF_AHEAD * stride));
+    if (p + stride < (I)P) {
+      prefetchL2(pos + 3 * (p + stride));
+      prefetchL2(v0 + 3 * (p + stride));
     }
     float q[3] = {pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]};
     float w0[3] = {v0[3 * p], v0[3 * p + 1], v0[3 * p + 2]};
