@@ -536,6 +536,8 @@ HFG_API int hfg_op_project(const int res[3], const float spacing[3], float dt, c
     check(launchRhsInit(g, v, sv, none, markers, code.p, sx, sy, sz, nullptr, r.p, x.p, false, p0.p, part.p, cs.p,
                         init.precond, s),
           "rhs");
+    // the CG kernels never store at non-fluid cells: both directions start zero
+    check(cudaMemsetAsync(p1.p, 0, sizeof(float) * NC, s), "memset");
     CgState host{};
     float* pb[2] = {p0.p, p1.p};
     int it = 0;

@@ -643,7 +643,10 @@ void mgSetup(Multigrid* m, const Dim3i& r, const uint8_t* mk0, const Code* code,
 void mgRunCg(Multigrid* m, const Dim3i& cg, float sx, float sy, float sz, const CgMaps& maps, const CgCode* code, void* x,
              bool xDouble, float* rvec, CgState* st, CgState* stHost, cudaStream_t s, long long& launches,
              const std::function<cudaGraphExec_t(const std::function<void()>&)>& capture, cudaGraphExec_t* chunk) {
+  // both direction buffers start zero: the CG kernels never store at non-fluid
+  // cells, and the fluid moves between solves
   check(cudaMemsetAsync(m->p[0].p, 0, m->p[0].bytes(), s), "memset");
+  check(cudaMemsetAsync(m->p[1].p, 0, m->p[1].bytes(), s), "memset");
   const float* z0 = mgVcycle(m, rvec, st, s, launches);  // z0 = V(b), rz = b.z0
   const int kChunk = 4;  // even: every chunk starts on p[0]
   auto body = [&] {

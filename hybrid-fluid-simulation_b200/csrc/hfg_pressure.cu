@@ -314,8 +314,9 @@ namespace {
 // 128-entry table per launch, indexed by the whole 7-bit CG code (fluid bit
 // and the six "not solid" bits; the entries are summed in the reference's
 // order), and the six off-diagonal terms are FP32 FMAs on the neighbour
-// values.  The entries of the non-fluid codes are 1, so that the Jacobi
-// preconditioner needs no test of the fluid bit (r * 1 = r).
+// values.  The non-fluid codes hold (-1, 1): the Jacobi preconditioner then
+// needs no test of the fluid bit (r * 1 = r), and a negative diagonal marks
+// a non-fluid cell (a fluid diagonal is a sum of positive scales, or 0).
 struct DiagTab {
   float2 e[128];  // (diagonal, its reciprocal)
 };
@@ -323,7 +324,7 @@ struct DiagTab {
 __device__ __forceinline__ void buildDiagTab(DiagTab& t, float sx, float sy, float sz) {
   const int tid = flatTid();
   if (tid < 128) {
-    float d = 1.f, inv = 1.f;
+    float d = -1.f, inv = 1.f;
     if (tid & 1) {
       d = diagOf((Code)tid, sx, sy, sz);
       inv = d != 0.f ? 1.0f / d : 0.f;
@@ -340,9 +341,10 @@ __device__ __forceinline__ void buildDiagTab(DiagTab& t, float sx, float sy, flo
 // them zero.  The halo outside the grid arrives zero-filled and the pitch
 // padding is zero too.  So the only neighbours that add anything are the
 // fluid ones, as in the reference's off-diagonal terms, and the sum is the
-// masked sum up to the sign of a zero.  At a non-fluid cell (d = 1) the sum
-// is not the identity row: kCgUpdate selects vc there, and kCgDirection only
-// uses the row times vc, which is zero there.
+// masked sum up to the sign of a zero.  At a non-fluid cell the row is the
+// identity and every CG vector stays zero for the whole solve (the RHS kernel
+// zeroes x, r and p there, and the updates add alpha or beta times zero), so
+// the CG kernels neither form the row nor store anything there.
 __device__ __forceinline__ float rowSum(float d, float sx, float sy, float sz, float vc, float vl, float vr, float vd,
                                         float vu, float vb, float vf) {
   float q = d * vc;
@@ -594,9 +596,8 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
     float (*t)[CTX + 2] = pt[i & 1];
 #pragma unroll
     for (int j = 0; j < RY; ++j) {
-      if (in[j] && ok) {
+      if (in[j] && ok && dCur[j] >= 0.f) {  // fluid cells only
         const int row = ty + 1 + j * CTY;
-        // cur is zero off the fluid, so cur * q adds nothing there whatever q is
         float q = rowSum(dCur[j], sx, sy, sz, cur[j], t[row][tx], t[row][tx + 2], t[row - 1][tx + 1],
                          t[row + 1][tx + 1], below[j], above[j]);
         pNew[c[j]] = cur[j];
@@ -704,10 +705,9 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
         CgCode k = S.code[ir][tx];
         const float2 e = tab.e[k];
         float rv = S.r[ir][tx];
-        if (!skip) {
+        if (!skip && (k & 1)) {  // x, r and z stay zero off the fluid
           float q = rowSum(e.x, sx, sy, sz, cur[j], S.p[row][tx + HXF - 1], S.p[row][tx + HXF + 1],
                            S.p[row - 1][tx + HXF], S.p[row + 1][tx + HXF], below[j], above);
-          q = (k & 1) ? q : cur[j];
           if (sizeof(TX) == 8)  // FP64 accumulation: x + alpha p, each operation rounded once
             xv[c[j]] = (TX)__dadd_rn((double)S.x[ir][tx], __dmul_rn((double)alpha, (double)cur[j]));
           else

@@ -575,6 +575,9 @@ void GridSolver::computePressure() {
                          xDouble(),
                          cgp_[0].p, partials_.p, cgState_.p, init.precond, stream_),
            "rhs");
+  // the CG kernels never store at non-fluid cells, and the fluid moves between
+  // solves: the second direction buffer starts zero too
+  check(cudaMemsetAsync(cgp_[1].p, 0, cgp_[1].bytes(), stream_), "memset");
   if (opt_.precond == HFG_PRECOND_MG) mgSetup(mg_, g_.r, markers_.p, code_.p, sx, sy, sz, stream_, launches_);
   stageEnd(4);
   stageBegin(5);
