@@ -35,7 +35,9 @@ PKG = os.path.join(ROOT, "hybrid-fluid-simulation_b200")
 sys.path.insert(0, PKG)
 
 METRIC = "Mcell-steps/s at 256^3 (dam break, plain FP32 path)"
-CG_DRAM_BYTES_PER_CELL = (107.12e6 + 18.07e6 + 146.51e6 + 38.64e6) / 224 ** 3
+# dram__bytes_read.sum + dram__bytes_write.sum of kCgDirection and kCgUpdate,
+# one launch each, ncu --set full on the 224^3 dam break (11.2 M cells)
+CG_DRAM_BYTES_PER_CELL = (105.90e6 + 6.42e6 + 146.36e6 + 11.13e6) / 224 ** 3
 UNIT = "Mcell-steps/s"
 
 
