@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(MX* MY)
         float az = applyA(L, k, vc, zAt);
         v = vc + kOmega * (bv - az) / diagOfC(k, L.sx, L.sy, L.sz);
       }
-      zo[c] = v;
+      if (k & 1) zo[c] = v;  // zero off the fluid for the whole solve (memset by mgRunCg)
       if (DOT) rz += (double)bv * (double)v;
       vb = vc;
       k = ka;
@@ -293,7 +293,7 @@ __global__ void __launch_bounds__(MX* MY)
 #pragma unroll 4
   for (int zz = z0; zz < z1; ++zz, c += pl) {
     const Code k = code[c];
-    z[c] = (k & 1) ? kOmega * __ldg(b + c) / diagOfC(k, L.sx, L.sy, L.sz) : 0.f;
+    if (k & 1) z[c] = kOmega * __ldg(b + c) / diagOfC(k, L.sx, L.sy, L.sz);  // zero elsewhere already
   }
 }
 
@@ -647,6 +647,9 @@ void mgRunCg(Multigrid* m, const Dim3i& cg, float sx, float sy, float sz, const 
   // cells, and the fluid moves between solves
   check(cudaMemsetAsync(m->p[0].p, 0, m->p[0].bytes(), s), "memset");
   check(cudaMemsetAsync(m->p[1].p, 0, m->p[1].bytes(), s), "memset");
+  // the marching level-0 sweeps store fluid cells only: the iterates start zero
+  check(cudaMemsetAsync(m->z0a.p, 0, m->z0a.bytes(), s), "memset");
+  check(cudaMemsetAsync(m->z0b.p, 0, m->z0b.bytes(), s), "memset");
   const float* z0 = mgVcycle(m, rvec, st, s, launches);  // z0 = V(b), rz = b.z0
   const int kChunk = 4;  // even: every chunk starts on p[0]
   auto body = [&] {
