@@ -59,6 +59,9 @@ template <class T> static inline bool isInsideSDF(T v) { return v < 0; }
 // EulerMathTool.cu:268-294 particle/grid transfer kernels
 template <class T> static inline T linearKernelFunc(T o) {
   T a = std::fabs(o);
+#ifdef ORC_PLANTED_MISTAKE  // a deliberate error, only in the build that checks the replay catches it
+  a = a * (T)1.01;
+#endif
   return a < 1 ? (T)1.0 - a : (T)0.0;
 }
 template <class T> static inline T quadraticKernelFunc(T o) {
@@ -99,6 +102,9 @@ template <class T> static inline T trilerp(const T* f, const GridGeom<T>& g, T p
   T ox = (rx - ((T)ix * g.h.x)) / g.h.x;
   T oy = (ry - ((T)iy * g.h.y)) / g.h.y;
   T oz = (rz - ((T)iz * g.h.z)) / g.h.z;
+#ifdef ORC_PLANTED_MISTAKE
+  ox = ox * (T)1.01;
+#endif
   T UBL = f[lin(ix, iy + 1, iz, g.r)], UBR = f[lin(ix + 1, iy + 1, iz, g.r)];
   T UFL = f[lin(ix, iy + 1, iz + 1, g.r)], UFR = f[lin(ix + 1, iy + 1, iz + 1, g.r)];
   T DBL = f[lin(ix, iy, iz, g.r)], DBR = f[lin(ix + 1, iy, iz, g.r)];
@@ -600,9 +606,11 @@ static int advectParticles(const GridGeom<T>& cc, const FC<T>& vel, std::vector<
     ++nsub;
   }
   // fixParticlesPosWithBoundarys: clampMode 0 = all particles,
-  // 1 = the reference launch shape (the first min(N, P) particles).
+  // 1 = the reference launch shape (the first min(N, P) particles),
+  // 2 = none (EulerParticles.cpp:319-322: no boundary SDF of the grid's size).
   i64 nclamp = P;
   if (clampMode == 1) nclamp = std::min<i64>(P, cc.r.size());
+  if (clampMode == 2) nclamp = 0;
   T mn[3] = {cc.o.x, cc.o.y, cc.o.z};
   T mx[3] = {cc.o.x + (T)cc.r.x * cc.h.x, cc.o.y + (T)cc.r.y * cc.h.y, cc.o.z + (T)cc.r.z * cc.h.z};
   for (i64 p = 0; p < nclamp; ++p)
@@ -1640,5 +1648,100 @@ long long orc_solver_num_particles(void* p) { return ORC_CALL((OrcSolver*)p, sNu
 void orc_solver_get_particles(void* p, float* pos, float* vel) { ORC_CALL((OrcSolver*)p, sGetParticles, pos, vel); }
 // stats: [cg iterations, final ||r||, ||b||, time, substeps, buffer flag]
 void orc_solver_stats(void* p, double* out) { ORC_CALL((OrcSolver*)p, sStats, out); }
+
+}  // extern "C"
+
+// ===========================================================================
+// Single stages for the replay of the reference's own unit tests
+// (oracle/reftests): each is one piece of the step above, exported alone.
+// ===========================================================================
+extern "C" {
+
+// SemiLagrangian.cpp:188-347 backTrace of M points (AoS xyz) through the
+// face-centred velocity on the grid (res, o, h); `samp` is the
+// ESamplingAlgorithm of the velocity samples.
+void orc_back_trace(int dbl, const int* res, const float* o, const float* h, const float* vx, const float* vy,
+                    const float* vz, const float* pos, long long M, float dt, int acc, int samp, float* out) {
+  if (dbl) {
+    GridGeom<double> g = mkGeom<double>(res, o, h);
+    FC<double> v = upFC<double>(g.r, vx, vy, vz);
+    for (i64 i = 0; i < M; ++i) {
+      double in[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]}, q[3];
+      backTrace<double>(v, g, (double)dt, acc, in, q, samp);
+      for (int a = 0; a < 3; ++a) out[3 * i + a] = (float)q[a];
+    }
+  } else {
+    GridGeom<float> g = mkGeom<float>(res, o, h);
+    FC<float> v = upFC<float>(g.r, vx, vy, vz);
+    for (i64 i = 0; i < M; ++i) backTrace<float>(v, g, dt, acc, pos + 3 * i, out + 3 * i, samp);
+  }
+}
+
+// EulerParticlesTool.cu:27-46 statisticalFluidDensity: particles per cell
+// (truncating binning of transPos2Index), as Real.
+void orc_particle_counts(const int* res, const float* o, const float* h, const float* pos, long long P, float* out) {
+  GridGeom<float> g = mkGeom<float>(res, o, h);
+  std::vector<float> cnt(g.r.size(), 0.0f);
+  for (i64 p = 0; p < P; ++p) cnt[binIndex(g, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2])] += 1.0f;
+  std::memcpy(out, cnt.data(), cnt.size() * sizeof(float));
+}
+
+// FieldMathTool.cu:370-395 divergence of a face-centred field.
+void orc_divergence_fc(int dbl, const int* res, const float* h, const float* vx, const float* vy, const float* vz,
+                       float* out) {
+  Res r{res[0], res[1], res[2]};
+  if (dbl) {
+    FC<double> v = upFC<double>(r, vx, vy, vz);
+    std::vector<double> d(r.size());
+    divergenceFC<double>(r, V3<double>{h[0], h[1], h[2]}, v, d.data());
+    down(d, out);
+  } else {
+    FC<float> v = upFC<float>(r, vx, vy, vz);
+    divergenceFC<float>(r, V3<float>{h[0], h[1], h[2]}, v, out);
+  }
+}
+
+// ExternalForcesSolver.cpp:50-58: gravity (0, -9.8, 0) plus the user force,
+// times dt, added to every face of (vx, vy, vz) in place.
+void orc_apply_external_forces(const int* res, float* vx, float* vy, float* vz, float dt, float fx, float fy,
+                               float fz) {
+  Solver<float> s;
+  s.dt = dt;
+  s.ext = V3<float>{fx, fy, fz};
+  Res r{res[0], res[1], res[2]};
+  FC<float> v = upFC<float>(r, vx, vy, vz);
+  s.applyForces(v);
+  downFC(v, vx, vy, vz);
+}
+
+// Boundary.cpp:115-150 updateBoundarys on nb solids: translation -= dt * vel,
+// each SDF resampled at the translated cell centres, the total marker
+// (-(first solid index) inside, UNKNOWN outside) and the solid face
+// velocities.  sdf0/sdfCur hold nb grids back to back; vel and trans 3 per
+// solid (trans is updated in place).
+void orc_boundarys_update(const int* res, const float* o, const float* h, int nb, const float* sdf0,
+                          const float* vel, float* trans, float dt, float* sdfCur, float* marker, float* svx,
+                          float* svy, float* svz) {
+  Solver<float> s;
+  s.create(dt, Res{res[0], res[1], res[2]}, V3<float>{o[0], o[1], o[2]}, V3<float>{h[0], h[1], h[2]});
+  i64 N = s.g.r.size();
+  for (int i = 0; i < nb; ++i) {
+    Boundary<float> b;
+    b.sdf0.assign(sdf0 + i * N, sdf0 + (i + 1) * N);
+    b.sdf = b.sdf0;
+    b.vel = V3<float>{vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]};
+    b.trans = V3<float>{trans[3 * i], trans[3 * i + 1], trans[3 * i + 2]};
+    s.bnd.push_back(b);
+  }
+  s.updateBoundarys();
+  for (int i = 0; i < nb; ++i) {
+    trans[3 * i] = s.bnd[i].trans.x;
+    trans[3 * i + 1] = s.bnd[i].trans.y;
+    trans[3 * i + 2] = s.bnd[i].trans.z;
+    if (sdfCur) std::memcpy(sdfCur + i * N, s.bnd[i].sdf.data(), N * sizeof(float));
+  }
+  if (marker) down(s.totalSDF, marker);
+  if (svx) downFC(s.solidVel, svx, svy, svz);
+}
 
 }  // extern "C"

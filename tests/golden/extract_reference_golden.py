@@ -1,7 +1,7 @@
 """Extract the known-answer data of the reference's own unit tests.
 
-Reads the gtest sources of junwei-jiang/Hybrid-Fluid-Simulation (default
-/root/reference/TestCase/MPhysics/Euler) and writes reference_golden.json
+Reads the gtest sources of junwei-jiang/Hybrid-Fluid-Simulation (the
+TestCase/MPhysics/Euler directory of a checkout) and writes reference_golden.json
 beside this script: for every TEST block its resolutions, explicit input
 assignments (NAME[i] = v), vector fills, scalar parameters, and every
 expectation of the form EXPECT_LT(abs(VAR[i] -/+ value), GRID_SOLVER_EPSILON),
@@ -12,7 +12,11 @@ Only data is extracted; the tests in tests/test_oracle_golden.py restate how
 each reference test wires that data (which arrays are inputs, which stage
 runs) and check the oracle against the expectations.
 
-    python tests/golden/extract_reference_golden.py [reference_euler_test_dir]
+    python tests/golden/extract_reference_golden.py <reference root>/TestCase/MPhysics/Euler
+
+The particle, semi-Lagrangian, boundary and external-force suites are not
+extracted here: their tests are replayed whole on the oracle
+(oracle/reftests, tests/test_reference_replay.py).
 """
 import json
 import os
@@ -20,13 +24,9 @@ import re
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT = "/root/reference/TestCase/MPhysics/Euler"
 FILES = {
     "Extrapolation": "UnitTest-Extrapolation/UnitTest-Extrapolation.cu",
     "PressureSolver": "UnitTest-PressureSolver/UnitTest-PressureSolver.cu",
-    "ParticlesAdvection": "UnitTest-ParticlesAdvection/UnitTest-ParticlesAdvection.cu",
-    "SemiLagrangian": "UnitTest-SemiLagrangian/UnitTest-SemiLagrangian.cu",
-    "ExternalForces": "UnitTest-ExternalForces/UnitTest-ExternalForces.cu",
     "GridFluidSolver": "IntegrationTest-GridFluidSolver/IntegrationTest-GridFluidSolver.cpp",
 }
 
@@ -92,7 +92,9 @@ def parse(path):
 
 
 def main():
-    base = sys.argv[1] if len(sys.argv) > 1 else DEFAULT
+    if len(sys.argv) != 2:
+        sys.exit(__doc__)
+    base = sys.argv[1]
     out = {"source": "junwei-jiang/Hybrid-Fluid-Simulation TestCase/MPhysics/Euler", "suites": {}}
     for suite, rel in FILES.items():
         p = os.path.join(base, rel)

@@ -1,8 +1,8 @@
 """Extract the known-answer data of the reference's cubic-sampling unit tests.
 
 Reads TestCase/MPhysics/DataStructure/UnitTest-ScalarGrid/
-UnitTest-CellCenteredScalarField.cu of junwei-jiang/Hybrid-Fluid-Simulation
-(default under /root/reference) and writes sampling_golden.json beside this
+UnitTest-CellCenteredScalarField.cu of a junwei-jiang/Hybrid-Fluid-Simulation
+checkout and writes sampling_golden.json beside this
 script.  Every case that samples a cell-centred scalar field with
 ESamplingAlgorithm::CATMULLROM / MONOCATMULLROM / CUBICBRIDSON /
 CLAMPCUBICBRIDSON is recorded with:
@@ -15,7 +15,7 @@ CLAMPCUBICBRIDSON is recorded with:
 Formulas are kept as the C++ text of the test (in terms of i, j, k and
 Res.x / Res.y); tests/test_oracle_golden.py evaluates them.
 
-    python tests/golden/extract_sampling_golden.py [reference_root]
+    python tests/golden/extract_sampling_golden.py <reference root>
 """
 import json
 import os
@@ -23,7 +23,6 @@ import re
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT = "/root/reference"
 REL = "TestCase/MPhysics/DataStructure/UnitTest-ScalarGrid/UnitTest-CellCenteredScalarField.cu"
 
 NUM = r"[-+]?(?:\d+\.?\d*|\.\d+)(?:[eE][-+]?\d+)?"
@@ -79,7 +78,9 @@ def parse(path):
 
 
 def main():
-    base = sys.argv[1] if len(sys.argv) > 1 else DEFAULT
+    if len(sys.argv) != 2:
+        sys.exit(__doc__)
+    base = sys.argv[1]
     cases = parse(os.path.join(base, REL))
     out = {"source": "junwei-jiang/Hybrid-Fluid-Simulation " + REL, "cases": cases}
     dst = os.path.join(HERE, "sampling_golden.json")
