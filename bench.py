@@ -10,9 +10,12 @@ Jacobi-preconditioned CG to a relative residual of 1e-6 with at most 200
 iterations, full velocity extrapolation.  The scene state (~3.5 GB) is far
 larger than the 126 MB L2, so no L2 flush is needed between steps.
 
-One process per GPU (torchrun for N > 1); every rank steps its own replica of
-the scene (weak scaling, no data-path collective); the time is the maximum
-over ranks of the CUDA-event time on each solver's stream.
+One process per GPU: with --gpus N > 1 and no torchrun environment the script
+starts N ranks itself under torch.distributed.run.  For the dam break every
+rank steps its own replica of the scene (weak scaling, no data-path
+collective); for --workload serve|batch the scenes are placed on ranks by
+their device-memory footprint.  The time is the maximum over ranks of the
+CUDA-event time on each solver's stream.
 
 --impl reference times the reference path on the host CPU (the reference has
 no CPU implementation of the grid step, so its CPU restatement in oracle/ is
@@ -38,14 +41,17 @@ METRIC = "Mcell-steps/s at 256^3 (dam break, plain FP32 path)"
 # dram__bytes_read.sum + dram__bytes_write.sum of kCgDirection and kCgUpdate,
 # one launch each, ncu --set full on the 224^3 dam break (11.2 M cells)
 CG_DRAM_BYTES_PER_CELL = (105.90e6 + 6.42e6 + 146.36e6 + 11.13e6) / 224 ** 3
+# Algorithmic bytes of one CFL substep per particle: position and v0 read and
+# written (FP32 xyz each); the corner-table gathers hit L2.
+SUBSTEP_BYTES_PER_PARTICLE = 48.0
 UNIT = "Mcell-steps/s"
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--res", type=int, default=256)
     ap.add_argument("--precond", default="jacobi", choices=["jacobi", "identity", "mg"])
@@ -117,6 +123,35 @@ def dist_setup(args):
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return world, rank, local
+
+
+def rank_plan(n_gpus: int, port: int):
+    """The command that runs this script on n_gpus ranks of this node (one
+    process per GPU, rendezvous on 127.0.0.1)."""
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n_gpus}",
+            "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + sys.argv[1:]
+
+
+def relaunch(n_gpus: int) -> int:
+    """--gpus N > 1 outside torchrun: start the N ranks and wait for them."""
+    import socket
+    sk = socket.socket()
+    sk.bind(("127.0.0.1", 0))
+    port = sk.getsockname()[1]
+    sk.close()
+    return subprocess.run(rank_plan(n_gpus, port)).returncode
+
+
+def init_ranks(world: int, local: int):
+    """The process group of a multi-rank run (NCCL, short timeout), or None."""
+    if world <= 1:
+        return None
+    import datetime
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return dist
 
 
 def run_reference(args):
@@ -213,11 +248,11 @@ def serve_requests(args, rng, batch=False):
     return out
 
 
-def run_server(args, reqs, arrivals, slots, precond):
+def run_server(args, reqs, arrivals, slots, precond, device=0):
     """Submit `reqs` at their arrival times (seconds from start) to a server
-    with `slots` concurrent scenes; returns its statistics."""
+    with `slots` concurrent scenes on `device`; returns its statistics."""
     import hfgrid
-    srv = hfgrid.Server(slots=slots, budget_bytes=150 * 10**9)
+    srv = hfgrid.Server(slots=slots, budget_bytes=150 * 10**9, device=device)
     t0 = time.perf_counter()
     ids = []
     for r, at in zip(reqs, arrivals):
@@ -237,10 +272,17 @@ def run_server(args, reqs, arrivals, slots, precond):
 
 
 def run_serve(args):
-    """C5 (serve) or C4 (batch) through the scene server, one JSON line."""
+    """C5 (serve) or C4 (batch) through the scene server, one JSON line.  With
+    N ranks every rank builds the same request list, the scenes are placed on
+    ranks by footprint (dist_util.assign_scenes, largest first under the
+    150 GB budget of each GPU) and each rank serves its share on its own GPU;
+    cell-steps add up and the wall time is the max over ranks."""
     import numpy as np
     import hfgrid
-    hfgrid.init(0)
+    import dist_util
+    world, rank, local = dist_setup(args)
+    pg = init_ranks(world, local)
+    hfgrid.init(local)
     batch = args.workload == "batch"
     rng = np.random.default_rng(2024)
     reqs = serve_requests(args, rng, batch=batch)
@@ -248,26 +290,76 @@ def run_serve(args):
         arrivals = [0.0] * len(reqs)
     else:
         arrivals = list(np.cumsum(rng.exponential(1.0 / args.rate, len(reqs))))
-    clocks = ClockSampler(0)
+    budget = 150 * 10**9
+    placed = list(range(len(reqs)))
+    if world > 1:
+        fp = [hfgrid.scene_bytes(r["res"], scene_particles(r), 1 + len(r["spheres"]), hfgrid.PRECOND_MG) for r in reqs]
+        plan, rejected = dist_util.assign_scenes(fp, world, budget)
+        placed = plan[rank]
+        assert dist_util.agree([i for p in plan for i in p] + [-1] + rejected, device="cuda")
+    mine = [reqs[i] for i in placed]
+    at = [arrivals[i] for i in placed]
+    clocks = ClockSampler(local)
     clocks.start()
-    mixed = run_server(args, reqs, arrivals, args.slots, hfgrid.PRECOND_MG)
+    if pg is not None:
+        pg.barrier()
+    mixed = run_server(args, mine, at, args.slots, hfgrid.PRECOND_MG, local)
     clk = clocks.stop()
+    plain = None
+    if not args.no_plain:
+        if pg is not None:
+            pg.barrier()
+        plain = run_server(args, mine, at, 1, hfgrid.PRECOND_JACOBI, local)
+    if pg is not None:
+        import torch.distributed as dist
+        gathered = [None] * world
+        dist.all_gather_object(gathered, {"mixed": mixed, "plain": plain, "clocks": clk, "n": len(mine)})
+        pg.barrier()
+        pg.destroy_process_group()
+        if rank != 0:
+            return
+        mixed = merge_server_stats([g["mixed"] for g in gathered])
+        plain = merge_server_stats([g["plain"] for g in gathered]) if plain is not None else None
+        clk = gathered[0]["clocks"]
     line = {
         "metric": "Mcell-steps/s and step latency, " + ("batched uneven scenes" if batch else "served request stream"),
-        "value": mixed["mcell_steps_per_s"], "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
-        "dtype": "f32 (MG preconditioner with BF16 coarse levels, FP64 dots)", "data": "synthetic (seeded)",
+        "value": mixed["mcell_steps_per_s"], "unit": UNIT, "n_gpus": world, "higher_is_better": True,
+        "scaling": "strong", "dtype": "f32 (MG preconditioner with BF16 coarse levels, FP64 dots)",
+        "data": "synthetic (seeded)",
         "config": {"workload": ("C4 batch: %d scenes, axes U{32..128}, fluid fraction U(0.2,0.5), 8 ppc, %d steps"
                                 % (len(reqs), args.scene_steps)) if batch else
                    ("C5 serve: %d requests, Poisson %.0f req/s, side log-uniform 32..256, 0-3 spheres, %d steps, "
-                    "150 GB budget" % (len(reqs), args.rate, args.scene_steps)),
-                   "slots": args.slots},
+                    "150 GB budget per GPU" % (len(reqs), args.rate, args.scene_steps)),
+                   "slots": args.slots, "placement": "scenes by footprint over %d rank(s)" % world},
         "served": mixed, "clocks": clk,
     }
-    if not args.no_plain:
-        plain = run_server(args, reqs, arrivals, 1, hfgrid.PRECOND_JACOBI)
+    if plain is not None:
         line["plain"] = plain
         line["speedup_vs_plain"] = mixed["mcell_steps_per_s"] / max(plain["mcell_steps_per_s"], 1e-9)
     print(json.dumps(line), flush=True)
+
+
+def scene_particles(r) -> int:
+    """Particles of a served/batched request, bounded by 8 per cell of its
+    fluid box (the server's own admission uses the same bound)."""
+    fx, fy, fz = r["fluid_max"]
+    nx, ny, nz = r["res"]
+    return int(8 * int(fx * nx) * int(fy * ny) * int(fz * nz))
+
+
+def merge_server_stats(parts):
+    """Whole-job statistics of several ranks' servers: counts and cell-steps
+    add up, the wall time is the longest, latency percentiles are the worst
+    rank's (each rank holds its own step-time distribution)."""
+    out = dict(parts[0])
+    for k in ("submitted", "completed", "failed", "rejected", "cell_steps", "peak_bytes"):
+        out[k] = sum(p[k] for p in parts)
+    for k in ("wall_s", "step_ms_p50", "step_ms_p99", "request_ms_p50", "request_ms_p99"):
+        out[k] = max(p[k] for p in parts)
+    out["failed_ids"] = [i for p in parts for i in p["failed_ids"]]
+    out["mcell_steps_per_s"] = out["cell_steps"] / max(out["wall_s"], 1e-9) / 1e6
+    out["ranks"] = len(parts)
+    return out
 
 
 def run_moving_boxes(args):
@@ -338,6 +430,8 @@ def run_moving_boxes(args):
 
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(relaunch(args.gpus))
     if args.impl == "reference":
         run_reference(args)
         return
@@ -347,28 +441,27 @@ def main():
     if args.workload != "dam-break":
         run_serve(args)
         return
-    import numpy as np
+    run_dam_break(args)
+
+
+def run_dam_break(args):
+    """The headline line: the 256^3 dam break, one replica per rank."""
     import torch
     import hfgrid
     import scenes
 
     world, rank, local = dist_setup(args)
-    pg = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        pg = dist
+    pg = init_ranks(world, local)
     hfgrid.init(local)
     torch.cuda.set_device(local)
     precond = {"jacobi": hfgrid.PRECOND_JACOBI, "identity": hfgrid.PRECOND_IDENTITY, "mg": hfgrid.PRECOND_MG}[args.precond]
     sc = scenes.dam_break_256(seed=rank, n=args.res)
+    opts = dict(precond=precond, tol_mode=hfgrid.TOL_RELATIVE, tol=1e-6, max_iter=200, advect_scalars=0,
+                clamp_mode=1, pressure_fp64=int(args.pressure_fp64), mg_smooth=args.mg_smooth)
 
     def warm_solver():
         """A solver in the state the timed steps start from: seeded, W steps in."""
-        w = scenes.gpu_solver(sc, precond=precond, tol_mode=hfgrid.TOL_RELATIVE, tol=1e-6, max_iter=200,
-                              advect_scalars=False, pressure_fp64=int(args.pressure_fp64), mg_smooth=args.mg_smooth)
+        w = scenes.gpu_solver(sc, **opts)
         for _ in range(args.warmup):
             w.update()
         w.synchronize()
@@ -397,19 +490,28 @@ def main():
     ms = ev0.elapsed_time(ev1)
     launches = s.launch_count - launches0
     clk = clocks.stop()
-    st = s.stats()
 
-    # dominant kernel: one CG iteration (direction + update kernels) timed
-    # back-to-back on the last system
+    # one CG iteration (direction + update kernels) timed back-to-back on the
+    # last system
     cg_ms = s.time_cg(40)
 
-    # per-stage device times of one more step (CUDA events around each stage;
-    # outside the timed region)
+    # one more step, outside the timed region, with per-stage and per-kernel
+    # device times and the convergence checks of the projection: the CG's
+    # recurrence residual, ||b - A x|| recomputed in FP64, and the divergence
+    # of the projected velocity
+    s.set_options(**opts, report_divergence=1)
     s.enable_timing(True)
     s.update()
-    stage_ms = dict(zip(("boundaries", "advection", "forces", "markers", "rhs", "cg", "gradient", "extrapolation"),
-                        (round(float(v), 3) for v in s.stats()["stage_ms"])))
+    st = s.stats()
     s.enable_timing(False)
+    stage_ms = dict(zip(("boundaries", "advection", "forces", "markers", "rhs", "cg", "gradient", "extrapolation"),
+                        (round(float(v), 3) for v in st["stage_ms"])))
+    particle_ms = dict(zip(("g2p", "substeps", "p2g"), (round(float(v), 3) for v in st["particle_ms"])))
+    bnorm = max(st["cg_rhs_norm"], 1e-300)
+    conv = {"cg_iterations": st["cg_iterations"], "cg_converged": bool(st["cg_converged"]),
+            "cg_rel_residual": st["cg_residual"] / bnorm, "cg_true_rel_residual_fp64": st["cg_true_residual"] / bnorm,
+            "divergence_rel": st["divergence_l2"] / bnorm, "substeps": st["substeps"],
+            "extrapolation_layers": st["extrapolation_layers"]}
     n = s.num_particles
     del s
 
@@ -463,23 +565,26 @@ def main():
         e2e["ms"] = max_over_ranks(e2e["ms"])
         e2e["ms_copy_after"] = max_over_ranks(e2e["ms_copy_after"])
     cg_ms = max_over_ranks(cg_ms)
+    sub_ms = max_over_ranks(float(st["particle_ms"][1]))
 
     if rank == 0:
-        import json as _json
         peaks = {}
         try:
             with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-                peaks = _json.load(f)
+                peaks = json.load(f)
         except OSError:
             pass
         hbm = float(peaks.get("hbm_gbs", 6650.0))
+        peak_source = "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks else "fallback 6650 GB/s"
         N = sc.n_cells
         value = N * args.steps * world / (ms / 1e3) / 1e6
-        algo_bytes = 25.0 * N  # compulsory bytes per CG iteration (d, x, r read + markers + x, r, d written)
+        # the dominant kernel of the step: the CFL particle substep
+        sub_launch_ms = sub_ms / max(conv["substeps"], 1)
+        sub_bytes = SUBSTEP_BYTES_PER_PARTICLE * n
+        sub_achieved = sub_bytes / (sub_launch_ms / 1e3) / 1e9
+        # the CG pair, 25 B/cell per iteration (d, x, r read + markers + x, r, d written)
+        algo_bytes = 25.0 * N
         achieved = algo_bytes / (cg_ms / 1e3) / 1e9
-        # DRAM bytes per cell of one CG iteration (kCgDirection + kCgUpdate) from the ncu capture at 224^3
-        # (profiles/cg_kernels_224cubed_ncu.md), scaled by the cell count
-        traffic = CG_DRAM_BYTES_PER_CELL * N
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -487,15 +592,17 @@ def main():
             "config": {"workload": f"dam break {args.res}^3, walls + two static boxes, 8 ppc, PIC/FLIP 0.95, "
                                    f"{args.precond}-PCG rel 1e-6 max 200", "res": [args.res] * 3,
                        "cells": N, "particles": n, "l2": "state > L2 (no flush needed)",
-                       "parallelism": f"replicas x{world}", "cg_iterations_last": st["cg_iterations"],
-                       "substeps_last": st["substeps"], "extrapolation_layers_last": st["extrapolation_layers"],
-                       "stage_ms_one_more_step": stage_ms},
-            "roofline": {"bound": "hbm", "kernel": "CG iteration (kCgDirection + kCgUpdate)",
-                         "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                         "traffic": traffic, "traffic_source": "ncu dram__bytes_read+write at 224^3, per cell, "
-                                                                   "scaled to this grid",
-                         "algorithmic_bytes_per_iter": algo_bytes, "ms_per_iter": cg_ms,
-                         "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback"},
+                       "parallelism": f"replicas x{world}", "convergence_one_more_step": conv,
+                       "stage_ms_one_more_step": stage_ms, "particle_ms_one_more_step": particle_ms},
+            "roofline": {"bound": "hbm", "kernel": "kSubstepStaged (one CFL particle substep)",
+                         "achieved": sub_achieved, "peak": hbm, "unit": "GB/s", "frac": sub_achieved / hbm,
+                         "traffic": None, "algorithmic_bytes_per_launch": sub_bytes,
+                         "bytes_per_particle": SUBSTEP_BYTES_PER_PARTICLE, "ms_per_launch": sub_launch_ms,
+                         "launches_per_step": conv["substeps"], "peak_source": peak_source,
+                         "cg_pair": {"kernel": "kCgDirection + kCgUpdate (one CG iteration)", "achieved": achieved,
+                                     "frac": achieved / hbm, "algorithmic_bytes_per_iter": algo_bytes,
+                                     "ms_per_iter": cg_ms, "traffic": CG_DRAM_BYTES_PER_CELL * N,
+                                     "traffic_source": "ncu dram__bytes_read+write at 224^3, per cell, scaled"}},
             "clocks": clk,
             "gpu_launches": launches,
         }
@@ -513,6 +620,7 @@ def main():
                 line["cpu_baseline"] = {"value": None, "error": str(ex)}
         print(json.dumps(line), flush=True)
     if pg is not None:
+        pg.barrier()
         pg.destroy_process_group()
 
 

@@ -929,22 +929,15 @@ namespace {
 constexpr long long kStaticP2GFaces = 1LL << 20;
 static __device__ __align__(256) float2 g_p2gStaticAcc[kStaticP2GFaces];
 
-constexpr int kMaxStaticDevices = 64;
-std::mutex g_p2gStaticMu;
-float2* g_p2gStaticPtr[kMaxStaticDevices] = {};
-
-// Address of the array on the current device, resolved once per device.
+// Address of the array on the current device.  In host code the symbol
+// g_p2gStaticAcc is a host-side stand-in, so the device address is looked up
+// on every call (a host-side table lookup once the module is loaded): an
+// address kept from an earlier call would go stale if the host reset the
+// device or recreated its primary context, which reloads the module.
 float2* staticP2GAccumulators() {
-  int dev = 0;
-  check(cudaGetDevice(&dev), "cudaGetDevice");
-  if (dev < 0 || dev >= kMaxStaticDevices) throw CudaError("device index beyond the static table", HFG_ERR_UNSUPPORTED);
-  std::lock_guard<std::mutex> lk(g_p2gStaticMu);
-  if (!g_p2gStaticPtr[dev]) {
-    float2* p = nullptr;
-    check(cudaGetSymbolAddress((void**)&p, g_p2gStaticAcc), "cudaGetSymbolAddress");
-    g_p2gStaticPtr[dev] = p;
-  }
-  return g_p2gStaticPtr[dev];
+  float2* p = nullptr;
+  check(cudaGetSymbolAddress((void**)&p, g_p2gStaticAcc), "cudaGetSymbolAddress");
+  return p;
 }
 
 }  // namespace

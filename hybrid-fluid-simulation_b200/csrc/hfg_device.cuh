@@ -445,6 +445,62 @@ __device__ __forceinline__ unsigned ldAcquire(const unsigned* p) {
   return v;
 }
 
+// ---------------------------------------------------------------------------
+// mbarrier and bulk-copy (TMA) plumbing shared by the streaming kernels.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smemAddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbarInit(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smemAddr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbarFenceInit() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbarExpectTx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smemAddr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbarTryWait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smemAddr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: false once the deadline has passed (the caller records an
+// error and drains what it issued).
+__device__ __forceinline__ bool mbarWait(uint64_t* bar, unsigned parity, unsigned long long deadline) {
+  while (!mbarTryWait(bar, parity))
+    if (globalNs() > deadline) return false;
+  return true;
+}
+// Untiled bulk copy global -> shared, completion counted on `bar` (16-byte
+// aligned addresses, size a multiple of 16).
+__device__ __forceinline__ void bulkLoad(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smemAddr(dst)),
+      "l"(src), "r"(bytes), "r"(smemAddr(bar))
+      : "memory");
+}
+// Untiled bulk copy shared -> global in the thread's current bulk group.
+__device__ __forceinline__ void bulkStore(void* dst, const void* src, unsigned bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smemAddr(src)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulkCommit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// Waits until at most N of this thread's bulk groups still read shared memory.
+template <int N> __device__ __forceinline__ void bulkWaitRead() {
+  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+// Waits until all of this thread's bulk groups have completed.
+__device__ __forceinline__ void bulkWaitAll() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+// Orders this thread's generic-proxy shared-memory writes before later
+// async-proxy (bulk copy) reads of them.
+__device__ __forceinline__ void fenceProxyAsyncShared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
 // Grid barrier of a cooperative launch (generation counting).  The wait is
 // bounded: past the deadline, or once another block has given up, the error
 // word is set and false returned, and the caller stops.

@@ -47,6 +47,7 @@ struct SubstepState {
   float subTime;            // time advanced so far
   int finished;
   int count;
+  int error;                // nonzero: a block gave up waiting for its particle stream
 };
 
 struct SolidVelTable {
@@ -142,6 +143,13 @@ inline int divergenceBlocks() { return 1024; }
 cudaError_t launchDivergenceNorm(const Geom& g, ConstFaceField v, const SolidVelTable& svTab,
                                  const uint8_t* markers, double* scratch, unsigned* ticketAndMax, double* sumOut,
                                  cudaStream_t s);
+// FP64 residual of a solve: out[0] = ||b - A x||^2, out[1] = ||b||^2 over the
+// fluid cells, b from the unprojected velocity v, A from the 16-bit codes
+// (pitched) and the FP32 scales, x pitched (FP32 or FP64).  `scratch` holds
+// 2 * divergenceBlocks() doubles.
+cudaError_t launchTrueResidual(const Geom& g, ConstFaceField v, const SolidVelTable& svTab, const uint8_t* markers,
+                               const Code* code, const void* x, bool xDouble, float sx, float sy, float sz,
+                               double* scratch, unsigned* ticket, double* out, cudaStream_t s);
 // p pitched, FP32 or (pDouble) FP64; the differences are rounded to FP32
 cudaError_t launchGradient(const Geom& g, float gx, float gy, float gz, const uint8_t* markers, const void* p,
                            bool pDouble, FaceField v, ConstFaceField svArr, const SolidVelTable& svTab,

@@ -234,6 +234,66 @@ __global__ void kDivergenceNorm(Geom g, ConstFaceField v, ConstFaceField svArr, 
   }
 }
 
+// The final residual check of a pressure solve, in FP64 on the GPU:
+// ||b - A x||^2 and ||b||^2 over the fluid cells.  b is recomputed from the
+// unprojected velocity (rhsAt, the reference's operation order), the entries
+// of A are the FP32 system's scales promoted to FP64 (fdmMatrixVectorMul,
+// EulerSolverTool.cu:199-227, with diagonal and neighbour terms from the
+// stencil code) and x is read as stored (FP32 or FP64).  The CG's own
+// recurrence residual drifts from this once FP32 round-off builds up.
+__global__ void kTrueResidual(Geom g, ConstFaceField v, SolidVelTable svTab, const uint8_t* __restrict__ mk,
+                              const Code* __restrict__ code, const void* __restrict__ xv, int xDouble, double sx,
+                              double sy, double sz, double* partials, unsigned* ticket, double* out) {
+  double rr = 0.0, bb = 0.0;
+  const Dim3i R = g.r;
+  const long long px = cgPitch(R.x), pl = px * R.y;
+  const ConstFaceField none{{nullptr, nullptr, nullptr}};
+  auto X = [&](long long i) -> double {
+    return xDouble ? ((const double*)xv)[i] : (double)((const float*)xv)[i];
+  };
+  const long long n = R.size();
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    if (mk[c] != kFluid) continue;
+    const int x = (int)(c % R.x);
+    const long long t = c / R.x;
+    const int y = (int)(t % R.y), z = (int)(t / R.y);
+    const double b = (double)rhsAt(g, v, none, svTab, mk, x, y, z);
+    const long long o = ((long long)z * R.y + y) * px + x;
+    const Code k = code[o];
+    double diag = 0.0;
+    if (k & 2) diag += sx;
+    if (k & 4) diag += sx;
+    if (k & 8) diag += sy;
+    if (k & 16) diag += sy;
+    if (k & 32) diag += sz;
+    if (k & 64) diag += sz;
+    double ax = diag * X(o);
+    if (nbFluid(k, 0)) ax -= sx * X(o - 1);
+    if (nbFluid(k, 1)) ax -= sx * X(o + 1);
+    if (nbFluid(k, 2)) ax -= sy * X(o - px);
+    if (nbFluid(k, 3)) ax -= sy * X(o + px);
+    if (nbFluid(k, 4)) ax -= sz * X(o - pl);
+    if (nbFluid(k, 5)) ax -= sz * X(o + pl);
+    const double r = b - ax;
+    rr += r * r;
+    bb += b * b;
+  }
+  if (gridSum2(rr, bb, partials, ticket) && flatTid() == 0) {
+    out[0] = rr;
+    out[1] = bb;
+    *ticket = 0;
+  }
+}
+cudaError_t launchTrueResidual(const Geom& g, ConstFaceField v, const SolidVelTable& svTab, const uint8_t* markers,
+                               const Code* code, const void* x, bool xDouble, float sx, float sy, float sz,
+                               double* scratch, unsigned* ticket, double* out, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(ticket, 0, sizeof(unsigned), s);
+  if (e != cudaSuccess) return e;
+  kTrueResidual<<<divergenceBlocks(), 256, 0, s>>>(g, v, svTab, markers, code, x, xDouble ? 1 : 0, (double)sx,
+                                                   (double)sy, (double)sz, scratch, ticket, out);
+  return cudaGetLastError();
+}
+
 template <int PC>
 __global__ void __launch_bounds__(TX* TY) kRhsInit(Geom g, ConstFaceField v, ConstFaceField svArr, SolidVelTable svTab,
                                                    const uint8_t* __restrict__ mk, const Code* __restrict__ code,
@@ -378,33 +438,6 @@ constexpr int FH = CTR + 2;          // 18 rows
 constexpr int kDirStages = 4, kUpdStages = 5;
 constexpr unsigned long long kWaitNs = 2000000000ull;  // a stage that takes 2 s to land is an error
 
-__device__ __forceinline__ uint32_t smemAddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbarInit(uint64_t* bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smemAddr(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbarFenceInit() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-__device__ __forceinline__ void mbarExpectTx(uint64_t* bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smemAddr(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbarTryWait(uint64_t* bar, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(ok)
-      : "r"(smemAddr(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Bounded wait: false once the deadline has passed.
-__device__ __forceinline__ bool mbarWait(uint64_t* bar, unsigned parity, unsigned long long deadline) {
-  while (!mbarTryWait(bar, parity))
-    if (globalNs() > deadline) return false;
-  return true;
-}
 __device__ __forceinline__ void tmaLoad3(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
   asm volatile(
       "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "

@@ -124,7 +124,7 @@ GridSolver::GridSolver(float dt, Dim3i res, const float origin[3], const float s
   check(cudaMemsetAsync(markers_.p, 0, N_, stream_), "memset");
   check(cudaMemsetAsync(cgx_.p, 0, cgx_.bytes(), stream_), "memset");
   check(cudaMemsetAsync(cgState_.p, 0, sizeof(CgState), stream_), "memset");
-  for (int i = 0; i < 16; ++i) check(cudaEventCreate(&ev_[i]), "cudaEventCreate");
+  for (int i = 0; i < kEvents; ++i) check(cudaEventCreate(&ev_[i]), "cudaEventCreate");
   check(cudaStreamSynchronize(stream_), "sync");
   extrapUsers(+1);  // last: a constructor that throws registers nothing
 }
@@ -141,7 +141,7 @@ GridSolver::~GridSolver() {
   pinnedPut(cgHost_);
   pinnedPut(subHost_);
   pinnedPut(extrapHost_);
-  for (int i = 0; i < 16; ++i)
+  for (int i = 0; i < kEvents; ++i)
     if (ev_[i]) cudaEventDestroy(ev_[i]);
   // the stream itself goes with own_, after the member arrays are freed on it
 }
@@ -417,12 +417,20 @@ void GridSolver::advectParticles(const FaceQuads& v, bool haveV0) {
   if (!haveV0) launched(launchSubstepBegin(g_, v, ppos_.p, pv0_.p, P_, subState_.p, stream_), "substep begin");
   long long nclamp = opt_.clamp_mode == 1 ? std::min<long long>(P_, N_) : P_;
   int slot = 0;
+  partMs_[1] = 0.f;
   for (;;) {
+    if (timing_) check(cudaEventRecord(ev_[18], stream_), "cudaEventRecord");
     for (int k = 0; k < kSubstepChunk && slot < subSlots_; ++k, ++slot)
       launched(launchSubstep(g_, v, ppos_.p, pv0_.p, P_, acc_rk_, dt_, cfl_, nclamp, subState_.p, slot, stream_),
                "substep");
+    if (timing_) check(cudaEventRecord(ev_[19], stream_), "cudaEventRecord");
     readBack(subHost_, subState_.p + slot, sizeof(SubstepState), stream_);
     check(cudaStreamSynchronize(stream_), "substep sync");
+    if (timing_) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, ev_[18], ev_[19]) == cudaSuccess) partMs_[1] += ms;
+    }
+    if (subHost_->error) throw CudaError("particle substep: a chunk load did not complete in time", HFG_ERR_TIMEOUT);
     if (subHost_->finished) { substeps_ = subHost_->count; break; }
     if (slot >= subSlots_) throw CudaError("CFL substep limit reached", HFG_ERR_STATE);
   }
@@ -458,15 +466,19 @@ void GridSolver::computeAdvection() {
   int mode = adv_ == HFG_ADV_PIC ? MODE_PIC : (adv_ == HFG_ADV_FLIP ? MODE_FLIP : MODE_MIX);
   int first = (mode != MODE_PIC && !velFlag_) ? 1 : 0;
   FaceQuads vq = beginParticleStep(cvel(ci));
+  if (timing_) check(cudaEventRecord(ev_[16], stream_), "cudaEventRecord");
   launched(launchParticleVelUpdate(g_, mode, alg_, cvel(ci), prev, first, mixing_, ppos_.p, pvel_.p, P_, stream_,
                                    &vq, pv0_.p, subState_.p),
            "particle velocity");
+  if (timing_) check(cudaEventRecord(ev_[17], stream_), "cudaEventRecord");
   if (mode != MODE_PIC) velFlag_ = true;
   startMirrorCopy(false);
   advectParticles(vq, alg_ == HFG_LINEAR);
   startMirrorCopy(true);
   float* copy[3] = {prev_[0].p, prev_[1].p, prev_[2].p};
+  if (timing_) check(cudaEventRecord(ev_[20], stream_), "cudaEventRecord");
   p2gFace(pvel_.p, vout, mode == MODE_PIC ? nullptr : copy, gv, doG, ev, doE);
+  if (timing_) check(cudaEventRecord(ev_[21], stream_), "cudaEventRecord");
   if (opt_.advect_scalars) {
     // colour (CC vector) then fluid domain (CC scalar): G2P once, P2G every step
     if (!vFlag_) {
@@ -585,7 +597,23 @@ void GridSolver::computePressure() {
   cgIters_ = cgHost_->iter;
   cgResid_ = std::sqrt(cgHost_->rr);
   cgBnorm_ = std::sqrt(cgHost_->bb);
-  cgConverged_ = cgHost_->iter < cgHost_->maxIter || cgHost_->maxIter == 0 ? 1 : 0;
+  // the stop rule of the solve (CuMatrixFreePCG.cpp:28,51, or relative) met
+  cgConverged_ = cgHost_->tolMode == 0 ? (std::sqrt(cgResid_) < cgHost_->tol ? 1 : 0)
+                                       : (cgBnorm_ == 0.0 || cgResid_ / cgBnorm_ < cgHost_->tol ? 1 : 0);
+  cgTrueResid_ = -1.0;
+  if (opt_.report_divergence) {
+    // the final residual check, ||b - A x|| in FP64 on the unprojected velocity
+    const int nb = divergenceBlocks();
+    divScratch_.alloc(2 * nb + 2, stream_);
+    divTicket_.alloc(2, stream_);
+    launched(launchTrueResidual(g_, cvel(ni), solidTable(), markers_.p, code_.p, xPtr(), xDouble(), sx, sy, sz,
+                                divScratch_.p, divTicket_.p, divScratch_.p + 2 * nb, stream_),
+             "true residual");
+    double rb[2] = {0.0, 0.0};
+    check(cudaMemcpyAsync(rb, divScratch_.p + 2 * nb, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream_), "read");
+    check(cudaStreamSynchronize(stream_), "sync");
+    cgTrueResid_ = std::sqrt(rb[0]);
+  }
   stageEnd(5);
   stageBegin(6);
   ConstFaceField noneSv{{nullptr, nullptr, nullptr}};
@@ -595,7 +623,7 @@ void GridSolver::computePressure() {
            "gradient");
   if (opt_.report_divergence) {
     const int nb = divergenceBlocks();
-    divScratch_.alloc(2 * nb + 1, stream_);
+    divScratch_.alloc(2 * nb + 2, stream_);
     divTicket_.alloc(2, stream_);
     launched(launchDivergenceNorm(g_, cvel(ni), solidTable(), markers_.p, divScratch_.p, divTicket_.p,
                                   divScratch_.p + 2 * nb, stream_),
@@ -657,6 +685,11 @@ void GridSolver::update() {
       float ms = 0.f;
       if (cudaEventElapsedTime(&ms, ev_[2 * i], ev_[2 * i + 1]) == cudaSuccess) stageMs_[i] = ms;
       else stageMs_[i] = 0.f;
+    }
+    if (adv_ != HFG_ADV_SEMI_LAGRANGIAN) {
+      float ms = 0.f;
+      partMs_[0] = cudaEventElapsedTime(&ms, ev_[16], ev_[17]) == cudaSuccess ? ms : 0.f;
+      partMs_[2] = cudaEventElapsedTime(&ms, ev_[20], ev_[21]) == cudaSuccess ? ms : 0.f;
     }
     cudaGetLastError();
   }
@@ -839,6 +872,7 @@ void GridSolver::getStats(hfg_stats_t* st) {
   st->divergence_max = divMax_;
   st->cg_residual = cgResid_;
   st->cg_rhs_norm = cgBnorm_;
+  st->cg_true_residual = cgTrueResid_;
   st->cg_converged = cgConverged_;
   st->substeps = substeps_;
   st->extrapolation_layers = extrapDepth_;
@@ -846,6 +880,7 @@ void GridSolver::getStats(hfg_stats_t* st) {
   st->num_particles = P_;
   st->fluid_cells = fluidCells_;
   for (int i = 0; i < 8; ++i) st->stage_ms[i] = stageMs_[i];
+  for (int i = 0; i < 3; ++i) st->particle_ms[i] = partMs_[i];
 }
 
 }  // namespace hfg

@@ -230,7 +230,7 @@ class GridSolver {
   long long cgIters_ = 0;
   double cgResid_ = 0, cgBnorm_ = 0;
   int cgConverged_ = 0, substeps_ = 0, extrapDepth_ = 0;
-  double divL2_ = 0, divMax_ = 0;
+  double divL2_ = 0, divMax_ = 0, cgTrueResid_ = -1.0;
   DArray<double> divScratch_;     // with report_divergence: reduction partials + sum
   DArray<unsigned> divTicket_;
   long long fluidCells_ = -1;
@@ -241,7 +241,11 @@ class GridSolver {
   cudaGraphExec_t cgGraph_[3] = {nullptr, nullptr, nullptr};
 
   bool timing_ = false;
-  cudaEvent_t ev_[16] = {};
+  // stages 0-7: events 2i, 2i+1; the particle transfers of the advection
+  // stage: G2P 16/17, each chunk of substeps 18/19, P2G 20/21
+  static constexpr int kEvents = 22;
+  cudaEvent_t ev_[kEvents] = {};
+  float partMs_[3] = {0.f, 0.f, 0.f};  // G2P, substeps (sum over chunks), P2G
   float stageMs_[8] = {};
 };
 

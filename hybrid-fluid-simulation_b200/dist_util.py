@@ -11,17 +11,12 @@ from __future__ import annotations
 
 from typing import List, Sequence, Tuple
 
-# Device bytes of one scene, per cell and per particle, from GridSolver's
-# allocations (hfg_solver.cu): two face-velocity buffers, the FLIP copy,
-# colour/domain double buffers, markers, solid index, stencil code, CG vectors,
-# P2G accumulators, extrapolation distance + bucket list.
-BYTES_PER_CELL = 3 * 4 * 2 + 3 * 4 + (3 * 2 + 2) * 4 + 1 + 1 + 2 + 4 * 4 + 3 * 8 + 3 * (2 + 4)
-BYTES_PER_PARTICLE = 12 * 4 + 4
 
-
-def scene_bytes(res: Sequence[int], particles: int) -> int:
-    n = int(res[0]) * int(res[1]) * int(res[2])
-    return n * BYTES_PER_CELL + particles * BYTES_PER_PARTICLE
+def scene_bytes(res: Sequence[int], particles: int, boundaries: int = 1, precond: int = 1) -> int:
+    """Device bytes of one scene: the library's own accounting
+    (hfg_scene_bytes), the footprint the scene server admits by."""
+    import hfgrid
+    return hfgrid.scene_bytes(tuple(int(v) for v in res), int(particles), boundaries, precond)
 
 
 def assign_scenes(footprints: Sequence[int], n_ranks: int, budget: int) -> Tuple[List[List[int]], List[int]]:

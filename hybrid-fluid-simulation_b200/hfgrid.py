@@ -52,11 +52,13 @@ class Stats(C.Structure):
         ("cg_converged", C.c_int), ("substeps", C.c_int), ("extrapolation_layers", C.c_int),
         ("sim_time", C.c_double), ("num_particles", C.c_longlong), ("fluid_cells", C.c_longlong),
         ("stage_ms", C.c_float * 8), ("divergence_l2", C.c_double), ("divergence_max", C.c_double),
+        ("cg_true_residual", C.c_double), ("particle_ms", C.c_float * 3),
     ]
 
     def as_dict(self) -> dict:
-        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "stage_ms"}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("stage_ms", "particle_ms")}
         d["stage_ms"] = list(self.stage_ms)
+        d["particle_ms"] = list(self.particle_ms)
         return d
 
 

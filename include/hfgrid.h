@@ -77,7 +77,8 @@ typedef struct {
   int mg_levels;          /* multigrid levels for HFG_PRECOND_MG (0 = auto) */
   int mg_smooth;          /* smoothing sweeps per level (0 = default) */
   int mg_half;            /* 1: multigrid smoothing stores in half precision */
-  int report_divergence;  /* 1: measure the divergence residual of every projection */
+  int report_divergence;  /* 1: measure the divergence residual of every projection
+                             and recompute the solve's residual ||b - A x|| in FP64 */
   int sampling;           /* HFG_SAMPLE_* of the semi-Lagrangian advection (setSamplingAlg,
                              AdvectionSolver.cpp:21-24; default trilinear) */
   int pressure_fp64;      /* 1: accumulate the pressure iterate in FP64 and take the
@@ -102,6 +103,11 @@ typedef struct {
                                cells after the projection (b as the RHS: -div u
                                plus the solid-face terms, 1/s) */
   double divergence_max;    /* max |b(u)| over the fluid cells after the projection */
+  double cg_true_residual;  /* with report_divergence: ||b - A x||_2 of the last solve,
+                               recomputed in FP64 on the GPU after it (-1 otherwise) */
+  float particle_ms[3];     /* when timing on: device time of the particle transfers of
+                               the advection stage: G2P, the substep launches (summed
+                               over their chunks), P2G with its normalisation */
 } hfg_stats_t;
 
 /* ---- library ---------------------------------------------------------- */
@@ -397,9 +403,12 @@ HFG_API int hfg_server_destroy(hfg_server_t srv);  /* drains first */
  *     array on a device: calls that overlap in time on one device race and
  *     give wrong results.  Serialise them.  Each call zeroes the accumulators
  *     it uses before scattering, so nothing has to be cleared in advance.
- *   - The first call on each device resolves the array's address on that
- *     device (the caller's current device).  Make that first call before any
- *     stream capture begins.
+ *   - Every call looks up the array's address on the caller's current
+ *     device.  With lazy module loading (the CUDA 12 default) the first call
+ *     on a device loads the library's device code there, which reserves the
+ *     8 MiB array and the code itself.  Make that first call before any
+ *     stream capture begins, and before the host's own allocator reserves
+ *     the rest of the device's memory.
  * Arguments, results and blocking behaviour are those of hfg_op_p2g_fc. */
 HFG_API int hfg_op_p2g_fc_static(const int res[3], const float origin[3], const float spacing[3], const float* pos,
                                  const float* vel, long long n, int alg, float* vx, float* vy, float* vz, float* wx,

@@ -33,8 +33,11 @@
 namespace MPhysicsAPI {
 extern "C" {
 #define MPHYSICS_REF(T) T&
+/* C++ callers keep the reference's default arguments (MPhysics.h:49-67). */
+#define MPHYSICS_DEFAULT(v) = v
 #else
 #define MPHYSICS_REF(T) T*
+#define MPHYSICS_DEFAULT(v)
 #endif
 
 #define MPHYSICS_API __attribute__((visibility("default")))
@@ -53,13 +56,18 @@ MPHYSICS_API void copyFluidSDFToCPU(const char* vSimulatorName, float* voSDF);
 MPHYSICS_API void copyFluidSDFGradientToCPU(const char* vSimulatorName, float* voSDFGradientX,
                                             float* voSDFGradientY, float* voSDFGradientZ);
 
-MPHYSICS_API unsigned int instanceRigidBoundary(const char* vSimulatorName, unsigned int vBoundaryIndex, float vPosX,
-                                                float vPosY, float vPosZ, float R00, float R01, float R02, float R10,
-                                                float R11, float R12, float R20, float R21, float R22);
-MPHYSICS_API void transformRigidBoundary(const char* vSimulatorName, unsigned int vBoundaryIndex,
-                                         unsigned int vBoundaryInstanceIndex, float vPosX, float vPosY, float vPosZ,
-                                         float R00, float R01, float R02, float R10, float R11, float R12, float R20,
-                                         float R21, float R22);
+MPHYSICS_API unsigned int instanceRigidBoundary(
+    const char* vSimulatorName, unsigned int vBoundaryIndex, float vPosX MPHYSICS_DEFAULT(0.0f),
+    float vPosY MPHYSICS_DEFAULT(0.0f), float vPosZ MPHYSICS_DEFAULT(0.0f), float R00 MPHYSICS_DEFAULT(1.0f),
+    float R01 MPHYSICS_DEFAULT(0.0f), float R02 MPHYSICS_DEFAULT(0.0f), float R10 MPHYSICS_DEFAULT(0.0f),
+    float R11 MPHYSICS_DEFAULT(1.0f), float R12 MPHYSICS_DEFAULT(0.0f), float R20 MPHYSICS_DEFAULT(0.0f),
+    float R21 MPHYSICS_DEFAULT(0.0f), float R22 MPHYSICS_DEFAULT(1.0f));
+MPHYSICS_API void transformRigidBoundary(
+    const char* vSimulatorName, unsigned int vBoundaryIndex, unsigned int vBoundaryInstanceIndex,
+    float vPosX MPHYSICS_DEFAULT(0.0f), float vPosY MPHYSICS_DEFAULT(0.0f), float vPosZ MPHYSICS_DEFAULT(0.0f),
+    float R00 MPHYSICS_DEFAULT(1.0f), float R01 MPHYSICS_DEFAULT(0.0f), float R02 MPHYSICS_DEFAULT(0.0f),
+    float R10 MPHYSICS_DEFAULT(0.0f), float R11 MPHYSICS_DEFAULT(1.0f), float R12 MPHYSICS_DEFAULT(0.0f),
+    float R20 MPHYSICS_DEFAULT(0.0f), float R21 MPHYSICS_DEFAULT(0.0f), float R22 MPHYSICS_DEFAULT(1.0f));
 MPHYSICS_API unsigned int getParticleSize(const char* vSimulatorName);
 MPHYSICS_API unsigned int getEulerParticleSize(const char* vSimulatorName);
 MPHYSICS_API unsigned int getNeighborDataSize(const char* vSimulatorName);

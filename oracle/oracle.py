@@ -2,7 +2,8 @@
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
 CPU-baseline leg of bench.py, never by the product.  The oracle restates the
-reference's grid step on the CPU (FP32 operation-by-operation, or FP64).
+reference's grid step on the CPU (FP32 with every operation rounded separately, in
+the reference's order, or FP64).
 """
 from __future__ import annotations
 

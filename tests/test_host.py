@@ -110,10 +110,20 @@ def _rank_main(rank, world, port, out):
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         m = dist_util.max_over_ranks(10.0 + rank)
+        # the library's own footprints of served scenes (hfg_scene_bytes)
         fp = [dist_util.scene_bytes((32 + 8 * i, 40, 48), 1000 * i) for i in range(7)]
         placed, rejected = dist_util.assign_scenes(fp, world, 10**9)
         same = dist_util.agree([i for p in placed for i in p] + [-1] + rejected)
-        out.put((rank, m, placed[rank], same))
+        # each rank's server statistics, gathered and merged as bench.py does
+        import bench
+        mine = {"submitted": len(placed[rank]), "completed": len(placed[rank]), "failed": 0, "rejected": 0,
+                "cell_steps": float(sum(fp[i] for i in placed[rank])), "peak_bytes": 1, "wall_s": 1.0 + rank,
+                "step_ms_p50": 2.0 + rank, "step_ms_p99": 5.0 + rank, "request_ms_p50": 1.0, "request_ms_p99": 3.0,
+                "failed_ids": [], "slots": 4}
+        gathered = [None] * world
+        dist.all_gather_object(gathered, mine)
+        merged = bench.merge_server_stats(gathered)
+        out.put((rank, m, placed[rank], same, merged))
     finally:
         dist.destroy_process_group()
 
@@ -126,13 +136,46 @@ def test_two_ranks_gloo():
     procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
     for p in procs:
         p.start()
-    res = sorted(q.get(timeout=120) for _ in range(2))
+    res = sorted((q.get(timeout=120) for _ in range(2)), key=lambda r: r[0])
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
     assert res[0][1] == res[1][1] == 11.0          # max over ranks
     assert res[0][3] and res[1][3]                 # identical assignment on both ranks
     assert sorted(res[0][2] + res[1][2]) == list(range(7))
+    fp = [dist_util.scene_bytes((32 + 8 * i, 40, 48), 1000 * i) for i in range(7)]
+    for merged in (res[0][4], res[1][4]):
+        assert merged["completed"] == 7 and merged["ranks"] == 2
+        assert merged["cell_steps"] == float(sum(fp))      # work adds up over ranks
+        assert merged["wall_s"] == 2.0 and merged["step_ms_p99"] == 6.0  # the slowest rank
+        assert merged["mcell_steps_per_s"] == merged["cell_steps"] / 2.0 / 1e6
+
+
+def test_rank_plan_for_two_gpus():
+    """`bench.py --gpus 2` outside torchrun starts two ranks of itself on
+    this node, rendezvous on 127.0.0.1, with its own arguments."""
+    import bench
+    cmd = bench.rank_plan(2, 29512)
+    assert cmd[1:3] == ["-m", "torch.distributed.run"]
+    assert "--nproc-per-node=2" in cmd and "--nnodes=1" in cmd
+    assert "--master-addr=127.0.0.1" in cmd and "--master-port=29512" in cmd
+    assert cmd[cmd.index("--master-port=29512") + 1].endswith("bench.py")
+
+
+def test_bench_starts_its_ranks(tmp_path):
+    """The reference arm through the self-launch with --gpus 2: rank 0 prints
+    the one line (n_gpus 2), rank 1 exits without work."""
+    import json
+    import subprocess
+    import sys
+    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2", "--steps", "1",
+           "--warmup", "3", "--cpu-sample-res", "16"]
+    out = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.strip().startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["config"]["res"] == [16, 16, 16]
 
 
 HOST_SRC = r"""
@@ -144,6 +187,11 @@ int main(void) {
   hfg_default_options(&o);
   %(ns)sloadScene("{ \"HybridSimulator\": 3 }");
   printf("%%s|%%d|%%u\n", %(ns)smphysics_last_error(), o.precond, %(ns)sgetParticleSize("none"));
+#ifdef __cplusplus
+  /* the reference's default arguments (MPhysics.h:49-67) */
+  unsigned int inst = MPhysicsAPI::instanceRigidBoundary("none", 0);
+  MPhysicsAPI::transformRigidBoundary("none", 0, inst);
+#endif
   return 0;
 }
 """

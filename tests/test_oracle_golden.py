@@ -139,8 +139,8 @@ def test_pressure_golden(name):
 
 
 def test_pressure_fp32_matches_fp64_on_golden_case():
-    """The FP32 oracle (operation-by-operation like the reference) and the
-    FP64 oracle agree on the 4^3 PCG known answer (MatrixFreePCG1)."""
+    """The FP32 oracle (each operation rounded to FP32) and the FP64 oracle
+    agree on the 4^3 PCG known answer (MatrixFreePCG1)."""
     off, vf, sf, h, dt = PRESSURE["PressureSolver_MatrixFreePCG1"]
     t = case("PressureSolver", "PressureSolver_MatrixFreePCG1")
     res = tuple(t["res"]["Res"])

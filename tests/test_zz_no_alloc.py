@@ -27,11 +27,22 @@ def _particles(rng, n):
     return pos, vel
 
 
-def test_static_p2g_rejects_oversized_grids():
+# (nx+1) ny nz + nx (ny+1) nz + nx ny (nz+1) faces: exactly the limit, and one over
+AT_LIMIT = (33, 46, 226)     # 1,048,576 faces
+ONE_OVER = (17, 85, 236)     # 1,048,577 faces
+
+
+def _faces(res):
+    return sum(int(np.prod(s)) for s in oracle.face_shapes(res))
+
+
+@pytest.mark.parametrize("res", [ONE_OVER, (101, 100, 100)])
+def test_static_p2g_rejects_oversized_grids(res):
     """The size check comes before any device work, so it runs without a GPU."""
+    assert _faces(ONE_OVER) == (1 << 20) + 1 and _faces(AT_LIMIT) == 1 << 20
     lib = hfgrid.lib()
     out = ctypes.c_void_p(16)  # never dereferenced: the call is rejected first
-    rc = lib.hfg_op_p2g_fc_static(hfgrid._i3((101, 100, 100)), hfgrid._f3(ORIGIN), hfgrid._f3(SPACING), None, None,
+    rc = lib.hfg_op_p2g_fc_static(hfgrid._i3(res), hfgrid._f3(ORIGIN), hfgrid._f3(SPACING), None, None,
                                   0, 2, out, out, out, None, None, None, None)
     assert rc == -1  # HFG_ERR_INVALID
     msg = lib.hfg_last_error().decode()
@@ -59,12 +70,11 @@ def test_static_p2g_matches_allocating_entry_point(cuda, alg):
             rw, gw = ref_w[a].cpu().numpy(), got_w[a].cpu().numpy()
             np.testing.assert_allclose(gw, rw, rtol=1e-5, atol=1e-5 * max(1.0, float(np.abs(rw).max())))
             np.testing.assert_allclose(g, r, rtol=1e-4, atol=1e-5 * max(1.0, float(np.abs(r).max())))
-    # the largest grid the fixed array holds, with every face weighted
-    res = (64, 64, 64)
-    faces = sum(int(np.prod(s)) for s in oracle.face_shapes(res))
-    assert faces <= 1 << 20
+    # a grid of exactly 2^20 faces: the z faces end on the array's last entry
+    res = AT_LIMIT
+    assert _faces(res) == 1 << 20
     rng = np.random.default_rng(79)
-    pos = (rng.random((300000, 3)) * 64).astype(np.float32)
+    pos = (rng.random((300000, 3)) * np.array(res)).astype(np.float32)
     vel = rng.standard_normal((300000, 3)).astype(np.float32)
     pd, vd = torch.from_numpy(pos).to(cuda), torch.from_numpy(vel).to(cuda)
     ref = [torch.empty(s, dtype=torch.float32, device=cuda) for s in oracle.face_shapes(res)]
