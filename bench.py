@@ -594,7 +594,7 @@ def run_dam_break(args):
                        "cells": N, "particles": n, "l2": "state > L2 (no flush needed)",
                        "parallelism": f"replicas x{world}", "convergence_one_more_step": conv,
                        "stage_ms_one_more_step": stage_ms, "particle_ms_one_more_step": particle_ms},
-            "roofline": {"bound": "hbm", "kernel": "kSubstepStaged (one CFL particle substep)",
+            "roofline": {"bound": "hbm", "kernel": "kSubstep (one CFL particle substep)",
                          "achieved": sub_achieved, "peak": hbm, "unit": "GB/s", "frac": sub_achieved / hbm,
                          "traffic": None, "algorithmic_bytes_per_launch": sub_bytes,
                          "bytes_per_particle": SUBSTEP_BYTES_PER_PARTICLE, "ms_per_launch": sub_launch_ms,

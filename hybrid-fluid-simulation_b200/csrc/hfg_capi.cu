@@ -1,6 +1,7 @@
 // hfg_capi.cu -- the extern "C" boundary of libhfgrid.so (declared in
 // include/hfgrid.h).  Exceptions never cross it: every entry point returns a
 // status and records the message for hfg_last_error().
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -23,6 +24,8 @@ int fail(int code, const std::string& msg) {
   return code;
 }
 
+std::atomic<int> g_allocFailAfter{0};
+
 template <class F> int guarded(F&& f) {
   try {
     return f();
@@ -36,6 +39,17 @@ template <class F> int guarded(F&& f) {
     return fail(HFG_ERR_INVALID, "unknown error");
   }
 }
+
+}  // namespace
+
+bool hfg::injectedAllocFailure() {
+  int n = g_allocFailAfter.load(std::memory_order_relaxed);
+  while (n > 0 && !g_allocFailAfter.compare_exchange_weak(n, n - 1)) {
+  }
+  return n == 1;  // this allocation took the count from 1 to 0
+}
+
+namespace {
 
 #define NEED(c, msg) \
   if (!(c)) return fail(HFG_ERR_INVALID, msg)
@@ -76,6 +90,48 @@ extern "C" {
 
 HFG_API const char* hfg_last_error(void) { return g_lastError.c_str(); }
 HFG_API const char* hfg_version(void) { return "hfgrid 0.1 (sm_100a)"; }
+
+HFG_API int hfg_test_inject_alloc_failure(int after) {
+  return guarded([&]() -> int {
+    NEED(after >= 0, "invalid arguments");
+    g_allocFailAfter.store(after);
+    return HFG_OK;
+  });
+}
+
+HFG_API int hfg_tune_save(const char* path) {
+  return guarded([&]() -> int {
+    NEED(path, "invalid arguments");
+    if (!saveTuning(path)) return fail(HFG_ERR_INVALID, std::string("cannot write ") + path);
+    return HFG_OK;
+  });
+}
+
+HFG_API int hfg_tune_load(const char* path, int* entries) {
+  return guarded([&]() -> int {
+    NEED(path, "invalid arguments");
+    const int n = loadTuning(path);
+    if (n < 0) return fail(HFG_ERR_INVALID, std::string("cannot read ") + path);
+    if (entries) *entries = n;
+    return HFG_OK;
+  });
+}
+
+HFG_API int hfg_selftest_bounded_waits(int wait_ms, int* mbarrier_timed_out, int* grid_barrier_timed_out) {
+  return guarded([&]() -> int {
+    NEED(wait_ms > 0 && wait_ms <= 10000 && mbarrier_timed_out && grid_barrier_timed_out, "invalid arguments");
+    DArray<unsigned> words;
+    DArray<int> out;
+    words.alloc(3);
+    out.alloc(2);
+    check(launchSelftestWaits((unsigned long long)wait_ms * 1000000ull, words.p, out.p, nullptr), "self-test");
+    int h[2] = {-1, -1};
+    check(cudaMemcpy(h, out.p, sizeof(h), cudaMemcpyDeviceToHost), "read");
+    *mbarrier_timed_out = h[0];
+    *grid_barrier_timed_out = h[1];
+    return HFG_OK;
+  });
+}
 
 HFG_API void hfg_default_options(hfg_options_t* o) {
   if (!o) return;

@@ -446,7 +446,7 @@ __device__ __forceinline__ unsigned ldAcquire(const unsigned* p) {
 }
 
 // ---------------------------------------------------------------------------
-// mbarrier and bulk-copy (TMA) plumbing shared by the streaming kernels.
+// mbarrier plumbing of the TMA-fed kernels.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t smemAddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -476,31 +476,6 @@ __device__ __forceinline__ bool mbarWait(uint64_t* bar, unsigned parity, unsigne
     if (globalNs() > deadline) return false;
   return true;
 }
-// Untiled bulk copy global -> shared, completion counted on `bar` (16-byte
-// aligned addresses, size a multiple of 16).
-__device__ __forceinline__ void bulkLoad(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smemAddr(dst)),
-      "l"(src), "r"(bytes), "r"(smemAddr(bar))
-      : "memory");
-}
-// Untiled bulk copy shared -> global in the thread's current bulk group.
-__device__ __forceinline__ void bulkStore(void* dst, const void* src, unsigned bytes) {
-  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smemAddr(src)),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void bulkCommit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-// Waits until at most N of this thread's bulk groups still read shared memory.
-template <int N> __device__ __forceinline__ void bulkWaitRead() {
-  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
-}
-// Waits until all of this thread's bulk groups have completed.
-__device__ __forceinline__ void bulkWaitAll() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-// Orders this thread's generic-proxy shared-memory writes before later
-// async-proxy (bulk copy) reads of them.
-__device__ __forceinline__ void fenceProxyAsyncShared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
 // Grid barrier of a cooperative launch (generation counting).  The wait is
 // bounded: past the deadline, or once another block has given up, the error
 // word is set and false returned, and the caller stops.

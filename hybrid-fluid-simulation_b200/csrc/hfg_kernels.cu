@@ -1232,198 +1232,8 @@ __global__ void __launch_bounds__(256, 4) kSubstep(Geom g, FaceQuads vel, float*
     st[slot + 1].count = cur.count + 1;
   }
 }
-// The same substep with the particle stream staged through shared memory by
-// bulk copies.  Each block of this persistent kernel walks chunks of
-// kChunk particles (chunk c = blockIdx.x + k gridDim.x); one thread keeps
-// kStreamStages chunks of positions and v0 in flight with
-// cp.async.bulk loads (one mbarrier per stage) and writes every finished
-// chunk back with cp.async.bulk stores from a double-buffered output tile.
-// The load/store instructions of the stream (three 4-byte accesses per
-// particle and array, 12 bytes apart) leave the LSU, which then serves only
-// the corner-table gathers.  A partial last chunk uses plain loads.
-constexpr int kChunk = kThreads;               // particles per chunk, one per thread
-constexpr int kStreamStages = 3;
-constexpr unsigned kChunkBytes = 12u * kChunk;  // one array's chunk: 3072 bytes, a multiple of 16
-constexpr unsigned long long kStreamWaitNs = 2000000000ull;
-
-struct __align__(128) SubstepSmem {
-  float in[kStreamStages][2][3 * kChunk];  // [stage][pos, v0][xyz of the chunk]
-  float out[2][2][3 * kChunk];             // [buffer][pos, v0]
-  uint64_t bar[kStreamStages];
-};
-
-// One particle's substep: q and w0 in, q (moved) and w0 (the next v0) out;
-// returns |v0 next|max, or 0 on the last substep.
-__device__ __forceinline__ float substepOne(const Geom& g, const FaceQuads& vel, int acc, float ds, float half,
-                                            float tq, float a29, float a39, float a49, bool last, bool clampIt,
-                                            float q[3], float w0[3]) {
-  if (acc == 0) {
-#pragma unroll
-    for (int a = 0; a < 3; ++a) q[a] = fmaf(ds, w0[a], q[a]);
-  } else if (acc == 1) {
-    float mid[3], w1[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) mid[a] = fmaf(half, w0[a], q[a]);
-    sampleFaceQuads(vel, g, mid[0], mid[1], mid[2], w1);
-#pragma unroll
-    for (int a = 0; a < 3; ++a) q[a] = fmaf(ds, w1[a], q[a]);
-  } else {
-    float mid[3], tf[3], acc3[3], w[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      mid[a] = fmaf(half, w0[a], q[a]);
-      acc3[a] = fmaf(a29, w0[a], q[a]);
-    }
-    sampleFaceQuads(vel, g, mid[0], mid[1], mid[2], w);
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      tf[a] = fmaf(tq, w[a], q[a]);
-      acc3[a] = fmaf(a39, w[a], acc3[a]);
-    }
-    sampleFaceQuads(vel, g, tf[0], tf[1], tf[2], w);
-#pragma unroll
-    for (int a = 0; a < 3; ++a) q[a] = fmaf(a49, w[a], acc3[a]);
-  }
-  if (last) {
-    if (clampIt) {
-      const float bmin[3] = {g.ox, g.oy, g.oz};
-      const float bmax[3] = {g.ox + (float)g.r.x * g.hx, g.oy + (float)g.r.y * g.hy, g.oz + (float)g.r.z * g.hz};
-#pragma unroll
-      for (int a = 0; a < 3; ++a) q[a] = fmaxf(bmin[a], fminf(q[a], bmax[a]));
-    }
-    return 0.f;
-  }
-  sampleFaceQuads(vel, g, q[0], q[1], q[2], w0);
-  return fmaxf(fabsf(w0[0]), fmaxf(fabsf(w0[1]), fabsf(w0[2])));
-}
-
-__global__ void __launch_bounds__(kThreads, 3) kSubstepStaged(Geom g, FaceQuads vel, float* __restrict__ pos,
-                                                             float* __restrict__ v0, long long P, int acc, float dt,
-                                                             float cfl, long long nclamp, SubstepState* st, int slot) {
-  const SubstepState cur = st[slot];
-  if (cur.finished) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) st[slot + 1] = cur;
-    return;
-  }
-  extern __shared__ __align__(128) unsigned char smemRaw[];
-  SubstepSmem& sm = *reinterpret_cast<SubstepSmem*>(smemRaw);
-  const float minH = fminf(fminf(g.hx, g.hy), g.hz);
-  bool last;
-  const float ds = substepSize(cur, dt, cfl, minH, last);
-  const float half = (float)(0.5 * (double)ds), tq = (float)(0.75 * (double)ds);
-  const float a29 = (float)(2.0 / 9.0 * (double)ds), a39 = (float)(3.0 / 9.0 * (double)ds),
-              a49 = (float)(4.0 / 9.0 * (double)ds);
-  const int t = threadIdx.x;
-  const long long nFull = P / kChunk;  // chunks moved by bulk copies
-  const long long mine = nFull > blockIdx.x ? (nFull - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-  auto chunkOf = [&](long long k) { return (long long)blockIdx.x + k * gridDim.x; };
-  if (t == 0) {
-    for (int s = 0; s < kStreamStages; ++s) mbarInit(&sm.bar[s], 1);
-    mbarFenceInit();
-    for (long long k = 0; k < mine && k < kStreamStages; ++k) {
-      const long long c = chunkOf(k);
-      mbarExpectTx(&sm.bar[k], 2 * kChunkBytes);
-      bulkLoad(sm.in[k][0], pos + 3 * c * kChunk, kChunkBytes, &sm.bar[k]);
-      bulkLoad(sm.in[k][1], v0 + 3 * c * kChunk, kChunkBytes, &sm.bar[k]);
-    }
-  }
-  __syncthreads();
-  float m = 0.f;
-  bool ok = true;
-  long long k = 0;
-  for (; k < mine; ++k) {
-    const int s = (int)(k % kStreamStages), o = (int)(k & 1);
-    const long long c = chunkOf(k);
-    if (!mbarWait(&sm.bar[s], (unsigned)((k / kStreamStages) & 1), globalNs() + kStreamWaitNs)) {
-      ok = false;  // this thread gave up; the block stops below
-    }
-    if (!__syncthreads_and(ok)) {
-      ok = false;
-      break;
-    }
-    float q[3], w0[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      q[a] = sm.in[s][0][3 * t + a];
-      w0[a] = sm.in[s][1][3 * t + a];
-    }
-    // every thread has its inputs; the stage takes the chunk kStreamStages on,
-    // and the output buffer of two chunks back has been read by its store
-    if (t == 0) bulkWaitRead<1>();
-    __syncthreads();
-    if (t == 0 && k + kStreamStages < mine) {
-      const long long cn = chunkOf(k + kStreamStages);
-      mbarExpectTx(&sm.bar[s], 2 * kChunkBytes);
-      bulkLoad(sm.in[s][0], pos + 3 * cn * kChunk, kChunkBytes, &sm.bar[s]);
-      bulkLoad(sm.in[s][1], v0 + 3 * cn * kChunk, kChunkBytes, &sm.bar[s]);
-    }
-    const long long p = c * kChunk + t;
-    m = fmaxf(m, substepOne(g, vel, acc, ds, half, tq, a29, a39, a49, last, p < nclamp, q, w0));
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      sm.out[o][0][3 * t + a] = q[a];
-      sm.out[o][1][3 * t + a] = w0[a];
-    }
-    fenceProxyAsyncShared();
-    __syncthreads();
-    if (t == 0) {
-      bulkStore(pos + 3 * c * kChunk, sm.out[o][0], kChunkBytes);
-      if (!last) bulkStore(v0 + 3 * c * kChunk, sm.out[o][1], kChunkBytes);
-      bulkCommit();
-    }
-  }
-  if (!ok && t == 0) {
-    atomicExch(&st[slot + 1].error, 1);
-    // the loads this block issued land before its shared memory is released
-    const unsigned long long deadline = globalNs() + kStreamWaitNs;
-    for (long long j = k; j < mine && j < k + kStreamStages; ++j)
-      if (!mbarWait(&sm.bar[j % kStreamStages], (unsigned)((j / kStreamStages) & 1), deadline)) break;
-  }
-  // the partial last chunk, by the block that would own it, with plain loads
-  if (ok && P % kChunk != 0 && blockIdx.x == (unsigned)(nFull % gridDim.x)) {
-    const long long p = nFull * kChunk + t;
-    if (p < P) {
-      float q[3] = {pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]};
-      float w0[3] = {v0[3 * p], v0[3 * p + 1], v0[3 * p + 2]};
-      m = fmaxf(m, substepOne(g, vel, acc, ds, half, tq, a29, a39, a49, last, p < nclamp, q, w0));
-      pos[3 * p] = q[0]; pos[3 * p + 1] = q[1]; pos[3 * p + 2] = q[2];
-      if (!last) { v0[3 * p] = w0[0]; v0[3 * p + 1] = w0[1]; v0[3 * p + 2] = w0[2]; }
-    }
-  }
-  if (t == 0) bulkWaitAll();
-  if (!last) blockMaxToGlobal(m, &st[slot + 1].maxAbsBits);
-  if (blockIdx.x == 0 && t == 0) {
-    st[slot + 1].subTime = __fadd_rn(cur.subTime, ds);
-    st[slot + 1].finished = last ? 1 : 0;
-    st[slot + 1].count = cur.count + 1;
-  }
-}
-
-namespace {
-int stagedSubstepGrid() {
-  static int grid = 0;
-  if (grid == 0) {
-    int perSM = 0;
-    if (cudaFuncSetAttribute(kSubstepStaged, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sizeof(SubstepSmem)) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kSubstepStaged, kThreads, sizeof(SubstepSmem)) !=
-            cudaSuccess ||
-        perSM < 1)
-      perSM = 1;
-    grid = numSMs() * perSM;
-  }
-  return grid;
-}
-}  // namespace
-
 cudaError_t launchSubstep(const Geom& g, FaceQuads vel, float* pos, float* v0, long long P, int acc, float dt,
                           float cfl, long long nclamp, SubstepState* st, int slot, cudaStream_t s) {
-  const bool aligned = ((reinterpret_cast<uintptr_t>(pos) | reinterpret_cast<uintptr_t>(v0)) & 15u) == 0;
-  if (aligned && P >= kChunk) {
-    int grid = (int)std::min<long long>(stagedSubstepGrid(), (P + kChunk - 1) / kChunk);
-    kSubstepStaged<<<grid, kThreads, sizeof(SubstepSmem), s>>>(g, vel, pos, v0, P, acc, dt, cfl, nclamp, st, slot);
-    return cudaGetLastError();
-  }
   if (index32(P))
     kSubstep<int><<<gridFor(P > 0 ? P : 1), kThreads, 0, s>>>(g, vel, pos, v0, P, acc, dt, cfl, nclamp, st, slot);
   else
@@ -1801,6 +1611,38 @@ __global__ void kAddConst(long long n, float* __restrict__ v, float a) {
 }
 cudaError_t launchAddConst(long long n, float* v, float a, cudaStream_t s) {
   kAddConst<<<gridFor(n), kThreads, 0, s>>>(n, v, a);
+  return cudaGetLastError();
+}
+
+// ===========================================================================
+// Self-test of the bounded waits.  Every wait of the TMA-fed and cooperative
+// kernels is bounded: past its limit it records an error and returns, so the
+// context stays usable.  These two kernels make the shared wait helpers run
+// out on purpose, on conditions that nothing will ever satisfy, without any
+// fault: an mbarrier phase expecting bytes no copy will deliver, and a grid
+// barrier expecting one arrival more than the grid has blocks.
+// ===========================================================================
+__global__ void kSelftestMbarrier(unsigned long long waitNs, int* out) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbarInit(&bar, 1);
+    mbarFenceInit();
+    mbarExpectTx(&bar, 16);  // this thread arrives; 16 bytes stay pending for good
+    const bool done = mbarWait(&bar, 0, globalNs() + waitNs);
+    out[0] = done ? 0 : 1;
+  }
+}
+__global__ void kSelftestGridBarrier(unsigned* words, int* out) {
+  // words: count, generation, error
+  const bool ok = gridBarrier(words, words + 1, words + 2, gridDim.x + 1);
+  if (threadIdx.x == 0 && blockIdx.x == 0) out[1] = ok ? 0 : 1;
+}
+cudaError_t launchSelftestWaits(unsigned long long waitNs, unsigned* words, int* out, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(words, 0, 3 * sizeof(unsigned), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(out, 0xff, 2 * sizeof(int), s);
+  if (e != cudaSuccess) return e;
+  kSelftestMbarrier<<<1, 32, 0, s>>>(waitNs, out);
+  kSelftestGridBarrier<<<2, 32, 0, s>>>(words, out);
   return cudaGetLastError();
 }
 

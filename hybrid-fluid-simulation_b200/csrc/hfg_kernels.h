@@ -3,6 +3,7 @@
 // cudaGetLastError() of its launch.
 #pragma once
 #include <cstdint>
+#include <vector>
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -47,7 +48,6 @@ struct SubstepState {
   float subTime;            // time advanced so far
   int finished;
   int count;
-  int error;                // nonzero: a block gave up waiting for its particle stream
 };
 
 struct SolidVelTable {
@@ -129,13 +129,28 @@ cudaError_t makeCgMaps(const Dim3i& cg, const CgCode* code, const float* r, cons
 cudaError_t makeHaloMap(const Dim3i& cg, const float* v, CUtensorMap* m);
 // precond: 0 identity, 1 Jacobi, 2 z read through mZ (must match CgState::precond);
 // mZ is the halo map of r (precond 0, 1) or of z (2); zr the same array.
+// colZ (optional, from launchFluidColumns): the fluid extent of every tile
+// column; blocks whose planes hold no fluid skip their stream.
 cudaError_t launchCgDirection(const Dim3i& cg, float sx, float sy, float sz, const CUtensorMap& mZ,
                               const CUtensorMap& mPo, const CUtensorMap& mCode, const CgCode* code, const float* zr,
                               const float* pOld, float* pNew, double* partials, CgState* st, int precond,
-                              cudaStream_t s);
+                              cudaStream_t s, const int* colZ = nullptr);
 cudaError_t launchCgUpdate(const Dim3i& cg, float sx, float sy, float sz, const CUtensorMap& mP, const CUtensorMap& mR,
                            const CUtensorMap& mX, const CUtensorMap& mCode, const float* p, void* x, bool xDouble,
-                           float* r, double* partials, CgState* st, int precond, cudaStream_t s);
+                           float* r, double* partials, CgState* st, int precond, cudaStream_t s,
+                           const int* colZ = nullptr);
+// Measured launch shapes of the CG kernels (family 0 direction, 1 update):
+// the z-chunk length used for the pitched grid cg, <= 0 erases.  The table is
+// process wide; saveTuning/loadTuning keep it in a text file.
+void setTunedCgZPer(int family, const Dim3i& cg, int zPer);
+int tunedCgZPer(int family, const Dim3i& cg);  // -1: none
+std::vector<int> cgZPerCandidates(const Dim3i& cg);
+bool saveTuning(const char* path);
+int loadTuning(const char* path);  // entries read, -1 if the file cannot be opened
+// Fluid extent of the CG tile columns (32 x 16 cells of the pitched grid cg,
+// all z), from the CG codes: colZ holds 2 * cgColumns(cg) ints.
+int cgColumns(const Dim3i& cg);
+cudaError_t launchFluidColumns(const Dim3i& cg, const CgCode* code, int* colZ, cudaStream_t s);
 // Divergence residual of the projected velocity over the fluid cells:
 // *sumOut = sum b^2 (FP64), ticketAndMax[1] = bits of max |b|.  `scratch`
 // holds 2 * divergenceBlocks() doubles.
@@ -258,5 +273,10 @@ cudaError_t launchSampleAlg(const Geom& g, int face, ConstFaceField f, const flo
 
 // ---- external forces (unit-field axpy on every face) ------------------------
 cudaError_t launchAddConst(long long n, float* v, float a, cudaStream_t s);
+
+// Runs the bounded-wait helpers against conditions nothing satisfies: out[0]
+// = 1 once an mbarrier wait of waitNs ran out, out[1] = 1 once a grid barrier
+// missing one arrival gave up (its own 1 s limit).  words: 3 scratch words.
+cudaError_t launchSelftestWaits(unsigned long long waitNs, unsigned* words, int* out, cudaStream_t s);
 
 }  // namespace hfg

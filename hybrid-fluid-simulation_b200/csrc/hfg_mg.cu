@@ -642,7 +642,8 @@ void mgSetup(Multigrid* m, const Dim3i& r, const uint8_t* mk0, const Code* code,
 // immediately once the state says done.
 void mgRunCg(Multigrid* m, const Dim3i& cg, float sx, float sy, float sz, const CgMaps& maps, const CgCode* code, void* x,
              bool xDouble, float* rvec, CgState* st, CgState* stHost, cudaStream_t s, long long& launches,
-             const std::function<cudaGraphExec_t(const std::function<void()>&)>& capture, cudaGraphExec_t* chunk) {
+             const std::function<cudaGraphExec_t(const std::function<void()>&)>& capture, cudaGraphExec_t* chunk,
+             const int* colZ) {
   // both direction buffers start zero: the CG kernels never store at non-fluid
   // cells, and the fluid moves between solves
   check(cudaMemsetAsync(m->p[0].p, 0, m->p[0].bytes(), s), "memset");
@@ -659,10 +660,10 @@ void mgRunCg(Multigrid* m, const Dim3i& cg, float sx, float sy, float sz, const 
       const int po = it & 1, pn = (it + 1) & 1;
       const int zi = z == m->z0a.p ? 0 : 1;
       check(launchCgDirection(cg, sx, sy, sz, m->zH[zi], m->pH[po], maps.codeH, code, z, m->p[po].p, m->p[pn].p,
-                              m->partials.p, st, 2, s),
+                              m->partials.p, st, 2, s, colZ),
             "cg direction");
       check(launchCgUpdate(cg, sx, sy, sz, m->pH[pn], maps.rI, maps.xI, maps.codeI, m->p[pn].p, x, xDouble, rvec,
-                           m->partials.p, st, 2, s),
+                           m->partials.p, st, 2, s, colZ),
             "cg update");
       launches += 2;
       z = mgVcycle(m, rvec, st, s, launches);

@@ -10,9 +10,12 @@
 // along z keeping the below / current / above planes in registers, so the z
 // neighbours cost no extra loads and no division is needed for indexing.
 #include <algorithm>
+#include <cstdio>
 #include <map>
 #include <mutex>
+#include <string>
 #include <utility>
+#include <vector>
 
 #include "hfg_kernels.h"
 
@@ -484,6 +487,17 @@ struct CgLaunch {
   int zPer;
 };
 
+// Fluid extent of the CG tile columns (CTX x CTR cells of the pitched grid,
+// every z): colZ[t] the lowest and colZ[cols + t] the highest plane holding a
+// fluid cell of column t = blockIdx.y * gridDim.x + blockIdx.x, or a range
+// that no chunk meets when the column has none.  Null: every block active.
+__device__ __forceinline__ bool columnActive(const int* colZ, int z0, int z1) {
+  if (!colZ) return true;
+  const unsigned cols = gridDim.x * gridDim.y, t = blockIdx.y * gridDim.x + blockIdx.x;
+  const int lo = __ldg(colZ + t), hi = __ldg(colZ + cols + t);
+  return lo < z1 && hi >= z0;
+}
+
 // Tiles over (x, y), z split into chunks so that the blocks fill whole waves
 // of the resident slots (wave count x chunk length minimal, chunks of at
 // least 3 planes).
@@ -499,12 +513,81 @@ int residentBlocks(const void* kernel) {
   return per;
 }
 
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Launch shapes picked by measurement.  autotuneCg (driven by the solver)
+// times the CG kernels of a grid for every z-chunk length in kTuneZPer and
+// records the fastest per kernel family; cgLaunch prefers a recorded shape to
+// its cost model.  The table is process wide and can be saved and loaded.
+namespace {
+constexpr int kTuneZPer[] = {3, 4, 5, 6, 8, 10, 12, 16, 20, 24, 32, 48, 64};
+std::mutex g_tuneMu;
+std::map<std::string, int> g_tune;  // "cg<family> nx ny nz" -> zPer
+
+std::string tuneKey(int family, const Dim3i& cg) {
+  return "cg" + std::to_string(family) + " " + std::to_string(cg.x) + " " + std::to_string(cg.y) + " " +
+         std::to_string(cg.z);
+}
+int tunedZPer(int family, const Dim3i& cg) {
+  std::lock_guard<std::mutex> lk(g_tuneMu);
+  auto it = g_tune.find(tuneKey(family, cg));
+  return it == g_tune.end() ? -1 : it->second;
+}
+}  // namespace
+
+void setTunedCgZPer(int family, const Dim3i& cg, int zPer) {
+  std::lock_guard<std::mutex> lk(g_tuneMu);
+  if (zPer > 0) g_tune[tuneKey(family, cg)] = zPer;
+  else g_tune.erase(tuneKey(family, cg));
+}
+int tunedCgZPer(int family, const Dim3i& cg) { return tunedZPer(family, cg); }
+std::vector<int> cgZPerCandidates(const Dim3i& cg) {
+  std::vector<int> v;
+  for (int z : kTuneZPer)
+    if (z <= cg.z) v.push_back(z);
+  if (v.empty()) v.push_back(cg.z);
+  return v;
+}
+bool saveTuning(const char* path) {
+  std::lock_guard<std::mutex> lk(g_tuneMu);
+  FILE* f = std::fopen(path, "w");
+  if (!f) return false;
+  std::fprintf(f, "# hfgrid launch shapes: cg<family 0 direction, 1 update> px ny nz zPer\n");
+  for (const auto& kv : g_tune) std::fprintf(f, "%s %d\n", kv.first.c_str(), kv.second);
+  return std::fclose(f) == 0;
+}
+int loadTuning(const char* path) {
+  FILE* f = std::fopen(path, "r");
+  if (!f) return -1;
+  char name[16];
+  int x, y, z, per, n = 0;
+  char line[256];
+  while (std::fgets(line, sizeof line, f)) {
+    if (line[0] == '#') continue;
+    if (std::sscanf(line, "%15s %d %d %d %d", name, &x, &y, &z, &per) != 5) continue;
+    if ((std::string(name) != "cg0" && std::string(name) != "cg1") || per < 1 || per > z) continue;
+    setTunedCgZPer(name[2] - '0', Dim3i{x, y, z}, per);
+    ++n;
+  }
+  std::fclose(f);
+  return n;
+}
+
+namespace {
+// family: 0 for kCgDirection, 1 for kCgUpdate (the key of the tuning table)
 template <class K>
-CgLaunch cgLaunch(const Dim3i& cg, K kernel) {
-  long long slots = (long long)numSMs() * residentBlocks((const void*)kernel);
+CgLaunch cgLaunch(const Dim3i& cg, K kernel, int family) {
   CgLaunch L;
   L.block = dim3(CTX, CTY, 1);
   int bx = (cg.x + CTX - 1) / CTX, by = (cg.y + CTR - 1) / CTR;
+  const int tuned = tunedZPer(family, cg);
+  if (tuned > 0) {
+    L.zPer = std::min(tuned, cg.z);
+    L.grid = dim3(bx, by, (cg.z + L.zPer - 1) / L.zPer);
+    return L;
+  }
+  long long slots = (long long)numSMs() * residentBlocks((const void*)kernel);
   long long tiles = (long long)bx * by;
   long long best = -1;
   int bestPer = cg.z;
@@ -538,7 +621,7 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
     kCgDirection(const __grid_constant__ CUtensorMap mZ, const __grid_constant__ CUtensorMap mPo,
                  const __grid_constant__ CUtensorMap mCode, Dim3i P, float sx, float sy, float sz,
                  const CgCode* __restrict__ code, const float* __restrict__ zr, const float* __restrict__ pOld,
-                 float* __restrict__ pNew, double* partials, CgState* st, int zPer) {
+                 float* __restrict__ pNew, double* partials, CgState* st, int zPer, const int* __restrict__ colZ) {
   __shared__ DirStage stg[kDirStages];
   __shared__ float pt[2][FH][CTX + 2];
   __shared__ DiagTab tab;
@@ -547,7 +630,10 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * CTX + tx;
   const int x0 = blockIdx.x * CTX, y0 = blockIdx.y * CTR;
   const int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, P.z);
-  const int nPlanes = z1 - z0, nLoad = nPlanes + 1;  // plane z1 is the last "above"
+  // a block whose planes hold no fluid cell of its tile column writes
+  // nothing and adds zero to the reduction: it skips the stream
+  const bool active = columnActive(colZ, z0, z1);
+  const int nPlanes = active ? z1 - z0 : 0, nLoad = nPlanes + 1;  // plane z1 is the last "above"
   auto issue = [&](int i) {
     DirStage& S = stg[i % kDirStages];
     uint64_t* b = &bar[i % kDirStages];
@@ -566,7 +652,7 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
   if (st->done) return;  // the same value in every thread
   allowNextGrid();
   if (tid == 0) {
-    int n = min(kDirStages, nLoad);
+    int n = active ? min(kDirStages, nLoad) : 0;
     for (int i = 0; i < n; ++i) issue(i);
     issued = n;
   }
@@ -585,7 +671,7 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
     c[j] = (unsigned)z0 * plane + (unsigned)y * (unsigned)P.x + (unsigned)x;
     // p of the plane below the chunk, own cell only
     below[j] = 0.f;
-    if (in[j] && z0 > 0) {
+    if (active && in[j] && z0 > 0) {
       unsigned b = c[j] - plane;
       below[j] = fmaf(beta, __ldg(pOld + b), fastZ<PC>(tab.e[__ldg(code + b)].y, __ldg(zr + b)));
     }
@@ -616,12 +702,12 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
       t[row][right ? CTX + 1 : 0] = pAt(row, right ? HXF + CTX : HXF - 1, right ? HXC + CTX : HXC - 1);
     }
   };
-  bool ok = mbarWait(&bar[0], 0, deadline);
-  if (ok) formTile(0, pt[0], cur, dCur);
-  int waited = 1;
+  bool ok = !active || mbarWait(&bar[0], 0, deadline);
+  if (ok && active) formTile(0, pt[0], cur, dCur);
+  int waited = active ? 1 : 0;
   bool fail = __syncthreads_or(!ok);
-  if (!fail && tid == 0 && kDirStages < nLoad) issue(kDirStages), issued = kDirStages + 1;
-  float acc = 0.f;
+  if (active && !fail && tid == 0 && kDirStages < nLoad) issue(kDirStages), issued = kDirStages + 1;
+  double acc = 0.0;  // FP64 dot partials: each product rounded to FP64, summed in FP64
   for (int i = 0; i < nPlanes && !fail; ++i) {
     ok = mbarWait(&bar[(i + 1) % kDirStages], (unsigned)(((i + 1) / kDirStages) & 1), deadline);
     waited = i + 2;
@@ -634,7 +720,7 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
         float q = rowSum(dCur[j], sx, sy, sz, cur[j], t[row][tx], t[row][tx + 2], t[row - 1][tx + 1],
                          t[row + 1][tx + 1], below[j], above[j]);
         pNew[c[j]] = cur[j];
-        acc = fmaf(cur[j], q, acc);
+        acc = fma((double)cur[j], (double)q, acc);
       }
       below[j] = cur[j];
       cur[j] = above[j];
@@ -651,7 +737,7 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
     }
     return;
   }
-  double pq = (double)acc, dummy = 0.0;
+  double pq = acc, dummy = 0.0;
   if (gridSum2(pq, dummy, partials, &st->ticket) && flatTid() == 0) {
     st->pAp = pq;
     st->alpha = (float)(st->rz / pq);
@@ -663,14 +749,15 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
 // of the stage ring), z = M^-1 r, the reductions r.r and r.z; the last block
 // checks convergence and forms beta (CuMatrixFreePCG.cpp:49-63).  The
 // |alpha| < FLT_EPSILON skip of CCuDenseVector::plusAlphaX
-// (CuDenseVector.cpp:178) is kept.  Per-thread partial sums run over one
-// z-column segment in FP32 and are combined in FP64.
+// (CuDenseVector.cpp:178) is kept.  The dot products accumulate in FP64 from
+// the first product: per-thread partials over one z-column segment, then a
+// fixed-order FP64 reduction over the grid.
 template <int PC, class TX>
 __global__ void __launch_bounds__(CTX* CTY, 4)
     kCgUpdate(const __grid_constant__ CUtensorMap mP, const __grid_constant__ CUtensorMap mR,
               const __grid_constant__ CUtensorMap mX, const __grid_constant__ CUtensorMap mCode, Dim3i P, float sx,
               float sy, float sz, const float* __restrict__ p, TX* __restrict__ xv, float* __restrict__ r,
-              double* partials, CgState* st, int zPer) {
+              double* partials, CgState* st, int zPer, const int* __restrict__ colZ) {
   constexpr int kUpdStages = kUpdStagesT<TX>;
   using Stage = UpdStage<TX>;
   __shared__ Stage stg[kUpdStages];
@@ -680,7 +767,8 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * CTX + tx;
   const int x0 = blockIdx.x * CTX, y0 = blockIdx.y * CTR;
   const int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, P.z);
-  const int nPlanes = z1 - z0, nLoad = nPlanes + 1;
+  const bool active = columnActive(colZ, z0, z1);  // as in kCgDirection
+  const int nPlanes = active ? z1 - z0 : 0, nLoad = nPlanes + 1;
   auto issue = [&](int i) {
     Stage& S = stg[i % kUpdStages];
     uint64_t* b = &bar[i % kUpdStages];
@@ -700,7 +788,7 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
   if (st->done) return;  // the same value in every thread
   allowNextGrid();
   if (tid == 0) {
-    int n = min(kUpdStages, nLoad);
+    int n = active ? min(kUpdStages, nLoad) : 0;
     for (int i = 0; i < n; ++i) issue(i);
     issued = n;
   }
@@ -717,14 +805,14 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
     const int y = y0 + ty + j * CTY;
     in[j] = x < P.x && y < P.y;
     c[j] = (unsigned)z0 * plane + (unsigned)y * (unsigned)P.x + (unsigned)x;
-    below[j] = (in[j] && z0 > 0) ? __ldg(p + c[j] - plane) : 0.f;
+    below[j] = (active && in[j] && z0 > 0) ? __ldg(p + c[j] - plane) : 0.f;
   }
-  bool ok = mbarWait(&bar[0], 0, deadline);
+  bool ok = !active || mbarWait(&bar[0], 0, deadline);
 #pragma unroll
-  for (int j = 0; j < RY; ++j) cur[j] = ok ? stg[0].p[ty + 1 + j * CTY][tx + HXF] : 0.f;
-  int waited = 1;
+  for (int j = 0; j < RY; ++j) cur[j] = (ok && active) ? stg[0].p[ty + 1 + j * CTY][tx + HXF] : 0.f;
+  int waited = active ? 1 : 0;
   bool fail = __syncthreads_or(!ok);
-  float arr = 0.f, arz = 0.f;
+  double arr = 0.0, arz = 0.0;  // FP64 dot partials
   for (int i = 0; i < nPlanes && !fail; ++i) {
     ok = mbarWait(&bar[(i + 1) % kUpdStages], (unsigned)(((i + 1) / kUpdStages) & 1), deadline);
     waited = i + 2;
@@ -749,8 +837,8 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
           r[c[j]] = rv;
         }
         float zz = fastZ<PC>(e.y, rv);
-        arr = fmaf(rv, rv, arr);
-        arz = fmaf(rv, zz, arz);
+        arr = fma((double)rv, (double)rv, arr);
+        arz = fma((double)rv, (double)zz, arz);
       }
       below[j] = cur[j];
       cur[j] = above;
@@ -766,7 +854,7 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
     }
     return;
   }
-  double rr = (double)arr, rz = (double)arz;
+  double rr = arr, rz = arz;
   if (gridSum2(rr, rz, partials, &st->ticket) && flatTid() == 0) {
     st->rr = rr;
     st->iter += 1;
@@ -841,37 +929,35 @@ int cgPartialsNeeded(const Dim3i& r) {
   const Dim3i cg = cgDims(r);
   CgGrid g = cgGrid(cg);
   long long n = (long long)g.grid.x * g.grid.y * g.grid.z;
-  CgLaunch a = cgLaunch(cg, kCgDirection<1>), b = cgLaunch(cg, kCgUpdate<1, float>),
-           d = cgLaunch(cg, kCgUpdate<1, double>);
-  n = std::max(n, (long long)a.grid.x * a.grid.y * a.grid.z);
-  n = std::max(n, (long long)b.grid.x * b.grid.y * b.grid.z);
-  n = std::max(n, (long long)d.grid.x * d.grid.y * d.grid.z);
+  // the CG kernels, at the shortest z chunk any launch shape (tuned or not) uses
+  const long long tiles = (long long)((cg.x + CTX - 1) / CTX) * ((cg.y + CTR - 1) / CTR);
+  n = std::max(n, tiles * ((cg.z + std::min(3, cg.z) - 1) / std::min(3, cg.z)));
   return 2 * (int)n;
 }
 
 cudaError_t launchCgDirection(const Dim3i& cg, float sx, float sy, float sz, const CUtensorMap& mZ,
                               const CUtensorMap& mPo, const CUtensorMap& mCode, const CgCode* code, const float* zr,
                               const float* pOld, float* pNew, double* partials, CgState* st, int precond,
-                              cudaStream_t s) {
+                              cudaStream_t s, const int* colZ) {
   switch (precond) {
     case 1: {
-      CgLaunch L = cgLaunch(cg, kCgDirection<1>);
+      CgLaunch L = cgLaunch(cg, kCgDirection<1>, 0);
       cudaError_t e = launchPdl(kCgDirection<1>, L.grid, L.block, s, mZ, mPo, mCode, cg, sx, sy, sz, code, zr, pOld,
-                                pNew, partials, st, L.zPer);
+                                pNew, partials, st, L.zPer, colZ);
       if (e != cudaSuccess) return e;
       break;
     }
     case 2: {
-      CgLaunch L = cgLaunch(cg, kCgDirection<2>);
+      CgLaunch L = cgLaunch(cg, kCgDirection<2>, 0);
       cudaError_t e = launchPdl(kCgDirection<2>, L.grid, L.block, s, mZ, mPo, mCode, cg, sx, sy, sz, code, zr, pOld,
-                                pNew, partials, st, L.zPer);
+                                pNew, partials, st, L.zPer, colZ);
       if (e != cudaSuccess) return e;
       break;
     }
     default: {
-      CgLaunch L = cgLaunch(cg, kCgDirection<0>);
+      CgLaunch L = cgLaunch(cg, kCgDirection<0>, 0);
       cudaError_t e = launchPdl(kCgDirection<0>, L.grid, L.block, s, mZ, mPo, mCode, cg, sx, sy, sz, code, zr, pOld,
-                                pNew, partials, st, L.zPer);
+                                pNew, partials, st, L.zPer, colZ);
       if (e != cudaSuccess) return e;
     }
   }
@@ -880,12 +966,12 @@ cudaError_t launchCgDirection(const Dim3i& cg, float sx, float sy, float sz, con
 
 cudaError_t launchCgUpdate(const Dim3i& cg, float sx, float sy, float sz, const CUtensorMap& mP, const CUtensorMap& mR,
                            const CUtensorMap& mX, const CUtensorMap& mCode, const float* p, void* x, bool xDouble,
-                           float* r, double* partials, CgState* st, int precond, cudaStream_t s) {
+                           float* r, double* partials, CgState* st, int precond, cudaStream_t s, const int* colZ) {
 #define HFG_CG_UPDATE(PCV, TXV)                                                                                   \
   {                                                                                                               \
-    CgLaunch L = cgLaunch(cg, kCgUpdate<PCV, TXV>);                                                             \
+    CgLaunch L = cgLaunch(cg, kCgUpdate<PCV, TXV>, 1);                                                             \
     cudaError_t e = launchPdl(kCgUpdate<PCV, TXV>, L.grid, L.block, s, mP, mR, mX, mCode, cg, sx, sy, sz, p,      \
-                              (TXV*)x, r, partials, st, L.zPer);                                              \
+                              (TXV*)x, r, partials, st, L.zPer, colZ);                                        \
     if (e != cudaSuccess) return e;                                                                             \
   }
   if (xDouble) {
@@ -898,6 +984,46 @@ cudaError_t launchCgUpdate(const Dim3i& cg, float sx, float sy, float sz, const 
     else HFG_CG_UPDATE(0, float)
   }
 #undef HFG_CG_UPDATE
+  return cudaGetLastError();
+}
+
+// Fluid extent of every CG tile column: one block per (column, z slice)
+// reduces the fluid planes of its slice; the column's range is their
+// min / max (atomics into colZ, set up by the launcher).
+__global__ void kFluidColumns(Dim3i cg, const CgCode* __restrict__ code, int zPer, int* colZ) {
+  const int x = blockIdx.x * CTX + threadIdx.x, y = blockIdx.y * CTR + threadIdx.y;
+  const int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, cg.z);
+  int lo = 0x7fffffff, hi = -1;
+  if (x < cg.x && y < cg.y)
+    for (int z = z0; z < z1; ++z)
+      if (code[((long long)z * cg.y + y) * cg.x + x] & 1) {
+        lo = min(lo, z);
+        hi = z;
+      }
+  __shared__ int sl[CTR], sh[CTR];
+  lo = __reduce_min_sync(0xffffffffu, lo);
+  hi = __reduce_max_sync(0xffffffffu, hi);
+  if (threadIdx.x == 0) { sl[threadIdx.y] = lo; sh[threadIdx.y] = hi; }
+  __syncthreads();
+  if (threadIdx.y == 0 && threadIdx.x < CTR) {
+    lo = __reduce_min_sync(0x0000ffffu, sl[threadIdx.x]);
+    hi = __reduce_max_sync(0x0000ffffu, sh[threadIdx.x]);
+    if (threadIdx.x == 0 && hi >= 0) {
+      const unsigned cols = gridDim.x * gridDim.y, t = blockIdx.y * gridDim.x + blockIdx.x;
+      atomicMin(colZ + t, lo);
+      atomicMax(colZ + cols + t, hi);
+    }
+  }
+}
+int cgColumns(const Dim3i& cg) { return ((cg.x + CTX - 1) / CTX) * ((cg.y + CTR - 1) / CTR); }
+cudaError_t launchFluidColumns(const Dim3i& cg, const CgCode* code, int* colZ, cudaStream_t s) {
+  const int cols = cgColumns(cg);
+  cudaError_t e = cudaMemsetAsync(colZ, 0x7f, sizeof(int) * cols, s);  // lo: 0x7f7f7f7f, above any plane
+  if (e == cudaSuccess) e = cudaMemsetAsync(colZ + cols, 0xff, sizeof(int) * cols, s);  // hi: -1
+  if (e != cudaSuccess) return e;
+  const int zPer = 16;
+  dim3 grid((cg.x + CTX - 1) / CTX, (cg.y + CTR - 1) / CTR, (cg.z + zPer - 1) / zPer);
+  kFluidColumns<<<grid, dim3(CTX, CTR), 0, s>>>(cg, code, zPer, colZ);
   return cudaGetLastError();
 }
 

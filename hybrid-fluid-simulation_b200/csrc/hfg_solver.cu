@@ -68,7 +68,8 @@ void mgSetup(Multigrid* m, const Dim3i& r, const uint8_t* mk0, const Code* code,
              cudaStream_t s, long long& launches);
 void mgRunCg(Multigrid* m, const Dim3i& cg, float sx, float sy, float sz, const CgMaps& maps, const CgCode* code, void* x,
              bool xDouble, float* rvec, CgState* st, CgState* stHost, cudaStream_t s, long long& launches,
-             const std::function<cudaGraphExec_t(const std::function<void()>&)>& capture, cudaGraphExec_t* chunk);
+             const std::function<cudaGraphExec_t(const std::function<void()>&)>& capture, cudaGraphExec_t* chunk,
+             const int* colZ);
 
 GridSolver::GridSolver(float dt, Dim3i res, const float origin[3], const float spacing[3]) {
   if (res.x <= 0 || res.y <= 0 || res.z <= 0) throw CudaError("resolution must be positive", HFG_ERR_INVALID);
@@ -101,6 +102,7 @@ GridSolver::GridSolver(float dt, Dim3i res, const float origin[3], const float s
   cgp_[0].alloc(NC_, stream_);
   cgp_[1].alloc(NC_, stream_);
   partials_.alloc(cgPartialsNeeded(res), stream_);
+  colZ_.alloc(2 * (size_t)cgColumns(cgDims(res)), stream_);
   check(makeCgMaps(cg_, cgc_.p, cgr_.p, cgx_.p, false, cgp_[0].p, cgp_[1].p, &maps_), "CG tensor maps");
   cgState_.alloc(1, stream_);
   subState_.alloc(subSlots_ + 1, stream_);
@@ -418,9 +420,13 @@ void GridSolver::advectParticles(const FaceQuads& v, bool haveV0) {
   long long nclamp = opt_.clamp_mode == 1 ? std::min<long long>(P_, N_) : P_;
   int slot = 0;
   partMs_[1] = 0.f;
+  // the first batch runs up to two short of the previous step's count without
+  // a read-back (the CFL rule changes the count slowly from step to step);
+  // then chunks of kSubstepChunk.  A launch past the last substep does nothing.
+  int batch = std::max(kSubstepChunk, substeps_ - 2);
   for (;;) {
     if (timing_) check(cudaEventRecord(ev_[18], stream_), "cudaEventRecord");
-    for (int k = 0; k < kSubstepChunk && slot < subSlots_; ++k, ++slot)
+    for (int k = 0; k < batch && slot < subSlots_; ++k, ++slot)
       launched(launchSubstep(g_, v, ppos_.p, pv0_.p, P_, acc_rk_, dt_, cfl_, nclamp, subState_.p, slot, stream_),
                "substep");
     if (timing_) check(cudaEventRecord(ev_[19], stream_), "cudaEventRecord");
@@ -430,9 +436,9 @@ void GridSolver::advectParticles(const FaceQuads& v, bool haveV0) {
       float ms = 0.f;
       if (cudaEventElapsedTime(&ms, ev_[18], ev_[19]) == cudaSuccess) partMs_[1] += ms;
     }
-    if (subHost_->error) throw CudaError("particle substep: a chunk load did not complete in time", HFG_ERR_TIMEOUT);
     if (subHost_->finished) { substeps_ = subHost_->count; break; }
     if (slot >= subSlots_) throw CudaError("CFL substep limit reached", HFG_ERR_STATE);
+    batch = kSubstepChunk;
   }
 }
 
@@ -499,11 +505,11 @@ void GridSolver::computeAdvection() {
 void GridSolver::cgIteration(int it, float sx, float sy, float sz, int pc) {
   const int po = it & 1, pn = (it + 1) & 1;
   launched(launchCgDirection(cg_, sx, sy, sz, maps_.rH, maps_.pH[po], maps_.codeH, cgc_.p, cgr_.p, cgp_[po].p,
-                             cgp_[pn].p, partials_.p, cgState_.p, pc, stream_),
+                             cgp_[pn].p, partials_.p, cgState_.p, pc, stream_, colZ_.p),
            "cg direction");
   launched(launchCgUpdate(cg_, sx, sy, sz, maps_.pH[pn], maps_.rI, maps_.xI, maps_.codeI, cgp_[pn].p, xPtr(), xDouble(),
                           cgr_.p,
-                          partials_.p, cgState_.p, pc, stream_),
+                          partials_.p, cgState_.p, pc, stream_, colZ_.p),
            "cg update");
 }
 
@@ -542,7 +548,7 @@ void GridSolver::runCg() {
   if (opt_.precond == HFG_PRECOND_MG) {
     auto cap = [this](const std::function<void()>& f) { return capture(f); };
     mgRunCg(mg_, cg_, sx, sy, sz, maps_, cgc_.p, xPtr(), xDouble(), cgr_.p, cgState_.p, cgHost_, stream_, launches_, cap,
-            &cgGraph_[2]);
+            &cgGraph_[2], colZ_.p);
   } else {
     const int pc = opt_.precond == HFG_PRECOND_JACOBI ? 1 : 0;
     // kCgChunk is even, so every chunk starts on the same p buffer
@@ -550,13 +556,22 @@ void GridSolver::runCg() {
       cgGraph_[pc] = capture([&] {
         for (int k = 0; k < kCgChunk; ++k) cgIteration(k, sx, sy, sz, pc);
       });
+    // as many chunks as the previous solve needed, less one, go out before the
+    // first convergence read; every kernel of a chunk past convergence returns
+    // at once
+    int batch = std::max(1, cgChunks_ - 1), chunks = 0;
     for (;;) {
-      check(cudaGraphLaunch(cgGraph_[pc], stream_), "cg chunk");
-      launches_ += 2 * kCgChunk;
+      for (int k = 0; k < batch; ++k) {
+        check(cudaGraphLaunch(cgGraph_[pc], stream_), "cg chunk");
+        launches_ += 2 * kCgChunk;
+        ++chunks;
+      }
       readBack(cgHost_, cgState_.p, sizeof(CgState), stream_);
       check(cudaStreamSynchronize(stream_), "cg sync");
       if (cgHost_->done) break;
+      batch = 1;
     }
+    cgChunks_ = (cgHost_->iter + kCgChunk - 1) / kCgChunk;
   }
   if (cgHost_->error) throw CudaError("pressure CG: a stage load did not complete in time", HFG_ERR_TIMEOUT);
 }
@@ -572,6 +587,7 @@ void GridSolver::computePressure() {
     launched(launchMarkersFromParticles(g_, ppos_.p, P_, markers_.p, stream_), "markers");
   }
   launched(launchStencilCode(g_.r, cg_.x, markers_.p, code_.p, stream_, cgc_.p), "stencil code");
+  launched(launchFluidColumns(cg_, cgc_.p, colZ_.p, stream_), "fluid columns");
   stageEnd(3);
   stageBegin(4);
   CgState init{};
@@ -590,6 +606,16 @@ void GridSolver::computePressure() {
   // the CG kernels never store at non-fluid cells, and the fluid moves between
   // solves: the second direction buffer starts zero too
   check(cudaMemsetAsync(cgp_[1].p, 0, cgp_[1].bytes(), stream_), "memset");
+  if (opt_.autotune && opt_.precond != HFG_PRECOND_MG && tunedCgZPer(0, cg_) < 0) {
+    // measure the launch shapes on this system, then set the solve up again
+    autotuneCg(sx, sy, sz, init.precond);
+    *cgHost_ = init;
+    check(cudaMemcpyAsync(cgState_.p, cgHost_, sizeof(CgState), cudaMemcpyHostToDevice, stream_), "cg state");
+    launched(launchRhsInit(g_, cvel(ni), none, solidTable(), markers_.p, code_.p, sx, sy, sz, nullptr, cgr_.p, xPtr(),
+                           xDouble(), cgp_[0].p, partials_.p, cgState_.p, init.precond, stream_),
+             "rhs");
+    check(cudaMemsetAsync(cgp_[1].p, 0, cgp_[1].bytes(), stream_), "memset");
+  }
   if (opt_.precond == HFG_PRECOND_MG) mgSetup(mg_, g_.r, markers_.p, code_.p, sx, sy, sz, stream_, launches_);
   stageEnd(4);
   stageBegin(5);
@@ -696,6 +722,67 @@ void GridSolver::update() {
 }
 
 void GridSolver::synchronize() { check(cudaStreamSynchronize(stream_), "sync"); }
+
+// The autotuner: every candidate z-chunk length of the CG kernels is timed on
+// the current system (a few iterations each, events around every kernel) and
+// the fastest per kernel is recorded for this grid size.  The iterations
+// change x, r and p; the caller sets the solve up again afterwards.  The
+// captured CG graphs hold launch shapes, so they are dropped.
+void GridSolver::autotuneCg(float sx, float sy, float sz, int pc) {
+  constexpr int kIters = 4;
+  const std::vector<int> cands = cgZPerCandidates(cg_);
+  cudaEvent_t e[3 * kIters + 1];
+  for (auto& x : e) check(cudaEventCreate(&x), "cudaEventCreate");
+  float best[2] = {1e30f, 1e30f};
+  int pick[2] = {cands[0], cands[0]};
+  CgState st{};
+  st.maxIter = 0x7fffffff;
+  st.precond = pc;
+  st.tolMode = HFG_TOL_RELATIVE;
+  st.tol = 0.0;  // never converges: every launch does its work
+  st.rz = 1.0;
+  st.bb = 1.0;
+  try {
+    for (int z : cands) {
+      setTunedCgZPer(0, cg_, z);
+      setTunedCgZPer(1, cg_, z);
+      *cgHost_ = st;
+      check(cudaMemcpyAsync(cgState_.p, cgHost_, sizeof(CgState), cudaMemcpyHostToDevice, stream_), "cg state");
+      cgIteration(0, sx, sy, sz, pc);  // warm-up
+      for (int it = 0; it < kIters; ++it) {
+        const int po = it & 1, pn = po ^ 1;
+        check(cudaEventRecord(e[3 * it], stream_), "event");
+        launched(launchCgDirection(cg_, sx, sy, sz, maps_.rH, maps_.pH[po], maps_.codeH, cgc_.p, cgr_.p,
+                                   cgp_[po].p, cgp_[pn].p, partials_.p, cgState_.p, pc, stream_, colZ_.p),
+                 "cg direction");
+        check(cudaEventRecord(e[3 * it + 1], stream_), "event");
+        launched(launchCgUpdate(cg_, sx, sy, sz, maps_.pH[pn], maps_.rI, maps_.xI, maps_.codeI, cgp_[pn].p, xPtr(),
+                                xDouble(), cgr_.p, partials_.p, cgState_.p, pc, stream_, colZ_.p),
+                 "cg update");
+        check(cudaEventRecord(e[3 * it + 2], stream_), "event");
+      }
+      check(cudaEventSynchronize(e[3 * kIters - 1]), "event sync");
+      float t[2] = {0.f, 0.f};
+      for (int it = 0; it < kIters; ++it)
+        for (int k = 0; k < 2; ++k) {
+          float ms = 0.f;
+          check(cudaEventElapsedTime(&ms, e[3 * it + k], e[3 * it + k + 1]), "elapsed");
+          t[k] += ms;
+        }
+      for (int k = 0; k < 2; ++k)
+        if (t[k] < best[k]) { best[k] = t[k]; pick[k] = z; }
+    }
+  } catch (...) {
+    for (auto& x : e) cudaEventDestroy(x);
+    setTunedCgZPer(0, cg_, -1);
+    setTunedCgZPer(1, cg_, -1);
+    throw;
+  }
+  for (auto& x : e) cudaEventDestroy(x);
+  setTunedCgZPer(0, cg_, pick[0]);
+  setTunedCgZPer(1, cg_, pick[1]);
+  dropGraphs();
+}
 
 float GridSolver::timeCg(int iters) {
   if (iters <= 0) throw CudaError("iterations must be positive", HFG_ERR_INVALID);

@@ -25,6 +25,11 @@ struct CudaError : std::runtime_error {
 
 void check(cudaError_t e, const char* what);
 
+// Host-side injection of a device allocation failure, for the failure-path
+// tests: once armed with n >= 1, the n-th following DArray allocation fails
+// as cudaMalloc would (HFG_ERR_NOMEM) without calling it.  Disarmed: 0.
+bool injectedAllocFailure();
+
 // Owning device array.  With a stream the memory comes from the
 // stream-ordered allocator and is returned with cudaFreeAsync on the same
 // stream, so creating and destroying scenes never synchronises the device
@@ -50,6 +55,7 @@ template <class T> struct DArray {
     if (count == n && p) return;
     release();
     if (count == 0) return;
+    if (injectedAllocFailure()) throw CudaError("device allocation failed: injected by the test hook", HFG_ERR_NOMEM);
     cudaError_t e;
     if (stream) e = cudaMallocAsync((void**)&p, count * sizeof(T), stream);
     else e = cudaMalloc((void**)&p, count * sizeof(T));
@@ -152,6 +158,7 @@ class GridSolver {
   void computePressure();
   void runCg();
   void cgIteration(int it, float sx, float sy, float sz, int pc);
+  void autotuneCg(float sx, float sy, float sz, int pc);
   // Records what f() launches on the solver's stream as an executable graph.
   template <class F> cudaGraphExec_t capture(F&& f);
   void dropGraphs();
@@ -197,11 +204,13 @@ class GridSolver {
   bool xDouble() const { return opt_.pressure_fp64 != 0; }
   void* xPtr() { return xDouble() ? (void*)cgx64_.p : (void*)cgx_.p; }
   DArray<double> partials_;
+  DArray<int> colZ_;  // fluid extent of the CG tile columns (launchFluidColumns), per solve
   DArray<CgState> cgState_;
   CgState* cgHost_ = nullptr;  // pinned
   DArray<SubstepState> subState_;
   SubstepState* subHost_ = nullptr;  // pinned
   int subSlots_ = 4096;
+  int cgChunks_ = 0;  // CG chunks the last Jacobi/identity solve needed
   DArray<float2> acc_[3], cacc_;
   DArray<float4> quads_[3];  // corner tables of the advecting velocity (particle substeps)
   DArray<uint16_t> dist_;

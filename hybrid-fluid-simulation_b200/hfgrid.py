@@ -42,7 +42,7 @@ class Options(C.Structure):
         ("precond", C.c_int), ("tol_mode", C.c_int), ("tol", C.c_double), ("max_iter", C.c_longlong),
         ("clamp_mode", C.c_int), ("advect_scalars", C.c_int), ("extrapolation_layers", C.c_int),
         ("mg_levels", C.c_int), ("mg_smooth", C.c_int), ("mg_half", C.c_int), ("report_divergence", C.c_int),
-        ("sampling", C.c_int), ("pressure_fp64", C.c_int),
+        ("sampling", C.c_int), ("pressure_fp64", C.c_int), ("autotune", C.c_int),
     ]
 
 
@@ -198,6 +198,10 @@ def _signatures(lib):
         "hfg_server_destroy": (C.c_int, [VP]),
         "hfg_op_seed_particles": (C.c_int, [I3, F3, F3, VP, VP, C.c_int, C.c_ulonglong, VP, C.c_longlong,
                                             C.POINTER(C.c_longlong), VP]),
+        "hfg_selftest_bounded_waits": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "hfg_test_inject_alloc_failure": (C.c_int, [C.c_int]),
+        "hfg_tune_save": (C.c_int, [C.c_char_p]),
+        "hfg_tune_load": (C.c_int, [C.c_char_p, C.POINTER(C.c_int)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -223,6 +227,30 @@ def _check(code: int):
 
 def init(device: int = 0):
     _check(lib().hfg_init(device))
+
+
+def selftest_bounded_waits(wait_ms: int = 20):
+    """(mbarrier wait timed out, grid barrier timed out) of the wait self-test."""
+    a, b = C.c_int(), C.c_int()
+    _check(lib().hfg_selftest_bounded_waits(wait_ms, C.byref(a), C.byref(b)))
+    return a.value, b.value
+
+
+def tune_save(path: str):
+    """Write the autotuner's launch shapes to `path`."""
+    _check(lib().hfg_tune_save(path.encode()))
+
+
+def tune_load(path: str) -> int:
+    """Add the launch shapes in `path` to the table; returns the entries read."""
+    n = C.c_int()
+    _check(lib().hfg_tune_load(path.encode(), C.byref(n)))
+    return n.value
+
+
+def inject_alloc_failure(after: int):
+    """Make the after-th device allocation from now on fail (0 disarms)."""
+    _check(lib().hfg_test_inject_alloc_failure(after))
 
 
 def default_options() -> Options:

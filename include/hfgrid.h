@@ -85,6 +85,12 @@ typedef struct {
                              gradient's differences in FP64 (the reference keeps
                              it in FP32, which bounds the divergence of the
                              projected field near 1e-4 of ||b|| on large grids) */
+  int autotune;           /* 1: on the first Jacobi / identity solve of a grid size,
+                             time the CG kernels at every candidate z-chunk length
+                             and keep the fastest for that size (process wide;
+                             hfg_tune_save / hfg_tune_load keep it across runs).
+                             The reference's fixed launch shape is
+                             EulerSolverTool.cu:650-656. */
 } hfg_options_t;
 
 typedef struct {
@@ -113,6 +119,21 @@ typedef struct {
 /* ---- library ---------------------------------------------------------- */
 HFG_API int hfg_init(int device);
 HFG_API const char* hfg_last_error(void);
+/* Self-test of the bounded waits every TMA-fed and cooperative kernel uses
+ * (no reference counterpart): an mbarrier wait of wait_ms on bytes no copy
+ * delivers, and a grid barrier missing one arrival (its own 1 s limit), both
+ * on the current device.  Each must give up and report it (*..._timed_out =
+ * 1), leaving the context usable; no fault is involved. */
+HFG_API int hfg_selftest_bounded_waits(int wait_ms, int* mbarrier_timed_out, int* grid_barrier_timed_out);
+/* Failure injection on the host (no reference counterpart): the after-th
+ * device allocation of the library from now on fails as cudaMalloc would
+ * (HFG_ERR_NOMEM), without calling it.  0 disarms. */
+HFG_API int hfg_test_inject_alloc_failure(int after);
+/* The launch shapes measured by the autotuner (option autotune), as a text
+ * file of "cg<0 direction | 1 update> px ny nz zchunk" lines; loading adds to
+ * the table and sets *entries.  No reference counterpart. */
+HFG_API int hfg_tune_save(const char* path);
+HFG_API int hfg_tune_load(const char* path, int* entries);
 HFG_API const char* hfg_version(void);
 HFG_API void hfg_default_options(hfg_options_t* o);
 

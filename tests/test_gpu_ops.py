@@ -171,6 +171,32 @@ def test_extrapolation_bit_exact(cuda):
         assert np.array_equal(host(vd[a]), ref3[a])
 
 
+def test_extrapolation_large_layers_bit_exact(cuda):
+    """Layers far larger than the one-block path takes (kExtrapSmallLayer =
+    4096 entries): a 96^3 face grid known only in a small blob, so the layer
+    at distance d holds ~d^2 faces (up to ~11,900) and the grid-strided path
+    with the bounded grid barrier between layers runs for most of the ~160
+    layers.  Values and
+    the UNKNOWN entries left must equal the oracle's bit for bit."""
+    rng = np.random.default_rng(17)
+    res = (96, 96, 96)
+    U = np.finfo(np.float32).max
+    v = face_arrays(res, rng)
+    for a in range(3):
+        keep = np.zeros(v[a].shape, bool)
+        keep[40:48, 44:52, 20:30] = rng.random((8, 8, 10)) < 0.7
+        v[a][~keep] = U
+    ref = oracle.extrapolate_fc(res, v, 1000)
+    for a in range(3):
+        _, mk = oracle.extrapolate(v[a].shape[::-1], v[a], 1000, with_markers=True)
+        widths = np.bincount(mk[mk != U].astype(np.int64))
+        assert (widths > 4096).sum() >= 50 and widths.max() > 11000  # the large-layer path runs
+    vd = [dev(a) for a in v]
+    hfgrid.op_extrapolate_fc(res, vd, 1000)
+    for a in range(3):
+        assert np.array_equal(host(vd[a]), ref[a])
+
+
 def test_extrapolation_cc_layers(cuda):
     rng = np.random.default_rng(8)
     res = (31, 7, 5)
