@@ -248,6 +248,35 @@ def serve_requests(args, rng, batch=False):
     return out
 
 
+def scene_descs(args, reqs, precond):
+    import hfgrid
+    return [hfgrid.scene_desc(r["res"], steps=args.scene_steps, spheres=r["spheres"], fluid_max=r["fluid_max"],
+                              seed=r["seed"], precond=precond, tol_mode=hfgrid.TOL_RELATIVE, tol=1e-6,
+                              max_iter=200) for r in reqs]
+
+
+def run_batched(args, reqs, precond, device=0):
+    """All scenes resident and stepped together through hfg_batch_*: the CFL
+    substeps of every scene in one launch per substep, replayed from a graph."""
+    import hfgrid
+    descs = scene_descs(args, reqs, precond)
+    t0 = time.perf_counter()
+    b = hfgrid.Batch(descs, threads=args.slots, device=device)
+    setup_s = time.perf_counter() - t0
+    ms = b.step(args.scene_steps)
+    cells = sum(int(r["res"][0]) * int(r["res"][1]) * int(r["res"][2]) for r in reqs)
+    subs = [b.stats(i)["substeps"] for i in range(len(reqs))]
+    b.close()
+    step_s = sum(ms) / 1e3
+    cs = float(cells * args.scene_steps)
+    # like the server's wall time, from the first scene built to the last step
+    wall_s = setup_s + step_s
+    return {"scenes": len(reqs), "steps": args.scene_steps, "step_ms": ms, "cell_steps": cs, "setup_s": setup_s,
+            "wall_s": wall_s, "mcell_steps_per_s": cs / max(wall_s, 1e-9) / 1e6,
+            "mcell_steps_per_s_steps_only": cs / max(step_s, 1e-9) / 1e6,
+            "substeps_max": max(subs) if subs else 0, "substeps_sum": sum(subs)}
+
+
 def run_server(args, reqs, arrivals, slots, precond, device=0):
     """Submit `reqs` at their arrival times (seconds from start) to a server
     with `slots` concurrent scenes on `device`; returns its statistics."""
@@ -259,9 +288,7 @@ def run_server(args, reqs, arrivals, slots, precond, device=0):
         dt = at - (time.perf_counter() - t0)
         if dt > 0:
             time.sleep(dt)
-        ids.append(srv.submit(hfgrid.scene_desc(r["res"], steps=args.scene_steps, spheres=r["spheres"],
-                                                fluid_max=r["fluid_max"], seed=r["seed"], precond=precond,
-                                                tol_mode=hfgrid.TOL_RELATIVE, tol=1e-6, max_iter=200)))
+        ids.append(srv.submit(scene_descs(args, [r], precond)[0]))
     srv.drain()
     st = srv.stats()
     infos = [srv.info(i) for i in ids]
@@ -304,6 +331,7 @@ def run_serve(args):
     if pg is not None:
         pg.barrier()
     mixed = run_server(args, mine, at, args.slots, hfgrid.PRECOND_MG, local)
+    batched = run_batched(args, mine, hfgrid.PRECOND_MG, local) if batch and mine else None
     clk = clocks.stop()
     plain = None
     if not args.no_plain:
@@ -313,7 +341,8 @@ def run_serve(args):
     if pg is not None:
         import torch.distributed as dist
         gathered = [None] * world
-        dist.all_gather_object(gathered, {"mixed": mixed, "plain": plain, "clocks": clk, "n": len(mine)})
+        dist.all_gather_object(gathered, {"mixed": mixed, "plain": plain, "clocks": clk, "n": len(mine),
+                                          "batched": batched})
         pg.barrier()
         pg.destroy_process_group()
         if rank != 0:
@@ -321,6 +350,12 @@ def run_serve(args):
         mixed = merge_server_stats([g["mixed"] for g in gathered])
         plain = merge_server_stats([g["plain"] for g in gathered]) if plain is not None else None
         clk = gathered[0]["clocks"]
+        parts = [g["batched"] for g in gathered if g["batched"]]
+        if parts:
+            wall = max(p["wall_s"] for p in parts)
+            cs = sum(p["cell_steps"] for p in parts)
+            batched = {"scenes": sum(p["scenes"] for p in parts), "cell_steps": cs, "wall_s": wall,
+                       "mcell_steps_per_s": cs / max(wall, 1e-9) / 1e6, "ranks": len(parts)}
     line = {
         "metric": "Mcell-steps/s and step latency, " + ("batched uneven scenes" if batch else "served request stream"),
         "value": mixed["mcell_steps_per_s"], "unit": UNIT, "n_gpus": world, "higher_is_better": True,
@@ -333,6 +368,10 @@ def run_serve(args):
                    "slots": args.slots, "placement": "scenes by footprint over %d rank(s)" % world},
         "served": mixed, "clocks": clk,
     }
+    if batched is not None:
+        # all scenes resident, stepped together: one substep launch for all
+        line["batched"] = batched
+        line["batched_vs_streams"] = batched["mcell_steps_per_s"] / max(mixed["mcell_steps_per_s"], 1e-9)
     if plain is not None:
         line["plain"] = plain
         line["speedup_vs_plain"] = mixed["mcell_steps_per_s"] / max(plain["mcell_steps_per_s"], 1e-9)

@@ -1155,6 +1155,73 @@ __device__ inline float substepSize(const SubstepState& s, float dt, float cfl, 
 // box clamp of fixParticlesPosWithBoundarys (EulerParticlesTool.cu:310-333) is
 // applied to the first `nclamp` particles; otherwise the next v0 and its max
 // are produced for slot+1.
+// One particle's substep: RK1/2/3 from its v0, the box clamp after the last
+// substep, otherwise the next v0 sampled and stored; returns max |v0 next|.
+template <typename I>
+__device__ __forceinline__ float substepParticle(const Geom& g, const FaceQuads& vel, float* __restrict__ pos,
+                                                 float* __restrict__ v0, I p, int acc, float ds, float half, float tq,
+                                                 float a29, float a39, float a49, bool last, bool clampIt) {
+  float q[3] = {pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]};
+  float w0[3] = {v0[3 * p], v0[3 * p + 1], v0[3 * p + 2]};
+  float m = 0.f;
+  if (acc == 0) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) q[a] = fmaf(ds, w0[a], q[a]);
+  } else if (acc == 1) {
+    float mid[3], w1[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) mid[a] = fmaf(half, w0[a], q[a]);
+    sampleFaceQuads(vel, g, mid[0], mid[1], mid[2], w1);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) q[a] = fmaf(ds, w1[a], q[a]);
+  } else {
+    // q + a29 w0 + a39 w1 + a49 w2, in that order, accumulated as soon as
+    // each sample is known so that fewer values stay live across a sample
+    float mid[3], tf[3], acc3[3], w[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      mid[a] = fmaf(half, w0[a], q[a]);
+      acc3[a] = fmaf(a29, w0[a], q[a]);
+    }
+    sampleFaceQuads(vel, g, mid[0], mid[1], mid[2], w);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      tf[a] = fmaf(tq, w[a], q[a]);
+      acc3[a] = fmaf(a39, w[a], acc3[a]);
+    }
+    sampleFaceQuads(vel, g, tf[0], tf[1], tf[2], w);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) q[a] = fmaf(a49, w[a], acc3[a]);
+  }
+  if (last) {
+    if (clampIt) {  // the box bounds are formed here, from the kernel parameters
+      const float bmin[3] = {g.ox, g.oy, g.oz};
+      const float bmax[3] = {g.ox + (float)g.r.x * g.hx, g.oy + (float)g.r.y * g.hy, g.oz + (float)g.r.z * g.hz};
+#pragma unroll
+      for (int a = 0; a < 3; ++a) q[a] = fmaxf(bmin[a], fminf(q[a], bmax[a]));
+    }
+  } else {
+    float v[3];
+    sampleFaceQuads(vel, g, q[0], q[1], q[2], v);
+    v0[3 * p] = v[0]; v0[3 * p + 1] = v[1]; v0[3 * p + 2] = v[2];
+    m = fmaxf(fabsf(v[0]), fmaxf(fabsf(v[1]), fabsf(v[2])));
+  }
+  pos[3 * p] = q[0]; pos[3 * p + 1] = q[1]; pos[3 * p + 2] = q[2];
+  return m;
+}
+
+// The RK coefficients of a substep of size ds (EulerParticles.cpp:281-301).
+struct SubstepCoef {
+  float ds, half, tq, a29, a39, a49;
+  __device__ explicit SubstepCoef(float d)
+      : ds(d), half((float)(0.5 * (double)d)), tq((float)(0.75 * (double)d)), a29((float)(2.0 / 9.0 * (double)d)),
+        a39((float)(3.0 / 9.0 * (double)d)), a49((float)(4.0 / 9.0 * (double)d)) {}
+};
+
+// One RK1/2/3 substep (EulerParticles.cpp:277-318).  After the last substep the
+// box clamp of fixParticlesPosWithBoundarys (EulerParticlesTool.cu:310-333) is
+// applied to the first `nclamp` particles; otherwise the next v0 and its max
+// are produced for slot+1.
 template <typename I>
 __global__ void __launch_bounds__(256, 4) kSubstep(Geom g, FaceQuads vel, float* __restrict__ pos,
                                                   float* __restrict__ v0, long long P,
@@ -1167,9 +1234,7 @@ __global__ void __launch_bounds__(256, 4) kSubstep(Geom g, FaceQuads vel, float*
   }
   float minH = fminf(fminf(g.hx, g.hy), g.hz);
   bool last;
-  float ds = substepSize(cur, dt, cfl, minH, last);
-  float half = (float)(0.5 * (double)ds), tq = (float)(0.75 * (double)ds);
-  float a29 = (float)(2.0 / 9.0 * (double)ds), a39 = (float)(3.0 / 9.0 * (double)ds), a49 = (float)(4.0 / 9.0 * (double)ds);
+  const SubstepCoef k(substepSize(cur, dt, cfl, minH, last));
   float m = 0.f;
   const I stride = (I)gridDim.x * blockDim.x;
   HFG_FOR_T(I, p, P) {
@@ -1179,59 +1244,89 @@ __global__ void __launch_bounds__(256, 4) kSubstep(Geom g, FaceQuads vel, float*
       prefetchL2(pos + 3 * (p + stride));
       prefetchL2(v0 + 3 * (p + stride));
     }
-    float q[3] = {pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]};
-    float w0[3] = {v0[3 * p], v0[3 * p + 1], v0[3 * p + 2]};
-    if (acc == 0) {
-#pragma unroll
-      for (int a = 0; a < 3; ++a) q[a] = fmaf(ds, w0[a], q[a]);
-    } else if (acc == 1) {
-      float mid[3], w1[3];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) mid[a] = fmaf(half, w0[a], q[a]);
-      sampleFaceQuads(vel, g, mid[0], mid[1], mid[2], w1);
-#pragma unroll
-      for (int a = 0; a < 3; ++a) q[a] = fmaf(ds, w1[a], q[a]);
-    } else {
-      // q + a29 w0 + a39 w1 + a49 w2, in that order, accumulated as soon as
-      // each sample is known so that fewer values stay live across a sample
-      float mid[3], tf[3], acc3[3], w[3];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        mid[a] = fmaf(half, w0[a], q[a]);
-        acc3[a] = fmaf(a29, w0[a], q[a]);
-      }
-      sampleFaceQuads(vel, g, mid[0], mid[1], mid[2], w);
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        tf[a] = fmaf(tq, w[a], q[a]);
-        acc3[a] = fmaf(a39, w[a], acc3[a]);
-      }
-      sampleFaceQuads(vel, g, tf[0], tf[1], tf[2], w);
-#pragma unroll
-      for (int a = 0; a < 3; ++a) q[a] = fmaf(a49, w[a], acc3[a]);
-    }
-    if (last) {
-      if ((long long)p < nclamp) {  // the box bounds are formed here, from the kernel parameters
-        const float bmin[3] = {g.ox, g.oy, g.oz};
-        const float bmax[3] = {g.ox + (float)g.r.x * g.hx, g.oy + (float)g.r.y * g.hy, g.oz + (float)g.r.z * g.hz};
-#pragma unroll
-        for (int a = 0; a < 3; ++a) q[a] = fmaxf(bmin[a], fminf(q[a], bmax[a]));
-      }
-    } else {
-      float v[3];
-      sampleFaceQuads(vel, g, q[0], q[1], q[2], v);
-      v0[3 * p] = v[0]; v0[3 * p + 1] = v[1]; v0[3 * p + 2] = v[2];
-      m = fmaxf(m, fmaxf(fabsf(v[0]), fmaxf(fabsf(v[1]), fabsf(v[2]))));
-    }
-    pos[3 * p] = q[0]; pos[3 * p + 1] = q[1]; pos[3 * p + 2] = q[2];
+    m = fmaxf(m, substepParticle<I>(g, vel, pos, v0, p, acc, k.ds, k.half, k.tq, k.a29, k.a39, k.a49, last,
+                                    (long long)p < nclamp));
   }
   if (!last) blockMaxToGlobal(m, &st[slot + 1].maxAbsBits);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    st[slot + 1].subTime = __fadd_rn(cur.subTime, ds);
+    st[slot + 1].subTime = __fadd_rn(cur.subTime, k.ds);
     st[slot + 1].finished = last ? 1 : 0;
     st[slot + 1].count = cur.count + 1;
   }
 }
+
+// The substep `slot` of many scenes in one launch (the batched mode).  Scene
+// s owns blocks [chunkStart[s], chunkStart[s + 1]), each a chunk of
+// kMultiChunk of its particles; a block finds its scene by binary search and
+// runs that scene's substep with the scene's own CFL state, exactly as
+// kSubstep would.  Scenes whose substeps are finished do nothing.
+constexpr int kMultiChunk = 8 * kThreads;
+__global__ void __launch_bounds__(256, 3) kSubstepMulti(const SubstepTask* __restrict__ tasks,
+                                                       const long long* __restrict__ chunkStart, int nScenes,
+                                                       int slot) {
+  __shared__ int sc;
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = nScenes - 1;  // the last scene whose first chunk is <= blockIdx.x
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (chunkStart[mid] <= (long long)blockIdx.x) lo = mid;
+      else hi = mid - 1;
+    }
+    sc = lo;
+  }
+  __syncthreads();
+  const SubstepTask& T = tasks[sc];
+  const long long chunk = (long long)blockIdx.x - chunkStart[sc];
+  const SubstepState cur = T.st[slot];
+  if (cur.finished) {
+    if (chunk == 0 && threadIdx.x == 0) T.st[slot + 1] = cur;
+    return;
+  }
+  const Geom g = T.g;
+  const FaceQuads vel = T.vel;
+  const float minH = fminf(fminf(g.hx, g.hy), g.hz);
+  bool last;
+  const SubstepCoef k(substepSize(cur, T.dt, T.cfl, minH, last));
+  float m = 0.f;
+  // the chunk's particles, indexed in 32 bits from the chunk's start
+  const long long p0 = chunk * kMultiChunk;
+  const int n = (int)(min(T.P, p0 + kMultiChunk) - p0);
+  const long long nclamp = T.nclamp - p0;
+  float* pos = T.pos + 3 * p0;
+  float* v0 = T.v0 + 3 * p0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x)
+    m = fmaxf(m, substepParticle<int>(g, vel, pos, v0, i, T.acc, k.ds, k.half, k.tq, k.a29, k.a39, k.a49, last,
+                                      (long long)i < nclamp));
+  if (!last) blockMaxToGlobal(m, &T.st[slot + 1].maxAbsBits);
+  if (chunk == 0 && threadIdx.x == 0) {
+    T.st[slot + 1].subTime = __fadd_rn(cur.subTime, k.ds);
+    T.st[slot + 1].finished = last ? 1 : 0;
+    T.st[slot + 1].count = cur.count + 1;
+  }
+}
+long long multiSubstepChunks(long long P) { return (P + kMultiChunk - 1) / kMultiChunk; }
+cudaError_t launchSubstepMulti(const SubstepTask* tasks, const long long* chunkStart, int nScenes,
+                               long long totalChunks, int slot, cudaStream_t s) {
+  if (nScenes <= 0 || totalChunks <= 0) return cudaSuccess;
+  kSubstepMulti<<<(unsigned)totalChunks, kThreads, 0, s>>>(tasks, chunkStart, nScenes, slot);
+  return cudaGetLastError();
+}
+
+// finished flag and substep count of every scene's state slot `slot`, into
+// host-mapped memory (two ints per scene)
+__global__ void kGatherSubstepStates(const SubstepTask* __restrict__ tasks, int nScenes, int slot, int* out) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nScenes; s += gridDim.x * blockDim.x) {
+    const SubstepState v = tasks[s].st[slot];
+    out[2 * s] = v.finished;
+    out[2 * s + 1] = v.count;
+  }
+}
+cudaError_t launchGatherSubstepStates(const SubstepTask* tasks, int nScenes, int slot, int* out, cudaStream_t s) {
+  if (nScenes <= 0) return cudaSuccess;
+  kGatherSubstepStates<<<(nScenes + 255) / 256, 256, 0, s>>>(tasks, nScenes, slot, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launchSubstep(const Geom& g, FaceQuads vel, float* pos, float* v0, long long P, int acc, float dt,
                           float cfl, long long nclamp, SubstepState* st, int slot, cudaStream_t s) {
   if (index32(P))

@@ -50,6 +50,20 @@ struct SubstepState {
   int count;
 };
 
+// One scene's CFL substep loop as a launch sees it (GridSolver::substepTask);
+// the batch stepper runs the substeps of many scenes in one launch per slot.
+struct SubstepTask {
+  Geom g;
+  FaceQuads vel;
+  float* pos;
+  float* v0;
+  long long P;
+  long long nclamp;
+  SubstepState* st;
+  int acc;
+  float dt, cfl;
+};
+
 struct SolidVelTable {
   const uint8_t* solidIdx;  // 0 = not solid, i+1 = solid of boundary i
   float vx[kMaxBoundaries], vy[kMaxBoundaries], vz[kMaxBoundaries];
@@ -245,6 +259,14 @@ cudaError_t launchSubstepBegin(const Geom& g, FaceQuads vel, const float* pos, f
                                SubstepState* st, cudaStream_t s);
 cudaError_t launchSubstep(const Geom& g, FaceQuads vel, float* pos, float* v0, long long P, int acc, float dt,
                           float cfl, long long nclamp, SubstepState* st, int slot, cudaStream_t s);
+// Batched substeps: slot `slot` of every scene of `tasks` (device array) in one
+// launch; chunkStart[s] = sum of multiSubstepChunks(P) over scenes < s (device
+// array), totalChunks the sum over all scenes.
+long long multiSubstepChunks(long long P);
+cudaError_t launchSubstepMulti(const SubstepTask* tasks, const long long* chunkStart, int nScenes,
+                               long long totalChunks, int slot, cudaStream_t s);
+// out[2 s] = finished, out[2 s + 1] = count of scene s's state slot `slot`
+cudaError_t launchGatherSubstepStates(const SubstepTask* tasks, int nScenes, int slot, int* out, cudaStream_t s);
 cudaError_t launchP2GFace(const Geom& g, int alg, const float* pos, const float* vel, long long P, float2* acc[3],
                           cudaStream_t s);
 cudaError_t launchP2GCell(const Geom& g, int alg, const float* pos, const float* val, int span, int comp, long long P,

@@ -32,6 +32,28 @@ void setLastError(const std::string& msg);  // hfg_capi.cu
 namespace {
 using Clock = std::chrono::steady_clock;
 
+// The dam break of a scene description: walls, its spheres, the fluid box,
+// the PIC/FLIP mix and seeded particles.
+std::unique_ptr<GridSolver> buildScene(const hfg_scene_desc_t& d) {
+  Dim3i res{d.res[0], d.res[1], d.res[2]};
+  const float origin[3] = {0.f, 0.f, 0.f};
+  const float h[3] = {1.0f / d.res[0], 1.0f / d.res[1], 1.0f / d.res[2]};
+  std::unique_ptr<GridSolver> sp(new GridSolver(d.dt, res, origin, h));
+  GridSolver& s = *sp;
+  const float still[3] = {0.f, 0.f, 0.f};
+  s.addAnalyticBoundary(0, nullptr, still);
+  for (int i = 0; i < d.n_spheres; ++i) {
+    const double p[6] = {d.spheres[i][0], d.spheres[i][1], d.spheres[i][2], d.spheres[i][3], 0.0, 0.0};
+    s.addAnalyticBoundary(1, p, still);
+  }
+  const float lo[3] = {0.f, 0.f, 0.f};
+  s.fluidDomainFromBBox(lo, d.fluid_max);
+  s.setAdvection(HFG_ADV_MIX_PIC_FLIP, HFG_RK3, HFG_LINEAR, d.cfl, d.mixing);
+  s.setOptions(d.options);
+  s.seedParticles(d.per_cell, d.seed);
+  return sp;
+}
+
 double msBetween(Clock::time_point a, Clock::time_point b) {
   return std::chrono::duration<double, std::milli>(b - a).count();
 }
@@ -303,21 +325,8 @@ class Server {
   static void run(const Request& r, std::vector<double>& stepMs, std::vector<float>& pos, hfg_stats_t& last,
                   long long& particles) {
     const hfg_scene_desc_t& d = r.d;
-    Dim3i res{d.res[0], d.res[1], d.res[2]};
-    const float origin[3] = {0.f, 0.f, 0.f};
-    const float h[3] = {1.0f / d.res[0], 1.0f / d.res[1], 1.0f / d.res[2]};
-    GridSolver s(d.dt, res, origin, h);
-    const float still[3] = {0.f, 0.f, 0.f};
-    s.addAnalyticBoundary(0, nullptr, still);
-    for (int i = 0; i < d.n_spheres; ++i) {
-      const double p[6] = {d.spheres[i][0], d.spheres[i][1], d.spheres[i][2], d.spheres[i][3], 0.0, 0.0};
-      s.addAnalyticBoundary(1, p, still);
-    }
-    const float lo[3] = {0.f, 0.f, 0.f};
-    s.fluidDomainFromBBox(lo, d.fluid_max);
-    s.setAdvection(HFG_ADV_MIX_PIC_FLIP, HFG_RK3, HFG_LINEAR, d.cfl, d.mixing);
-    s.setOptions(d.options);
-    s.seedParticles(d.per_cell, d.seed);
+    std::unique_ptr<GridSolver> sp = buildScene(d);
+    GridSolver& s = *sp;
     particles = s.numParticles();
     stepMs.reserve(d.steps);
     for (int k = 0; k < d.steps; ++k) {
@@ -364,6 +373,238 @@ template <class F> int guardedS(F&& f) {
 
 struct hfg_server_s {
   std::unique_ptr<Server> s;
+};
+
+namespace {
+// ---------------------------------------------------------------------------
+// Batched lockstep stepping (hfg_batch_*).  All scenes stay resident and
+// advance together, one step at a time:
+//   A. every scene's boundaries and the advection up to the CFL substeps, on
+//      its own stream (a pool of host threads issues them);
+//   B. the substeps of all scenes: one kSubstepMulti launch per substep slot
+//      covers the particles of every scene, each with its own CFL state; the
+//      launches of a step form one CUDA graph (recaptured when the predicted
+//      substep count changes), followed by one read-back of every scene's
+//      state;
+//   C. every scene's P2G, pressure solve (graph-replayed CG chunks) and
+//      extrapolation, again on the scenes' own streams from the pool.
+// A scene's results are those it has alone, up to the order of the P2G
+// float atomics.
+class WorkPool {
+ public:
+  WorkPool(int device, int threads) {
+    for (int i = 0; i < threads; ++i)
+      th_.emplace_back([this, device] {
+        cudaSetDevice(device);
+        long long seen = 0;
+        for (;;) {
+          std::function<void(int)> job;
+          {
+            std::unique_lock<std::mutex> lk(mu_);
+            cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+            if (stop_) return;
+            seen = gen_;
+            job = job_;
+          }
+          drain(job);
+        }
+      });
+  }
+  ~WorkPool() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : th_) t.join();
+  }
+  // f(i) for every i in [0, n) on the pool (the caller takes part); the first
+  // exception is rethrown here once all have finished
+  void run(int n, const std::function<void(int)>& f) {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      job_ = f;
+      n_ = n;
+      next_ = 0;
+      done_ = 0;
+      err_ = nullptr;
+      ++gen_;
+    }
+    cv_.notify_all();
+    drain(f);
+    std::unique_lock<std::mutex> lk(mu_);
+    fin_.wait(lk, [&] { return done_ == n_; });
+    if (err_) std::rethrow_exception(err_);
+  }
+
+ private:
+  void drain(const std::function<void(int)>& f) {
+    for (;;) {
+      int i;
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (next_ >= n_) return;
+        i = next_++;
+      }
+      try {
+        f(i);
+      } catch (...) {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (!err_) err_ = std::current_exception();
+      }
+      std::lock_guard<std::mutex> lk(mu_);
+      if (++done_ == n_) fin_.notify_all();
+    }
+  }
+  std::vector<std::thread> th_;
+  std::mutex mu_;
+  std::condition_variable cv_, fin_;
+  std::function<void(int)> job_;
+  int n_ = 0, next_ = 0, done_ = 0;
+  long long gen_ = 0;
+  bool stop_ = false;
+  std::exception_ptr err_;
+};
+
+class Batch {
+ public:
+  Batch(int device, const hfg_scene_desc_t* d, int n, int threads) : device_(device), pool_(device, threads) {
+    check(cudaSetDevice(device), "cudaSetDevice");
+    std::string why;
+    for (int i = 0; i < n; ++i)
+      if (!validDesc(d[i], why)) throw CudaError("scene " + std::to_string(i) + ": " + why, HFG_ERR_INVALID);
+    sc_.resize(n);
+    pool_.run(n, [&](int i) { sc_[i] = buildScene(d[i]); });
+    check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    ready_.resize(n);
+    for (auto& e : ready_) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+    check(cudaEventCreateWithFlags(&subDone_, cudaEventDisableTiming), "cudaEventCreate");
+    check(cudaHostAlloc((void**)&tasksHost_, sizeof(SubstepTask) * n, cudaHostAllocDefault), "cudaHostAlloc");
+    check(cudaHostAlloc((void**)&startHost_, sizeof(long long) * (n + 1), cudaHostAllocDefault), "cudaHostAlloc");
+    check(cudaHostAlloc((void**)&flags_, sizeof(int) * 2 * n, cudaHostAllocMapped), "cudaHostAlloc");
+    check(cudaHostGetDevicePointer((void**)&flagsDev_, flags_, 0), "cudaHostGetDevicePointer");
+    tasks_.alloc(n);
+    start_.alloc(n + 1);
+    counts_.assign(n, 0);
+  }
+  ~Batch() {
+    if (stream_) cudaStreamSynchronize(stream_);
+    if (graph_) cudaGraphExecDestroy(graph_);
+    for (auto& e : ready_) cudaEventDestroy(e);
+    if (subDone_) cudaEventDestroy(subDone_);
+    if (tasksHost_) cudaFreeHost(tasksHost_);
+    if (startHost_) cudaFreeHost(startHost_);
+    if (flags_) cudaFreeHost(flags_);
+    sc_.clear();
+    tasks_.release();
+    start_.release();
+    if (stream_) cudaStreamDestroy(stream_);
+  }
+
+  void step() {
+    const int n = (int)sc_.size();
+    std::vector<char> particles(n, 0);
+    // A: boundaries, G2P and the first substep sample of every scene
+    pool_.run(n, [&](int i) {
+      GridSolver& s = *sc_[i];
+      s.stepBoundaries();
+      particles[i] = s.advectBegin() ? 1 : 0;
+      if (particles[i]) check(cudaEventRecord(ready_[i], s.stream()), "cudaEventRecord");
+    });
+    // B: the substeps of all scenes in shared launches
+    std::vector<int> who;
+    long long chunks = 0;
+    for (int i = 0; i < n; ++i)
+      if (particles[i]) {
+        tasksHost_[who.size()] = sc_[i]->substepTask();
+        startHost_[who.size()] = chunks;
+        chunks += multiSubstepChunks(tasksHost_[who.size()].P);
+        who.push_back(i);
+      }
+    const int m = (int)who.size();
+    if (m > 0) {
+      startHost_[m] = chunks;
+      check(cudaMemcpyAsync(tasks_.p, tasksHost_, sizeof(SubstepTask) * m, cudaMemcpyHostToDevice, stream_), "copy");
+      check(cudaMemcpyAsync(start_.p, startHost_, sizeof(long long) * (m + 1), cudaMemcpyHostToDevice, stream_),
+            "copy");
+      for (int i : who) check(cudaStreamWaitEvent(stream_, ready_[i], 0), "cudaStreamWaitEvent");
+      int predicted = 4;
+      for (int i : who) predicted = std::max(predicted, counts_[i]);
+      // a graph of `predicted` launches (slots 0 ..) while the scene set and
+      // its chunking stay the same; then chunks of 4 launches until done
+      if (!graph_ || graphSlots_ != predicted || graphScenes_ != m || graphChunks_ != chunks) {
+        if (graph_) cudaGraphExecDestroy(graph_);
+        graph_ = nullptr;
+        cudaGraph_t g = nullptr;
+        check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
+        cudaError_t e = cudaSuccess;
+        for (int k = 0; k < predicted && e == cudaSuccess; ++k)
+          e = launchSubstepMulti(tasks_.p, start_.p, m, chunks, k, stream_);
+        if (e == cudaSuccess) e = launchGatherSubstepStates(tasks_.p, m, predicted, flagsDev_, stream_);
+        cudaError_t ec = cudaStreamEndCapture(stream_, &g);
+        check(e, "substep launches");
+        check(ec, "capture");
+        e = cudaGraphInstantiate(&graph_, g, 0);
+        cudaGraphDestroy(g);
+        check(e, "cudaGraphInstantiate");
+        graphSlots_ = predicted;
+        graphScenes_ = m;
+        graphChunks_ = chunks;
+      }
+      check(cudaGraphLaunch(graph_, stream_), "substep graph");
+      int slot = predicted;
+      for (;;) {
+        check(cudaStreamSynchronize(stream_), "substep sync");
+        bool all = true;
+        for (int j = 0; j < m; ++j) all = all && flags_[2 * j] != 0;
+        if (all) break;
+        if (slot >= 4000) throw CudaError("CFL substep limit reached", HFG_ERR_STATE);
+        for (int k = 0; k < 4; ++k, ++slot)
+          check(launchSubstepMulti(tasks_.p, start_.p, m, chunks, slot, stream_), "substep");
+        check(launchGatherSubstepStates(tasks_.p, m, slot, flagsDev_, stream_), "gather");
+      }
+      for (int j = 0; j < m; ++j) counts_[who[j]] = flags_[2 * j + 1];
+      check(cudaEventRecord(subDone_, stream_), "cudaEventRecord");
+    }
+    // C: P2G, pressure and extrapolation of every scene
+    pool_.run(n, [&](int i) {
+      GridSolver& s = *sc_[i];
+      if (particles[i]) {
+        check(cudaStreamWaitEvent(s.stream(), subDone_, 0), "cudaStreamWaitEvent");
+        s.substepsDone(counts_[i]);
+        s.advectEnd();
+      }
+      s.solvePressure();
+      s.synchronize();
+    });
+  }
+
+  GridSolver& scene(int i) { return *sc_.at(i); }
+  int size() const { return (int)sc_.size(); }
+
+ private:
+  int device_;
+  WorkPool pool_;
+  std::vector<std::unique_ptr<GridSolver>> sc_;
+  cudaStream_t stream_ = nullptr;
+  std::vector<cudaEvent_t> ready_;
+  cudaEvent_t subDone_ = nullptr;
+  SubstepTask* tasksHost_ = nullptr;
+  long long* startHost_ = nullptr;
+  int* flags_ = nullptr;  // mapped: finished, count per scene
+  int* flagsDev_ = nullptr;
+  DArray<SubstepTask> tasks_;
+  DArray<long long> start_;
+  std::vector<int> counts_;
+  cudaGraphExec_t graph_ = nullptr;
+  int graphSlots_ = 0, graphScenes_ = 0;
+  long long graphChunks_ = -1;
+};
+
+}  // namespace
+
+struct hfg_batch_s {
+  std::unique_ptr<Batch> b;
 };
 
 extern "C" {
@@ -463,6 +704,60 @@ HFG_API int hfg_server_destroy(hfg_server_t srv) {
   return guardedS([&]() -> int {
     if (!srv) throw CudaError("null server", HFG_ERR_INVALID);
     delete srv;
+    return HFG_OK;
+  });
+}
+
+HFG_API int hfg_batch_create(int device, const hfg_scene_desc_t* scenes, int n, int threads, hfg_batch_t* out) {
+  return guardedS([&]() -> int {
+    if (!out || !scenes || n <= 0 || threads <= 0 || threads > 256)
+      throw CudaError("invalid arguments", HFG_ERR_INVALID);
+    auto* h = new hfg_batch_s();
+    try {
+      h->b.reset(new Batch(device, scenes, n, threads));
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+    return HFG_OK;
+  });
+}
+
+HFG_API int hfg_batch_step(hfg_batch_t b, int steps, double* ms) {
+  return guardedS([&]() -> int {
+    if (!b || !b->b || steps < 0) throw CudaError("invalid arguments", HFG_ERR_INVALID);
+    for (int k = 0; k < steps; ++k) {
+      auto t0 = Clock::now();
+      b->b->step();
+      if (ms) ms[k] = msBetween(t0, Clock::now());
+    }
+    return HFG_OK;
+  });
+}
+
+HFG_API int hfg_batch_scene_stats(hfg_batch_t b, int scene, hfg_stats_t* st) {
+  return guardedS([&]() -> int {
+    if (!b || !b->b || !st || scene < 0 || scene >= b->b->size()) throw CudaError("invalid arguments", HFG_ERR_INVALID);
+    b->b->scene(scene).getStats(st);
+    return HFG_OK;
+  });
+}
+
+HFG_API int hfg_batch_particles(hfg_batch_t b, int scene, float* pos, long long capacity) {
+  return guardedS([&]() -> int {
+    if (!b || !b->b || !pos || scene < 0 || scene >= b->b->size()) throw CudaError("invalid arguments", HFG_ERR_INVALID);
+    GridSolver& s = b->b->scene(scene);
+    if (capacity < 3 * s.numParticles()) throw CudaError("particle buffer too small", HFG_ERR_INVALID);
+    s.getParticles(pos, nullptr);
+    return HFG_OK;
+  });
+}
+
+HFG_API int hfg_batch_destroy(hfg_batch_t b) {
+  return guardedS([&]() -> int {
+    if (!b) throw CudaError("null batch", HFG_ERR_INVALID);
+    delete b;
     return HFG_OK;
   });
 }

@@ -413,10 +413,9 @@ FaceQuads GridSolver::beginParticleStep(ConstFaceField vin) {
 }
 
 // EulerParticles.cpp:231-325.  Substeps are launched speculatively in chunks;
-// a launch whose slot is already finished does nothing.  With haveV0 the
-// first sample (v0 and its max) is already in place, from the LINEAR G2P.
-void GridSolver::advectParticles(const FaceQuads& v, bool haveV0) {
-  if (!haveV0) launched(launchSubstepBegin(g_, v, ppos_.p, pv0_.p, P_, subState_.p, stream_), "substep begin");
+// a launch whose slot is already finished does nothing.  The first sample (v0
+// and its max) is already in place (advectBegin).
+void GridSolver::advectParticles(const FaceQuads& v) {
   long long nclamp = opt_.clamp_mode == 1 ? std::min<long long>(P_, N_) : P_;
   int slot = 0;
   partMs_[1] = 0.f;
@@ -448,12 +447,21 @@ void GridSolver::advectParticles(const FaceQuads& v, bool haveV0) {
 // forces of ExternalForcesSolver.cpp:50-58 are folded into the pass that
 // writes the advected velocity.
 void GridSolver::computeAdvection() {
+  if (advectBegin()) {
+    advectParticles(vq_);
+    advectEnd();
+  }
+}
+
+// The advection up to the CFL substeps: the whole semi-Lagrangian advection
+// (returns false), or for the particle solvers the corner tables, the G2P
+// velocity update and the first substep sample (returns true).
+bool GridSolver::advectBegin() {
   finishMirrorCopy();
   int ci = cur(), ni = nxt();
   float gv[3], ev[3];
   bool doG, doE;
   forcesTerms(gv, doG, ev, doE);
-  float* vout[3] = {vel_[ni][0].p, vel_[ni][1].p, vel_[ni][2].p};
   if (adv_ == HFG_ADV_SEMI_LAGRANGIAN) {
     stageBegin(1);
     launched(launchSLFace(g_, acc_rk_, dt_, cvel(ci), cvel(ci), mvel(ni), gv, doG, ev, doE, stream_, opt_.sampling),
@@ -464,22 +472,53 @@ void GridSolver::computeAdvection() {
       launched(launchSLCell(g_, acc_rk_, dt_, cvel(ci), in, out, 4, stream_, opt_.sampling), "sl cell");
     }
     stageEnd(1);
-    return;
+    return false;
   }
   if (P_ <= 0) throw CudaError("particle advection needs particles", HFG_ERR_STATE);
   stageBegin(1);
   ConstFaceField prev{{prev_[0].p, prev_[1].p, prev_[2].p}};
   int mode = adv_ == HFG_ADV_PIC ? MODE_PIC : (adv_ == HFG_ADV_FLIP ? MODE_FLIP : MODE_MIX);
   int first = (mode != MODE_PIC && !velFlag_) ? 1 : 0;
-  FaceQuads vq = beginParticleStep(cvel(ci));
+  vq_ = beginParticleStep(cvel(ci));
   if (timing_) check(cudaEventRecord(ev_[16], stream_), "cudaEventRecord");
   launched(launchParticleVelUpdate(g_, mode, alg_, cvel(ci), prev, first, mixing_, ppos_.p, pvel_.p, P_, stream_,
-                                   &vq, pv0_.p, subState_.p),
+                                   &vq_, pv0_.p, subState_.p),
            "particle velocity");
   if (timing_) check(cudaEventRecord(ev_[17], stream_), "cudaEventRecord");
   if (mode != MODE_PIC) velFlag_ = true;
+  // the LINEAR G2P also took the first substep sample (v0 and its max)
+  if (alg_ != HFG_LINEAR)
+    launched(launchSubstepBegin(g_, vq_, ppos_.p, pv0_.p, P_, subState_.p, stream_), "substep begin");
   startMirrorCopy(false);
-  advectParticles(vq, alg_ == HFG_LINEAR);
+  return true;
+}
+
+// The CFL substeps of this scene alone, as the batch stepper's shared launches
+// would run them (substepTask).
+SubstepTask GridSolver::substepTask() {
+  SubstepTask t;
+  t.g = g_;
+  t.vel = vq_;
+  t.pos = ppos_.p;
+  t.v0 = pv0_.p;
+  t.P = P_;
+  t.nclamp = opt_.clamp_mode == 1 ? std::min<long long>(P_, N_) : P_;
+  t.st = subState_.p;
+  t.acc = acc_rk_;
+  t.dt = dt_;
+  t.cfl = cfl_;
+  return t;
+}
+
+// The particle advection after the substeps: P2G of the velocities (with the
+// FLIP copy and the external forces) and of the carried scalars.
+void GridSolver::advectEnd() {
+  int ci = cur(), ni = nxt();
+  float gv[3], ev[3];
+  bool doG, doE;
+  forcesTerms(gv, doG, ev, doE);
+  float* vout[3] = {vel_[ni][0].p, vel_[ni][1].p, vel_[ni][2].p};
+  int mode = adv_ == HFG_ADV_PIC ? MODE_PIC : (adv_ == HFG_ADV_FLIP ? MODE_FLIP : MODE_MIX);
   startMirrorCopy(true);
   float* copy[3] = {prev_[0].p, prev_[1].p, prev_[2].p};
   if (timing_) check(cudaEventRecord(ev_[20], stream_), "cudaEventRecord");
@@ -687,10 +726,14 @@ void GridSolver::extrapolate() {
   stageEnd(7);
 }
 
-void GridSolver::updateWithoutPressure() {
+void GridSolver::stepBoundaries() {
   stageBegin(0);
   updateBoundarys();
   stageEnd(0);
+}
+
+void GridSolver::updateWithoutPressure() {
+  stepBoundaries();
   computeAdvection();
 }
 

@@ -147,11 +147,22 @@ class GridSolver {
   long long launches() const { return launches_; }
   const hfg_options_t& options() const { return opt_; }
 
+  // The step in phases, for a driver that runs the CFL substeps of several
+  // scenes in shared launches (BatchStepper): updateWithoutPressure() is
+  //   boundaries; advectBegin(); [substeps]; advectEnd()
+  // and a true advectBegin() needs the substeps run on substepTask() and then
+  // substepsDone(count) before advectEnd().
+  void stepBoundaries();
+  bool advectBegin();
+  SubstepTask substepTask();
+  void substepsDone(int count) { substeps_ = count; }
+  void advectEnd();
+
  private:
   void updateBoundarys();
   void computeAdvection();
   FaceQuads beginParticleStep(ConstFaceField vin);
-  void advectParticles(const FaceQuads& v, bool haveV0);
+  void advectParticles(const FaceQuads& v);
   void p2gFace(const float* vel, float* const out[3], float* const copy[3], const float add[3], bool doAdd,
                const float add2[3], bool doAdd2);
   void p2gCell(const float* vals, int span, int comp, float* out);
@@ -213,6 +224,7 @@ class GridSolver {
   int cgChunks_ = 0;  // CG chunks the last Jacobi/identity solve needed
   DArray<float2> acc_[3], cacc_;
   DArray<float4> quads_[3];  // corner tables of the advecting velocity (particle substeps)
+  FaceQuads vq_{};           // their pointers during an advection
   DArray<uint16_t> dist_;
   DArray<uint8_t> mask_;
   DArray<unsigned int> list_, hist_, offsets_, cursor_;

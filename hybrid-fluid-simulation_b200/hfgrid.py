@@ -201,6 +201,11 @@ def _signatures(lib):
         "hfg_selftest_bounded_waits": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "hfg_test_inject_alloc_failure": (C.c_int, [C.c_int]),
         "hfg_tune_save": (C.c_int, [C.c_char_p]),
+        "hfg_batch_create": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+        "hfg_batch_step": (C.c_int, [VP, C.c_int, C.c_void_p]),
+        "hfg_batch_scene_stats": (C.c_int, [VP, C.c_int, C.POINTER(Stats)]),
+        "hfg_batch_particles": (C.c_int, [VP, C.c_int, PF, C.c_longlong]),
+        "hfg_batch_destroy": (C.c_int, [VP]),
         "hfg_tune_load": (C.c_int, [C.c_char_p, C.POINTER(C.c_int)]),
     }
     for name, (res, args) in sig.items():
@@ -690,6 +695,45 @@ def scene_bytes(res, particles, boundaries=1, precond=PRECOND_JACOBI) -> int:
     out = C.c_longlong()
     _check(lib().hfg_scene_bytes(_i3(res), particles, boundaries, precond, C.byref(out)))
     return out.value
+
+
+class Batch:
+    """hfg_batch_*: many resident dam-break scenes stepped together, the CFL
+    substeps of all of them in one launch per substep."""
+
+    def __init__(self, descs, threads: int = 16, device: int = 0):
+        arr = (SceneDesc * len(descs))(*descs)
+        h = C.c_void_p()
+        _check(lib().hfg_batch_create(device, C.cast(arr, C.c_void_p), len(descs), threads, C.byref(h)))
+        self._h = h
+        self.n = len(descs)
+
+    def step(self, steps: int = 1):
+        """Advances every scene `steps` steps; returns each step's wall ms."""
+        ms = (C.c_double * max(steps, 1))()
+        _check(lib().hfg_batch_step(self._h, steps, C.cast(ms, C.c_void_p)))
+        return list(ms[:steps])
+
+    def stats(self, scene: int) -> dict:
+        st = Stats()
+        _check(lib().hfg_batch_scene_stats(self._h, scene, C.byref(st)))
+        return st.as_dict()
+
+    def particles(self, scene: int, n: int) -> np.ndarray:
+        out = np.empty((n, 3), np.float32)
+        _check(lib().hfg_batch_particles(self._h, scene, _fptr(out), 3 * n))
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _check(lib().hfg_batch_destroy(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Server:

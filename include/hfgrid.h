@@ -411,6 +411,22 @@ HFG_API int hfg_server_drain(hfg_server_t srv);  /* waits until every submitted 
 HFG_API int hfg_server_stats(hfg_server_t srv, hfg_server_stats_t* st);
 HFG_API int hfg_server_destroy(hfg_server_t srv);  /* drains first */
 
+/* Batched lockstep stepping (no reference counterpart; the reference steps
+ * its simulators one after another, MPhysics.cpp:19-25): n dam-break scenes
+ * (their `steps` field is ignored) stay resident on `device` and advance
+ * together.  Per step the CFL substeps of all scenes run in one launch per
+ * substep (each scene keeping its own CFL state), the launches of a step
+ * replayed from a CUDA graph; the other stages run on the scenes' own
+ * streams, issued by `threads` host threads.  A scene's results are those it
+ * has alone, up to the order of the P2G float atomics. */
+typedef struct hfg_batch_s* hfg_batch_t;
+HFG_API int hfg_batch_create(int device, const hfg_scene_desc_t* scenes, int n, int threads, hfg_batch_t* out);
+/* `steps` steps of every scene; ms (optional) receives each step's host wall time */
+HFG_API int hfg_batch_step(hfg_batch_t b, int steps, double* ms);
+HFG_API int hfg_batch_scene_stats(hfg_batch_t b, int scene, hfg_stats_t* st);
+HFG_API int hfg_batch_particles(hfg_batch_t b, int scene, float* pos, long long capacity);
+HFG_API int hfg_batch_destroy(hfg_batch_t b);
+
 /* hfg_op_p2g_fc without any device allocation.  This entry point has no
  * counterpart in the reference.  It is for callers that may not allocate
  * device memory at call time (a fixed-memory real-time loop, or a host whose

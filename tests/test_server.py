@@ -120,3 +120,31 @@ def test_analytic_solids_match_host_sdfs(cuda):
     # spacing enters as FP32 on the device and FP64 on the host: cell classes
     # agree except where a centre lies on a solid surface
     assert (got != ref).mean() < 1e-3
+
+
+@pytest.mark.gpu
+def test_batch_matches_each_scene_alone(cuda):
+    """hfg_batch_*: the CFL substeps of all scenes in one launch per substep
+    (each scene with its own CFL state), the rest on the scenes' streams.
+    Every scene ends where it ends alone: the same substep counts, particle
+    positions within 1e-4 (P2G float atomics add in scheduling order)."""
+    reqs = _requests()
+    alone = []
+    srv = hfgrid.Server(slots=1, budget_bytes=8 << 30)
+    for d in reqs:
+        rid = srv.submit(d)
+        inf = srv.wait(rid)
+        assert inf["status"] == 2, inf
+        alone.append((inf, srv.particles(rid, inf["particles"])))
+    srv.close()
+    b = hfgrid.Batch(reqs, threads=3)
+    ms = b.step(4)
+    assert len(ms) == 4 and all(m > 0 for m in ms)
+    for i, (inf0, pos0) in enumerate(alone):
+        st = b.stats(i)
+        assert st["num_particles"] == inf0["particles"]
+        assert st["substeps"] == inf0["last"]["substeps"]
+        assert abs(st["cg_iterations"] - inf0["last"]["cg_iterations"]) <= 1
+        pos = b.particles(i, st["num_particles"])
+        assert np.abs(pos - pos0).max() < 1e-4
+    b.close()
