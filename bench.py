@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--mg-smooth", type=int, default=0, help="multigrid smoothing sweeps per level (0: library default)")
     ap.add_argument("--pressure-fp64", action="store_true",
                     help="accumulate the pressure in FP64 (divergence follows the CG residual)")
+    ap.add_argument("--fp64-check", action="store_true",
+                    help="moving-boxes: step the layout at 128x64x128 beside the FP64 oracle and report the per-step "
+                         "error (and the oracle's time as the CPU baseline)")
     ap.add_argument("--requests", type=int, default=100, help="serve/batch: number of scenes")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: arrivals per second")
     ap.add_argument("--slots", type=int, default=16, help="serve/batch: concurrent scenes")
@@ -464,7 +467,63 @@ def run_moving_boxes(args):
                        "pressure": "fp64" if args.pressure_fp64 else "fp32",
                        "cells": N, "particles": s.num_particles},
             "per_step": per_step, "clocks": clk}
+    del s
+    if args.fp64_check:
+        line["cpu_baseline"], line["fp64_check"] = moving_boxes_cpu_leg(args.pressure_fp64)
     print(json.dumps(line), flush=True)
+
+
+def moving_boxes_cpu_leg(pressure_fp64, res=(128, 64, 128), steps=3):
+    """The moving-boxes layout scaled down to 128x64x128, stepped on the GPU
+    (the timed line's options) and in the FP64 oracle (Jacobi-PCG to 1e-10)
+    side by side: the oracle's steps are the CPU baseline, and each step's
+    GPU result is compared with them (velocity relative L2, marker agreement,
+    largest particle-position difference)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import hfgrid
+    import oracle
+    import scenes
+    threads = os.cpu_count() or 1
+    oracle.lib().orc_set_num_threads(threads)
+    sc, paths = scenes.moving_boxes(res, seed=0)
+    g = scenes.gpu_solver(sc, precond=hfgrid.PRECOND_MG, tol_mode=hfgrid.TOL_RELATIVE, tol=1e-6, max_iter=200,
+                          report_divergence=1, pressure_fp64=int(pressure_fp64))
+    o = oracle.Solver(sc.dt, sc.res, sc.origin, sc.spacing, dbl=1)
+    for sdf, v in scenes.boundaries(sc):
+        o.add_solid_boundary(sdf, v)
+    o.set_fluid_domain_field(oracle.fluid_domain_from_bbox(sc.res, sc.origin, sc.spacing, *scenes.fluid_bbox(sc)))
+    o.set_advection(hfgrid.ADV_MIX_PIC_FLIP, 2, 2, sc.cfl, sc.mixing, 1, 0)
+    pos, vel = g.particles()
+    o.set_particles(pos, vel)
+    o.set_pcg(1, 1, 1e-10, 20000)
+    rows, cpu_s = [], 0.0
+    for k in range(steps):
+        t = k * sc.dt
+        for i, p in enumerate(paths):
+            g.set_boundary_velocity(i + 1, p.velocity(t))
+            o.set_boundary_velocity(i + 1, p.velocity(t))
+        g.update()
+        t0 = time.perf_counter()
+        o.update()
+        cpu_s += time.perf_counter() - t0
+        st = g.stats()
+        vg, vo = g.velocity_field(), o.velocity_field()
+        num = sum(float(np.sum((a.astype(np.float64) - b) ** 2)) for a, b in zip(vg, vo))
+        den = sum(float(np.sum(np.asarray(b, np.float64) ** 2)) for b in vo)
+        gp, _ = g.particles()
+        op, _ = o.particles()
+        rows.append({"step": k + 1, "vel_rel_l2": (num / max(den, 1e-300)) ** 0.5,
+                     "markers_equal": float((g.markers() == o.markers()).mean()),
+                     "max_pos_diff": float(np.abs(gp - op).max()), "cg_iterations": st["cg_iterations"],
+                     "divergence_rel": st["divergence_l2"] / max(st["cg_rhs_norm"], 1e-300)})
+    cells = sc.n_cells
+    base = {"value": cells * steps / cpu_s / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{steps} steps of the moving-boxes layout at {res[0]}x{res[1]}x{res[2]}, FP64 oracle, "
+                      f"Jacobi-PCG to 1e-10, {threads} threads"}
+    check = {"res": list(res), "oracle": "FP64, Jacobi-PCG rel 1e-10", "gpu": "the timed line's options",
+             "per_step": rows}
+    return base, check
 
 
 def main():
