@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--mg-smooth", type=int, default=0, help="multigrid smoothing sweeps per level (0: library default)")
     ap.add_argument("--pressure-fp64", action="store_true",
                     help="accumulate the pressure in FP64 (divergence follows the CG residual)")
+    ap.add_argument("--ref-cpu", action="store_true",
+                    help="reference arm: time the FP64 oracle port on the host cores even where the reference's "
+                         "own CUDA build is present")
     ap.add_argument("--fp64-check", action="store_true",
                     help="moving-boxes: step the layout at 128x64x128 beside the FP64 oracle and report the per-step "
                          "error (and the oracle's time as the CPU baseline)")
@@ -158,11 +161,20 @@ def init_ranks(world: int, local: int):
 
 
 def run_reference(args):
-    """CPU arm: the oracle's FP64 restatement of the same step, rank 0 only."""
+    """The reference arm, rank 0 only.  With the reference's own CUDA step
+    built (oracle/_ref/refgpu) and a GPU visible, that step on the same
+    workload as our arm; otherwise the oracle's FP64 restatement on the host
+    cores, on a bounded sample."""
     world, rank, _ = dist_setup(args)
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refgpu
+    if refgpu.available() and not args.ref_cpu:
+        import torch
+        if torch.cuda.is_available():
+            run_reference_gpu(args)
+            return
     import numpy as np
     import oracle
     import scenes
@@ -197,6 +209,80 @@ def run_reference(args):
                          "sample": f"{args.steps} steps of the dam-break layout at {n}^3 (FP64 oracle)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    print(json.dumps(line), flush=True)
+
+
+def run_reference_gpu(args):
+    """The reference's CGridFluidSolver (its CUDA sources built unmodified
+    for sm_100a) stepping the 256^3 dam break: walls and the two static boxes
+    as SDF boundaries, the fluid domain from the bounding box, the PIC/FLIP
+    mix seeded by the reference itself (8 per cell outside the solids, the
+    count of our arm; linear transfers, CFL 1, mixing 0.05), its own pressure
+    solve (identity preconditioner,
+    sqrt(r.r) < 1e-3) with the iteration cap at the workload's 200.  Steps are
+    timed with CUDA events on the default stream, where the reference
+    launches everything."""
+    import torch
+    import refgpu
+    import scenes
+    torch.cuda.set_device(0)
+    # the reference writes progress notes to stdout (e.g. EulerParticles.cpp:258);
+    # they go to stderr here so that stdout carries the one JSON line
+    sys.stdout.flush()
+    saved_stdout = os.dup(1)
+    os.dup2(2, 1)
+    sc = scenes.dam_break_256(seed=0, n=args.res)
+    t_setup = time.perf_counter()
+    r = refgpu.RefSolver(sc.dt, sc.res, sc.origin, sc.spacing)
+    for sdf, _ in scenes.boundaries(sc):
+        r.add_solid_boundary(sdf)
+    r.generate_fluid_domain_from_bbox(*scenes.fluid_bbox(sc))
+    r.update_boundaries()
+    n = r.set_mix_pic_flip(sc.per_cell, sc.cfl, sc.mixing)
+    r.set_cg_iteration_cap(200)
+    r.synchronize()
+    setup_s = time.perf_counter() - t_setup
+    for _ in range(args.warmup):
+        r.update()
+    r.synchronize()
+    refgpu.RefSolver.take_ax_calls()
+    stream = torch.cuda.default_stream()
+    clocks = ClockSampler(0)
+    clocks.start()
+    per_step, iters = [], []
+    for _ in range(args.steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r.update()
+        e1.record(stream)
+        e1.synchronize()
+        per_step.append(e0.elapsed_time(e1))
+        iters.append(max(refgpu.RefSolver.take_ax_calls() - 1, 0))
+    clk = clocks.stop()
+    ms = sum(per_step) / len(per_step)
+    value = sc.n_cells / (ms / 1e3) / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded dam break)",
+        "config": {"workload": f"dam break {args.res}^3, walls + two static boxes, 8 ppc, PIC/FLIP 0.95, "
+                               "the reference's own pressure solve (identity-PCG, sqrt(r.r) < 1e-3) capped at 200",
+                   "res": [args.res] * 3, "cells": sc.n_cells, "particles": n,
+                   "implementation": "the reference's CGridFluidSolver, its CUDA sources built unmodified for "
+                                     "sm_100a (oracle/refgpu/build.sh), driven through its C++ API",
+                   "l2": "state > L2 (no flush needed)"},
+        "cg_iterations_per_step": iters, "ms_per_step_each": per_step, "setup_s": setup_s, "clocks": clk,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": f"{args.steps} steps of the {args.res}^3 dam break after {args.warmup} warm-up "
+                                   "steps: the reference's own CUDA step on this B200 (one host thread drives it)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    r.close()
+    import ctypes
+    ctypes.CDLL(None).fflush(None)
+    os.dup2(saved_stdout, 1)
+    os.close(saved_stdout)
     print(json.dumps(line), flush=True)
 
 
