@@ -419,6 +419,13 @@ HFG_API int hfg_solver_get_particles(hfg_solver_t s, float* pos, float* vel) {
     return HFG_OK;
   });
 }
+HFG_API int hfg_solver_sort_particles(hfg_solver_t s) {
+  return guarded([&]() -> int {
+    SOLVER(s);
+    S.sortParticles();
+    return HFG_OK;
+  });
+}
 HFG_API int hfg_solver_set_particle_mirror(hfg_solver_t s, float* pos, float* vel, long long capacity) {
   return guarded([&]() -> int {
     SOLVER(s);

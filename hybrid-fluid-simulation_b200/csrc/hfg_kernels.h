@@ -255,6 +255,16 @@ cudaError_t launchParticleVelUpdate(const Geom& g, int mode, int alg, ConstFaceF
 // faceQuadCount(r, a) entries.
 long long faceQuadCount(const Dim3i& r, int a);
 cudaError_t launchFaceQuads(const Dim3i& r, ConstFaceField v, float4* const out[3], cudaStream_t s);
+
+// hfg_sort.cu: the stable permutation that orders P particles by cell
+// (perm[j] = index of the j-th particle in cell order, ties in index order).
+// Scratch: key[P], off[N cells], sums[sortScanBlocks(N)].
+long long sortScanBlocks(long long nCells);
+cudaError_t launchSortPermutation(const Geom& g, const float* pos, long long P, unsigned int* key, unsigned int* off,
+                                  unsigned int* sums, unsigned int* perm, cudaStream_t s);
+// out[width*j + k] = in[width*perm[j] + k], width 1 or 3
+cudaError_t launchGather(const float* in, int width, const unsigned int* perm, long long P, float* out,
+                         cudaStream_t s);
 cudaError_t launchSubstepBegin(const Geom& g, FaceQuads vel, const float* pos, float* v0, long long P,
                                SubstepState* st, cudaStream_t s);
 cudaError_t launchSubstep(const Geom& g, FaceQuads vel, float* pos, float* v0, long long P, int acc, float dt,

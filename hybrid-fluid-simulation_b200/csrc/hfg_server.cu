@@ -72,7 +72,7 @@ double percentile(std::vector<double> v, double q) {
 // index, stencil code and CG vectors on the pitched grid, P2G accumulators,
 // face corner tables, extrapolation scratch, boundary SDFs, particles) plus
 // the multigrid levels.
-long long sceneBytes(const int res[3], long long particles, int boundaries, int precond) {
+long long sceneBytes(const int res[3], long long particles, int boundaries, int precond, bool sorting = false) {
   const long long nx = res[0], ny = res[1], nz = res[2];
   const long long N = nx * ny * nz;
   const long long F = (nx + 1) * ny * nz + nx * (ny + 1) * nz + nx * ny * (nz + 1);
@@ -88,6 +88,7 @@ long long sceneBytes(const int res[3], long long particles, int boundaries, int 
   b += N * 4 * (long long)boundaries;
   b += particles * (4 * 3 * 4 + 4);  // pos, vel, v0, vector scalars, scalar
   if (precond == HFG_PRECOND_MG) b += NC * 4 * 4 + N * 2;  // level-0 z x2, p x2; coarse levels
+  if (sorting) b += particles * (4 + 4 + 12) + N * 4;      // sort keys, permutation, gather buffer; cell offsets
   b += 64ll << 20;             // partials, state, allocator granularity
   return b;
 }
@@ -148,7 +149,8 @@ class Server {
     auto r = std::make_unique<Request>();
     r->d = d;
     r->cells = (long long)d.res[0] * d.res[1] * d.res[2];
-    r->footprint = sceneBytes(d.res, particlesBound(d), 1 + d.n_spheres, d.options.precond);
+    r->footprint = sceneBytes(d.res, particlesBound(d), 1 + d.n_spheres, d.options.precond,
+                              d.options.sort_interval > 0);
     r->submitted = Clock::now();
     std::lock_guard<std::mutex> lk(mu_);
     r->id = ++nextId_;

@@ -302,6 +302,7 @@ void GridSolver::setOptions(const hfg_options_t& o) {
   if (o.sampling < 0 || o.sampling > 4) throw CudaError("sampling algorithm must be in [0, 4]", HFG_ERR_INVALID);
   if (o.extrapolation_layers < 0 || o.extrapolation_layers > kMaxLayers)
     throw CudaError("extrapolation layers must be in [0, 1000]", HFG_ERR_INVALID);
+  if (o.sort_interval < 0) throw CudaError("sort interval must be >= 0", HFG_ERR_INVALID);
   bool mgChanged = o.precond == HFG_PRECOND_MG &&
                    (!mg_ || o.mg_levels != opt_.mg_levels || o.mg_smooth != opt_.mg_smooth || o.mg_half != opt_.mg_half);
   const bool fp64Changed = (o.pressure_fp64 != 0) != (opt_.pressure_fp64 != 0);
@@ -476,6 +477,8 @@ bool GridSolver::advectBegin() {
   }
   if (P_ <= 0) throw CudaError("particle advection needs particles", HFG_ERR_STATE);
   stageBegin(1);
+  if (opt_.sort_interval > 0 && particleSteps_ > 0 && particleSteps_ % opt_.sort_interval == 0) sortParticles();
+  ++particleSteps_;
   ConstFaceField prev{{prev_[0].p, prev_[1].p, prev_[2].p}};
   int mode = adv_ == HFG_ADV_PIC ? MODE_PIC : (adv_ == HFG_ADV_FLIP ? MODE_FLIP : MODE_MIX);
   int first = (mode != MODE_PIC && !velFlag_) ? 1 : 0;
@@ -491,6 +494,31 @@ bool GridSolver::advectBegin() {
     launched(launchSubstepBegin(g_, vq_, ppos_.p, pv0_.p, P_, subState_.p, stream_), "substep begin");
   startMirrorCopy(false);
   return true;
+}
+
+// The particles in cell order (hfg_sort.cu), with their velocities and
+// carried colour / domain values.  v at the substep start is not carried: each
+// step's velocity update writes it before the substeps read it.
+void GridSolver::sortParticles() {
+  if (P_ <= 0) return;
+  finishMirrorCopy();
+  sortKey_.alloc(P_, stream_);
+  sortPerm_.alloc(P_, stream_);
+  sortOff_.alloc(N_, stream_);
+  sortSums_.alloc(sortScanBlocks(N_), stream_);
+  launched(launchSortPermutation(g_, ppos_.p, P_, sortKey_.p, sortOff_.p, sortSums_.p, sortPerm_.p, stream_),
+           "particle sort", 6);
+  sortTmp_.alloc(3 * P_, stream_);
+  for (DArray<float>* a : {&ppos_, &pvel_, &pvector_}) {
+    if (!a->p || a->n != (size_t)(3 * P_)) continue;
+    launched(launchGather(a->p, 3, sortPerm_.p, P_, sortTmp_.p, stream_), "particle gather");
+    a->swap(sortTmp_);
+  }
+  if (pscalar_.p && pscalar_.n == (size_t)P_) {
+    launched(launchGather(pscalar_.p, 1, sortPerm_.p, P_, sortTmp_.p, stream_), "particle gather");
+    check(cudaMemcpyAsync(pscalar_.p, sortTmp_.p, sizeof(float) * P_, cudaMemcpyDeviceToDevice, stream_),
+          "particle gather copy");
+  }
 }
 
 // The CFL substeps of this scene alone, as the batch stepper's shared launches

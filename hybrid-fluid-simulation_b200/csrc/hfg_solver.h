@@ -11,6 +11,7 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/hfgrid.h"
@@ -68,6 +69,12 @@ template <class T> struct DArray {
     n = count;
   }
   size_t bytes() const { return n * sizeof(T); }
+  void swap(DArray& o) {
+    std::swap(p, o.p);
+    std::swap(n, o.n);
+    std::swap(s, o.s);
+    std::swap(async, o.async);
+  }
 };
 
 // Small pinned host blocks (state read-backs) from a process-wide free list:
@@ -136,6 +143,8 @@ class GridSolver {
   void getParticles(float* pos, float* vel);
   // host mirror filled by every update (hfg_solver_set_particle_mirror)
   void setParticleMirror(float* pos, float* vel, long long capacity);
+  // Reorders the particles (and their carried values) by cell, stable.
+  void sortParticles();
   void getStats(hfg_stats_t* st);
   void synchronize();
   float timeCg(int iters);
@@ -232,6 +241,10 @@ class GridSolver {
 
   long long P_ = 0;
   DArray<float> ppos_, pvel_, pv0_, pscalar_, pvector_;
+  // the particle sort (option sort_interval, sortParticles)
+  long long particleSteps_ = 0;
+  DArray<unsigned int> sortKey_, sortPerm_, sortOff_, sortSums_;
+  DArray<float> sortTmp_;
 
   std::vector<DArray<float>*> bsdf_;
   std::vector<float> bvel_, btrans_;

@@ -42,7 +42,7 @@ class Options(C.Structure):
         ("precond", C.c_int), ("tol_mode", C.c_int), ("tol", C.c_double), ("max_iter", C.c_longlong),
         ("clamp_mode", C.c_int), ("advect_scalars", C.c_int), ("extrapolation_layers", C.c_int),
         ("mg_levels", C.c_int), ("mg_smooth", C.c_int), ("mg_half", C.c_int), ("report_divergence", C.c_int),
-        ("sampling", C.c_int), ("pressure_fp64", C.c_int), ("autotune", C.c_int),
+        ("sampling", C.c_int), ("pressure_fp64", C.c_int), ("autotune", C.c_int), ("sort_interval", C.c_int),
     ]
 
 
@@ -144,6 +144,7 @@ def _signatures(lib):
         "hfg_solver_transfer_vel_to_particles": (C.c_int, [S, VP, C.c_longlong, C.c_int, VP]),
         "hfg_solver_num_particles": (C.c_longlong, [S]),
         "hfg_solver_get_particles": (C.c_int, [S, PF, PF]),
+        "hfg_solver_sort_particles": (C.c_int, [S]),
         "hfg_solver_set_particle_mirror": (C.c_int, [S, PF, PF, C.c_longlong]),
         "hfg_solver_get_stats": (C.c_int, [S, C.POINTER(Stats)]),
         "hfg_solver_get_grid": (C.c_int, [S, I3, F3, F3]),
@@ -463,6 +464,10 @@ class Solver:
         vel = np.empty((n, 3), np.float32)
         _check(lib().hfg_solver_get_particles(self._h, _fptr(pos), _fptr(vel)))
         return pos, vel
+
+    def sort_particles(self):
+        """Reorder the particles by cell now (stable; no reference counterpart)."""
+        _check(lib().hfg_solver_sort_particles(self._h))
 
     def copy_particles_into(self, pos: np.ndarray, vel: Optional[np.ndarray] = None):
         _check(lib().hfg_solver_get_particles(self._h, _fptr(pos), None if vel is None else _fptr(vel)))

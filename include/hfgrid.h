@@ -91,6 +91,14 @@ typedef struct {
                              hfg_tune_save / hfg_tune_load keep it across runs).
                              The reference's fixed launch shape is
                              EulerSolverTool.cu:650-656. */
+  int sort_interval;      /* k > 0: at the start of every k-th particle step
+                             after the first, reorder the particles by cell
+                             (stable counting sort; velocities and carried
+                             values follow), so that the substeps and the P2G
+                             scatter keep touching neighbouring entries as the
+                             flow mixes.  0 (default): the seeding order is
+                             kept, as the reference keeps it.  The order of
+                             hfg_solver_get_particles follows the sort. */
 } hfg_options_t;
 
 typedef struct {
@@ -198,6 +206,10 @@ HFG_API int hfg_solver_mix_vel_field_with_others(hfg_solver_t s, const float* vx
 HFG_API int hfg_solver_transfer_vel_to_particles(hfg_solver_t s, const float* pos, long long n, int alg, float* vel);
 HFG_API long long hfg_solver_num_particles(hfg_solver_t s);
 HFG_API int hfg_solver_get_particles(hfg_solver_t s, float* pos, float* vel);
+/* Reorder the particles by cell now: stable (particles of one cell keep
+ * their relative order), velocities and carried values follow.  No
+ * reference counterpart (the reference keeps the seeding order). */
+HFG_API int hfg_solver_sort_particles(hfg_solver_t s);
 /* Host mirror of the particles (an extension; the reference's viewer calls
  * copyEulerParticlesPos/VelToCPU after every update, MPhysicsAPI.h).  While a
  * mirror is set, every update also copies the particle positions and
