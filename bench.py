@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--workload", default="dam-break", choices=["dam-break", "serve", "batch", "moving-boxes"],
                     help="dam-break: the 256^3 headline line; serve: Poisson stream of mixed-size requests "
                          "through the scene server vs each request run plain; batch: many uneven scenes at once")
+    ap.add_argument("--mg-half", type=int, default=1, choices=[0, 1, 2],
+                    help="multigrid storage: 0 FP32, 1 BF16 coarse levels, 2 BF16 level-0 smoothing iterates too")
     ap.add_argument("--mg-smooth", type=int, default=0, help="multigrid smoothing sweeps per level (0: library default)")
     ap.add_argument("--pressure-fp64", action="store_true",
                     help="accumulate the pressure in FP64 (divergence follows the CG residual)")
@@ -512,7 +514,7 @@ def run_moving_boxes(args):
     s.set_advection(hfgrid.ADV_MIX_PIC_FLIP, hfgrid.RK3, hfgrid.LINEAR, sc.cfl, sc.mixing)
     s.set_options(precond=hfgrid.PRECOND_MG, tol_mode=hfgrid.TOL_RELATIVE, tol=1e-6, max_iter=200,
                   advect_scalars=0, report_divergence=1, pressure_fp64=int(args.pressure_fp64),
-                  sort_interval=args.sort_interval)
+                  sort_interval=args.sort_interval, mg_half=args.mg_half)
     s.seed_particles(sc.per_cell, sc.seed)
     stream = torch.cuda.ExternalStream(s.stream)
     t = 0.0
@@ -554,16 +556,16 @@ def run_moving_boxes(args):
             "config": {"workload": "C3: 512x256x512 dam break, three boxes (side 0.2) on sinusoidal paths "
                                    "(amplitude 0.1, period 2 s), 8 ppc, MG-PCG rel 1e-6 max 200",
                        "pressure": "fp64" if args.pressure_fp64 else "fp32",
-                       "particle_sort_interval": args.sort_interval,
+                       "particle_sort_interval": args.sort_interval, "mg_half": args.mg_half,
                        "cells": N, "particles": s.num_particles},
             "per_step": per_step, "clocks": clk}
     del s
     if args.fp64_check:
-        line["cpu_baseline"], line["fp64_check"] = moving_boxes_cpu_leg(args.pressure_fp64)
+        line["cpu_baseline"], line["fp64_check"] = moving_boxes_cpu_leg(args.pressure_fp64, args.mg_half)
     print(json.dumps(line), flush=True)
 
 
-def moving_boxes_cpu_leg(pressure_fp64, res=(128, 64, 128), steps=3):
+def moving_boxes_cpu_leg(pressure_fp64, mg_half=1, res=(128, 64, 128), steps=3):
     """The moving-boxes layout scaled down to 128x64x128, stepped on the GPU
     (the timed line's options) and in the FP64 oracle (Jacobi-PCG to 1e-10)
     side by side: the oracle's steps are the CPU baseline, and each step's
@@ -578,7 +580,7 @@ def moving_boxes_cpu_leg(pressure_fp64, res=(128, 64, 128), steps=3):
     oracle.lib().orc_set_num_threads(threads)
     sc, paths = scenes.moving_boxes(res, seed=0)
     g = scenes.gpu_solver(sc, precond=hfgrid.PRECOND_MG, tol_mode=hfgrid.TOL_RELATIVE, tol=1e-6, max_iter=200,
-                          report_divergence=1, pressure_fp64=int(pressure_fp64))
+                          report_divergence=1, pressure_fp64=int(pressure_fp64), mg_half=mg_half)
     o = oracle.Solver(sc.dt, sc.res, sc.origin, sc.spacing, dbl=1)
     for sdf, v in scenes.boundaries(sc):
         o.add_solid_boundary(sdf, v)
@@ -649,7 +651,7 @@ def run_dam_break(args):
     precond = {"jacobi": hfgrid.PRECOND_JACOBI, "identity": hfgrid.PRECOND_IDENTITY, "mg": hfgrid.PRECOND_MG}[args.precond]
     sc = scenes.dam_break_256(seed=rank, n=args.res)
     opts = dict(precond=precond, tol_mode=hfgrid.TOL_RELATIVE, tol=1e-6, max_iter=200, advect_scalars=0,
-                clamp_mode=1, pressure_fp64=int(args.pressure_fp64), mg_smooth=args.mg_smooth,
+                clamp_mode=1, pressure_fp64=int(args.pressure_fp64), mg_smooth=args.mg_smooth, mg_half=args.mg_half,
                 sort_interval=args.sort_interval)
 
     def warm_solver():
@@ -786,6 +788,7 @@ def run_dam_break(args):
                                    f"{args.precond}-PCG rel 1e-6 max 200", "res": [args.res] * 3,
                        "cells": N, "particles": n, "l2": "state > L2 (no flush needed)",
                        "parallelism": f"replicas x{world}", "particle_sort_interval": args.sort_interval,
+                       "mg_half": args.mg_half if args.precond == "mg" else None,
                        "convergence_one_more_step": conv,
                        "stage_ms_one_more_step": stage_ms, "particle_ms_one_more_step": particle_ms},
             "roofline": {"bound": "hbm", "kernel": "kSubstep (one CFL particle substep)",

@@ -17,8 +17,10 @@
 //    symmetric operator and plain CG applies;
 //  * coarsest level (<= 512 cells): many Jacobi sweeps in one block's shared
 //    memory;
-//  * precision: level-0 vectors FP32; every coarser level stores its
-//    right-hand side and iterate in BF16 (or FP16) and computes in FP32.
+//  * precision: every coarser level stores its right-hand side and iterate
+//    in BF16 and computes in FP32; level 0 keeps its right-hand side (the
+//    CG's r) in FP32 and, with half mode 2, stores its smoothing iterates in
+//    BF16 as well, all but the last sweep's, which the CG reads in FP32.
 //
 // Every kernel returns at once when the CG has converged (CgState::done), so
 // chunks of iterations can be launched without host round trips.
@@ -211,9 +213,9 @@ SweepGrid sweepGrid(const Dim3i& r, bool reduce) {
 // and the arithmetic are those of kJacobi, so the sweeps agree bit for bit;
 // only the order of the r.z partial sums differs.
 constexpr int MX = 32, MY = 8;
-template <class TC, bool CORR, bool DOT>
+template <class TC, bool CORR, bool DOT, class TZI = float, class TZO = float>
 __global__ void __launch_bounds__(MX* MY)
-    kJacobiZ(Lvl L, Dim3i rc, const float* __restrict__ b, const float* __restrict__ zi, float* __restrict__ zo,
+    kJacobiZ(Lvl L, Dim3i rc, const float* __restrict__ b, const TZI* __restrict__ zi, TZO* __restrict__ zo,
              const TC* __restrict__ zc, const Code* __restrict__ code, double* partials, CgState* st, int zLen) {
   waitPrevGrid();
   if (st->done) return;
@@ -227,7 +229,7 @@ __global__ void __launch_bounds__(MX* MY)
     // iterate (with the coarse correction) at cell i of plane zz, 0 off the fluid
     auto value = [&](unsigned i, int zz, Code ki) -> float {
       if (!(ki & 1)) return 0.f;
-      float v = __ldg(zi + i);
+      float v = ld(zi, i);
       if (CORR) v += ld(zc, par(x, y, zz));
       return v;
     };
@@ -248,14 +250,14 @@ __global__ void __launch_bounds__(MX* MY)
           if (d == 5) return va;
           int dx, dy, dz;
           nbrOf(d, dx, dy, dz);
-          float w = __ldg(zi + c + dx + dy * L.r.x);
+          float w = ld(zi, c + dx + dy * L.r.x);
           if (CORR) w += ld(zc, par(x + dx, y + dy, z));
           return w;
         };
         float az = applyA(L, k, vc, zAt);
         v = vc + kOmega * (bv - az) / diagOfC(k, L.sx, L.sy, L.sz);
       }
-      if (k & 1) zo[c] = v;  // zero off the fluid for the whole solve (memset by mgRunCg)
+      if (k & 1) zo[c] = cvt<TZO>(v);  // zero off the fluid for the whole solve (memset by mgRunCg)
       if (DOT) rz += (double)bv * (double)v;
       vb = vc;
       k = ka;
@@ -279,8 +281,9 @@ __global__ void __launch_bounds__(MX* MY)
 
 // kJacobiFirst on level 0 with the launch shape of kJacobiZ: z = omega b /
 // diag along a column of zLen planes.
+template <class TZO>
 __global__ void __launch_bounds__(MX* MY)
-    kJacobiFirstZ(Lvl L, const float* __restrict__ b, float* __restrict__ z, const Code* __restrict__ code,
+    kJacobiFirstZ(Lvl L, const float* __restrict__ b, TZO* __restrict__ z, const Code* __restrict__ code,
                   const CgState* st, int zLen) {
   waitPrevGrid();
   if (st->done) return;
@@ -293,7 +296,7 @@ __global__ void __launch_bounds__(MX* MY)
 #pragma unroll 4
   for (int zz = z0; zz < z1; ++zz, c += pl) {
     const Code k = code[c];
-    if (k & 1) z[c] = kOmega * __ldg(b + c) / diagOfC(k, L.sx, L.sy, L.sz);  // zero elsewhere already
+    if (k & 1) z[c] = cvt<TZO>(kOmega * __ldg(b + c) / diagOfC(k, L.sx, L.sy, L.sz));  // zero elsewhere already
   }
 }
 
@@ -389,13 +392,15 @@ struct Multigrid {
   Dim3i r0;                          // level 0 = the pitched grid of the pressure system
   Dim3i rLogical;                    // the solver's grid (level-0 markers are unpitched)
   int smooth = 2;
-  bool half = true;
+  bool half = true;                  // coarse levels in BF16
+  bool half0 = false;                // level-0 smoothing iterates in BF16 too (marching sweeps only)
   std::vector<Dim3i> res;            // level resolutions, [0] = fine
   std::vector<DArray<uint8_t>*> mk;  // levels >= 1
   std::vector<DArray<Code>*> code;   // levels >= 1
   std::vector<DArray<uint16_t>*> b16, z16a, z16b;  // levels >= 1 (BF16 / FP16 storage)
   std::vector<DArray<float>*> b32, z32a, z32b;     // levels >= 1 when !half
   DArray<float> z0a, z0b;            // level 0 iterate (FP32)
+  DArray<uint16_t> z0h[2];           // level 0 BF16 iterates (half0)
   DArray<float> p[2];
   DArray<double> partials;
   CUtensorMap zH[2], pH[2];          // halo tensor maps of z0a / z0b and p[0] / p[1]
@@ -415,11 +420,13 @@ struct Multigrid {
   int levels() const { return (int)res.size(); }
 };
 
-Multigrid* mgCreate(const Dim3i& r, int levels, int smooth, bool half, cudaStream_t s) {
+Multigrid* mgCreate(const Dim3i& r, int levels, int smooth, int halfMode, cudaStream_t s) {
   auto* m = new Multigrid();
   m->r0 = r;
   m->smooth = smooth > 0 ? smooth : 3;  // 3 sweeps: fewest ms per solve at 256^3 (2: 67.3, 3: 65.6, 4: 66.9 ms per step)
+  const bool half = halfMode != 0;
   m->half = half;
+  m->half0 = halfMode == 2 && marchLevel0(r);
   m->res.push_back(r);
   Dim3i cur = r;
   while ((levels <= 0 || (int)m->res.size() < levels) && cur.size() > kCoarseMax) {
@@ -435,6 +442,10 @@ Multigrid* mgCreate(const Dim3i& r, int levels, int smooth, bool half, cudaStrea
   long long N = r.size();
   m->z0a.alloc(N, s);
   m->z0b.alloc(N, s);
+  if (m->half0) {
+    m->z0h[0].alloc(N, s);
+    m->z0h[1].alloc(N, s);
+  }
   m->p[0].alloc(N, s);
   m->p[1].alloc(N, s);
   const dim3 mg = marchGrid(r).grid;
@@ -517,11 +528,25 @@ const float* vcycleT(Multigrid* m, const float* r0, CgState* st, cudaStream_t s,
   // which ping-pong buffer holds the current iterate of each level
   std::vector<int> curBuf(L, 0);
   float* z0[2] = {m->z0a.p, m->z0b.p};
+  // half0: the level-0 iterates in BF16 (h0), except the last sweep's, which
+  // goes to z0a in FP32 for the CG
+  using BF = __nv_bfloat16;
+  const bool h0 = m->half0 && marching && L > 1;
+  BF* hz[2] = {(BF*)m->z0h[0].p, (BF*)m->z0h[1].p};
   // downward sweep
   for (int l = 0; l < L - 1; ++l) {
-    if (l == 0) {
+    if (l == 0 && h0) {
+      march(kJacobiFirstZ<BF>, lv[0], r0, hz[0], codeOf(0), (const CgState*)st);
+      int cb = 0;
+      for (int k = 1; k < nu; ++k, cb ^= 1)
+        march(kJacobiZ<float, false, false, BF, BF>, lv[0], lv[0].r, r0, (const BF*)hz[cb], hz[cb ^ 1],
+              (const float*)nullptr, codeOf(0), (double*)nullptr, st);
+      curBuf[0] = cb;
+      run(kResidualRestrict<float, BF, TS>, gridOf(lv[1].r), blk, lv[0], lv[1].r, r0, (const BF*)hz[cb], codeOf(0),
+          bL[1], (const CgState*)st);
+    } else if (l == 0) {
       if (marching)
-        march(kJacobiFirstZ, lv[0], r0, z0[0], codeOf(0), (const CgState*)st);
+        march(kJacobiFirstZ<float>, lv[0], r0, z0[0], codeOf(0), (const CgState*)st);
       else
         run(kJacobiFirst<float, float>, gridOf(lv[0].r), blk, lv[0], r0, z0[0], codeOf(0), (const CgState*)st);
       int cb = 0;
@@ -560,7 +585,25 @@ const float* vcycleT(Multigrid* m, const float* r0, CgState* st, cudaStream_t s,
   // upward sweep: prolongation fused into the first post-smoothing sweep
   for (int l = L - 2; l >= 0; --l) {
     const TS* zc = (curBuf[l + 1] == 0) ? zaL[l + 1] : zbL[l + 1];
-    if (l == 0) {
+    if (l == 0 && h0) {
+      int cb = curBuf[0];
+      for (int k = 0; k < nu; ++k, cb ^= 1) {
+        const bool last = k == nu - 1;
+        const BF* zi = hz[cb];
+        if (k == 0 && last)
+          march(kJacobiZ<TS, true, true, BF, float>, lv[0], lv[1].r, r0, zi, z0[0], zc, codeOf(0), m->partials.p, st);
+        else if (k == 0)
+          march(kJacobiZ<TS, true, false, BF, BF>, lv[0], lv[1].r, r0, zi, hz[cb ^ 1], zc, codeOf(0), (double*)nullptr,
+                st);
+        else if (last)
+          march(kJacobiZ<float, false, true, BF, float>, lv[0], lv[0].r, r0, zi, z0[0], (const float*)nullptr,
+                codeOf(0), m->partials.p, st);
+        else
+          march(kJacobiZ<float, false, false, BF, BF>, lv[0], lv[0].r, r0, zi, hz[cb ^ 1], (const float*)nullptr,
+                codeOf(0), (double*)nullptr, st);
+      }
+      curBuf[0] = 0;  // the result is in z0[0]
+    } else if (l == 0) {
       int cb = curBuf[0];
       for (int k = 0; k < nu; ++k, cb ^= 1) {
         const bool last = k == nu - 1;
@@ -651,6 +694,8 @@ void mgRunCg(Multigrid* m, const Dim3i& cg, float sx, float sy, float sz, const 
   // the marching level-0 sweeps store fluid cells only: the iterates start zero
   check(cudaMemsetAsync(m->z0a.p, 0, m->z0a.bytes(), s), "memset");
   check(cudaMemsetAsync(m->z0b.p, 0, m->z0b.bytes(), s), "memset");
+  for (auto& h : m->z0h)
+    if (h.p) check(cudaMemsetAsync(h.p, 0, h.bytes(), s), "memset");
   const float* z0 = mgVcycle(m, rvec, st, s, launches);  // z0 = V(b), rz = b.z0
   const int kChunk = 4;  // even: every chunk starts on p[0]
   auto body = [&] {

@@ -62,7 +62,7 @@ constexpr int kSubstepChunk = 4;   // CFL substeps launched between completion r
 }  // namespace
 
 // Multigrid preconditioner hooks (hfg_mg.cu).
-Multigrid* mgCreate(const Dim3i& cg, int levels, int smooth, bool half, cudaStream_t s);
+Multigrid* mgCreate(const Dim3i& cg, int levels, int smooth, int halfMode, cudaStream_t s);
 void mgDestroy(Multigrid* m);
 void mgSetup(Multigrid* m, const Dim3i& r, const uint8_t* mk0, const Code* code, float sx, float sy, float sz,
              cudaStream_t s, long long& launches);
@@ -303,6 +303,7 @@ void GridSolver::setOptions(const hfg_options_t& o) {
   if (o.extrapolation_layers < 0 || o.extrapolation_layers > kMaxLayers)
     throw CudaError("extrapolation layers must be in [0, 1000]", HFG_ERR_INVALID);
   if (o.sort_interval < 0) throw CudaError("sort interval must be >= 0", HFG_ERR_INVALID);
+  if (o.mg_half < 0 || o.mg_half > 2) throw CudaError("mg_half must be 0, 1 or 2", HFG_ERR_INVALID);
   bool mgChanged = o.precond == HFG_PRECOND_MG &&
                    (!mg_ || o.mg_levels != opt_.mg_levels || o.mg_smooth != opt_.mg_smooth || o.mg_half != opt_.mg_half);
   const bool fp64Changed = (o.pressure_fp64 != 0) != (opt_.pressure_fp64 != 0);
@@ -319,7 +320,7 @@ void GridSolver::setOptions(const hfg_options_t& o) {
   if (mgChanged) {
     dropGraphs();
     if (mg_) mgDestroy(mg_);
-    mg_ = mgCreate(cg_, o.mg_levels, o.mg_smooth, o.mg_half != 0, stream_);
+    mg_ = mgCreate(cg_, o.mg_levels, o.mg_smooth, o.mg_half, stream_);
   }
 }
 

@@ -76,7 +76,13 @@ typedef struct {
   int extrapolation_layers; /* default 1000 (GridFluidSolver.cpp:176) */
   int mg_levels;          /* multigrid levels for HFG_PRECOND_MG (0 = auto) */
   int mg_smooth;          /* smoothing sweeps per level (0 = default) */
-  int mg_half;            /* 1: multigrid smoothing stores in half precision */
+  int mg_half;            /* multigrid storage: 0 FP32 on every level; 1 (default)
+                             the coarse levels store their right-hand sides and
+                             iterates in BF16; 2 as 1, and level 0's smoothing
+                             iterates in BF16 too (grids with the marching
+                             level-0 sweeps), the last sweep's output, which the
+                             CG reads, staying FP32.  Arithmetic is FP32 on every
+                             level and the CG's dot products FP64. */
   int report_divergence;  /* 1: measure the divergence residual of every projection
                              and recompute the solve's residual ||b - A x|| in FP64 */
   int sampling;           /* HFG_SAMPLE_* of the semi-Lagrangian advection (setSamplingAlg,

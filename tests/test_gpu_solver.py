@@ -173,12 +173,13 @@ def test_c1_dam_break_vs_fp64(cuda, steps):
     assert vel_rel_l2(g.velocity_field(), o.velocity_field()) < (1e-4 if steps == 1 else 1e-3)
 
 
-@pytest.mark.parametrize("half", [1, 0])
+@pytest.mark.parametrize("half", [2, 1, 0])
 def test_multigrid_marching_sweeps_vs_fp64(cuda, half):
     """The multigrid PCG with the level-0 sweeps that march along z (72 x 44 x
     78: enough tile columns for two blocks per SM) against the FP64 oracle
     solved to 1e-10, one step from rest: markers equal and the projected
-    velocity within 1e-4 relative L2."""
+    velocity within 1e-4 relative L2.  half: 0 FP32 storage everywhere, 1
+    BF16 coarse levels, 2 BF16 level-0 smoothing iterates as well."""
     sc = small_scene((72, 44, 78))
     g = scenes.gpu_solver(sc, precond=hfgrid.PRECOND_MG, tol_mode=1, tol=1e-6, max_iter=200, mg_half=half)
     o = oracle_twin(sc, g, 1, 1, 1, 1e-10, 20000, scalars=False)
