@@ -66,7 +66,8 @@ def parse():
     ap.add_argument("--pressure-fp64", action="store_true",
                     help="accumulate the pressure in FP64 (divergence follows the CG residual)")
     ap.add_argument("--sort-interval", type=int, default=0,
-                    help="dam-break / moving-boxes: reorder the particles by cell every k steps (0: never)")
+                    help="dam-break / moving-boxes: reorder the particles by cell every k steps (0: never); "
+                         "it runs with clamp_mode 0 (every particle pushed out of the solids)")
     ap.add_argument("--ref-cpu", action="store_true",
                     help="reference arm: time the FP64 oracle port on the host cores even where the reference's "
                          "own CUDA build is present")
@@ -514,7 +515,7 @@ def run_moving_boxes(args):
     s.set_advection(hfgrid.ADV_MIX_PIC_FLIP, hfgrid.RK3, hfgrid.LINEAR, sc.cfl, sc.mixing)
     s.set_options(precond=hfgrid.PRECOND_MG, tol_mode=hfgrid.TOL_RELATIVE, tol=1e-6, max_iter=200,
                   advect_scalars=0, report_divergence=1, pressure_fp64=int(args.pressure_fp64),
-                  sort_interval=args.sort_interval, mg_half=args.mg_half)
+                  sort_interval=args.sort_interval, mg_half=args.mg_half, clamp_mode=0 if args.sort_interval else 1)
     s.seed_particles(sc.per_cell, sc.seed)
     stream = torch.cuda.ExternalStream(s.stream)
     t = 0.0
@@ -651,7 +652,8 @@ def run_dam_break(args):
     precond = {"jacobi": hfgrid.PRECOND_JACOBI, "identity": hfgrid.PRECOND_IDENTITY, "mg": hfgrid.PRECOND_MG}[args.precond]
     sc = scenes.dam_break_256(seed=rank, n=args.res)
     opts = dict(precond=precond, tol_mode=hfgrid.TOL_RELATIVE, tol=1e-6, max_iter=200, advect_scalars=0,
-                clamp_mode=1, pressure_fp64=int(args.pressure_fp64), mg_smooth=args.mg_smooth, mg_half=args.mg_half,
+                clamp_mode=0 if args.sort_interval else 1, pressure_fp64=int(args.pressure_fp64),
+                mg_smooth=args.mg_smooth, mg_half=args.mg_half,
                 sort_interval=args.sort_interval)
 
     def warm_solver():

@@ -502,6 +502,13 @@ bool GridSolver::advectBegin() {
 // step's velocity update writes it before the substeps read it.
 void GridSolver::sortParticles() {
   if (P_ <= 0) return;
+  // With clamp_mode 1 the boundary fix reaches only the first min(N, P)
+  // particles, as the reference's launch does (EulerParticlesTool.cu:880); a
+  // new order would change which particles those are.
+  if (opt_.clamp_mode == 1 && P_ > N_)
+    throw CudaError("the particle sort needs clamp_mode 0 when there are more particles than cells: with clamp_mode 1 "
+                    "the order decides which particles the boundary fix reaches",
+                    HFG_ERR_INVALID);
   finishMirrorCopy();
   sortKey_.alloc(P_, stream_);
   sortPerm_.alloc(P_, stream_);

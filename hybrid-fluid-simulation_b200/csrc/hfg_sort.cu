@@ -132,12 +132,40 @@ __global__ void kSortScatter(const unsigned int* __restrict__ key, long long P, 
     perm[atomicAdd(off + key[p], 1u)] = (unsigned int)p;
 }
 
+// Heap sort of a[0, n) ascending, in place: O(n log n) for the rare large
+// bucket (particles crowded into one cell).
+__device__ void heapSort(unsigned int* a, unsigned int n) {
+  auto sift = [&](unsigned int i, unsigned int m) {
+    unsigned int v = a[i];
+    for (;;) {
+      unsigned int ch = 2 * i + 1;
+      if (ch >= m) break;
+      if (ch + 1 < m && a[ch + 1] > a[ch]) ++ch;
+      if (a[ch] <= v) break;
+      a[i] = a[ch];
+      i = ch;
+    }
+    a[i] = v;
+  };
+  for (unsigned int i = n / 2; i-- > 0;) sift(i, n);
+  for (unsigned int m = n; m-- > 1;) {
+    unsigned int t = a[0];
+    a[0] = a[m];
+    a[m] = t;
+    sift(0, m);
+  }
+}
+
 // After the scatter off[c] is the end of bucket c and off[c - 1] its start.
-// Buckets hold a handful of particles (8 per fluid cell when seeded), so an
-// insertion sort per cell is enough.
+// Buckets hold a handful of particles (8 per fluid cell when seeded): an
+// insertion sort per cell, or a heap sort for a bucket beyond 32.
 __global__ void kSortBuckets(const unsigned int* __restrict__ off, long long n, unsigned int* __restrict__ perm) {
   for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
     unsigned int b = c ? off[c - 1] : 0u, e = off[c];
+    if (e - b > 32) {
+      heapSort(perm + b, e - b);
+      continue;
+    }
     for (unsigned int i = b + 1; i < e; ++i) {
       unsigned int v = perm[i];
       unsigned int j = i;

@@ -4,7 +4,10 @@ No reference counterpart: the reference keeps its seeding order.  The sort
 must be a stable permutation by cell (the binning of transPos2Index,
 EulerMathTool.cu:29-40), restated here with numpy's stable argsort, and
 stepping with it must give the results of stepping without it, up to the
-order of the FP32 P2G atomics.
+order of the FP32 P2G atomics.  The cases run with clamp_mode 0: under the
+reference's clamp (the boundary fix reaches the first min(N, P) particles
+only) the order decides which particles those are, so there the sort is
+refused when P > N.
 """
 import numpy as np
 import pytest
@@ -33,7 +36,7 @@ def scene():
 
 def test_sort_is_the_stable_permutation_by_cell(cuda):
     sc = scene()
-    g = scenes.gpu_solver(sc, precond=1, tol_mode=1, tol=1e-6, max_iter=400, advect_scalars=True)
+    g = scenes.gpu_solver(sc, precond=1, tol_mode=1, tol=1e-6, max_iter=400, advect_scalars=True, clamp_mode=0)
     for _ in range(4):
         g.update()
     pos, vel = g.particles()
@@ -56,8 +59,8 @@ def test_steps_with_sorting_match_steps_without(cuda, interval):
     the velocity field within 1e-5 relative L2 and the particle sets within
     1e-5 (the P2G atomics add in another order), markers >= 99.9 % equal."""
     sc = scene()
-    a = scenes.gpu_solver(sc, precond=1, tol_mode=1, tol=1e-6, max_iter=400, advect_scalars=True)
-    b = scenes.gpu_solver(sc, precond=1, tol_mode=1, tol=1e-6, max_iter=400, advect_scalars=True,
+    a = scenes.gpu_solver(sc, precond=1, tol_mode=1, tol=1e-6, max_iter=400, advect_scalars=True, clamp_mode=0)
+    b = scenes.gpu_solver(sc, precond=1, tol_mode=1, tol=1e-6, max_iter=400, advect_scalars=True, clamp_mode=0,
                           sort_interval=interval)
     for _ in range(5):
         a.update()
@@ -77,3 +80,16 @@ def test_steps_with_sorting_match_steps_without(cuda, interval):
     dist, idx = cKDTree(pa.astype(np.float64)).query(pb.astype(np.float64))
     assert dist.max() < 1e-5
     assert len(np.unique(idx)) == len(idx)
+
+
+def test_sort_refused_under_the_reference_clamp_with_more_particles_than_cells(cuda):
+    import hfgrid
+    sc = scene()
+    g = scenes.gpu_solver(sc, clamp_mode=1)
+    assert g.num_particles > sc.n_cells
+    with pytest.raises(hfgrid.HfgError) as e:
+        g.sort_particles()
+    assert "clamp_mode" in str(e.value)
+    pos0, _ = g.particles()
+    g.update()  # the solver is unchanged and still steps
+    assert g.num_particles == len(pos0)
