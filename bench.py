@@ -68,6 +68,9 @@ def parse():
     ap.add_argument("--sort-interval", type=int, default=0,
                     help="dam-break / moving-boxes: reorder the particles by cell every k steps (0: never); "
                          "it runs with clamp_mode 0 (every particle pushed out of the solids)")
+    ap.add_argument("--clamp-mode", type=int, default=None, choices=[0, 1],
+                    help="boundary fix of the particles: 1 the first min(N, P) as the reference, 0 all "
+                         "(default 1, or 0 with --sort-interval)")
     ap.add_argument("--ref-cpu", action="store_true",
                     help="reference arm: time the FP64 oracle port on the host cores even where the reference's "
                          "own CUDA build is present")
@@ -515,7 +518,7 @@ def run_moving_boxes(args):
     s.set_advection(hfgrid.ADV_MIX_PIC_FLIP, hfgrid.RK3, hfgrid.LINEAR, sc.cfl, sc.mixing)
     s.set_options(precond=hfgrid.PRECOND_MG, tol_mode=hfgrid.TOL_RELATIVE, tol=1e-6, max_iter=200,
                   advect_scalars=0, report_divergence=1, pressure_fp64=int(args.pressure_fp64),
-                  sort_interval=args.sort_interval, mg_half=args.mg_half, clamp_mode=0 if args.sort_interval else 1)
+                  sort_interval=args.sort_interval, mg_half=args.mg_half, clamp_mode=clamp_mode(args))
     s.seed_particles(sc.per_cell, sc.seed)
     stream = torch.cuda.ExternalStream(s.stream)
     t = 0.0
@@ -623,6 +626,12 @@ def moving_boxes_cpu_leg(pressure_fp64, mg_half=1, res=(128, 64, 128), steps=3):
     return base, check
 
 
+def clamp_mode(args) -> int:
+    if args.clamp_mode is not None:
+        return args.clamp_mode
+    return 0 if args.sort_interval else 1
+
+
 def main():
     args = parse()
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
@@ -652,7 +661,7 @@ def run_dam_break(args):
     precond = {"jacobi": hfgrid.PRECOND_JACOBI, "identity": hfgrid.PRECOND_IDENTITY, "mg": hfgrid.PRECOND_MG}[args.precond]
     sc = scenes.dam_break_256(seed=rank, n=args.res)
     opts = dict(precond=precond, tol_mode=hfgrid.TOL_RELATIVE, tol=1e-6, max_iter=200, advect_scalars=0,
-                clamp_mode=0 if args.sort_interval else 1, pressure_fp64=int(args.pressure_fp64),
+                clamp_mode=clamp_mode(args), pressure_fp64=int(args.pressure_fp64),
                 mg_smooth=args.mg_smooth, mg_half=args.mg_half,
                 sort_interval=args.sort_interval)
 
@@ -790,6 +799,7 @@ def run_dam_break(args):
                                    f"{args.precond}-PCG rel 1e-6 max 200", "res": [args.res] * 3,
                        "cells": N, "particles": n, "l2": "state > L2 (no flush needed)",
                        "parallelism": f"replicas x{world}", "particle_sort_interval": args.sort_interval,
+                       "clamp_mode": clamp_mode(args),
                        "mg_half": args.mg_half if args.precond == "mg" else None,
                        "convergence_one_more_step": conv,
                        "stage_ms_one_more_step": stage_ms, "particle_ms_one_more_step": particle_ms},
