@@ -258,10 +258,17 @@ cudaError_t launchFaceQuads(const Dim3i& r, ConstFaceField v, float4* const out[
 
 // hfg_sort.cu: the stable permutation that orders P particles by cell
 // (perm[j] = index of the j-th particle in cell order, ties in index order).
-// Scratch: key[P], off[N cells], sums[sortScanBlocks(N)].
-long long sortScanBlocks(long long nCells);
-cudaError_t launchSortPermutation(const Geom& g, const float* pos, long long P, unsigned int* key, unsigned int* off,
-                                  unsigned int* sums, unsigned int* perm, cudaStream_t s);
+// Scratch: keyA, keyB, valA, valB of P entries, counts of
+// sortCountEntries(P), sums of sortScanBlocks(sortCountEntries(P)); *perm
+// is set to valA or valB.
+struct SortScratch {
+  unsigned int *keyA, *keyB, *valA, *valB, *counts, *sums;
+};
+long long sortCountEntries(long long P);
+long long sortScanBlocks(long long entries);
+int sortPassesLaunches(long long nCells);  // kernels one sort launches
+cudaError_t launchSortPermutation(const Geom& g, const float* pos, long long P, const SortScratch& sc,
+                                  const unsigned int** perm, cudaStream_t s);
 // out[width*j + k] = in[width*perm[j] + k], width 1 or 3
 cudaError_t launchGather(const float* in, int width, const unsigned int* perm, long long P, float* out,
                          cudaStream_t s);

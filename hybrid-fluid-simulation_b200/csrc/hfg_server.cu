@@ -88,7 +88,7 @@ long long sceneBytes(const int res[3], long long particles, int boundaries, int 
   b += N * 4 * (long long)boundaries;
   b += particles * (4 * 3 * 4 + 4);  // pos, vel, v0, vector scalars, scalar
   if (precond == HFG_PRECOND_MG) b += NC * 4 * 4 + N * 2;  // level-0 z x2, p x2; coarse levels
-  if (sorting) b += particles * (4 + 4 + 12) + N * 4;      // sort keys, permutation, gather buffer; cell offsets
+  if (sorting) b += particles * (16 + 12) + particles / 16;  // radix keys and values x2, gather buffer, digit counts
   b += 64ll << 20;             // partials, state, allocator granularity
   return b;
 }

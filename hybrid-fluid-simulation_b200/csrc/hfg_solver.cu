@@ -510,20 +510,24 @@ void GridSolver::sortParticles() {
                     "the order decides which particles the boundary fix reaches",
                     HFG_ERR_INVALID);
   finishMirrorCopy();
-  sortKey_.alloc(P_, stream_);
-  sortPerm_.alloc(P_, stream_);
-  sortOff_.alloc(N_, stream_);
-  sortSums_.alloc(sortScanBlocks(N_), stream_);
-  launched(launchSortPermutation(g_, ppos_.p, P_, sortKey_.p, sortOff_.p, sortSums_.p, sortPerm_.p, stream_),
-           "particle sort", 6);
+  for (int i = 0; i < 2; ++i) {
+    sortKey_[i].alloc(P_, stream_);
+    sortVal_[i].alloc(P_, stream_);
+  }
+  const long long entries = sortCountEntries(P_);
+  sortCounts_.alloc(entries, stream_);
+  sortSums_.alloc(sortScanBlocks(entries), stream_);
+  const SortScratch sc{sortKey_[0].p, sortKey_[1].p, sortVal_[0].p, sortVal_[1].p, sortCounts_.p, sortSums_.p};
+  const unsigned int* perm = nullptr;
+  launched(launchSortPermutation(g_, ppos_.p, P_, sc, &perm, stream_), "particle sort", sortPassesLaunches(N_));
   sortTmp_.alloc(3 * P_, stream_);
   for (DArray<float>* a : {&ppos_, &pvel_, &pvector_}) {
     if (!a->p || a->n != (size_t)(3 * P_)) continue;
-    launched(launchGather(a->p, 3, sortPerm_.p, P_, sortTmp_.p, stream_), "particle gather");
+    launched(launchGather(a->p, 3, perm, P_, sortTmp_.p, stream_), "particle gather");
     a->swap(sortTmp_);
   }
   if (pscalar_.p && pscalar_.n == (size_t)P_) {
-    launched(launchGather(pscalar_.p, 1, sortPerm_.p, P_, sortTmp_.p, stream_), "particle gather");
+    launched(launchGather(pscalar_.p, 1, perm, P_, sortTmp_.p, stream_), "particle gather");
     check(cudaMemcpyAsync(pscalar_.p, sortTmp_.p, sizeof(float) * P_, cudaMemcpyDeviceToDevice, stream_),
           "particle gather copy");
   }

@@ -243,7 +243,7 @@ class GridSolver {
   DArray<float> ppos_, pvel_, pv0_, pscalar_, pvector_;
   // the particle sort (option sort_interval, sortParticles)
   long long particleSteps_ = 0;
-  DArray<unsigned int> sortKey_, sortPerm_, sortOff_, sortSums_;
+  DArray<unsigned int> sortKey_[2], sortVal_[2], sortCounts_, sortSums_;
   DArray<float> sortTmp_;
 
   std::vector<DArray<float>*> bsdf_;

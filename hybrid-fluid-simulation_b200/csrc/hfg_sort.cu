@@ -5,16 +5,20 @@
 // Particles seeded cell by cell start out ordered, so the lanes of a warp
 // touch neighbouring corner-table entries in the substeps and neighbouring
 // faces in the P2G scatter, where lane groups with equal corners merge their
-// atomics.  A mixing flow spreads that order out.  This is a stable counting
-// sort by the particle's cell (the binning of transPos2Index,
-// EulerMathTool.cu:29-40), deterministic although its scatter uses atomics:
-//   keys      key[p] = cell of particle p; count[cell] += 1
-//   scan      exclusive prefix sums of the counts, in place (3 passes)
-//   scatter   slot = atomicAdd(&off[key], 1); perm[slot] = p
-//             (off[c] then holds the end of bucket c)
-//   buckets   each cell's bucket sorted by original index: the order within a
-//             cell is the previous order, whatever the atomics' order was
+// atomics.  A mixing flow spreads that order out.  This is a stable LSD radix
+// sort of the particles by cell (the binning of transPos2Index,
+// EulerMathTool.cu:29-40), 8 bits per pass, deterministic:
+//   keys      key[p] = cell of particle p, value p
+//   per pass  hist     per tile of 4096 particles, the count of each digit
+//             scan     exclusive prefix sums of the counts, digit-major, so a
+//                      digit's slots go to the tiles in particle order
+//             scatter  each tile walks its particles in order, 256 at a time;
+//                      a particle's slot is its digit's running base plus the
+//                      particles before it with that digit (__match_any_sync
+//                      within a warp, per-warp counts across warps)
 //   gather    out[j] = in[perm[j]] for each particle array
+// The cost does not depend on how the particles are spread over the cells
+// (a cell can hold thousands where the flow presses particles onto a wall).
 #include <algorithm>
 
 #include "hfg_kernels.h"
@@ -34,13 +38,9 @@ inline int sortGrid(long long n, int threads = kSortThreads, int perSM = 16) {
   return (int)std::max(1LL, std::min(b, cap));
 }
 
-__global__ void kSortKeys(Geom g, const float* __restrict__ pos, long long P, unsigned int* __restrict__ key,
-                          unsigned int* __restrict__ count) {
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x) {
-    unsigned int c = (unsigned int)binCell(g, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]);
-    key[p] = c;
-    atomicAdd(count + c, 1u);
-  }
+__global__ void kSortKeys(Geom g, const float* __restrict__ pos, long long P, unsigned int* __restrict__ key) {
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x)
+    key[p] = (unsigned int)binCell(g, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]);
 }
 
 // Exclusive scan of a block-sized tile in place; the tile's total goes to
@@ -126,55 +126,67 @@ __global__ void kScanAdd(unsigned int* __restrict__ a, long long n, const unsign
     a[i] += sums[i / kScanTile];
 }
 
-__global__ void kSortScatter(const unsigned int* __restrict__ key, long long P, unsigned int* __restrict__ off,
-                             unsigned int* __restrict__ perm) {
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x)
-    perm[atomicAdd(off + key[p], 1u)] = (unsigned int)p;
-}
+constexpr int kRadixBits = 8, kRadixDigits = 1 << kRadixBits;
+constexpr int kRadixThreads = 256, kRadixRounds = 16, kRadixTile = kRadixThreads * kRadixRounds;
+constexpr int kRadixWarps = kRadixThreads / 32;
+static_assert(kRadixThreads == kRadixDigits, "one thread per digit");
 
-// Heap sort of a[0, n) ascending, in place: O(n log n) for the rare large
-// bucket (particles crowded into one cell).
-__device__ void heapSort(unsigned int* a, unsigned int n) {
-  auto sift = [&](unsigned int i, unsigned int m) {
-    unsigned int v = a[i];
-    for (;;) {
-      unsigned int ch = 2 * i + 1;
-      if (ch >= m) break;
-      if (ch + 1 < m && a[ch + 1] > a[ch]) ++ch;
-      if (a[ch] <= v) break;
-      a[i] = a[ch];
-      i = ch;
-    }
-    a[i] = v;
-  };
-  for (unsigned int i = n / 2; i-- > 0;) sift(i, n);
-  for (unsigned int m = n; m-- > 1;) {
-    unsigned int t = a[0];
-    a[0] = a[m];
-    a[m] = t;
-    sift(0, m);
+// counts[d * tiles + t] = particles of tile t whose digit (at shift) is d
+__global__ void __launch_bounds__(kRadixThreads) kRadixHist(const unsigned int* __restrict__ key, long long P,
+                                                            int shift, unsigned int* __restrict__ counts,
+                                                            long long tiles) {
+  __shared__ unsigned int h[kRadixDigits];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const long long base = (long long)blockIdx.x * kRadixTile;
+  for (int r = 0; r < kRadixRounds; ++r) {
+    long long i = base + r * kRadixThreads + threadIdx.x;
+    if (i < P) atomicAdd(&h[(key[i] >> shift) & (kRadixDigits - 1)], 1u);
   }
+  __syncthreads();
+  counts[(long long)threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
 }
 
-// After the scatter off[c] is the end of bucket c and off[c - 1] its start.
-// Buckets hold a handful of particles (8 per fluid cell when seeded): an
-// insertion sort per cell, or a heap sort for a bucket beyond 32.
-__global__ void kSortBuckets(const unsigned int* __restrict__ off, long long n, unsigned int* __restrict__ perm) {
-  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
-    unsigned int b = c ? off[c - 1] : 0u, e = off[c];
-    if (e - b > 32) {
-      heapSort(perm + b, e - b);
-      continue;
+// Stable scatter of one tile, given the scanned counts.  valIn == nullptr:
+// the values are the particle indices.
+__global__ void __launch_bounds__(kRadixThreads) kRadixScatter(const unsigned int* __restrict__ keyIn,
+                                                               const unsigned int* __restrict__ valIn, long long P,
+                                                               int shift, const unsigned int* __restrict__ scanned,
+                                                               long long tiles, unsigned int* __restrict__ keyOut,
+                                                               unsigned int* __restrict__ valOut) {
+  __shared__ unsigned int base[kRadixDigits];
+  __shared__ unsigned int wcnt[kRadixWarps][kRadixDigits];
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  base[t] = scanned[(long long)t * tiles + blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < kRadixWarps; ++k) wcnt[k][t] = 0;
+  __syncthreads();
+  const long long tile0 = (long long)blockIdx.x * kRadixTile;
+  for (int r = 0; r < kRadixRounds; ++r) {
+    const long long i = tile0 + r * kRadixThreads + t;
+    const bool valid = i < P;
+    const unsigned int key = valid ? keyIn[i] : 0u;
+    const unsigned int d = (key >> shift) & (kRadixDigits - 1);
+    // invalid lanes get a tag no digit has, so they never join a group
+    const unsigned int peers = __match_any_sync(0xffffffffu, valid ? d : (unsigned)kRadixDigits + lane);
+    const unsigned int rankW = __popc(peers & ((1u << lane) - 1u));
+    if (valid && rankW == 0) wcnt[w][d] = __popc(peers);
+    __syncthreads();
+    if (valid) {
+      unsigned int slot = base[d] + rankW;
+      for (int k = 0; k < w; ++k) slot += wcnt[k][d];
+      keyOut[slot] = key;
+      valOut[slot] = valIn ? valIn[i] : (unsigned int)i;
     }
-    for (unsigned int i = b + 1; i < e; ++i) {
-      unsigned int v = perm[i];
-      unsigned int j = i;
-      while (j > b && perm[j - 1] > v) {
-        perm[j] = perm[j - 1];
-        --j;
-      }
-      perm[j] = v;
+    __syncthreads();
+    unsigned int tot = 0;
+#pragma unroll
+    for (int k = 0; k < kRadixWarps; ++k) {
+      tot += wcnt[k][t];
+      wcnt[k][t] = 0;
     }
+    base[t] += tot;
+    __syncthreads();
   }
 }
 
@@ -190,24 +202,41 @@ __global__ void kGather(const float* __restrict__ in, const unsigned int* __rest
 
 }  // namespace
 
-long long sortScanBlocks(long long nCells) { return (nCells + kScanTile - 1) / kScanTile; }
+long long sortTiles(long long P) { return (P + kRadixTile - 1) / kRadixTile; }
+long long sortCountEntries(long long P) { return (long long)kRadixDigits * std::max(1LL, sortTiles(P)); }
+long long sortScanBlocks(long long entries) { return (entries + kScanTile - 1) / kScanTile; }
 
-cudaError_t launchSortPermutation(const Geom& g, const float* pos, long long P, unsigned int* key, unsigned int* off,
-                                  unsigned int* sums, unsigned int* perm, cudaStream_t s) {
+cudaError_t launchSortPermutation(const Geom& g, const float* pos, long long P, const SortScratch& sc,
+                                  const unsigned int** perm, cudaStream_t s) {
   const long long n = g.r.size();
   if (n >= (1LL << 32) || P >= (1LL << 32)) return cudaErrorInvalidValue;
-  cudaError_t e = cudaMemsetAsync(off, 0, sizeof(unsigned int) * n, s);
-  if (e != cudaSuccess) return e;
-  if (P > 0) kSortKeys<<<sortGrid(P), kSortThreads, 0, s>>>(g, pos, P, key, off);
-  const long long nb = sortScanBlocks(n);
-  kScanTiles<<<(unsigned)nb, kScanThreads, 0, s>>>(off, n, sums);
-  kScanSums<<<1, kScanThreads, 0, s>>>(sums, (int)nb);
-  kScanAdd<<<sortGrid(n), kSortThreads, 0, s>>>(off, n, sums);
-  if (P > 0) {
-    kSortScatter<<<sortGrid(P), kSortThreads, 0, s>>>(key, P, off, perm);
-    kSortBuckets<<<sortGrid(n), kSortThreads, 0, s>>>(off, n, perm);
+  *perm = sc.valA;
+  if (P <= 0) return cudaSuccess;
+  int bits = 1;
+  while (bits < 32 && ((n - 1) >> bits) != 0) ++bits;
+  const int passes = (bits + kRadixBits - 1) / kRadixBits;
+  const long long tiles = sortTiles(P), entries = sortCountEntries(P), nb = sortScanBlocks(entries);
+  kSortKeys<<<sortGrid(P), kSortThreads, 0, s>>>(g, pos, P, sc.keyA);
+  unsigned int *kIn = sc.keyA, *kOut = sc.keyB, *vIn = nullptr, *vOut = sc.valA;
+  for (int pass = 0; pass < passes; ++pass) {
+    const int shift = pass * kRadixBits;
+    kRadixHist<<<(unsigned)tiles, kRadixThreads, 0, s>>>(kIn, P, shift, sc.counts, tiles);
+    kScanTiles<<<(unsigned)nb, kScanThreads, 0, s>>>(sc.counts, entries, sc.sums);
+    kScanSums<<<1, kScanThreads, 0, s>>>(sc.sums, (int)nb);
+    kScanAdd<<<sortGrid(entries), kSortThreads, 0, s>>>(sc.counts, entries, sc.sums);
+    kRadixScatter<<<(unsigned)tiles, kRadixThreads, 0, s>>>(kIn, vIn, P, shift, sc.counts, tiles, kOut, vOut);
+    std::swap(kIn, kOut);
+    vIn = vOut;
+    vOut = (vOut == sc.valA) ? sc.valB : sc.valA;
   }
+  *perm = vIn;
   return cudaGetLastError();
+}
+
+int sortPassesLaunches(long long nCells) {
+  int bits = 1;
+  while (bits < 32 && ((nCells - 1) >> bits) != 0) ++bits;
+  return 1 + 5 * ((bits + kRadixBits - 1) / kRadixBits);
 }
 
 cudaError_t launchGather(const float* in, int width, const unsigned int* perm, long long P, float* out,
