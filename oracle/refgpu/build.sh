@@ -5,19 +5,29 @@
 # stand-in headers of shim/ for the Windows, boost, assimp and D3D11 headers
 # they name, plus stubs.cpp for the two mesh/CLD entry points that
 # GridFluidSolver.cpp links against and driver.cu (the C ABI the tests and
-# the bench's reference arm load).  Output: oracle/_ref/refgpu/libhfg_refgpu.so.
+# the bench's reference arm load).  Output: oracle/_ref/refgpu/libhfg_refgpu.so,
+# or with "fp64" as $2 the reference's FP64 build (its own -DDOUBLE_REAL
+# switch) as oracle/_ref/refgpu/libhfg_refgpu64.so.
 # Test infrastructure only; nothing is copied out of the reference.
-# Usage: oracle/refgpu/build.sh <reference root>
+# Usage: oracle/refgpu/build.sh <reference root> [fp64]
 set -euo pipefail
-REF=${1:?usage: build.sh <reference root>}
+REF=${1:?usage: build.sh <reference root> [fp64]}
+VARIANT=${2:-}
 SRC="$REF/MPhysics"
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/../_ref/refgpu"
-OBJ="$OUT/obj"
-mkdir -p "$OBJ"
 NVCC=${NVCC:-nvcc}
 FLAGS=(-x cu -std=c++17 -O3 -gencode arch=compute_100a,code=sm_100a -rdc=true -Xcompiler -fPIC -w
        -I"$HERE/shim" -I"$SRC")
+if [ "$VARIANT" = fp64 ]; then
+  OBJ="$OUT/obj64"
+  LIB="$OUT/libhfg_refgpu64.so"
+  FLAGS+=(-DDOUBLE_REAL)
+else
+  OBJ="$OUT/obj"
+  LIB="$OUT/libhfg_refgpu.so"
+fi
+mkdir -p "$OBJ"
 # the grid step and everything it links (GridFluidSolver.cpp names the four
 # HybridSimulator / CLD kernels files at the end of the list)
 UNITS=(EulerSolverTool.cu FieldMathTool.cu EulerParticlesTool.cu EulerMathTool.cu BoundaryTool.cu ThrustWapper.cu
@@ -49,6 +59,6 @@ OBJS=()
 for u in "${UNITS[@]}"; do OBJS+=("$OBJ/${u%.*}.o"); done
 OBJS+=("$OBJ/stubs.o" "$OBJ/driver.o")
 "$NVCC" -gencode arch=compute_100a,code=sm_100a -dlink -Xcompiler -fPIC "${OBJS[@]}" -o "$OBJ/dlink.o"
-g++ -shared -o "$OUT/libhfg_refgpu.so" "${OBJS[@]}" "$OBJ/dlink.o" -L"${CUDA_HOME:-/usr/local/cuda}/lib64" \
+g++ -shared -o "$LIB" "${OBJS[@]}" "$OBJ/dlink.o" -L"${CUDA_HOME:-/usr/local/cuda}/lib64" \
     -lcudart -lcublas -lcusparse -Wl,--no-undefined
-echo "built $OUT/libhfg_refgpu.so"
+echo "built $LIB"

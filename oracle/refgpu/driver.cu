@@ -23,7 +23,9 @@
 // iteration cap through CCuMatrixFreePCG::setIterationNum.  Both reach the
 // PCG object through the pressure solver's private member, which is why the
 // reference headers are included with private access opened below; no
-// arithmetic of the reference is changed.
+// arithmetic of the reference is changed.  Built with -DDOUBLE_REAL (the
+// reference's own switch) the whole step runs in FP64, and every array of
+// this ABI is double.
 #include <cstdio>
 #include <memory>
 #include <stdexcept>
@@ -93,6 +95,10 @@ extern "C" {
 
 const char* rg_last_error() { return g_err.c_str(); }
 
+// sizeof(Real) of this build: 4, or 8 when built with -DDOUBLE_REAL.  Every
+// array argument below is of that type.
+int rg_real_size() { return (int)sizeof(Real); }
+
 int rg_init() {
   return guarded([] {
     if (!CCudaContextManager::getInstance().getIsInit()) CCudaContextManager::getInstance().initCudaContext();
@@ -117,18 +123,18 @@ void* rg_create(float dt, const int res[3], const float origin[3], const float s
 
 void rg_destroy(void* h) { delete static_cast<RefScene*>(h); }
 
-int rg_add_solid(void* h, const float* sdf) {
+int rg_add_solid(void* h, const Real* sdf) {
   return guarded([&] {
     RefScene* s = scene(h);
-    CCellCenteredScalarField f(s->res, s->origin, s->spacing, const_cast<float*>(sdf));
+    CCellCenteredScalarField f(s->res, s->origin, s->spacing, const_cast<Real*>(sdf));
     s->solver->addSolidBoundary(f);
   });
 }
 
-int rg_set_fluid_domain(void* h, const float* dom) {
+int rg_set_fluid_domain(void* h, const Real* dom) {
   return guarded([&] {
     RefScene* s = scene(h);
-    CCellCenteredScalarField f(s->res, s->origin, s->spacing, const_cast<float*>(dom));
+    CCellCenteredScalarField f(s->res, s->origin, s->spacing, const_cast<Real*>(dom));
     s->solver->setFluidDomainField(f);
   });
 }
@@ -155,7 +161,7 @@ int rg_update_boundaries(void* h) {
 // domain and the total solid SDF; returns the reference's particle count, or
 // -1 on error.  When pos is given its n particles replace the seeded ones,
 // and n must equal that count.
-long long rg_set_mix_pic_flip(void* h, int ppc, float cfl, float mixing, const float* pos, long long n) {
+long long rg_set_mix_pic_flip(void* h, int ppc, float cfl, float mixing, const Real* pos, long long n) {
   long long count = -1;
   int rc = guarded([&] {
     RefScene* s = scene(h);
@@ -190,7 +196,7 @@ unsigned long long rg_take_ax_calls() {
   return c;
 }
 
-int rg_velocity(void* h, float* x, float* y, float* z) {
+int rg_velocity(void* h, Real* x, Real* y, Real* z) {
   return guarded([&] {
     const CFaceCenteredVectorField& v = scene(h)->solver->getVelocityField();
     toHost(v.getConstGridDataX(), x);
@@ -204,7 +210,7 @@ long long rg_num_particles(void* h) {
   return (s && s->mix) ? (long long)s->mix->getEulerParticles().getNumOfParticles() : 0;
 }
 
-int rg_particles(void* h, float* pos, float* vel) {
+int rg_particles(void* h, Real* pos, Real* vel) {
   return guarded([&] {
     RefScene* s = scene(h);
     if (!s->mix) throw std::runtime_error("no particles: the advection solver is not the PIC/FLIP mix");
@@ -213,11 +219,11 @@ int rg_particles(void* h, float* pos, float* vel) {
   });
 }
 
-int rg_markers(void* h, float* m) {
+int rg_markers(void* h, Real* m) {
   return guarded([&] { toHost(scene(h)->solver->getPressureSolver()->getMarkers().getConstGridData(), m); });
 }
 
-int rg_pressure(void* h, float* p) {
+int rg_pressure(void* h, Real* p) {
   return guarded([&] { toHost(scene(h)->solver->getPressureSolver()->getConstVectorx().getConstVectorValue(), p); });
 }
 

@@ -28,8 +28,11 @@ def test_driver_declares_the_bound_entry_points():
         assert n in binding, n
 
 
-@pytest.mark.skipif(not refgpu.available(), reason="oracle/_ref/refgpu is not built")
-def test_reference_library_loads_and_exports():
-    lib = ctypes.CDLL(refgpu.LIB)
+@pytest.mark.parametrize("fp64", [False, True])
+def test_reference_library_loads_and_exports(fp64):
+    if not refgpu.available(fp64):
+        pytest.skip("oracle/_ref/refgpu is not built")
+    lib = ctypes.CDLL(refgpu.LIB64 if fp64 else refgpu.LIB)
     for n in driver_exports():
         assert hasattr(lib, n), n
+    assert lib.rg_real_size() == (8 if fp64 else 4)
