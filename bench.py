@@ -44,6 +44,9 @@ CG_DRAM_BYTES_PER_CELL = (105.90e6 + 6.42e6 + 146.36e6 + 11.13e6) / 224 ** 3
 # Algorithmic bytes of one CFL substep per particle: position and v0 read and
 # written (FP32 xyz each); the corner-table gathers hit L2.
 SUBSTEP_BYTES_PER_PARTICLE = 48.0
+# dram__bytes_read.sum + dram__bytes_write.sum of one kSubstep launch, ncu
+# --set full on the 160^3 dam break (7.57 M particles), per particle
+SUBSTEP_DRAM_BYTES_PER_PARTICLE = (243.0e6 + 130.0e6) / 7565040
 UNIT = "Mcell-steps/s"
 
 
@@ -805,7 +808,9 @@ def run_dam_break(args):
                        "stage_ms_one_more_step": stage_ms, "particle_ms_one_more_step": particle_ms},
             "roofline": {"bound": "hbm", "kernel": "kSubstep (one CFL particle substep)",
                          "achieved": sub_achieved, "peak": hbm, "unit": "GB/s", "frac": sub_achieved / hbm,
-                         "traffic": None, "algorithmic_bytes_per_launch": sub_bytes,
+                         "traffic": SUBSTEP_DRAM_BYTES_PER_PARTICLE * n,
+                         "traffic_source": "ncu dram__bytes_read+write at 160^3, per particle, scaled",
+                         "algorithmic_bytes_per_launch": sub_bytes,
                          "bytes_per_particle": SUBSTEP_BYTES_PER_PARTICLE, "ms_per_launch": sub_launch_ms,
                          "launches_per_step": conv["substeps"], "peak_source": peak_source,
                          "cg_pair": {"kernel": "kCgDirection + kCgUpdate (one CG iteration)", "achieved": achieved,

@@ -1592,6 +1592,11 @@ template <class T> static void sGetParticles(OrcSolver* S, float* pos, float* ve
   if (pos) down(s.ppos, pos);
   if (vel) down(s.pvel, vel);
 }
+template <class T> static void sGetParticles64(OrcSolver* S, double* pos, double* vel) {
+  Solver<T>& s = pick<T>(S);
+  if (pos) for (size_t i = 0; i < s.ppos.size(); ++i) pos[i] = (double)s.ppos[i];
+  if (vel) for (size_t i = 0; i < s.pvel.size(); ++i) vel[i] = (double)s.pvel[i];
+}
 template <class T> static void sStats(OrcSolver* S, double* out) {
   Solver<T>& s = pick<T>(S);
   out[0] = (double)s.lastIters; out[1] = s.lastResid; out[2] = s.lastBnorm;
@@ -1646,6 +1651,9 @@ void orc_solver_get_solid_sdf(void* p, float* x) { ORC_CALL((OrcSolver*)p, sGetS
 void orc_solver_get_solid_vel(void* p, float* x, float* y, float* z) { ORC_CALL((OrcSolver*)p, sGetSolidVel, x, y, z); }
 long long orc_solver_num_particles(void* p) { return ORC_CALL((OrcSolver*)p, sNumParticles); }
 void orc_solver_get_particles(void* p, float* pos, float* vel) { ORC_CALL((OrcSolver*)p, sGetParticles, pos, vel); }
+void orc_solver_get_particles_f64(void* p, double* pos, double* vel) {
+  ORC_CALL((OrcSolver*)p, sGetParticles64, pos, vel);
+}
 // stats: [cg iterations, final ||r||, ||b||, time, substeps, buffer flag]
 void orc_solver_stats(void* p, double* out) { ORC_CALL((OrcSolver*)p, sStats, out); }
 

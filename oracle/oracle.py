@@ -90,6 +90,7 @@ def lib():
             "orc_solver_solve_pressure": (C.c_int, [vp]),
             "orc_solver_get_velocity": (None, [vp, C.c_int, PF, PF, PF]),
             "orc_solver_get_velocity_f64": (None, [vp, PD, PD, PD]),
+            "orc_solver_get_particles_f64": (None, [vp, PD, PD]),
             "orc_solver_get_fluid_domain": (None, [vp, PF]),
             "orc_solver_get_color": (None, [vp, PF, PF, PF]),
             "orc_solver_get_markers": (None, [vp, PU8]),
@@ -456,6 +457,14 @@ class Solver:
         pos = np.empty((n, 3), np.float32)
         vel = np.empty((n, 3), np.float32)
         lib().orc_solver_get_particles(self._h, fp(pos), fp(vel))
+        return pos, vel
+
+    def particles_f64(self):
+        """Positions and velocities at the solver's own precision (FP64 for dbl=1)."""
+        n = self.num_particles
+        pos = np.empty((n, 3), np.float64)
+        vel = np.empty((n, 3), np.float64)
+        lib().orc_solver_get_particles_f64(self._h, pos.ctypes.data_as(PD), vel.ctypes.data_as(PD))
         return pos, vel
 
     def stats(self):

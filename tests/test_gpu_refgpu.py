@@ -204,7 +204,7 @@ def test_fp64_oracle_matches_the_reference_fp64_step(cuda, which):
         it_r = max(r.take_ax_calls() - 1, 0)
         it_o = o.stats()["cg_iterations"]
         rp, _ = r.particles()
-        op, _ = o.particles()
+        op, _ = o.particles_f64()
         vr = r.velocity_field()
         vo = o.velocity_field_f64()
         err = rel_l2(vo, vr)
