@@ -46,7 +46,7 @@ CG_DRAM_BYTES_PER_CELL = (105.90e6 + 6.42e6 + 146.36e6 + 11.13e6) / 224 ** 3
 SUBSTEP_BYTES_PER_PARTICLE = 48.0
 # dram__bytes_read.sum + dram__bytes_write.sum of one kSubstep launch, ncu
 # --set full on the 160^3 dam break (7.57 M particles), per particle
-SUBSTEP_DRAM_BYTES_PER_PARTICLE = (243.0e6 + 130.0e6) / 7565040
+SUBSTEP_DRAM_BYTES_PER_PARTICLE = (243.88e6 + 133.72e6) / 7565040
 UNIT = "Mcell-steps/s"
 
 
