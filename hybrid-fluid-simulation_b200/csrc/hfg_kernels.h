@@ -143,8 +143,9 @@ cudaError_t makeCgMaps(const Dim3i& cg, const CgCode* code, const float* r, cons
 cudaError_t makeHaloMap(const Dim3i& cg, const float* v, CUtensorMap* m);
 // precond: 0 identity, 1 Jacobi, 2 z read through mZ (must match CgState::precond);
 // mZ is the halo map of r (precond 0, 1) or of z (2); zr the same array.
-// colZ (optional, from launchFluidColumns): the fluid extent of every tile
-// column; blocks whose planes hold no fluid skip their stream.
+// colZ (optional, from launchCgSchedule): the solve's schedule; the grid is
+// then one block per work item (a tile column's run of fluid planes), sized
+// for one wave.  Null: the dense grid over every tile and z chunk.
 cudaError_t launchCgDirection(const Dim3i& cg, float sx, float sy, float sz, const CUtensorMap& mZ,
                               const CUtensorMap& mPo, const CUtensorMap& mCode, const CgCode* code, const float* zr,
                               const float* pOld, float* pNew, double* partials, CgState* st, int precond,
@@ -161,10 +162,13 @@ int tunedCgZPer(int family, const Dim3i& cg);  // -1: none
 std::vector<int> cgZPerCandidates(const Dim3i& cg);
 bool saveTuning(const char* path);
 int loadTuning(const char* path);  // entries read, -1 if the file cannot be opened
-// Fluid extent of the CG tile columns (32 x 16 cells of the pitched grid cg,
-// all z), from the CG codes: colZ holds 2 * cgColumns(cg) ints.
+// The schedule of the CG kernels for a solve, from the CG codes: the fluid
+// extent of every tile column (32 x 16 cells of the pitched grid cg, all z)
+// and the work items cut from it for one wave of blocks of the kernels of
+// `precond`.  sched holds cgScheduleInts(cg) ints.
 int cgColumns(const Dim3i& cg);
-cudaError_t launchFluidColumns(const Dim3i& cg, const CgCode* code, int* colZ, cudaStream_t s);
+int cgScheduleInts(const Dim3i& cg);
+cudaError_t launchCgSchedule(const Dim3i& cg, const CgCode* code, int* sched, int precond, cudaStream_t s);
 // Divergence residual of the projected velocity over the fluid cells:
 // *sumOut = sum b^2 (FP64), ticketAndMax[1] = bits of max |b|.  `scratch`
 // holds 2 * divergenceBlocks() doubles.

@@ -487,15 +487,39 @@ struct CgLaunch {
   int zPer;
 };
 
-// Fluid extent of the CG tile columns (CTX x CTR cells of the pitched grid,
-// every z): colZ[t] the lowest and colZ[cols + t] the highest plane holding a
-// fluid cell of column t = blockIdx.y * gridDim.x + blockIdx.x, or a range
-// that no chunk meets when the column has none.  Null: every block active.
-__device__ __forceinline__ bool columnActive(const int* colZ, int z0, int z1) {
-  if (!colZ) return true;
-  const unsigned cols = gridDim.x * gridDim.y, t = blockIdx.y * gridDim.x + blockIdx.x;
-  const int lo = __ldg(colZ + t), hi = __ldg(colZ + cols + t);
-  return lo < z1 && hi >= z0;
+// The CG schedule of a solve (launchCgSchedule), in one int array:
+//   [0, cols)            the lowest plane holding a fluid cell of each tile
+//                        column (CTX x CTR cells of the pitched grid, all z),
+//   [cols, 2 cols)       the highest (a range no plane meets: no fluid),
+//   [2 cols]             the number of work items,
+//   [schedItemsOffset)   the items (column, z0, z1, 0): one per CG block, the
+//                        fluid planes of the active columns cut into chunks
+//                        so that the items about fill one wave of blocks.
+// A block past the last item only joins the reductions.  Null: the dense
+// grid, block (x, y, z) on tile (x, y) and planes [z zPer, (z + 1) zPer).
+__host__ __device__ __forceinline__ int schedItemsOffset(int cols) { return (2 * cols + 1 + 3) & ~3; }
+
+__device__ __forceinline__ bool cgBlockWork(const int* sched, const Dim3i& P, int zPer, int& x0, int& y0, int& z0,
+                                            int& z1) {
+  if (!sched) {
+    x0 = blockIdx.x * CTX;
+    y0 = blockIdx.y * CTR;
+    z0 = blockIdx.z * zPer;
+    z1 = min(z0 + zPer, P.z);
+    return true;
+  }
+  const int tilesX = (P.x + CTX - 1) / CTX, cols = tilesX * ((P.y + CTR - 1) / CTR);
+  const int n = __ldg(sched + 2 * cols);
+  if ((int)blockIdx.x >= n) {
+    x0 = y0 = z0 = z1 = 0;
+    return false;
+  }
+  const int4 w = __ldg(reinterpret_cast<const int4*>(sched + schedItemsOffset(cols)) + blockIdx.x);
+  x0 = (w.x % tilesX) * CTX;
+  y0 = (w.x / tilesX) * CTR;
+  z0 = w.y;
+  z1 = w.z;
+  return true;
 }
 
 // Tiles over (x, y), z split into chunks so that the blocks fill whole waves
@@ -514,6 +538,12 @@ int residentBlocks(const void* kernel) {
 }
 
 }  // namespace
+
+// Work items of a CG schedule: one wave of the CG kernels of this
+// preconditioner (the fewest resident blocks of the direction and both update
+// kernels, at most kSchedPerSM per SM).
+constexpr int kSchedPerSM = 8;
+int cgScheduleTarget(int precond);
 
 // ---------------------------------------------------------------------------
 // Launch shapes picked by measurement.  autotuneCg (driven by the solver)
@@ -575,11 +605,17 @@ int loadTuning(const char* path) {
 }
 
 namespace {
-// family: 0 for kCgDirection, 1 for kCgUpdate (the key of the tuning table)
+// family: 0 for kCgDirection, 1 for kCgUpdate (the key of the tuning table).
+// With a schedule the grid is one block per possible work item.
 template <class K>
-CgLaunch cgLaunch(const Dim3i& cg, K kernel, int family) {
+CgLaunch cgLaunch(const Dim3i& cg, K kernel, int family, const int* sched = nullptr, int precond = 1) {
   CgLaunch L;
   L.block = dim3(CTX, CTY, 1);
+  if (sched) {
+    L.zPer = 0;
+    L.grid = dim3(cgScheduleTarget(precond) + cgColumns(cg), 1, 1);
+    return L;
+  }
   int bx = (cg.x + CTX - 1) / CTX, by = (cg.y + CTR - 1) / CTR;
   const int tuned = tunedZPer(family, cg);
   if (tuned > 0) {
@@ -628,12 +664,7 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
   __shared__ __align__(8) uint64_t bar[kDirStages];
   __shared__ int issued;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * CTX + tx;
-  const int x0 = blockIdx.x * CTX, y0 = blockIdx.y * CTR;
-  const int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, P.z);
-  // a block whose planes hold no fluid cell of its tile column writes
-  // nothing and adds zero to the reduction: it skips the stream
-  const bool active = columnActive(colZ, z0, z1);
-  const int nPlanes = active ? z1 - z0 : 0, nLoad = nPlanes + 1;  // plane z1 is the last "above"
+  int x0 = 0, y0 = 0, z0 = 0, z1 = 0;
   auto issue = [&](int i) {
     DirStage& S = stg[i % kDirStages];
     uint64_t* b = &bar[i % kDirStages];
@@ -651,6 +682,10 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
   waitPrevGrid();
   if (st->done) return;  // the same value in every thread
   allowNextGrid();
+  // a block with no work item (sched) writes nothing and adds zero to the
+  // reduction; the schedule was written before the kernels before this one
+  const bool active = cgBlockWork(colZ, P, zPer, x0, y0, z0, z1);
+  const int nPlanes = active ? z1 - z0 : 0, nLoad = nPlanes + 1;  // plane z1 is the last "above"
   if (tid == 0) {
     int n = active ? min(kDirStages, nLoad) : 0;
     for (int i = 0; i < n; ++i) issue(i);
@@ -765,10 +800,7 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
   __shared__ __align__(8) uint64_t bar[kUpdStages];
   __shared__ int issued;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * CTX + tx;
-  const int x0 = blockIdx.x * CTX, y0 = blockIdx.y * CTR;
-  const int z0 = blockIdx.z * zPer, z1 = min(z0 + zPer, P.z);
-  const bool active = columnActive(colZ, z0, z1);  // as in kCgDirection
-  const int nPlanes = active ? z1 - z0 : 0, nLoad = nPlanes + 1;
+  int x0 = 0, y0 = 0, z0 = 0, z1 = 0;
   auto issue = [&](int i) {
     Stage& S = stg[i % kUpdStages];
     uint64_t* b = &bar[i % kUpdStages];
@@ -787,6 +819,8 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
   waitPrevGrid();
   if (st->done) return;  // the same value in every thread
   allowNextGrid();
+  const bool active = cgBlockWork(colZ, P, zPer, x0, y0, z0, z1);  // as in kCgDirection
+  const int nPlanes = active ? z1 - z0 : 0, nLoad = nPlanes + 1;
   if (tid == 0) {
     int n = active ? min(kUpdStages, nLoad) : 0;
     for (int i = 0; i < n; ++i) issue(i);
@@ -925,6 +959,30 @@ void cgWarmLaunchCache() {
   residentBlocks((const void*)kCgUpdate<2, double>);
 }
 
+int cgScheduleTarget(int precond) {
+  int per = kSchedPerSM;
+  auto take = [&](const void* k) { per = std::min(per, residentBlocks(k)); };
+  if (precond == 1) {
+    take((const void*)kCgDirection<1>);
+    take((const void*)kCgUpdate<1, float>);
+    take((const void*)kCgUpdate<1, double>);
+  } else if (precond == 2) {
+    take((const void*)kCgDirection<2>);
+    take((const void*)kCgUpdate<2, float>);
+    take((const void*)kCgUpdate<2, double>);
+  } else {
+    take((const void*)kCgDirection<0>);
+    take((const void*)kCgUpdate<0, float>);
+    take((const void*)kCgUpdate<0, double>);
+  }
+  return numSMs() * std::max(1, per);
+}
+
+int cgScheduleInts(const Dim3i& cg) {
+  const int cols = cgColumns(cg);
+  return schedItemsOffset(cols) + 4 * (numSMs() * kSchedPerSM + cols);
+}
+
 int cgPartialsNeeded(const Dim3i& r) {
   const Dim3i cg = cgDims(r);
   CgGrid g = cgGrid(cg);
@@ -932,6 +990,7 @@ int cgPartialsNeeded(const Dim3i& r) {
   // the CG kernels, at the shortest z chunk any launch shape (tuned or not) uses
   const long long tiles = (long long)((cg.x + CTX - 1) / CTX) * ((cg.y + CTR - 1) / CTR);
   n = std::max(n, tiles * ((cg.z + std::min(3, cg.z) - 1) / std::min(3, cg.z)));
+  n = std::max(n, (long long)numSMs() * kSchedPerSM + tiles);  // a schedule's grid
   return 2 * (int)n;
 }
 
@@ -941,21 +1000,21 @@ cudaError_t launchCgDirection(const Dim3i& cg, float sx, float sy, float sz, con
                               cudaStream_t s, const int* colZ) {
   switch (precond) {
     case 1: {
-      CgLaunch L = cgLaunch(cg, kCgDirection<1>, 0);
+      CgLaunch L = cgLaunch(cg, kCgDirection<1>, 0, colZ, 1);
       cudaError_t e = launchPdl(kCgDirection<1>, L.grid, L.block, s, mZ, mPo, mCode, cg, sx, sy, sz, code, zr, pOld,
                                 pNew, partials, st, L.zPer, colZ);
       if (e != cudaSuccess) return e;
       break;
     }
     case 2: {
-      CgLaunch L = cgLaunch(cg, kCgDirection<2>, 0);
+      CgLaunch L = cgLaunch(cg, kCgDirection<2>, 0, colZ, 2);
       cudaError_t e = launchPdl(kCgDirection<2>, L.grid, L.block, s, mZ, mPo, mCode, cg, sx, sy, sz, code, zr, pOld,
                                 pNew, partials, st, L.zPer, colZ);
       if (e != cudaSuccess) return e;
       break;
     }
     default: {
-      CgLaunch L = cgLaunch(cg, kCgDirection<0>, 0);
+      CgLaunch L = cgLaunch(cg, kCgDirection<0>, 0, colZ, 0);
       cudaError_t e = launchPdl(kCgDirection<0>, L.grid, L.block, s, mZ, mPo, mCode, cg, sx, sy, sz, code, zr, pOld,
                                 pNew, partials, st, L.zPer, colZ);
       if (e != cudaSuccess) return e;
@@ -969,7 +1028,7 @@ cudaError_t launchCgUpdate(const Dim3i& cg, float sx, float sy, float sz, const 
                            float* r, double* partials, CgState* st, int precond, cudaStream_t s, const int* colZ) {
 #define HFG_CG_UPDATE(PCV, TXV)                                                                                   \
   {                                                                                                               \
-    CgLaunch L = cgLaunch(cg, kCgUpdate<PCV, TXV>, 1);                                                             \
+    CgLaunch L = cgLaunch(cg, kCgUpdate<PCV, TXV>, 1, colZ, PCV);                                                             \
     cudaError_t e = launchPdl(kCgUpdate<PCV, TXV>, L.grid, L.block, s, mP, mR, mX, mCode, cg, sx, sy, sz, p,      \
                               (TXV*)x, r, partials, st, L.zPer, colZ);                                        \
     if (e != cudaSuccess) return e;                                                                             \
@@ -1016,14 +1075,81 @@ __global__ void kFluidColumns(Dim3i cg, const CgCode* __restrict__ code, int zPe
   }
 }
 int cgColumns(const Dim3i& cg) { return ((cg.x + CTX - 1) / CTX) * ((cg.y + CTR - 1) / CTR); }
-cudaError_t launchFluidColumns(const Dim3i& cg, const CgCode* code, int* colZ, cudaStream_t s) {
+
+// The work items of a schedule from the columns' fluid extents: chunks of
+// zLen = max(zMin, ceil(S / target)) planes, S the fluid planes of all active
+// columns, so the items are at most target + (active columns); they are
+// written column by column, bottom to top.  One block.
+constexpr int kListThreads = 1024;
+__global__ void __launch_bounds__(kListThreads) kCgWorkList(int cols, int target, int zMin, int* sched) {
+  const int* lo = sched;
+  const int* hi = sched + cols;
+  int4* items = reinterpret_cast<int4*>(sched + schedItemsOffset(cols));
+  __shared__ unsigned long long total;
+  __shared__ int warpTot[kListThreads / 32];
+  __shared__ int carry;
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  if (t == 0) {
+    total = 0;
+    carry = 0;
+  }
+  __syncthreads();
+  unsigned long long mine = 0;
+  for (int c = t; c < cols; c += kListThreads)
+    if (hi[c] >= lo[c]) mine += (unsigned long long)(hi[c] - lo[c] + 1);
+  atomicAdd(&total, mine);
+  __syncthreads();
+  const long long S = (long long)total;
+  const int zLen = (int)max((long long)zMin, (S + target - 1) / max(target, 1));
+  for (int c0 = 0; c0 < cols; c0 += kListThreads) {
+    const int c = c0 + t;
+    int n = 0, l = 0;
+    if (c < cols && hi[c] >= lo[c]) {
+      l = lo[c];
+      n = (hi[c] - l + zLen) / zLen;
+    }
+    int inc = n;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, inc, d);
+      if (lane >= d) inc += y;
+    }
+    if (lane == 31) warpTot[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+      int x = warpTot[lane], xi = x;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, xi, d);
+        if (lane >= d) xi += y;
+      }
+      warpTot[lane] = xi - x;
+    }
+    __syncthreads();
+    int k = carry + warpTot[w] + inc - n;
+    for (int i = 0; i < n; ++i, ++k) {
+      const int z0 = l + i * zLen;
+      items[k] = make_int4(c, z0, min(z0 + zLen, hi[c] + 1), 0);
+    }
+    __syncthreads();
+    if (t == kListThreads - 1) carry = k;
+    __syncthreads();
+  }
+  if (t == 0) sched[2 * cols] = carry;
+}
+
+cudaError_t launchCgSchedule(const Dim3i& cg, const CgCode* code, int* sched, int precond, cudaStream_t s) {
   const int cols = cgColumns(cg);
-  cudaError_t e = cudaMemsetAsync(colZ, 0x7f, sizeof(int) * cols, s);  // lo: 0x7f7f7f7f, above any plane
-  if (e == cudaSuccess) e = cudaMemsetAsync(colZ + cols, 0xff, sizeof(int) * cols, s);  // hi: -1
+  cudaError_t e = cudaMemsetAsync(sched, 0x7f, sizeof(int) * cols, s);  // lo: 0x7f7f7f7f, above any plane
+  if (e == cudaSuccess) e = cudaMemsetAsync(sched + cols, 0xff, sizeof(int) * cols, s);  // hi: -1
   if (e != cudaSuccess) return e;
   const int zPer = 16;
   dim3 grid((cg.x + CTX - 1) / CTX, (cg.y + CTR - 1) / CTR, (cg.z + zPer - 1) / zPer);
-  kFluidColumns<<<grid, dim3(CTX, CTR), 0, s>>>(cg, code, zPer, colZ);
+  kFluidColumns<<<grid, dim3(CTX, CTR), 0, s>>>(cg, code, zPer, sched);
+  // the shortest chunk: the tuned z-chunk length of the direction kernel, else 3 planes
+  const int tuned = tunedZPer(0, cg);
+  const int zMin = tuned > 0 ? tuned : std::min(3, cg.z);
+  kCgWorkList<<<1, kListThreads, 0, s>>>(cols, cgScheduleTarget(precond), zMin, sched);
   return cudaGetLastError();
 }
 

@@ -102,7 +102,9 @@ GridSolver::GridSolver(float dt, Dim3i res, const float origin[3], const float s
   cgp_[0].alloc(NC_, stream_);
   cgp_[1].alloc(NC_, stream_);
   partials_.alloc(cgPartialsNeeded(res), stream_);
-  colZ_.alloc(2 * (size_t)cgColumns(cgDims(res)), stream_);
+  colZ_.alloc((size_t)cgScheduleInts(cgDims(res)), stream_);
+  // an empty schedule (no work items) until the first solve builds one
+  check(cudaMemsetAsync(colZ_.p, 0, colZ_.bytes(), stream_), "memset");
   check(makeCgMaps(cg_, cgc_.p, cgr_.p, cgx_.p, false, cgp_[0].p, cgp_[1].p, &maps_), "CG tensor maps");
   cgState_.alloc(1, stream_);
   subState_.alloc(subSlots_ + 1, stream_);
@@ -666,7 +668,9 @@ void GridSolver::computePressure() {
     launched(launchMarkersFromParticles(g_, ppos_.p, P_, markers_.p, stream_), "markers");
   }
   launched(launchStencilCode(g_.r, cg_.x, markers_.p, code_.p, stream_, cgc_.p), "stencil code");
-  launched(launchFluidColumns(cg_, cgc_.p, colZ_.p, stream_), "fluid columns");
+  const int schedPc =
+      opt_.precond == HFG_PRECOND_MG ? 2 : (opt_.precond == HFG_PRECOND_JACOBI ? 1 : 0);
+  launched(launchCgSchedule(cg_, cgc_.p, colZ_.p, schedPc, stream_), "cg schedule", 2);
   stageEnd(3);
   stageBegin(4);
   CgState init{};
@@ -829,6 +833,8 @@ void GridSolver::autotuneCg(float sx, float sy, float sz, int pc) {
     for (int z : cands) {
       setTunedCgZPer(0, cg_, z);
       setTunedCgZPer(1, cg_, z);
+      // the schedule's shortest chunk is the tuned length
+      launched(launchCgSchedule(cg_, cgc_.p, colZ_.p, pc, stream_), "cg schedule", 2);
       *cgHost_ = st;
       check(cudaMemcpyAsync(cgState_.p, cgHost_, sizeof(CgState), cudaMemcpyHostToDevice, stream_), "cg state");
       cgIteration(0, sx, sy, sz, pc);  // warm-up
@@ -864,6 +870,7 @@ void GridSolver::autotuneCg(float sx, float sy, float sz, int pc) {
   for (auto& x : e) cudaEventDestroy(x);
   setTunedCgZPer(0, cg_, pick[0]);
   setTunedCgZPer(1, cg_, pick[1]);
+  launched(launchCgSchedule(cg_, cgc_.p, colZ_.p, pc, stream_), "cg schedule", 2);
   dropGraphs();
 }
 

@@ -224,7 +224,7 @@ class GridSolver {
   bool xDouble() const { return opt_.pressure_fp64 != 0; }
   void* xPtr() { return xDouble() ? (void*)cgx64_.p : (void*)cgx_.p; }
   DArray<double> partials_;
-  DArray<int> colZ_;  // fluid extent of the CG tile columns (launchFluidColumns), per solve
+  DArray<int> colZ_;  // the CG schedule of the solve (launchCgSchedule)
   DArray<CgState> cgState_;
   CgState* cgHost_ = nullptr;  // pinned
   DArray<SubstepState> subState_;
