@@ -168,6 +168,12 @@ int loadTuning(const char* path);  // entries read, -1 if the file cannot be ope
 // `precond`.  sched holds cgScheduleInts(cg) ints.
 int cgColumns(const Dim3i& cg);
 int cgScheduleInts(const Dim3i& cg);
+int cgScheduleTarget(int precond);  // work items of one wave (the schedule's grid: this + cgColumns)
+// Layout of a schedule: ints [0, cols) and [cols, 2 cols) the lowest and
+// highest fluid plane of each tile column (kCgTileX x kCgTileY cells), [2 cols]
+// the item count, from schedItemsOffset(cols) the items (column, z0, z1, 0).
+constexpr int kCgTileX = 32, kCgTileY = 16;
+__host__ __device__ inline int schedItemsOffset(int cols) { return (2 * cols + 1 + 3) & ~3; }
 cudaError_t launchCgSchedule(const Dim3i& cg, const CgCode* code, int* sched, int precond, cudaStream_t s);
 // Divergence residual of the projected velocity over the fluid cells:
 // *sumOut = sum b^2 (FP64), ticketAndMax[1] = bits of max |b|.  `scratch`

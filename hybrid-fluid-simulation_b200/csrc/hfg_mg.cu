@@ -213,16 +213,49 @@ SweepGrid sweepGrid(const Dim3i& r, bool reduce) {
 // and the arithmetic are those of kJacobi, so the sweeps agree bit for bit;
 // only the order of the r.z partial sums differs.
 constexpr int MX = 32, MY = 8;
+static_assert(MX == kCgTileX && 2 * MY == kCgTileY, "two sweep blocks per tile column of the CG schedule");
+
+// The cells a level-0 marching block sweeps: with the CG schedule of the
+// solve (launchCgSchedule), two blocks per work item, the lower and upper 8
+// rows of its 32 x 16 tile column over its run of fluid planes (a block past
+// the last item sweeps nothing); without, the dense grid (tile x, tile y, z
+// chunk of zLen planes).  Cells off the fluid keep z = 0 and add nothing to
+// r.z, so skipping the planes no fluid cell of the column occupies changes
+// no value.
+__device__ __forceinline__ void mgBlockWork(const int* sched, const Dim3i& r, int zLen, int& x0, int& y0, int& z0,
+                                            int& z1) {
+  if (!sched) {
+    x0 = blockIdx.x * MX;
+    y0 = blockIdx.y * MY;
+    z0 = blockIdx.z * zLen;
+    z1 = min(z0 + zLen, r.z);
+    return;
+  }
+  const int tilesX = (r.x + kCgTileX - 1) / kCgTileX, cols = tilesX * ((r.y + kCgTileY - 1) / kCgTileY);
+  const int item = blockIdx.x >> 1;
+  if (item >= __ldg(sched + 2 * cols)) {
+    x0 = y0 = z0 = z1 = 0;
+    return;
+  }
+  const int4 w = __ldg(reinterpret_cast<const int4*>(sched + schedItemsOffset(cols)) + item);
+  x0 = (w.x % tilesX) * kCgTileX;
+  y0 = (w.x / tilesX) * kCgTileY + (blockIdx.x & 1) * MY;
+  z0 = w.y;
+  z1 = w.z;
+}
+
 template <class TC, bool CORR, bool DOT, class TZI = float, class TZO = float>
 __global__ void __launch_bounds__(MX* MY)
     kJacobiZ(Lvl L, Dim3i rc, const float* __restrict__ b, const TZI* __restrict__ zi, TZO* __restrict__ zo,
-             const TC* __restrict__ zc, const Code* __restrict__ code, double* partials, CgState* st, int zLen) {
+             const TC* __restrict__ zc, const Code* __restrict__ code, double* partials, CgState* st, int zLen,
+             const int* __restrict__ sched) {
   waitPrevGrid();
   if (st->done) return;
   allowNextGrid();
   double rz = 0.0, dummy = 0.0;
-  const int x = blockIdx.x * MX + threadIdx.x, y = blockIdx.y * MY + threadIdx.y;
-  const int z0 = blockIdx.z * zLen, z1 = min(z0 + zLen, L.r.z);
+  int xb, yb, z0, z1;
+  mgBlockWork(sched, L.r, zLen, xb, yb, z0, z1);
+  const int x = xb + threadIdx.x, y = yb + threadIdx.y;
   if (x < L.r.x && y < L.r.y && z0 < z1) {
     const unsigned pl = (unsigned)L.r.x * L.r.y;
     auto par = [&](int i, int j, int k) { return ((unsigned)(k >> 1) * rc.y + (j >> 1)) * rc.x + (i >> 1); };
@@ -284,12 +317,13 @@ __global__ void __launch_bounds__(MX* MY)
 template <class TZO>
 __global__ void __launch_bounds__(MX* MY)
     kJacobiFirstZ(Lvl L, const float* __restrict__ b, TZO* __restrict__ z, const Code* __restrict__ code,
-                  const CgState* st, int zLen) {
+                  const CgState* st, int zLen, const int* __restrict__ sched) {
   waitPrevGrid();
   if (st->done) return;
   allowNextGrid();
-  const int x = blockIdx.x * MX + threadIdx.x, y = blockIdx.y * MY + threadIdx.y;
-  const int z0 = blockIdx.z * zLen, z1 = min(z0 + zLen, L.r.z);
+  int xb, yb, z0, z1;
+  mgBlockWork(sched, L.r, zLen, xb, yb, z0, z1);
+  const int x = xb + threadIdx.x, y = yb + threadIdx.y;
   if (x >= L.r.x || y >= L.r.y) return;
   const unsigned pl = (unsigned)L.r.x * L.r.y;
   unsigned c = ((unsigned)z0 * L.r.y + y) * L.r.x + x;
@@ -450,7 +484,7 @@ Multigrid* mgCreate(const Dim3i& r, int levels, int smooth, int halfMode, cudaSt
   m->p[1].alloc(N, s);
   const dim3 mg = marchGrid(r).grid;
   m->partials.alloc(std::max({cgPartialsNeeded(r), 2 * (int)(gridOf(r).x * gridOf(r).y * gridOf(r).z),
-                              2 * (int)(mg.x * mg.y * mg.z)}),
+                              2 * (int)(mg.x * mg.y * mg.z), 2 * 2 * (cgScheduleTarget(2) + cgColumns(r))}),
                     s);
   check(makeHaloMap(r, m->z0a.p, &m->zH[0]), "multigrid tensor map");
   check(makeHaloMap(r, m->z0b.p, &m->zH[1]), "multigrid tensor map");
@@ -499,7 +533,7 @@ void mgSetupLevels(Multigrid* m, const uint8_t* mk0, const Code* code0, float sx
 namespace {
 template <class TS>
 const float* vcycleT(Multigrid* m, const float* r0, CgState* st, cudaStream_t s, long long& launches, TS* const* bL,
-                     TS* const* zaL, TS* const* zbL) {
+                     TS* const* zaL, TS* const* zbL, const int* sched) {
   const int L = m->levels();
   std::vector<Lvl> lv(L);
   for (int l = 0; l < L; ++l) {
@@ -524,7 +558,11 @@ const float* vcycleT(Multigrid* m, const float* r0, CgState* st, cudaStream_t s,
   // a level-0 sweep marching along z
   const SweepGrid mg0 = marchGrid(lv[0].r);
   const bool marching = marchLevel0(lv[0].r);
-  auto march = [&](auto kernel, auto... args) { run(kernel, mg0.grid, dim3(MX, MY), args..., mg0.zPer); };
+  // with the solve's CG schedule: two blocks per work item, fluid runs only
+  const dim3 schedGrid(2 * (cgScheduleTarget(2) + cgColumns(lv[0].r)), 1, 1);
+  auto march = [&](auto kernel, auto... args) {
+    run(kernel, sched ? schedGrid : mg0.grid, dim3(MX, MY), args..., mg0.zPer, sched);
+  };
   // which ping-pong buffer holds the current iterate of each level
   std::vector<int> curBuf(L, 0);
   float* z0[2] = {m->z0a.p, m->z0b.p};
@@ -653,7 +691,8 @@ const float* vcycleT(Multigrid* m, const float* r0, CgState* st, cudaStream_t s,
 
 // z = V(r0) (returned: one of the two level-0 buffers), and st->rz /
 // st->beta updated by the last sweep.
-const float* mgVcycle(Multigrid* m, const float* r0, CgState* st, cudaStream_t s, long long& launches) {
+const float* mgVcycle(Multigrid* m, const float* r0, CgState* st, cudaStream_t s, long long& launches,
+                      const int* sched) {
   const int L = m->levels();
   if (m->half) {
     std::vector<__nv_bfloat16*> b(L, nullptr), za(L, nullptr), zb(L, nullptr);
@@ -662,7 +701,7 @@ const float* mgVcycle(Multigrid* m, const float* r0, CgState* st, cudaStream_t s
       za[l] = (__nv_bfloat16*)m->z16a[l - 1]->p;
       zb[l] = (__nv_bfloat16*)m->z16b[l - 1]->p;
     }
-    return vcycleT<__nv_bfloat16>(m, r0, st, s, launches, b.data(), za.data(), zb.data());
+    return vcycleT<__nv_bfloat16>(m, r0, st, s, launches, b.data(), za.data(), zb.data(), sched);
   } else {
     std::vector<float*> b(L, nullptr), za(L, nullptr), zb(L, nullptr);
     for (int l = 1; l < L; ++l) {
@@ -670,7 +709,7 @@ const float* mgVcycle(Multigrid* m, const float* r0, CgState* st, cudaStream_t s
       za[l] = m->z32a[l - 1]->p;
       zb[l] = m->z32b[l - 1]->p;
     }
-    return vcycleT<float>(m, r0, st, s, launches, b.data(), za.data(), zb.data());
+    return vcycleT<float>(m, r0, st, s, launches, b.data(), za.data(), zb.data(), sched);
   }
 }
 
@@ -696,7 +735,7 @@ void mgRunCg(Multigrid* m, const Dim3i& cg, float sx, float sy, float sz, const 
   check(cudaMemsetAsync(m->z0b.p, 0, m->z0b.bytes(), s), "memset");
   for (auto& h : m->z0h)
     if (h.p) check(cudaMemsetAsync(h.p, 0, h.bytes(), s), "memset");
-  const float* z0 = mgVcycle(m, rvec, st, s, launches);  // z0 = V(b), rz = b.z0
+  const float* z0 = mgVcycle(m, rvec, st, s, launches, colZ);  // z0 = V(b), rz = b.z0
   const int kChunk = 4;  // even: every chunk starts on p[0]
   auto body = [&] {
     const float* z = z0;
@@ -711,7 +750,7 @@ void mgRunCg(Multigrid* m, const Dim3i& cg, float sx, float sy, float sz, const 
                            m->partials.p, st, 2, s, colZ),
             "cg update");
       launches += 2;
-      z = mgVcycle(m, rvec, st, s, launches);
+      z = mgVcycle(m, rvec, st, s, launches, colZ);
     }
     m->chunkLaunches = launches - before;
     // the V-cycle always leaves its result in the same level-0 buffer

@@ -497,7 +497,7 @@ struct CgLaunch {
 //                        so that the items about fill one wave of blocks.
 // A block past the last item only joins the reductions.  Null: the dense
 // grid, block (x, y, z) on tile (x, y) and planes [z zPer, (z + 1) zPer).
-__host__ __device__ __forceinline__ int schedItemsOffset(int cols) { return (2 * cols + 1 + 3) & ~3; }
+static_assert(CTX == kCgTileX && CTR == kCgTileY, "the schedule's tile is the CG kernels' tile");
 
 __device__ __forceinline__ bool cgBlockWork(const int* sched, const Dim3i& P, int zPer, int& x0, int& y0, int& z0,
                                             int& z1) {
