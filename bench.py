@@ -72,11 +72,9 @@ def parse():
     ap.add_argument("--pressure-fp64", action="store_true",
                     help="accumulate the pressure in FP64 (divergence follows the CG residual)")
     ap.add_argument("--sort-interval", type=int, default=0,
-                    help="dam-break / moving-boxes: reorder the particles by cell every k steps (0: never); "
-                         "it runs with clamp_mode 0 (every particle pushed out of the solids)")
+                    help="dam-break / moving-boxes: reorder the particles by cell every k steps (0: never)")
     ap.add_argument("--clamp-mode", type=int, default=None, choices=[0, 1],
-                    help="boundary fix of the particles: 1 the first min(N, P) as the reference, 0 all "
-                         "(default 1, or 0 with --sort-interval)")
+                    help="boundary fix of the particles: 1 the first min(N, P) as the reference (default), 0 all")
     ap.add_argument("--ref-cpu", action="store_true",
                     help="reference arm: time the FP64 oracle port on the host cores even where the reference's "
                          "own CUDA build is present")
@@ -633,9 +631,7 @@ def moving_boxes_cpu_leg(pressure_fp64, mg_half=1, res=(128, 64, 128), steps=3):
 
 
 def clamp_mode(args) -> int:
-    if args.clamp_mode is not None:
-        return args.clamp_mode
-    return 0 if args.sort_interval else 1
+    return 1 if args.clamp_mode is None else args.clamp_mode
 
 
 def main():

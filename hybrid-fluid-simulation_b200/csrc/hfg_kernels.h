@@ -276,8 +276,10 @@ struct SortScratch {
 };
 long long sortCountEntries(long long P);
 long long sortScanBlocks(long long entries);
-int sortPassesLaunches(long long nCells);  // kernels one sort launches
-cudaError_t launchSortPermutation(const Geom& g, const float* pos, long long P, const SortScratch& sc,
+int sortPassesLaunches(long long nCells, bool grouped);  // kernels one sort launches
+// split in (0, P): particles [0, split) and [split, P) are sorted each within
+// its own index range (stable); otherwise all together.
+cudaError_t launchSortPermutation(const Geom& g, const float* pos, long long P, long long split, const SortScratch& sc,
                                   const unsigned int** perm, cudaStream_t s);
 // out[width*j + k] = in[width*perm[j] + k], width 1 or 3
 cudaError_t launchGather(const float* in, int width, const unsigned int* perm, long long P, float* out,

@@ -505,12 +505,9 @@ bool GridSolver::advectBegin() {
 void GridSolver::sortParticles() {
   if (P_ <= 0) return;
   // With clamp_mode 1 the boundary fix reaches only the first min(N, P)
-  // particles, as the reference's launch does (EulerParticlesTool.cu:880); a
-  // new order would change which particles those are.
-  if (opt_.clamp_mode == 1 && P_ > N_)
-    throw CudaError("the particle sort needs clamp_mode 0 when there are more particles than cells: with clamp_mode 1 "
-                    "the order decides which particles the boundary fix reaches",
-                    HFG_ERR_INVALID);
+  // particles, as the reference's launch does (EulerParticlesTool.cu:880):
+  // those stay the first ones, each group sorted within its own range.
+  const long long split = (opt_.clamp_mode == 1 && P_ > N_) ? N_ : 0;
   finishMirrorCopy();
   for (int i = 0; i < 2; ++i) {
     sortKey_[i].alloc(P_, stream_);
@@ -521,7 +518,8 @@ void GridSolver::sortParticles() {
   sortSums_.alloc(sortScanBlocks(entries), stream_);
   const SortScratch sc{sortKey_[0].p, sortKey_[1].p, sortVal_[0].p, sortVal_[1].p, sortCounts_.p, sortSums_.p};
   const unsigned int* perm = nullptr;
-  launched(launchSortPermutation(g_, ppos_.p, P_, sc, &perm, stream_), "particle sort", sortPassesLaunches(N_));
+  launched(launchSortPermutation(g_, ppos_.p, P_, split, sc, &perm, stream_), "particle sort",
+           sortPassesLaunches(N_, split > 0));
   sortTmp_.alloc(3 * P_, stream_);
   for (DArray<float>* a : {&ppos_, &pvel_, &pvector_}) {
     if (!a->p || a->n != (size_t)(3 * P_)) continue;

@@ -8,7 +8,10 @@
 // atomics.  A mixing flow spreads that order out.  This is a stable LSD radix
 // sort of the particles by cell (the binning of transPos2Index,
 // EulerMathTool.cu:29-40), 8 bits per pass, deterministic:
-//   keys      key[p] = cell of particle p, value p
+//   keys      key[p] = cell of particle p, value p; with a split, one more
+//             bit above the cell for the particles from the split on, so the
+//             particles below it stay the first ones (the boundary fix of the
+//             reference's launch reaches exactly those, EulerParticlesTool.cu:880)
 //   per pass  hist     per tile of 4096 particles, the count of each digit
 //             scan     exclusive prefix sums of the counts, digit-major, so a
 //                      digit's slots go to the tiles in particle order
@@ -38,9 +41,12 @@ inline int sortGrid(long long n, int threads = kSortThreads, int perSM = 16) {
   return (int)std::max(1LL, std::min(b, cap));
 }
 
-__global__ void kSortKeys(Geom g, const float* __restrict__ pos, long long P, unsigned int* __restrict__ key) {
+// key = cell, with groupBit added for the particles from `split` on, so each
+// group stays together in its own index range
+__global__ void kSortKeys(Geom g, const float* __restrict__ pos, long long P, long long split, unsigned int groupBit,
+                          unsigned int* __restrict__ key) {
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x)
-    key[p] = (unsigned int)binCell(g, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]);
+    key[p] = (unsigned int)binCell(g, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]) | (p >= split ? groupBit : 0u);
 }
 
 // Exclusive scan of a block-sized tile in place; the tile's total goes to
@@ -206,17 +212,24 @@ long long sortTiles(long long P) { return (P + kRadixTile - 1) / kRadixTile; }
 long long sortCountEntries(long long P) { return (long long)kRadixDigits * std::max(1LL, sortTiles(P)); }
 long long sortScanBlocks(long long entries) { return (entries + kScanTile - 1) / kScanTile; }
 
-cudaError_t launchSortPermutation(const Geom& g, const float* pos, long long P, const SortScratch& sc,
+int sortKeyBits(long long nCells, bool grouped) {
+  int bits = 1;
+  while (bits < 32 && ((nCells - 1) >> bits) != 0) ++bits;
+  return bits + (grouped ? 1 : 0);
+}
+
+cudaError_t launchSortPermutation(const Geom& g, const float* pos, long long P, long long split, const SortScratch& sc,
                                   const unsigned int** perm, cudaStream_t s) {
   const long long n = g.r.size();
-  if (n >= (1LL << 32) || P >= (1LL << 32)) return cudaErrorInvalidValue;
+  if (n >= (1LL << 31) || P >= (1LL << 32)) return cudaErrorInvalidValue;
   *perm = sc.valA;
   if (P <= 0) return cudaSuccess;
-  int bits = 1;
-  while (bits < 32 && ((n - 1) >> bits) != 0) ++bits;
+  const bool grouped = split > 0 && split < P;
+  const int bits = sortKeyBits(n, grouped);
+  const unsigned int groupBit = grouped ? 1u << (bits - 1) : 0u;
   const int passes = (bits + kRadixBits - 1) / kRadixBits;
   const long long tiles = sortTiles(P), entries = sortCountEntries(P), nb = sortScanBlocks(entries);
-  kSortKeys<<<sortGrid(P), kSortThreads, 0, s>>>(g, pos, P, sc.keyA);
+  kSortKeys<<<sortGrid(P), kSortThreads, 0, s>>>(g, pos, P, grouped ? split : P, groupBit, sc.keyA);
   unsigned int *kIn = sc.keyA, *kOut = sc.keyB, *vIn = nullptr, *vOut = sc.valA;
   for (int pass = 0; pass < passes; ++pass) {
     const int shift = pass * kRadixBits;
@@ -233,10 +246,8 @@ cudaError_t launchSortPermutation(const Geom& g, const float* pos, long long P, 
   return cudaGetLastError();
 }
 
-int sortPassesLaunches(long long nCells) {
-  int bits = 1;
-  while (bits < 32 && ((nCells - 1) >> bits) != 0) ++bits;
-  return 1 + 5 * ((bits + kRadixBits - 1) / kRadixBits);
+int sortPassesLaunches(long long nCells, bool grouped) {
+  return 1 + 5 * ((sortKeyBits(nCells, grouped) + kRadixBits - 1) / kRadixBits);
 }
 
 cudaError_t launchGather(const float* in, int width, const unsigned int* perm, long long P, float* out,

@@ -104,10 +104,12 @@ typedef struct {
                              scatter keep touching neighbouring entries as the
                              flow mixes.  0 (default): the seeding order is
                              kept, as the reference keeps it.  The order of
-                             hfg_solver_get_particles follows the sort.  With
-                             more particles than cells it needs clamp_mode 0:
-                             under clamp_mode 1 the order decides which
-                             particles the boundary fix reaches. */
+                             hfg_solver_get_particles follows the sort.  Under
+                             clamp_mode 1 with more particles than cells, the
+                             first N particles (those the boundary fix
+                             reaches) and the others are sorted each within
+                             their own index range, so the fix reaches the
+                             same particles. */
 } hfg_options_t;
 
 typedef struct {
@@ -216,9 +218,10 @@ HFG_API int hfg_solver_transfer_vel_to_particles(hfg_solver_t s, const float* po
 HFG_API long long hfg_solver_num_particles(hfg_solver_t s);
 HFG_API int hfg_solver_get_particles(hfg_solver_t s, float* pos, float* vel);
 /* Reorder the particles by cell now: stable (particles of one cell keep
- * their relative order), velocities and carried values follow.  No
- * reference counterpart (the reference keeps the seeding order).  Fails with
- * HFG_ERR_INVALID under clamp_mode 1 with more particles than cells. */
+ * their relative order), velocities and carried values follow; under
+ * clamp_mode 1 with more particles than cells the first N and the rest are
+ * sorted each within its own range (see sort_interval).  No reference
+ * counterpart (the reference keeps the seeding order). */
 HFG_API int hfg_solver_sort_particles(hfg_solver_t s);
 /* Host mirror of the particles (an extension; the reference's viewer calls
  * copyEulerParticlesPos/VelToCPU after every update, MPhysicsAPI.h).  While a

@@ -4,10 +4,9 @@ No reference counterpart: the reference keeps its seeding order.  The sort
 must be a stable permutation by cell (the binning of transPos2Index,
 EulerMathTool.cu:29-40), restated here with numpy's stable argsort, and
 stepping with it must give the results of stepping without it, up to the
-order of the FP32 P2G atomics.  The cases run with clamp_mode 0: under the
-reference's clamp (the boundary fix reaches the first min(N, P) particles
-only) the order decides which particles those are, so there the sort is
-refused when P > N.
+order of the FP32 P2G atomics.  Under the reference's clamp (the boundary
+fix reaches the first min(N, P) particles only) each of the two ranges is
+sorted within itself.
 """
 import numpy as np
 import pytest
@@ -53,14 +52,14 @@ def test_sort_is_the_stable_permutation_by_cell(cuda):
     assert np.array_equal(pos3, pos2)
 
 
-@pytest.mark.parametrize("interval", [1, 2])
-def test_steps_with_sorting_match_steps_without(cuda, interval):
+@pytest.mark.parametrize("interval,clamp", [(1, 0), (2, 0), (2, 1)])
+def test_steps_with_sorting_match_steps_without(cuda, interval, clamp):
     """Same scene stepped with and without the sort: equal substep counts,
     the velocity field within 1e-5 relative L2 and the particle sets within
     1e-5 (the P2G atomics add in another order), markers >= 99.9 % equal."""
     sc = scene()
-    a = scenes.gpu_solver(sc, precond=1, tol_mode=1, tol=1e-6, max_iter=400, advect_scalars=True, clamp_mode=0)
-    b = scenes.gpu_solver(sc, precond=1, tol_mode=1, tol=1e-6, max_iter=400, advect_scalars=True, clamp_mode=0,
+    a = scenes.gpu_solver(sc, precond=1, tol_mode=1, tol=1e-6, max_iter=400, advect_scalars=True, clamp_mode=clamp)
+    b = scenes.gpu_solver(sc, precond=1, tol_mode=1, tol=1e-6, max_iter=400, advect_scalars=True, clamp_mode=clamp,
                           sort_interval=interval)
     for _ in range(5):
         a.update()
@@ -82,14 +81,22 @@ def test_steps_with_sorting_match_steps_without(cuda, interval):
     assert len(np.unique(idx)) == len(idx)
 
 
-def test_sort_refused_under_the_reference_clamp_with_more_particles_than_cells(cuda):
-    import hfgrid
+def test_sort_keeps_the_particles_the_reference_clamp_reaches(cuda):
+    """Under clamp_mode 1 the boundary fix reaches the first min(N, P)
+    particles only (EulerParticlesTool.cu:880).  With P > N the sort orders
+    the first N and the rest each within its own range, so the fix reaches
+    the same particles: the permutation is the stable argsort by cell of each
+    range."""
     sc = scene()
-    g = scenes.gpu_solver(sc, clamp_mode=1)
-    assert g.num_particles > sc.n_cells
-    with pytest.raises(hfgrid.HfgError) as e:
-        g.sort_particles()
-    assert "clamp_mode" in str(e.value)
-    pos0, _ = g.particles()
-    g.update()  # the solver is unchanged and still steps
-    assert g.num_particles == len(pos0)
+    g = scenes.gpu_solver(sc, precond=1, tol_mode=1, tol=1e-6, max_iter=400, clamp_mode=1)
+    n = sc.n_cells
+    assert g.num_particles > n
+    for _ in range(4):
+        g.update()
+    pos, vel = g.particles()
+    keys = cell_keys(pos, sc.res, sc.origin, sc.spacing)
+    perm = np.concatenate([np.argsort(keys[:n], kind="stable"), n + np.argsort(keys[n:], kind="stable")])
+    g.sort_particles()
+    pos2, vel2 = g.particles()
+    assert np.array_equal(pos2, pos[perm])
+    assert np.array_equal(vel2, vel[perm])
