@@ -612,9 +612,9 @@ def moving_boxes_cpu_leg(pressure_fp64, mg_half=1, res=(128, 64, 128), steps=3):
         unknown = np.finfo(np.float32).max
         num = den = 0.0
         for a, b in zip(vg, vo):
-            k = (a != unknown) & (b != unknown)  # faces both know
-            num += float(np.sum((a[k].astype(np.float64) - b[k]) ** 2))
-            den += float(np.sum(np.asarray(b[k], np.float64) ** 2))
+            known = (a != unknown) & (b != unknown)  # faces both know
+            num += float(np.sum((a[known].astype(np.float64) - b[known]) ** 2))
+            den += float(np.sum(np.asarray(b[known], np.float64) ** 2))
         gp, _ = g.particles()
         op, _ = o.particles()
         rows.append({"step": k + 1, "vel_rel_l2": (num / max(den, 1e-300)) ** 0.5,
