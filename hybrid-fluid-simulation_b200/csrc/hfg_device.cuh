@@ -143,6 +143,16 @@ struct FaceQuads {
   const float4* c[3];
 };
 
+// The corner-table entries of the last sample of each component, kept in
+// registers across the RK stages of one substep: a particle moves a fraction
+// of a cell per substep, so the next sample mostly falls in the same stencil
+// cell, and its two 16-byte loads are not repeated (the values are the same
+// ones, the tables do not change during the substeps).
+struct QuadCache {
+  unsigned e[3];
+  float4 lo[3], hi[3];
+};
+
 struct FaceSampler {
   AxisW cc[3], fc[3];
   __device__ __forceinline__ FaceSampler(const Geom& g, float px, float py, float pz) {
@@ -196,6 +206,28 @@ struct FaceSampler {
     const float b0 = fmaf(wy, a01 - a00, a00), b1 = fmaf(wy, a11 - a10, a10);
     return fmaf(wz, b1 - b0, b0);
   }
+  // sampleQuads through the cache: the loads only when the entry differs
+  // from the cached one (or fresh)
+  __device__ __forceinline__ float sampleQuadsCached(const Geom& g, int a, const float4* __restrict__ Q, QuadCache& c,
+                                                     bool fresh) const {
+    const AxisW& X = a == 0 ? fc[0] : cc[0];
+    const AxisW& Y = a == 1 ? fc[1] : cc[1];
+    const AxisW& Z = a == 2 ? fc[2] : cc[2];
+    unsigned lx = (unsigned)(g.r.x + (a == 0) + 1), ly = (unsigned)(g.r.y + (a == 1) + 1);
+    unsigned pl = lx * ly;
+    const unsigned e = ((unsigned)Z.j * ly + (unsigned)Y.j) * lx + (unsigned)X.j;
+    if (fresh || e != c.e[a]) {
+      c.lo[a] = __ldg(Q + e);
+      c.hi[a] = __ldg(Q + e + pl);
+      c.e[a] = e;
+    }
+    const float4 q0 = c.lo[a], q1 = c.hi[a];
+    const float wx = X.w1, wy = Y.w1, wz = Z.w1;
+    const float a00 = fmaf(wx, q0.y - q0.x, q0.x), a01 = fmaf(wx, q0.w - q0.z, q0.z);
+    const float a10 = fmaf(wx, q1.y - q1.x, q1.x), a11 = fmaf(wx, q1.w - q1.z, q1.z);
+    const float b0 = fmaf(wy, a01 - a00, a00), b1 = fmaf(wy, a11 - a10, a10);
+    return fmaf(wz, b1 - b0, b0);
+  }
   // sample of the difference field f - h at the same point
   __device__ __forceinline__ float sampleDiff(const Geom& g, int a, const float* __restrict__ f,
                                               const float* __restrict__ h) const {
@@ -220,6 +252,12 @@ __device__ __forceinline__ void sampleFaceQuads(const FaceQuads& v, const Geom& 
   FaceSampler s(g, px, py, pz);
 #pragma unroll
   for (int a = 0; a < 3; ++a) out[a] = s.sampleQuads(g, a, v.c[a]);
+}
+__device__ __forceinline__ void sampleFaceQuadsCached(const FaceQuads& v, const Geom& g, float px, float py, float pz,
+                                                      float out[3], QuadCache& c, bool fresh) {
+  FaceSampler s(g, px, py, pz);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) out[a] = s.sampleQuadsCached(g, a, v.c[a], c, fresh);
 }
 
 // Cubic samplers (MPhysics/EulerMathTool.cu:134-240, FieldMathTool.cu:106-173).

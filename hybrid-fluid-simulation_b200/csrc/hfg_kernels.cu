@@ -1164,6 +1164,8 @@ __device__ __forceinline__ float substepParticle(const Geom& g, const FaceQuads&
   float q[3] = {pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]};
   float w0[3] = {v0[3 * p], v0[3 * p + 1], v0[3 * p + 2]};
   float m = 0.f;
+  QuadCache qc;
+  bool fresh = true;  // no entry cached yet
   if (acc == 0) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) q[a] = fmaf(ds, w0[a], q[a]);
@@ -1171,7 +1173,8 @@ __device__ __forceinline__ float substepParticle(const Geom& g, const FaceQuads&
     float mid[3], w1[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) mid[a] = fmaf(half, w0[a], q[a]);
-    sampleFaceQuads(vel, g, mid[0], mid[1], mid[2], w1);
+    sampleFaceQuadsCached(vel, g, mid[0], mid[1], mid[2], w1, qc, true);
+    fresh = false;
 #pragma unroll
     for (int a = 0; a < 3; ++a) q[a] = fmaf(ds, w1[a], q[a]);
   } else {
@@ -1183,13 +1186,14 @@ __device__ __forceinline__ float substepParticle(const Geom& g, const FaceQuads&
       mid[a] = fmaf(half, w0[a], q[a]);
       acc3[a] = fmaf(a29, w0[a], q[a]);
     }
-    sampleFaceQuads(vel, g, mid[0], mid[1], mid[2], w);
+    sampleFaceQuadsCached(vel, g, mid[0], mid[1], mid[2], w, qc, true);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       tf[a] = fmaf(tq, w[a], q[a]);
       acc3[a] = fmaf(a39, w[a], acc3[a]);
     }
-    sampleFaceQuads(vel, g, tf[0], tf[1], tf[2], w);
+    sampleFaceQuadsCached(vel, g, tf[0], tf[1], tf[2], w, qc, false);
+    fresh = false;
 #pragma unroll
     for (int a = 0; a < 3; ++a) q[a] = fmaf(a49, w[a], acc3[a]);
   }
@@ -1202,7 +1206,7 @@ __device__ __forceinline__ float substepParticle(const Geom& g, const FaceQuads&
     }
   } else {
     float v[3];
-    sampleFaceQuads(vel, g, q[0], q[1], q[2], v);
+    sampleFaceQuadsCached(vel, g, q[0], q[1], q[2], v, qc, fresh);
     v0[3 * p] = v[0]; v0[3 * p + 1] = v[1]; v0[3 * p + 2] = v[2];
     m = fmaxf(fabsf(v[0]), fmaxf(fabsf(v[1]), fabsf(v[2])));
   }
