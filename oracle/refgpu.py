@@ -49,6 +49,8 @@ def lib(fp64: bool = False):
         for name in ("rg_add_solid", "rg_set_fluid_domain", "rg_markers", "rg_pressure"):
             getattr(L, name).restype = C.c_int
             getattr(L, name).argtypes = [C.c_void_p, PR]
+        L.rg_add_moving_solid.restype = C.c_int
+        L.rg_add_moving_solid.argtypes = [C.c_void_p, PR, PF]
         L.rg_fluid_domain_bbox.restype = C.c_int
         L.rg_fluid_domain_bbox.argtypes = [C.c_void_p, PF, PF]
         L.rg_update_boundaries.restype = C.c_int
@@ -117,8 +119,13 @@ class RefSolver:
         assert a.shape == self.res[::-1]
         return a
 
-    def add_solid_boundary(self, sdf):
-        self._check(self._L.rg_add_solid(self._h, self._p(self._cell(sdf))))
+    def add_solid_boundary(self, sdf, vel=None):
+        """addSolidBoundary(sdf); with a nonzero velocity, the boundary moves
+        at it (CBoundarys::addBoundary(sdf, vel))."""
+        if vel is None or not any(vel):
+            self._check(self._L.rg_add_solid(self._h, self._p(self._cell(sdf))))
+        else:
+            self._check(self._L.rg_add_moving_solid(self._h, self._p(self._cell(sdf)), _f3(vel)))
 
     def set_fluid_domain_field(self, dom):
         self._check(self._L.rg_set_fluid_domain(self._h, self._p(self._cell(dom))))

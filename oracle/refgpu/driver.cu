@@ -131,6 +131,18 @@ int rg_add_solid(void* h, const Real* sdf) {
   });
 }
 
+// A solid moving at a constant velocity: CBoundarys::addBoundary(sdf, vel)
+// (Boundary.cpp:92-113; each update moves it by -dt vel and resamples its
+// SDF, Boundary.cpp:115-136).  GridFluidSolver::addSolidBoundary passes no
+// velocity, so the driver reaches the boundaries directly.
+int rg_add_moving_solid(void* h, const Real* sdf, const float vel[3]) {
+  return guarded([&] {
+    RefScene* s = scene(h);
+    CCellCenteredScalarField f(s->res, s->origin, s->spacing, const_cast<Real*>(sdf));
+    s->solver->m_Boundarys.addBoundary(f, Vector3(vel[0], vel[1], vel[2]));
+  });
+}
+
 int rg_set_fluid_domain(void* h, const Real* dom) {
   return guarded([&] {
     RefScene* s = scene(h);
