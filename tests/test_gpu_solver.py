@@ -363,6 +363,24 @@ def test_moving_boxes_c3_layout_downscaled_vs_fp64(cuda):
         print("%4d  %18.3e  %13.5f  %8.2e  %8d  %16.3e" % r)
 
 
+@pytest.mark.parametrize("precond", [hfgrid.PRECOND_IDENTITY, hfgrid.PRECOND_JACOBI, hfgrid.PRECOND_MG])
+def test_step_with_no_fluid(cuda, precond):
+    """A fluid domain with no cell in it (semi-Lagrangian advection, so no
+    particles either), on a grid where the multigrid level-0 sweeps march:
+    the CG schedule has no work item, the solve stops at once, and the
+    velocity field stays finite."""
+    sc = scenes.Scene(res=(72, 44, 78), fluid_max=(0.0, 0.0, 0.0), seed=1)
+    g = scenes.gpu_solver(sc, precond=precond, tol_mode=1, tol=1e-6, max_iter=200,
+                          kind=hfgrid.ADV_SEMI_LAGRANGIAN)
+    for _ in range(2):
+        g.update()
+    st = g.stats()
+    assert st["cg_iterations"] == 0
+    assert (g.markers() != 1).all()
+    for v in g.velocity_field():
+        assert np.isfinite(v[v != U]).all()
+
+
 def test_semi_lagrangian_solver_catmull_rom(cuda):
     """The solver in semi-Lagrangian mode with the Catmull-Rom sampler
     (setSamplingAlg) against the FP64 oracle with the same sampler."""
