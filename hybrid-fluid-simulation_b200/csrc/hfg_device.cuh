@@ -52,8 +52,19 @@ __host__ __device__ inline long long linc(int x, int y, int z, const Dim3i& r) {
   return ((long long)z * r.y + y) * r.x + x;
 }
 
-// floorCUDA (MPhysics/EulerMathTool.cu:93-103); floorCUDA(-1.0f) == -2.
-__host__ __device__ inline int floorRef(float v) { return v >= 0.f ? (int)v : (int)v - 1; }
+// floorCUDA (MPhysics/EulerMathTool.cu:93-103); floorCUDA(-1.0f) == -2.  The
+// argument is clamped to +-2^30 first: a point far outside the grid (a
+// back-trace through UNKNOWN = FLT_MAX velocities lands ~1e36 away) would
+// otherwise convert to INT_MIN and the "- 1", or the caller's "+ 1" of a
+// stencil offset, would overflow; signed overflow is undefined, and the
+// compiler may then fold one comparison of a clamp and not the other and
+// leave an index outside the grid.  Every grid index lies far inside
+// +-2^30, so the clamped result selects the same cells; a NaN (which fmaxf
+// drops) still yields NaN weights.
+__host__ __device__ inline int floorRef(float v) {
+  v = fminf(fmaxf(v, -1073741824.f), 1073741824.f);
+  return v >= 0.f ? (int)v : (int)v - 1;
+}
 
 // Exact-rounding helpers: the listed expressions must round like the
 // reference's separate float operations (no contraction into FMA).
@@ -125,9 +136,10 @@ struct AxisW {
 __device__ __forceinline__ void axisWeights(float t, int n, AxisW& a) {
   float f = floorf(t);
   a.w1 = t - f;
-  int i = (int)f;
+  int i = (int)f;  // saturates far outside the grid
   a.i0 = clampi(i, n);
-  a.i1 = clampi(i + 1, n);
+  // clamp(i + 1) without forming i + 1 first (it overflows at i = INT_MAX)
+  a.i1 = min(max(i, -1), n - 2) + 1;
   a.j = min(max(i, -1), n - 1) + 1;
 }
 
