@@ -149,7 +149,7 @@ cudaError_t makeHaloMap(const Dim3i& cg, const float* v, CUtensorMap* m);
 cudaError_t launchCgDirection(const Dim3i& cg, float sx, float sy, float sz, const CUtensorMap& mZ,
                               const CUtensorMap& mPo, const CUtensorMap& mCode, const CgCode* code, const float* zr,
                               const float* pOld, float* pNew, double* partials, CgState* st, int precond,
-                              cudaStream_t s, const int* colZ = nullptr);
+                              cudaStream_t s, const int* colZ = nullptr, bool xDouble = false);
 cudaError_t launchCgUpdate(const Dim3i& cg, float sx, float sy, float sz, const CUtensorMap& mP, const CUtensorMap& mR,
                            const CUtensorMap& mX, const CUtensorMap& mCode, const float* p, void* x, bool xDouble,
                            float* r, double* partials, CgState* st, int precond, cudaStream_t s,
@@ -168,13 +168,16 @@ int loadTuning(const char* path);  // entries read, -1 if the file cannot be ope
 // `precond`.  sched holds cgScheduleInts(cg) ints.
 int cgColumns(const Dim3i& cg);
 int cgScheduleInts(const Dim3i& cg);
-int cgScheduleTarget(int precond);  // work items of one wave (the schedule's grid: this + cgColumns)
+// work items of one wave of the CG kernels of this preconditioner and
+// iterate type (the schedule's grid: this + cgColumns)
+int cgScheduleTarget(int precond, bool xDouble);
 // Layout of a schedule: ints [0, cols) and [cols, 2 cols) the lowest and
 // highest fluid plane of each tile column (kCgTileX x kCgTileY cells), [2 cols]
 // the item count, from schedItemsOffset(cols) the items (column, z0, z1, 0).
 constexpr int kCgTileX = 32, kCgTileY = 16;
 __host__ __device__ inline int schedItemsOffset(int cols) { return (2 * cols + 1 + 3) & ~3; }
-cudaError_t launchCgSchedule(const Dim3i& cg, const CgCode* code, int* sched, int precond, cudaStream_t s);
+cudaError_t launchCgSchedule(const Dim3i& cg, const CgCode* code, int* sched, int precond, bool xDouble,
+                             cudaStream_t s);
 // Divergence residual of the projected velocity over the fluid cells:
 // *sumOut = sum b^2 (FP64), ticketAndMax[1] = bits of max |b|.  `scratch`
 // holds 2 * divergenceBlocks() doubles.

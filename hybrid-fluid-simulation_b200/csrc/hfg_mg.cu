@@ -233,11 +233,13 @@ __device__ __forceinline__ void mgBlockWork(const int* sched, const Dim3i& r, in
   }
   const int tilesX = (r.x + kCgTileX - 1) / kCgTileX, cols = tilesX * ((r.y + kCgTileY - 1) / kCgTileY);
   const int item = blockIdx.x >> 1;
-  if (item >= __ldg(sched + 2 * cols)) {
-    x0 = y0 = z0 = z1 = 0;
-    return;
-  }
+  x0 = y0 = z0 = z1 = 0;
+  const int n = __ldg(sched + 2 * cols);
+  if (item >= n || 2 * n > (int)gridDim.x) return;
   const int4 w = __ldg(reinterpret_cast<const int4*>(sched + schedItemsOffset(cols)) + item);
+  // an item that is not a run of this grid is not swept (the CG kernels,
+  // which read the same schedule, report it)
+  if (w.x < 0 || w.x >= cols || w.y < 0 || w.y >= w.z || w.z > r.z) return;
   x0 = (w.x % tilesX) * kCgTileX;
   y0 = (w.x / tilesX) * kCgTileY + (blockIdx.x & 1) * MY;
   z0 = w.y;
@@ -422,6 +424,10 @@ __global__ void kCoarseSolve(Lvl L, const TB* __restrict__ b, TZ* __restrict__ z
 }
 }  // namespace
 
+// Work items a multigrid solve's schedule can hold: the larger of the two
+// iterate types' targets (the sweeps do not know which one the CG uses).
+int mgScheduleTarget() { return std::max(cgScheduleTarget(2, false), cgScheduleTarget(2, true)); }
+
 struct Multigrid {
   Dim3i r0;                          // level 0 = the pitched grid of the pressure system
   Dim3i rLogical;                    // the solver's grid (level-0 markers are unpitched)
@@ -484,7 +490,7 @@ Multigrid* mgCreate(const Dim3i& r, int levels, int smooth, int halfMode, cudaSt
   m->p[1].alloc(N, s);
   const dim3 mg = marchGrid(r).grid;
   m->partials.alloc(std::max({cgPartialsNeeded(r), 2 * (int)(gridOf(r).x * gridOf(r).y * gridOf(r).z),
-                              2 * (int)(mg.x * mg.y * mg.z), 2 * 2 * (cgScheduleTarget(2) + cgColumns(r))}),
+                              2 * (int)(mg.x * mg.y * mg.z), 2 * 2 * (mgScheduleTarget() + cgColumns(r))}),
                     s);
   check(makeHaloMap(r, m->z0a.p, &m->zH[0]), "multigrid tensor map");
   check(makeHaloMap(r, m->z0b.p, &m->zH[1]), "multigrid tensor map");
@@ -559,7 +565,7 @@ const float* vcycleT(Multigrid* m, const float* r0, CgState* st, cudaStream_t s,
   const SweepGrid mg0 = marchGrid(lv[0].r);
   const bool marching = marchLevel0(lv[0].r);
   // with the solve's CG schedule: two blocks per work item, fluid runs only
-  const dim3 schedGrid(2 * (cgScheduleTarget(2) + cgColumns(lv[0].r)), 1, 1);
+  const dim3 schedGrid(2 * (mgScheduleTarget() + cgColumns(lv[0].r)), 1, 1);
   auto march = [&](auto kernel, auto... args) {
     run(kernel, sched ? schedGrid : mg0.grid, dim3(MX, MY), args..., mg0.zPer, sched);
   };
@@ -744,7 +750,7 @@ void mgRunCg(Multigrid* m, const Dim3i& cg, float sx, float sy, float sz, const 
       const int po = it & 1, pn = (it + 1) & 1;
       const int zi = z == m->z0a.p ? 0 : 1;
       check(launchCgDirection(cg, sx, sy, sz, m->zH[zi], m->pH[po], maps.codeH, code, z, m->p[po].p, m->p[pn].p,
-                              m->partials.p, st, 2, s, colZ),
+                              m->partials.p, st, 2, s, colZ, xDouble),
             "cg direction");
       check(launchCgUpdate(cg, sx, sy, sz, m->pH[pn], maps.rI, maps.xI, maps.codeI, m->p[pn].p, x, xDouble, rvec,
                            m->partials.p, st, 2, s, colZ),

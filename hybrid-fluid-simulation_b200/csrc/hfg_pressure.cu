@@ -499,8 +499,11 @@ struct CgLaunch {
 // grid, block (x, y, z) on tile (x, y) and planes [z zPer, (z + 1) zPer).
 static_assert(CTX == kCgTileX && CTR == kCgTileY, "the schedule's tile is the CG kernels' tile");
 
+// A work item that is not a run of planes of a column of this grid (or a
+// count beyond the grid) is not used: the block stays idle and the solve
+// reports error 4.
 __device__ __forceinline__ bool cgBlockWork(const int* sched, const Dim3i& P, int zPer, int& x0, int& y0, int& z0,
-                                            int& z1) {
+                                            int& z1, CgState* st) {
   if (!sched) {
     x0 = blockIdx.x * CTX;
     y0 = blockIdx.y * CTR;
@@ -508,13 +511,19 @@ __device__ __forceinline__ bool cgBlockWork(const int* sched, const Dim3i& P, in
     z1 = min(z0 + zPer, P.z);
     return true;
   }
+  x0 = y0 = z0 = z1 = 0;
   const int tilesX = (P.x + CTX - 1) / CTX, cols = tilesX * ((P.y + CTR - 1) / CTR);
   const int n = __ldg(sched + 2 * cols);
-  if ((int)blockIdx.x >= n) {
-    x0 = y0 = z0 = z1 = 0;
+  if (n < 0 || n > (int)gridDim.x) {
+    if (threadIdx.x == 0 && threadIdx.y == 0) cgFail(st, 4);
     return false;
   }
+  if ((int)blockIdx.x >= n) return false;
   const int4 w = __ldg(reinterpret_cast<const int4*>(sched + schedItemsOffset(cols)) + blockIdx.x);
+  if (w.x < 0 || w.x >= cols || w.y < 0 || w.y >= w.z || w.z > P.z) {
+    if (threadIdx.x == 0 && threadIdx.y == 0) cgFail(st, 4);
+    return false;
+  }
   x0 = (w.x % tilesX) * CTX;
   y0 = (w.x / tilesX) * CTR;
   z0 = w.y;
@@ -543,7 +552,7 @@ int residentBlocks(const void* kernel) {
 // preconditioner (the fewest resident blocks of the direction and both update
 // kernels, at most kSchedPerSM per SM).
 constexpr int kSchedPerSM = 8;
-int cgScheduleTarget(int precond);
+int cgScheduleTarget(int precond, bool xDouble);
 
 // ---------------------------------------------------------------------------
 // Launch shapes picked by measurement.  autotuneCg (driven by the solver)
@@ -608,12 +617,13 @@ namespace {
 // family: 0 for kCgDirection, 1 for kCgUpdate (the key of the tuning table).
 // With a schedule the grid is one block per possible work item.
 template <class K>
-CgLaunch cgLaunch(const Dim3i& cg, K kernel, int family, const int* sched = nullptr, int precond = 1) {
+CgLaunch cgLaunch(const Dim3i& cg, K kernel, int family, const int* sched = nullptr, int precond = 1,
+                  bool xDouble = false) {
   CgLaunch L;
   L.block = dim3(CTX, CTY, 1);
   if (sched) {
     L.zPer = 0;
-    L.grid = dim3(cgScheduleTarget(precond) + cgColumns(cg), 1, 1);
+    L.grid = dim3(cgScheduleTarget(precond, xDouble) + cgColumns(cg), 1, 1);
     return L;
   }
   int bx = (cg.x + CTX - 1) / CTX, by = (cg.y + CTR - 1) / CTR;
@@ -684,7 +694,7 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
   allowNextGrid();
   // a block with no work item (sched) writes nothing and adds zero to the
   // reduction; the schedule was written before the kernels before this one
-  const bool active = cgBlockWork(colZ, P, zPer, x0, y0, z0, z1);
+  const bool active = cgBlockWork(colZ, P, zPer, x0, y0, z0, z1, st);
   const int nPlanes = active ? z1 - z0 : 0, nLoad = nPlanes + 1;  // plane z1 is the last "above"
   if (tid == 0) {
     int n = active ? min(kDirStages, nLoad) : 0;
@@ -819,7 +829,7 @@ __global__ void __launch_bounds__(CTX* CTY, 4)
   waitPrevGrid();
   if (st->done) return;  // the same value in every thread
   allowNextGrid();
-  const bool active = cgBlockWork(colZ, P, zPer, x0, y0, z0, z1);  // as in kCgDirection
+  const bool active = cgBlockWork(colZ, P, zPer, x0, y0, z0, z1, st);  // as in kCgDirection
   const int nPlanes = active ? z1 - z0 : 0, nLoad = nPlanes + 1;
   if (tid == 0) {
     int n = active ? min(kUpdStages, nLoad) : 0;
@@ -959,21 +969,18 @@ void cgWarmLaunchCache() {
   residentBlocks((const void*)kCgUpdate<2, double>);
 }
 
-int cgScheduleTarget(int precond) {
+int cgScheduleTarget(int precond, bool xDouble) {
   int per = kSchedPerSM;
   auto take = [&](const void* k) { per = std::min(per, residentBlocks(k)); };
   if (precond == 1) {
     take((const void*)kCgDirection<1>);
-    take((const void*)kCgUpdate<1, float>);
-    take((const void*)kCgUpdate<1, double>);
+    take(xDouble ? (const void*)kCgUpdate<1, double> : (const void*)kCgUpdate<1, float>);
   } else if (precond == 2) {
     take((const void*)kCgDirection<2>);
-    take((const void*)kCgUpdate<2, float>);
-    take((const void*)kCgUpdate<2, double>);
+    take(xDouble ? (const void*)kCgUpdate<2, double> : (const void*)kCgUpdate<2, float>);
   } else {
     take((const void*)kCgDirection<0>);
-    take((const void*)kCgUpdate<0, float>);
-    take((const void*)kCgUpdate<0, double>);
+    take(xDouble ? (const void*)kCgUpdate<0, double> : (const void*)kCgUpdate<0, float>);
   }
   return numSMs() * std::max(1, per);
 }
@@ -997,24 +1004,24 @@ int cgPartialsNeeded(const Dim3i& r) {
 cudaError_t launchCgDirection(const Dim3i& cg, float sx, float sy, float sz, const CUtensorMap& mZ,
                               const CUtensorMap& mPo, const CUtensorMap& mCode, const CgCode* code, const float* zr,
                               const float* pOld, float* pNew, double* partials, CgState* st, int precond,
-                              cudaStream_t s, const int* colZ) {
+                              cudaStream_t s, const int* colZ, bool xDouble) {
   switch (precond) {
     case 1: {
-      CgLaunch L = cgLaunch(cg, kCgDirection<1>, 0, colZ, 1);
+      CgLaunch L = cgLaunch(cg, kCgDirection<1>, 0, colZ, 1, xDouble);
       cudaError_t e = launchPdl(kCgDirection<1>, L.grid, L.block, s, mZ, mPo, mCode, cg, sx, sy, sz, code, zr, pOld,
                                 pNew, partials, st, L.zPer, colZ);
       if (e != cudaSuccess) return e;
       break;
     }
     case 2: {
-      CgLaunch L = cgLaunch(cg, kCgDirection<2>, 0, colZ, 2);
+      CgLaunch L = cgLaunch(cg, kCgDirection<2>, 0, colZ, 2, xDouble);
       cudaError_t e = launchPdl(kCgDirection<2>, L.grid, L.block, s, mZ, mPo, mCode, cg, sx, sy, sz, code, zr, pOld,
                                 pNew, partials, st, L.zPer, colZ);
       if (e != cudaSuccess) return e;
       break;
     }
     default: {
-      CgLaunch L = cgLaunch(cg, kCgDirection<0>, 0, colZ, 0);
+      CgLaunch L = cgLaunch(cg, kCgDirection<0>, 0, colZ, 0, xDouble);
       cudaError_t e = launchPdl(kCgDirection<0>, L.grid, L.block, s, mZ, mPo, mCode, cg, sx, sy, sz, code, zr, pOld,
                                 pNew, partials, st, L.zPer, colZ);
       if (e != cudaSuccess) return e;
@@ -1028,7 +1035,7 @@ cudaError_t launchCgUpdate(const Dim3i& cg, float sx, float sy, float sz, const 
                            float* r, double* partials, CgState* st, int precond, cudaStream_t s, const int* colZ) {
 #define HFG_CG_UPDATE(PCV, TXV)                                                                                   \
   {                                                                                                               \
-    CgLaunch L = cgLaunch(cg, kCgUpdate<PCV, TXV>, 1, colZ, PCV);                                                             \
+    CgLaunch L = cgLaunch(cg, kCgUpdate<PCV, TXV>, 1, colZ, PCV, xDouble);                                                             \
     cudaError_t e = launchPdl(kCgUpdate<PCV, TXV>, L.grid, L.block, s, mP, mR, mX, mCode, cg, sx, sy, sz, p,      \
                               (TXV*)x, r, partials, st, L.zPer, colZ);                                        \
     if (e != cudaSuccess) return e;                                                                             \
@@ -1081,7 +1088,7 @@ int cgColumns(const Dim3i& cg) { return ((cg.x + CTX - 1) / CTX) * ((cg.y + CTR 
 // columns, so the items are at most target + (active columns); they are
 // written column by column, bottom to top.  One block.
 constexpr int kListThreads = 1024;
-__global__ void __launch_bounds__(kListThreads) kCgWorkList(int cols, int target, int zMin, int* sched) {
+__global__ void __launch_bounds__(kListThreads) kCgWorkList(int cols, int target, int zMin, int capacity, int* sched) {
   const int* lo = sched;
   const int* hi = sched + cols;
   int4* items = reinterpret_cast<int4*>(sched + schedItemsOffset(cols));
@@ -1129,16 +1136,19 @@ __global__ void __launch_bounds__(kListThreads) kCgWorkList(int cols, int target
     int k = carry + warpTot[w] + inc - n;
     for (int i = 0; i < n; ++i, ++k) {
       const int z0 = l + i * zLen;
-      items[k] = make_int4(c, z0, min(z0 + zLen, hi[c] + 1), 0);
+      if (k < capacity) items[k] = make_int4(c, z0, min(z0 + zLen, hi[c] + 1), 0);
     }
     __syncthreads();
     if (t == kListThreads - 1) carry = k;
     __syncthreads();
   }
+  // more items than the buffer holds cannot happen (at most target + cols);
+  // if it did, a count past the grid makes the CG kernels report error 4
   if (t == 0) sched[2 * cols] = carry;
 }
 
-cudaError_t launchCgSchedule(const Dim3i& cg, const CgCode* code, int* sched, int precond, cudaStream_t s) {
+cudaError_t launchCgSchedule(const Dim3i& cg, const CgCode* code, int* sched, int precond, bool xDouble,
+                             cudaStream_t s) {
   const int cols = cgColumns(cg);
   cudaError_t e = cudaMemsetAsync(sched, 0x7f, sizeof(int) * cols, s);  // lo: 0x7f7f7f7f, above any plane
   if (e == cudaSuccess) e = cudaMemsetAsync(sched + cols, 0xff, sizeof(int) * cols, s);  // hi: -1
@@ -1149,7 +1159,8 @@ cudaError_t launchCgSchedule(const Dim3i& cg, const CgCode* code, int* sched, in
   // the shortest chunk: the tuned z-chunk length of the direction kernel, else 3 planes
   const int tuned = tunedZPer(0, cg);
   const int zMin = tuned > 0 ? tuned : std::min(3, cg.z);
-  kCgWorkList<<<1, kListThreads, 0, s>>>(cols, cgScheduleTarget(precond), zMin, sched);
+  kCgWorkList<<<1, kListThreads, 0, s>>>(cols, cgScheduleTarget(precond, xDouble), zMin,
+                                         (cgScheduleInts(cg) - schedItemsOffset(cols)) / 4, sched);
   return cudaGetLastError();
 }
 

@@ -584,7 +584,7 @@ void GridSolver::advectEnd() {
 void GridSolver::cgIteration(int it, float sx, float sy, float sz, int pc) {
   const int po = it & 1, pn = (it + 1) & 1;
   launched(launchCgDirection(cg_, sx, sy, sz, maps_.rH, maps_.pH[po], maps_.codeH, cgc_.p, cgr_.p, cgp_[po].p,
-                             cgp_[pn].p, partials_.p, cgState_.p, pc, stream_, colZ_.p),
+                             cgp_[pn].p, partials_.p, cgState_.p, pc, stream_, colZ_.p, xDouble()),
            "cg direction");
   launched(launchCgUpdate(cg_, sx, sy, sz, maps_.pH[pn], maps_.rI, maps_.xI, maps_.codeI, cgp_[pn].p, xPtr(), xDouble(),
                           cgr_.p,
@@ -652,6 +652,7 @@ void GridSolver::runCg() {
     }
     cgChunks_ = (cgHost_->iter + kCgChunk - 1) / kCgChunk;
   }
+  if (cgHost_->error == 4) throw CudaError("pressure CG: a work item of the schedule is invalid", HFG_ERR_STATE);
   if (cgHost_->error) throw CudaError("pressure CG: a stage load did not complete in time", HFG_ERR_TIMEOUT);
 }
 
@@ -668,7 +669,7 @@ void GridSolver::computePressure() {
   launched(launchStencilCode(g_.r, cg_.x, markers_.p, code_.p, stream_, cgc_.p), "stencil code");
   const int schedPc =
       opt_.precond == HFG_PRECOND_MG ? 2 : (opt_.precond == HFG_PRECOND_JACOBI ? 1 : 0);
-  launched(launchCgSchedule(cg_, cgc_.p, colZ_.p, schedPc, stream_), "cg schedule", 2);
+  launched(launchCgSchedule(cg_, cgc_.p, colZ_.p, schedPc, xDouble(), stream_), "cg schedule", 2);
   stageEnd(3);
   stageBegin(4);
   CgState init{};
@@ -832,7 +833,7 @@ void GridSolver::autotuneCg(float sx, float sy, float sz, int pc) {
       setTunedCgZPer(0, cg_, z);
       setTunedCgZPer(1, cg_, z);
       // the schedule's shortest chunk is the tuned length
-      launched(launchCgSchedule(cg_, cgc_.p, colZ_.p, pc, stream_), "cg schedule", 2);
+      launched(launchCgSchedule(cg_, cgc_.p, colZ_.p, pc, xDouble(), stream_), "cg schedule", 2);
       *cgHost_ = st;
       check(cudaMemcpyAsync(cgState_.p, cgHost_, sizeof(CgState), cudaMemcpyHostToDevice, stream_), "cg state");
       cgIteration(0, sx, sy, sz, pc);  // warm-up
@@ -840,7 +841,7 @@ void GridSolver::autotuneCg(float sx, float sy, float sz, int pc) {
         const int po = it & 1, pn = po ^ 1;
         check(cudaEventRecord(e[3 * it], stream_), "event");
         launched(launchCgDirection(cg_, sx, sy, sz, maps_.rH, maps_.pH[po], maps_.codeH, cgc_.p, cgr_.p,
-                                   cgp_[po].p, cgp_[pn].p, partials_.p, cgState_.p, pc, stream_, colZ_.p),
+                                   cgp_[po].p, cgp_[pn].p, partials_.p, cgState_.p, pc, stream_, colZ_.p, xDouble()),
                  "cg direction");
         check(cudaEventRecord(e[3 * it + 1], stream_), "event");
         launched(launchCgUpdate(cg_, sx, sy, sz, maps_.pH[pn], maps_.rI, maps_.xI, maps_.codeI, cgp_[pn].p, xPtr(),
@@ -868,7 +869,7 @@ void GridSolver::autotuneCg(float sx, float sy, float sz, int pc) {
   for (auto& x : e) cudaEventDestroy(x);
   setTunedCgZPer(0, cg_, pick[0]);
   setTunedCgZPer(1, cg_, pick[1]);
-  launched(launchCgSchedule(cg_, cgc_.p, colZ_.p, pc, stream_), "cg schedule", 2);
+  launched(launchCgSchedule(cg_, cgc_.p, colZ_.p, pc, xDouble(), stream_), "cg schedule", 2);
   dropGraphs();
 }
 
@@ -891,6 +892,7 @@ float GridSolver::timeCg(int iters) {
   float ms = 0.f;
   check(cudaEventElapsedTime(&ms, ev_[14], ev_[15]), "elapsed");
   check(cudaMemcpy(cgHost_, cgState_.p, sizeof(CgState), cudaMemcpyDeviceToHost), "read cg state");
+  if (cgHost_->error == 4) throw CudaError("pressure CG: a work item of the schedule is invalid", HFG_ERR_STATE);
   if (cgHost_->error) throw CudaError("pressure CG: a stage load did not complete in time", HFG_ERR_TIMEOUT);
   return ms / iters;
 }
