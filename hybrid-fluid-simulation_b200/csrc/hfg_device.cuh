@@ -144,13 +144,16 @@ __device__ __forceinline__ void axisWeights(float t, int n, AxisW& a) {
 }
 
 // Corner table of a face grid of nx x ny x nz values: (nx + 1) x (ny + 1) x
-// (nz + 2) float4, entry (L, jy, jx) = (f[z][y0][x0], f[z][y0][x1],
-// f[z][y1][x0], f[z][y1][x1]) with z = clamp(L - 1), x0 = clamp(jx - 1),
-// x1 = clamp(jx), y0 = clamp(jy - 1), y1 = clamp(jy).  Entry (AxisW::j of y,
-// AxisW::j of x) of a sample holds the four corners of one z layer of its
-// trilinear stencil, so one 16-byte load serves four corners; layers
-// AxisW::j and AxisW::j + 1 of z are the stencil's clamp(i) and clamp(i + 1),
-// because the padding layers 0 and nz + 1 repeat the end layers.
+// (nz + 2) float4, entry (L, jy, jx) = (f[z][y0][x0], f[z][y0][x1] -
+// f[z][y0][x0], f[z][y1][x0], f[z][y1][x1] - f[z][y1][x0]) with
+// z = clamp(L - 1), x0 = clamp(jx - 1), x1 = clamp(jx), y0 = clamp(jy - 1),
+// y1 = clamp(jy).  Entry (AxisW::j of y, AxisW::j of x) of a sample holds the
+// four corners of one z layer of its trilinear stencil, so one 16-byte load
+// serves four corners; layers AxisW::j and AxisW::j + 1 of z are the
+// stencil's clamp(i) and clamp(i + 1), because the padding layers 0 and
+// nz + 1 repeat the end layers.  The two x differences are the FP32
+// subtractions the x lerps of every sample would otherwise repeat: stored
+// once, they give the same values.
 struct FaceQuads {
   const float4* c[3];
 };
@@ -213,8 +216,8 @@ struct FaceSampler {
     const float4* q = Q + ((unsigned)Z.j * ly + (unsigned)Y.j) * lx + (unsigned)X.j;
     const float4 q0 = __ldg(q), q1 = __ldg(q + pl);
     const float wx = X.w1, wy = Y.w1, wz = Z.w1;
-    const float a00 = fmaf(wx, q0.y - q0.x, q0.x), a01 = fmaf(wx, q0.w - q0.z, q0.z);
-    const float a10 = fmaf(wx, q1.y - q1.x, q1.x), a11 = fmaf(wx, q1.w - q1.z, q1.z);
+    const float a00 = fmaf(wx, q0.y, q0.x), a01 = fmaf(wx, q0.w, q0.z);  // .y, .w: the x differences
+    const float a10 = fmaf(wx, q1.y, q1.x), a11 = fmaf(wx, q1.w, q1.z);
     const float b0 = fmaf(wy, a01 - a00, a00), b1 = fmaf(wy, a11 - a10, a10);
     return fmaf(wz, b1 - b0, b0);
   }
@@ -235,8 +238,8 @@ struct FaceSampler {
     }
     const float4 q0 = c.lo[a], q1 = c.hi[a];
     const float wx = X.w1, wy = Y.w1, wz = Z.w1;
-    const float a00 = fmaf(wx, q0.y - q0.x, q0.x), a01 = fmaf(wx, q0.w - q0.z, q0.z);
-    const float a10 = fmaf(wx, q1.y - q1.x, q1.x), a11 = fmaf(wx, q1.w - q1.z, q1.z);
+    const float a00 = fmaf(wx, q0.y, q0.x), a01 = fmaf(wx, q0.w, q0.z);  // .y, .w: the x differences
+    const float a10 = fmaf(wx, q1.y, q1.x), a11 = fmaf(wx, q1.w, q1.z);
     const float b0 = fmaf(wy, a01 - a00, a00), b1 = fmaf(wy, a11 - a10, a10);
     return fmaf(wz, b1 - b0, b0);
   }

@@ -1100,7 +1100,8 @@ __global__ void kFaceQuads(Dim3i r, ConstFaceField v, float4* q0, float4* q1, fl
     const unsigned x0 = jx > 0 ? jx - 1 : 0, x1 = jx < nx ? jx : nx - 1;
     const unsigned y0 = jy > 0 ? jy - 1 : 0, y1 = jy < ny ? jy : ny - 1;
     const unsigned b0 = (z * ny + y0) * nx, b1 = (z * ny + y1) * nx;
-    out[e] = make_float4(__ldg(f + b0 + x0), __ldg(f + b0 + x1), __ldg(f + b1 + x0), __ldg(f + b1 + x1));
+    const float f00 = __ldg(f + b0 + x0), f01 = __ldg(f + b0 + x1), f10 = __ldg(f + b1 + x0), f11 = __ldg(f + b1 + x1);
+    out[e] = make_float4(f00, __fsub_rn(f01, f00), f10, __fsub_rn(f11, f10));
   }
 }
 long long faceQuadCount(const Dim3i& r, int a) {
