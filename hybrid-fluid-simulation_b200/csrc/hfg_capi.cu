@@ -782,7 +782,7 @@ HFG_API int hfg_op_advect_particles(const int res[3], const float origin[3], con
     Scratch<float4> q0(faceQuadCount(g.r, 0), s), q1(faceQuadCount(g.r, 1), s), q2(faceQuadCount(g.r, 2), s);
     float4* quads[3] = {q0.p, q1.p, q2.p};
     check(launchFaceQuads(g.r, ConstFaceField{{vx, vy, vz}}, quads, s), "face corner tables");
-    FaceQuads v{{q0.p, q1.p, q2.p}};
+    FaceQuads v = makeFaceQuads(g, q0.p, q1.p, q2.p);
     check(launchSubstepBegin(g, v, pos, v0.p, n, ss.p, s), "substep");
     long long nclamp = clamp_mode == 1 ? std::min<long long>(n, g.r.size()) : n;
     SubstepState host{};

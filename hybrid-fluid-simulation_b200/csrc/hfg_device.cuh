@@ -129,7 +129,7 @@ __device__ inline void sampleFace(const ConstFaceField& v, const Geom& cc, float
 // (EulerParticlesTool.cu:113-115); rounding differs in the last bits.
 struct AxisW {
   int i0, i1;
-  int j;  // corner-table entry: the floor index clamped to [-1, n - 1], plus one
+  int j;  // corner-table entry less one: the floor index clamped to [-1, n - 1]
   float w1;
 };
 
@@ -140,23 +140,57 @@ __device__ __forceinline__ void axisWeights(float t, int n, AxisW& a) {
   a.i0 = clampi(i, n);
   // clamp(i + 1) without forming i + 1 first (it overflows at i = INT_MAX)
   a.i1 = min(max(i, -1), n - 2) + 1;
-  a.j = min(max(i, -1), n - 1) + 1;
+  a.j = min(max(i, -1), n - 1);
 }
 
 // Corner table of a face grid of nx x ny x nz values: (nx + 1) x (ny + 1) x
 // (nz + 2) float4, entry (L, jy, jx) = (f[z][y0][x0], f[z][y0][x1] -
 // f[z][y0][x0], f[z][y1][x0], f[z][y1][x1] - f[z][y1][x0]) with
 // z = clamp(L - 1), x0 = clamp(jx - 1), x1 = clamp(jx), y0 = clamp(jy - 1),
-// y1 = clamp(jy).  Entry (AxisW::j of y, AxisW::j of x) of a sample holds the
-// four corners of one z layer of its trilinear stencil, so one 16-byte load
-// serves four corners; layers AxisW::j and AxisW::j + 1 of z are the
-// stencil's clamp(i) and clamp(i + 1), because the padding layers 0 and
-// nz + 1 repeat the end layers.  The two x differences are the FP32
+// y1 = clamp(jy).  Entry (AxisW::j + 1 of y, AxisW::j + 1 of x) of a sample
+// holds the four corners of one z layer of its trilinear stencil, so one
+// 16-byte load serves four corners; layers AxisW::j + 1 and AxisW::j + 2 of z
+// are the stencil's clamp(i) and clamp(i + 1), because the padding layers 0
+// and nz + 1 repeat the end layers.  The two x differences are the FP32
 // subtractions the x lerps of every sample would otherwise repeat: stored
 // once, they give the same values.
 struct FaceQuads {
+  // entry (1, 1, 1) of each component's table: AxisW::j is the entry index
+  // less one, so a sample's entry is c[a] + (jz * ly + jy) * lx + jx, at
+  // least c[a] - (pl + lx + 1), the table's first entry
   const float4* c[3];
+  // Sampling constants of the grid, formed once on the host (makeFaceQuads)
+  // so that a kernel reads them as launch parameters: the coordinate of a
+  // point on axis k is p * inv + offF on the face grid of that axis and
+  // p * inv + offC (offF - 1/2) on the cell-centred one; jF and jC clamp the
+  // floor index on those two grids (n and n - 1 for n cells); lx, ly and pl
+  // are the row length, the rows per layer and the layer size of component
+  // a's table.
+  float inv[3], offF[3], offC[3];
+  int jF[3], jC[3];
+  unsigned lx[3], ly[3], pl[3];
 };
+
+inline FaceQuads makeFaceQuads(const Geom& g, const float4* q0, const float4* q1, const float4* q2) {
+  FaceQuads q;
+  const float4* base[3] = {q0, q1, q2};
+  const float h[3] = {g.hx, g.hy, g.hz}, o[3] = {g.ox, g.oy, g.oz};
+  const int n[3] = {g.r.x, g.r.y, g.r.z};
+  for (int k = 0; k < 3; ++k) {
+    q.inv[k] = 1.0f / h[k];
+    q.offF[k] = -(o[k] * q.inv[k]);
+    q.offC[k] = q.offF[k] - 0.5f;
+    q.jF[k] = n[k];
+    q.jC[k] = n[k] - 1;
+  }
+  for (int a = 0; a < 3; ++a) {
+    q.lx[a] = (unsigned)(n[0] + (a == 0) + 1);
+    q.ly[a] = (unsigned)(n[1] + (a == 1) + 1);
+    q.pl[a] = q.lx[a] * q.ly[a];
+    q.c[a] = base[a] + (q.pl[a] + q.lx[a] + 1);
+  }
+  return q;
+}
 
 // The corner-table entries of the last sample of each component, kept in
 // registers across the RK stages of one substep: a particle moves a fraction
@@ -164,7 +198,7 @@ struct FaceQuads {
 // cell, and its two 16-byte loads are not repeated (the values are the same
 // ones, the tables do not change during the substeps).
 struct QuadCache {
-  unsigned e[3];
+  int e[3];
   float4 lo[3], hi[3];
 };
 
@@ -178,6 +212,16 @@ struct FaceSampler {
     axisWeights(ux, g.r.x + 1, fc[0]);
     axisWeights(uy, g.r.y + 1, fc[1]);
     axisWeights(uz, g.r.z + 1, fc[2]);
+  }
+  // the same sampler from the constants of a corner-table set: one FMA per
+  // coordinate (the two forms round alike up to the last bit)
+  __device__ __forceinline__ FaceSampler(const FaceQuads& q, float px, float py, float pz) {
+    const float p[3] = {px, py, pz};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      axisWeights(fmaf(p[k], q.inv[k], q.offC[k]), q.jC[k] + 1, cc[k]);
+      axisWeights(fmaf(p[k], q.inv[k], q.offF[k]), q.jF[k] + 1, fc[k]);
+    }
   }
   // weights and 8 linear indices of component `a` (corner order z, y, x);
   // 32-bit index arithmetic (every grid holds fewer than 2^31 entries)
@@ -207,14 +251,12 @@ struct FaceSampler {
   // 16-byte loads instead of eight 4-byte ones, reduced by lerps along x,
   // then y, then z (seven FMAs; rounding differs from the weighted sum in the
   // last bits, and equal corners return their value exactly)
-  __device__ __forceinline__ float sampleQuads(const Geom& g, int a, const float4* __restrict__ Q) const {
+  __device__ __forceinline__ float sampleQuads(const FaceQuads& T, int a) const {
     const AxisW& X = a == 0 ? fc[0] : cc[0];
     const AxisW& Y = a == 1 ? fc[1] : cc[1];
     const AxisW& Z = a == 2 ? fc[2] : cc[2];
-    unsigned lx = (unsigned)(g.r.x + (a == 0) + 1), ly = (unsigned)(g.r.y + (a == 1) + 1);
-    unsigned pl = lx * ly;
-    const float4* q = Q + ((unsigned)Z.j * ly + (unsigned)Y.j) * lx + (unsigned)X.j;
-    const float4 q0 = __ldg(q), q1 = __ldg(q + pl);
+    const float4* q = T.c[a] + (Z.j * (int)T.ly[a] + Y.j) * (int)T.lx[a] + X.j;
+    const float4 q0 = __ldg(q), q1 = __ldg(q + T.pl[a]);
     const float wx = X.w1, wy = Y.w1, wz = Z.w1;
     const float a00 = fmaf(wx, q0.y, q0.x), a01 = fmaf(wx, q0.w, q0.z);  // .y, .w: the x differences
     const float a10 = fmaf(wx, q1.y, q1.x), a11 = fmaf(wx, q1.w, q1.z);
@@ -223,17 +265,14 @@ struct FaceSampler {
   }
   // sampleQuads through the cache: the loads only when the entry differs
   // from the cached one (or fresh)
-  __device__ __forceinline__ float sampleQuadsCached(const Geom& g, int a, const float4* __restrict__ Q, QuadCache& c,
-                                                     bool fresh) const {
+  __device__ __forceinline__ float sampleQuadsCached(const FaceQuads& T, int a, QuadCache& c, bool fresh) const {
     const AxisW& X = a == 0 ? fc[0] : cc[0];
     const AxisW& Y = a == 1 ? fc[1] : cc[1];
     const AxisW& Z = a == 2 ? fc[2] : cc[2];
-    unsigned lx = (unsigned)(g.r.x + (a == 0) + 1), ly = (unsigned)(g.r.y + (a == 1) + 1);
-    unsigned pl = lx * ly;
-    const unsigned e = ((unsigned)Z.j * ly + (unsigned)Y.j) * lx + (unsigned)X.j;
+    const int e = (Z.j * (int)T.ly[a] + Y.j) * (int)T.lx[a] + X.j;
     if (fresh || e != c.e[a]) {
-      c.lo[a] = __ldg(Q + e);
-      c.hi[a] = __ldg(Q + e + pl);
+      c.lo[a] = __ldg(T.c[a] + e);
+      c.hi[a] = __ldg(T.c[a] + e + T.pl[a]);
       c.e[a] = e;
     }
     const float4 q0 = c.lo[a], q1 = c.hi[a];
@@ -262,17 +301,16 @@ __device__ __forceinline__ void sampleFaceFast(const ConstFaceField& v, const Ge
 #pragma unroll
   for (int a = 0; a < 3; ++a) out[a] = s.sample(g, a, v.c[a]);
 }
-__device__ __forceinline__ void sampleFaceQuads(const FaceQuads& v, const Geom& g, float px, float py, float pz,
-                                                float out[3]) {
-  FaceSampler s(g, px, py, pz);
+__device__ __forceinline__ void sampleFaceQuads(const FaceQuads& v, float px, float py, float pz, float out[3]) {
+  FaceSampler s(v, px, py, pz);
 #pragma unroll
-  for (int a = 0; a < 3; ++a) out[a] = s.sampleQuads(g, a, v.c[a]);
+  for (int a = 0; a < 3; ++a) out[a] = s.sampleQuads(v, a);
 }
-__device__ __forceinline__ void sampleFaceQuadsCached(const FaceQuads& v, const Geom& g, float px, float py, float pz,
-                                                      float out[3], QuadCache& c, bool fresh) {
-  FaceSampler s(g, px, py, pz);
+__device__ __forceinline__ void sampleFaceQuadsCached(const FaceQuads& v, float px, float py, float pz, float out[3],
+                                                      QuadCache& c, bool fresh) {
+  FaceSampler s(v, px, py, pz);
 #pragma unroll
-  for (int a = 0; a < 3; ++a) out[a] = s.sampleQuadsCached(g, a, v.c[a], c, fresh);
+  for (int a = 0; a < 3; ++a) out[a] = s.sampleQuadsCached(v, a, c, fresh);
 }
 
 // Cubic samplers (MPhysics/EulerMathTool.cu:134-240, FieldMathTool.cu:106-173).

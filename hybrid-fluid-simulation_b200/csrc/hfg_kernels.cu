@@ -1020,11 +1020,11 @@ __global__ void kParticleVelUpdateLinear(Geom g, int mode, FaceQuads vinQ, Const
       prefetchL2(pos + 3 * (p + stride));
       prefetchL2(vel + 3 * (p + stride));
     }
-    FaceSampler fs(g, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]);
+    FaceSampler fs(vinQ, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]);
     float pic[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      pic[a] = fs.sampleQuads(g, a, vinQ.c[a]);
+      pic[a] = fs.sampleQuads(vinQ, a);
       v0[3 * p + a] = pic[a];
       m = fmaxf(m, fabsf(pic[a]));
     }
@@ -1122,7 +1122,7 @@ __global__ void kSubstepBegin(Geom g, FaceQuads vel, const float* __restrict__ p
   float m = 0.f;
   HFG_FOR_T(I, p, P) {
     float v[3];
-    sampleFaceQuads(vel, g, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2], v);
+    sampleFaceQuads(vel, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2], v);
     v0[3 * p] = v[0]; v0[3 * p + 1] = v[1]; v0[3 * p + 2] = v[2];
     m = fmaxf(m, fmaxf(fabsf(v[0]), fmaxf(fabsf(v[1]), fabsf(v[2]))));
   }
@@ -1174,7 +1174,7 @@ __device__ __forceinline__ float substepParticle(const Geom& g, const FaceQuads&
     float mid[3], w1[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) mid[a] = fmaf(half, w0[a], q[a]);
-    sampleFaceQuadsCached(vel, g, mid[0], mid[1], mid[2], w1, qc, true);
+    sampleFaceQuadsCached(vel, mid[0], mid[1], mid[2], w1, qc, true);
     fresh = false;
 #pragma unroll
     for (int a = 0; a < 3; ++a) q[a] = fmaf(ds, w1[a], q[a]);
@@ -1187,13 +1187,13 @@ __device__ __forceinline__ float substepParticle(const Geom& g, const FaceQuads&
       mid[a] = fmaf(half, w0[a], q[a]);
       acc3[a] = fmaf(a29, w0[a], q[a]);
     }
-    sampleFaceQuadsCached(vel, g, mid[0], mid[1], mid[2], w, qc, true);
+    sampleFaceQuadsCached(vel, mid[0], mid[1], mid[2], w, qc, true);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       tf[a] = fmaf(tq, w[a], q[a]);
       acc3[a] = fmaf(a39, w[a], acc3[a]);
     }
-    sampleFaceQuadsCached(vel, g, tf[0], tf[1], tf[2], w, qc, false);
+    sampleFaceQuadsCached(vel, tf[0], tf[1], tf[2], w, qc, false);
     fresh = false;
 #pragma unroll
     for (int a = 0; a < 3; ++a) q[a] = fmaf(a49, w[a], acc3[a]);
@@ -1207,7 +1207,7 @@ __device__ __forceinline__ float substepParticle(const Geom& g, const FaceQuads&
     }
   } else {
     float v[3];
-    sampleFaceQuadsCached(vel, g, q[0], q[1], q[2], v, qc, fresh);
+    sampleFaceQuadsCached(vel, q[0], q[1], q[2], v, qc, fresh);
     v0[3 * p] = v[0]; v0[3 * p + 1] = v[1]; v0[3 * p + 2] = v[2];
     m = fmaxf(fabsf(v[0]), fmaxf(fabsf(v[1]), fabsf(v[2])));
   }
@@ -1270,6 +1270,7 @@ __global__ void __launch_bounds__(256, 3) kSubstepMulti(const SubstepTask* __res
                                                        const long long* __restrict__ chunkStart, int nScenes,
                                                        int slot) {
   __shared__ int sc;
+  __shared__ FaceQuads sq;
   if (threadIdx.x == 0) {
     int lo = 0, hi = nScenes - 1;  // the last scene whose first chunk is <= blockIdx.x
     while (lo < hi) {
@@ -1278,6 +1279,7 @@ __global__ void __launch_bounds__(256, 3) kSubstepMulti(const SubstepTask* __res
       else hi = mid - 1;
     }
     sc = lo;
+    sq = tasks[lo].vel;
   }
   __syncthreads();
   const SubstepTask& T = tasks[sc];
@@ -1288,7 +1290,9 @@ __global__ void __launch_bounds__(256, 3) kSubstepMulti(const SubstepTask* __res
     return;
   }
   const Geom g = T.g;
-  const FaceQuads vel = T.vel;
+  // the scene's tables and sampling constants, read from shared memory where
+  // used (held in registers they spill)
+  const FaceQuads& vel = sq;
   const float minH = fminf(fminf(g.hx, g.hy), g.hz);
   bool last;
   const SubstepCoef k(substepSize(cur, T.dt, T.cfl, minH, last));

@@ -413,7 +413,7 @@ FaceQuads GridSolver::beginParticleStep(ConstFaceField vin) {
   }
   launched(launchFaceQuads(g_.r, vin, quads, stream_), "face corner tables");
   check(cudaMemsetAsync(subState_.p, 0, sizeof(SubstepState) * (subSlots_ + 1), stream_), "memset");
-  return FaceQuads{{quads[0], quads[1], quads[2]}};
+  return makeFaceQuads(g_, quads[0], quads[1], quads[2]);
 }
 
 // EulerParticles.cpp:231-325.  Substeps are launched speculatively in chunks;
