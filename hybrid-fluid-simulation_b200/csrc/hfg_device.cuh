@@ -9,6 +9,7 @@
 // (MPhysics/FieldMathTool.cu:800-808).
 #pragma once
 #include <cfloat>
+#include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
 #include <utility>
@@ -143,6 +144,23 @@ __device__ __forceinline__ void axisWeights(float t, int n, AxisW& a) {
   a.j = min(max(i, -1), n - 1);
 }
 
+// axisWeights with the coordinate clamped first to [-1, hi], hi the float
+// below n: the floor index is then in [-1, n - 1] with no integer clamp.  A
+// coordinate outside that range selects the same edge corners as the integer
+// clamp does, which hold equal values (the table's x differences and the y
+// and z corner pairs there are exact zeros), so every finite coordinate
+// samples the same value as with axisWeights; a NaN coordinate samples the
+// edge instead of returning NaN.
+__device__ __forceinline__ void clampedAxis(float t, float hi, int jmax, AxisW& a) {
+  const float c = fminf(fmaxf(t, -1.0f), hi);
+  const float f = floorf(c);
+  a.w1 = c - f;
+  const int i = (int)f;
+  a.i0 = max(i, 0);
+  a.i1 = min(i + 1, jmax);
+  a.j = i;
+}
+
 // Corner table of a face grid of nx x ny x nz values: (nx + 1) x (ny + 1) x
 // (nz + 2) float4, entry (L, jy, jx) = (f[z][y0][x0], f[z][y0][x1] -
 // f[z][y0][x0], f[z][y1][x0], f[z][y1][x1] - f[z][y1][x0]) with
@@ -162,11 +180,12 @@ struct FaceQuads {
   // Sampling constants of the grid, formed once on the host (makeFaceQuads)
   // so that a kernel reads them as launch parameters: the coordinate of a
   // point on axis k is p * inv + offF on the face grid of that axis and
-  // p * inv + offC (offF - 1/2) on the cell-centred one; jF and jC clamp the
-  // floor index on those two grids (n and n - 1 for n cells); lx, ly and pl
-  // are the row length, the rows per layer and the layer size of component
-  // a's table.
-  float inv[3], offF[3], offC[3];
+  // p * inv + offC (offF - 1/2) on the cell-centred one; hiF and hiC, the
+  // float below n + 1 and n for n cells, bound the coordinate on those two
+  // grids, and jF and jC (n and n - 1) are the largest floor index there;
+  // lx, ly and pl are the row length, the rows per layer and the layer size
+  // of component a's table.
+  float inv[3], offF[3], offC[3], hiF[3], hiC[3];
   int jF[3], jC[3];
   unsigned lx[3], ly[3], pl[3];
 };
@@ -182,6 +201,8 @@ inline FaceQuads makeFaceQuads(const Geom& g, const float4* q0, const float4* q1
     q.offC[k] = q.offF[k] - 0.5f;
     q.jF[k] = n[k];
     q.jC[k] = n[k] - 1;
+    q.hiF[k] = std::nextafter((float)(n[k] + 1), 0.0f);
+    q.hiC[k] = std::nextafter((float)n[k], 0.0f);
   }
   for (int a = 0; a < 3; ++a) {
     q.lx[a] = (unsigned)(n[0] + (a == 0) + 1);
@@ -214,13 +235,14 @@ struct FaceSampler {
     axisWeights(uz, g.r.z + 1, fc[2]);
   }
   // the same sampler from the constants of a corner-table set: one FMA per
-  // coordinate (the two forms round alike up to the last bit)
+  // coordinate (the two forms round alike up to the last bit), and the
+  // coordinate clamped to [-1, n) before the floor (clampedAxis)
   __device__ __forceinline__ FaceSampler(const FaceQuads& q, float px, float py, float pz) {
     const float p[3] = {px, py, pz};
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      axisWeights(fmaf(p[k], q.inv[k], q.offC[k]), q.jC[k] + 1, cc[k]);
-      axisWeights(fmaf(p[k], q.inv[k], q.offF[k]), q.jF[k] + 1, fc[k]);
+      clampedAxis(fmaf(p[k], q.inv[k], q.offC[k]), q.hiC[k], q.jC[k], cc[k]);
+      clampedAxis(fmaf(p[k], q.inv[k], q.offF[k]), q.hiF[k], q.jF[k], fc[k]);
     }
   }
   // weights and 8 linear indices of component `a` (corner order z, y, x);

@@ -1218,6 +1218,7 @@ __device__ __forceinline__ float substepParticle(const Geom& g, const FaceQuads&
 // The RK coefficients of a substep of size ds (EulerParticles.cpp:281-301).
 struct SubstepCoef {
   float ds, half, tq, a29, a39, a49;
+  SubstepCoef() = default;
   __device__ explicit SubstepCoef(float d)
       : ds(d), half((float)(0.5 * (double)d)), tq((float)(0.75 * (double)d)), a29((float)(2.0 / 9.0 * (double)d)),
         a39((float)(3.0 / 9.0 * (double)d)), a49((float)(4.0 / 9.0 * (double)d)) {}
@@ -1226,20 +1227,31 @@ struct SubstepCoef {
 // One RK1/2/3 substep (EulerParticles.cpp:277-318).  After the last substep the
 // box clamp of fixParticlesPosWithBoundarys (EulerParticlesTool.cu:310-333) is
 // applied to the first `nclamp` particles; otherwise the next v0 and its max
-// are produced for slot+1.
-template <typename I>
+// are produced for slot+1.  ACC: the RK order (0, 1, 2), fixed per
+// instantiation so that the particle loop carries no branch on it.
+template <typename I, int ACC>
 __global__ void __launch_bounds__(256, 4) kSubstep(Geom g, FaceQuads vel, float* __restrict__ pos,
-                                                  float* __restrict__ v0, long long P,
-                         int acc, float dt, float cfl, long long nclamp, SubstepState* st, int slot) {
+                                                  float* __restrict__ v0, long long P, float dt, float cfl,
+                                                  long long nclamp, SubstepState* st, int slot) {
   const SubstepState cur = st[slot];
   if (cur.finished) {
     // carry the finished state forward so later speculative launches no-op
     if (blockIdx.x == 0 && threadIdx.x == 0) st[slot + 1] = cur;
     return;
   }
-  float minH = fminf(fminf(g.hx, g.hy), g.hz);
-  bool last;
-  const SubstepCoef k(substepSize(cur, dt, cfl, minH, last));
+  // the substep size and RK coefficients, formed once per block: held in
+  // shared memory, a use is one load where registers would have to give way
+  // to recomputing them (FP64 products) inside the particle loop
+  __shared__ SubstepCoef sk;
+  __shared__ int sLast;
+  if (threadIdx.x == 0) {
+    bool l;
+    sk = SubstepCoef(substepSize(cur, dt, cfl, fminf(fminf(g.hx, g.hy), g.hz), l));
+    sLast = l ? 1 : 0;
+  }
+  __syncthreads();
+  const SubstepCoef& k = sk;
+  const bool last = sLast != 0;
   float m = 0.f;
   const I stride = (I)gridDim.x * blockDim.x;
   HFG_FOR_T(I, p, P) {
@@ -1249,7 +1261,7 @@ __global__ void __launch_bounds__(256, 4) kSubstep(Geom g, FaceQuads vel, float*
       prefetchL2(pos + 3 * (p + stride));
       prefetchL2(v0 + 3 * (p + stride));
     }
-    m = fmaxf(m, substepParticle<I>(g, vel, pos, v0, p, acc, k.ds, k.half, k.tq, k.a29, k.a39, k.a49, last,
+    m = fmaxf(m, substepParticle<I>(g, vel, pos, v0, p, ACC, k.ds, k.half, k.tq, k.a29, k.a39, k.a49, last,
                                     (long long)p < nclamp));
   }
   if (!last) blockMaxToGlobal(m, &st[slot + 1].maxAbsBits);
@@ -1338,11 +1350,18 @@ cudaError_t launchGatherSubstepStates(const SubstepTask* tasks, int nScenes, int
 
 cudaError_t launchSubstep(const Geom& g, FaceQuads vel, float* pos, float* v0, long long P, int acc, float dt,
                           float cfl, long long nclamp, SubstepState* st, int slot, cudaStream_t s) {
-  if (index32(P))
-    kSubstep<int><<<gridFor(P > 0 ? P : 1), kThreads, 0, s>>>(g, vel, pos, v0, P, acc, dt, cfl, nclamp, st, slot);
-  else
-    kSubstep<long long><<<gridFor(P > 0 ? P : 1), kThreads, 0, s>>>(g, vel, pos, v0, P, acc, dt, cfl, nclamp, st,
-                                                                     slot);
+  const int grid = gridFor(P > 0 ? P : 1);
+#define HFG_SUBSTEP(I, A) kSubstep<I, A><<<grid, kThreads, 0, s>>>(g, vel, pos, v0, P, dt, cfl, nclamp, st, slot)
+  if (index32(P)) {
+    if (acc == 0) HFG_SUBSTEP(int, 0);
+    else if (acc == 1) HFG_SUBSTEP(int, 1);
+    else HFG_SUBSTEP(int, 2);
+  } else {
+    if (acc == 0) HFG_SUBSTEP(long long, 0);
+    else if (acc == 1) HFG_SUBSTEP(long long, 1);
+    else HFG_SUBSTEP(long long, 2);
+  }
+#undef HFG_SUBSTEP
   return cudaGetLastError();
 }
 
