@@ -935,6 +935,42 @@ HFG_API int hfg_op_build_fluid_sdf(const int res[3], const float* domain, float*
     return HFG_OK;
   });
 }
+namespace {
+int fluidSideSdf(const int res[3], const float* density, const float* solid_sdf, float* out, int distance,
+                 bool outside, void* stream) {
+  return guarded([&]() -> int {
+    NEED(validRes(res) && density && solid_sdf && out && distance >= 0 && distance <= 100000, "invalid arguments");
+    Dim3i r = toRes(res);
+    cudaStream_t s = st(stream);
+    Scratch<unsigned int> fa(r.size(), s), fb(r.size(), s), cnt(2, s);
+    unsigned int* host = nullptr;
+    check(cudaMallocHost((void**)&host, sizeof(unsigned int)), "cudaMallocHost");
+    cudaError_t e = launchFluidSideSdf(r, density, solid_sdf, outside, distance, out, fa.p, fb.p, cnt.p, host, s);
+    cudaFreeHost(host);
+    check(e, outside ? "fluid outside sdf" : "fluid inside sdf");
+    check(cudaStreamSynchronize(s), "sync");
+    return HFG_OK;
+  });
+}
+}  // namespace
+HFG_API int hfg_op_build_fluid_outside_sdf(const int res[3], const float* density, const float* solid_sdf, float* out,
+                                           int distance, void* stream) {
+  return fluidSideSdf(res, density, solid_sdf, out, distance, true, stream);
+}
+HFG_API int hfg_op_build_fluid_inside_sdf(const int res[3], const float* density, const float* solid_sdf, float* out,
+                                          int distance, void* stream) {
+  return fluidSideSdf(res, density, solid_sdf, out, distance, false, stream);
+}
+HFG_API int hfg_op_build_mixed_fluid_outside_sdf(const int res[3], const float* grid_density,
+                                                 const float* mixed_density, const float* grid_outside_sdf,
+                                                 float* out, void* stream) {
+  return guarded([&]() -> int {
+    NEED(validRes(res) && grid_density && mixed_density && grid_outside_sdf && out, "invalid arguments");
+    check(launchMixedOutsideSdf(toRes(res), grid_density, mixed_density, grid_outside_sdf, out, st(stream)),
+          "mixed outside sdf");
+    return HFG_OK;
+  });
+}
 HFG_API int hfg_op_fluid_domain_from_bbox(const int res[3], const float origin[3], const float spacing[3],
                                           const float mn[3], const float mx[3], float* out, void* stream) {
   return guarded([&]() -> int {

@@ -836,6 +836,123 @@ cudaError_t launchFluidSdf(const Dim3i& r, const float* dom, float* sdf, int lay
 }
 
 // ===========================================================================
+// Inside / outside distance fields of the fluid density (the hybrid
+// coupler's buildFluidInsideSDF / buildFluidOutsideSDF,
+// HybridSimulatorBuildSDF.cu:4-146,177-238).  Sweep 0 gives solids 0,
+// surface cells (density 0.2) the seed value s (0.2 - 0.5 inside, 0.5 - 0.2
+// outside), cells of density 0 (inside) or 1 (outside) 0 and the rest
+// UNKNOWN; sweep d then gives every UNKNOWN 6-neighbour of a cell holding
+// d - 1 + s the value d + s, and negative values end as 0.  The reference
+// sweeps the whole grid `distance` times; here each sweep visits the
+// previous shell only (frontier lists, as launchFluidSdf).
+// ===========================================================================
+namespace {
+__device__ __forceinline__ bool realEq(float a, float b) { return fabsf(__fsub_rn(a, b)) < FLT_MIN; }  // isRealEQ
+}  // namespace
+
+__global__ void kSideSdfInit(Dim3i r, const float* __restrict__ density, const float* __restrict__ solid,
+                             float seed, float zero, float* __restrict__ out, unsigned int* __restrict__ front,
+                             unsigned int* __restrict__ count) {
+  HFG_FOR(c, r.size()) {
+    const float rho = density[c];
+    float v = kUnknown;
+    bool surface = false;
+    if (solid[c] < 0.f) {
+      v = 0.f;
+    } else if (realEq(rho, (float)kSurf)) {
+      v = seed;
+      surface = true;
+    } else if (realEq(rho, zero)) {
+      v = 0.f;
+    }
+    out[c] = v;
+    if (surface) front[atomicAdd(count, 1u)] = (unsigned int)c;
+  }
+}
+
+__global__ void kSideSdfLayer(Dim3i r, float* __restrict__ out, const unsigned int* __restrict__ front, unsigned int n,
+                              unsigned int* __restrict__ next, unsigned int* __restrict__ count, float v) {
+  HFG_FOR(i, (long long)n) {
+    const long long c = front[i];
+    int x, y, z;
+    cellCoord(c, r, x, y, z);
+    const int dx[6] = {-1, 1, 0, 0, 0, 0}, dy[6] = {0, 0, -1, 1, 0, 0}, dz[6] = {0, 0, 0, 0, -1, 1};
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const long long nb = linc(x + dx[k], y + dy[k], z + dz[k], r);
+      const int old = atomicCAS((int*)(out + nb), __float_as_int(kUnknown), __float_as_int(v));
+      if (old == __float_as_int(kUnknown)) next[atomicAdd(count, 1u)] = (unsigned int)nb;
+    }
+  }
+}
+
+// buildFluidSDFPostProcess (HybridSimulatorBuildSDF.cu:122-137)
+__global__ void kNegativeToZero(long long n, float* __restrict__ out) {
+  HFG_FOR(i, n) {
+    if (out[i] < 0.f) out[i] = 0.f;
+  }
+}
+
+cudaError_t launchFluidSideSdf(const Dim3i& r, const float* density, const float* solid, bool outside, int distance,
+                               float* out, unsigned int* frontA, unsigned int* frontB, unsigned int* counts,
+                               unsigned int* hostCount, cudaStream_t s) {
+  // the reference's UInt + double expressions, rounded to Real once
+  const double seed = outside ? 0.5 - kSurf : kSurf - 0.5;
+  if (distance > 0) {
+    cudaError_t e = cudaMemsetAsync(counts, 0, sizeof(unsigned int) * 2, s);
+    if (e != cudaSuccess) return e;
+    kSideSdfInit<<<gridFor(r.size()), kThreads, 0, s>>>(r, density, solid, (float)seed, outside ? 1.f : 0.f, out,
+                                                         frontA, counts);
+    unsigned int* cur = frontA;
+    unsigned int* nxt = frontB;
+    int slot = 0;
+    for (int d = 1; d < distance; ++d) {
+      // sweep d looks for (d + s) - 1; where that is not the value sweep
+      // d - 1 wrote, the reference's shell stops growing
+      if ((float)((double)d + seed - 1) != (float)((double)(d - 1) + seed)) break;
+      e = cudaMemcpyAsync(hostCount, counts + slot, sizeof(unsigned int), cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) return e;
+      const unsigned int n = *hostCount;
+      if (n == 0) break;
+      e = cudaMemsetAsync(counts + (slot ^ 1), 0, sizeof(unsigned int), s);
+      if (e != cudaSuccess) return e;
+      kSideSdfLayer<<<gridFor(n), kThreads, 0, s>>>(r, out, cur, n, nxt, counts + (slot ^ 1),
+                                                   (float)((double)d + seed));
+      e = cudaGetLastError();
+      if (e != cudaSuccess) return e;
+      std::swap(cur, nxt);
+      slot ^= 1;
+    }
+  }
+  kNegativeToZero<<<gridFor(r.size()), kThreads, 0, s>>>(r.size(), out);
+  return cudaGetLastError();
+}
+
+// buildMixedFluidOutsideSDF (HybridSimulatorBuildSDF.cu:139-175): at a cell of
+// grid density 0.2, 0.5 minus the mixed density (negative -> 0); elsewhere
+// the grid fluid's outside distance.
+__global__ void kMixedOutsideSdf(long long n, const float* __restrict__ gridDensity,
+                                 const float* __restrict__ mixedDensity, const float* __restrict__ gridOutside,
+                                 float* __restrict__ out) {
+  HFG_FOR(c, n) {
+    float v;
+    if (realEq(gridDensity[c], (float)kSurf)) {
+      v = __double2float_rn(0.5 - (double)mixedDensity[c]);
+      if (v < 0.f) v = 0.f;
+    } else {
+      v = gridOutside[c];
+    }
+    out[c] = v;
+  }
+}
+cudaError_t launchMixedOutsideSdf(const Dim3i& r, const float* gridDensity, const float* mixedDensity,
+                                  const float* gridOutside, float* out, cudaStream_t s) {
+  kMixedOutsideSdf<<<gridFor(r.size()), kThreads, 0, s>>>(r.size(), gridDensity, mixedDensity, gridOutside, out);
+  return cudaGetLastError();
+}
+
+// ===========================================================================
 // Particles
 // ===========================================================================
 

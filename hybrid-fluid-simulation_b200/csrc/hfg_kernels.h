@@ -237,6 +237,14 @@ void extrapUsers(int delta);
 
 // ---- fluid SDF (buildFluidSDF); frontier buffers hold N cells each; counts 2;
 // hostCount pinned.  Blocks (one host read per layer).
+// The hybrid coupler's inside / outside distance fields of a fluid density
+// (frontier lists of r.size() entries each, two counters, one pinned host
+// word; the stream is synchronised once per sweep) and its mixed outside field.
+cudaError_t launchFluidSideSdf(const Dim3i& r, const float* density, const float* solid, bool outside, int distance,
+                               float* out, unsigned int* frontA, unsigned int* frontB, unsigned int* counts,
+                               unsigned int* hostCount, cudaStream_t s);
+cudaError_t launchMixedOutsideSdf(const Dim3i& r, const float* gridDensity, const float* mixedDensity,
+                                  const float* gridOutside, float* out, cudaStream_t s);
 cudaError_t launchFluidSdf(const Dim3i& r, const float* dom, float* sdf, int layers, unsigned int* frontA,
                            unsigned int* frontB, unsigned int* counts, unsigned int* hostCount, cudaStream_t s);
 // mixFieldWithDensity of a cell grid (face = 0, a[0], b[0]) or of the three

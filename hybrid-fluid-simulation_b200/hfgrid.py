@@ -180,6 +180,9 @@ def _signatures(lib):
         "hfg_op_sl_advect_cc": (C.c_int, [I3, F3, F3, VP, VP, VP, VP, C.c_float, C.c_int, VP, VP]),
         "hfg_op_fluid_domain_from_bbox": (C.c_int, [I3, F3, F3, F3, F3, VP, VP]),
         "hfg_op_build_fluid_sdf": (C.c_int, [I3, VP, VP, C.c_int, VP]),
+        "hfg_op_build_fluid_outside_sdf": (C.c_int, [I3, VP, VP, VP, C.c_int, VP]),
+        "hfg_op_build_fluid_inside_sdf": (C.c_int, [I3, VP, VP, VP, C.c_int, VP]),
+        "hfg_op_build_mixed_fluid_outside_sdf": (C.c_int, [I3, VP, VP, VP, VP, VP]),
         "hfg_op_build_fluid_density": (C.c_int, [I3, VP, VP, VP, VP]),
         "hfg_op_mix_field_with_density_cc": (C.c_int, [C.c_longlong, VP, VP, VP, VP, VP]),
         "hfg_op_mix_field_with_density_fc": (C.c_int, [I3, VP, VP, VP, VP, VP, VP, VP, VP, VP]),
@@ -666,6 +669,24 @@ def op_build_fluid_density(res, domain, solid_sdf, out, stream=None):
 
 def op_build_fluid_sdf(res, domain, sdf, layers=1000, stream=None):
     _check(lib().hfg_op_build_fluid_sdf(_i3(res), _ptr(domain), _ptr(sdf), layers, _stream(stream)))
+
+
+def op_build_fluid_outside_sdf(res, density, solid_sdf, out, distance=1000, stream=None):
+    """buildFluidOutsideSDFInvoker (HybridSimulatorBuildSDF.cu:177-207)."""
+    _check(lib().hfg_op_build_fluid_outside_sdf(_i3(res), _ptr(density), _ptr(solid_sdf), _ptr(out), distance,
+                                                _stream(stream)))
+
+
+def op_build_fluid_inside_sdf(res, density, solid_sdf, out, distance=1000, stream=None):
+    """buildFluidInsideSDFInvoker (HybridSimulatorBuildSDF.cu:209-238)."""
+    _check(lib().hfg_op_build_fluid_inside_sdf(_i3(res), _ptr(density), _ptr(solid_sdf), _ptr(out), distance,
+                                               _stream(stream)))
+
+
+def op_build_mixed_fluid_outside_sdf(res, grid_density, mixed_density, grid_outside_sdf, out, stream=None):
+    """buildMixedFluidOutsideSDFInvoker (HybridSimulatorBuildSDF.cu:240-266)."""
+    _check(lib().hfg_op_build_mixed_fluid_outside_sdf(_i3(res), _ptr(grid_density), _ptr(mixed_density),
+                                                      _ptr(grid_outside_sdf), _ptr(out), _stream(stream)))
 
 
 def op_seed_particles(res, origin, spacing, fluid_sdf, solid_sdf, per_cell, seed, pos=None, capacity=0, stream=None):

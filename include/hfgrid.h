@@ -349,6 +349,25 @@ HFG_API int hfg_op_mix_particle_vel_pic_flip(const float* pic, const float* flip
 /* buildFluidDensityInvoker  EulerSolverTool.cu:408-448,787-810; solid_sdf < 0 inside solids */
 HFG_API int hfg_op_build_fluid_density(const int res[3], const float* domain, const float* solid_sdf, float* out,
                                        void* stream);
+/* buildFluidOutsideSDFInvoker / buildFluidInsideSDFInvoker of the hybrid
+ * coupler  HybridSimulatorBuildSDF.cu:4-146,177-238: the distance in cells
+ * from the surface cells (density 0.2) into the air (outside) or the fluid
+ * (inside) of a fluid density field (hfg_op_build_fluid_density), grown over
+ * `distance` sweeps as the reference's invokers do (it passes 1000); solids
+ * (solid_sdf < 0) and the other side hold 0, cells no sweep reaches UNKNOWN
+ * (FLT_MAX), negative values end as 0.  distance 0 only clamps `out`'s
+ * negative values to 0.  0 <= distance <= 100000.  Blocks (one host read per
+ * sweep). */
+HFG_API int hfg_op_build_fluid_outside_sdf(const int res[3], const float* density, const float* solid_sdf, float* out,
+                                           int distance, void* stream);
+HFG_API int hfg_op_build_fluid_inside_sdf(const int res[3], const float* density, const float* solid_sdf, float* out,
+                                          int distance, void* stream);
+/* buildMixedFluidOutsideSDFInvoker  HybridSimulatorBuildSDF.cu:139-175,240-266:
+ * at a cell of grid density 0.2, 0.5 - mixed density (negative -> 0);
+ * elsewhere grid_outside_sdf */
+HFG_API int hfg_op_build_mixed_fluid_outside_sdf(const int res[3], const float* grid_density,
+                                                 const float* mixed_density, const float* grid_outside_sdf,
+                                                 float* out, void* stream);
 /* generateFluidDomainFromBBoxInvoker  EulerSolverTool.cu:989-1013 */
 HFG_API int hfg_op_fluid_domain_from_bbox(const int res[3], const float origin[3], const float spacing[3],
                                           const float mn[3], const float mx[3], float* out, void* stream);

@@ -1120,6 +1120,70 @@ void orc_build_fluid_density(const int* res, const float* dom, const float* soli
       }
 }
 
+// HybridSimulatorBuildSDF.cu:4-146,177-238 buildFluidInsideSDF /
+// buildFluidOutsideSDF, driven as their invokers: sweep 0 sets solids (solid
+// SDF < 0) to 0, cells of the surface density 0.2 to the seed value (0.2 -
+// 0.5 inside, 0.5 - 0.2 outside), cells of density 0 (inside) or 1
+// (outside) to 0 and the rest to UNKNOWN; sweep i (1 .. distance - 1) gives
+// an UNKNOWN cell the value i + seed when a clamp-to-edge 6-neighbour holds
+// i - 1 + seed (equality as isRealEQ, |a - b| < FLT_MIN); finally negative
+// values become 0 (buildFluidSDFPostProcess, :122-137).  Every shell value is
+// formed in double and rounded to float once, as the reference's mixed
+// UInt/double expressions are.  A cell written in sweep i never holds the
+// value sweep i tests for, so reading the previous sweep's copy is the
+// reference's in-place sweep.
+void orc_build_fluid_side_sdf(const int* res, const float* density, const float* solid, int outside, int distance,
+                              float* out) {
+  Res r{res[0], res[1], res[2]};
+  const double FS = 0.2;  // FluidSurfaceDensity (Common.h:244)
+  const double seed = outside ? 0.5 - FS : FS - 0.5;
+  const float zeroDensity = outside ? 1.0f : 0.0f;
+  const float U = FLT_MAX;
+  auto eq = [](float a, float b) { return std::fabs(a - b) < FLT_MIN; };
+  i64 N = r.size();
+  if (distance > 0)
+    for (i64 c = 0; c < N; ++c) {
+      if (solid[c] < 0) out[c] = 0.f;
+      else if (eq(density[c], (float)FS)) out[c] = (float)seed;
+      else if (eq(density[c], zeroDensity)) out[c] = 0.f;
+      else out[c] = U;
+    }
+  const int dx[6] = {-1, 1, 0, 0, 0, 0}, dy[6] = {0, 0, -1, 1, 0, 0}, dz[6] = {0, 0, 0, 0, -1, 1};
+  std::vector<float> prev(N);
+  for (int i = 1; i < distance; ++i) {
+    std::memcpy(prev.data(), out, N * sizeof(float));
+    const float target = (float)((double)i + seed - 1), value = (float)((double)i + seed);
+    bool any = false;
+    for (int z = 0; z < r.z; ++z)
+      for (int y = 0; y < r.y; ++y)
+        for (int x = 0; x < r.x; ++x) {
+          i64 c = lin(x, y, z, r);
+          if (prev[c] != U) continue;
+          for (int k = 0; k < 6; ++k)
+            if (eq(prev[lin(x + dx[k], y + dy[k], z + dz[k], r)], target)) { out[c] = value; any = true; break; }
+        }
+    if (!any) break;
+  }
+  for (i64 c = 0; c < N; ++c)
+    if (out[c] < 0) out[c] = 0.f;
+}
+
+// HybridSimulatorBuildSDF.cu:139-175,240-266 buildMixedFluidOutsideSDF: at a
+// cell of grid density 0.2, 0.5 minus the mixed density (negative -> 0);
+// elsewhere the grid fluid's outside SDF.
+void orc_build_mixed_fluid_outside_sdf(const int* res, const float* gridDensity, const float* mixedDensity,
+                                       const float* gridOutside, float* out) {
+  Res r{res[0], res[1], res[2]};
+  for (i64 c = 0; c < r.size(); ++c) {
+    if (std::fabs(gridDensity[c] - (float)0.2) < FLT_MIN) {
+      float v = (float)(0.5 - (double)mixedDensity[c]);
+      out[c] = v < 0 ? 0.f : v;
+    } else {
+      out[c] = gridOutside[c];
+    }
+  }
+}
+
 // HybridSimulatorMixFieldWithDensity.cu:6-265 mixFieldWithDensity: B := (wA A +
 // wB B) / (wA + wB) where wA + wB > FLT_EPSILON (B kept elsewhere).  On a
 // face grid the weights are the means of the two adjacent cells (clamp to

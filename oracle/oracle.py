@@ -46,6 +46,8 @@ def lib():
             "orc_fluid_domain_from_bbox": (None, [I3, F3, F3, F3, F3, PF]),
             "orc_build_fluid_sdf": (None, [I3, PF, C.c_int, PF]),
             "orc_build_fluid_density": (None, [I3, PF, PF, PF]),
+            "orc_build_fluid_side_sdf": (None, [I3, PF, PF, C.c_int, C.c_int, PF]),
+            "orc_build_mixed_fluid_outside_sdf": (None, [I3, PF, PF, PF, PF]),
             "orc_mix_field_with_density_cc": (None, [C.c_longlong, PF, PF, PF, PF]),
             "orc_mix_field_with_density_fc": (None, [I3, PF, PF, PF, PF, PF, PF, PF, PF]),
             "orc_mix_particle_vel": (None, [PF, PF, PF, C.c_longlong, C.c_float, C.c_float, C.c_float, C.c_float,
@@ -167,6 +169,25 @@ def build_fluid_sdf(res, domain, layers=1000):
 def build_fluid_density(res, domain, solid_sdf):
     out = np.empty(res[::-1], np.float32)
     lib().orc_build_fluid_density(i3(res), fp(f32(domain).reshape(-1)), fp(f32(solid_sdf).reshape(-1)), fp(out))
+    return out
+
+
+def build_fluid_side_sdf(res, density, solid_sdf, outside, distance=1000, out=None):
+    """buildFluidOutsideSDF (outside) / buildFluidInsideSDF with their
+    invokers' `distance` sweeps (HybridSimulatorBuildSDF.cu:4-146,177-238).
+    `out` is the field the sweeps start from (read only when distance is 0)."""
+    out = np.zeros(res[::-1], np.float32) if out is None else f32(out).reshape(res[::-1]).copy()
+    lib().orc_build_fluid_side_sdf(i3(res), fp(f32(density).reshape(-1)), fp(f32(solid_sdf).reshape(-1)),
+                                   int(bool(outside)), int(distance), fp(out))
+    return out
+
+
+def build_mixed_fluid_outside_sdf(res, grid_density, mixed_density, grid_outside):
+    """buildMixedFluidOutsideSDF (HybridSimulatorBuildSDF.cu:139-175,240-266)."""
+    out = np.empty(res[::-1], np.float32)
+    lib().orc_build_mixed_fluid_outside_sdf(i3(res), fp(f32(grid_density).reshape(-1)),
+                                            fp(f32(mixed_density).reshape(-1)), fp(f32(grid_outside).reshape(-1)),
+                                            fp(out))
     return out
 
 

@@ -35,6 +35,7 @@ declare -A SUITES=(
   [ExternalForces]="Euler/UnitTest-ExternalForces/UnitTest-ExternalForces.cu"
   [Extrapolation]="Euler/UnitTest-Extrapolation/UnitTest-Extrapolation.cu"
   [PressureSolver]="Euler/UnitTest-PressureSolver/UnitTest-PressureSolver.cu"
+  [HybridHelper]="Hybrid/UnitTest-HybridHelper/UnitTest-HybridHelper.cu"
   [GridFluidSolver]="Euler/IntegrationTest-GridFluidSolver/IntegrationTest-GridFluidSolver.cpp"
   [CellCenteredScalarField]="DataStructure/UnitTest-ScalarGrid/UnitTest-CellCenteredScalarField.cu"
   [CellCenteredVectorField]="DataStructure/UnitTest-CellCenteredVectorGrid/UnitTest-CellCenteredVectorField.cu"

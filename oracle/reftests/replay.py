@@ -31,6 +31,7 @@ SOURCES = {
     "ExternalForces": "TestCase/MPhysics/Euler/UnitTest-ExternalForces/UnitTest-ExternalForces.cu",
     "Extrapolation": "TestCase/MPhysics/Euler/UnitTest-Extrapolation/UnitTest-Extrapolation.cu",
     "PressureSolver": "TestCase/MPhysics/Euler/UnitTest-PressureSolver/UnitTest-PressureSolver.cu",
+    "HybridHelper": "TestCase/MPhysics/Hybrid/UnitTest-HybridHelper/UnitTest-HybridHelper.cu",
     "GridFluidSolver": "TestCase/MPhysics/Euler/IntegrationTest-GridFluidSolver/IntegrationTest-GridFluidSolver.cpp",
     "CellCenteredScalarField": "TestCase/MPhysics/DataStructure/UnitTest-ScalarGrid/UnitTest-CellCenteredScalarField.cu",
     "CellCenteredVectorField":

@@ -41,6 +41,7 @@ typedef size_t SizeT;
 #define GRID_SOLVER_EPSILON 1e-4
 #define FluidDomainValue 500
 #define SolidDomainValue 400
+#define FluidSurfaceDensity 0.2  // Common.h:244
 #define AirDomainValue 300
 
 // ----------------------------------------------------------------- oracle ABI
@@ -88,6 +89,17 @@ void orc_solver_set_fluid_domain(void* p, const float* d);
 void orc_solver_add_external_force(void* p, float x, float y, float z);
 int orc_solver_update(void* p);
 void orc_solver_get_velocity(void* p, int which, float* x, float* y, float* z);
+void orc_solver_get_fluid_domain(void* p, float* d);
+void orc_fluid_domain_from_bbox(const int* res, const float* o, const float* h, const float* mn, const float* mx,
+                                float* out);
+void orc_build_fluid_density(const int* res, const float* dom, const float* solid, float* out);
+void orc_build_fluid_side_sdf(const int* res, const float* density, const float* solid, int outside, int distance,
+                              float* out);
+void orc_build_mixed_fluid_outside_sdf(const int* res, const float* gridDensity, const float* mixedDensity,
+                                       const float* gridOutside, float* out);
+void orc_mix_field_with_density_cc(long long n, const float* a, float* b, const float* wa, const float* wb);
+void orc_mix_field_with_density_fc(const int* res, const float* ax, const float* ay, const float* az, float* bx,
+                                   float* by, float* bz, const float* wa, const float* wb);
 }
 
 // Operations of the reference that the oracle does not restate (they are
@@ -969,7 +981,22 @@ class CGridFluidSolver {
   template <class P> void setAdvectionSolver(const P&) { RT_NOT_RESTATED("CGridFluidSolver::setAdvectionSolver"); }
   void generateCurFluidSDF() { RT_NOT_RESTATED("CGridFluidSolver::generateCurFluidSDF"); }
   void generateCurFluidDensity() { RT_NOT_RESTATED("CGridFluidSolver::generateCurFluidDensity"); }
-  CCellCenteredScalarField getFluidDomainField() const { RT_NOT_RESTATED("CGridFluidSolver::getFluidDomainField"); }
+  // GridFluidSolver.cpp:551-555: the box into the fluid-domain field
+  void generateFluidDomainFromBBox(Vector3 mn, Vector3 mx) {
+    int rr[3] = {m_R.x, m_R.y, m_R.z};
+    float oo[3] = {m_O.x, m_O.y, m_O.z}, hh[3] = {m_H.x, m_H.y, m_H.z};
+    float a[3] = {mn.x, mn.y, mn.z}, b[3] = {mx.x, mx.y, mx.z};
+    std::vector<float> d((size_t)m_R.x * m_R.y * m_R.z);
+    RT_TOUCH;
+    orc_fluid_domain_from_bbox(rr, oo, hh, a, b, d.data());
+    orc_solver_set_fluid_domain(m_S.get(), d.data());
+  }
+  CCellCenteredScalarField getFluidDomainField() const {
+    CCellCenteredScalarField f(m_R, m_O, m_H);
+    RT_TOUCH;
+    orc_solver_get_fluid_domain(m_S.get(), f.getGridDataGPUPtr());
+    return f;
+  }
   CCellCenteredScalarField getFluidDensityField() const { RT_NOT_RESTATED("CGridFluidSolver::getFluidDensityField"); }
   CCellCenteredScalarField getFluidSDFField() const { RT_NOT_RESTATED("CGridFluidSolver::getFluidSDFField"); }
   std::shared_ptr<CPressureSolver> getPressureSolver() const { RT_NOT_RESTATED("CGridFluidSolver::getPressureSolver"); }
@@ -986,6 +1013,72 @@ class CGridFluidSolver {
   std::shared_ptr<void> m_S;
 };
 
+// ---------------------------------------------- the hybrid coupler's helpers
+// EulerSolverTool.cu:787-810
+inline void buildFluidDensityInvoker(const CCellCenteredScalarField& dom, const CCellCenteredScalarField& solid,
+                                     CCellCenteredScalarField& out) {
+  int r[3]; float o[3], h[3];
+  dom.geom(r, o, h);
+  out.setGridParameters(dom.getResolution(), dom.getOrigin(), dom.getSpacing());
+  RT_TOUCH;
+  orc_build_fluid_density(r, dom.getConstGridDataGPUPtr(), solid.getConstGridDataGPUPtr(), out.getGridDataGPUPtr());
+}
+// HybridSimulatorBuildSDF.cu:177-238
+inline void buildFluidSideSDF(const CCellCenteredScalarField& density, const CCellCenteredScalarField& solid,
+                              CCellCenteredScalarField& out, UInt distance, int outside) {
+  int r[3]; float o[3], h[3];
+  density.geom(r, o, h);
+  RT_TOUCH;
+  orc_build_fluid_side_sdf(r, density.getConstGridDataGPUPtr(), solid.getConstGridDataGPUPtr(), outside,
+                           (int)distance, out.getGridDataGPUPtr());
+}
+inline void buildFluidOutsideSDFInvoker(const CCellCenteredScalarField& density, const CCellCenteredScalarField& solid,
+                                        CCellCenteredScalarField& out, UInt distance) {
+  buildFluidSideSDF(density, solid, out, distance, 1);
+}
+inline void buildFluidInsideSDFInvoker(const CCellCenteredScalarField& density, const CCellCenteredScalarField& solid,
+                                       CCellCenteredScalarField& out, UInt distance) {
+  buildFluidSideSDF(density, solid, out, distance, 0);
+}
+// HybridSimulatorBuildSDF.cu:240-266
+inline void buildMixedFluidOutsideSDFInvoker(const CCellCenteredScalarField& gridDensity,
+                                             const CCellCenteredScalarField& mixedDensity,
+                                             const CCellCenteredScalarField& gridOutside,
+                                             CCellCenteredScalarField& out) {
+  int r[3]; float o[3], h[3];
+  gridDensity.geom(r, o, h);
+  RT_TOUCH;
+  orc_build_mixed_fluid_outside_sdf(r, gridDensity.getConstGridDataGPUPtr(), mixedDensity.getConstGridDataGPUPtr(),
+                                    gridOutside.getConstGridDataGPUPtr(), out.getGridDataGPUPtr());
+}
+// HybridSimulatorMixFieldWithDensity.cu:128-265: scalar, cell vector (each
+// component with the same cell weights) and face vector fields
+inline void mixFieldWithDensityInvoker(const CCellCenteredScalarField& a, CCellCenteredScalarField& b,
+                                       const CCellCenteredScalarField& wa, const CCellCenteredScalarField& wb) {
+  const Vector3i r = a.getResolution();
+  RT_TOUCH;
+  orc_mix_field_with_density_cc((long long)r.x * r.y * r.z, a.getConstGridDataGPUPtr(), b.getGridDataGPUPtr(),
+                                wa.getConstGridDataGPUPtr(), wb.getConstGridDataGPUPtr());
+}
+inline void mixFieldWithDensityInvoker(const CCellCenteredVectorField& a, CCellCenteredVectorField& b,
+                                       const CCellCenteredScalarField& wa, const CCellCenteredScalarField& wb) {
+  const Vector3i r = a.getResolution();
+  const long long n = (long long)r.x * r.y * r.z;
+  RT_TOUCH;
+  for (int k = 0; k < 3; ++k)
+    orc_mix_field_with_density_cc(n, a.comp(k).data(), b.comp(k).data(), wa.getConstGridDataGPUPtr(),
+                                  wb.getConstGridDataGPUPtr());
+}
+inline void mixFieldWithDensityInvoker(const CFaceCenteredVectorField& a, CFaceCenteredVectorField& b,
+                                       const CCellCenteredScalarField& wa, const CCellCenteredScalarField& wb) {
+  int r[3]; float o[3], h[3];
+  wa.geom(r, o, h);
+  RT_TOUCH;
+  orc_mix_field_with_density_fc(r, a.comp(0).data(), a.comp(1).data(), a.comp(2).data(), b.comp(0).data(),
+                                b.comp(1).data(), b.comp(2).data(), wa.getConstGridDataGPUPtr(),
+                                wb.getConstGridDataGPUPtr());
+}
+
 // particle advection solvers handed to CGridFluidSolver by the frame tests
 struct CParticleAdvectionStub {
   template <class... A> void resizeParticleInCell(A&&...) {}
@@ -999,7 +1092,6 @@ struct CMixPICAndFLIP : CParticleAdvectionStub {};
 typedef std::shared_ptr<CParticleInCell> ParticleInCellSolverPtr;
 typedef std::shared_ptr<CFluidImplicitParticle> FluidImplicitParticleSolverPtr;
 typedef std::shared_ptr<CMixPICAndFLIP> MixPICAndFLIPSolverPtr;
-template <class... A> inline void buildFluidInsideSDFInvoker(A&&...) { RT_NOT_RESTATED("buildFluidInsideSDFInvoker"); }
 
 // --------------------------------------------------------- CUDA context
 class CCudaContextManager {

@@ -423,6 +423,57 @@ def test_fluid_density_bit_exact(cuda):
     assert set(np.unique(ref)) <= {0.0, np.float32(0.2), 1.0}
 
 
+def _density_case(seed, res):
+    """A fluid density of the reference's buildFluidDensity (oracle) over a
+    blocky fluid domain with scattered solid cells."""
+    rng = np.random.default_rng(seed)
+    dom = np.where(rng.random(res[::-1]) < 0.15, -500.0, 500.0).astype(np.float32)
+    dom[:, : res[1] // 2, : res[0] * 2 // 3] = -500.0
+    solid = np.where(rng.random(res[::-1]) < 0.05, -1.0, np.finfo(np.float32).max).astype(np.float32)
+    solid[0], solid[-1] = -1.0, -1.0
+    return oracle.build_fluid_density(res, dom, solid), solid
+
+
+@pytest.mark.parametrize("outside", [False, True])
+def test_fluid_side_sdf_bit_exact(cuda, outside):
+    """buildFluidInsideSDF / buildFluidOutsideSDF of the hybrid coupler
+    (HybridSimulatorBuildSDF.cu:4-146,177-238): the frontier BFS gives the
+    reference's swept shells exactly, with the invokers' 1000 sweeps, a short
+    sweep count that leaves cells UNKNOWN, and 0 sweeps (clamp only)."""
+    res = (29, 21, 17)
+    density, solid = _density_case(70 + outside, res)
+    op = hfgrid.op_build_fluid_outside_sdf if outside else hfgrid.op_build_fluid_inside_sdf
+    for distance in (1000, 3):
+        out = torch.empty(res[::-1], dtype=torch.float32, device=cuda)
+        op(res, dev(density), dev(solid), out, distance)
+        ref = oracle.build_fluid_side_sdf(res, density, solid, outside, distance)
+        assert np.array_equal(host(out), ref)
+        if distance == 3:
+            assert (ref == np.finfo(np.float32).max).any(), "3 sweeps should leave far cells UNKNOWN"
+        else:
+            assert ref.max() > 3
+    start = np.random.default_rng(72).standard_normal(res[::-1]).astype(np.float32)
+    out = dev(start)
+    op(res, dev(density), dev(solid), out, 0)
+    assert np.array_equal(host(out), oracle.build_fluid_side_sdf(res, density, solid, outside, 0, out=start))
+
+
+def test_mixed_fluid_outside_sdf_bit_exact(cuda):
+    """buildMixedFluidOutsideSDF (HybridSimulatorBuildSDF.cu:139-175): 0.5 -
+    mixed density at surface cells (negative -> 0), the grid's outside SDF
+    elsewhere."""
+    res = (23, 19, 13)
+    density, solid = _density_case(73, res)
+    grid_out = oracle.build_fluid_side_sdf(res, density, solid, True, 1000)
+    mixed = (density + np.random.default_rng(74).random(res[::-1]).astype(np.float32)).astype(np.float32)
+    out = torch.empty(res[::-1], dtype=torch.float32, device=cuda)
+    hfgrid.op_build_mixed_fluid_outside_sdf(res, dev(density), dev(mixed), dev(grid_out), out)
+    ref = oracle.build_mixed_fluid_outside_sdf(res, density, mixed, grid_out)
+    assert np.array_equal(host(out), ref)
+    surf = density == np.float32(0.2)
+    assert surf.any() and (ref[surf] == 0).any() and (ref[surf] > 0).any()
+
+
 def test_mix_field_with_density(cuda):
     """mixFieldWithDensity (HybridSimulatorMixFieldWithDensity.cu): cell and
     face grids, zero total weight leaves B unchanged."""

@@ -13,7 +13,9 @@ tests/golden/reference_replay.json.
 This pins the oracle -- the checker of every GPU parity test -- for the
 particle and advection half of the step (P2G, G2P, CFL particle advection,
 markers, binning, back-trace and semi-Lagrangian advection, trilinear and
-cubic sampling, boundaries) as well as the pressure and extrapolation half.
+cubic sampling, boundaries) as well as the pressure and extrapolation half,
+and the hybrid coupler's helpers that follow the step (field mixing, fluid
+density, inside / outside distance fields).
 
 test_replay_record checks the committed record; the live tests rebuild and
 rerun the replay when HFG_REFERENCE_ROOT names a reference checkout.
@@ -40,6 +42,10 @@ FLOORS = {
     "ParticlesAdvection": 2000, "SemiLagrangian": 70000, "BoundarySDF": 14000, "ExternalForces": 190000,
     "Extrapolation": 1000, "PressureSolver": 1300, "GridFluidSolver": 800, "CellCenteredScalarField": 9000,
     "CellCenteredVectorField": 20000, "FaceCenteredVectorField": 9000,
+    # the hybrid coupler's helpers (UnitTest-HybridHelper.cu: field mixing,
+    # the fluid domain from a box, fluid density and the inside / outside
+    # distance fields)
+    "HybridHelper": 850,
 }
 
 # Tests of those sources that are not replayed, and why.
