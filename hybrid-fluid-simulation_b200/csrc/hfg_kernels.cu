@@ -1537,9 +1537,12 @@ __global__ void kP2GFaceLinear(Geom g, const float* __restrict__ pos, const floa
         vx[k] = w[k] * val;
         vw[k] = w[k];
       }
-      // lanes with the same clamped floor entries (AxisW::j, which fix both
-      // corners of an axis) share all eight corners; the key is the index of
-      // those entries in a grid one larger per axis (< 2^31)
+      // lanes with the same clamped floor indices (AxisW::j, -1 .. n - 1, which
+      // fix both corners of an axis) share all eight corners; the key is
+      // their linear index in a grid one larger per axis, less a constant, in
+      // 32-bit unsigned arithmetic: distinct triples give distinct keys, and
+      // the keys that wrap below zero land above 2^32 - 2^31, never on a dead
+      // lane's 0x80000000 | lane
       const AxisW& X = a == 0 ? fs.fc[0] : fs.cc[0];
       const AxisW& Y = a == 1 ? fs.fc[1] : fs.cc[1];
       const AxisW& Z = a == 2 ? fs.fc[2] : fs.cc[2];
