@@ -237,6 +237,19 @@ struct FaceSampler {
   // the same sampler from the constants of a corner-table set: one FMA per
   // coordinate (the two forms round alike up to the last bit), and the
   // coordinate clamped to [-1, n) before the floor (clampedAxis)
+  // The same with the integer index clamps of axisWeights (same corners and
+  // weights at every finite point): in the G2P kernel, which also forms the
+  // corner indices of the FLIP difference, this form is the faster one
+  // (1.03 against 1.19 ms per 256^3 step).
+  struct IndexClamp {};
+  __device__ __forceinline__ FaceSampler(const FaceQuads& q, float px, float py, float pz, IndexClamp) {
+    const float p[3] = {px, py, pz};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      axisWeights(fmaf(p[k], q.inv[k], q.offC[k]), q.jC[k] + 1, cc[k]);
+      axisWeights(fmaf(p[k], q.inv[k], q.offF[k]), q.jF[k] + 1, fc[k]);
+    }
+  }
   __device__ __forceinline__ FaceSampler(const FaceQuads& q, float px, float py, float pz) {
     const float p[3] = {px, py, pz};
 #pragma unroll

@@ -1137,7 +1137,7 @@ __global__ void kParticleVelUpdateLinear(Geom g, int mode, FaceQuads vinQ, Const
       prefetchL2(pos + 3 * (p + stride));
       prefetchL2(vel + 3 * (p + stride));
     }
-    FaceSampler fs(vinQ, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]);
+    FaceSampler fs(vinQ, pos[3 * p], pos[3 * p + 1], pos[3 * p + 2], FaceSampler::IndexClamp{});
     float pic[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
