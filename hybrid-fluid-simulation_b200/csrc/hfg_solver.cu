@@ -480,7 +480,12 @@ bool GridSolver::advectBegin() {
   }
   if (P_ <= 0) throw CudaError("particle advection needs particles", HFG_ERR_STATE);
   stageBegin(1);
-  if (opt_.sort_interval > 0 && particleSteps_ > 0 && particleSteps_ % opt_.sort_interval == 0) sortParticles();
+  if (opt_.sort_interval > 0) {
+    // the sort's buffers are taken at the first particle step, not at the
+    // first sort: growing the allocator's pool by about 1 GB can take 0.2 s
+    reserveSortScratch();
+    if (particleSteps_ > 0 && particleSteps_ % opt_.sort_interval == 0) sortParticles();
+  }
   ++particleSteps_;
   ConstFaceField prev{{prev_[0].p, prev_[1].p, prev_[2].p}};
   int mode = adv_ == HFG_ADV_PIC ? MODE_PIC : (adv_ == HFG_ADV_FLIP ? MODE_FLIP : MODE_MIX);
@@ -502,13 +507,9 @@ bool GridSolver::advectBegin() {
 // The particles in cell order (hfg_sort.cu), with their velocities and
 // carried colour / domain values.  v at the substep start is not carried: each
 // step's velocity update writes it before the substeps read it.
-void GridSolver::sortParticles() {
-  if (P_ <= 0) return;
-  // With clamp_mode 1 the boundary fix reaches only the first min(N, P)
-  // particles, as the reference's launch does (EulerParticlesTool.cu:880):
-  // those stay the first ones, each group sorted within its own range.
-  const long long split = (opt_.clamp_mode == 1 && P_ > N_) ? N_ : 0;
-  finishMirrorCopy();
+// The sort's keys, values, digit counts and gather buffer for P_ particles
+// (no-ops once they have that size).
+void GridSolver::reserveSortScratch() {
   for (int i = 0; i < 2; ++i) {
     sortKey_[i].alloc(P_, stream_);
     sortVal_[i].alloc(P_, stream_);
@@ -516,11 +517,21 @@ void GridSolver::sortParticles() {
   const long long entries = sortCountEntries(P_);
   sortCounts_.alloc(entries, stream_);
   sortSums_.alloc(sortScanBlocks(entries), stream_);
+  sortTmp_.alloc(3 * P_, stream_);
+}
+
+void GridSolver::sortParticles() {
+  if (P_ <= 0) return;
+  // With clamp_mode 1 the boundary fix reaches only the first min(N, P)
+  // particles, as the reference's launch does (EulerParticlesTool.cu:880):
+  // those stay the first ones, each group sorted within its own range.
+  const long long split = (opt_.clamp_mode == 1 && P_ > N_) ? N_ : 0;
+  finishMirrorCopy();
+  reserveSortScratch();
   const SortScratch sc{sortKey_[0].p, sortKey_[1].p, sortVal_[0].p, sortVal_[1].p, sortCounts_.p, sortSums_.p};
   const unsigned int* perm = nullptr;
   launched(launchSortPermutation(g_, ppos_.p, P_, split, sc, &perm, stream_), "particle sort",
            sortPassesLaunches(N_, split > 0));
-  sortTmp_.alloc(3 * P_, stream_);
   for (DArray<float>* a : {&ppos_, &pvel_, &pvector_}) {
     if (!a->p || a->n != (size_t)(3 * P_)) continue;
     launched(launchGather(a->p, 3, perm, P_, sortTmp_.p, stream_), "particle gather");

@@ -145,6 +145,7 @@ class GridSolver {
   void setParticleMirror(float* pos, float* vel, long long capacity);
   // Reorders the particles (and their carried values) by cell, stable.
   void sortParticles();
+  void reserveSortScratch();
   void getStats(hfg_stats_t* st);
   void synchronize();
   float timeCg(int iters);
