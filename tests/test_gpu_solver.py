@@ -381,6 +381,32 @@ def test_step_with_no_fluid(cuda, precond):
         assert np.isfinite(v[v != U]).all()
 
 
+@pytest.mark.parametrize("kind", [hfgrid.ADV_SEMI_LAGRANGIAN, hfgrid.ADV_MIX_PIC_FLIP])
+@pytest.mark.parametrize("precond", [hfgrid.PRECOND_IDENTITY, hfgrid.PRECOND_JACOBI, hfgrid.PRECOND_MG])
+def test_step_with_fluid_everywhere(cuda, precond, kind):
+    """The other end from test_step_with_no_fluid: every non-solid cell is
+    fluid, so the pressure system has no air (Dirichlet) cell and the
+    extrapolation has nothing left to fill.  The right-hand side is
+    consistent, the CG converges, and the pressure holds the fluid at rest
+    against gravity: velocities stay at the FP32 noise level (the FP64
+    oracle's are ~1e-7), markers equal the oracle's, particles stay put."""
+    sc = scenes.Scene(res=(14, 12, 10), fluid_max=(1.0, 1.0, 1.0), seed=2)
+    g = scenes.gpu_solver(sc, precond=precond, tol_mode=1, tol=1e-6, max_iter=400, kind=kind)
+    o = oracle_twin(sc, g, 1, 1, 1, 1e-10, 2000, kind=kind, scalars=False)
+    pos0 = g.particles()[0] if kind != hfgrid.ADV_SEMI_LAGRANGIAN else None
+    for _ in range(2):
+        g.update()
+        o.update()
+        assert g.stats()["cg_converged"] == 1
+    assert np.array_equal(g.markers(), o.markers())
+    assert (g.markers() == 1).sum() == (o.markers() != 2).sum()
+    for a in g.velocity_field():
+        known = a[a != U]
+        assert np.isfinite(known).all() and np.abs(known).max() < 1e-3
+    if pos0 is not None:
+        assert np.abs(g.particles()[0] - pos0).max() < 1e-4
+
+
 def test_semi_lagrangian_solver_catmull_rom(cuda):
     """The solver in semi-Lagrangian mode with the Catmull-Rom sampler
     (setSamplingAlg) against the FP64 oracle with the same sampler."""
