@@ -458,7 +458,73 @@ def test_fluid_side_sdf_bit_exact(cuda, outside):
     assert np.array_equal(host(out), oracle.build_fluid_side_sdf(res, density, solid, outside, 0, out=start))
 
 
-def test_mixed_fluid_outside_sdf_bit_exact(cuda):
+def _shell_index(v, seed, passable, seeds):
+    """Shell k of every value k + seed (formed in double, rounded to float as
+    the reference does); seeds 0, unreached or other cells -1."""
+    k = np.full(v.shape, -1, np.int32)
+    near = np.rint(v.astype(np.float64) - seed)
+    ok = passable & (v != np.finfo(np.float32).max) & (near >= 1)
+    ok &= v == (near + seed).astype(np.float32)
+    k[ok] = near[ok].astype(np.int32)
+    k[seeds] = 0
+    return k
+
+
+def _neighbour_extremes(k):
+    """Min and max of the six clamp-to-edge neighbours' shells, over the
+    neighbours that hold one (k >= 0)."""
+    big = np.int32(1 << 30)
+    lo = np.where(k >= 0, k, big)
+    hi = k.copy()
+    p_lo, p_hi = np.pad(lo, 1, mode="edge"), np.pad(hi, 1, mode="edge")
+    mn = np.full(k.shape, big, np.int32)
+    mx = np.full(k.shape, -1, np.int32)
+    for axis in range(3):
+        for d in (-1, 1):
+            sl = [slice(1, -1)] * 3
+            sl[axis] = slice(1 + d, p_lo.shape[axis] - 1 + d)
+            mn = np.minimum(mn, p_lo[tuple(sl)])
+            mx = np.maximum(mx, p_hi[tuple(sl)])
+    return mn, mx
+
+
+@pytest.mark.parametrize("outside", [False, True])
+def test_fluid_side_sdf_properties_256(cuda, outside):
+    """The inside / outside distance fields at the benchmark's size (the
+    256^3 dam break's fluid density, solids included), by the properties
+    that define a breadth-first distance: every reached cell has a
+    neighbour exactly one shell nearer the surface and none nearer than
+    that, and no unreached cell touches a shell short of the sweep limit."""
+    import scenes
+    sc = scenes.dam_break_256()
+    res = sc.res
+    dom = oracle.fluid_domain_from_bbox(res, sc.origin, sc.spacing, *scenes.fluid_bbox(sc))
+    solid = scenes.total_solid(sc)
+    rho = torch.empty(res[::-1], dtype=torch.float32, device=cuda)
+    hfgrid.op_build_fluid_density(res, dev(dom), dev(solid), rho)
+    out = torch.empty_like(rho)
+    op = hfgrid.op_build_fluid_outside_sdf if outside else hfgrid.op_build_fluid_inside_sdf
+    distance = 1000
+    op(res, rho, dev(solid), out, distance)
+    density, v = host(rho), host(out)
+    open_ = solid >= 0
+    seeds = open_ & (density == np.float32(0.2))
+    # the sweeps grow into the air (outside) or the fluid's interior (inside)
+    passable = open_ & (density == (np.float32(0.0) if outside else np.float32(1.0)))
+    U = np.finfo(np.float32).max
+    # cells that are neither seeds nor passable hold 0; seeds hold max(seed, 0)
+    seed = 0.5 - 0.2 if outside else 0.2 - 0.5
+    assert (v[~(seeds | passable)] == 0).all()
+    assert (v[seeds] == np.float32(max(seed, 0.0))).all() and seeds.any()
+    k = _shell_index(v, seed, passable, seeds)
+    reached = passable & (v != U)
+    assert (k[reached] >= 1).all(), "a reached cell holds a value that is no shell"
+    mn, mx = _neighbour_extremes(k)
+    assert (mn[reached] == k[reached] - 1).all()
+    unreached = passable & (v == U)
+    assert not (mn[unreached] < distance - 1).any()
+    assert k.max() > 10  # the shells reach well into the domain
+
     """buildMixedFluidOutsideSDF (HybridSimulatorBuildSDF.cu:139-175): 0.5 -
     mixed density at surface cells (negative -> 0), the grid's outside SDF
     elsewhere."""
