@@ -71,6 +71,9 @@ def parse():
     ap.add_argument("--mg-smooth", type=int, default=0, help="multigrid smoothing sweeps per level (0: library default)")
     ap.add_argument("--pressure-fp64", action="store_true",
                     help="accumulate the pressure in FP64 (divergence follows the CG residual)")
+    ap.add_argument("--autotune", type=int, default=0, choices=[0, 1],
+                    help="dam-break: 1 times the CG launch shapes at the first solve and keeps the fastest "
+                         "(option autotune; done in the warm-up)")
     ap.add_argument("--sort-interval", type=int, default=0,
                     help="dam-break / moving-boxes: reorder the particles by cell every k steps (0: never)")
     ap.add_argument("--clamp-mode", type=int, default=None, choices=[0, 1],
@@ -665,7 +668,7 @@ def run_dam_break(args):
     opts = dict(precond=precond, tol_mode=hfgrid.TOL_RELATIVE, tol=1e-6, max_iter=200, advect_scalars=0,
                 clamp_mode=clamp_mode(args), pressure_fp64=int(args.pressure_fp64),
                 mg_smooth=args.mg_smooth, mg_half=args.mg_half,
-                sort_interval=args.sort_interval)
+                sort_interval=args.sort_interval, autotune=args.autotune)
 
     def warm_solver():
         """A solver in the state the timed steps start from: seeded, W steps in."""
@@ -801,7 +804,7 @@ def run_dam_break(args):
                                    f"{args.precond}-PCG rel 1e-6 max 200", "res": [args.res] * 3,
                        "cells": N, "particles": n, "l2": "state > L2 (no flush needed)",
                        "parallelism": f"replicas x{world}", "particle_sort_interval": args.sort_interval,
-                       "clamp_mode": clamp_mode(args),
+                       "cg_autotune": args.autotune, "clamp_mode": clamp_mode(args),
                        "mg_half": args.mg_half if args.precond == "mg" else None,
                        "convergence_one_more_step": conv,
                        "stage_ms_one_more_step": stage_ms, "particle_ms_one_more_step": particle_ms},
